@@ -1,0 +1,165 @@
+"""Seeded synthetic SDP instances in SDPA format, and the .dat-s writer.
+
+The instance families are the workloads this solver is measured on:
+
+* MaxCut relaxation of an Erdos-Renyi graph G(n, p): one n x n block,
+  c = 1_m, F0 = L/4 (L the weighted graph Laplacian), F_i = e_i e_i^T.  In
+  SDPA's dual form this is  max (L/4).Y  s.t. Y_ii = 1, Y psd.
+* Lovasz theta of G(n, p): one n x n block, m = 1 + |E|, c = (1, 0, ..., 0),
+  F0 = J (all ones), F1 = I, one F_k = E_ij per edge (upper entry 1).
+* Random strictly feasible SDP: a dense n-block plus an LP block; every A_i
+  has floor(density * n(n+1)/2) upper-triangle N(0,1) entries at uniformly
+  chosen positions plus one LP diagonal entry; b_i = Tr(A_i) so X0 = I is
+  feasible, C = sum_i y0_i A_i + I with y0 ~ N(0,1) so Z0 = I is feasible
+  (file F0 = -C, c = b).
+* Batched MaxCut: per seed s, n ~ U{20..120}, p ~ U(0.05, 0.3), edge weights
+  U(0, 1).  Warm-start sets use n ~ U{50..200}.
+
+Indices in an `Instance` are 1-based exactly as in a .dat-s file (block l,
+row i <= column j; k = 0 is F0).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Instance:
+    m: int
+    blocks: list          # signed block sizes as in the file (negative = LP)
+    c: np.ndarray         # (m,) float64
+    k: np.ndarray         # (nnz,) int32, matrix index 0..m
+    l: np.ndarray         # (nnz,) int32, 1-based block
+    i: np.ndarray         # (nnz,) int32, 1-based row    (i <= j)
+    j: np.ndarray         # (nnz,) int32, 1-based column
+    v: np.ndarray         # (nnz,) float64
+    name: str = ""
+
+    def to_dats(self) -> str:
+        """SDPA sparse format text (the reader is IO::read, sdpa_io.cpp:33-73, :473-540)."""
+        out = [f'"{self.name or "sdpa_b200 instance"}"',
+               f"{self.m} = mDIM", f"{len(self.blocks)} = nBLOCK",
+               " ".join(str(int(b)) for b in self.blocks) + " = bLOCKsTRUCT",
+               " ".join(repr(float(x)) for x in self.c)]
+        order = np.lexsort((self.j, self.i, self.l, self.k))
+        for q in order:
+            out.append(f"{int(self.k[q])} {int(self.l[q])} {int(self.i[q])} {int(self.j[q])} "
+                       f"{float(self.v[q])!r}")
+        return "\n".join(out) + "\n"
+
+    def write(self, path: str) -> None:
+        with open(path, "w") as f:
+            f.write(self.to_dats())
+
+
+def _gnp_edges(n: int, p: float, rng: np.random.Generator):
+    iu, ju = np.triu_indices(n, 1)
+    keep = rng.random(iu.size) < p
+    return iu[keep], ju[keep]
+
+
+def maxcut_from_graph(n: int, ei: np.ndarray, ej: np.ndarray, w: np.ndarray, name: str = "") -> Instance:
+    """MaxCut SDP relaxation of a weighted graph (edges 0-based, ei < ej)."""
+    deg = np.zeros(n)
+    np.add.at(deg, ei, w)
+    np.add.at(deg, ej, w)
+    # F0 = L/4: diagonal deg/4, off-diagonal -w/4 (upper triangle only)
+    dk = np.zeros(n, np.int32)
+    di = np.arange(1, n + 1, dtype=np.int32)
+    ok = deg != 0.0
+    k = [dk[ok], np.zeros(ei.size, np.int32), np.arange(1, n + 1, dtype=np.int32)]
+    ii = [di[ok], (ei + 1).astype(np.int32), di]
+    jj = [di[ok], (ej + 1).astype(np.int32), di]
+    vv = [deg[ok] / 4.0, -w / 4.0, np.ones(n)]
+    return Instance(m=n, blocks=[n], c=np.ones(n), k=np.concatenate(k),
+                    l=np.ones(sum(a.size for a in k), np.int32), i=np.concatenate(ii),
+                    j=np.concatenate(jj), v=np.concatenate(vv), name=name)
+
+
+def maxcut(n: int = 100, p: float = 0.1, seed: int = 1, unit_weights: bool = True) -> Instance:
+    """MaxCut of G(n, p) from `seed` (numpy default_rng)."""
+    rng = np.random.default_rng(seed)
+    ei, ej = _gnp_edges(n, p, rng)
+    w = np.ones(ei.size) if unit_weights else rng.uniform(0.0, 1.0, ei.size)
+    return maxcut_from_graph(n, ei, ej, w, name=f"maxcut G({n},{p}) seed {seed}")
+
+
+def batch_maxcut_params(seed: int, nmin: int = 20, nmax: int = 120):
+    """(n, p, rng) of one batched-MaxCut instance: n ~ U{nmin..nmax}, p ~ U(0.05, 0.3)."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(nmin, nmax + 1))
+    p = float(rng.uniform(0.05, 0.3))
+    return n, p, rng
+
+
+def batch_maxcut_graph(seed: int, nmin: int = 20, nmax: int = 120):
+    """The weighted graph (n, ei, ej, w) of one batched-MaxCut instance."""
+    n, p, rng = batch_maxcut_params(seed, nmin, nmax)
+    ei, ej = _gnp_edges(n, p, rng)
+    w = rng.uniform(0.0, 1.0, ei.size)
+    return n, ei, ej, w
+
+
+def batch_maxcut(seed: int, nmin: int = 20, nmax: int = 120) -> Instance:
+    n, ei, ej, w = batch_maxcut_graph(seed, nmin, nmax)
+    return maxcut_from_graph(n, ei, ej, w, name=f"batched maxcut seed {seed}")
+
+
+def lovasz_theta(n: int = 200, p: float = 0.5, seed: int = 1) -> Instance:
+    """Lovasz theta SDP of G(n, p) from `seed`."""
+    rng = np.random.default_rng(seed)
+    ei, ej = _gnp_edges(n, p, rng)
+    ne = ei.size
+    m = 1 + ne
+    iu, ju = np.triu_indices(n)
+    k = np.concatenate([np.zeros(iu.size, np.int32), np.ones(n, np.int32),
+                        np.arange(2, m + 1, dtype=np.int32)])
+    ii = np.concatenate([iu + 1, np.arange(1, n + 1), ei + 1]).astype(np.int32)
+    jj = np.concatenate([ju + 1, np.arange(1, n + 1), ej + 1]).astype(np.int32)
+    v = np.concatenate([np.ones(iu.size), np.ones(n), np.ones(ne)])
+    c = np.zeros(m)
+    c[0] = 1.0
+    return Instance(m=m, blocks=[n], c=c, k=k, l=np.ones(k.size, np.int32), i=ii, j=jj, v=v,
+                    name=f"lovasz theta G({n},{p}) seed {seed}")
+
+
+def random_sdp(m: int = 2000, n: int = 500, nlp: int = 50, density: float = 0.01,
+               lp_per_constraint: int = 1, seed: int = 1) -> Instance:
+    """Random strictly feasible SDP with blocks {n, -nlp} (see module doc)."""
+    rng = np.random.default_rng(seed)
+    ntri = n * (n + 1) // 2
+    per = int(np.floor(density * ntri))
+    iu, ju = np.triu_indices(n)
+    ks, ls, is_, js, vs = [], [], [], [], []
+    C = np.zeros((n, n))
+    Clp = np.ones(nlp)
+    C[np.diag_indices(n)] = 1.0
+    y0 = rng.standard_normal(m)
+    b = np.zeros(m)
+    for a in range(m):
+        pos = rng.choice(ntri, size=per, replace=False)
+        val = rng.standard_normal(per)
+        r, s = iu[pos], ju[pos]
+        lpi = rng.choice(nlp, size=lp_per_constraint, replace=False)
+        lpv = rng.standard_normal(lp_per_constraint)
+        ks += [np.full(per + lp_per_constraint, a + 1, np.int32)]
+        ls += [np.concatenate([np.ones(per, np.int32), np.full(lp_per_constraint, 2, np.int32)])]
+        is_ += [np.concatenate([r + 1, lpi + 1]).astype(np.int32)]
+        js += [np.concatenate([s + 1, lpi + 1]).astype(np.int32)]
+        vs += [np.concatenate([val, lpv])]
+        b[a] = val[r == s].sum() + lpv.sum()
+        np.add.at(C, (r, s), y0[a] * val)
+        off = r != s
+        np.add.at(C, (s[off], r[off]), y0[a] * val[off])
+        np.add.at(Clp, lpi, y0[a] * lpv)
+    # file F0 = -C (upper triangle, dense) and the LP part
+    ks.insert(0, np.zeros(ntri + nlp, np.int32))
+    ls.insert(0, np.concatenate([np.ones(ntri, np.int32), np.full(nlp, 2, np.int32)]))
+    is_.insert(0, np.concatenate([iu + 1, np.arange(1, nlp + 1)]).astype(np.int32))
+    js.insert(0, np.concatenate([ju + 1, np.arange(1, nlp + 1)]).astype(np.int32))
+    vs.insert(0, np.concatenate([-C[iu, ju], -Clp]))
+    return Instance(m=m, blocks=[n, -nlp], c=b, k=np.concatenate(ks), l=np.concatenate(ls),
+                    i=np.concatenate(is_), j=np.concatenate(js), v=np.concatenate(vs),
+                    name=f"random sdp m={m} n={n} lp={nlp} seed {seed}")
