@@ -1,0 +1,160 @@
+/* sdpa_b200 C ABI: the drop-in boundary of the B200 SDP solver.
+ *
+ * Plain C types only (no C++ or torch types), int status codes (0 = success,
+ * negative = error; see SDPAB_E*), explicit CUDA stream handles passed as
+ * void*.  Two families:
+ *
+ *  1. Whole-problem handle API mirroring the reference's public C++ class
+ *     SDPA (sdpa_call.h:91-267): create, read .dat-s / parameter files or
+ *     input elements, initializeSolve, solve, result getters.  The C++ class
+ *     of the same shape is declared in sdpa_call.h of this directory; these
+ *     functions are its C binding for FFI callers (ctypes, MEX, cgo ...).
+ *
+ *  2. Batched API: thousands of single-block SDPs solved by one persistent
+ *     kernel launch (no counterpart in the reference, which solves one problem
+ *     per process; its per-problem semantics are those of SDPA::solve,
+ *     sdpa_solve.cpp:59-233).
+ *
+ * Index conventions of the batched API: entries are 0-based (row, col) with
+ * row <= col (upper triangle, as SDPA stores them, sdpa_struct.h:82-139);
+ * matrix 0 of an instance is F0 as written in the .dat-s file (the solver
+ * negates it to C = -F0 like IO::setElement, sdpa_io.cpp:511), matrices
+ * 1..m are F_1..F_m.  Results follow the reference's getters: xvec is
+ * getResultXVec (sdpa_call.cpp:668-671), X is getResultXMat (the solver's
+ * internal Z, :673-694), Y is getResultYMat (internal X, :696-717),
+ * primal/dual objectives are getPrimalObj / getDualObj (:719-729), phase is
+ * getPhaseValue's code (:769-786).
+ */
+#ifndef SDPA_B200_H
+#define SDPA_B200_H
+
+#if defined(__GNUC__)
+#define SDPAB_API __attribute__((visibility("default")))
+#else
+#define SDPAB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDPAB_OK 0
+#define SDPAB_EINVAL (-1)      /* invalid argument */
+#define SDPAB_ECUDA (-2)       /* CUDA runtime error (message via sdpab_last_error) */
+#define SDPAB_ESIZE (-3)       /* instance larger than the configured limits */
+#define SDPAB_ENODEV (-4)      /* no CUDA device */
+#define SDPAB_ESTATE (-5)      /* call out of order (e.g. solve before input) */
+#define SDPAB_EIO (-6)         /* file could not be opened or parsed */
+
+/* Phase codes: SDPA::PhaseType order (sdpa_call.h:95-96). */
+#define SDPAB_noINFO 0
+#define SDPAB_pFEAS 1
+#define SDPAB_dFEAS 2
+#define SDPAB_pdFEAS 3
+#define SDPAB_pdINF 4
+#define SDPAB_pFEAS_dINF 5
+#define SDPAB_pINF_dFEAS 6
+#define SDPAB_pdOPT 7
+#define SDPAB_pUNBD 8
+#define SDPAB_dUNBD 9
+
+/* Solver parameters, the ten numeric fields of the reference's Parameter
+ * (sdpa_parts.h; param.sdpa lines 1-10, read by Parameter::readFile,
+ * sdpa_parts.cpp:231-263). */
+typedef struct sdpab_params {
+  int maxIteration;
+  double epsilonStar, lambdaStar, omegaStar, lowerBound, upperBound;
+  double betaStar, betaBar, gammaStar, epsilonDash;
+} sdpab_params;
+
+/* Fills p with Parameter::setDefaultParameter(type) (sdpa_parts.cpp:182-224):
+ * 0 = PARAMETER_DEFAULT, 1 = UNSTABLE_BUT_FAST, 2 = STABLE_BUT_SLOW. */
+SDPAB_API int sdpab_default_params(int type, sdpab_params* p);
+
+/* Reads the ten numeric lines of a param.sdpa file
+ * (replaces Parameter::readFile, sdpa_parts.cpp:231-263). */
+SDPAB_API int sdpab_read_params(const char* path, sdpab_params* p);
+
+/* Last error message of the calling thread (static storage). */
+SDPAB_API const char* sdpab_last_error(void);
+
+/* Library version string. */
+SDPAB_API const char* sdpab_version(void);
+
+/* ---------------------------------------------------------------- batched API */
+
+/* Precision modes of the batched solver. */
+#define SDPAB_PREC_FP64 0    /* every step in FP64 (the plain path) */
+#define SDPAB_PREC_MIXED 1   /* FP32 bulk products and Schur factorisation with
+                                FP64 refinement, FP64 residuals/gap/step length,
+                                FP64 everywhere once mu < mixed_mu_switch */
+
+typedef struct sdpab_batch {
+  int count;                   /* number of instances */
+  int nmax, mmax;              /* upper bounds of n and m over the batch */
+  const int* n;                /* [count] order of the single SDP block */
+  const int* m;                /* [count] number of constraints */
+  const long long* vec_off;    /* [count] offset of the instance's b / xvec (m doubles) */
+  const double* b;             /* c vector of the .dat-s file (b of the internal problem) */
+  const long long* mat_off;    /* [count] offset into mat_ptr of the instance's m+2 pointers */
+  const long long* mat_ptr;    /* entry ranges: matrix k of instance i is
+                                  [mat_ptr[mat_off[i]+k], mat_ptr[mat_off[i]+k+1]) */
+  const int* row;              /* entries: 0-based row (row <= col) */
+  const int* col;              /* entries: 0-based column */
+  const double* val;           /* entries: value as written in the file */
+  const long long* dense_off;  /* [count] offset of the instance's n*n blocks in X / Y arrays */
+} sdpab_batch;
+
+typedef struct sdpab_batch_init {
+  const int* flag;             /* [count] nonzero: start from the given point */
+  const double* xvec;          /* x (vec_off layout), as SDPA::inputInitXVec */
+  const double* X;             /* user X (dense_off layout), as inputInitXMat */
+  const double* Y;             /* user Y (dense_off layout), as inputInitYMat */
+} sdpab_batch_init;
+
+typedef struct sdpab_batch_result {
+  double* xvec;                /* [vec_off layout] getResultXVec; may be NULL */
+  double* X;                   /* [dense_off layout] getResultXMat(1); may be NULL */
+  double* Y;                   /* [dense_off layout] getResultYMat(1); may be NULL */
+  double* primal_obj;          /* [count] getPrimalObj */
+  double* dual_obj;            /* [count] getDualObj */
+  double* mu;                  /* [count] getMu */
+  double* primal_error;        /* [count] getPrimalError */
+  double* dual_error;          /* [count] getDualError */
+  int* iterations;             /* [count] getIteration */
+  int* phase;                  /* [count] getPhaseValue code */
+  int* status;                 /* [count] 0 ok; 1 warm start not strictly interior
+                                  (standard start used); <0 instance rejected */
+} sdpab_batch_result;
+
+typedef struct sdpab_batch_config {
+  int precision;               /* SDPAB_PREC_FP64 or SDPAB_PREC_MIXED */
+  int ctas_per_sm;             /* resident solver blocks per SM (0 = auto) */
+  double mixed_mu_switch;      /* mixed mode: switch to FP64 below this mu (0 = 1e-6) */
+} sdpab_batch_config;
+
+/* Solves a batch whose arrays (problem, init, result) are all DEVICE pointers,
+ * asynchronously on `stream` (a cudaStream_t, NULL = default stream).
+ * `order` (device, optional) gives the processing order of the instances;
+ * largest-first balances the persistent schedule.  init may be NULL. */
+SDPAB_API int sdpab_batch_solve(const sdpab_batch* prob, const sdpab_batch_init* init,
+                      const sdpab_params* prm, const sdpab_batch_config* cfg,
+                      sdpab_batch_result* res, const int* order, void* stream);
+
+/* Same batch with HOST pointers: copies the inputs to the device, solves,
+ * copies the results back and synchronises.  The largest-first order is
+ * computed here. */
+SDPAB_API int sdpab_batch_solve_host(const sdpab_batch* prob, const sdpab_batch_init* init,
+                           const sdpab_params* prm, const sdpab_batch_config* cfg,
+                           sdpab_batch_result* res);
+
+/* Device memory the batched solver keeps between calls (workspace, staging). */
+SDPAB_API long long sdpab_workspace_bytes(void);
+/* Frees that memory on the current device. */
+SDPAB_API int sdpab_release_workspace(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SDPA_B200_H */

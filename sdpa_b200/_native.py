@@ -1,0 +1,102 @@
+"""ctypes binding of the C ABI in include/sdpa_b200.h (libsdpa_b200.so).
+
+The library is loaded from sdpa_b200/_lib/ only; there is no fallback: if the
+shared object is missing every solver entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_int, c_longlong, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libsdpa_b200.so")
+
+# status codes
+OK, EINVAL, ECUDA, ESIZE, ENODEV, ESTATE, EIO = 0, -1, -2, -3, -4, -5, -6
+PREC_FP64, PREC_MIXED = 0, 1
+PHASES = ["noINFO", "pFEAS", "dFEAS", "pdFEAS", "pdINF", "pFEAS_dINF", "pINF_dFEAS", "pdOPT",
+          "pUNBD", "dUNBD"]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("maxIteration", c_int), ("epsilonStar", c_double), ("lambdaStar", c_double),
+                ("omegaStar", c_double), ("lowerBound", c_double), ("upperBound", c_double),
+                ("betaStar", c_double), ("betaBar", c_double), ("gammaStar", c_double),
+                ("epsilonDash", c_double)]
+
+
+class Batch(ctypes.Structure):
+    _fields_ = [("count", c_int), ("nmax", c_int), ("mmax", c_int), ("n", c_void_p), ("m", c_void_p),
+                ("vec_off", c_void_p), ("b", c_void_p), ("mat_off", c_void_p), ("mat_ptr", c_void_p),
+                ("row", c_void_p), ("col", c_void_p), ("val", c_void_p), ("dense_off", c_void_p)]
+
+
+class BatchInit(ctypes.Structure):
+    _fields_ = [("flag", c_void_p), ("xvec", c_void_p), ("X", c_void_p), ("Y", c_void_p)]
+
+
+class BatchResult(ctypes.Structure):
+    _fields_ = [("xvec", c_void_p), ("X", c_void_p), ("Y", c_void_p), ("primal_obj", c_void_p),
+                ("dual_obj", c_void_p), ("mu", c_void_p), ("primal_error", c_void_p),
+                ("dual_error", c_void_p), ("iterations", c_void_p), ("phase", c_void_p),
+                ("status", c_void_p)]
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("precision", c_int), ("ctas_per_sm", c_int), ("mixed_mu_switch", c_double)]
+
+
+# (name, restype, argtypes) of every exported function of include/sdpa_b200.h
+SIGNATURES = [
+    ("sdpab_default_params", c_int, [c_int, POINTER(Params)]),
+    ("sdpab_read_params", c_int, [c_char_p, POINTER(Params)]),
+    ("sdpab_last_error", c_char_p, []),
+    ("sdpab_version", c_char_p, []),
+    ("sdpab_batch_solve", c_int, [POINTER(Batch), POINTER(BatchInit), POINTER(Params),
+                                  POINTER(BatchConfig), POINTER(BatchResult), c_void_p, c_void_p]),
+    ("sdpab_batch_solve_host", c_int, [POINTER(Batch), POINTER(BatchInit), POINTER(Params),
+                                       POINTER(BatchConfig), POINTER(BatchResult)]),
+    ("sdpab_workspace_bytes", c_longlong, []),
+    ("sdpab_release_workspace", c_int, []),
+]
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"sdpa_b200 native library missing: {LIB_PATH} "
+                               "(build it with `python -m sdpa_b200.build`)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class SolverError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str):
+    if rc != OK:
+        msg = lib().sdpab_last_error().decode(errors="replace")
+        raise SolverError(f"{what} failed ({rc}): {msg}")
+
+
+def default_params(kind: int = 0) -> Params:
+    p = Params()
+    check(lib().sdpab_default_params(kind, ctypes.byref(p)), "sdpab_default_params")
+    return p
+
+
+def read_params(path: str) -> Params:
+    p = Params()
+    check(lib().sdpab_read_params(path.encode(), ctypes.byref(p)), "sdpab_read_params")
+    return p

@@ -1,0 +1,214 @@
+"""Batched solve of many single-block SDPs through the C ABI
+(sdpab_batch_solve / sdpab_batch_solve_host).
+
+`pack(instances)` turns `Instance`s (one SDP block each) into the flat arrays
+of `sdpab_batch`; `solve_host` runs the host-pointer entry point (copies
+inside the call); `DeviceBatch` keeps a packed batch resident in device
+memory (torch tensors as allocation plumbing only) and solves it with the
+device-pointer entry point on a given stream.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .instances import Instance
+
+
+@dataclass
+class Packed:
+    count: int
+    nmax: int
+    mmax: int
+    n: np.ndarray          # int32
+    m: np.ndarray          # int32
+    vec_off: np.ndarray    # int64
+    b: np.ndarray          # float64
+    mat_off: np.ndarray    # int64
+    mat_ptr: np.ndarray    # int64
+    row: np.ndarray        # int32 (0-based)
+    col: np.ndarray        # int32
+    val: np.ndarray        # float64
+    dense_off: np.ndarray  # int64
+    nvec: int
+    nden: int
+
+    def h2d_bytes(self) -> int:
+        return sum(a.nbytes for a in (self.n, self.m, self.vec_off, self.b, self.mat_off, self.mat_ptr,
+                                      self.row, self.col, self.val, self.dense_off)) + 4 * self.count
+
+
+def pack(instances: list[Instance]) -> Packed:
+    cnt = len(instances)
+    n = np.zeros(cnt, np.int32)
+    m = np.zeros(cnt, np.int32)
+    vec_off = np.zeros(cnt, np.int64)
+    mat_off = np.zeros(cnt, np.int64)
+    dense_off = np.zeros(cnt, np.int64)
+    bs, ptrs, rows, cols, vals = [], [], [], [], []
+    nv = npn = ne = nd = 0
+    for q, it in enumerate(instances):
+        if len(it.blocks) != 1 or it.blocks[0] < 2:
+            raise ValueError("batched solver takes one SDP block per instance")
+        nb = int(it.blocks[0])
+        n[q], m[q] = nb, it.m
+        vec_off[q], mat_off[q], dense_off[q] = nv, npn, nd
+        order = np.lexsort((it.j, it.i, it.k))
+        k = it.k[order]
+        r = it.i[order] - 1
+        c = it.j[order] - 1
+        v = it.v[order]
+        # entries are stored upper-triangular
+        sw = r > c
+        r2 = np.where(sw, c, r)
+        c2 = np.where(sw, r, c)
+        counts = np.bincount(k, minlength=it.m + 1)
+        ptr = ne + np.concatenate([[0], np.cumsum(counts)])
+        bs.append(np.asarray(it.c, np.float64))
+        ptrs.append(ptr.astype(np.int64))
+        rows.append(r2.astype(np.int32))
+        cols.append(c2.astype(np.int32))
+        vals.append(v.astype(np.float64))
+        nv += it.m
+        npn += it.m + 2
+        ne += k.size
+        nd += nb * nb
+    return Packed(cnt, int(n.max()), int(m.max()), n, m, vec_off, np.concatenate(bs), mat_off,
+                  np.concatenate(ptrs), np.concatenate(rows), np.concatenate(cols),
+                  np.concatenate(vals), dense_off, nv, nd)
+
+
+@dataclass
+class BatchResult:
+    primal_obj: np.ndarray
+    dual_obj: np.ndarray
+    mu: np.ndarray
+    primal_error: np.ndarray
+    dual_error: np.ndarray
+    iterations: np.ndarray
+    phase: np.ndarray
+    status: np.ndarray
+    xvec: np.ndarray | None = None
+    X: np.ndarray | None = None
+    Y: np.ndarray | None = None
+
+    def x_of(self, P: Packed, q: int) -> np.ndarray:
+        return self.xvec[P.vec_off[q]:P.vec_off[q] + P.m[q]]
+
+    def mat_of(self, which: np.ndarray, P: Packed, q: int) -> np.ndarray:
+        nb = int(P.n[q])
+        return which[P.dense_off[q]:P.dense_off[q] + nb * nb].reshape(nb, nb, order="F")
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p).value
+
+
+def _params(params):
+    if params is None:
+        return N.default_params(0)
+    if isinstance(params, N.Params):
+        return params
+    p = N.default_params(0)
+    for k, v in params.items():
+        setattr(p, k, v)
+    return p
+
+
+def _config(precision=N.PREC_FP64, ctas_per_sm=0, mixed_mu_switch=0.0):
+    return N.BatchConfig(precision, ctas_per_sm, mixed_mu_switch)
+
+
+def solve_host(P: Packed, params=None, precision=N.PREC_FP64, want_x=True, want_mats=False,
+               init=None, ctas_per_sm=0) -> BatchResult:
+    """sdpab_batch_solve_host on host arrays.  init = (flag, xvec, X, Y) in
+    the packed layouts (user X / Y as in SDPA::inputInitXMat / inputInitYMat)."""
+    L = N.lib()
+    cnt = P.count
+    arrs = {k: np.ascontiguousarray(getattr(P, k)) for k in
+            ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col", "val", "dense_off")}
+    bt = N.Batch(cnt, P.nmax, P.mmax, *[_ptr(arrs[k]) for k in
+                                         ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col",
+                                          "val", "dense_off")])
+    res = BatchResult(*[np.zeros(cnt) for _ in range(5)], *[np.zeros(cnt, np.int32) for _ in range(3)])
+    res.xvec = np.zeros(P.nvec) if want_x else None
+    res.X = np.zeros(P.nden) if want_mats else None
+    res.Y = np.zeros(P.nden) if want_mats else None
+    br = N.BatchResult(_ptr(res.xvec), _ptr(res.X), _ptr(res.Y), _ptr(res.primal_obj), _ptr(res.dual_obj),
+                       _ptr(res.mu), _ptr(res.primal_error), _ptr(res.dual_error), _ptr(res.iterations),
+                       _ptr(res.phase), _ptr(res.status))
+    bi = None
+    keep = []
+    if init is not None:
+        flag, xv, Xu, Yu = (np.ascontiguousarray(init[0], np.int32), np.ascontiguousarray(init[1], np.float64),
+                            np.ascontiguousarray(init[2], np.float64), np.ascontiguousarray(init[3], np.float64))
+        keep = [flag, xv, Xu, Yu]
+        bi = ctypes.byref(N.BatchInit(_ptr(flag), _ptr(xv), _ptr(Xu), _ptr(Yu)))
+    prm = _params(params)
+    cfg = _config(precision, ctas_per_sm)
+    N.check(L.sdpab_batch_solve_host(ctypes.byref(bt), bi, ctypes.byref(prm), ctypes.byref(cfg),
+                                     ctypes.byref(br)), "sdpab_batch_solve_host")
+    del keep
+    return res
+
+
+class DeviceBatch:
+    """A packed batch resident in device memory (torch tensors hold the
+    allocations), solved by sdpab_batch_solve on a CUDA stream."""
+
+    def __init__(self, P: Packed, device="cuda", want_mats=False):
+        import torch
+        self.P = P
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+        self.d = {k: t(getattr(P, k)) for k in
+                  ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col", "val", "dense_off")}
+        order = np.argsort(-(P.n.astype(np.int64) ** 2 + P.m), kind="stable").astype(np.int32)
+        self.order = t(order)
+        cnt = P.count
+        f64 = dict(dtype=torch.float64, device=device)
+        i32 = dict(dtype=torch.int32, device=device)
+        self.sc = torch.zeros(5, cnt, **f64)
+        self.ic = torch.zeros(3, cnt, **i32)
+        self.xvec = torch.zeros(P.nvec, **f64)
+        self.X = torch.zeros(P.nden, **f64) if want_mats else None
+        self.Y = torch.zeros(P.nden, **f64) if want_mats else None
+        self.init = None
+        dp = lambda x: x.data_ptr()
+        self._bt = N.Batch(cnt, P.nmax, P.mmax, *[dp(self.d[k]) for k in
+                                                   ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row",
+                                                    "col", "val", "dense_off")])
+        self._br = N.BatchResult(dp(self.xvec), dp(self.X) if want_mats else None,
+                                 dp(self.Y) if want_mats else None,
+                                 *[dp(self.sc[q]) for q in range(5)], *[dp(self.ic[q]) for q in range(3)])
+
+    def set_init(self, flag, xvec, X, Y):
+        import torch
+        dev = self.xvec.device
+        self._init_t = [torch.as_tensor(np.ascontiguousarray(flag, np.int32), device=dev),
+                        torch.as_tensor(np.ascontiguousarray(xvec, np.float64), device=dev),
+                        torch.as_tensor(np.ascontiguousarray(X, np.float64), device=dev),
+                        torch.as_tensor(np.ascontiguousarray(Y, np.float64), device=dev)]
+        self.init = N.BatchInit(*[x.data_ptr() for x in self._init_t])
+
+    def solve(self, params=None, precision=N.PREC_FP64, stream=None, ctas_per_sm=0):
+        import torch
+        prm = _params(params)
+        cfg = _config(precision, ctas_per_sm)
+        s = stream if stream is not None else torch.cuda.current_stream()
+        N.check(N.lib().sdpab_batch_solve(ctypes.byref(self._bt),
+                                          ctypes.byref(self.init) if self.init is not None else None,
+                                          ctypes.byref(prm), ctypes.byref(cfg), ctypes.byref(self._br),
+                                          self.order.data_ptr(), s.cuda_stream), "sdpab_batch_solve")
+
+    def result(self) -> BatchResult:
+        sc = self.sc.cpu().numpy()
+        ic = self.ic.cpu().numpy()
+        r = BatchResult(*sc, *ic)
+        r.xvec = self.xvec.cpu().numpy()
+        if self.X is not None:
+            r.X = self.X.cpu().numpy()
+            r.Y = self.Y.cpu().numpy()
+        return r

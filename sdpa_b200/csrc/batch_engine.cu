@@ -1,0 +1,683 @@
+// Batched persistent SDP solver: one launch solves a whole batch of
+// single-block SDPs.  Each thread block repeatedly takes the next instance
+// from a device work queue (atomic counter over a largest-first order) and
+// runs SDPA's complete Mehrotra predictor-corrector loop for it
+// (SDPA::solve, sdpa_solve.cpp:59-233), with every dense step executed
+// cooperatively by the block on an L2-resident per-block workspace.
+//
+// Per iteration (reference operation sequence, sdpa_newton.cpp:2755-2809):
+//   predictor: R = beta mu Z^-1 - X; [X D Z^-1]; g = -A.(R - XDZ^-1) + r_p;
+//              Schur B by formula F3 (calF3_thread_2, sdpa_newton.cpp:1319-1403);
+//              adjusted Cholesky (sdpa_dpotrf.cpp:31-33); dy; dZ; dX (symmetrised)
+//   corrector: R -= dX dZ Z^-1; g; dy (same factor); dZ; dX
+//   step:      Lanczos (n > 20) or dense eigenvalue (n <= 20) minimum
+//              eigenvalue of L^-1 dX L^-T (sdpa_linear.cpp:29-182)
+//   update:    X, y, Z; Cholesky + inverse of X and Z, Z^-1 (sdpa_dataset.cpp:117-171)
+//   residuals, mu, objectives (sdpa_dataset.cpp:585-608, sdpa_parts.cpp:914-1060)
+// The scalar rules live in ipm_control.h, shared with the host-driven solver.
+// There are no inter-block waits: the only synchronisation is __syncthreads.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+#include <algorithm>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "cta_linalg.cuh"
+#include "ipm_control.h"
+#include "sdpa_b200.h"
+#include "sdpab_internal.h"
+
+namespace sdpab {
+
+constexpr int NT = 256;
+constexpr int TRI_MAX = 64;  // Lanczos tridiagonal order bound (sqrt(n)+11 for n < 2800)
+
+struct BatchArgs {
+  sdpab_batch p;
+  sdpab_batch_init init;
+  sdpab_batch_result r;
+  Params prm;
+  const int* order;
+  double* ws;
+  long long ws_stride;  // doubles per block
+  int* queue;
+};
+
+// Sparse helpers over one matrix's entry range -----------------------------
+
+// A . W for a symmetric A stored as upper-triangle entries and a general W
+// (Lal::getInnerProduct(Sparse, Dense), sdpa_linear.cpp:318-460).
+__device__ __forceinline__ double sp_dot(const int* row, const int* col, const double* val,
+                                         long long beg, long long end, const double* W, int ld)
+{
+  double s = 0.0;
+  for (long long e = beg; e < end; ++e) {
+    int r = row[e], c = col[e];
+    double v = val[e];
+    s += (r == c) ? v * W[r + (size_t)ld * r] : v * (W[r + (size_t)ld * c] + W[c + (size_t)ld * r]);
+  }
+  return s;
+}
+
+// W += scale * A (both triangles), block-parallel over entries.
+__device__ __forceinline__ void sp_axpy_block(const int* row, const int* col, const double* val,
+                                              long long beg, long long end, double scale, double* W,
+                                              int ld)
+{
+  for (long long e = beg + threadIdx.x; e < end; e += NT) {
+    int r = row[e], c = col[e];
+    double v = scale * val[e];
+    atomicAdd(&W[r + (size_t)ld * c], v);
+    if (r != c) atomicAdd(&W[c + (size_t)ld * r], v);
+  }
+}
+
+// W += scale * sum_k coef[k] A_k, one thread per constraint
+// (InputData::multi_plusToA, sdpa_dataset.cpp:427-433).  mp points at the
+// instance's F0 pointer; A_k is matrix k+1.
+__device__ __forceinline__ void sp_axpy_constraints(const int* row, const int* col,
+                                                    const double* val, const long long* mp, int m,
+                                                    const double* coef, double scale, double* W,
+                                                    int ld)
+{
+  for (int k = threadIdx.x; k < m; k += NT) {
+    const double s = scale * coef[k];
+    for (long long e = mp[k + 1]; e < mp[k + 2]; ++e) {
+      int r = row[e], c = col[e];
+      double v = s * val[e];
+      atomicAdd(&W[r + (size_t)ld * c], v);
+      if (r != c) atomicAdd(&W[c + (size_t)ld * r], v);
+    }
+  }
+}
+
+// calF3_thread_2 (sdpa_newton.cpp:1319-1403): Tr(A_i X A_j Z^-1) with A_j
+// outer (its entries alpha,beta) and A_i inner (gamma,delta).
+__device__ __forceinline__ double f3_value(const int* row, const int* col, const double* val,
+                                           long long jb, long long je, long long ib, long long ie,
+                                           const double* X, const double* Zi, int n)
+{
+  double ret = 0.0;
+  for (long long e1 = jb; e1 < je; ++e1) {
+    const int al = row[e1], be = col[e1];
+    const double v1 = val[e1];
+    const double* Xa = X + (size_t)n * al;
+    const double* Xb = X + (size_t)n * be;
+    const double* Za = Zi + (size_t)n * al;
+    const double* Zb = Zi + (size_t)n * be;
+    double sum = 0.0;
+    if (al != be) {
+      for (long long e2 = ib; e2 < ie; ++e2) {
+        const int ga = row[e2], de = col[e2];
+        double plu = (ga != de)
+                         ? Zb[de] * Xa[ga] + Zb[ga] * Xa[de] + Za[de] * Xb[ga] + Za[ga] * Xb[de]
+                         : Zb[de] * Xa[ga] + Za[de] * Xb[ga];
+        sum += val[e2] * plu;
+      }
+    } else {
+      for (long long e2 = ib; e2 < ie; ++e2) {
+        const int ga = row[e2], de = col[e2];
+        double plu = (ga != de) ? Zb[de] * Xa[ga] + Zb[ga] * Xa[de] : Zb[de] * Xa[ga];
+        sum += val[e2] * plu;
+      }
+    }
+    ret += v1 * sum;
+  }
+  return ret;
+}
+
+// Minimum eigenvalue of L D L^T --------------------------------------------
+
+struct EigScratch {
+  double *q, *qold, *r, *w, *t;   // Lanczos vectors (n)
+  double *d, *e, *work;           // tridiagonal (TRI_MAX), work 6*TRI_MAX
+  double* M;                      // dense n <= 20 matrix (400)
+  double* red;
+  double* s_val;                  // broadcast slot
+};
+
+// Lal::getMinEigen (sdpa_linear.cpp:29-143), Lanczos on L D L^T with the
+// reference's start vector, stopping rule and error correction; the
+// tridiagonal eigen-solve (dsteqr in the reference) is a warp multisection
+// for the smallest Ritz value plus inverse iteration for its eigenvector's
+// last component.
+__device__ double lanczos_min_eig(int n, const double* L, const double* D, EigScratch& s)
+{
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int i = tid; i < n; i += NT) { s.q[i] = 0.0; s.r[i] = 1.0; }
+  if (tid < TRI_MAX) { s.d[tid] = 1.0e50; s.e[tid] = 0.0; }
+  __syncthreads();
+  double beta = sqrt((double)n);
+  double mn = 1.0e51, mn_old = 1.0e52, err = 1.0e10;
+  int k = 0, kk = 0;
+  const double sqn = sqrt((double)n);
+  while (k < n && k < sqn + 10 && k < TRI_MAX - 1 && beta > 1.0e-16 &&
+         (fabs(mn - mn_old) > 1.0e-5 * fabs(mn) + 1.0e-8 ||
+          fabs(err * beta) > 1.0e-2 * fabs(mn) + 1.0e-4)) {
+    const double ib = 1.0 / beta;
+    for (int i = tid; i < n; i += NT) { s.qold[i] = s.q[i]; s.q[i] = s.r[i] * ib; }
+    __syncthreads();
+    // w = L^T q  (column i of L dotted with q), one warp per output
+    for (int i = wid; i < n; i += NT / 32) {
+      double a = 0.0;
+      for (int kx = i + lane; kx < n; kx += 32) a += L[kx + (size_t)n * i] * s.q[kx];
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane == 0) s.w[i] = a;
+    }
+    __syncthreads();
+    // t = D w  (D symmetric: column i dotted with w)
+    for (int i = wid; i < n; i += NT / 32) {
+      double a = 0.0;
+      for (int kx = lane; kx < n; kx += 32) a += D[kx + (size_t)n * i] * s.w[kx];
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane == 0) s.t[i] = a;
+    }
+    __syncthreads();
+    // w = L t
+    for (int i = tid; i < n; i += NT) {
+      double a = 0.0;
+      for (int kx = 0; kx <= i; ++kx) a += L[i + (size_t)n * kx] * s.t[kx];
+      s.w[i] = a;
+    }
+    __syncthreads();
+    const double alpha = cta::dot_vec<NT>(n, s.q, s.w, s.red);
+    if (tid == 0) s.d[k] = alpha;
+    for (int i = tid; i < n; i += NT) s.r[i] = (s.w[i] - alpha * s.q[i]) - beta * s.qold[i];
+    __syncthreads();
+    if (kk >= sqrt((double)k) || k == n - 1 || k > sqrt((double)n + 9)) {
+      kk = 0;
+      if (wid == 0) {
+        double lam = cta::tridiag_min_eig_warp(k + 1, s.d, s.e);
+        if (lane == 0) {
+          s.s_val[0] = lam;
+          s.s_val[1] = cta::tridiag_evec_last(k + 1, s.d, s.e, lam, s.work);
+        }
+      }
+      __syncthreads();
+      mn_old = mn;
+      mn = s.s_val[0];
+      err = s.s_val[1];
+      __syncthreads();
+    }
+    const double rr = cta::dot_vec<NT>(n, s.r, s.r, s.red);
+    beta = sqrt(rr);
+    if (tid == 0) s.e[k] = beta;
+    __syncthreads();
+    ++k;
+    ++kk;
+  }
+  return mn - fabs(err * beta);
+}
+
+// n <= 20: minimum eigenvalue of the lower triangle of M = L D L^T
+// (Jal::getMinEigen QR branch + dsyev, sdpa_jordan.cpp:81-89,
+// sdpa_linear.cpp:145-182) via Householder tridiagonalisation (warp 0) and
+// multisection.  W1, W2 are n x n scratch in global memory.
+__device__ double dense_min_eig(int n, const double* L, const double* D, double* W1, double* W2,
+                                double* gsm, EigScratch& s)
+{
+  cta::gemm<NT>(n, false, D, n, true, L, n, W1, n, 1.0, 0.0, gsm);   // D L^T
+  cta::gemm<NT>(n, false, L, n, false, W1, n, W2, n, 1.0, 0.0, gsm); // L (D L^T)
+  const int tid = threadIdx.x, lane = tid & 31;
+  double* M = s.M;  // n x n symmetric copy of the lower triangle
+  for (int t = tid; t < n * n; t += NT) {
+    int i = t % n, j = t / n;
+    M[i + n * j] = (i >= j) ? W2[i + (size_t)n * j] : W2[j + (size_t)n * i];
+  }
+  __syncthreads();
+  if (tid < 32) {
+    double* v = s.work;        // n
+    double* p = s.work + 32;   // n
+    for (int k = 0; k + 2 < n; ++k) {
+      const int len = n - k - 1;
+      double x = (lane < len) ? M[(k + 1 + lane) + n * k] : 0.0;
+      double nrm2 = x * x;
+      for (int o = 16; o > 0; o >>= 1) nrm2 += __shfl_xor_sync(0xffffffffu, nrm2, o);
+      double x0 = __shfl_sync(0xffffffffu, x, 0);
+      double alpha = (x0 >= 0.0) ? -sqrt(nrm2) : sqrt(nrm2);
+      double vi = (lane == 0) ? x - alpha : x;
+      double vn2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
+      if (lane == 0) s.e[k] = (nrm2 > 0.0) ? alpha : 0.0;
+      if (!(vn2 > 0.0)) { __syncwarp(); continue; }
+      if (lane < len) v[lane] = vi;
+      __syncwarp();
+      // p = (2 / vn2) * S v over the trailing block
+      double pi = 0.0;
+      if (lane < len) {
+        for (int c = 0; c < len; ++c) pi += M[(k + 1 + lane) + n * (k + 1 + c)] * v[c];
+        pi *= 2.0 / vn2;
+      }
+      double kv = (lane < len) ? pi * v[lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) kv += __shfl_xor_sync(0xffffffffu, kv, o);
+      kv /= vn2;  // K = v^T p / v^T v
+      double wi = pi - kv * vi;
+      if (lane < len) p[lane] = wi;
+      __syncwarp();
+      if (lane < len) {
+        for (int c = 0; c < len; ++c)
+          M[(k + 1 + lane) + n * (k + 1 + c)] -= v[lane] * p[c] + p[lane] * v[c];
+      }
+      __syncwarp();
+    }
+    if (lane < n) s.d[lane] = M[lane + n * lane];
+    if (n >= 2 && lane == 0) s.e[n - 2] = M[(n - 1) + n * (n - 2)];
+    __syncwarp();
+    double lam = cta::tridiag_min_eig_warp(n, s.d, s.e);
+    if (lane == 0) s.s_val[0] = lam;
+  }
+  __syncthreads();
+  double r = s.s_val[0];
+  __syncthreads();
+  return r;
+}
+
+__device__ double min_eig(int n, const double* L, const double* D, double* W1, double* W2,
+                          double* gsm, EigScratch& s)
+{
+  return (n > 20) ? lanczos_min_eig(n, L, D, s) : dense_min_eig(n, L, D, W1, W2, gsm, s);
+}
+
+// The solver -----------------------------------------------------------------
+
+__global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
+{
+  extern __shared__ double smem[];
+  const int nmax = a.p.nmax, mmax = a.p.mmax;
+  double* gsm = smem;                                   // GEMM staging 2*GK*GT
+  double* red = gsm + 2 * cta::GK * cta::GT;            // 32
+  double* vy = red + 32;                                // y   (mmax)
+  double* vdy = vy + mmax;                              // dy  (mmax)
+  double* vg = vdy + mmax;                              // g   (mmax)
+  double* vrp = vg + mmax;                              // r_p (mmax)
+  EigScratch es;
+  es.q = vrp + mmax;
+  es.qold = es.q + nmax;
+  es.r = es.qold + nmax;
+  es.w = es.r + nmax;
+  es.t = es.w + nmax;
+  es.d = es.t + nmax;
+  es.e = es.d + TRI_MAX;
+  es.work = es.e + TRI_MAX;
+  es.M = es.work + 6 * TRI_MAX;
+  es.s_val = es.M + 400;
+  es.red = red;
+  int* s_nnz = (int*)(es.s_val + 4);                     // mmax ints
+
+  __shared__ int s_inst, s_flag;
+  __shared__ Scalars S;
+  const int tid = threadIdx.x;
+  const Params& P = a.prm;
+
+  double* wsb = a.ws + (size_t)blockIdx.x * a.ws_stride;
+  const size_t nn = (size_t)nmax * nmax;
+  double* X = wsb;
+  double* Z = X + nn;
+  double* Zi = Z + nn;
+  double* LXi = Zi + nn;
+  double* LZi = LXi + nn;
+  double* D = LZi + nn;
+  double* XDZ = D + nn;
+  double* R = XDZ + nn;
+  double* dX = R + nn;
+  double* dZ = dX + nn;
+  double* W1 = dZ + nn;
+  double* W2 = W1 + nn;
+  double* X0 = W2 + nn;
+  double* Z0 = X0 + nn;
+  double* B = Z0 + nn;  // mmax * mmax
+
+  for (;;) {
+    if (tid == 0) s_inst = atomicAdd(a.queue, 1);
+    __syncthreads();
+    const int q = s_inst;
+    __syncthreads();
+    if (q >= a.p.count) break;
+    const int inst = a.order ? a.order[q] : q;
+    const int n = a.p.n[inst], m = a.p.m[inst];
+    if (n < 1 || m < 1 || n > nmax || m > mmax) {
+      if (tid == 0) a.r.status[inst] = SDPAB_ESIZE;
+      continue;
+    }
+    const long long* mp = a.p.mat_ptr + a.p.mat_off[inst];  // m+2 pointers
+    const int* er = a.p.row;
+    const int* ec = a.p.col;
+    const double* ev = a.p.val;
+    const double* bv = a.p.b + a.p.vec_off[inst];
+    const double lam = P.lambdaStar;
+    const int nn_i = n * n;
+
+    // entries must index inside the block: reject the instance otherwise
+    {
+      int bad = 0;
+      for (long long e = mp[0] + tid; e < mp[m + 1]; e += NT) {
+        const int r = er[e], c = ec[e];
+        bad |= (r < 0 || c < 0 || r >= n || c >= n);
+      }
+      if (__syncthreads_or(bad)) {
+        if (tid == 0) a.r.status[inst] = SDPAB_EINVAL;
+        continue;
+      }
+    }
+    // NonZeroEffect per constraint (diagonal 1, off-diagonal 2; sdpa_struct.cpp:1339-1341)
+    for (int k = tid; k < m; k += NT) {
+      int c = 0;
+      for (long long e = mp[k + 1]; e < mp[k + 2]; ++e) c += (er[e] == ec[e]) ? 1 : 2;
+      s_nnz[k] = c;
+    }
+
+    // ---------------- initial point
+    bool warm = a.init.flag && a.init.flag[inst];
+    int status = 0;
+    if (warm) {
+      const double* Xu = a.init.X + a.p.dense_off[inst];
+      const double* Yu = a.init.Y + a.p.dense_off[inst];
+      const double* xv = a.init.xvec + a.p.vec_off[inst];
+      for (int t = tid; t < nn_i; t += NT) { Z[t] = Xu[t]; X[t] = Yu[t]; W1[t] = Xu[t]; W2[t] = Yu[t]; }
+      for (int k = tid; k < m; k += NT) vy[k] = -xv[k];
+      __syncthreads();
+      // strict interiority check (the reference ignores computeInverse's
+      // failure here, sdpa_solve.cpp:63; this solver falls back instead)
+      int fx = cta::cholesky<NT>(n, W2, n, false, &s_flag);
+      int fz = fx ? 1 : cta::cholesky<NT>(n, W1, n, false, &s_flag);
+      if (fx || fz) { warm = false; status = 1; }
+      else {
+        cta::tri_inverse<NT>(n, W2, n, LXi, n);
+        cta::tri_inverse<NT>(n, W1, n, LZi, n);
+        cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
+      }
+    }
+    if (!warm) {
+      for (int t = tid; t < nn_i; t += NT) {
+        bool dg = (t % n) == (t / n);
+        X[t] = dg ? lam : 0.0;
+        Z[t] = dg ? lam : 0.0;
+        LXi[t] = dg ? 1.0 / sqrt(lam) : 0.0;
+        LZi[t] = dg ? 1.0 / sqrt(lam) : 0.0;
+        Zi[t] = dg ? 1.0 / lam : 0.0;
+      }
+      for (int k = tid; k < m; k += NT) vy[k] = 0.0;
+    }
+    __syncthreads();
+    if (warm) {
+      for (int t = tid; t < nn_i; t += NT) { X0[t] = X[t]; Z0[t] = Z[t]; }
+      __syncthreads();
+    }
+
+    // residuals: r_p = b - A.X, D = C - Z - sum y_k A_k (Residuals::compute)
+    auto residuals = [&](double& nrp, double& nrd) {
+      double mx = 0.0;
+      for (int k = tid; k < m; k += NT) {
+        double r = bv[k] - sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], X, n);
+        vrp[k] = r;
+        mx = fmax(mx, fabs(r));
+      }
+      nrp = cta::block_max<NT>(mx, red);
+      for (int t = tid; t < nn_i; t += NT) D[t] = -Z[t];
+      __syncthreads();
+      sp_axpy_block(er, ec, ev, mp[0], mp[1], -1.0, D, n);  // C = -F0
+      sp_axpy_constraints(er, ec, ev, mp, m, vy, -1.0, D, n);
+      __syncthreads();
+      mx = 0.0;
+      for (int t = tid; t < nn_i; t += NT) mx = fmax(mx, fabs(D[t]));
+      nrd = cta::block_max<NT>(mx, red);
+    };
+    // C . W with C = -F0
+    auto c_dot = [&](const double* W) {
+      double s = 0.0;
+      for (long long e = mp[0] + tid; e < mp[1]; e += NT) {
+        int r = er[e], c = ec[e];
+        double v = -ev[e];
+        s += (r == c) ? v * W[r + (size_t)n * r] : v * (W[r + (size_t)n * c] + W[c + (size_t)n * r]);
+      }
+      return cta::block_sum<NT>(s, red);
+    };
+
+    double nrp, nrd;
+    residuals(nrp, nrd);
+    double mu0;
+    if (warm) mu0 = cta::dot_mat<NT>(n, X, n, Z, n, red) / n;
+    else mu0 = lam * lam;
+    {
+      double objP = c_dot(X);
+      double objD = cta::dot_vec<NT>(m, bv, vy, red);
+      if (tid == 0) {
+        init_scalars(S, P, n, mu0, nrp, nrd, objP, objD);
+        update_check(S, P);
+      }
+    }
+    __syncthreads();
+
+    int iter = 0;
+    for (;;) {
+      if (tid == 0) s_flag = update_check(S, P) ? 1 : 0;
+      __syncthreads();
+      if (!s_flag || iter >= P.maxIteration) break;
+      if (tid == 0) predictor_setup(S, P);
+      __syncthreads();
+      const bool dinf = dual_infeasible(S);
+      const double bm = S.beta * S.mu;
+
+      // ---- predictor: rMat and gVec (sdpa_newton.cpp:793-883)
+      for (int t = tid; t < nn_i; t += NT) R[t] = bm * Zi[t] - X[t];
+      __syncthreads();
+      const double* G = R;
+      if (dinf) {
+        cta::gemm<NT>(n, false, X, n, false, D, n, W1, n, 1.0, 0.0, gsm);
+        cta::gemm<NT>(n, false, W1, n, false, Zi, n, XDZ, n, 1.0, 0.0, gsm);
+        for (int t = tid; t < nn_i; t += NT) W2[t] = R[t] - XDZ[t];
+        __syncthreads();
+        G = W2;
+      }
+      for (int k = tid; k < m; k += NT) vg[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], G, n) + vrp[k];
+      // ---- Schur complement by F3 (compute_bMat_dense_SDP3, sdpa_newton.cpp:2019-2125)
+      for (int t = tid; t < m * m; t += NT) {
+        const int i = t % m, j = t / m;
+        const int inz = s_nnz[i], jnz = s_nnz[j];
+        if (jnz < inz || (inz == jnz && i < j)) continue;
+        double v = f3_value(er, ec, ev, mp[j + 1], mp[j + 2], mp[i + 1], mp[i + 2], X, Zi, n);
+        B[i + (size_t)m * j] = v;
+        B[j + (size_t)m * i] = v;
+      }
+      __syncthreads();
+      // ---- adjusted Cholesky and solve (compute_DyVec, sdpa_newton.cpp:2672-2716)
+      if (cta::cholesky<NT>(m, B, m, true, &s_flag)) break;
+      for (int k = tid; k < m; k += NT) vdy[k] = vg[k];
+      __syncthreads();
+      cta::chol_solve<NT>(m, B, m, vdy, red);
+
+      // ---- dZ, dX (compute_DzMat / compute_DxMat, sdpa_newton.cpp:2718-2752)
+      auto direction = [&]() {
+        for (int t = tid; t < nn_i; t += NT) dZ[t] = dinf ? D[t] : 0.0;
+        __syncthreads();
+        sp_axpy_constraints(er, ec, ev, mp, m, vdy, -1.0, dZ, n);
+        __syncthreads();
+        cta::gemm<NT>(n, false, X, n, false, dZ, n, W1, n, 1.0, 0.0, gsm);
+        cta::gemm<NT>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm);
+        for (int t = tid; t < nn_i; t += NT) {
+          const int i = t % n, j = t / n;
+          if (i >= j) {
+            double lo = R[i + n * j] - W2[i + n * j];
+            double up = R[j + n * i] - W2[j + n * i];
+            double s = 0.5 * (lo + up);
+            dX[i + n * j] = s;
+            dX[j + n * i] = s;
+          }
+        }
+        __syncthreads();
+      };
+      direction();
+      {
+        double CdX = c_dot(dX);
+        double bdy = cta::dot_vec<NT>(m, bv, vdy, red);
+        double xdz = cta::dot_mat<NT>(n, X, n, dZ, n, red);
+        double dxz = cta::dot_mat<NT>(n, dX, n, Z, n, red);
+        double dxdz = cta::dot_mat<NT>(n, dX, n, dZ, n, red);
+        if (tid == 0) {
+          predictor_step(S, CdX, bdy);
+          corrector_beta(S, P, xdz, dxz, dxdz);
+        }
+        __syncthreads();
+      }
+
+      // ---- corrector (Newton::Mehrotra(CORRECTOR))
+      {
+        const double bm2 = S.beta * S.mu;
+        cta::gemm<NT>(n, false, dX, n, false, dZ, n, W1, n, 1.0, 0.0, gsm);
+        cta::gemm<NT>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm);
+        for (int t = tid; t < nn_i; t += NT) {
+          double rr = bm2 * Zi[t] - X[t];
+          rr = rr - W2[t];
+          R[t] = rr;
+          W1[t] = dinf ? rr - XDZ[t] : rr;
+        }
+        __syncthreads();
+        for (int k = tid; k < m; k += NT) vdy[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], W1, n) + vrp[k];
+        __syncthreads();
+        cta::chol_solve<NT>(m, B, m, vdy, red);
+        direction();
+      }
+
+      // ---- step length (StepLength::MehrotraCorrector)
+      {
+        const double minX = min_eig(n, LXi, dX, W1, W2, gsm, es);
+        const double minZ = min_eig(n, LZi, dZ, W1, W2, gsm, es);
+        double CdX = c_dot(dX);
+        double bdy = cta::dot_vec<NT>(m, bv, vdy, red);
+        double xdz = cta::dot_mat<NT>(n, X, n, dZ, n, red);
+        double dxz = cta::dot_mat<NT>(n, dX, n, Z, n, red);
+        double dxdz = cta::dot_mat<NT>(n, dX, n, dZ, n, red);
+        if (tid == 0) corrector_step(S, P, minX, minZ, CdX, bdy, xdz, dxz, dxdz, S.objD, S.objP);
+        __syncthreads();
+      }
+
+      // ---- update (Solutions::update, sdpa_dataset.cpp:145-171)
+      {
+        const double ap = S.alphaP, ad = S.alphaD;
+        for (int t = tid; t < nn_i; t += NT) {
+          X[t] += ap * dX[t];
+          Z[t] += ad * dZ[t];
+        }
+        for (int k = tid; k < m; k += NT) vy[k] += ad * vdy[k];
+        __syncthreads();
+        for (int t = tid; t < nn_i; t += NT) { W2[t] = X[t]; W1[t] = Z[t]; }
+        __syncthreads();
+        if (cannot_move(S)) break;
+        if (cta::cholesky<NT>(n, W2, n, false, &s_flag)) break;
+        cta::tri_inverse<NT>(n, W2, n, LXi, n);
+        if (cta::cholesky<NT>(n, W1, n, false, &s_flag)) break;
+        cta::tri_inverse<NT>(n, W1, n, LZi, n);
+        cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
+      }
+      // ---- residuals and scalars
+      {
+        double xz = cta::dot_mat<NT>(n, X, n, Z, n, red);
+        residuals(nrp, nrd);
+        double objP = c_dot(X);
+        double objD = cta::dot_vec<NT>(m, bv, vy, red);
+        double x0zM, xMz0;
+        if (warm) {
+          x0zM = cta::dot_mat<NT>(n, X0, n, Z, n, red);
+          xMz0 = cta::dot_mat<NT>(n, X, n, Z0, n, red);
+        } else {
+          x0zM = lam * cta::trace<NT>(n, Z, n, red);
+          xMz0 = lam * cta::trace<NT>(n, X, n, red);
+        }
+        if (tid == 0) after_update(S, P, xz, nrp, nrd, objP, objD, x0zM, xMz0);
+        __syncthreads();
+      }
+      ++iter;
+    }
+    // final residuals (sdpa_solve.cpp:204) and results
+    residuals(nrp, nrd);
+    if (tid == 0) {
+      a.r.primal_obj[inst] = -S.objD;
+      a.r.dual_obj[inst] = -S.objP;
+      a.r.mu[inst] = S.mu;
+      a.r.primal_error[inst] = nrd;
+      a.r.dual_error[inst] = nrp;
+      a.r.iterations[inst] = iter;
+      a.r.phase[inst] = user_phase(S.phase);
+      a.r.status[inst] = status;
+    }
+    if (a.r.xvec) {
+      double* xo = a.r.xvec + a.p.vec_off[inst];
+      for (int k = tid; k < m; k += NT) xo[k] = -vy[k];
+    }
+    if (a.r.X) {
+      double* o = a.r.X + a.p.dense_off[inst];
+      for (int t = tid; t < nn_i; t += NT) o[t] = Z[t];
+    }
+    if (a.r.Y) {
+      double* o = a.r.Y + a.p.dense_off[inst];
+      for (int t = tid; t < nn_i; t += NT) o[t] = X[t];
+    }
+    __syncthreads();
+  }
+}
+
+// Host side -----------------------------------------------------------------
+
+static size_t smem_bytes(int nmax, int mmax)
+{
+  size_t d = 2 * cta::GK * cta::GT + 32 + 4 * (size_t)mmax + 5 * (size_t)nmax + 2 * TRI_MAX +
+             6 * TRI_MAX + 400 + 4;
+  return d * sizeof(double) + (size_t)mmax * sizeof(int) + 64;
+}
+
+static long long ws_doubles(int nmax, int mmax)
+{
+  long long nn = (long long)nmax * nmax;
+  long long s = 14 * nn + (long long)mmax * mmax;
+  return (s + 31) / 32 * 32;  // 256-byte aligned per block
+}
+
+int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
+                       const sdpab_params* prm, const sdpab_batch_config* cfg,
+                       sdpab_batch_result* res, const int* order, cudaStream_t stream)
+{
+  if (!prob || !prm || !res || prob->count < 0 || prob->nmax < 1 || prob->mmax < 1)
+    return set_error(SDPAB_EINVAL, "batch_solve: invalid arguments");
+  if (prob->count == 0) return SDPAB_OK;
+  if (prob->nmax > 1024 || prob->mmax > 2048)
+    return set_error(SDPAB_ESIZE, "batch_solve: nmax <= 1024 and mmax <= 2048 are supported");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(SDPAB_ENODEV, "no CUDA device");
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t shm = smem_bytes(prob->nmax, prob->mmax);
+  if (shm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(batch_ipm_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)shm);
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_ipm_fp64, NT, shm);
+  if (per_sm < 1) return set_error(SDPAB_ESIZE, "batch_solve: kernel does not fit on an SM");
+  int want = (cfg && cfg->ctas_per_sm > 0) ? cfg->ctas_per_sm : 2;
+  per_sm = std::min(per_sm, want);
+  int grid = std::min(prob->count, sms * per_sm);
+  const long long stride = ws_doubles(prob->nmax, prob->mmax);
+  Workspace& W = workspace();
+  double* ws = (double*)W.get((size_t)grid * stride * sizeof(double) + 256);
+  if (!ws) return set_error(SDPAB_ECUDA, "workspace allocation failed");
+  int* queue = W.counter();
+  cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
+  BatchArgs a;
+  a.p = *prob;
+  if (init) a.init = *init; else memset(&a.init, 0, sizeof(a.init));
+  a.r = *res;
+  memcpy(&a.prm, prm, sizeof(Params));
+  a.order = order;
+  a.ws = ws;
+  a.ws_stride = stride;
+  a.queue = queue;
+  batch_ipm_fp64<<<grid, NT, shm, stream>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "batch_ipm_fp64 launch");
+  return SDPAB_OK;
+}
+
+}  // namespace sdpab

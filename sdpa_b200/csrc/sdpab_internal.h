@@ -1,0 +1,36 @@
+// Internal helpers shared by the library's translation units: thread-local
+// error text, CUDA error mapping and the per-device cached workspace.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "sdpa_b200.h"
+
+namespace sdpab {
+
+int set_error(int code, const char* msg);
+int cuda_error(cudaError_t e, const char* where);
+
+// Device memory kept between solver calls on the current device: the
+// per-block workspace of the batched solver plus a small counter page.
+// Grows on demand; sdpab_release_workspace frees it.
+class Workspace {
+ public:
+  void* get(size_t bytes);
+  int* counter();
+  size_t bytes() const { return bytes_; }
+  void release();
+
+ private:
+  void* ptr_ = nullptr;
+  size_t bytes_ = 0;
+  int* counter_ = nullptr;
+};
+
+Workspace& workspace();
+
+int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
+                       const sdpab_params* prm, const sdpab_batch_config* cfg,
+                       sdpab_batch_result* res, const int* order, cudaStream_t stream);
+
+}  // namespace sdpab

@@ -1,0 +1,196 @@
+"""Regenerates the golden fixtures in this directory by running the REFERENCE
+solver (oracle/_ref/ref_batch, compiled from the reference sources by
+oracle/Makefile) on seeded instances from sdpa_b200.instances.
+
+Run here (where the reference sources exist):
+    make -C oracle && python tests/golden/make_golden.py [--large]
+
+Fixtures (all from the reference's own output, never hand-written):
+  known_answers.json   example1/example2 of the reference manual, with the
+                       manual's printed values and the reference's run here
+  small.npz / small.json   small instances: objectives, iterations, phase, x,
+                       and the final Y/X blocks (MaxCut, Lovasz theta, random
+                       SDP with an LP block, batched-MaxCut seeds 0..63)
+  mc100_trace.json     per-iteration (mu, objP, objD, alphaP, alphaD, beta)
+                       of MaxCut G(100, 0.1) seed 1 at epsilonStar = 1e-7
+  large.json / large.npz  (--large) Lovasz theta G(200, 0.5) seed 1 and the
+                       random m=2000 SDP seed 1: objectives, iterations, x
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from sdpa_b200 import instances as inst  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref", "ref_batch")
+
+
+def example1():
+    """Example 1 of the reference manual: m=3, one 2x2 block."""
+    E = [(0, 1, 1, 1, -11.0), (0, 1, 2, 2, 23.0), (1, 1, 1, 1, 10.0), (1, 1, 1, 2, 4.0),
+         (2, 1, 2, 2, -8.0), (3, 1, 1, 2, -8.0), (3, 1, 2, 2, -2.0)]
+    a = np.array(E, dtype=object)
+    return inst.Instance(m=3, blocks=[2], c=np.array([48.0, -8.0, 20.0]),
+                         k=a[:, 0].astype(np.int32), l=a[:, 1].astype(np.int32),
+                         i=a[:, 2].astype(np.int32), j=a[:, 3].astype(np.int32),
+                         v=a[:, 4].astype(float), name="example1")
+
+
+def example2():
+    """Example 2 of the reference manual: m=5, blocks {2, 3, -2}."""
+    F = [
+        ([[-1.4, -3.2], [-3.2, -28]], [[15, -12, 2.1], [-12, 16, -3.8], [2.1, -3.8, 15]], [1.8, -4.0]),
+        ([[0.5, 5.2], [5.2, -5.3]], [[7.8, -2.4, 6.0], [-2.4, 4.2, 6.5], [6.0, 6.5, 2.1]], [-4.5, -3.5]),
+        ([[1.7, 7.0], [7.0, -9.3]], [[-1.9, -0.9, -1.3], [-0.9, -0.8, -2.1], [-1.3, -2.1, 4.0]], [-0.2, -3.7]),
+        ([[6.3, -7.5], [-7.5, -3.3]], [[0.2, 8.8, 5.4], [8.8, 3.4, -0.4], [5.4, -0.4, 7.5]], [-3.3, -4.0]),
+        ([[-2.4, -2.5], [-2.5, -2.9]], [[3.4, -3.2, -4.5], [-3.2, 3.0, -4.8], [-4.5, -4.8, 3.6]], [4.8, 9.7]),
+        ([[-6.5, -5.4], [-5.4, -6.6]], [[6.7, -7.2, -3.6], [-7.2, 7.3, -3.0], [-3.6, -3.0, -1.4]], [6.1, -1.5]),
+    ]
+    E = []
+    for k, (b1, b2, lp) in enumerate(F):
+        for l, B in ((1, b1), (2, b2)):
+            B = np.array(B, dtype=float)
+            for r in range(B.shape[0]):
+                for s in range(r, B.shape[0]):
+                    if B[r, s] != 0.0:
+                        E.append((k, l, r + 1, s + 1, B[r, s]))
+        for t, v in enumerate(lp):
+            if v != 0.0:
+                E.append((k, 3, t + 1, t + 1, float(v)))
+    a = np.array(E, dtype=object)
+    return inst.Instance(m=5, blocks=[2, 3, -2], c=np.array([1.1, -10, 6.6, 19, 4.1]),
+                         k=a[:, 0].astype(np.int32), l=a[:, 1].astype(np.int32),
+                         i=a[:, 2].astype(np.int32), j=a[:, 3].astype(np.int32),
+                         v=a[:, 4].astype(float), name="example2")
+
+
+PARAM_1E8 = """200 maxIteration
+1.0E-8 epsilonStar
+1.0E2 lambdaStar
+2.0 omegaStar
+-1.0E20 lowerBound
+1.0E20 upperBound
+0.1 betaStar
+0.2 betaBar
+0.9 gammaStar
+1.0E-8 epsilonDash
+%+10.16e xPrint
+%+10.16e XPrint
+%+10.16e YPrint
+%+10.16e infPrint
+"""
+
+
+def run_ref(instances, tmp, param=None, trace=False, procs=1, threads=1):
+    paths = []
+    for q, it in enumerate(instances):
+        p = os.path.join(tmp, f"i{q}.dat-s")
+        it.write(p)
+        paths.append(p)
+    cmd = [REF, "--dump", tmp] + (["--param", param] if param else []) + (["--trace"] if trace else [])
+    cmd += ["--procs", str(procs)] + paths
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS=str(threads))
+    out = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True).stdout
+    res, tr = {}, {}
+    for line in out.splitlines():
+        t = line.split()
+        if t[0] == "RESULT":
+            res[t[1]] = dict(iterations=int(t[2]), phase=t[3], primal_obj=float(t[4]),
+                             dual_obj=float(t[5]), seconds=float(t[6]))
+        elif t[0] == "TRACE" and len(t) >= 11 and t[2].isdigit():
+            tr.setdefault(t[1], []).append([float(x) for x in t[3:11]])
+    outl = []
+    for q, it in enumerate(instances):
+        p = paths[q]
+        r = res[p]
+        b = os.path.join(tmp, f"i{q}")
+        r["xvec"] = np.fromfile(b + ".xvec.bin")
+        r["X"], r["Y"] = [], []
+        for l, s in enumerate(it.blocks, start=1):
+            n = s * s if s > 1 else abs(s)
+            r["X"].append(np.fromfile(b + f".X{l}.bin"))
+            r["Y"].append(np.fromfile(b + f".Y{l}.bin"))
+        if trace:
+            r["trace"] = tr.get(p, [])
+        outl.append(r)
+    return outl
+
+
+def small_cases():
+    cases = [("mc100", inst.maxcut(100, 0.1, 1)), ("mc20", inst.maxcut(20, 0.3, 1)),
+             ("mc50w", inst.maxcut(50, 0.2, 5, unit_weights=False)),
+             ("lt20", inst.lovasz_theta(20, 0.5, 1)), ("lt40", inst.lovasz_theta(40, 0.3, 2)),
+             ("rnd40", inst.random_sdp(m=40, n=12, nlp=5, density=0.1, seed=3)),
+             ("rnd120", inst.random_sdp(m=120, n=30, nlp=8, density=0.05, seed=4)),
+             ("ex2", example2())]
+    cases += [(f"bmc{s}", inst.batch_maxcut(s)) for s in range(64)]
+    return cases
+
+
+def main():
+    large = "--large" in sys.argv
+    with tempfile.TemporaryDirectory() as tmp:
+        ppath = os.path.join(tmp, "param_1e-8.sdpa")
+        with open(ppath, "w") as f:
+            f.write(PARAM_1E8)
+        # known answers (manual section 6) + reference runs here
+        r_def = run_ref([example1(), example2()], tmp)
+        r_p8 = run_ref([example1(), example2()], tmp, param=ppath)
+        ka = {"manual": {"example1": {"iterations": 10, "primal_obj": -4.1899996163866390e+01,
+                                      "dual_obj": -4.1899999999999999e+01, "epsilonStar": 1e-7},
+                         "example2": {"iterations": 13, "primal_obj": 3.2062693405e+01,
+                                      "dual_obj": 3.2062692354e+01, "epsilonStar": 1e-7}},
+              "reference_default": {}, "reference_param_1e-8": {}}
+        for name, a, b in zip(["example1", "example2"], r_def, r_p8):
+            for key, r in (("reference_default", a), ("reference_param_1e-8", b)):
+                ka[key][name] = {k: (v.tolist() if isinstance(v, np.ndarray) else v)
+                                 for k, v in r.items() if k in ("iterations", "phase", "primal_obj",
+                                                                "dual_obj", "xvec")}
+        with open(os.path.join(HERE, "known_answers.json"), "w") as f:
+            json.dump(ka, f, indent=1)
+
+        cases = small_cases()
+        res = run_ref([c[1] for c in cases], tmp, procs=8)
+        meta, arrays = {}, {}
+        for (name, it), r in zip(cases, res):
+            meta[name] = {k: r[k] for k in ("iterations", "phase", "primal_obj", "dual_obj")}
+            arrays[name + ".xvec"] = r["xvec"]
+            if it.blocks[0] <= 50 or name == "mc100":
+                for l in range(len(it.blocks)):
+                    arrays[name + f".X{l + 1}"] = r["X"][l]
+                    arrays[name + f".Y{l + 1}"] = r["Y"][l]
+        with open(os.path.join(HERE, "small.json"), "w") as f:
+            json.dump(meta, f, indent=1)
+        np.savez_compressed(os.path.join(HERE, "small.npz"), **arrays)
+
+        tr = run_ref([inst.maxcut(100, 0.1, 1)], tmp, trace=True)[0]
+        with open(os.path.join(HERE, "mc100_trace.json"), "w") as f:
+            json.dump({"columns": ["mu", "thetaP", "thetaD", "objP", "objD",
+                                   "alphaP", "alphaD", "beta"], "rows": tr["trace"],
+                       "iterations": tr["iterations"]}, f, indent=1)
+
+        if large:
+            big = [("lt200", inst.lovasz_theta(200, 0.5, 1)), ("rnd2000", inst.random_sdp(seed=1))]
+            meta, arrays = {}, {}
+            for name, it in big:
+                r = run_ref([it], tmp, threads=os.cpu_count() or 8)[0]
+                meta[name] = {k: r[k] for k in ("iterations", "phase", "primal_obj", "dual_obj",
+                                                "seconds")}
+                arrays[name + ".xvec"] = r["xvec"]
+                print(name, meta[name], flush=True)
+            with open(os.path.join(HERE, "large.json"), "w") as f:
+                json.dump(meta, f, indent=1)
+            np.savez_compressed(os.path.join(HERE, "large.npz"), **arrays)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,84 @@
+"""Batched persistent solver (sdpab_batch_solve_host / sdpab_batch_solve)
+against the reference solver's results (golden fixtures) and the oracle."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from golden_util import GOLDEN, rel, small
+
+pytestmark = pytest.mark.gpu
+
+_spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+MG = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(MG)
+
+# Parity bar (floating point): objectives within 1e-6 relative of the
+# reference, x within 1e-5 (absolute, as the values are O(1)..O(10)).
+OBJ_TOL = 1e-6
+X_TOL = 1e-5
+
+
+def _solve(names, precision=0, **kw):
+    from sdpa_b200 import batch
+    cases = dict(MG.small_cases())
+    insts = [cases[n] for n in names]
+    P = batch.pack(insts)
+    return P, batch.solve_host(P, precision=precision, **kw)
+
+
+def test_batched_maxcut_matches_reference():
+    meta, arr = small()
+    names = [f"bmc{s}" for s in range(64)] + ["mc100", "mc20", "mc50w"]
+    P, r = _solve(names, want_mats=True)
+    iters_equal = 0
+    for q, nm in enumerate(names):
+        g = meta[nm]
+        assert r.status[q] == 0
+        assert r.phase[q] == 7, (nm, r.phase[q])  # pdOPT
+        assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
+        assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL, nm
+        assert np.max(np.abs(r.x_of(P, q) - arr[nm + ".xvec"])) < X_TOL, nm
+        iters_equal += int(r.iterations[q] == g["iterations"])
+        assert abs(int(r.iterations[q]) - g["iterations"]) <= 1
+    assert iters_equal >= len(names) - 2
+    q = names.index("mc100")
+    Y = r.mat_of(r.Y, P, q)
+    assert np.max(np.abs(Y - arr["mc100.Y1"].reshape(100, 100, order="F"))) < 1e-4
+
+
+def test_batched_general_constraints_match_reference():
+    """Lovasz theta (m > n, two-entry constraints) through the same kernel."""
+    meta, arr = small()
+    names = ["lt20", "lt40"]
+    P, r = _solve(names)
+    for q, nm in enumerate(names):
+        g = meta[nm]
+        assert r.phase[q] == 7
+        assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL
+        assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL
+        assert np.max(np.abs(r.x_of(P, q) - arr[nm + ".xvec"])) < X_TOL
+
+
+def test_device_path_equals_host_path():
+    import torch
+    from sdpa_b200 import batch
+    cases = dict(MG.small_cases())
+    insts = [cases[f"bmc{s}"] for s in range(16)]
+    P = batch.pack(insts)
+    h = batch.solve_host(P)
+    db = batch.DeviceBatch(P)
+    db.solve()
+    torch.cuda.synchronize()
+    d = db.result()
+    assert np.array_equal(h.iterations, d.iterations)
+    assert np.allclose(h.primal_obj, d.primal_obj, rtol=1e-12, atol=0)
+
+
+def test_empty_and_oversized_instances():
+    from sdpa_b200 import batch, instances
+    P = batch.pack([instances.batch_maxcut(3)])
+    P.n[0] = 5000  # larger than the supported block order: rejected with a code
+    with pytest.raises(Exception):
+        batch.solve_host(P)

@@ -1,0 +1,61 @@
+"""The CPU oracle (oracle/sdpa_oracle.py) pinned against the reference
+solver's own results (tests/golden, produced by oracle/_ref from the reference
+sources) and the known answers printed in the reference manual."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from golden_util import GOLDEN, known_answers, rel, small
+from oracle import sdpa_oracle as O
+
+_spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+MG = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(MG)
+
+
+def test_manual_known_answers():
+    ka = known_answers()
+    for name, inst in (("example1", MG.example1()), ("example2", MG.example2())):
+        r = O.solve(O.parse_dats(inst.to_dats()))
+        man = ka["manual"][name]
+        assert r.iterations == man["iterations"]
+        assert O.PHASE_NAMES[r.phase] == "pdOPT"
+        assert rel(r.primal_obj, man["primal_obj"]) < 1e-9
+        assert rel(r.dual_obj, man["dual_obj"]) < 1e-9
+        ref = ka["reference_default"][name]
+        assert rel(r.primal_obj, ref["primal_obj"]) < 1e-12
+        assert np.allclose(r.xvec, ref["xvec"], atol=1e-9, rtol=0)
+
+
+def test_param_file_epsilon_1e8():
+    ka = known_answers()
+    p = O.Params(maxIteration=200, epsilonStar=1e-8, lambdaStar=1e2, omegaStar=2.0, lowerBound=-1e20,
+                 upperBound=1e20, betaStar=0.1, betaBar=0.2, gammaStar=0.9, epsilonDash=1e-8)
+    for name, inst in (("example1", MG.example1()), ("example2", MG.example2())):
+        r = O.solve(O.parse_dats(inst.to_dats()), p)
+        ref = ka["reference_param_1e-8"][name]
+        assert r.iterations == ref["iterations"]
+        assert rel(r.primal_obj, ref["primal_obj"]) < 1e-10
+
+
+@pytest.mark.parametrize("name", ["mc20", "mc50w", "lt20", "lt40", "rnd40", "ex2", "bmc0", "bmc1",
+                                  "bmc5"])
+def test_oracle_matches_reference(name):
+    meta, arr = small()
+    inst = dict(MG.small_cases())[name]
+    r = O.solve(O.parse_dats(inst.to_dats()))
+    g = meta[name]
+    assert O.PHASE_NAMES[r.phase] == g["phase"]
+    assert r.iterations == g["iterations"]
+    assert rel(r.primal_obj, g["primal_obj"]) < 1e-9
+    assert rel(r.dual_obj, g["dual_obj"]) < 1e-9
+    assert np.max(np.abs(r.xvec - arr[name + ".xvec"])) < 1e-6
+
+
+def test_dats_roundtrip():
+    inst = MG.example2()
+    P = O.parse_dats(inst.to_dats())
+    assert P.m == 5 and P.blocks == [2, 3, -2]
+    assert len(P.entries[0]) == len([1 for k in inst.k if k == 0])
