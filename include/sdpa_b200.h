@@ -148,6 +148,27 @@ SDPAB_API int sdpab_batch_solve_host(const sdpab_batch* prob, const sdpab_batch_
                            const sdpab_params* prm, const sdpab_batch_config* cfg,
                            sdpab_batch_result* res);
 
+/* Batched solve that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc while running, e.g. a
+ * process whose own memory pool already holds the device's memory, or a
+ * service that must not allocate after start-up because cudaMalloc
+ * synchronises the device and may fail under memory pressure.  Arguments are
+ * those of sdpab_batch_solve (all DEVICE pointers; the caller owns inputs and
+ * outputs).  The solver's scratch is a fixed region of
+ * SDPAB_NOALLOC_SCRATCH_BYTES inside this library, held on every GPU that
+ * loads it until the process exits; one solver block needs
+ * 8 * (14 * nmax^2 + mmax^2) bytes of it (nmax = mmax = 120 fits 19 blocks,
+ * the largest accepted size is about nmax = mmax = 528), larger batches run
+ * with fewer concurrent blocks, and sizes whose single block does not fit are
+ * rejected with SDPAB_ESIZE.  The first call on a device looks up the
+ * region's device address; make that first call before any stream capture.
+ * Calls share the region (it keeps the last call's contents; the queue
+ * counter is cleared each call): calls that overlap on the GPU race. */
+#define SDPAB_NOALLOC_SCRATCH_BYTES (32ull * 1024ull * 1024ull)
+SDPAB_API int sdpab_batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
+                                        const sdpab_params* prm, sdpab_batch_result* res,
+                                        const int* order, void* stream);
+
 /* Device memory the batched solver keeps between calls (workspace, staging). */
 SDPAB_API long long sdpab_workspace_bytes(void);
 /* Frees that memory on the current device. */

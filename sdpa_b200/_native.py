@@ -57,6 +57,8 @@ SIGNATURES = [
                                   POINTER(BatchConfig), POINTER(BatchResult), c_void_p, c_void_p]),
     ("sdpab_batch_solve_host", c_int, [POINTER(Batch), POINTER(BatchInit), POINTER(Params),
                                        POINTER(BatchConfig), POINTER(BatchResult)]),
+    ("sdpab_batch_solve_noalloc", c_int, [POINTER(Batch), POINTER(BatchInit), POINTER(Params),
+                                          POINTER(BatchResult), c_void_p, c_void_p]),
     ("sdpab_workspace_bytes", c_longlong, []),
     ("sdpab_release_workspace", c_int, []),
 ]

@@ -680,4 +680,93 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   return SDPAB_OK;
 }
 
+// No-allocation variant of the batched solve ---------------------------------
+//
+// Some callers cannot call cudaMalloc once they are running: a process whose
+// own memory pool has already reserved the device's memory, or a service that
+// must not allocate after start-up because cudaMalloc synchronises the device
+// and can fail when memory is tight or fragmented.  For them the batched
+// solver can run on a fixed scratch region that is part of this library
+// instead of the growable workspace.  The region is a file-scope device
+// array, so every GPU that loads the library holds it until the process
+// exits.  Host code must not use the array's name as a device address: the
+// address is fetched once per device with cudaGetSymbolAddress (the first
+// call on a device does this set-up, so make that first call before any
+// stream capture).  All calls share the one region and it keeps the previous
+// call's contents; the work-queue counter is cleared on every call, and two
+// calls that overlap on the GPU race on the region.
+static __device__ __align__(256) double g_noalloc_scratch[SDPAB_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_base[64] = {nullptr};
+
+int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
+                        const sdpab_params* prm, sdpab_batch_result* res, const int* order,
+                        cudaStream_t stream)
+{
+  if (!prob || !prm || !res || prob->count < 0 || prob->nmax < 1 || prob->mmax < 1)
+    return set_error(SDPAB_EINVAL, "batch_solve_noalloc: invalid arguments");
+  if (prob->count == 0) return SDPAB_OK;
+  if (prob->nmax > 1024 || prob->mmax > 2048)
+    return set_error(SDPAB_ESIZE, "batch_solve_noalloc: nmax <= 1024 and mmax <= 2048 are supported");
+  const long long stride = ws_doubles(prob->nmax, prob->mmax);
+  const long long head = 32;  // doubles reserved for the work-queue counter
+  const long long capacity = ((long long)(SDPAB_NOALLOC_SCRATCH_BYTES / sizeof(double)) - head) / stride;
+  if (capacity < 1)
+    return set_error(SDPAB_ESIZE,
+                     "batch_solve_noalloc: one block's workspace (14*nmax^2 + mmax^2 doubles) "
+                     "exceeds the 32 MiB scratch region; use sdpab_batch_solve");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return set_error(SDPAB_ENODEV, "batch_solve_noalloc: no CUDA device");
+  double* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return cuda_error(e, "batch_solve_noalloc: cudaGetSymbolAddress");
+      g_noalloc_base[dev] = (double*)p;
+    }
+    base = g_noalloc_base[dev];
+  }
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t shm = smem_bytes(prob->nmax, prob->mmax);
+  if (shm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(batch_ipm_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)shm);
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_ipm_fp64, NT, shm);
+  if (per_sm < 1) return set_error(SDPAB_ESIZE, "batch_solve_noalloc: kernel does not fit on an SM");
+  per_sm = std::min(per_sm, 2);
+  const long long grid = std::min<long long>(std::min<long long>(prob->count, (long long)sms * per_sm),
+                                             capacity);
+  int* queue = (int*)base;
+  cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return cuda_error(e, "batch_solve_noalloc: clearing the queue counter");
+  BatchArgs a;
+  a.p = *prob;
+  if (init) a.init = *init; else memset(&a.init, 0, sizeof(a.init));
+  a.r = *res;
+  memcpy(&a.prm, prm, sizeof(Params));
+  a.order = order;
+  a.ws = base + head;
+  a.ws_stride = stride;
+  a.queue = queue;
+  batch_ipm_fp64<<<(int)grid, NT, shm, stream>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "batch_solve_noalloc: launch");
+  return SDPAB_OK;
+}
+
 }  // namespace sdpab
+
+extern "C" int sdpab_batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
+                                         const sdpab_params* prm, sdpab_batch_result* res,
+                                         const int* order, void* stream)
+{
+  return sdpab::batch_solve_noalloc(prob, init, prm, res, order, (cudaStream_t)stream);
+}
