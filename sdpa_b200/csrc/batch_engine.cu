@@ -33,6 +33,16 @@ namespace sdpab {
 
 constexpr int NT = 256;
 constexpr int TRI_MAX = 64;  // Lanczos tridiagonal order bound (sqrt(n)+11 for n < 2800)
+// Largest Lanczos matrix kept in shared memory (n <= 110 in FP64); larger
+// blocks run the Lanczos matvecs from global memory.
+constexpr int LANCZOS_SMEM_DOUBLES = 12288;
+
+__host__ __device__ __forceinline__ int big_doubles(int nmax)
+{
+  const int g = 2 * 16 * 96;  // GEMM staging (largest single-tile GEMM, n <= 96)
+  const int m2 = nmax * nmax;
+  return (m2 <= LANCZOS_SMEM_DOUBLES && m2 > g) ? m2 : g;
+}
 
 struct BatchArgs {
   sdpab_batch p;
@@ -134,21 +144,25 @@ struct EigScratch {
   double *q, *qold, *r, *w, *t;   // Lanczos vectors (n)
   double *d, *e, *work;           // tridiagonal (TRI_MAX), work 6*TRI_MAX
   double* M;                      // dense n <= 20 matrix (400)
-  double* red;
+  cta::Reducer* R;
   double* s_val;                  // broadcast slot
 };
 
-// Lal::getMinEigen (sdpa_linear.cpp:29-143), Lanczos on L D L^T with the
-// reference's start vector, stopping rule and error correction; the
-// tridiagonal eigen-solve (dsteqr in the reference) is a warp multisection
-// for the smallest Ritz value plus inverse iteration for its eigenvector's
-// last component.
-__device__ double lanczos_min_eig(int n, const double* L, const double* D, EigScratch& s)
+// Lal::getMinEigen (sdpa_linear.cpp:29-143): Lanczos on M = L D L^T with
+// the reference's start vector (all ones), stopping rule and error
+// correction.  M is formed once by two GEMMs (the reference applies L^T, D, L
+// to each Lanczos vector; the products agree to rounding), so each step is a
+// single coalesced matvec.  The tridiagonal eigen-solve (dsteqr in the
+// reference) is a warp multisection for the smallest Ritz value plus inverse
+// iteration for the last component of its eigenvector.
+__device__ double lanczos_min_eig(int n, const double* M, EigScratch& s)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  // every thread owns the vector entries i = tid, tid + NT, ...
   for (int i = tid; i < n; i += NT) { s.q[i] = 0.0; s.r[i] = 1.0; }
-  if (tid < TRI_MAX) { s.d[tid] = 1.0e50; s.e[tid] = 0.0; }
-  __syncthreads();
+  if (wid == 0) {
+    for (int i = lane; i < TRI_MAX; i += 32) { s.d[i] = 1.0e50; s.e[i] = 0.0; }
+  }
   double beta = sqrt((double)n);
   double mn = 1.0e51, mn_old = 1.0e52, err = 1.0e10;
   int k = 0, kk = 0;
@@ -159,71 +173,78 @@ __device__ double lanczos_min_eig(int n, const double* L, const double* D, EigSc
     const double ib = 1.0 / beta;
     for (int i = tid; i < n; i += NT) { s.qold[i] = s.q[i]; s.q[i] = s.r[i] * ib; }
     __syncthreads();
-    // w = L^T q  (column i of L dotted with q), one warp per output
-    for (int i = wid; i < n; i += NT / 32) {
-      double a = 0.0;
-      for (int kx = i + lane; kx < n; kx += 32) a += L[kx + (size_t)n * i] * s.q[kx];
-      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-      if (lane == 0) s.w[i] = a;
+    // w = M q: each warp takes 4 columns at a time (M column i dotted with q)
+    double part = 0.0;
+    for (int i0 = wid * 4; i0 < n; i0 += NT / 8) {
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      const double* c0 = M + (size_t)n * i0;
+      for (int kx = lane; kx < n; kx += 32) {
+        const double qk = s.q[kx];
+        a0 += c0[kx] * qk;
+        if (i0 + 1 < n) a1 += c0[kx + n] * qk;
+        if (i0 + 2 < n) a2 += c0[kx + 2 * n] * qk;
+        if (i0 + 3 < n) a3 += c0[kx + 3 * n] * qk;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+      }
+      if (lane < 4 && i0 + lane < n) {
+        const double wv = (lane == 0) ? a0 : (lane == 1) ? a1 : (lane == 2) ? a2 : a3;
+        s.w[i0 + lane] = wv;
+        part += s.q[i0 + lane] * wv;
+      }
     }
-    __syncthreads();
-    // t = D w  (D symmetric: column i dotted with w)
-    for (int i = wid; i < n; i += NT / 32) {
-      double a = 0.0;
-      for (int kx = lane; kx < n; kx += 32) a += D[kx + (size_t)n * i] * s.w[kx];
-      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-      if (lane == 0) s.t[i] = a;
-    }
-    __syncthreads();
-    // w = L t
+    const double alpha = cta::block_sum<NT>(part, *s.R);  // barrier also publishes w
+    double rpart = 0.0;
     for (int i = tid; i < n; i += NT) {
-      double a = 0.0;
-      for (int kx = 0; kx <= i; ++kx) a += L[i + (size_t)n * kx] * s.t[kx];
-      s.w[i] = a;
+      const double rv = (s.w[i] - alpha * s.q[i]) - beta * s.qold[i];
+      s.r[i] = rv;
+      rpart += rv * rv;
     }
-    __syncthreads();
-    const double alpha = cta::dot_vec<NT>(n, s.q, s.w, s.red);
-    if (tid == 0) s.d[k] = alpha;
-    for (int i = tid; i < n; i += NT) s.r[i] = (s.w[i] - alpha * s.q[i]) - beta * s.qold[i];
-    __syncthreads();
-    if (kk >= sqrt((double)k) || k == n - 1 || k > sqrt((double)n + 9)) {
-      kk = 0;
-      if (wid == 0) {
-        double lam = cta::tridiag_min_eig_warp(k + 1, s.d, s.e);
+    if (wid == 0) {
+      if (lane == 0) s.d[k] = alpha;
+      __syncwarp();
+      if (kk >= sqrt((double)k) || k == n - 1 || k > sqrt((double)n + 9)) {
+        const double lam = cta::tridiag_min_eig_warp(k + 1, s.d, s.e);
         if (lane == 0) {
           s.s_val[0] = lam;
           s.s_val[1] = cta::tridiag_evec_last(k + 1, s.d, s.e, lam, s.work);
+          s.s_val[2] = 1.0;
         }
+      } else if (lane == 0) {
+        s.s_val[2] = 0.0;
       }
-      __syncthreads();
+    }
+    // the barrier of this reduction also publishes warp 0's eigen result
+    const double rr = cta::block_sum<NT>(rpart, *s.R);
+    if (s.s_val[2] != 0.0) {
+      kk = 0;
       mn_old = mn;
       mn = s.s_val[0];
       err = s.s_val[1];
-      __syncthreads();
     }
-    const double rr = cta::dot_vec<NT>(n, s.r, s.r, s.red);
     beta = sqrt(rr);
     if (tid == 0) s.e[k] = beta;
-    __syncthreads();
     ++k;
     ++kk;
   }
+  __syncthreads();
   return mn - fabs(err * beta);
 }
 
 // n <= 20: minimum eigenvalue of the lower triangle of M = L D L^T
 // (Jal::getMinEigen QR branch + dsyev, sdpa_jordan.cpp:81-89,
 // sdpa_linear.cpp:145-182) via Householder tridiagonalisation (warp 0) and
-// multisection.  W1, W2 are n x n scratch in global memory.
-__device__ double dense_min_eig(int n, const double* L, const double* D, double* W1, double* W2,
-                                double* gsm, EigScratch& s)
+// multisection.
+__device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
 {
-  cta::gemm<NT>(n, false, D, n, true, L, n, W1, n, 1.0, 0.0, gsm);   // D L^T
-  cta::gemm<NT>(n, false, L, n, false, W1, n, W2, n, 1.0, 0.0, gsm); // L (D L^T)
   const int tid = threadIdx.x, lane = tid & 31;
   double* M = s.M;  // n x n symmetric copy of the lower triangle
   for (int t = tid; t < n * n; t += NT) {
-    int i = t % n, j = t / n;
+    const int i = t % n, j = t / n;
     M[i + n * j] = (i >= j) ? W2[i + (size_t)n * j] : W2[j + (size_t)n * i];
   }
   __syncthreads();
@@ -232,18 +253,18 @@ __device__ double dense_min_eig(int n, const double* L, const double* D, double*
     double* p = s.work + 32;   // n
     for (int k = 0; k + 2 < n; ++k) {
       const int len = n - k - 1;
-      double x = (lane < len) ? M[(k + 1 + lane) + n * k] : 0.0;
+      const double x = (lane < len) ? M[(k + 1 + lane) + n * k] : 0.0;
       double nrm2 = x * x;
       for (int o = 16; o > 0; o >>= 1) nrm2 += __shfl_xor_sync(0xffffffffu, nrm2, o);
-      double x0 = __shfl_sync(0xffffffffu, x, 0);
-      double alpha = (x0 >= 0.0) ? -sqrt(nrm2) : sqrt(nrm2);
-      double vi = (lane == 0) ? x - alpha : x;
-      double vn2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
+      const double x0 = __shfl_sync(0xffffffffu, x, 0);
+      const double alpha = (x0 >= 0.0) ? -sqrt(nrm2) : sqrt(nrm2);
+      const double vi = (lane == 0) ? x - alpha : x;
+      const double vn2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
       if (lane == 0) s.e[k] = (nrm2 > 0.0) ? alpha : 0.0;
       if (!(vn2 > 0.0)) { __syncwarp(); continue; }
       if (lane < len) v[lane] = vi;
       __syncwarp();
-      // p = (2 / vn2) * S v over the trailing block
+      // p = (2 / vn2) S v on the trailing block; K = v^T p / v^T v; w = p - K v
       double pi = 0.0;
       if (lane < len) {
         for (int c = 0; c < len; ++c) pi += M[(k + 1 + lane) + n * (k + 1 + c)] * v[c];
@@ -251,8 +272,8 @@ __device__ double dense_min_eig(int n, const double* L, const double* D, double*
       }
       double kv = (lane < len) ? pi * v[lane] : 0.0;
       for (int o = 16; o > 0; o >>= 1) kv += __shfl_xor_sync(0xffffffffu, kv, o);
-      kv /= vn2;  // K = v^T p / v^T v
-      double wi = pi - kv * vi;
+      kv /= vn2;
+      const double wi = pi - kv * vi;
       if (lane < len) p[lane] = wi;
       __syncwarp();
       if (lane < len) {
@@ -264,19 +285,30 @@ __device__ double dense_min_eig(int n, const double* L, const double* D, double*
     if (lane < n) s.d[lane] = M[lane + n * lane];
     if (n >= 2 && lane == 0) s.e[n - 2] = M[(n - 1) + n * (n - 2)];
     __syncwarp();
-    double lam = cta::tridiag_min_eig_warp(n, s.d, s.e);
+    const double lam = cta::tridiag_min_eig_warp(n, s.d, s.e);
     if (lane == 0) s.s_val[0] = lam;
   }
   __syncthreads();
-  double r = s.s_val[0];
+  const double r = s.s_val[0];
   __syncthreads();
   return r;
 }
 
+// Minimum eigenvalue of L D L^T (Jal::getMinEigen, sdpa_jordan.cpp:58-109):
+// Lanczos for n > 20, dense for n <= 20.  W1, W2: n x n scratch.
 __device__ double min_eig(int n, const double* L, const double* D, double* W1, double* W2,
-                          double* gsm, EigScratch& s)
+                          double* gsm, int gsm_doubles, EigScratch& s)
 {
-  return (n > 20) ? lanczos_min_eig(n, L, D, s) : dense_min_eig(n, L, D, W1, W2, gsm, s);
+  cta::gemm<NT>(n, false, D, n, true, L, n, W1, n, 1.0, 0.0, gsm);   // D L^T
+  cta::gemm<NT>(n, false, L, n, false, W1, n, W2, n, 1.0, 0.0, gsm); // L (D L^T)
+  if (n <= 20) return dense_min_eig(n, W2, s);
+  const double* M = W2;
+  if (n * n <= gsm_doubles) {  // stage M in shared memory for the Lanczos steps
+    for (int t = threadIdx.x; t < n * n; t += NT) gsm[t] = W2[t];
+    __syncthreads();
+    M = gsm;
+  }
+  return lanczos_min_eig(n, M, s);
 }
 
 // The solver -----------------------------------------------------------------
@@ -285,9 +317,11 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 {
   extern __shared__ double smem[];
   const int nmax = a.p.nmax, mmax = a.p.mmax;
-  double* gsm = smem;                                   // GEMM staging 2*GK*GT
-  double* red = gsm + 2 * cta::GK * cta::GT;            // 32
-  double* vy = red + 32;                                // y   (mmax)
+  const int gsm_doubles = big_doubles(nmax);
+  double* gsm = smem;                                   // GEMM staging / Lanczos matrix
+  double* sD = gsm + gsm_doubles;                       // diagonal block NB*LDD
+  double* redbuf = sD + cta::SD_DOUBLES;             // 2 * NT/32
+  double* vy = redbuf + 2 * (NT / 32);                  // y   (mmax)
   double* vdy = vy + mmax;                              // dy  (mmax)
   double* vg = vdy + mmax;                              // g   (mmax)
   double* vrp = vg + mmax;                              // r_p (mmax)
@@ -302,7 +336,8 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
   es.work = es.e + TRI_MAX;
   es.M = es.work + 6 * TRI_MAX;
   es.s_val = es.M + 400;
-  es.red = red;
+  cta::Reducer RD{redbuf, 0};
+  es.R = &RD;
   int* s_nnz = (int*)(es.s_val + 4);                     // mmax ints
 
   __shared__ int s_inst, s_flag;
@@ -379,12 +414,12 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       __syncthreads();
       // strict interiority check (the reference ignores computeInverse's
       // failure here, sdpa_solve.cpp:63; this solver falls back instead)
-      int fx = cta::cholesky<NT>(n, W2, n, false, &s_flag);
-      int fz = fx ? 1 : cta::cholesky<NT>(n, W1, n, false, &s_flag);
+      int fx = cta::cholesky<NT>(n, W2, n, false, sD, gsm, &s_flag);
+      int fz = fx ? 1 : cta::cholesky<NT>(n, W1, n, false, sD, gsm, &s_flag);
       if (fx || fz) { warm = false; status = 1; }
       else {
-        cta::tri_inverse<NT>(n, W2, n, LXi, n);
-        cta::tri_inverse<NT>(n, W1, n, LZi, n);
+        cta::tri_inverse<NT>(n, W2, n, LXi, n, sD, gsm);
+        cta::tri_inverse<NT>(n, W1, n, LZi, n, sD, gsm);
         cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
     }
@@ -413,7 +448,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         vrp[k] = r;
         mx = fmax(mx, fabs(r));
       }
-      nrp = cta::block_max<NT>(mx, red);
+      nrp = cta::block_max<NT>(mx, RD);
       for (int t = tid; t < nn_i; t += NT) D[t] = -Z[t];
       __syncthreads();
       sp_axpy_block(er, ec, ev, mp[0], mp[1], -1.0, D, n);  // C = -F0
@@ -421,7 +456,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       __syncthreads();
       mx = 0.0;
       for (int t = tid; t < nn_i; t += NT) mx = fmax(mx, fabs(D[t]));
-      nrd = cta::block_max<NT>(mx, red);
+      nrd = cta::block_max<NT>(mx, RD);
     };
     // C . W with C = -F0
     auto c_dot = [&](const double* W) {
@@ -431,17 +466,17 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         double v = -ev[e];
         s += (r == c) ? v * W[r + (size_t)n * r] : v * (W[r + (size_t)n * c] + W[c + (size_t)n * r]);
       }
-      return cta::block_sum<NT>(s, red);
+      return cta::block_sum<NT>(s, RD);
     };
 
     double nrp, nrd;
     residuals(nrp, nrd);
     double mu0;
-    if (warm) mu0 = cta::dot_mat<NT>(n, X, n, Z, n, red) / n;
+    if (warm) mu0 = cta::dot_mat<NT>(n, X, Z, RD) / n;
     else mu0 = lam * lam;
     {
       double objP = c_dot(X);
-      double objD = cta::dot_vec<NT>(m, bv, vy, red);
+      double objD = cta::dot_vec<NT>(m, bv, vy, RD);
       if (tid == 0) {
         init_scalars(S, P, n, mu0, nrp, nrd, objP, objD);
         update_check(S, P);
@@ -482,10 +517,10 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       }
       __syncthreads();
       // ---- adjusted Cholesky and solve (compute_DyVec, sdpa_newton.cpp:2672-2716)
-      if (cta::cholesky<NT>(m, B, m, true, &s_flag)) break;
+      if (cta::cholesky<NT>(m, B, m, true, sD, gsm, &s_flag)) break;
       for (int k = tid; k < m; k += NT) vdy[k] = vg[k];
       __syncthreads();
-      cta::chol_solve<NT>(m, B, m, vdy, red);
+      cta::chol_solve<NT>(m, B, m, vdy, sD);
 
       // ---- dZ, dX (compute_DzMat / compute_DxMat, sdpa_newton.cpp:2718-2752)
       auto direction = [&]() {
@@ -510,10 +545,10 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       direction();
       {
         double CdX = c_dot(dX);
-        double bdy = cta::dot_vec<NT>(m, bv, vdy, red);
-        double xdz = cta::dot_mat<NT>(n, X, n, dZ, n, red);
-        double dxz = cta::dot_mat<NT>(n, dX, n, Z, n, red);
-        double dxdz = cta::dot_mat<NT>(n, dX, n, dZ, n, red);
+        double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);
+        double xdz = cta::dot_mat<NT>(n, X, dZ, RD);
+        double dxz = cta::dot_mat<NT>(n, dX, Z, RD);
+        double dxdz = cta::dot_mat<NT>(n, dX, dZ, RD);
         if (tid == 0) {
           predictor_step(S, CdX, bdy);
           corrector_beta(S, P, xdz, dxz, dxdz);
@@ -535,19 +570,19 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         __syncthreads();
         for (int k = tid; k < m; k += NT) vdy[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], W1, n) + vrp[k];
         __syncthreads();
-        cta::chol_solve<NT>(m, B, m, vdy, red);
+        cta::chol_solve<NT>(m, B, m, vdy, sD);
         direction();
       }
 
       // ---- step length (StepLength::MehrotraCorrector)
       {
-        const double minX = min_eig(n, LXi, dX, W1, W2, gsm, es);
-        const double minZ = min_eig(n, LZi, dZ, W1, W2, gsm, es);
+        const double minX = min_eig(n, LXi, dX, W1, W2, gsm, gsm_doubles, es);
+        const double minZ = min_eig(n, LZi, dZ, W1, W2, gsm, gsm_doubles, es);
         double CdX = c_dot(dX);
-        double bdy = cta::dot_vec<NT>(m, bv, vdy, red);
-        double xdz = cta::dot_mat<NT>(n, X, n, dZ, n, red);
-        double dxz = cta::dot_mat<NT>(n, dX, n, Z, n, red);
-        double dxdz = cta::dot_mat<NT>(n, dX, n, dZ, n, red);
+        double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);
+        double xdz = cta::dot_mat<NT>(n, X, dZ, RD);
+        double dxz = cta::dot_mat<NT>(n, dX, Z, RD);
+        double dxdz = cta::dot_mat<NT>(n, dX, dZ, RD);
         if (tid == 0) corrector_step(S, P, minX, minZ, CdX, bdy, xdz, dxz, dxdz, S.objD, S.objP);
         __syncthreads();
       }
@@ -564,25 +599,25 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         for (int t = tid; t < nn_i; t += NT) { W2[t] = X[t]; W1[t] = Z[t]; }
         __syncthreads();
         if (cannot_move(S)) break;
-        if (cta::cholesky<NT>(n, W2, n, false, &s_flag)) break;
-        cta::tri_inverse<NT>(n, W2, n, LXi, n);
-        if (cta::cholesky<NT>(n, W1, n, false, &s_flag)) break;
-        cta::tri_inverse<NT>(n, W1, n, LZi, n);
+        if (cta::cholesky<NT>(n, W2, n, false, sD, gsm, &s_flag)) break;
+        cta::tri_inverse<NT>(n, W2, n, LXi, n, sD, gsm);
+        if (cta::cholesky<NT>(n, W1, n, false, sD, gsm, &s_flag)) break;
+        cta::tri_inverse<NT>(n, W1, n, LZi, n, sD, gsm);
         cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
       // ---- residuals and scalars
       {
-        double xz = cta::dot_mat<NT>(n, X, n, Z, n, red);
+        double xz = cta::dot_mat<NT>(n, X, Z, RD);
         residuals(nrp, nrd);
         double objP = c_dot(X);
-        double objD = cta::dot_vec<NT>(m, bv, vy, red);
+        double objD = cta::dot_vec<NT>(m, bv, vy, RD);
         double x0zM, xMz0;
         if (warm) {
-          x0zM = cta::dot_mat<NT>(n, X0, n, Z, n, red);
-          xMz0 = cta::dot_mat<NT>(n, X, n, Z0, n, red);
+          x0zM = cta::dot_mat<NT>(n, X0, Z, RD);
+          xMz0 = cta::dot_mat<NT>(n, X, Z0, RD);
         } else {
-          x0zM = lam * cta::trace<NT>(n, Z, n, red);
-          xMz0 = lam * cta::trace<NT>(n, X, n, red);
+          x0zM = lam * cta::trace<NT>(n, Z, RD);
+          xMz0 = lam * cta::trace<NT>(n, X, RD);
         }
         if (tid == 0) after_update(S, P, xz, nrp, nrd, objP, objD, x0zM, xMz0);
         __syncthreads();
@@ -621,7 +656,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 
 static size_t smem_bytes(int nmax, int mmax)
 {
-  size_t d = 2 * cta::GK * cta::GT + 32 + 4 * (size_t)mmax + 5 * (size_t)nmax + 2 * TRI_MAX +
+  size_t d = (size_t)big_doubles(nmax) + cta::SD_DOUBLES + 2 * (NT / 32) + 4 * (size_t)mmax + 5 * (size_t)nmax + 2 * TRI_MAX +
              6 * TRI_MAX + 400 + 4;
   return d * sizeof(double) + (size_t)mmax * sizeof(int) + 64;
 }

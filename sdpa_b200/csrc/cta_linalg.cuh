@@ -1,9 +1,12 @@
 // CTA-cooperative dense linear algebra for one small SDP block (order n up to
 // a few hundred), the building blocks of the batched persistent solver.
 // Every routine is called by ALL threads of the block with identical
-// arguments and ends with a __syncthreads(); matrices are column-major FP64
-// in global memory (L2-resident working set), tiles are staged through shared
-// memory.  Nothing here waits on another block.
+// arguments; matrices are column-major FP64 in global memory (the block's
+// L2-resident workspace) and tiles are staged through shared memory.
+// Factorisations and triangular solves are blocked by 32: the 32 x 32
+// diagonal block is handled by one warp with shuffles, everything else is a
+// block-wide tile update, so the number of block barriers grows with n/32,
+// not with n.  Nothing here waits on another thread block.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -11,108 +14,147 @@
 namespace sdpab {
 namespace cta {
 
+constexpr int NB = 32;      // blocking of factorisations / solves
+constexpr int LDD = 33;     // leading dimension of the shared diagonal block
+// Shared diagonal-block buffer: NB x NB block (leading dimension LDD) followed
+// by the NB reciprocals of its diagonal.
+constexpr int SD_DOUBLES = NB * LDD + NB;
+
 // ------------------------------------------------------------ reductions
+// Block reductions with ONE barrier: partials go to one of two alternating
+// shared slots, so a fast thread entering the next reduction cannot overwrite
+// a slot that a slow thread is still reading (that thread must first pass
+// the next reduction's barrier).  All threads must call in the same order.
+struct Reducer {
+  double* buf;  // 2 * (NT/32) doubles
+  int parity;
+};
+
 template <int NT>
-__device__ __forceinline__ double block_sum(double v, double* red)
+__device__ __forceinline__ double block_sum(double v, Reducer& R)
 {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) red[wid] = v;
+  double* slot = R.buf + R.parity * (NT / 32);
+  R.parity ^= 1;
+  if ((threadIdx.x & 31) == 0) slot[threadIdx.x >> 5] = v;
   __syncthreads();
   double s = 0.0;
 #pragma unroll
-  for (int w = 0; w < NT / 32; ++w) s += red[w];
-  __syncthreads();
+  for (int w = 0; w < NT / 32; ++w) s += slot[w];
   return s;
 }
 
 template <int NT>
-__device__ __forceinline__ double block_max(double v, double* red)
+__device__ __forceinline__ double block_max(double v, Reducer& R)
 {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double* slot = R.buf + R.parity * (NT / 32);
+  R.parity ^= 1;
+  if ((threadIdx.x & 31) == 0) slot[threadIdx.x >> 5] = v;
   __syncthreads();
-  if (lane == 0) red[wid] = v;
-  __syncthreads();
-  double s = red[0];
+  double s = slot[0];
 #pragma unroll
-  for (int w = 1; w < NT / 32; ++w) s = fmax(s, red[w]);
-  __syncthreads();
+  for (int w = 1; w < NT / 32; ++w) s = fmax(s, slot[w]);
   return s;
 }
 
 // Full Frobenius inner product of two n x n column-major matrices.
 template <int NT>
-__device__ double dot_mat(int n, const double* A, int lda, const double* B, int ldb, double* red)
+__device__ double dot_mat(int n, const double* A, const double* B, Reducer& R)
 {
   double s = 0.0;
   const int tot = n * n;
-  for (int t = threadIdx.x; t < tot; t += NT) {
-    int i = t % n, j = t / n;
-    s += A[i + (size_t)lda * j] * B[i + (size_t)ldb * j];
-  }
-  return block_sum<NT>(s, red);
+  for (int t = threadIdx.x; t < tot; t += NT) s += A[t] * B[t];
+  return block_sum<NT>(s, R);
 }
 
 template <int NT>
-__device__ double trace(int n, const double* A, int lda, double* red)
+__device__ double trace(int n, const double* A, Reducer& R)
 {
   double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += NT) s += A[i + (size_t)lda * i];
-  return block_sum<NT>(s, red);
+  for (int i = threadIdx.x; i < n; i += NT) s += A[i + (size_t)n * i];
+  return block_sum<NT>(s, R);
 }
 
 template <int NT>
-__device__ double dot_vec(int n, const double* a, const double* b, double* red)
+__device__ double dot_vec(int n, const double* a, const double* b, Reducer& R)
 {
   double s = 0.0;
   for (int i = threadIdx.x; i < n; i += NT) s += a[i] * b[i];
-  return block_sum<NT>(s, red);
+  return block_sum<NT>(s, R);
 }
 
 // ------------------------------------------------------------ GEMM
-// C = alpha * op(A) * op(B) + beta * C for square n x n operands.
+// C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C.
 // 64 x 64 output tiles, 256 threads as a 16 x 16 grid with 4 x 4 outputs each
 // (rows ty + 16 i, columns tx + 16 j), K staged in chunks of 32.
-// smem: 2 * 32 * 64 doubles.
-constexpr int GT = 64, GK = 32;
+// lower = true updates only entries with (row + diag_off >= col) and skips
+// tiles entirely above that diagonal (trailing updates of factorisations).
+// smem: 2 * 32 * 64 doubles.  Ends with a barrier.
+constexpr int GT = 64, GK = 16;
 template <int NT>
-__device__ void gemm(int n, bool tA, const double* A, int lda, bool tB, const double* B, int ldb,
-                     double* C, int ldc, double alpha, double beta, double* smem)
+__device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const double* A, int lda, bool tB,
+                          const double* B, int ldb, double* C, int ldc, double alpha, double beta,
+                          double* smem, bool lower = false, int diag_off = 0)
 {
   static_assert(NT == 256, "gemm tile mapping assumes 256 threads");
+  constexpr int PER = GK * GT / NT;  // staged elements per thread and operand (8)
   double* As = smem;             // [GK][GT]  As[k*GT + r]
   double* Bs = smem + GK * GT;   // [GK][GT]  Bs[k*GT + c]
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int tiles = (n + GT - 1) / GT;
-  for (int tile = 0; tile < tiles * tiles; ++tile) {
-    const int r0 = (tile % tiles) * GT, c0 = (tile / tiles) * GT;
+  const int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT;
+  double ra[PER], rb[PER];
+  // global -> registers for the chunk (r0, c0, k0); the loads of the next
+  // chunk are issued before the current chunk is multiplied.
+  auto fetch = [&](int r0, int c0, int k0) {
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int t = threadIdx.x + u * NT;
+      int r, k;
+      if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
+      const int gr = r0 + r, gk = k0 + k;
+      ra[u] = (gr < M && gk < K) ? (tA ? A[gk + (size_t)lda * gr] : A[gr + (size_t)lda * gk]) : 0.0;
+      int c;
+      if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
+      const int gc = c0 + c, gk2 = k0 + k;
+      rb[u] = (gc < N && gk2 < K) ? (tB ? B[gc + (size_t)ldb * gk2] : B[gk2 + (size_t)ldb * gc]) : 0.0;
+    }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int t = threadIdx.x + u * NT;
+      int r, k;
+      if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
+      As[k * GT + r] = ra[u];
+      int c;
+      if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
+      Bs[k * GT + c] = rb[u];
+    }
+  };
+  // list of (tile, k0) steps, skipping tiles above the diagonal when lower
+  auto tile_live = [&](int tile) {
+    const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
+    return !(lower && r0 + GT - 1 + diag_off < c0);
+  };
+  int tile = 0;
+  while (tile < tm * tn && !tile_live(tile)) ++tile;
+  if (tile < tm * tn) fetch((tile % tm) * GT, (tile / tm) * GT, 0);
+  while (tile < tm * tn) {
+    const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
     double acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    for (int k0 = 0; k0 < n; k0 += GK) {
-      // stage op(A)[r0:r0+64, k0:k0+32] and op(B)[k0:k0+32, c0:c0+64]
-      for (int t = threadIdx.x; t < GK * GT; t += NT) {
-        int r, k;
-        if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
-        int gr = r0 + r, gk = k0 + k;
-        double v = 0.0;
-        if (gr < n && gk < n) v = tA ? A[gk + (size_t)lda * gr] : A[gr + (size_t)lda * gk];
-        As[k * GT + r] = v;
-      }
-      for (int t = threadIdx.x; t < GK * GT; t += NT) {
-        int c, k;
-        if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
-        int gc = c0 + c, gk = k0 + k;
-        double v = 0.0;
-        if (gc < n && gk < n) v = tB ? B[gc + (size_t)ldb * gk] : B[gk + (size_t)ldb * gc];
-        Bs[k * GT + c] = v;
-      }
+    int next = tile + 1;
+    while (next < tm * tn && !tile_live(next)) ++next;
+    for (int k0 = 0; k0 < K; k0 += GK) {
+      store();
       __syncthreads();
-      const int kmax = min(GK, n - k0);
+      if (k0 + GK < K) fetch(r0, c0, k0 + GK);
+      else if (next < tm * tn) fetch((next % tm) * GT, (next / tm) * GT, 0);
+      const int kmax = min(GK, K - k0);
       for (int k = 0; k < kmax; ++k) {
         double a[4], b[4];
 #pragma unroll
@@ -128,12 +170,72 @@ __device__ void gemm(int n, bool tA, const double* A, int lda, bool tB, const do
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      int gr = r0 + ty + 16 * i;
-      if (gr >= n) continue;
+      const int gr = r0 + ty + 16 * i;
+      if (gr >= M) continue;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        int gc = c0 + tx + 16 * j;
-        if (gc >= n) continue;
+        const int gc = c0 + tx + 16 * j;
+        if (gc >= N) continue;
+        if (lower && gr + diag_off < gc) continue;
+        double* cp = C + gr + (size_t)ldc * gc;
+        *cp = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
+      }
+    }
+    tile = next;
+  }
+  __syncthreads();
+}
+
+// Square n x n product as ONE output tile of (16 R) x (16 R), R = ceil(n/16)
+// (n <= 96): thread (tx, ty) of the 16 x 16 grid owns rows ty + 16 i and
+// columns tx + 16 j, i, j < R, so no padding beyond the next multiple of 16
+// is computed.  K is staged in chunks of 16 (smem 2 * 16 * 16R doubles).
+template <int NT, int R>
+__device__ __noinline__ void gemm_tile(int n, bool tA, const double* A, int lda, bool tB, const double* B, int ldb,
+                          double* C, int ldc, double alpha, double beta, double* smem)
+{
+  constexpr int T = 16 * R, KC = 16;
+  double* As = smem;            // [KC][T]
+  double* Bs = smem + KC * T;   // [KC][T]
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[R][R];
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+#pragma unroll
+    for (int j = 0; j < R; ++j) acc[i][j] = 0.0;
+  for (int k0 = 0; k0 < n; k0 += KC) {
+    for (int t = threadIdx.x; t < KC * T; t += NT) {
+      int r, k;
+      if (!tA) { r = t % T; k = t / T; } else { k = t % KC; r = t / KC; }
+      const int gk = k0 + k;
+      As[k * T + r] = (r < n && gk < n) ? (tA ? A[gk + (size_t)lda * r] : A[r + (size_t)lda * gk]) : 0.0;
+      int c;
+      if (!tB) { k = t % KC; c = t / KC; } else { c = t % T; k = t / T; }
+      const int gk2 = k0 + k;
+      Bs[k * T + c] = (c < n && gk2 < n) ? (tB ? B[c + (size_t)ldb * gk2] : B[gk2 + (size_t)ldb * c]) : 0.0;
+    }
+    __syncthreads();
+    const int kmax = min(KC, n - k0);
+    for (int k = 0; k < kmax; ++k) {
+      double a[R], b[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) a[i] = As[k * T + ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < R; ++j) b[j] = Bs[k * T + tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < R; ++i)
+#pragma unroll
+        for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int gr = ty + 16 * i;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int gc = tx + 16 * j;
+      if (gr < n && gc < n) {
         double* cp = C + gr + (size_t)ldc * gc;
         *cp = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
       }
@@ -142,201 +244,387 @@ __device__ void gemm(int n, bool tA, const double* A, int lda, bool tB, const do
   __syncthreads();
 }
 
-// ------------------------------------------------------------ Cholesky
-// In-place lower Cholesky (right-looking).  adjust = true applies the
-// reference's Schur-complement rule (rATL_dpotrfL, sdpa_dpotrf.cpp:31-33):
-// pivot < -1e-6 fails, pivot < 1e-14 becomes 1e100.  adjust = false is
-// LAPACK dpotrf's rule (pivot <= 0 or NaN fails).  Returns 0 on success, else
-// the failing column + 1.  The strict upper triangle is zeroed.
+// Square GEMM dispatch: one exact-size tile for n <= 96, 64 x 64 tiles above.
+// smem must hold 2 * 16 * 96 doubles.
 template <int NT>
-__device__ int cholesky(int n, double* A, int lda, bool adjust, int* s_flag)
+__device__ __forceinline__ void gemm(int n, bool tA, const double* A, int lda, bool tB, const double* B,
+                                     int ldb, double* C, int ldc, double alpha, double beta, double* smem)
 {
-  for (int j = 0; j < n; ++j) {
-    if (threadIdx.x == 0) {
-      double d = A[j + (size_t)lda * j];
-      int fail = 0;
+  if (n <= 32) gemm_tile<NT, 2>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+  else if (n <= 48) gemm_tile<NT, 3>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+  else if (n <= 64) gemm_tile<NT, 4>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+  else if (n <= 80) gemm_tile<NT, 5>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+  else if (n <= 96) gemm_tile<NT, 6>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+  else gemm_rect<NT>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+}
+
+// ------------------------------------------------------------ warp Cholesky
+// Factors the bs x bs (bs <= 32) lower triangle held in sD (leading
+// dimension LDD) in place with one warp: lane r keeps row r in registers and
+// the column of each step is broadcast with shuffles (no shared-memory
+// traffic inside the factorisation).  Pivot rules as cholesky() below; kb is
+// the block's offset, used in the returned failing column (0 = success).
+__device__ __noinline__ int warp_potrf32(int bs, double* sD, bool adjust, int kb)
+{
+  const int lane = threadIdx.x & 31;
+  double a[32];
+#pragma unroll
+  for (int c = 0; c < 32; ++c) a[c] = (c <= lane && lane < bs) ? sD[lane + LDD * c] : 0.0;
+  int fail = 0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < bs && !fail) {
+      double d = __shfl_sync(0xffffffffu, a[j], j);
       if (adjust) {
-        if (d < -1.0e-6 || d != d) fail = 1;
+        if (d < -1.0e-6 || d != d) fail = kb + j + 1;
         else if (d < 1.0e-14) d = 1.0e100;
       } else if (!(d > 0.0)) {
-        fail = 1;
+        fail = kb + j + 1;
       }
-      if (!fail) A[j + (size_t)lda * j] = sqrt(d);
-      *s_flag = fail ? j + 1 : 0;
+      if (!fail) {
+        const double ljj = sqrt(d);
+        const double inv = 1.0 / ljj;
+        if (lane == j) a[j] = ljj;
+        else if (lane > j) a[j] *= inv;
+        const double lrj = a[j];
+#pragma unroll
+        for (int c = j + 1; c < 32; ++c) {
+          const double lcj = __shfl_sync(0xffffffffu, lrj, c);
+          if (lane >= c) a[c] -= lrj * lcj;
+        }
+      }
     }
-    __syncthreads();
-    if (*s_flag) { int f = *s_flag; __syncthreads(); return f; }
-    const double inv = 1.0 / A[j + (size_t)lda * j];
-    for (int i = j + 1 + threadIdx.x; i < n; i += NT) A[i + (size_t)lda * j] *= inv;
-    __syncthreads();
-    const int rem = n - j - 1;
-    for (int t = threadIdx.x; t < rem * rem; t += NT) {
-      int i = j + 1 + t % rem, k = j + 1 + t / rem;
-      if (i >= k) A[i + (size_t)lda * k] -= A[i + (size_t)lda * j] * A[k + (size_t)lda * j];
-    }
-    __syncthreads();
   }
-  for (int t = threadIdx.x; t < n * n; t += NT) {
-    int i = t % n, k = t / n;
+  if (!fail && lane < bs) {
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+      if (c <= lane) sD[lane + LDD * c] = a[c];
+  }
+  return fail;
+}
+
+// ------------------------------------------------------------ Cholesky
+// In-place lower Cholesky, right-looking, blocked by 32.  adjust = true is
+// the reference's Schur-complement rule (rATL_dpotrfL,
+// sdpa_dpotrf.cpp:31-33): pivot < -1e-6 fails, pivot < 1e-14 becomes 1e100.
+// adjust = false is LAPACK dpotrf's rule (pivot <= 0 or NaN fails).  NaN
+// pivots fail under both rules.  Returns 0 on success, else the failing
+// column + 1.  The strict upper triangle is zeroed on success.
+// sD: SD_DOUBLES doubles; smem: GEMM staging.
+template <int NT>
+__device__ int cholesky(int n, double* A, int lda, bool adjust, double* sD, double* smem, int* s_flag)
+{
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int kb = 0; kb < n; kb += NB) {
+    const int bs = min(NB, n - kb);
+    // (a) diagonal block: staged by all threads, factored by warp 0 (lane r owns row r)
+    for (int t = tid; t < NB * NB; t += NT) {
+      const int r = t % NB, c = t / NB;
+      if (r < bs && c <= r) sD[r + LDD * c] = A[(kb + r) + (size_t)lda * (kb + c)];
+    }
+    __syncthreads();
+    if (wid == 0) {
+      const int fail = warp_potrf32(bs, sD, adjust, kb);
+      if (lane == 0) *s_flag = fail;
+      if (!fail && lane < bs) sD[NB * LDD + lane] = 1.0 / sD[lane + LDD * lane];
+    }
+    __syncthreads();
+    const int f = *s_flag;
+    if (f) { __syncthreads(); return f; }
+    for (int t = tid; t < NB * NB; t += NT) {
+      const int r = t % NB, c = t / NB;
+      if (r < bs && c <= r) A[(kb + r) + (size_t)lda * (kb + c)] = sD[r + LDD * c];
+    }
+    const int r0 = kb + bs, rem = n - r0;
+    if (rem > 0) {
+      // (b) panel: A[r, kb:kb+bs] := A[r, kb:kb+bs] L_bb^{-T}; each warp solves
+      //     four rows at a time (four independent shuffle chains)
+      for (int rb = r0 + 4 * wid; rb < n; rb += 4 * (NT / 32)) {
+        double x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          x[u] = (lane < bs && rb + u < n) ? A[(rb + u) + (size_t)lda * (kb + lane)] : 0.0;
+        for (int c = 0; c < bs; ++c) {
+          const double dinv = sD[NB * LDD + c];
+          const double lc = (lane > c && lane < bs) ? sD[lane + LDD * c] : 0.0;
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (lane == c) x[u] *= dinv;
+            const double xc = __shfl_sync(0xffffffffu, x[u], c);
+            x[u] -= xc * lc;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (lane < bs && rb + u < n) A[(rb + u) + (size_t)lda * (kb + lane)] = x[u];
+      }
+      __syncthreads();
+      // (c) trailing: A22 -= P P^T (lower triangle), P = A[r0:, kb:kb+bs]
+      const double* P = A + r0 + (size_t)lda * kb;
+      gemm_rect<NT>(rem, rem, bs, false, P, lda, true, P, lda, A + r0 + (size_t)lda * r0, lda, -1.0, 1.0,
+                    smem, true, 0);
+    }
+  }
+  for (int t = tid; t < n * n; t += NT) {
+    const int i = t % n, k = t / n;
     if (i < k) A[i + (size_t)lda * k] = 0.0;
   }
   __syncthreads();
   return 0;
 }
 
-// Linv = L^{-1} for lower-triangular L (right-looking forward substitution on
-// all columns at once).  Linv must not alias L.
+// Li = L^{-1} for lower-triangular L: solves L Li = I blocked by 32
+// (diagonal block substitution one warp per column, trailing GEMM update).
+// Li must not alias L.
 template <int NT>
-__device__ void tri_inverse(int n, const double* L, int ldl, double* Li, int ldi)
+__device__ void tri_inverse(int n, const double* L, int ldl, double* Li, int ldi, double* sD, double* smem)
 {
-  for (int t = threadIdx.x; t < n * n; t += NT) {
-    int i = t % n, j = t / n;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int t = tid; t < n * n; t += NT) {
+    const int i = t % n, j = t / n;
     Li[i + (size_t)ldi * j] = (i == j) ? 1.0 : 0.0;
   }
-  __syncthreads();
-  for (int k = 0; k < n; ++k) {
-    const double inv = 1.0 / L[k + (size_t)ldl * k];
-    for (int j = threadIdx.x; j <= k; j += NT) Li[k + (size_t)ldi * j] *= inv;
+  for (int kb = 0; kb < n; kb += NB) {
+    const int bs = min(NB, n - kb);
+    for (int t = tid; t < NB * NB; t += NT) {
+      const int r = t % NB, c = t / NB;
+      if (r < bs && c <= r) sD[r + LDD * c] = L[(kb + r) + (size_t)ldl * (kb + c)];
+    }
+    for (int r = tid; r < bs; r += NT) sD[NB * LDD + r] = 1.0 / L[(kb + r) + (size_t)ldl * (kb + r)];
     __syncthreads();
-    const int rows = n - k - 1, cols = k + 1;
-    for (int t = threadIdx.x; t < rows * cols; t += NT) {
-      int i = k + 1 + t % rows, j = t / rows;
-      Li[i + (size_t)ldi * j] -= L[i + (size_t)ldl * k] * Li[k + (size_t)ldi * j];
+    // (a) Li[kb:kb+bs, 0:kb+bs] = L_bb^{-1} Li[kb:kb+bs, 0:kb+bs], four columns per warp
+    for (int cb = 4 * wid; cb < kb + bs; cb += 4 * (NT / 32)) {
+      double x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        x[u] = (lane < bs && cb + u < kb + bs) ? Li[(kb + lane) + (size_t)ldi * (cb + u)] : 0.0;
+      for (int p = 0; p < bs; ++p) {
+        const double dinv = sD[NB * LDD + p];
+        const double lp = (lane > p && lane < bs) ? sD[lane + LDD * p] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (lane == p) x[u] *= dinv;
+          const double xp = __shfl_sync(0xffffffffu, x[u], p);
+          x[u] -= lp * xp;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (lane < bs && cb + u < kb + bs) Li[(kb + lane) + (size_t)ldi * (cb + u)] = x[u];
+    }
+    __syncthreads();
+    // (b) Li[kb+bs:, 0:kb+bs] -= L[kb+bs:, kb:kb+bs] Li[kb:kb+bs, 0:kb+bs]
+    const int r0 = kb + bs, rem = n - r0;
+    if (rem > 0)
+      gemm_rect<NT>(rem, kb + bs, bs, false, L + r0 + (size_t)ldl * kb, ldl, false, Li + kb, ldi,
+                    Li + r0, ldi, -1.0, 1.0, smem);
+  }
+  __syncthreads();
+}
+
+// x = L^{-T} L^{-1} x for a Cholesky factor L (lower); x in shared memory.
+// Blocked by 32: each diagonal block is staged in shared memory by all
+// threads and solved by warp 0 with shuffles; the other rows are updated
+// block-wide.  sD: SD_DOUBLES doubles.
+template <int NT>
+__device__ void chol_solve(int n, const double* L, int ldl, double* x, double* sD)
+{
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  auto stage = [&](int kb, int bs) {
+    for (int t = tid; t < NB * NB; t += NT) {
+      const int r = t % NB, c = t / NB;
+      if (r < bs && c <= r) sD[r + LDD * c] = L[(kb + r) + (size_t)ldl * (kb + c)];
+    }
+    for (int r = tid; r < bs; r += NT) sD[NB * LDD + r] = 1.0 / L[(kb + r) + (size_t)ldl * (kb + r)];
+    __syncthreads();
+  };
+  // forward: L z = x
+  for (int kb = 0; kb < n; kb += NB) {
+    const int bs = min(NB, n - kb);
+    stage(kb, bs);
+    if (wid == 0) {
+      double v = (lane < bs) ? x[kb + lane] : 0.0;
+      for (int p = 0; p < bs; ++p) {
+        if (lane == p) v *= sD[NB * LDD + p];
+        const double vp = __shfl_sync(0xffffffffu, v, p);
+        if (lane > p && lane < bs) v -= sD[lane + LDD * p] * vp;
+      }
+      if (lane < bs) x[kb + lane] = v;
+    }
+    __syncthreads();
+    for (int i = kb + bs + tid; i < n; i += NT) {
+      double s = 0.0;
+#pragma unroll 8
+      for (int p = 0; p < bs; ++p) s += L[i + (size_t)ldl * (kb + p)] * x[kb + p];
+      x[i] -= s;
     }
     __syncthreads();
   }
-}
-
-// x = L^{-T} L^{-1} x for a Cholesky factor L (lower), vector in shared memory.
-// Row-oriented substitution: each step is a block-wide dot product.
-template <int NT>
-__device__ void chol_solve(int n, const double* L, int ldl, double* x, double* red)
-{
-  // forward: L z = x
-  for (int i = 0; i < n; ++i) {
-    double s = 0.0;
-    for (int k = threadIdx.x; k < i; k += NT) s += L[i + (size_t)ldl * k] * x[k];
-    s = block_sum<NT>(s, red);
-    if (threadIdx.x == 0) x[i] = (x[i] - s) / L[i + (size_t)ldl * i];
-    __syncthreads();
-  }
   // backward: L^T x = z
-  for (int i = n - 1; i >= 0; --i) {
-    double s = 0.0;
-    for (int k = i + 1 + threadIdx.x; k < n; k += NT) s += L[k + (size_t)ldl * i] * x[k];
-    s = block_sum<NT>(s, red);
-    if (threadIdx.x == 0) x[i] = (x[i] - s) / L[i + (size_t)ldl * i];
+  const int nblk = (n + NB - 1) / NB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int kb = b * NB, bs = min(NB, n - kb);
+    stage(kb, bs);
+    if (wid == 0) {
+      double v = (lane < bs) ? x[kb + lane] : 0.0;
+      for (int p = bs - 1; p >= 0; --p) {
+        if (lane == p) v *= sD[NB * LDD + p];
+        const double vp = __shfl_sync(0xffffffffu, v, p);
+        if (lane < p) v -= sD[p + LDD * lane] * vp;
+      }
+      if (lane < bs) x[kb + lane] = v;
+    }
+    __syncthreads();
+    for (int i = wid; i < kb; i += NT / 32) {
+      double s = (lane < bs) ? L[(kb + lane) + (size_t)ldl * i] * x[kb + lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) x[i] -= s;
+    }
     __syncthreads();
   }
 }
 
 // ------------------------------------------------------------ eigenvalues
-// Number of eigenvalues < x of the symmetric tridiagonal (d, e) of order k
-// (Sturm sequence count).
+// Number of eigenvalues < x of the symmetric tridiagonal (d, e) of order k:
+// sign changes of the leading principal minors p_i(x) of T - xI (Sturm
+// sequence), by the division-free recurrence
+//   p_{i+1} = (d_i - x) p_i - e_{i-1}^2 p_{i-1},
+// rescaled by a power of two whenever |p_i| leaves [2^-400, 2^400].
 __device__ __forceinline__ int sturm_count(int k, const double* d, const double* e, double x)
 {
-  int cnt = 0;
-  double q = 1.0;
-  for (int i = 0; i < k; ++i) {
-    double off = (i > 0) ? e[i - 1] * e[i - 1] : 0.0;
-    q = d[i] - x - ((i > 0) ? off / q : 0.0);
-    if (q == 0.0) q = -1.0e-300;
-    if (q < 0.0) ++cnt;
+  double pm = 1.0, p = d[0] - x;
+  int cnt = (p < 0.0) ? 1 : 0;
+  for (int i = 1; i < k; ++i) {
+    double pn = (d[i] - x) * p - e[i - 1] * e[i - 1] * pm;
+    if (pn == 0.0) pn = (p < 0.0) ? 1.0e-300 : -1.0e-300;  // a zero minor counts as a sign change
+    cnt += ((pn < 0.0) != (p < 0.0)) ? 1 : 0;
+    pm = p;
+    p = pn;
+    const int ex = ilogb(p);
+    if (ex > 400 || ex < -400) {
+      p = scalbn(p, -ex);
+      pm = scalbn(pm, -ex);
+    }
   }
   return cnt;
 }
 
-// Smallest eigenvalue of a symmetric tridiagonal (d, e) of order k by warp
-// multisection of the Gershgorin interval (each round splits the bracket into
-// 33 parts).  Called by one full warp; every lane returns the value.
+// Smallest eigenvalue of a symmetric tridiagonal (d, e) of order k.  Warp
+// multisection of the Gershgorin interval (33 parts per round) until the
+// bracket is narrow, then Newton steps on det(T - xI) (its smallest root is
+// approached monotonically from the left), each kept inside the bracket,
+// until the step is below one ulp.  Called by one full warp; every lane
+// returns the value.
 __device__ double tridiag_min_eig_warp(int k, const double* d, const double* e)
 {
   const int lane = threadIdx.x & 31;
   double lo = 1.0e300, hi = -1.0e300;
   for (int i = 0; i < k; ++i) {
-    double r = ((i > 0) ? fabs(e[i - 1]) : 0.0) + ((i < k - 1) ? fabs(e[i]) : 0.0);
+    const double r = ((i > 0) ? fabs(e[i - 1]) : 0.0) + ((i < k - 1) ? fabs(e[i]) : 0.0);
     lo = fmin(lo, d[i] - r);
     hi = fmax(hi, d[i] + r);
   }
-  double span = fmax(fabs(lo), fabs(hi));
+  const double span = fmax(fabs(lo), fabs(hi));
   lo -= 1.0e-15 * span + 1.0e-300;
   hi += 1.0e-15 * span + 1.0e-300;
   for (int round = 0; round < 24; ++round) {
-    double w = (hi - lo) / 33.0;
-    double x = lo + w * (lane + 1);
-    int c = sturm_count(k, d, e, x);
-    unsigned ball = __ballot_sync(0xffffffffu, c >= 1);
-    // first lane whose point has at least one eigenvalue below it
-    int f = ball ? (__ffs(ball) - 1) : 32;
-    double nlo = lo + w * f;
-    double nhi = (f < 32) ? lo + w * (f + 1) : hi;
+    const double w = (hi - lo) / 33.0;
+    const double x = lo + w * (lane + 1);
+    const int c = sturm_count(k, d, e, x);
+    const unsigned ball = __ballot_sync(0xffffffffu, c >= 1);
+    const int f = ball ? (__ffs(ball) - 1) : 32;  // first point with an eigenvalue below it
+    const double nlo = lo + w * f;
+    const double nhi = (f < 32) ? lo + w * (f + 1) : hi;
     lo = nlo;
     hi = nhi;
-    if (hi - lo <= 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1.0e-300) break;
+    if (hi - lo <= 1.0e-7 * fmax(fabs(lo), fabs(hi)) + 1.0e-300) break;
   }
-  return 0.5 * (lo + hi);
+  // Newton on f(x) = det(T - xI) from the left end of the bracket, with
+  // P_{i+1} = (d_i - x) P_i - e^2 P_{i-1} and its derivative
+  // D_{i+1} = -P_i + (d_i - x) D_i - e^2 D_{i-1}, rescaled together.
+  double x = lo;
+  for (int it = 0; it < 20; ++it) {
+    double Pm = 1.0, P = d[0] - x, Dm = 0.0, Dv = -1.0;
+    for (int i = 1; i < k; ++i) {
+      const double e2 = e[i - 1] * e[i - 1];
+      const double dx = d[i] - x;
+      const double Pn = dx * P - e2 * Pm;
+      const double Dn = -P + dx * Dv - e2 * Dm;
+      Pm = P; P = Pn; Dm = Dv; Dv = Dn;
+      const int ex = ilogb(fmax(fabs(P), fabs(Dv)));
+      if (ex > 400 || ex < -400) {
+        P = scalbn(P, -ex); Pm = scalbn(Pm, -ex); Dv = scalbn(Dv, -ex); Dm = scalbn(Dm, -ex);
+      }
+    }
+    if (!(Dv != 0.0) || P != P || Dv != Dv) break;
+    const double xn = x - P / Dv;
+    if (!(xn >= lo) || !(xn <= hi)) break;
+    if (fabs(xn - x) <= 2.2e-16 * fabs(xn)) { x = xn; break; }
+    x = xn;
+  }
+  return x;
 }
 
 // Last component (index k-1) of the unit eigenvector of the tridiagonal (d, e)
-// for eigenvalue lam, by two steps of inverse iteration with partial
-// pivoting.  Called by one thread; work needs 5*k doubles.
-__device__ double tridiag_evec_last(int k, const double* d, const double* e, double lam,
-                                    double* work)
+// for eigenvalue lam: two steps of inverse iteration on T - (lam - tiny) I
+// with partial pivoting (pivot reciprocals computed once).  Called by one
+// thread; work needs 6*k doubles; k <= 64.
+__device__ double tridiag_evec_last(int k, const double* d, const double* e, double lam, double* work)
 {
-  if (k == 1) return 1.0;
-  double* a = work;          // sub
-  double* b = work + k;      // diag
-  double* c = work + 2 * k;  // super
-  double* c2 = work + 3 * k; // second super (fill-in from pivoting)
+  if (k <= 1) return 1.0;
+  if (k > 64) k = 64;
+  double* a = work;           // sub-diagonal (row i, column i-1)
+  double* b = work + k;       // diagonal, then its reciprocal
+  double* c = work + 2 * k;   // first super-diagonal
+  double* c2 = work + 3 * k;  // second super-diagonal (fill-in of pivoting)
   double* v = work + 4 * k;
+  double* pl = work + 5 * k;  // multipliers
+  unsigned long long swp = 0ull;
   double span = 0.0;
   for (int i = 0; i < k; ++i) span = fmax(span, fabs(d[i]) + ((i < k - 1) ? fabs(e[i]) : 0.0));
-  double shift = lam - 1.0e-13 * (span + 1.0e-300);
-  for (int i = 0; i < k; ++i) v[i] = 1.0;
-  // LU with partial pivoting of the tridiagonal T - shift I.
-  double* piv_l = work + 5 * k;  // multipliers, k doubles
-  int pivrow[64];
-  for (int i = 0; i < k; ++i) { a[i] = (i > 0) ? e[i - 1] : 0.0; b[i] = d[i] - shift; c[i] = (i < k - 1) ? e[i] : 0.0; c2[i] = 0.0; }
+  const double shift = lam - 1.0e-13 * (span + 1.0e-300);
+  for (int i = 0; i < k; ++i) {
+    a[i] = (i > 0) ? e[i - 1] : 0.0;
+    b[i] = d[i] - shift;
+    c[i] = (i < k - 1) ? e[i] : 0.0;
+    c2[i] = 0.0;
+    v[i] = 1.0;
+  }
   for (int i = 0; i < k - 1; ++i) {
-    // rows i and i+1; a[i+1] is the entry below the pivot
-    if (fabs(a[i + 1]) > fabs(b[i])) {
-      // swap rows i and i+1
+    if (fabs(a[i + 1]) > fabs(b[i])) {  // swap rows i and i+1
       double t;
       t = b[i]; b[i] = a[i + 1]; a[i + 1] = t;
       t = c[i]; c[i] = b[i + 1]; b[i + 1] = t;
       t = c2[i]; c2[i] = c[i + 1]; c[i + 1] = t;
-      pivrow[i] = 1;
-    } else {
-      pivrow[i] = 0;
+      swp |= (1ull << i);
     }
-    double piv = (b[i] != 0.0) ? b[i] : 1.0e-300;
-    double l = a[i + 1] / piv;
-    piv_l[i] = l;
+    const double rinv = 1.0 / ((b[i] != 0.0) ? b[i] : 1.0e-300);
+    b[i] = rinv;
+    const double l = a[i + 1] * rinv;
+    pl[i] = l;
     b[i + 1] -= l * c[i];
     c[i + 1] -= l * c2[i];
   }
-  if (b[k - 1] == 0.0) b[k - 1] = 1.0e-300;
+  b[k - 1] = 1.0 / ((b[k - 1] != 0.0) ? b[k - 1] : 1.0e-300);
   for (int itn = 0; itn < 2; ++itn) {
-    // apply row swaps and L^{-1}
     for (int i = 0; i < k - 1; ++i) {
-      if (pivrow[i]) { double t = v[i]; v[i] = v[i + 1]; v[i + 1] = t; }
-      v[i + 1] -= piv_l[i] * v[i];
+      if (swp & (1ull << i)) { const double t = v[i]; v[i] = v[i + 1]; v[i + 1] = t; }
+      v[i + 1] -= pl[i] * v[i];
     }
-    // back substitution with U (diag b, super c, super2 c2)
+    double nrm = 0.0;
     for (int i = k - 1; i >= 0; --i) {
       double s = v[i];
       if (i + 1 < k) s -= c[i] * v[i + 1];
       if (i + 2 < k) s -= c2[i] * v[i + 2];
-      double piv = (b[i] != 0.0) ? b[i] : 1.0e-300;
-      v[i] = s / piv;
+      v[i] = s * b[i];
+      nrm = fmax(nrm, fabs(v[i]));
     }
-    double nrm = 0.0;
-    for (int i = 0; i < k; ++i) nrm = fmax(nrm, fabs(v[i]));
-    for (int i = 0; i < k; ++i) v[i] /= nrm;
+    const double inv = 1.0 / nrm;
+    for (int i = 0; i < k; ++i) v[i] *= inv;
   }
   double s2 = 0.0;
   for (int i = 0; i < k; ++i) s2 += v[i] * v[i];
-  return v[k - 1] / sqrt(s2);
+  return v[k - 1] * rsqrt(s2);
 }
 
 }  // namespace cta
