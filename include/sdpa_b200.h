@@ -81,6 +81,64 @@ SDPAB_API const char* sdpab_last_error(void);
 /* Library version string. */
 SDPAB_API const char* sdpab_version(void);
 
+/* ------------------------------------------------------- whole-problem API */
+
+/* Opaque handle of one problem: a C binding of the drop-in C++ class SDPA
+ * (sdpa_call.h in this directory), for FFI callers.  The solve is the
+ * host-driven CUDA solver: any number of SDP blocks plus LP blocks. */
+typedef struct sdpab_sdpa sdpab_sdpa;
+
+typedef struct sdpab_sdpa_info_t {
+  double primal_obj, dual_obj;       /* getPrimalObj / getDualObj */
+  double primal_error, dual_error;   /* getPrimalError / getDualError */
+  double mu, duality_gap;            /* getMu / getDualityGap */
+  double solve_seconds;              /* getSolveTime */
+  int iterations;                    /* getIteration */
+  int phase;                         /* getPhaseValue code */
+  int m, nblock;                     /* getConstraintNumber / getBlockNumber */
+} sdpab_sdpa_info_t;
+
+/* new SDPA() / delete (sdpa_call.cpp:38-55) */
+SDPAB_API sdpab_sdpa* sdpab_sdpa_new(void);
+SDPAB_API void sdpab_sdpa_free(sdpab_sdpa* h);
+/* setParameter* (sdpa_call.cpp:62-143) from the ten numeric parameters */
+SDPAB_API int sdpab_sdpa_set_params(sdpab_sdpa* h, const sdpab_params* prm);
+/* SDPA::readInput (sdpa_call.cpp:897-944); sparse_type: 0 AUTO (by the
+ * ".dat-s" suffix), 1 SPARSE, 2 DENSE */
+SDPAB_API int sdpab_sdpa_read_input(sdpab_sdpa* h, const char* path, int sparse_type);
+/* SDPA::setInitPoint(true) + SDPA::readInit (sdpa_call.cpp:946-991) */
+SDPAB_API int sdpab_sdpa_read_init(sdpab_sdpa* h, const char* path, int sparse_type);
+/* SDPA::readParameter (sdpa_call.cpp:993-1003) */
+SDPAB_API int sdpab_sdpa_read_param(sdpab_sdpa* h, const char* path);
+/* inputConstraintNumber / inputBlockNumber / inputBlockSize / inputBlockType /
+ * inputCVec / inputElement (sdpa_call.cpp:245-341) for nnz 1-based entries
+ * (k = 0 is F0) followed by initializeUpperTriangle */
+SDPAB_API int sdpab_sdpa_input_problem(sdpab_sdpa* h, int m, int nblock, const int* block_struct,
+                                       const double* c, long long nnz, const int* k, const int* l,
+                                       const int* i, const int* j, const double* v);
+/* setInitPoint(true) + inputInitXVec / inputInitXMat / inputInitYMat
+ * (sdpa_call.cpp:148-159, :343-434); X[l], Y[l] dense column-major per SDP
+ * block, a vector per LP block */
+SDPAB_API int sdpab_sdpa_set_init(sdpab_sdpa* h, const double* xvec, const double* const* X,
+                                  const double* const* Y);
+/* SDPA::initializeSolve + SDPA::solve (sdpa_solve.cpp:10-43, :59-233) */
+SDPAB_API int sdpab_sdpa_solve(sdpab_sdpa* h);
+/* scalar getters (sdpa_call.cpp:719-847) */
+SDPAB_API int sdpab_sdpa_info(sdpab_sdpa* h, sdpab_sdpa_info_t* out);
+/* getResultXVec (sdpa_call.cpp:668-671), copied into out[m] */
+SDPAB_API int sdpab_sdpa_get_xvec(sdpab_sdpa* h, double* out);
+/* getResultXMat (which = 0) / getResultYMat (which = 1) of block l
+ * (sdpa_call.cpp:673-717), copied into out */
+SDPAB_API int sdpab_sdpa_get_block(sdpab_sdpa* h, int l, int which, double* out);
+/* getBlockSize / getBlockType (sdpa_call.cpp:813-847) */
+SDPAB_API int sdpab_sdpa_block_size(sdpab_sdpa* h, int l, int* size, int* is_sdp);
+/* SDPA::getDimacsError (IO::computeDimacs, sdpa_io.cpp:775-813): err7[1..6] */
+SDPAB_API int sdpab_sdpa_dimacs(sdpab_sdpa* h, double* err7);
+/* SDPA::writeInitSparse (sdpa_call.cpp:1199-1220) */
+SDPAB_API int sdpab_sdpa_write_init(sdpab_sdpa* h, const char* path);
+/* SDPA::copyCurrentToInit (sdpa_call.cpp:1238-1245) + setInitPoint(true) */
+SDPAB_API int sdpab_sdpa_copy_current_to_init(sdpab_sdpa* h);
+
 /* ---------------------------------------------------------------- batched API */
 
 /* Precision modes of the batched solver. */

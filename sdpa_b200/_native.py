@@ -47,6 +47,13 @@ class BatchConfig(ctypes.Structure):
     _fields_ = [("precision", c_int), ("ctas_per_sm", c_int), ("mixed_mu_switch", c_double)]
 
 
+class SdpaInfo(ctypes.Structure):
+    _fields_ = [("primal_obj", c_double), ("dual_obj", c_double), ("primal_error", c_double),
+                ("dual_error", c_double), ("mu", c_double), ("duality_gap", c_double),
+                ("solve_seconds", c_double), ("iterations", c_int), ("phase", c_int), ("m", c_int),
+                ("nblock", c_int)]
+
+
 # (name, restype, argtypes) of every exported function of include/sdpa_b200.h
 SIGNATURES = [
     ("sdpab_default_params", c_int, [c_int, POINTER(Params)]),
@@ -60,6 +67,23 @@ SIGNATURES = [
     ("sdpab_batch_solve_noalloc", c_int, [POINTER(Batch), POINTER(BatchInit), POINTER(Params),
                                           POINTER(BatchResult), c_void_p, c_void_p]),
     ("sdpab_workspace_bytes", c_longlong, []),
+    ("sdpab_sdpa_new", c_void_p, []),
+    ("sdpab_sdpa_free", None, [c_void_p]),
+    ("sdpab_sdpa_set_params", c_int, [c_void_p, POINTER(Params)]),
+    ("sdpab_sdpa_read_input", c_int, [c_void_p, c_char_p, c_int]),
+    ("sdpab_sdpa_read_init", c_int, [c_void_p, c_char_p, c_int]),
+    ("sdpab_sdpa_read_param", c_int, [c_void_p, c_char_p]),
+    ("sdpab_sdpa_input_problem", c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_longlong, c_void_p,
+                                         c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sdpab_sdpa_set_init", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sdpab_sdpa_solve", c_int, [c_void_p]),
+    ("sdpab_sdpa_info", c_int, [c_void_p, POINTER(SdpaInfo)]),
+    ("sdpab_sdpa_get_xvec", c_int, [c_void_p, c_void_p]),
+    ("sdpab_sdpa_get_block", c_int, [c_void_p, c_int, c_int, c_void_p]),
+    ("sdpab_sdpa_block_size", c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),
+    ("sdpab_sdpa_dimacs", c_int, [c_void_p, c_void_p]),
+    ("sdpab_sdpa_write_init", c_int, [c_void_p, c_char_p]),
+    ("sdpab_sdpa_copy_current_to_init", c_int, [c_void_p]),
     ("sdpab_release_workspace", c_int, []),
 ]
 

@@ -45,7 +45,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             continue
         cmd = [NVCC] + ARCH + CFLAGS + ["-c", src, "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [NVCC] + CFLAGS + ["-x", "c++", "-c", src, "-o", obj]
+            cmd = [NVCC] + ARCH + CFLAGS + ["-x", "c++", "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

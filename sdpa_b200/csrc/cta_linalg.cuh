@@ -264,7 +264,7 @@ __device__ __forceinline__ void gemm(int n, bool tA, const double* A, int lda, b
 // the column of each step is broadcast with shuffles (no shared-memory
 // traffic inside the factorisation).  Pivot rules as cholesky() below; kb is
 // the block's offset, used in the returned failing column (0 = success).
-__device__ __noinline__ int warp_potrf32(int bs, double* sD, bool adjust, int kb)
+static __device__ __noinline__ int warp_potrf32(int bs, double* sD, bool adjust, int kb)
 {
   const int lane = threadIdx.x & 31;
   double a[32];
@@ -515,7 +515,7 @@ __device__ __forceinline__ int sturm_count(int k, const double* d, const double*
 // approached monotonically from the left), each kept inside the bracket,
 // until the step is below one ulp.  Called by one full warp; every lane
 // returns the value.
-__device__ double tridiag_min_eig_warp(int k, const double* d, const double* e)
+static __device__ double tridiag_min_eig_warp(int k, const double* d, const double* e)
 {
   const int lane = threadIdx.x & 31;
   double lo = 1.0e300, hi = -1.0e300;
@@ -569,7 +569,7 @@ __device__ double tridiag_min_eig_warp(int k, const double* d, const double* e)
 // for eigenvalue lam: two steps of inverse iteration on T - (lam - tiny) I
 // with partial pivoting (pivot reciprocals computed once).  Called by one
 // thread; work needs 6*k doubles; k <= 64.
-__device__ double tridiag_evec_last(int k, const double* d, const double* e, double lam, double* work)
+static __device__ double tridiag_evec_last(int k, const double* d, const double* e, double lam, double* work)
 {
   if (k <= 1) return 1.0;
   if (k > 64) k = 64;

@@ -1,0 +1,935 @@
+// class SDPA (include/sdpa_call.h): the reference's public C++ API
+// (sdpa_call.h:91-267, sdpa_call.cpp) on top of the host-driven CUDA solver
+// (solver.h), plus the SDPA file readers and the extern "C" handle API of
+// include/sdpa_b200.h.  Input staging follows the reference: inputElement
+// swaps i > j to the upper triangle (sdpa_call.cpp:330-332) and
+// initializeUpperTriangle sorts the staged elements; .dat-s values are kept
+// as written (F0 is negated to C inside the solver, sdpa_io.cpp:511).
+#include "sdpa_call.h"
+
+#include <ctype.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "ipm_control.h"
+#include "sdpa_b200.h"
+#include "sdpab_internal.h"
+#include "solver.h"
+
+namespace sdpab {
+
+struct SdpaImpl {
+  Params prm = default_params(0);
+  int ptype = 0;
+  double kappa = 12.0;  // KAPPA (sdpa_call.cpp:41)
+  FILE* display = nullptr;
+  FILE* fpout = nullptr;
+  bool isInitPoint = false;
+  int numThreads = 0;
+  char xPrint[32] = "%+8.3e", XPrint[32] = "%+8.3e", YPrint[32] = "%+8.3e", infPrint[32] = "%+10.16e";
+  ProblemData prob;
+  InitPoint init;
+  bool initialized = false;
+  bool solved = false;
+  Solver solver;
+  std::vector<double> xvec;
+  std::vector<std::vector<double>> Xres, Yres;
+  int err = 0;
+  std::string errmsg;
+  void fail(int code, const std::string& msg)
+  {
+    if (!err) {
+      err = code;
+      errmsg = msg;
+    }
+  }
+  int nb() const { return (int)prob.blockStruct.size(); }
+  bool isSdp(int l) const  // 0-based file block
+  {
+    const int s = prob.blockStruct[l];
+    const int t = (l < (int)prob.blockType.size()) ? prob.blockType[l] : 0;
+    return s >= 2 && t == 0;
+  }
+  int blockDim(int l) const { return std::abs(prob.blockStruct[l]); }
+  void ensureInit()
+  {
+    const int nb_ = nb();
+    if ((int)init.X.size() != nb_) {
+      init.X.assign(nb_, {});
+      init.Y.assign(nb_, {});
+    }
+    for (int l = 0; l < nb_; ++l) {
+      const size_t need = isSdp(l) ? (size_t)blockDim(l) * blockDim(l) : (size_t)blockDim(l);
+      if (init.X[l].size() != need) init.X[l].assign(need, 0.0);
+      if (init.Y[l].size() != need) init.Y[l].assign(need, 0.0);
+    }
+    if ((int)init.xvec.size() != prob.m) init.xvec.assign(prob.m, 0.0);
+  }
+};
+
+// ----------------------------------------------------------- text scanning
+// Numbers are read out of any punctuation, like the reference's
+// "%*[^0-9+-]" scans (sdpa_io.cpp:33-73).
+struct Scanner {
+  const char* p;
+  const char* end;
+  bool next(double& v)
+  {
+    while (p < end) {
+      const char c = *p;
+      if (isdigit((unsigned char)c) ||
+          ((c == '+' || c == '-' || c == '.') && p + 1 < end &&
+           (isdigit((unsigned char)p[1]) || (p[1] == '.' && p + 2 < end && isdigit((unsigned char)p[2]))))) {
+        char* e = nullptr;
+        v = strtod(p, &e);
+        if (e == p) { ++p; continue; }
+        p = e;
+        return true;
+      }
+      ++p;
+    }
+    return false;
+  }
+  bool nextInt(int& v)
+  {
+    double d;
+    if (!next(d)) return false;
+    v = (int)d;
+    return true;
+  }
+};
+
+static bool slurp(const char* path, std::string& out)
+{
+  FILE* f = fopen(path, "rb");
+  if (!f) return false;
+  char buf[1 << 16];
+  size_t r;
+  out.clear();
+  while ((r = fread(buf, 1, sizeof(buf), f)) > 0) out.append(buf, r);
+  fclose(f);
+  return true;
+}
+
+// IO::read header + data (sdpa_io.cpp:33-73, :230-606): leading lines that
+// start with '"' or '*' are title/comments; then m, nBlock, block struct, c,
+// and either sparse "k l i j v" lines or dense block matrices F0..Fm.
+int parse_sdpa(const std::string& text, bool sparse, ProblemData& P, std::string& why)
+{
+  size_t pos = 0;
+  while (pos < text.size()) {
+    const size_t eol = text.find('\n', pos);
+    const size_t e = (eol == std::string::npos) ? text.size() : eol;
+    if (e > pos && (text[pos] == '"' || text[pos] == '*')) { pos = e + 1; continue; }
+    if (e == pos) { pos = e + 1; continue; }
+    break;
+  }
+  Scanner S{text.c_str() + pos, text.c_str() + text.size()};
+  int m, nb;
+  if (!S.nextInt(m) || !S.nextInt(nb) || m < 1 || nb < 1) { why = "bad header (m, nBlock)"; return SDPAB_EIO; }
+  P = ProblemData();
+  P.m = m;
+  P.blockStruct.resize(nb);
+  P.blockType.assign(nb, 0);
+  for (int l = 0; l < nb; ++l) {
+    if (!S.nextInt(P.blockStruct[l]) || P.blockStruct[l] == 0) { why = "bad block struct"; return SDPAB_EIO; }
+    if (P.blockStruct[l] < 0) P.blockType[l] = 2;
+  }
+  P.c.resize(m);
+  for (int k = 0; k < m; ++k)
+    if (!S.next(P.c[k])) { why = "short c vector"; return SDPAB_EIO; }
+  if (sparse) {
+    double v[5];
+    while (true) {
+      int got = 0;
+      for (; got < 5; ++got)
+        if (!S.next(v[got])) break;
+      if (got < 5) break;
+      Entry e{(int)v[0], (int)v[1], (int)v[2], (int)v[3], v[4]};
+      if (e.k < 0 || e.k > m || e.l < 1 || e.l > nb) { why = "entry index out of range"; return SDPAB_EIO; }
+      if (P.blockStruct[e.l - 1] < 0 && e.i != e.j) { why = "LP entry with i != j"; return SDPAB_EIO; }
+      P.entries.push_back(e);
+    }
+  } else {
+    for (int k = 0; k <= m; ++k) {
+      for (int l = 0; l < nb; ++l) {
+        const int s = P.blockStruct[l];
+        if (s > 0) {
+          for (int i = 0; i < s; ++i)
+            for (int j = 0; j < s; ++j) {
+              double v;
+              if (!S.next(v)) { why = "short dense data"; return SDPAB_EIO; }
+              if (v != 0.0 && i <= j) P.entries.push_back({k, l + 1, i + 1, j + 1, v});
+            }
+        } else {
+          for (int i = 0; i < -s; ++i) {
+            double v;
+            if (!S.next(v)) { why = "short dense data"; return SDPAB_EIO; }
+            if (v != 0.0) P.entries.push_back({k, l + 1, i + 1, i + 1, v});
+          }
+        }
+      }
+    }
+  }
+  return SDPAB_OK;
+}
+
+// Initial point file (IO::read of the init point, sdpa_io.cpp:75-227): the
+// x vector, then "1 l i j v" (user X) / "2 l i j v" (user Y) lines (sparse)
+// or the dense X and Y block matrices.
+int parse_init(const std::string& text, bool sparse, SdpaImpl& I, std::string& why)
+{
+  I.ensureInit();
+  Scanner S{text.c_str(), text.c_str() + text.size()};
+  for (int k = 0; k < I.prob.m; ++k)
+    if (!S.next(I.init.xvec[k])) { why = "short x vector"; return SDPAB_EIO; }
+  auto put = [&](int target, int l, int i, int j, double v) -> bool {
+    if (l < 1 || l > I.nb()) return false;
+    std::vector<double>& M = (target == 1) ? I.init.X[l - 1] : I.init.Y[l - 1];
+    const int n = I.blockDim(l - 1);
+    if (i < 1 || j < 1 || i > n || j > n) return false;
+    if (I.isSdp(l - 1)) {
+      M[(i - 1) + (size_t)n * (j - 1)] = v;
+      M[(j - 1) + (size_t)n * (i - 1)] = v;
+    } else {
+      if (i != j) return false;
+      M[i - 1] = v;
+    }
+    return true;
+  };
+  if (sparse) {
+    double v[5];
+    while (true) {
+      int got = 0;
+      for (; got < 5; ++got)
+        if (!S.next(v[got])) break;
+      if (got < 5) break;
+      if (v[4] == 0.0) continue;
+      if (!put((int)v[0], (int)v[1], (int)v[2], (int)v[3], v[4])) { why = "bad init entry"; return SDPAB_EIO; }
+    }
+  } else {
+    for (int target = 1; target <= 2; ++target)
+      for (int l = 1; l <= I.nb(); ++l) {
+        const int n = I.blockDim(l - 1);
+        if (I.isSdp(l - 1)) {
+          for (int i = 1; i <= n; ++i)
+            for (int j = 1; j <= n; ++j) {
+              double x;
+              if (!S.next(x)) { why = "short dense init"; return SDPAB_EIO; }
+              if (i <= j) put(target, l, i, j, x);
+            }
+        } else {
+          for (int i = 1; i <= n; ++i) {
+            double x;
+            if (!S.next(x)) { why = "short dense init"; return SDPAB_EIO; }
+            put(target, l, i, i, x);
+          }
+        }
+      }
+  }
+  return SDPAB_OK;
+}
+
+// Smallest eigenvalue of a small symmetric matrix (host, cyclic Jacobi), for
+// the DIMACS errors.
+static double host_min_eig(std::vector<double> A, int n)
+{
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < j; ++i) off += A[i + (size_t)n * j] * A[i + (size_t)n * j];
+    if (off < 1e-30) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = A[p + (size_t)n * q];
+        if (fabs(apq) < 1e-300) continue;
+        const double app = A[p + (size_t)n * p], aqq = A[q + (size_t)n * q];
+        const double th = (aqq - app) / (2 * apq);
+        const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
+        const double c = 1 / sqrt(t * t + 1), s = t * c;
+        for (int k = 0; k < n; ++k) {
+          const double akp = A[k + (size_t)n * p], akq = A[k + (size_t)n * q];
+          A[k + (size_t)n * p] = c * akp - s * akq;
+          A[k + (size_t)n * q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double apk = A[p + (size_t)n * k], aqk = A[q + (size_t)n * k];
+          A[p + (size_t)n * k] = c * apk - s * aqk;
+          A[q + (size_t)n * k] = s * apk + c * aqk;
+        }
+      }
+  }
+  double mn = 1e300;
+  for (int i = 0; i < n; ++i) mn = std::min(mn, A[i + (size_t)n * i]);
+  return mn;
+}
+
+}  // namespace sdpab
+
+using sdpab::SdpaImpl;
+
+SDPA::SDPA() : impl_(new SdpaImpl()) {}
+SDPA::~SDPA() { delete impl_; }
+
+void SDPA::setParameterType(ParameterType type)
+{
+  impl_->ptype = (int)type;
+  impl_->prm = sdpab::default_params((int)type);
+}
+void SDPA::setParameterMaxIteration(SDPA_INT v) { impl_->prm.maxIteration = v; }
+void SDPA::setParameterEpsilonStar(double v) { impl_->prm.epsilonStar = v; }
+void SDPA::setParameterLambdaStar(double v) { impl_->prm.lambdaStar = v; }
+void SDPA::setParameterOmegaStar(double v) { impl_->prm.omegaStar = v; }
+void SDPA::setParameterLowerBound(double v) { impl_->prm.lowerBound = v; }
+void SDPA::setParameterUpperBound(double v) { impl_->prm.upperBound = v; }
+void SDPA::setParameterBetaStar(double v) { impl_->prm.betaStar = v; }
+void SDPA::setParameterBetaBar(double v) { impl_->prm.betaBar = v; }
+void SDPA::setParameterGammaStar(double v) { impl_->prm.gammaStar = v; }
+void SDPA::setParameterEpsilonDash(double v) { impl_->prm.epsilonDash = v; }
+void SDPA::setParameterPrintXVec(char* s) { snprintf(impl_->xPrint, 32, "%s", s); }
+void SDPA::setParameterPrintXMat(char* s) { snprintf(impl_->XPrint, 32, "%s", s); }
+void SDPA::setParameterPrintYMat(char* s) { snprintf(impl_->YPrint, 32, "%s", s); }
+void SDPA::setParameterPrintInformation(char* s) { snprintf(impl_->infPrint, 32, "%s", s); }
+void SDPA::setDisplay(FILE* f) { impl_->display = f; }
+void SDPA::setResultFile(FILE* f) { impl_->fpout = f; }
+void SDPA::setInitPoint(bool b) { impl_->isInitPoint = b; }
+void SDPA::setNumThreads(SDPA_INT n) { impl_->numThreads = n; }
+
+SDPA::ParameterType SDPA::getParameterType() { return (ParameterType)impl_->ptype; }
+SDPA_INT SDPA::getParameterMaxIteration() { return impl_->prm.maxIteration; }
+double SDPA::getParameterEpsilonStar() { return impl_->prm.epsilonStar; }
+double SDPA::getParameterLambdaStar() { return impl_->prm.lambdaStar; }
+double SDPA::getParameterOmegaStar() { return impl_->prm.omegaStar; }
+double SDPA::getParameterLowerBound() { return impl_->prm.lowerBound; }
+double SDPA::getParameterUpperBound() { return impl_->prm.upperBound; }
+double SDPA::getParameterBetaStar() { return impl_->prm.betaStar; }
+double SDPA::getParameterBetaBar() { return impl_->prm.betaBar; }
+double SDPA::getParameterGammaStar() { return impl_->prm.gammaStar; }
+double SDPA::getParameterEpsilonDash() { return impl_->prm.epsilonDash; }
+char* SDPA::getParameterPrintXVec() { return impl_->xPrint; }
+char* SDPA::getParameterPrintXMat() { return impl_->XPrint; }
+char* SDPA::getParameterPrintYMat() { return impl_->YPrint; }
+char* SDPA::getParameterPrintInformation() { return impl_->infPrint; }
+FILE* SDPA::getDisplay() { return impl_->display; }
+FILE* SDPA::getResultFile() { return impl_->fpout; }
+bool SDPA::getInitPoint() { return impl_->isInitPoint; }
+SDPA_INT SDPA::getNumThreads() { return impl_->numThreads; }
+
+void SDPA::inputConstraintNumber(SDPA_INT m)
+{
+  impl_->prob.m = m;
+  impl_->prob.c.assign(m, 0.0);
+}
+void SDPA::inputBlockNumber(SDPA_INT nBlock)
+{
+  impl_->prob.blockStruct.assign(nBlock, 0);
+  impl_->prob.blockType.assign(nBlock, 0);
+}
+void SDPA::inputBlockSize(SDPA_INT l, SDPA_INT size)
+{
+  if (l < 1 || l > impl_->nb()) return impl_->fail(SDPAB_EINVAL, "inputBlockSize: l out of range");
+  impl_->prob.blockStruct[l - 1] = size;
+  if (size < 0) impl_->prob.blockType[l - 1] = 2;
+}
+void SDPA::inputBlockType(SDPA_INT l, ConeType t)
+{
+  if (l < 1 || l > impl_->nb()) return impl_->fail(SDPAB_EINVAL, "inputBlockType: l out of range");
+  impl_->prob.blockType[l - 1] = (int)t;
+}
+void SDPA::inputCVec(SDPA_INT k, double v)
+{
+  if (k < 1 || k > impl_->prob.m) return impl_->fail(SDPAB_EINVAL, "inputCVec: k out of range");
+  impl_->prob.c[k - 1] = v;
+}
+void SDPA::inputElement(SDPA_INT k, SDPA_INT l, SDPA_INT i, SDPA_INT j, double v, bool inputCheck)
+{
+  SdpaImpl& I = *impl_;
+  if (inputCheck || true) {  // range errors are always reported (the reference may crash instead)
+    if (k < 0 || k > I.prob.m) return I.fail(SDPAB_EINVAL, "inputElement: k out of range");
+    if (l < 1 || l > I.nb()) return I.fail(SDPAB_EINVAL, "inputElement: l out of range");
+    const int dim = I.blockDim(l - 1);
+    if (i < 1 || j < 1 || i > dim || j > dim) return I.fail(SDPAB_EINVAL, "inputElement: i/j out of range");
+    if (!I.isSdp(l - 1) && i != j) return I.fail(SDPAB_EINVAL, "inputElement: i != j in an LP block");
+  }
+  if (i > j) std::swap(i, j);
+  I.prob.entries.push_back({k, l, i, j, v});
+}
+void SDPA::inputInitXVec(SDPA_INT k, double v)
+{
+  impl_->ensureInit();
+  if (k < 1 || k > impl_->prob.m) return impl_->fail(SDPAB_EINVAL, "inputInitXVec: k out of range");
+  impl_->init.xvec[k - 1] = v;
+}
+static void set_init(SdpaImpl& I, bool isX, int l, int i, int j, double v)
+{
+  I.ensureInit();
+  if (l < 1 || l > I.nb()) return I.fail(SDPAB_EINVAL, "inputInit: l out of range");
+  const int n = I.blockDim(l - 1);
+  if (i < 1 || j < 1 || i > n || j > n) return I.fail(SDPAB_EINVAL, "inputInit: i/j out of range");
+  std::vector<double>& M = isX ? I.init.X[l - 1] : I.init.Y[l - 1];
+  if (I.isSdp(l - 1)) {
+    M[(i - 1) + (size_t)n * (j - 1)] = v;
+    M[(j - 1) + (size_t)n * (i - 1)] = v;
+  } else {
+    if (i != j) return I.fail(SDPAB_EINVAL, "inputInit: i != j in an LP block");
+    M[i - 1] = v;
+  }
+}
+void SDPA::inputInitXMat(SDPA_INT l, SDPA_INT i, SDPA_INT j, double v) { set_init(*impl_, true, l, i, j, v); }
+void SDPA::inputInitYMat(SDPA_INT l, SDPA_INT i, SDPA_INT j, double v) { set_init(*impl_, false, l, i, j, v); }
+
+void SDPA::initializeUpperTriangleSpace()
+{
+  impl_->prob.entries.clear();
+}
+void SDPA::initializeUpperTriangle(bool inputTwiceCheck)
+{
+  // sortNonZeroElements / checkNonZeroElements (sdpa_call.cpp:446-501)
+  std::vector<sdpab::Entry>& E = impl_->prob.entries;
+  std::stable_sort(E.begin(), E.end(), [](const sdpab::Entry& a, const sdpab::Entry& b) {
+    if (a.k != b.k) return a.k < b.k;
+    if (a.l != b.l) return a.l < b.l;
+    if (a.i != b.i) return a.i < b.i;
+    return a.j < b.j;
+  });
+  if (inputTwiceCheck) {
+    for (size_t q = 1; q < E.size(); ++q)
+      if (E[q].k == E[q - 1].k && E[q].l == E[q - 1].l && E[q].i == E[q - 1].i && E[q].j == E[q - 1].j)
+        return impl_->fail(SDPAB_EINVAL, "initializeUpperTriangle: element input twice");
+  }
+}
+void SDPA::initializeSolve()
+{
+  SdpaImpl& I = *impl_;
+  if (I.err) return;
+  const int rc = I.solver.setup(I.prob, I.prm, I.kappa);
+  if (rc != SDPAB_OK) return I.fail(rc, sdpab_last_error());
+  I.initialized = true;
+  I.solved = false;
+}
+void SDPA::resetParameters() {}
+void SDPA::solve()
+{
+  SdpaImpl& I = *impl_;
+  if (I.err) return;
+  if (!I.initialized) return I.fail(SDPAB_ESTATE, "solve called before initializeSolve");
+  if (I.isInitPoint) I.ensureInit();
+  const int rc = I.solver.solve(I.isInitPoint ? &I.init : nullptr);
+  if (rc != SDPAB_OK) return I.fail(rc, sdpab_last_error());
+  I.solved = true;
+  I.xvec = I.solver.xvec();
+  I.Xres.assign(I.nb(), {});
+  I.Yres.assign(I.nb(), {});
+  for (int l = 1; l <= I.nb(); ++l) {
+    I.Xres[l - 1] = I.solver.resultX(l);
+    I.Yres[l - 1] = I.solver.resultY(l);
+  }
+  if (I.display) {
+    const sdpab::SolveStats& s = I.solver.stats();
+    char ph[32];
+    getPhaseString(ph);
+    fprintf(I.display, "phase.value  = %s\n   Iteration = %d\n          mu = %+.16e\n", ph, s.iterations, s.mu);
+    fprintf(I.display, "objValPrimal = %+.16e\nobjValDual   = %+.16e\n", s.primal_obj, s.dual_obj);
+    fprintf(I.display, "p.feas.error = %+.16e\nd.feas.error = %+.16e\n", s.primal_error, s.dual_error);
+  }
+  if (I.fpout) {
+    printResultXVec(I.fpout);
+  }
+}
+
+double* SDPA::getResultXVec() { return impl_->solved ? impl_->xvec.data() : nullptr; }
+double* SDPA::getResultXMat(SDPA_INT l)
+{
+  if (!impl_->solved || l < 1 || l > impl_->nb()) return nullptr;
+  return impl_->Xres[l - 1].data();
+}
+double* SDPA::getResultYMat(SDPA_INT l)
+{
+  if (!impl_->solved || l < 1 || l > impl_->nb()) return nullptr;
+  return impl_->Yres[l - 1].data();
+}
+double SDPA::getPrimalObj() { return impl_->solver.stats().primal_obj; }
+double SDPA::getDualObj() { return impl_->solver.stats().dual_obj; }
+double SDPA::getPrimalError() { return impl_->solver.stats().primal_error; }
+double SDPA::getDualError() { return impl_->solver.stats().dual_error; }
+double SDPA::getDigits()
+{
+  const sdpab::SolveStats& s = impl_->solver.stats();
+  const double mean = (fabs(s.objValPrimal) + fabs(s.objValDual)) / 2.0;
+  return -log10(fabs(getDualityGap() / mean));
+}
+SDPA_INT SDPA::getIteration() { return impl_->solver.stats().iterations; }
+double SDPA::getMu() { return impl_->solver.stats().mu; }
+double SDPA::getDualityGap()
+{
+  const sdpab::SolveStats& s = impl_->solver.stats();
+  return fabs(s.objValPrimal - s.objValDual);
+}
+SDPA::PhaseType SDPA::getPhaseValue() { return (PhaseType)impl_->solver.stats().phase; }
+void SDPA::getPhaseString(char* str)
+{
+  static const char* names[] = {"noINFO    ", "pFEAS     ", "dFEAS     ", "pdFEAS    ", "pdINF     ",
+                                "pFEAS_dINF", "pINF_dFEAS", "pdOPT     ", "pUNBD     ", "dUNBD     "};
+  // SDPA::getPhaseString prints the internal (reversed) phase name (sdpa_call.cpp:788-803)
+  int v = impl_->solver.stats().internal_phase;
+  switch (v) {
+    case 1: v = 2; break;
+    case 2: v = 1; break;
+    case 5: v = 6; break;
+    case 6: v = 5; break;
+    case 8: v = 9; break;
+    case 9: v = 8; break;
+  }
+  strcpy(str, names[(v >= 0 && v < 10) ? v : 0]);
+}
+double SDPA::getSolveTime() { return impl_->solver.stats().solve_seconds; }
+SDPA_INT SDPA::getConstraintNumber() { return impl_->prob.m; }
+SDPA_INT SDPA::getBlockNumber() { return impl_->nb(); }
+SDPA_INT SDPA::getBlockSize(SDPA_INT l)
+{
+  if (l < 1 || l > impl_->nb()) return 0;
+  return impl_->blockDim(l - 1);
+}
+SDPA::ConeType SDPA::getBlockType(SDPA_INT l)
+{
+  if (l < 1 || l > impl_->nb()) return SDP;
+  return impl_->isSdp(l - 1) ? SDP : LP;
+}
+
+// IO::computeDimacs (sdpa_io.cpp:775-813), on the host from the results.
+void SDPA::getDimacsError(double* d)
+{
+  SdpaImpl& I = *impl_;
+  for (int q = 0; q <= 6; ++q) d[q] = 0.0;
+  if (!I.solved) return;
+  const int m = I.prob.m, nb = I.nb();
+  // internal X = Y result, Z = X result, y = -x
+  std::vector<double> rp(I.prob.c);
+  std::vector<std::vector<double>> Dm(nb);
+  double b1 = 0.0, c1 = 0.0;
+  for (double v : I.prob.c) b1 = std::max(b1, fabs(v));
+  for (int l = 0; l < nb; ++l) {
+    Dm[l].assign(I.Xres[l].size(), 0.0);
+    for (size_t t = 0; t < Dm[l].size(); ++t) Dm[l][t] = -I.Xres[l][t];
+  }
+  for (const sdpab::Entry& e : I.prob.entries) {
+    const int l = e.l - 1;
+    const int n = I.blockDim(l);
+    const bool sdp = I.isSdp(l);
+    auto Y = [&](int i, int j) { return sdp ? I.Yres[l][(i - 1) + (size_t)n * (j - 1)] : I.Yres[l][i - 1]; };
+    auto addD = [&](int i, int j, double v) {
+      if (sdp) {
+        Dm[l][(i - 1) + (size_t)n * (j - 1)] += v;
+        if (i != j) Dm[l][(j - 1) + (size_t)n * (i - 1)] += v;
+      } else {
+        Dm[l][i - 1] += v;
+      }
+    };
+    if (e.k == 0) {
+      c1 = std::max(c1, fabs(e.v));
+      addD(e.i, e.j, -e.v);  // C = -F0
+    } else {
+      const double a = (e.i == e.j || !sdp) ? e.v * Y(e.i, e.j) : e.v * (Y(e.i, e.j) + Y(e.j, e.i));
+      rp[e.k - 1] -= a;
+      addD(e.i, e.j, e.v * I.xvec[e.k - 1]);  // -A_k y_k with y = -x
+    }
+  }
+  double pn = 0.0, dn = 0.0, xz = 0.0;
+  for (double v : rp) pn += v * v;
+  double xmin = 1e300, zmin = 1e300;
+  for (int l = 0; l < nb; ++l) {
+    for (double v : Dm[l]) dn += v * v;
+    for (size_t t = 0; t < I.Xres[l].size(); ++t) xz += I.Xres[l][t] * I.Yres[l][t];
+    if (I.isSdp(l)) {
+      xmin = std::min(xmin, sdpab::host_min_eig(I.Yres[l], I.blockDim(l)));
+      zmin = std::min(zmin, sdpab::host_min_eig(I.Xres[l], I.blockDim(l)));
+    } else {
+      for (double v : I.Yres[l]) xmin = std::min(xmin, v);
+      for (double v : I.Xres[l]) zmin = std::min(zmin, v);
+    }
+  }
+  (void)m;
+  const sdpab::SolveStats& s = I.solver.stats();
+  const double ctx = s.objValPrimal, bty = s.objValDual;
+  d[1] = sqrt(pn) / (1 + b1);
+  d[2] = std::max(0.0, -xmin / (1 + b1));
+  d[3] = sqrt(dn) / (1 + c1);
+  d[4] = std::max(0.0, -zmin / (1 + c1));
+  d[5] = (ctx - bty) / (1 + fabs(ctx) + fabs(bty));
+  d[6] = xz / (1 + fabs(ctx) + fabs(bty));
+}
+void SDPA::printDimacsError(double* d, char* fmt, FILE* fp)
+{
+  if (!fp) return;
+  static const char* what[] = {"", "[||Ax-b|| / (1+||b||_1)]", "[max(0, -lambda(x)/(1+||b||_1))]",
+                               "[||A^Ty + z - c || / (1+||c||_1)]", "[max(0, -lambda(z)/(1+||c||_1))]",
+                               "[(<c,x> - <b,y>) / (1 + |<c,x>| + |<b,y>|)]", "[<x,z> / (1 + |<c,x>| + |<b,y>|)]"};
+  fprintf(fp, "\n* DIMACS_ERRORS * \n");
+  for (int q = 1; q <= 6; ++q) {
+    fprintf(fp, "err%d = ", q);
+    fprintf(fp, fmt, d[q]);
+    fprintf(fp, "  %s\n", what[q]);
+  }
+  fprintf(fp, "\n");
+}
+void SDPA::printResultXVec(FILE* fp)
+{
+  if (!fp || !impl_->solved) return;
+  fprintf(fp, "{");
+  for (size_t k = 0; k < impl_->xvec.size(); ++k) {
+    fprintf(fp, impl_->xPrint, impl_->xvec[k]);
+    if (k + 1 < impl_->xvec.size()) fprintf(fp, ",");
+  }
+  fprintf(fp, "}\n");
+}
+static void print_blocks(SdpaImpl& I, std::vector<std::vector<double>>& M, const char* fmt, FILE* fp)
+{
+  fprintf(fp, "{\n");
+  for (int l = 0; l < I.nb(); ++l) {
+    const int n = I.blockDim(l);
+    if (I.isSdp(l)) {
+      fprintf(fp, "{\n");
+      for (int i = 0; i < n; ++i) {
+        fprintf(fp, "{");
+        for (int j = 0; j < n; ++j) {
+          fprintf(fp, fmt, M[l][i + (size_t)n * j]);
+          if (j + 1 < n) fprintf(fp, ",");
+        }
+        fprintf(fp, "}%s\n", i + 1 < n ? "," : "");
+      }
+      fprintf(fp, "}\n");
+    } else {
+      fprintf(fp, "{");
+      for (int i = 0; i < n; ++i) {
+        fprintf(fp, fmt, M[l][i]);
+        if (i + 1 < n) fprintf(fp, ",");
+      }
+      fprintf(fp, "}\n");
+    }
+  }
+  fprintf(fp, "}\n");
+}
+void SDPA::printResultXMat(FILE* fp)
+{
+  if (fp && impl_->solved) print_blocks(*impl_, impl_->Xres, impl_->XPrint, fp);
+}
+void SDPA::printResultYMat(FILE* fp)
+{
+  if (fp && impl_->solved) print_blocks(*impl_, impl_->Yres, impl_->YPrint, fp);
+}
+void SDPA::printComputationTime(FILE* fp)
+{
+  if (fp) fprintf(fp, "    solve time = %.6f\n", getSolveTime());
+}
+void SDPA::printParameters(FILE* fp)
+{
+  if (!fp) return;
+  const sdpab::Params& p = impl_->prm;
+  fprintf(fp, "** Parameters **\nmaxIteration = %d\nepsilonStar  = %+8.3e\nlambdaStar   = %+8.3e\n",
+          p.maxIteration, p.epsilonStar, p.lambdaStar);
+  fprintf(fp, "omegaStar    = %+8.3e\nlowerBound   = %+8.3e\nupperBound   = %+8.3e\n", p.omegaStar,
+          p.lowerBound, p.upperBound);
+  fprintf(fp, "betaStar     = %+8.3e\nbetaBar      = %+8.3e\ngammaStar    = %+8.3e\nepsilonDash  = %+8.3e\n",
+          p.betaStar, p.betaBar, p.gammaStar, p.epsilonDash);
+}
+void SDPA::printSDPAVersion(FILE* fp)
+{
+  if (fp) fprintf(fp, "%s\n", sdpab_version());
+}
+
+void SDPA::readInput(char* filename, FILE* fpout, SparseType type)
+{
+  SdpaImpl& I = *impl_;
+  std::string txt, why;
+  if (!filename || !sdpab::slurp(filename, txt)) return I.fail(SDPAB_EIO, "readInput: cannot open data file");
+  bool sparse;
+  if (type == AUTO) {
+    const size_t len = strlen(filename);
+    sparse = len >= 2 && filename[len - 1] == 's' && filename[len - 2] == '-';
+  } else {
+    sparse = (type == SPARSE);
+  }
+  if (fpout) fprintf(fpout, "data   is %s  : %s\n", filename, sparse ? "sparse" : "dense");
+  const int rc = sdpab::parse_sdpa(txt, sparse, I.prob, why);
+  if (rc != SDPAB_OK) return I.fail(rc, "readInput: " + why);
+}
+void SDPA::readInit(char* filename, FILE* fpout, SparseType type)
+{
+  SdpaImpl& I = *impl_;
+  std::string txt, why;
+  if (!filename || !sdpab::slurp(filename, txt)) return I.fail(SDPAB_EIO, "readInit: cannot open init file");
+  bool sparse;
+  if (type == AUTO) {
+    const size_t len = strlen(filename);
+    sparse = len >= 2 && filename[len - 1] == 's' && filename[len - 2] == '-';
+  } else {
+    sparse = (type == SPARSE);
+  }
+  if (fpout) fprintf(fpout, "initial is %s  : %s\n", filename, sparse ? "sparse" : "dense");
+  const int rc = sdpab::parse_init(txt, sparse, I, why);
+  if (rc != SDPAB_OK) return I.fail(rc, "readInit: " + why);
+}
+void SDPA::readParameter(char* filename, FILE* fpout)
+{
+  sdpab_params p;
+  if (sdpab_read_params(filename, &p) != SDPAB_OK) return impl_->fail(SDPAB_EIO, "readParameter failed");
+  memcpy(&impl_->prm, &p, sizeof(p));
+  if (fpout) fprintf(fpout, "param  is %s \n", filename);
+}
+// SDPA::writeInputSparse (sdpa_call.cpp:1137-1197)
+void SDPA::writeInputSparse(char* filename, char* fmt)
+{
+  SdpaImpl& I = *impl_;
+  FILE* f = fopen(filename, "w");
+  if (!f) return I.fail(SDPAB_EIO, "writeInputSparse: cannot open file");
+  fprintf(f, "%d\n%d\n", I.prob.m, I.nb());
+  for (int l = 0; l < I.nb(); ++l) fprintf(f, "%d ", I.prob.blockStruct[l]);
+  fprintf(f, "\n");
+  for (int k = 0; k < I.prob.m; ++k) {
+    fprintf(f, fmt, I.prob.c[k]);
+    fprintf(f, " ");
+  }
+  fprintf(f, "\n");
+  std::vector<sdpab::Entry> E = I.prob.entries;
+  std::stable_sort(E.begin(), E.end(), [](const sdpab::Entry& a, const sdpab::Entry& b) {
+    return a.k != b.k ? a.k < b.k : a.l != b.l ? a.l < b.l : a.i != b.i ? a.i < b.i : a.j < b.j;
+  });
+  for (const sdpab::Entry& e : E) {
+    fprintf(f, "%d %d %d %d ", e.k, e.l, e.i, e.j);
+    fprintf(f, fmt, e.v);
+    fprintf(f, "\n");
+  }
+  fclose(f);
+}
+// SDPA::writeInitSparse (sdpa_call.cpp:1199-1220): x, then user X (1) and Y (2)
+void SDPA::writeInitSparse(char* filename, char* fmt)
+{
+  SdpaImpl& I = *impl_;
+  if (!I.solved) return I.fail(SDPAB_ESTATE, "writeInitSparse: no solution");
+  FILE* f = fopen(filename, "w");
+  if (!f) return I.fail(SDPAB_EIO, "writeInitSparse: cannot open file");
+  for (int k = 0; k < I.prob.m; ++k) {
+    fprintf(f, fmt, I.xvec[k]);
+    fprintf(f, " ");
+  }
+  fprintf(f, "\n");
+  for (int target = 1; target <= 2; ++target)
+    for (int l = 0; l < I.nb(); ++l) {
+      const std::vector<double>& M = (target == 1) ? I.Xres[l] : I.Yres[l];
+      const int n = I.blockDim(l);
+      if (I.isSdp(l)) {
+        for (int i = 0; i < n; ++i)
+          for (int j = i; j < n; ++j) {
+            const double v = M[i + (size_t)n * j];
+            if (v == 0.0) continue;
+            fprintf(f, "%d %d %d %d ", target, l + 1, i + 1, j + 1);
+            fprintf(f, fmt, v);
+            fprintf(f, "\n");
+          }
+      } else {
+        for (int i = 0; i < n; ++i) {
+          if (M[i] == 0.0) continue;
+          fprintf(f, "%d %d %d %d ", target, l + 1, i + 1, i + 1);
+          fprintf(f, fmt, M[i]);
+          fprintf(f, "\n");
+        }
+      }
+    }
+  fclose(f);
+}
+void SDPA::terminate()
+{
+  impl_->solver.release();
+  impl_->initialized = false;
+  impl_->solved = false;
+  impl_->xvec.clear();
+  impl_->Xres.clear();
+  impl_->Yres.clear();
+}
+// SDPA::copyCurrentToInit (sdpa_call.cpp:1238-1245): the last point becomes
+// the initial point of the next solve.
+void SDPA::copyCurrentToInit()
+{
+  SdpaImpl& I = *impl_;
+  if (!I.solved) return;
+  I.ensureInit();
+  I.init.xvec = I.xvec;
+  for (int l = 0; l < I.nb(); ++l) {
+    I.init.X[l] = I.Xres[l];
+    I.init.Y[l] = I.Yres[l];
+  }
+}
+void SDPA::setKappa(double k) { impl_->kappa = k; }
+int SDPA::getErrorCode() { return impl_->err; }
+const char* SDPA::getErrorMessage() { return impl_->errmsg.c_str(); }
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+SDPAB_API sdpab_sdpa* sdpab_sdpa_new(void) { return (sdpab_sdpa*)new SDPA(); }
+SDPAB_API void sdpab_sdpa_free(sdpab_sdpa* h) { delete (SDPA*)h; }
+
+static int status_of(SDPA* p)
+{
+  const int e = p->getErrorCode();
+  if (e) sdpab::set_error(e, p->getErrorMessage());
+  return e;
+}
+
+SDPAB_API int sdpab_sdpa_set_params(sdpab_sdpa* h, const sdpab_params* prm)
+{
+  if (!h || !prm) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  p->setParameterMaxIteration(prm->maxIteration);
+  p->setParameterEpsilonStar(prm->epsilonStar);
+  p->setParameterLambdaStar(prm->lambdaStar);
+  p->setParameterOmegaStar(prm->omegaStar);
+  p->setParameterLowerBound(prm->lowerBound);
+  p->setParameterUpperBound(prm->upperBound);
+  p->setParameterBetaStar(prm->betaStar);
+  p->setParameterBetaBar(prm->betaBar);
+  p->setParameterGammaStar(prm->gammaStar);
+  p->setParameterEpsilonDash(prm->epsilonDash);
+  return SDPAB_OK;
+}
+SDPAB_API int sdpab_sdpa_read_input(sdpab_sdpa* h, const char* path, int sparse_type)
+{
+  if (!h || !path) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  p->readInput((char*)path, NULL, (SDPA::SparseType)sparse_type);
+  return status_of(p);
+}
+SDPAB_API int sdpab_sdpa_read_init(sdpab_sdpa* h, const char* path, int sparse_type)
+{
+  if (!h || !path) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  p->setInitPoint(true);
+  p->readInit((char*)path, NULL, (SDPA::SparseType)sparse_type);
+  return status_of(p);
+}
+SDPAB_API int sdpab_sdpa_read_param(sdpab_sdpa* h, const char* path)
+{
+  if (!h || !path) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  p->readParameter((char*)path, NULL);
+  return status_of(p);
+}
+SDPAB_API int sdpab_sdpa_input_problem(sdpab_sdpa* h, int m, int nblock, const int* block_struct,
+                                       const double* c, long long nnz, const int* k, const int* l,
+                                       const int* i, const int* j, const double* v)
+{
+  if (!h || !block_struct || !c) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  p->inputConstraintNumber(m);
+  p->inputBlockNumber(nblock);
+  for (int b = 0; b < nblock; ++b) {
+    p->inputBlockSize(b + 1, block_struct[b]);
+    p->inputBlockType(b + 1, block_struct[b] < 0 ? SDPA::LP : SDPA::SDP);
+  }
+  p->initializeUpperTriangleSpace();
+  for (int q = 0; q < m; ++q) p->inputCVec(q + 1, c[q]);
+  for (long long e = 0; e < nnz; ++e) p->inputElement(k[e], l[e], i[e], j[e], v[e]);
+  p->initializeUpperTriangle(false);
+  return status_of(p);
+}
+SDPAB_API int sdpab_sdpa_set_init(sdpab_sdpa* h, const double* xvec, const double* const* X,
+                                  const double* const* Y)
+{
+  if (!h || !xvec || !X || !Y) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  p->setInitPoint(true);
+  const int m = p->getConstraintNumber(), nb = p->getBlockNumber();
+  for (int k = 1; k <= m; ++k) p->inputInitXVec(k, xvec[k - 1]);
+  for (int l = 1; l <= nb; ++l) {
+    const int n = p->getBlockSize(l);
+    const bool sdp = p->getBlockType(l) == SDPA::SDP;
+    for (int i = 1; i <= n; ++i)
+      for (int j = sdp ? i : i; j <= (sdp ? n : i); ++j) {
+        const size_t off = sdp ? (size_t)(i - 1) + (size_t)n * (j - 1) : (size_t)(i - 1);
+        p->inputInitXMat(l, i, j, X[l - 1][off]);
+        p->inputInitYMat(l, i, j, Y[l - 1][off]);
+      }
+  }
+  return status_of(p);
+}
+SDPAB_API int sdpab_sdpa_solve(sdpab_sdpa* h)
+{
+  if (!h) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  p->initializeSolve();
+  if (status_of(p)) return p->getErrorCode();
+  p->solve();
+  return status_of(p);
+}
+SDPAB_API int sdpab_sdpa_info(sdpab_sdpa* h, sdpab_sdpa_info_t* out)
+{
+  if (!h || !out) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  out->primal_obj = p->getPrimalObj();
+  out->dual_obj = p->getDualObj();
+  out->primal_error = p->getPrimalError();
+  out->dual_error = p->getDualError();
+  out->mu = p->getMu();
+  out->duality_gap = p->getDualityGap();
+  out->solve_seconds = p->getSolveTime();
+  out->iterations = p->getIteration();
+  out->phase = (int)p->getPhaseValue();
+  out->m = p->getConstraintNumber();
+  out->nblock = p->getBlockNumber();
+  return SDPAB_OK;
+}
+SDPAB_API int sdpab_sdpa_get_xvec(sdpab_sdpa* h, double* out)
+{
+  SDPA* p = (SDPA*)h;
+  const double* x = p ? p->getResultXVec() : nullptr;
+  if (!x || !out) return sdpab::set_error(SDPAB_ESTATE, "no result");
+  memcpy(out, x, sizeof(double) * p->getConstraintNumber());
+  return SDPAB_OK;
+}
+SDPAB_API int sdpab_sdpa_get_block(sdpab_sdpa* h, int l, int which, double* out)
+{
+  SDPA* p = (SDPA*)h;
+  if (!p || !out || l < 1 || l > p->getBlockNumber()) return sdpab::set_error(SDPAB_EINVAL, "bad block");
+  const double* M = (which == 0) ? p->getResultXMat(l) : p->getResultYMat(l);
+  if (!M) return sdpab::set_error(SDPAB_ESTATE, "no result");
+  const int n = p->getBlockSize(l);
+  const size_t len = (p->getBlockType(l) == SDPA::SDP) ? (size_t)n * n : (size_t)n;
+  memcpy(out, M, len * sizeof(double));
+  return SDPAB_OK;
+}
+SDPAB_API int sdpab_sdpa_block_size(sdpab_sdpa* h, int l, int* size, int* is_sdp)
+{
+  SDPA* p = (SDPA*)h;
+  if (!p || l < 1 || l > p->getBlockNumber()) return sdpab::set_error(SDPAB_EINVAL, "bad block");
+  *size = p->getBlockSize(l);
+  *is_sdp = p->getBlockType(l) == SDPA::SDP;
+  return SDPAB_OK;
+}
+SDPAB_API int sdpab_sdpa_dimacs(sdpab_sdpa* h, double* err7)
+{
+  if (!h || !err7) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  ((SDPA*)h)->getDimacsError(err7);
+  return SDPAB_OK;
+}
+SDPAB_API int sdpab_sdpa_write_init(sdpab_sdpa* h, const char* path)
+{
+  if (!h || !path) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  SDPA* p = (SDPA*)h;
+  p->writeInitSparse((char*)path, (char*)"%+.17e");
+  return status_of(p);
+}
+SDPAB_API int sdpab_sdpa_copy_current_to_init(sdpab_sdpa* h)
+{
+  if (!h) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  ((SDPA*)h)->copyCurrentToInit();
+  ((SDPA*)h)->setInitPoint(true);
+  return SDPAB_OK;
+}
+
+}  // extern "C"

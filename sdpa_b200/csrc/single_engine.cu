@@ -1,0 +1,1187 @@
+// Device kernels and host orchestration of the host-driven solver
+// (solver.h).  The operation sequence is the reference's (SDPA::solve,
+// sdpa_solve.cpp:59-233; Newton::Mehrotra, sdpa_newton.cpp:2755-2809); the
+// scalar rules are ipm_control.h.  Dense n x n blocks and the m x m Schur
+// matrix stay resident in HBM; block-level pieces (diagonal-block Cholesky,
+// Lanczos, Schur solve) run as single thread-block kernels built from
+// cta_linalg.cuh / eig.cuh, everything else as grid kernels.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <numeric>
+#include <vector>
+
+#include "cta_linalg.cuh"
+#include "eig.cuh"
+#include "ipm_control.h"
+#include "sdpa_b200.h"
+#include "sdpab_internal.h"
+#include "solver.h"
+
+namespace sdpab {
+
+enum Formula { F1 = 1, F2 = 2, F3 = 3 };
+
+// ------------------------------------------------------------------ kernels
+
+__global__ void k_set_identity(int n, double* A, double v)
+{
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < (long long)n * n) A[t] = ((t % n) == (t / n)) ? v : 0.0;
+}
+
+// out = a * x + b * y (element-wise, len entries)
+__global__ void k_axpby(long long len, double* out, double a, const double* x, double b, const double* y)
+{
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < len) out[t] = a * x[t] + (y ? b * y[t] : 0.0);
+}
+
+// out = a * x + b * y - z  (rMat of the corrector: beta mu Z^-1 - X - dX dZ Z^-1)
+__global__ void k_axpby_sub(long long len, double* out, double a, const double* x, double b,
+                            const double* y, const double* z)
+{
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < len) out[t] = (a * x[t] + b * y[t]) - z[t];
+}
+
+// dX = sym(R - W): lower = (lower + upper) / 2 mirrored (Lal::getSymmetrize,
+// sdpa_linear.cpp:591-618, applied to R - X dZ Z^-1)
+__global__ void k_sym_diff(int n, double* dX, const double* R, const double* W)
+{
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int i = t % n, j = t / n;
+  if (i < j) return;
+  const double lo = R[i + (size_t)n * j] - W[i + (size_t)n * j];
+  const double up = R[j + (size_t)n * i] - W[j + (size_t)n * i];
+  const double s = 0.5 * (lo + up);
+  dX[i + (size_t)n * j] = s;
+  dX[j + (size_t)n * i] = s;
+}
+
+// rows x cols copy between leading dimensions
+__global__ void k_copy2d(int rows, int cols, const double* src, int lds, double* dst, int ldd)
+{
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)rows * cols) return;
+  const int i = t % rows, j = t / rows;
+  dst[i + (size_t)ldd * j] = src[i + (size_t)lds * j];
+}
+
+// Per-constraint inner products out[cons[q]] += sign * (A_q . W) over the
+// entries a block holds (Lal::getInnerProduct(Sparse, Dense),
+// sdpa_linear.cpp:318-460).  One warp per constraint.
+__global__ void k_sp_dot(int nc, const int* cons, const long long* ptr, const int* row, const int* col,
+                         const double* val, const double* W, int n, double sign, double* out)
+{
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nc) return;
+  double s = 0.0;
+  for (long long e = ptr[warp] + lane; e < ptr[warp + 1]; e += 32) {
+    const int r = row[e], c = col[e];
+    const double v = val[e];
+    s += (r == c) ? v * W[r + (size_t)n * r] : v * (W[r + (size_t)n * c] + W[c + (size_t)n * r]);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) atomicAdd(&out[cons[warp]], sign * s);
+}
+
+// W += scale * sum_q coef[cons[q]] A_q (InputData::multi_plusToA,
+// sdpa_dataset.cpp:427-433).  One warp per constraint, atomics for shared
+// positions.
+__global__ void k_sp_scatter(int nc, const int* cons, const long long* ptr, const int* row,
+                             const int* col, const double* val, const double* coef, double scale,
+                             double* W, int n)
+{
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nc) return;
+  const double s = scale * (coef ? coef[cons[warp]] : 1.0);
+  for (long long e = ptr[warp] + lane; e < ptr[warp + 1]; e += 32) {
+    const int r = row[e], c = col[e];
+    const double v = s * val[e];
+    atomicAdd(&W[r + (size_t)n * c], v);
+    if (r != c) atomicAdd(&W[c + (size_t)n * r], v);
+  }
+}
+
+// Schur complement by formula F3 for every pair whose dominant constraint
+// uses F3 (compute_bMat_dense_SDP3 + calF3_thread_2, sdpa_newton.cpp:2019-2125,
+// :1319-1403).  One thread per ordered (i, j) pair of the block's constraints.
+__global__ void k_f3(int nc, const int* cons, const long long* ptr, const int* row, const int* col,
+                     const double* val, const int* nnz, const int* formula, const double* X,
+                     const double* Zi, int n, double* B, int m)
+{
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nc * nc) return;
+  const int il = t % nc, jl = t / nc;
+  if (formula[jl] != F3) return;
+  const int gi = cons[il], gj = cons[jl];
+  const int inz = nnz[il], jnz = nnz[jl];
+  if (jnz < inz || (inz == jnz && gi < gj)) return;
+  double ret = 0.0;
+  for (long long e1 = ptr[jl]; e1 < ptr[jl + 1]; ++e1) {
+    const int al = row[e1], be = col[e1];
+    const double* Xa = X + (size_t)n * al;
+    const double* Xb = X + (size_t)n * be;
+    const double* Za = Zi + (size_t)n * al;
+    const double* Zb = Zi + (size_t)n * be;
+    double sum = 0.0;
+    for (long long e2 = ptr[il]; e2 < ptr[il + 1]; ++e2) {
+      const int ga = row[e2], de = col[e2];
+      double plu;
+      if (al != be) {
+        plu = (ga != de) ? Zb[de] * Xa[ga] + Zb[ga] * Xa[de] + Za[de] * Xb[ga] + Za[ga] * Xb[de]
+                         : Zb[de] * Xa[ga] + Za[de] * Xb[ga];
+      } else {
+        plu = (ga != de) ? Zb[de] * Xa[ga] + Zb[ga] * Xa[de] : Zb[de] * Xa[ga];
+      }
+      sum += val[e2] * plu;
+    }
+    ret += val[e1] * sum;
+  }
+  atomicAdd(&B[gi + (size_t)m * gj], ret);
+  if (gi != gj) atomicAdd(&B[gj + (size_t)m * gi], ret);
+}
+
+// F1 step 1 (Lal::let(work1,'=',xMat,'*',Aj), sdpa_newton.cpp:1859-1863):
+// T_q = X A_j for a chunk of F1/F2 constraints, A_j given column-wise with
+// both triangles (csc).  One block per (q, column c).
+__global__ void k_f1_left(int n, int q0, const int* f1list, const long long* cptr_base,
+                          const long long* csc_ptr, const int* csc_row, const double* csc_val,
+                          const double* X, double* T)
+{
+  const int q = blockIdx.y, c = blockIdx.x;
+  const int f = f1list[q0 + q];
+  const long long* cp = cptr_base + (size_t)f * (n + 1);
+  const long long beg = csc_ptr[f] + cp[c], end = csc_ptr[f] + cp[c + 1];
+  double* Tc = T + (size_t)q * n * n + (size_t)n * c;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double s = 0.0;
+    for (long long e = beg; e < end; ++e) s += X[i + (size_t)n * csc_row[e]] * csc_val[e];
+    Tc[i] = s;
+  }
+}
+
+// F1 step 3 (calF1, sdpa_newton.cpp:885-889, driver :1868-1907):
+// B_ij += A_i . G_j for every i dominated by j.  Blocks (q, part): q is the
+// chunk entry, the constraints i are dealt to the warps of all parts.
+__global__ void k_f1_dot(int nc, int q0, const int* f1list, const int* cons, const long long* ptr,
+                         const int* row, const int* col, const double* val, const int* nnz,
+                         const double* G, int n, double* B, int m)
+{
+  const int q = blockIdx.x;
+  const int jl = f1list[q0 + q];
+  const int gj = cons[jl], jnz = nnz[jl];
+  const double* Gq = G + (size_t)q * n * n;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int wid = blockIdx.y * nw + (threadIdx.x >> 5), stride = gridDim.y * nw;
+  for (int il = wid; il < nc; il += stride) {
+    const int gi = cons[il], inz = nnz[il];
+    if (jnz < inz || (inz == jnz && gi < gj)) continue;
+    double s = 0.0;
+    for (long long e = ptr[il] + lane; e < ptr[il + 1]; e += 32) {
+      const int r = row[e], c = col[e];
+      const double v = val[e];
+      s += (r == c) ? v * Gq[r + (size_t)n * r] : v * (Gq[r + (size_t)n * c] + Gq[c + (size_t)n * r]);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      atomicAdd(&B[gi + (size_t)m * gj], s);
+      if (gi != gj) atomicAdd(&B[gj + (size_t)m * gi], s);
+    }
+  }
+}
+
+// LP part of the Schur complement (compute_bMat_dense_LP,
+// sdpa_newton.cpp:2562-2602): B_ij += x_t z_t^-1 a_it a_jt for each LP
+// coordinate t and each pair of constraints touching it.  One block per t.
+__global__ void k_lp_bmat(const long long* tptr, const int* tk, const double* tv, const double* x,
+                          const double* zi, double* B, int m)
+{
+  const int t = blockIdx.x;
+  const long long beg = tptr[t], cnt = tptr[t + 1] - beg;
+  const double xz = x[t] * zi[t];
+  for (long long p = threadIdx.x; p < cnt * cnt; p += blockDim.x) {
+    const long long a1 = p % cnt, a2 = p / cnt;
+    if (a2 < a1) continue;  // k2 >= k1 in list order
+    const int j = tk[beg + a1], i = tk[beg + a2];
+    const double v = xz * tv[beg + a2] * tv[beg + a1];
+    atomicAdd(&B[i + (size_t)m * j], v);
+    if (i != j) atomicAdd(&B[j + (size_t)m * i], v);
+  }
+}
+
+// LP inner products per constraint: out[k] += sign * sum_t a_kt w_t
+__global__ void k_lp_dot(int m, const long long* ptr, const int* idx, const double* val, const double* w,
+                         double sign, double* out)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  double s = 0.0;
+  for (long long e = ptr[k]; e < ptr[k + 1]; ++e) s += val[e] * w[idx[e]];
+  out[k] += sign * s;
+}
+
+// LP scatter: w_t += scale * sum_k coef_k a_kt (one thread per LP coordinate)
+__global__ void k_lp_scatter(int nlp, const long long* tptr, const int* tk, const double* tv,
+                             const double* coef, double scale, double* w)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nlp) return;
+  double s = 0.0;
+  for (long long e = tptr[t]; e < tptr[t + 1]; ++e) s += coef[tk[e]] * tv[e];
+  w[t] += scale * s;
+}
+
+// Element-wise LP vectors
+__global__ void k_lp_ops(int op, int nlp, double a, double b, double* o, const double* x, const double* y,
+                         const double* z, const double* w)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nlp) return;
+  switch (op) {
+    case 0: o[t] = a * x[t] - y[t]; break;                         // R = a zi - x
+    case 1: o[t] = (a * x[t] - y[t]) - z[t] * w[t] * x[t]; break;  // R = a zi - x - dx dz zi
+    case 2: o[t] = x[t] * y[t] * z[t]; break;                      // x D zi
+    case 3: o[t] = x[t] - y[t] * z[t] * w[t]; break;               // dx = R - x dz zi
+    default: break;
+  }
+}
+
+// 1/x, 1/sqrt(x) of the LP block (Jal::getInvChol / getInvCholAndInv LP part,
+// sdpa_jordan.cpp:170-177, :201-203); flags x < 0.
+__global__ void k_lp_inv(int nlp, const double* x, double* lx, double* xi, int* bad)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nlp) return;
+  if (x[t] < 0.0) atomicOr(bad, 1);
+  lx[t] = 1.0 / sqrt(x[t]);
+  if (xi) xi[t] = 1.0 / x[t];
+}
+
+// Deterministic reductions (mode 0: dot product, mode 1: max |a|): per-block
+// partials, then an in-order combination.
+__global__ void k_dot_partial(long long len, const double* a, const double* b, double* part, int mode)
+{
+  double s = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < len;
+       t += (long long)gridDim.x * blockDim.x) {
+    if (mode == 0) s += a[t] * b[t];
+    else s = fmax(s, fabs(a[t]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v = __shfl_xor_sync(0xffffffffu, s, o);
+    s = (mode == 1) ? fmax(s, v) : s + v;
+  }
+  __shared__ double w[32];
+  if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) r = (mode == 1) ? fmax(r, w[q]) : r + w[q];
+    part[blockIdx.x] = r;
+  }
+}
+
+__global__ void k_dot_final(int np, const double* part, double* out, int mode, int accumulate, double scale)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double r = 0.0;
+  for (int q = 0; q < np; ++q) r = (mode == 1) ? fmax(r, part[q]) : r + part[q];
+  r *= scale;
+  if (accumulate) *out = (mode == 1) ? fmax(*out, r) : *out + r;
+  else *out = r;
+}
+
+// trace of an n x n matrix into out (accumulate)
+__global__ void k_trace(int n, const double* A, double* out, double scale)
+{
+  __shared__ double w[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += A[i + (size_t)n * i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) r += w[q];
+    *out += scale * r;
+  }
+}
+
+// C = alpha op(A) op(B) + beta C over 64 x 64 output tiles, one tile per
+// block, z = batch (strided); lower skips tiles above the diagonal.
+__global__ void __launch_bounds__(NT) k_gemm(int M, int N, int K, int tA, const double* A, int lda,
+                                             long long sA, int tB, const double* B, int ldb, long long sB,
+                                             double* C, int ldc, long long sC, double alpha, double beta,
+                                             int lower)
+{
+  extern __shared__ double smem[];
+  const int r0 = blockIdx.x * cta::GT, c0 = blockIdx.y * cta::GT;
+  if (lower && r0 + cta::GT - 1 < c0) return;
+  const int z = blockIdx.z;
+  A += sA * z;
+  B += sB * z;
+  C += sC * z;
+  const double* Ap = tA ? A + (size_t)lda * r0 : A + r0;
+  const double* Bp = tB ? B + c0 : B + (size_t)ldb * c0;
+  cta::gemm_rect<NT>(min(cta::GT, M - r0), min(cta::GT, N - c0), K, tA, Ap, lda, tB, Bp, ldb,
+                     C + r0 + (size_t)ldc * c0, ldc, alpha, beta, smem, lower != 0, r0 - c0);
+}
+
+// Diagonal block of the blocked Cholesky: one block factors A[0:bs, 0:bs]
+// (leading dimension lda) with the chosen pivot rule; first failure (global
+// column + 1) is written to *flag if *flag is still 0.
+__global__ void __launch_bounds__(NT) k_chol_diag(int bs, double* A, int lda, int adjust, int col0, int* flag)
+{
+  extern __shared__ double smem[];
+  __shared__ int s_flag;
+  double* sD = smem + 2 * cta::GK * cta::GT;
+  if (*flag) return;
+  const int f = cta::cholesky<NT>(bs, A, lda, adjust != 0, sD, smem, &s_flag);
+  if (f && threadIdx.x == 0) atomicCAS(flag, 0, col0 + f);
+}
+
+// Li = L^{-1} of a bs x bs lower-triangular block (lda) into Li (ld bs)
+__global__ void __launch_bounds__(NT) k_tri_inv(int bs, const double* L, int lda, double* Li, int ldi,
+                                                const int* flag)
+{
+  extern __shared__ double smem[];
+  double* sD = smem + 2 * cta::GK * cta::GT;
+  if (flag && *flag) return;
+  cta::tri_inverse<NT>(bs, L, lda, Li, ldi, sD, smem);
+}
+
+// x = L^{-T} L^{-1} x (Lal::solveSystems, sdpa_linear.cpp:843-862)
+__global__ void __launch_bounds__(NT) k_chol_solve(int m, const double* L, double* x)
+{
+  extern __shared__ double smem[];
+  cta::chol_solve<NT>(m, L, m, x, smem);
+}
+
+// minimum eigenvalue of a formed M = L D L^T (n x n, global) into *out
+__global__ void __launch_bounds__(NT) k_min_eig(int n, const double* M, double* out)
+{
+  extern __shared__ double smem[];
+  __shared__ double redbuf[2 * (NT / 32)];
+  cta::Reducer RD{redbuf, 0};
+  EigScratch es;
+  es.q = smem;
+  es.qold = es.q + n;
+  es.r = es.qold + n;
+  es.w = es.r + n;
+  es.t = es.w + n;
+  es.d = es.t + n;
+  es.e = es.d + TRI_MAX;
+  es.work = es.e + TRI_MAX;
+  es.M = es.work + 6 * TRI_MAX;
+  es.s_val = es.M + 400;
+  es.R = &RD;
+  const double v = (n > 20) ? lanczos_min_eig(n, M, es) : dense_min_eig(n, M, es);
+  if (threadIdx.x == 0) *out = v;
+}
+
+// ------------------------------------------------------------------ host side
+
+static inline int nblk(long long n, int t = 256) { return (int)((n + t - 1) / t); }
+
+struct SdpBlock {
+  int n = 0;
+  int fileBlock = 0;  // 1-based
+  // device dense matrices (n x n)
+  double *C = nullptr, *X = nullptr, *Z = nullptr, *Zi = nullptr, *LXi = nullptr, *LZi = nullptr;
+  double *D = nullptr, *XDZ = nullptr, *R = nullptr, *dX = nullptr, *dZ = nullptr, *W1 = nullptr,
+         *W2 = nullptr, *X0 = nullptr, *Z0 = nullptr, *Lt = nullptr;
+  // constraints touching this block (host-built, device copies)
+  int nc = 0;
+  std::vector<int> hcons, hnnz, hform;
+  std::vector<long long> hptr;
+  std::vector<int> hrow, hcol;
+  std::vector<double> hval;
+  int *cons = nullptr, *nnz = nullptr, *form = nullptr, *row = nullptr, *col = nullptr;
+  long long* ptr = nullptr;
+  double* val = nullptr;
+  // F1/F2 constraints (local indices) and their symmetric CSC
+  std::vector<int> hf1;
+  int* f1 = nullptr;
+  long long *csc_cptr = nullptr, *csc_ptr = nullptr;
+  int* csc_row = nullptr;
+  double* csc_val = nullptr;
+};
+
+struct DevState {
+  int m = 0, nlp = 0, nDim = 0;
+  Params prm;
+  std::vector<int> blockStruct, blockKind, blockIndex;  // kind 0 SDP, 2 LP; index = SDP idx or LP offset
+  std::vector<SdpBlock> sdp;
+  // LP
+  double *lpC = nullptr, *lpx = nullptr, *lpz = nullptr, *lpzi = nullptr, *lplx = nullptr, *lplz = nullptr,
+         *lpD = nullptr, *lpR = nullptr, *lpXDZ = nullptr, *lpdx = nullptr, *lpdz = nullptr, *lpW = nullptr,
+         *lpx0 = nullptr, *lpz0 = nullptr, *lptmp = nullptr;
+  long long *lp_ptr = nullptr, *lpT_ptr = nullptr;
+  int *lp_idx = nullptr, *lpT_k = nullptr;
+  double *lp_val = nullptr, *lpT_v = nullptr;
+  // vectors
+  double *b = nullptr, *y = nullptr, *dy = nullptr, *g = nullptr, *rp = nullptr, *ytmp = nullptr;
+  double* B = nullptr;      // m x m
+  double* Linv = nullptr;   // panel inverse scratch (NBG x NBG)
+  double* T = nullptr;      // panel / F1 scratch
+  size_t Tsize = 0;
+  double* part = nullptr;   // reduction partials
+  double* sc = nullptr;     // scalar slots
+  int* flag = nullptr;
+  std::vector<void*> allocs;
+  double* alloc(size_t n)
+  {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) return nullptr;
+    allocs.push_back(p);
+    return (double*)p;
+  }
+  template <class T>
+  T* upload(const std::vector<T>& v)
+  {
+    void* p = nullptr;
+    size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    allocs.push_back(p);
+    if (!v.empty()) cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return (T*)p;
+  }
+  ~DevState()
+  {
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+static const int NBG = 128;        // panel width of the grid-level Cholesky
+static const int F1_CHUNK = 32;    // F1 constraints processed per batched GEMM
+
+static size_t chol_smem() { return (2 * cta::GK * cta::GT + cta::SD_DOUBLES) * sizeof(double); }
+
+static void gemm(DevState& S, int M, int N, int K, bool tA, const double* A, int lda, bool tB,
+                 const double* B, int ldb, double* C, int ldc, double alpha, double beta, bool lower = false,
+                 int batch = 1, long long sA = 0, long long sB = 0, long long sC = 0)
+{
+  if (M <= 0 || N <= 0) return;
+  dim3 grid((M + cta::GT - 1) / cta::GT, (N + cta::GT - 1) / cta::GT, batch);
+  k_gemm<<<grid, NT, 2 * cta::GK * cta::GT * sizeof(double)>>>(M, N, K, tA, A, lda, sA, tB, B, ldb, sB, C,
+                                                               ldc, sC, alpha, beta, lower ? 1 : 0);
+}
+
+// Blocked right-looking Cholesky of an n x n matrix (lda = n) in place.
+// Returns 0 or the failing column + 1.
+static int cholesky_grid(DevState& S, double* A, int n, bool adjust)
+{
+  cudaMemset(S.flag, 0, sizeof(int));
+  for (int kb = 0; kb < n; kb += NBG) {
+    const int bs = std::min(NBG, n - kb);
+    double* Ad = A + kb + (size_t)n * kb;
+    k_chol_diag<<<1, NT, chol_smem()>>>(bs, Ad, n, adjust ? 1 : 0, kb, S.flag);
+    const int rem = n - kb - bs;
+    if (rem <= 0) continue;
+    k_tri_inv<<<1, NT, chol_smem()>>>(bs, Ad, n, S.Linv, bs, S.flag);
+    double* P = A + (kb + bs) + (size_t)n * kb;
+    // panel: P <- P L_bb^{-T}
+    gemm(S, rem, bs, bs, false, P, n, true, S.Linv, bs, S.T, rem, 1.0, 0.0);
+    k_copy2d<<<nblk((long long)rem * bs), 256>>>(rem, bs, S.T, rem, P, n);
+    // trailing: A22 -= P P^T (lower)
+    gemm(S, rem, rem, bs, false, P, n, true, P, n, A + (kb + bs) + (size_t)n * (kb + bs), n, -1.0, 1.0, true);
+  }
+  int f = 0;
+  cudaMemcpy(&f, S.flag, sizeof(int), cudaMemcpyDeviceToHost);
+  return f;
+}
+
+// Deterministic reduction of len elements into sc[slot]
+static void dot(DevState& S, long long len, const double* a, const double* b, int slot, bool acc,
+                int mode = 0, double scale = 1.0)
+{
+  const int g = (int)std::min<long long>(256, std::max<long long>(1, (len + 1023) / 1024));
+  if (len > 0) k_dot_partial<<<g, 256>>>(len, a, b, S.part, mode);
+  k_dot_final<<<1, 32>>>(len > 0 ? g : 0, S.part, S.sc + slot, mode, acc ? 1 : 0, scale);
+}
+
+static void read_scalars(DevState& S, double* h, int n)
+{
+  cudaMemcpy(h, S.sc, n * sizeof(double), cudaMemcpyDeviceToHost);
+}
+
+Solver::Solver() {}
+Solver::~Solver() { release(); }
+
+void Solver::release()
+{
+  delete d_;
+  d_ = nullptr;
+}
+
+int Solver::formula_count(int f) const
+{
+  if (!d_) return 0;
+  int c = 0;
+  for (const SdpBlock& b : d_->sdp)
+    for (int x : b.hform) c += (x == f);
+  return c;
+}
+
+int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
+{
+  release();
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(SDPAB_ENODEV, "no CUDA device");
+  d_ = new DevState();
+  DevState& S = *d_;
+  S.m = p.m;
+  S.prm = prm;
+  const int m = p.m;
+  if (m < 1) return set_error(SDPAB_EINVAL, "constraint number must be positive");
+  // BlockStruct::makeInternalStructure (sdpa_block.cpp:66-95)
+  const int nb = (int)p.blockStruct.size();
+  S.blockStruct.assign(nb, 0);
+  S.blockKind.assign(nb, 0);
+  S.blockIndex.assign(nb, 0);
+  int nsdp = 0, nlp = 0;
+  for (int l = 0; l < nb; ++l) {
+    int s = p.blockStruct[l];
+    int t = (l < (int)p.blockType.size()) ? p.blockType[l] : 0;
+    if (t == 1) return set_error(SDPAB_EINVAL, "SOCP blocks are not supported (as in the reference)");
+    if (s >= 2 && t == 0) {
+      S.blockKind[l] = 0; S.blockIndex[l] = nsdp++; S.blockStruct[l] = s;
+    } else if (s < 0 || t == 2) {
+      S.blockKind[l] = 2; S.blockIndex[l] = nlp; S.blockStruct[l] = std::abs(s); nlp += std::abs(s);
+    } else if (s == 1) {
+      S.blockKind[l] = 2; S.blockIndex[l] = nlp; S.blockStruct[l] = 1; nlp += 1;
+    } else {
+      return set_error(SDPAB_EINVAL, "invalid block struct");
+    }
+  }
+  S.nlp = nlp;
+  S.sdp.resize(nsdp);
+  S.nDim = nlp;
+  for (int l = 0; l < nb; ++l)
+    if (S.blockKind[l] == 0) {
+      SdpBlock& B = S.sdp[S.blockIndex[l]];
+      B.n = S.blockStruct[l];
+      B.fileBlock = l + 1;
+      S.nDim += B.n;
+    }
+  // sort entries by (k, l, i, j) and split per block / constraint
+  std::vector<Entry> E = p.entries;
+  for (Entry& e : E)
+    if (e.i > e.j) std::swap(e.i, e.j);
+  std::stable_sort(E.begin(), E.end(), [](const Entry& a, const Entry& b) {
+    if (a.k != b.k) return a.k < b.k;
+    if (a.l != b.l) return a.l < b.l;
+    if (a.i != b.i) return a.i < b.i;
+    return a.j < b.j;
+  });
+  std::vector<std::vector<double>> Ch(nsdp);
+  for (int q = 0; q < nsdp; ++q) Ch[q].assign((size_t)S.sdp[q].n * S.sdp[q].n, 0.0);
+  std::vector<double> Clp(nlp, 0.0);
+  // per block: constraint -> entries
+  std::vector<std::vector<std::vector<int>>> per(nsdp);  // [block][k] -> entry indices
+  for (int q = 0; q < nsdp; ++q) per[q].assign(m, {});
+  std::vector<std::vector<std::pair<int, double>>> lpk(m);  // constraint -> (t, v)
+  for (size_t q = 0; q < E.size(); ++q) {
+    const Entry& e = E[q];
+    if (e.k < 0 || e.k > m || e.l < 1 || e.l > nb) return set_error(SDPAB_EINVAL, "entry index out of range");
+    const int l = e.l - 1;
+    const int dim = S.blockStruct[l];
+    if (e.i < 1 || e.j < 1 || e.i > dim || e.j > dim) return set_error(SDPAB_EINVAL, "entry outside its block");
+    if (S.blockKind[l] == 0) {
+      const int bi = S.blockIndex[l];
+      const int n = S.sdp[bi].n;
+      if (e.k == 0) {
+        // C = -F0 (sdpa_io.cpp:511); duplicates accumulate
+        Ch[bi][(e.i - 1) + (size_t)n * (e.j - 1)] -= e.v;
+        if (e.i != e.j) Ch[bi][(e.j - 1) + (size_t)n * (e.i - 1)] -= e.v;
+      } else {
+        per[bi][e.k - 1].push_back((int)q);
+      }
+    } else {
+      if (e.i != e.j) return set_error(SDPAB_EINVAL, "LP block entries must be diagonal");
+      const int t = S.blockIndex[l] + e.i - 1;
+      if (e.k == 0) Clp[t] -= e.v;
+      else lpk[e.k - 1].push_back({t, e.v});
+    }
+  }
+  // device allocations per SDP block
+  for (int q = 0; q < nsdp; ++q) {
+    SdpBlock& B = S.sdp[q];
+    const size_t nn = (size_t)B.n * B.n;
+    B.C = S.upload(Ch[q]);
+    double** mats[] = {&B.X, &B.Z, &B.Zi, &B.LXi, &B.LZi, &B.D, &B.XDZ, &B.R, &B.dX, &B.dZ, &B.W1, &B.W2,
+                       &B.X0, &B.Z0, &B.Lt};
+    for (double** mp : mats) {
+      *mp = S.alloc(nn);
+      if (!*mp) return set_error(SDPAB_ECUDA, "device allocation failed (block matrices)");
+    }
+    // constraint index (InputData::initialize_index_SDP, sdpa_dataset.cpp:268-305)
+    B.hptr.push_back(0);
+    for (int k = 0; k < m; ++k) {
+      if (per[q][k].empty()) continue;
+      B.hcons.push_back(k);
+      int eff = 0;
+      for (int ei : per[q][k]) {
+        const Entry& e = E[ei];
+        B.hrow.push_back(e.i - 1);
+        B.hcol.push_back(e.j - 1);
+        B.hval.push_back(e.v);
+        eff += (e.i == e.j) ? 1 : 2;  // NonZeroEffect (sdpa_struct.cpp:1339-1341)
+      }
+      B.hnnz.push_back(eff);
+      B.hptr.push_back((long long)B.hrow.size());
+    }
+    B.nc = (int)B.hcons.size();
+  }
+  // formula choice: Newton::computeFormula_SDP (sdpa_newton.cpp:515-695)
+  for (int q = 0; q < nsdp; ++q) {
+    SdpBlock& B = S.sdp[q];
+    const double n = B.n;
+    B.hform.assign(B.nc, F3);
+    for (int jl = 0; jl < B.nc; ++jl) {
+      const double jnz = B.hnnz[jl];
+      double up = jnz;
+      for (int il = 0; il < B.nc; ++il) {
+        const int inz = B.hnnz[il];
+        if (inz < jnz) up += inz;
+        else if (inz == jnz && B.hcons[il] > B.hcons[jl]) up += inz;
+      }
+      const double f1 = kappa * n * jnz + n * n * n + kappa * up;
+      const double f2 = kappa * n * jnz + kappa * (n + 1) * up;
+      const double f3 = kappa * (2 * kappa * jnz + 1) * up;
+      const long long count = B.hptr[jl + 1] - B.hptr[jl];
+      const bool dense = count >= (long long)(n * n * 0.20);  // SparseMatrix::changeToDense threshold
+      int f;
+      if (dense) {
+        f = (f1 < f2) ? F1 : F2;
+      } else if (f1 < f2 && f1 < f3) {
+        f = (n <= 200 && 2.0 * n >= jnz) ? F3 : F1;
+      } else if (f2 < f3) {
+        f = F2;
+      } else {
+        f = F3;
+      }
+      B.hform[jl] = f;
+      if (f != F3) B.hf1.push_back(jl);
+    }
+  }
+  // device copies of the constraint index + F1 column structures
+  size_t Tneed = 0;
+  for (int q = 0; q < nsdp; ++q) {
+    SdpBlock& B = S.sdp[q];
+    B.cons = S.upload(B.hcons);
+    B.nnz = S.upload(B.hnnz);
+    B.form = S.upload(B.hform);
+    B.ptr = S.upload(B.hptr);
+    B.row = S.upload(B.hrow);
+    B.col = S.upload(B.hcol);
+    B.val = S.upload(B.hval);
+    B.f1 = S.upload(B.hf1);
+    if (!B.hf1.empty()) {
+      // symmetric CSC of each F1 constraint, indexed by local constraint id
+      std::vector<long long> cptr((size_t)B.nc * (B.n + 1), 0), eptr(B.nc + 1, 0);
+      std::vector<int> crow;
+      std::vector<double> cval;
+      for (int jl = 0; jl < B.nc; ++jl) {
+        eptr[jl] = (long long)crow.size();
+        if (B.hform[jl] == F3) { eptr[jl + 1] = eptr[jl]; continue; }
+        std::vector<std::vector<std::pair<int, double>>> cols(B.n);
+        for (long long e = B.hptr[jl]; e < B.hptr[jl + 1]; ++e) {
+          cols[B.hcol[e]].push_back({B.hrow[e], B.hval[e]});
+          if (B.hrow[e] != B.hcol[e]) cols[B.hrow[e]].push_back({B.hcol[e], B.hval[e]});
+        }
+        long long base = (long long)crow.size();
+        for (int c = 0; c < B.n; ++c) {
+          cptr[(size_t)jl * (B.n + 1) + c] = (long long)crow.size() - base;
+          for (auto& pr : cols[c]) { crow.push_back(pr.first); cval.push_back(pr.second); }
+        }
+        cptr[(size_t)jl * (B.n + 1) + B.n] = (long long)crow.size() - base;
+      }
+      eptr[B.nc] = (long long)crow.size();
+      B.csc_cptr = S.upload(cptr);
+      B.csc_ptr = S.upload(eptr);
+      B.csc_row = S.upload(crow);
+      B.csc_val = S.upload(cval);
+      Tneed = std::max(Tneed, (size_t)2 * F1_CHUNK * B.n * B.n);
+    }
+  }
+  // LP data
+  {
+    std::vector<long long> ptr(m + 1, 0);
+    std::vector<int> idx;
+    std::vector<double> val;
+    std::vector<std::vector<std::pair<int, double>>> byT(nlp);
+    for (int k = 0; k < m; ++k) {
+      for (auto& pr : lpk[k]) {
+        idx.push_back(pr.first);
+        val.push_back(pr.second);
+        byT[pr.first].push_back({k, pr.second});
+      }
+      ptr[k + 1] = (long long)idx.size();
+    }
+    std::vector<long long> tptr(nlp + 1, 0);
+    std::vector<int> tk;
+    std::vector<double> tv;
+    for (int t = 0; t < nlp; ++t) {
+      for (auto& pr : byT[t]) { tk.push_back(pr.first); tv.push_back(pr.second); }
+      tptr[t + 1] = (long long)tk.size();
+    }
+    S.lp_ptr = S.upload(ptr);
+    S.lp_idx = S.upload(idx);
+    S.lp_val = S.upload(val);
+    S.lpT_ptr = S.upload(tptr);
+    S.lpT_k = S.upload(tk);
+    S.lpT_v = S.upload(tv);
+    S.lpC = S.upload(Clp);
+    double** lps[] = {&S.lpx, &S.lpz, &S.lpzi, &S.lplx, &S.lplz, &S.lpD, &S.lpR, &S.lpXDZ, &S.lpdx,
+                      &S.lpdz, &S.lpW, &S.lpx0, &S.lpz0, &S.lptmp};
+    for (double** pp : lps) *pp = S.alloc(nlp);
+  }
+  S.b = S.upload(p.c);
+  S.y = S.alloc(m);
+  S.dy = S.alloc(m);
+  S.g = S.alloc(m);
+  S.rp = S.alloc(m);
+  S.ytmp = S.alloc(m);
+  S.B = S.alloc((size_t)m * m);
+  S.Linv = S.alloc((size_t)NBG * NBG);
+  int nmaxb = 1;
+  for (auto& B : S.sdp) nmaxb = std::max(nmaxb, B.n);
+  Tneed = std::max(Tneed, (size_t)std::max(m, nmaxb) * NBG);
+  S.T = S.alloc(Tneed);
+  S.Tsize = Tneed;
+  S.part = S.alloc(256);
+  S.sc = S.alloc(64);
+  void* fp = nullptr;
+  if (cudaMalloc(&fp, 256) != cudaSuccess) return set_error(SDPAB_ECUDA, "device allocation failed");
+  S.allocs.push_back(fp);
+  S.flag = (int*)fp;
+  if (!S.B || !S.T || !S.b) return set_error(SDPAB_ECUDA, "device allocation failed (Schur matrix)");
+  // shared memory limits of the block-level kernels
+  cudaFuncSetAttribute(k_min_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "setup");
+  return SDPAB_OK;
+}
+
+int Solver::solve(const InitPoint* init)
+{
+  if (!d_) return set_error(SDPAB_ESTATE, "solve before initializeSolve");
+  DevState& S = *d_;
+  const Params& P = S.prm;
+  const int m = S.m, nlp = S.nlp;
+  const double lam = P.lambdaStar;
+  auto t_start = std::chrono::steady_clock::now();
+  stats_ = SolveStats();
+  const int nsdp = (int)S.sdp.size();
+
+  // ------------------------------------------------ initial point
+  bool warm = init != nullptr;
+  if (warm) {
+    // user X -> internal Z, user Y -> internal X, x -> y = -x (sdpa_call.cpp:343-434)
+    std::vector<double> ny(m);
+    for (int k = 0; k < m; ++k) ny[k] = (k < (int)init->xvec.size()) ? -init->xvec[k] : 0.0;
+    cudaMemcpy(S.y, ny.data(), m * sizeof(double), cudaMemcpyHostToDevice);
+    std::vector<double> hx(nlp, 0.0), hz(nlp, 0.0);
+    for (int l = 0; l < (int)S.blockKind.size(); ++l) {
+      const std::vector<double>& Xu = init->X[l];
+      const std::vector<double>& Yu = init->Y[l];
+      if (S.blockKind[l] == 0) {
+        SdpBlock& B = S.sdp[S.blockIndex[l]];
+        const size_t nn = (size_t)B.n * B.n;
+        if (Xu.size() != nn || Yu.size() != nn) return set_error(SDPAB_EINVAL, "init point block size");
+        cudaMemcpy(B.Z, Xu.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+        cudaMemcpy(B.X, Yu.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+      } else {
+        for (int t = 0; t < S.blockStruct[l]; ++t) {
+          hz[S.blockIndex[l] + t] = Xu[t];
+          hx[S.blockIndex[l] + t] = Yu[t];
+        }
+      }
+    }
+    if (nlp) {
+      cudaMemcpy(S.lpx, hx.data(), nlp * sizeof(double), cudaMemcpyHostToDevice);
+      cudaMemcpy(S.lpz, hz.data(), nlp * sizeof(double), cudaMemcpyHostToDevice);
+    }
+  }
+  // Solutions::computeInverse (sdpa_dataset.cpp:117-142); returns false on failure
+  auto compute_inverse = [&]() -> bool {
+    bool ok = true;
+    for (SdpBlock& B : S.sdp) {
+      const long long nn = (long long)B.n * B.n;
+      k_axpby<<<nblk(nn), 256>>>(nn, B.W1, 1.0, B.X, 0.0, nullptr);
+      if (cholesky_grid(S, B.W1, B.n, false)) { ok = false; break; }
+      k_tri_inv<<<1, NT, chol_smem()>>>(B.n, B.W1, B.n, B.LXi, B.n, nullptr);
+      k_axpby<<<nblk(nn), 256>>>(nn, B.W2, 1.0, B.Z, 0.0, nullptr);
+      if (cholesky_grid(S, B.W2, B.n, false)) { ok = false; break; }
+      k_tri_inv<<<1, NT, chol_smem()>>>(B.n, B.W2, B.n, B.LZi, B.n, nullptr);
+      gemm(S, B.n, B.n, B.n, true, B.LZi, B.n, false, B.LZi, B.n, B.Zi, B.n, 1.0, 0.0);
+    }
+    if (ok && nlp) {
+      cudaMemset(S.flag, 0, sizeof(int));
+      k_lp_inv<<<nblk(nlp), 256>>>(nlp, S.lpx, S.lplx, nullptr, S.flag);
+      k_lp_inv<<<nblk(nlp), 256>>>(nlp, S.lpz, S.lplz, S.lpzi, S.flag);
+      int bad = 0;
+      cudaMemcpy(&bad, S.flag, sizeof(int), cudaMemcpyDeviceToHost);
+      if (bad) ok = false;
+    }
+    return ok;
+  };
+  if (warm) {
+    // this solver checks strict interiority of the given point and falls
+    // back to the standard start (the reference ignores the failure here,
+    // sdpa_solve.cpp:63)
+    if (!compute_inverse()) {
+      warm = false;
+      stats_.warm_start_rejected = 1;
+    }
+  }
+  if (!warm) {
+    // Solutions::initialize (sdpa_dataset.cpp:47-74)
+    for (SdpBlock& B : S.sdp) {
+      const long long nn = (long long)B.n * B.n;
+      k_set_identity<<<nblk(nn), 256>>>(B.n, B.X, lam);
+      k_set_identity<<<nblk(nn), 256>>>(B.n, B.Z, lam);
+      k_set_identity<<<nblk(nn), 256>>>(B.n, B.LXi, 1.0 / sqrt(lam));
+      k_set_identity<<<nblk(nn), 256>>>(B.n, B.LZi, 1.0 / sqrt(lam));
+      k_set_identity<<<nblk(nn), 256>>>(B.n, B.Zi, 1.0 / lam);
+    }
+    if (nlp) {
+      std::vector<double> v(nlp, lam), v2(nlp, 1.0 / sqrt(lam)), v3(nlp, 1.0 / lam);
+      cudaMemcpy(S.lpx, v.data(), nlp * sizeof(double), cudaMemcpyHostToDevice);
+      cudaMemcpy(S.lpz, v.data(), nlp * sizeof(double), cudaMemcpyHostToDevice);
+      cudaMemcpy(S.lplx, v2.data(), nlp * sizeof(double), cudaMemcpyHostToDevice);
+      cudaMemcpy(S.lplz, v2.data(), nlp * sizeof(double), cudaMemcpyHostToDevice);
+      cudaMemcpy(S.lpzi, v3.data(), nlp * sizeof(double), cudaMemcpyHostToDevice);
+    }
+    cudaMemset(S.y, 0, m * sizeof(double));
+  }
+  if (warm) {
+    for (SdpBlock& B : S.sdp) {
+      const long long nn = (long long)B.n * B.n;
+      k_axpby<<<nblk(nn), 256>>>(nn, B.X0, 1.0, B.X, 0.0, nullptr);
+      k_axpby<<<nblk(nn), 256>>>(nn, B.Z0, 1.0, B.Z, 0.0, nullptr);
+    }
+    if (nlp) {
+      k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpx0, 1.0, S.lpx, 0.0, nullptr);
+      k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpz0, 1.0, S.lpz, 0.0, nullptr);
+    }
+  }
+
+  // ------------------------------------------------ helpers
+  // out[k] = base[k] + sign * sum_blocks A_k . W   (W per block; LP vector wl)
+  auto a_dot = [&](double* out, const double* base, double sign, std::vector<const double*> W,
+                   const double* wl) {
+    if (base) cudaMemcpy(out, base, m * sizeof(double), cudaMemcpyDeviceToDevice);
+    else cudaMemset(out, 0, m * sizeof(double));
+    for (int q = 0; q < nsdp; ++q) {
+      SdpBlock& B = S.sdp[q];
+      if (B.nc) k_sp_dot<<<nblk((long long)B.nc * 32), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val,
+                                                              W[q], B.n, sign, out);
+    }
+    if (nlp) k_lp_dot<<<nblk(m), 256>>>(m, S.lp_ptr, S.lp_idx, S.lp_val, wl, sign, out);
+  };
+  // residuals (Residuals::compute, sdpa_dataset.cpp:585-608): rp = b - A.X,
+  // D = C - Z - sum y_k A_k; sc[0] = |rp|max, sc[1] = |D|max
+  auto residuals = [&]() {
+    std::vector<const double*> Xs;
+    for (auto& B : S.sdp) Xs.push_back(B.X);
+    a_dot(S.rp, S.b, -1.0, Xs, S.lpx);
+    dot(S, m, S.rp, nullptr, 0, false, 1);
+    bool first = true;
+    for (SdpBlock& B : S.sdp) {
+      const long long nn = (long long)B.n * B.n;
+      k_axpby<<<nblk(nn), 256>>>(nn, B.D, 1.0, B.C, -1.0, B.Z);
+      if (B.nc) k_sp_scatter<<<nblk((long long)B.nc * 32), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val,
+                                                                  S.y, -1.0, B.D, B.n);
+      dot(S, nn, B.D, nullptr, 1, !first, 1);
+      first = false;
+    }
+    if (nlp) {
+      k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpD, 1.0, S.lpC, -1.0, S.lpz);
+      k_lp_scatter<<<nblk(nlp), 256>>>(nlp, S.lpT_ptr, S.lpT_k, S.lpT_v, S.y, -1.0, S.lpD);
+      dot(S, nlp, S.lpD, nullptr, 1, !first, 1);
+      first = false;
+    }
+    if (first) cudaMemset(S.sc + 1, 0, sizeof(double));
+  };
+  // sum over blocks of <A, B> (full Frobenius) + LP into sc[slot]
+  auto ip = [&](int slot, std::vector<const double*> A, std::vector<const double*> Bm, const double* al,
+                const double* bl) {
+    bool acc = false;
+    for (int q = 0; q < nsdp; ++q) {
+      dot(S, (long long)S.sdp[q].n * S.sdp[q].n, A[q], Bm[q], slot, acc);
+      acc = true;
+    }
+    if (nlp) { dot(S, nlp, al, bl, slot, acc); acc = true; }
+    if (!acc) cudaMemset(S.sc + slot, 0, sizeof(double));
+  };
+  auto mats = [&](int which) {
+    std::vector<const double*> v;
+    for (auto& B : S.sdp) {
+      switch (which) {
+        case 0: v.push_back(B.X); break;
+        case 1: v.push_back(B.Z); break;
+        case 2: v.push_back(B.dX); break;
+        case 3: v.push_back(B.dZ); break;
+        case 4: v.push_back(B.C); break;
+        case 5: v.push_back(B.X0); break;
+        case 6: v.push_back(B.Z0); break;
+      }
+    }
+    return v;
+  };
+
+  residuals();
+  ip(2, mats(4), mats(0), S.lpC, S.lpx);  // objP = C.X
+  dot(S, m, S.b, S.y, 3, false);          // objD = b.y
+  if (warm) ip(4, mats(0), mats(1), S.lpx, S.lpz);  // X.Z
+  double h[16];
+  read_scalars(S, h, 5);
+  Scalars sc;
+  const double mu0 = warm ? h[4] / S.nDim : lam * lam;
+  init_scalars(sc, P, S.nDim, mu0, h[0], h[1], h[2], h[3]);
+  update_check(sc, P);
+
+  int iter = 0;
+  while (true) {
+    if (!update_check(sc, P) || iter >= P.maxIteration) break;
+    predictor_setup(sc, P);
+    const bool dinf = dual_infeasible(sc);
+    // ---- predictor rMat / gVec (Newton::compute_rMat, Make_gVec)
+    std::vector<const double*> Wv;
+    for (SdpBlock& B : S.sdp) {
+      const long long nn = (long long)B.n * B.n;
+      k_axpby<<<nblk(nn), 256>>>(nn, B.R, sc.beta * sc.mu, B.Zi, -1.0, B.X);
+      if (dinf) {
+        gemm(S, B.n, B.n, B.n, false, B.X, B.n, false, B.D, B.n, B.W1, B.n, 1.0, 0.0);
+        gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.XDZ, B.n, 1.0, 0.0);
+        k_axpby<<<nblk(nn), 256>>>(nn, B.W2, 1.0, B.R, -1.0, B.XDZ);
+        Wv.push_back(B.W2);
+      } else {
+        Wv.push_back(B.R);
+      }
+    }
+    const double* Wl = S.lpR;
+    if (nlp) {
+      k_lp_ops<<<nblk(nlp), 256>>>(0, nlp, sc.beta * sc.mu, 0, S.lpR, S.lpzi, S.lpx, nullptr, nullptr);
+      if (dinf) {
+        k_lp_ops<<<nblk(nlp), 256>>>(2, nlp, 0, 0, S.lpXDZ, S.lpx, S.lpD, S.lpzi, nullptr);
+        k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpW, 1.0, S.lpR, -1.0, S.lpXDZ);
+        Wl = S.lpW;
+      }
+    }
+    a_dot(S.g, S.rp, -1.0, Wv, Wl);
+    // ---- Schur complement (Newton::Make_bMat)
+    cudaMemset(S.B, 0, (size_t)m * m * sizeof(double));
+    for (SdpBlock& B : S.sdp) {
+      if (!B.nc) continue;
+      k_f3<<<nblk((long long)B.nc * B.nc), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val, B.nnz, B.form,
+                                                  B.X, B.Zi, B.n, S.B, m);
+      const int nf = (int)B.hf1.size();
+      for (int q0 = 0; q0 < nf; q0 += F1_CHUNK) {
+        const int cnt = std::min(F1_CHUNK, nf - q0);
+        const size_t nn = (size_t)B.n * B.n;
+        double* T = S.T;
+        double* G = S.T + (size_t)F1_CHUNK * nn;
+        k_f1_left<<<dim3(B.n, cnt), 256>>>(B.n, q0, B.f1, B.csc_cptr, B.csc_ptr, B.csc_row, B.csc_val, B.X, T);
+        gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn);
+        k_f1_dot<<<dim3(cnt, 16), 256>>>(B.nc, q0, B.f1, B.cons, B.ptr, B.row, B.col, B.val, B.nnz, G, B.n, S.B, m);
+      }
+    }
+    if (nlp) k_lp_bmat<<<nlp, 256>>>(S.lpT_ptr, S.lpT_k, S.lpT_v, S.lpx, S.lpzi, S.B, m);
+    // ---- Cholesky with adjustment + solve (Newton::compute_DyVec)
+    if (cholesky_grid(S, S.B, m, true)) {
+      stats_.cholesky_failed = 1;
+      break;
+    }
+    cudaMemcpy(S.dy, S.g, m * sizeof(double), cudaMemcpyDeviceToDevice);
+    k_chol_solve<<<1, NT, cta::SD_DOUBLES * sizeof(double)>>>(m, S.B, S.dy);
+
+    // ---- dZ and dX (compute_DzMat / compute_DxMat)
+    auto direction = [&]() {
+      for (SdpBlock& B : S.sdp) {
+        const long long nn = (long long)B.n * B.n;
+        if (dinf) k_axpby<<<nblk(nn), 256>>>(nn, B.dZ, 1.0, B.D, 0.0, nullptr);
+        else cudaMemset(B.dZ, 0, nn * sizeof(double));
+        if (B.nc) k_sp_scatter<<<nblk((long long)B.nc * 32), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val,
+                                                                    S.dy, -1.0, B.dZ, B.n);
+        gemm(S, B.n, B.n, B.n, false, B.X, B.n, false, B.dZ, B.n, B.W1, B.n, 1.0, 0.0);
+        gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.W2, B.n, 1.0, 0.0);
+        k_sym_diff<<<nblk(nn), 256>>>(B.n, B.dX, B.R, B.W2);
+      }
+      if (nlp) {
+        if (dinf) k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpdz, 1.0, S.lpD, 0.0, nullptr);
+        else cudaMemset(S.lpdz, 0, nlp * sizeof(double));
+        k_lp_scatter<<<nblk(nlp), 256>>>(nlp, S.lpT_ptr, S.lpT_k, S.lpT_v, S.dy, -1.0, S.lpdz);
+        k_lp_ops<<<nblk(nlp), 256>>>(3, nlp, 0, 0, S.lpdx, S.lpR, S.lpx, S.lpdz, S.lpzi);
+      }
+    };
+    direction();
+    auto step_products = [&]() {
+      ip(5, mats(4), mats(2), S.lpC, S.lpdx);   // C.dX
+      dot(S, m, S.b, S.dy, 6, false);            // b.dy
+      ip(7, mats(0), mats(3), S.lpx, S.lpdz);   // X.dZ
+      ip(8, mats(2), mats(1), S.lpdx, S.lpz);   // dX.Z
+      ip(9, mats(2), mats(3), S.lpdx, S.lpdz);  // dX.dZ
+    };
+    step_products();
+    read_scalars(S, h, 10);
+    predictor_step(sc, h[5], h[6]);
+    corrector_beta(sc, P, h[7], h[8], h[9]);
+
+    // ---- corrector
+    Wv.clear();
+    for (SdpBlock& B : S.sdp) {
+      const long long nn = (long long)B.n * B.n;
+      gemm(S, B.n, B.n, B.n, false, B.dX, B.n, false, B.dZ, B.n, B.W1, B.n, 1.0, 0.0);
+      gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.W2, B.n, 1.0, 0.0);
+      k_axpby_sub<<<nblk(nn), 256>>>(nn, B.R, sc.beta * sc.mu, B.Zi, -1.0, B.X, B.W2);
+      if (dinf) {
+        k_axpby<<<nblk(nn), 256>>>(nn, B.W1, 1.0, B.R, -1.0, B.XDZ);
+        Wv.push_back(B.W1);
+      } else {
+        Wv.push_back(B.R);
+      }
+    }
+    Wl = S.lpR;
+    if (nlp) {
+      k_lp_ops<<<nblk(nlp), 256>>>(1, nlp, sc.beta * sc.mu, 0, S.lpR, S.lpzi, S.lpx, S.lpdx, S.lpdz);
+      if (dinf) {
+        k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpW, 1.0, S.lpR, -1.0, S.lpXDZ);
+        Wl = S.lpW;
+      }
+    }
+    a_dot(S.dy, S.rp, -1.0, Wv, Wl);
+    k_chol_solve<<<1, NT, cta::SD_DOUBLES * sizeof(double)>>>(m, S.B, S.dy);
+    direction();
+
+    // ---- step length (StepLength::MehrotraCorrector)
+    double minX = 1.0e50, minZ = 1.0e50;
+    for (SdpBlock& B : S.sdp) {
+      const size_t shm = (size_t)(5 * B.n + 2 * TRI_MAX + 6 * TRI_MAX + 400 + 4) * sizeof(double);
+      gemm(S, B.n, B.n, B.n, false, B.dX, B.n, true, B.LXi, B.n, B.W1, B.n, 1.0, 0.0);
+      gemm(S, B.n, B.n, B.n, false, B.LXi, B.n, false, B.W1, B.n, B.W2, B.n, 1.0, 0.0);
+      k_min_eig<<<1, NT, shm>>>(B.n, B.W2, S.sc + 10);
+      gemm(S, B.n, B.n, B.n, false, B.dZ, B.n, true, B.LZi, B.n, B.W1, B.n, 1.0, 0.0);
+      gemm(S, B.n, B.n, B.n, false, B.LZi, B.n, false, B.W1, B.n, B.W2, B.n, 1.0, 0.0);
+      k_min_eig<<<1, NT, shm>>>(B.n, B.W2, S.sc + 11);
+      double mm[2];
+      cudaMemcpy(mm, S.sc + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+      minX = std::min(minX, mm[0]);
+      minZ = std::min(minZ, mm[1]);
+    }
+    if (nlp) {
+      // LP part of Jal::getMinEigen (sdpa_jordan.cpp:99-105): dx_t / x_t
+      std::vector<double> a(nlp), bb(nlp), cc(nlp), dd(nlp);
+      cudaMemcpy(a.data(), S.lpdx, nlp * sizeof(double), cudaMemcpyDeviceToHost);
+      cudaMemcpy(bb.data(), S.lplx, nlp * sizeof(double), cudaMemcpyDeviceToHost);
+      cudaMemcpy(cc.data(), S.lpdz, nlp * sizeof(double), cudaMemcpyDeviceToHost);
+      cudaMemcpy(dd.data(), S.lplz, nlp * sizeof(double), cudaMemcpyDeviceToHost);
+      for (int t = 0; t < nlp; ++t) {
+        minX = std::min(minX, a[t] * bb[t] * bb[t]);
+        minZ = std::min(minZ, cc[t] * dd[t] * dd[t]);
+      }
+    }
+    step_products();
+    read_scalars(S, h, 10);
+    corrector_step(sc, P, minX, minZ, h[5], h[6], h[7], h[8], h[9], sc.objD, sc.objP);
+    {
+      double row[8] = {sc.mu, sc.thetaP, sc.thetaD, sc.objP, sc.objD, sc.alphaP, sc.alphaD, sc.beta};
+      stats_.trace.insert(stats_.trace.end(), row, row + 8);
+    }
+
+    // ---- update (Solutions::update)
+    for (SdpBlock& B : S.sdp) {
+      const long long nn = (long long)B.n * B.n;
+      k_axpby<<<nblk(nn), 256>>>(nn, B.X, 1.0, B.X, sc.alphaP, B.dX);
+      k_axpby<<<nblk(nn), 256>>>(nn, B.Z, 1.0, B.Z, sc.alphaD, B.dZ);
+    }
+    if (nlp) {
+      k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpx, 1.0, S.lpx, sc.alphaP, S.lpdx);
+      k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpz, 1.0, S.lpz, sc.alphaD, S.lpdz);
+    }
+    k_axpby<<<nblk(m), 256>>>(m, S.y, 1.0, S.y, sc.alphaD, S.dy);
+    if (cannot_move(sc)) break;
+    if (!compute_inverse()) break;
+    // ---- residuals, mu, objectives, rho
+    residuals();
+    ip(2, mats(4), mats(0), S.lpC, S.lpx);
+    dot(S, m, S.b, S.y, 3, false);
+    ip(4, mats(0), mats(1), S.lpx, S.lpz);
+    if (warm) {
+      ip(13, mats(5), mats(1), S.lpx0, S.lpz);
+      ip(14, mats(0), mats(6), S.lpx, S.lpz0);
+    } else {
+      cudaMemset(S.sc + 13, 0, 2 * sizeof(double));
+      for (SdpBlock& B : S.sdp) {
+        k_trace<<<1, 256>>>(B.n, B.Z, S.sc + 13, lam);
+        k_trace<<<1, 256>>>(B.n, B.X, S.sc + 14, lam);
+      }
+    }
+    read_scalars(S, h, 16);
+    double x0zM = h[13], xMz0 = h[14];
+    if (!warm && nlp) {
+      std::vector<double> a(nlp), bb(nlp);
+      cudaMemcpy(a.data(), S.lpz, nlp * sizeof(double), cudaMemcpyDeviceToHost);
+      cudaMemcpy(bb.data(), S.lpx, nlp * sizeof(double), cudaMemcpyDeviceToHost);
+      for (int t = 0; t < nlp; ++t) { x0zM += lam * a[t]; xMz0 += lam * bb[t]; }
+    }
+    after_update(sc, P, h[4], h[0], h[1], h[2], h[3], x0zM, xMz0);
+    ++iter;
+  }
+  // final residuals (sdpa_solve.cpp:204), results
+  residuals();
+  read_scalars(S, h, 2);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_error(e, "solve");
+  stats_.iterations = iter;
+  stats_.internal_phase = sc.phase;
+  stats_.phase = user_phase(sc.phase);
+  stats_.primal_obj = -sc.objD;
+  stats_.dual_obj = -sc.objP;
+  stats_.objValPrimal = sc.objP;
+  stats_.objValDual = sc.objD;
+  stats_.primal_error = h[1];
+  stats_.dual_error = h[0];
+  stats_.mu = sc.mu;
+  xvec_.assign(m, 0.0);
+  cudaMemcpy(xvec_.data(), S.y, m * sizeof(double), cudaMemcpyDeviceToHost);
+  for (double& v : xvec_) v = -v;
+  const int nb = (int)S.blockKind.size();
+  Xres_.assign(nb, {});
+  Yres_.assign(nb, {});
+  std::vector<double> hx(nlp), hz(nlp);
+  if (nlp) {
+    cudaMemcpy(hx.data(), S.lpx, nlp * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(hz.data(), S.lpz, nlp * sizeof(double), cudaMemcpyDeviceToHost);
+  }
+  for (int l = 0; l < nb; ++l) {
+    if (S.blockKind[l] == 0) {
+      SdpBlock& B = S.sdp[S.blockIndex[l]];
+      const size_t nn = (size_t)B.n * B.n;
+      Xres_[l].resize(nn);
+      Yres_[l].resize(nn);
+      cudaMemcpy(Xres_[l].data(), B.Z, nn * sizeof(double), cudaMemcpyDeviceToHost);
+      cudaMemcpy(Yres_[l].data(), B.X, nn * sizeof(double), cudaMemcpyDeviceToHost);
+    } else {
+      const int off = S.blockIndex[l], len = S.blockStruct[l];
+      Xres_[l].assign(hz.begin() + off, hz.begin() + off + len);
+      Yres_[l].assign(hx.begin() + off, hx.begin() + off + len);
+    }
+  }
+  stats_.solve_seconds =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "solve");
+  return SDPAB_OK;
+}
+
+}  // namespace sdpab

@@ -1,0 +1,84 @@
+// Host-driven solver for one SDPA problem with any block structure (SDP
+// blocks + LP block), the engine behind the drop-in SDPA class.  Host C++
+// runs the Mehrotra predictor-corrector control (ipm_control.h, the
+// reference's sdpa_parts.cpp scalar logic); every vector/matrix step is a
+// CUDA kernel on device-resident data.  No CPU fallback exists.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "ipm_control.h"
+
+namespace sdpab {
+
+// One nonzero of F_k (k = 0 is F0) exactly as a .dat-s line states it:
+// 1-based block l, row i, column j (i <= j after staging), value v.
+struct Entry {
+  int k, l, i, j;
+  double v;
+};
+
+// A problem in SDPA's input form (the .dat-s file / inputElement calls).
+struct ProblemData {
+  int m = 0;
+  std::vector<int> blockStruct;   // signed block sizes (negative = LP)
+  std::vector<int> blockType;     // 0 = SDP, 1 = SOCP (rejected), 2 = LP (SDPA::ConeType)
+  std::vector<double> c;          // the m-vector c (b of the internal problem)
+  std::vector<Entry> entries;
+};
+
+// Warm start in the user's terms (SDPA::inputInitXVec / XMat / YMat): dense
+// column-major n x n per SDP block, a vector per LP block, in file block order.
+struct InitPoint {
+  std::vector<double> xvec;
+  std::vector<std::vector<double>> X, Y;
+};
+
+struct SolveStats {
+  int iterations = 0;
+  int phase = 0;            // SDPA::PhaseType code (after reverse + getPhaseValue)
+  int internal_phase = 0;
+  double primal_obj = 0, dual_obj = 0;  // getPrimalObj / getDualObj
+  double primal_error = 0, dual_error = 0;
+  double mu = 0;
+  double objValPrimal = 0, objValDual = 0;  // internal SolveInfo values
+  double solve_seconds = 0;
+  int cholesky_failed = 0;
+  int warm_start_rejected = 0;
+  std::vector<double> trace;  // per iteration: mu, thetaP, thetaD, objP, objD, alphaP, alphaD, beta
+};
+
+struct DevState;  // device buffers (single_engine.cu)
+
+class Solver {
+ public:
+  Solver();
+  ~Solver();
+  Solver(const Solver&) = delete;
+  Solver& operator=(const Solver&) = delete;
+
+  // SDPA::initializeSolve (sdpa_solve.cpp:10-43): block layout, constraint
+  // index, formula choice (computeFormula_SDP), device upload.  Returns an
+  // SDPAB_* status.
+  int setup(const ProblemData& p, const Params& prm, double kappa);
+  // SDPA::solve (sdpa_solve.cpp:59-233); init may be NULL.
+  int solve(const InitPoint* init);
+  void release();
+
+  const SolveStats& stats() const { return stats_; }
+  // Results in the reference getters' layout (file block order, 1-based l).
+  const std::vector<double>& xvec() const { return xvec_; }
+  const std::vector<double>& resultX(int l) const { return Xres_[l - 1]; }  // getResultXMat
+  const std::vector<double>& resultY(int l) const { return Yres_[l - 1]; }  // getResultYMat
+  int formula_count(int f) const;  // number of (constraint, block) pairs using F1/F2/F3
+
+ private:
+  DevState* d_ = nullptr;
+  SolveStats stats_;
+  std::vector<double> xvec_;
+  std::vector<std::vector<double>> Xres_, Yres_;
+};
+
+}  // namespace sdpab

@@ -1,0 +1,150 @@
+"""The drop-in SDPA class (host-driven CUDA solver) through the whole-problem
+C ABI, against the reference manual's known answers and the reference
+solver's results (golden fixtures): multiple SDP blocks, LP blocks, F1 and
+F3 Schur formulas, the .dat-s and .dat readers, warm start."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from golden_util import GOLDEN, known_answers, large, rel, small
+
+pytestmark = pytest.mark.gpu
+
+_spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+MG = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(MG)
+
+OBJ_TOL = 1e-6   # relative objective tolerance
+X_TOL = 1e-5     # absolute tolerance on x (SDPA's xVec)
+
+
+def _solve(inst, params=None, path=None, sparse_type=0):
+    from sdpa_b200.sdpa import SDPA
+    s = SDPA()
+    if params:
+        s.setParameter(**params)
+    if path:
+        s.readInput(path, sparse_type)
+    else:
+        s.inputProblem(inst)
+    s.solve()
+    return s
+
+
+def test_manual_examples():
+    ka = known_answers()
+    for name, inst in (("example1", MG.example1()), ("example2", MG.example2())):
+        s = _solve(inst)
+        man = ka["manual"][name]
+        assert s.getPhaseString() == "pdOPT"
+        assert s.getIteration() == man["iterations"], name
+        assert rel(s.getPrimalObj(), man["primal_obj"]) < 1e-8
+        assert rel(s.getDualObj(), man["dual_obj"]) < 1e-8
+        ref = ka["reference_default"][name]
+        assert np.max(np.abs(s.getResultXVec() - np.array(ref["xvec"]))) < X_TOL
+
+
+def test_param_1e8_examples():
+    ka = known_answers()
+    prm = dict(maxIteration=200, epsilonStar=1e-8, lowerBound=-1e20, upperBound=1e20, epsilonDash=1e-8)
+    for name, inst in (("example1", MG.example1()), ("example2", MG.example2())):
+        s = _solve(inst, prm)
+        ref = ka["reference_param_1e-8"][name]
+        assert s.getIteration() == ref["iterations"]
+        assert rel(s.getPrimalObj(), ref["primal_obj"]) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["mc100", "mc20", "mc50w", "lt20", "lt40", "rnd40", "rnd120", "ex2"])
+def test_small_instances_match_reference(name, tmp_path):
+    meta, arr = small()
+    inst = dict(MG.small_cases())[name]
+    path = str(tmp_path / f"{name}.dat-s")
+    inst.write(path)
+    s = _solve(None, path=path)   # through the .dat-s reader
+    g = meta[name]
+    assert s.getPhaseString() == g["phase"]
+    assert abs(s.getIteration() - g["iterations"]) <= 1
+    assert rel(s.getPrimalObj(), g["primal_obj"]) < OBJ_TOL
+    assert rel(s.getDualObj(), g["dual_obj"]) < OBJ_TOL
+    assert np.max(np.abs(s.getResultXVec() - arr[name + ".xvec"])) < X_TOL
+    if name + ".Y1" in arr:
+        Y = s.getResultYMat(1)
+        assert np.max(np.abs(Y.ravel(order="F") - arr[name + ".Y1"])) < 1e-4
+
+
+def test_dense_dat_reader(tmp_path):
+    """example2 written in the dense .dat format (F0..Fm as full block matrices)."""
+    ka = known_answers()
+    inst = MG.example2()
+    lines = ["*dense example2", "5", "3", "2 3 -2", " ".join(map(str, inst.c))]
+    for k in range(6):
+        B1, B2, lp = np.zeros((2, 2)), np.zeros((3, 3)), np.zeros(2)
+        for kk, l, i, j, v in zip(inst.k, inst.l, inst.i, inst.j, inst.v):
+            if kk != k:
+                continue
+            if l == 1:
+                B1[i - 1, j - 1] = B1[j - 1, i - 1] = v
+            elif l == 2:
+                B2[i - 1, j - 1] = B2[j - 1, i - 1] = v
+            else:
+                lp[i - 1] = v
+        lines.append("{ " + str(B1.tolist()) + str(B2.tolist()) + str(lp.tolist()) + " }")
+    p = tmp_path / "example2.dat"
+    p.write_text("\n".join(lines).replace("[", "{").replace("]", "}") + "\n")
+    s = _solve(None, path=str(p))
+    assert s.getIteration() == ka["manual"]["example2"]["iterations"]
+    assert rel(s.getPrimalObj(), ka["manual"]["example2"]["primal_obj"]) < 1e-8
+
+
+def test_warm_start_and_fallback():
+    """copyCurrentToInit re-solve (example4 of the reference's libexample) and
+    the strict-interiority fallback of a non-interior initial point."""
+    from sdpa_b200.sdpa import SDPA
+    inst = dict(MG.small_cases())["mc20"]
+    s = SDPA()
+    s.inputProblem(inst)
+    s.solve()
+    obj = s.getPrimalObj()
+    x = s.getResultXVec()
+    Xm, Ym = s.getResultXMat(1), s.getResultYMat(1)
+    # a strictly interior point near the optimum: shift toward the centre
+    t = SDPA()
+    t.inputProblem(inst)
+    t.setInitPoint(x - 0.1, [Xm + 0.1 * np.eye(20)], [0.9 * Ym + 0.1 * np.eye(20)])
+    t.solve()
+    assert t.getPhaseString() == "pdOPT"
+    assert rel(t.getPrimalObj(), obj) < OBJ_TOL
+    # a non-interior point (X indefinite) falls back to the standard start
+    u = SDPA()
+    u.inputProblem(inst)
+    u.setInitPoint(np.zeros(20), [-np.eye(20)], [np.eye(20)])
+    u.solve()
+    assert u.getPhaseString() == "pdOPT"
+    assert rel(u.getPrimalObj(), obj) < OBJ_TOL
+    assert u.getIteration() == s.getIteration()
+
+
+def test_dimacs_errors_small():
+    s = _solve(MG.example1())
+    d = s.getDimacsError()
+    assert d[1] < 1e-7 and d[3] < 1e-7 and abs(d[5]) < 1e-6 and d[2] == 0.0 and d[4] == 0.0
+
+
+@pytest.mark.parametrize("name", ["lt200", "rnd2000"])
+def test_large_configs_match_reference(name):
+    """Lovasz theta G(200, 0.5) (m = 9986, F3, dense 9986^2 Schur) and the random
+    m = 2000 SDP with blocks {500, LP 50} (F1 formula)."""
+    from sdpa_b200 import instances
+    meta, arr = large()
+    if meta is None:
+        pytest.skip("large fixtures not generated")
+    inst = instances.lovasz_theta(200, 0.5, 1) if name == "lt200" else instances.random_sdp(seed=1)
+    s = _solve(inst)
+    g = meta[name]
+    assert s.getPhaseString() == g["phase"]
+    assert abs(s.getIteration() - g["iterations"]) <= 1
+    assert rel(s.getPrimalObj(), g["primal_obj"]) < OBJ_TOL
+    assert rel(s.getDualObj(), g["dual_obj"]) < OBJ_TOL
+    assert np.max(np.abs(s.getResultXVec() - arr[name + ".xvec"])) < X_TOL
