@@ -139,6 +139,46 @@ SDPAB_API int sdpab_sdpa_write_init(sdpab_sdpa* h, const char* path);
 /* SDPA::copyCurrentToInit (sdpa_call.cpp:1238-1245) + setInitPoint(true) */
 SDPAB_API int sdpab_sdpa_copy_current_to_init(sdpab_sdpa* h);
 
+/* ------------------------------------------------ learned warm start (MPNN) */
+
+/* No counterpart in the reference.  A 3-layer message-passing network over
+ * the MaxCut graph predicts, per node, r_i = 4 x_i / d_i (x = SDPA's x
+ * vector, d = weighted degree); the batched solver turns the proposed x into
+ * a strictly interior start (SDPAB_INIT_DUAL).  BF16 weights, FP32
+ * accumulation, hand-written forward / backward / Adam kernels; all pointers
+ * are device pointers. */
+#define SDPAB_MPNN_HIDDEN 64
+#define SDPAB_MPNN_FEATURES 8
+#define SDPAB_MPNN_LAYERS 3
+
+typedef struct sdpab_graph_batch {
+  int num_nodes;           /* nodes of all graphs of the batch */
+  long long num_edges;     /* directed edges (each undirected edge twice) */
+  const int* rowptr;       /* [num_nodes+1] CSR over destination nodes */
+  const int* col;          /* [num_edges] source node of each edge */
+  const float* aval;       /* [num_edges] a_ij = w_ij / (d_i + 1)  (i destination) */
+  const float* aval_t;     /* [num_edges] a_ji for the same (i, j) slot (transpose) */
+  const float* feat;       /* [num_nodes * SDPAB_MPNN_FEATURES] node features */
+  int mask_count;          /* nodes counted by the loss mask (0 = all) */
+} sdpab_graph_batch;
+
+SDPAB_API long long sdpab_mpnn_num_params(void);
+/* float counts of the activation and backward scratch buffers for num_nodes */
+SDPAB_API long long sdpab_mpnn_act_floats(int num_nodes);
+SDPAB_API long long sdpab_mpnn_scratch_floats(int num_nodes);
+/* out[num_nodes] = predicted r per node */
+SDPAB_API int sdpab_mpnn_forward(const sdpab_graph_batch* g, const unsigned short* weights_bf16, float* act,
+                                 float* out, void* stream);
+/* loss = sum_i mask_i (r_i - target_i)^2 / count and grads[num_params] */
+SDPAB_API int sdpab_mpnn_loss_grad(const sdpab_graph_batch* g, const unsigned short* weights_bf16, float* act,
+                                   float* scratch, const float* target, const float* mask, float* grads,
+                                   float* loss, void* stream);
+/* one Adam step on the FP32 master weights, refreshing the BF16 copy */
+SDPAB_API int sdpab_mpnn_adam(float* master, unsigned short* weights_bf16, const float* grads, float* m1,
+                              float* m2, int step, float lr, float beta1, float beta2, float eps,
+                              float weight_decay, void* stream);
+SDPAB_API int sdpab_mpnn_to_bf16(const float* master, unsigned short* weights_bf16, void* stream);
+
 /* ---------------------------------------------------------------- batched API */
 
 /* Precision modes of the batched solver. */
@@ -163,11 +203,20 @@ typedef struct sdpab_batch {
   const long long* dense_off;  /* [count] offset of the instance's n*n blocks in X / Y arrays */
 } sdpab_batch;
 
+#define SDPAB_INIT_NONE 0      /* standard start lambda* I */
+#define SDPAB_INIT_POINT 1     /* start from the given (x, X, Y) */
+#define SDPAB_INIT_DUAL 2      /* start from a proposed x only (constraints X_ii = b_i, i.e.
+                                  F_i = e_i e_i^T): the solver shifts x until
+                                  X = sum F_i x_i - F0 is positive definite with margin
+                                  init_margin * mean |F0_ii|, and sets
+                                  Y = D X^-1 D with unit-scaled diagonal */
+
 typedef struct sdpab_batch_init {
-  const int* flag;             /* [count] nonzero: start from the given point */
+  const int* flag;             /* [count] SDPAB_INIT_* per instance */
   const double* xvec;          /* x (vec_off layout), as SDPA::inputInitXVec */
   const double* X;             /* user X (dense_off layout), as inputInitXMat */
   const double* Y;             /* user Y (dense_off layout), as inputInitYMat */
+  double init_margin;          /* SDPAB_INIT_DUAL interiority margin (0 = 0.02) */
 } sdpab_batch_init;
 
 typedef struct sdpab_batch_result {

@@ -33,7 +33,13 @@ class Batch(ctypes.Structure):
 
 
 class BatchInit(ctypes.Structure):
-    _fields_ = [("flag", c_void_p), ("xvec", c_void_p), ("X", c_void_p), ("Y", c_void_p)]
+    _fields_ = [("flag", c_void_p), ("xvec", c_void_p), ("X", c_void_p), ("Y", c_void_p),
+                ("init_margin", c_double)]
+
+
+class GraphBatch(ctypes.Structure):
+    _fields_ = [("num_nodes", c_int), ("num_edges", c_longlong), ("rowptr", c_void_p), ("col", c_void_p),
+                ("aval", c_void_p), ("aval_t", c_void_p), ("feat", c_void_p), ("mask_count", c_int)]
 
 
 class BatchResult(ctypes.Structure):
@@ -67,6 +73,15 @@ SIGNATURES = [
     ("sdpab_batch_solve_noalloc", c_int, [POINTER(Batch), POINTER(BatchInit), POINTER(Params),
                                           POINTER(BatchResult), c_void_p, c_void_p]),
     ("sdpab_workspace_bytes", c_longlong, []),
+    ("sdpab_mpnn_num_params", c_longlong, []),
+    ("sdpab_mpnn_act_floats", c_longlong, [c_int]),
+    ("sdpab_mpnn_scratch_floats", c_longlong, [c_int]),
+    ("sdpab_mpnn_forward", c_int, [POINTER(GraphBatch), c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sdpab_mpnn_loss_grad", c_int, [POINTER(GraphBatch), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p]),
+    ("sdpab_mpnn_adam", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, ctypes.c_float,
+                                ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_void_p]),
+    ("sdpab_mpnn_to_bf16", c_int, [c_void_p, c_void_p, c_void_p]),
     ("sdpab_sdpa_new", c_void_p, []),
     ("sdpab_sdpa_free", None, [c_void_p]),
     ("sdpab_sdpa_set_params", c_int, [c_void_p, POINTER(Params)]),

@@ -143,10 +143,11 @@ def solve_host(P: Packed, params=None, precision=N.PREC_FP64, want_x=True, want_
     bi = None
     keep = []
     if init is not None:
-        flag, xv, Xu, Yu = (np.ascontiguousarray(init[0], np.int32), np.ascontiguousarray(init[1], np.float64),
-                            np.ascontiguousarray(init[2], np.float64), np.ascontiguousarray(init[3], np.float64))
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        flag, xv, Xu, Yu = np.ascontiguousarray(init[0], np.int32), conv(init[1]), conv(init[2]), conv(init[3])
+        margin = float(init[4]) if len(init) > 4 else 0.0
         keep = [flag, xv, Xu, Yu]
-        bi = ctypes.byref(N.BatchInit(_ptr(flag), _ptr(xv), _ptr(Xu), _ptr(Yu)))
+        bi = ctypes.byref(N.BatchInit(_ptr(flag), _ptr(xv), _ptr(Xu), _ptr(Yu), margin))
     prm = _params(params)
     cfg = _config(precision, ctas_per_sm)
     N.check(L.sdpab_batch_solve_host(ctypes.byref(bt), bi, ctypes.byref(prm), ctypes.byref(cfg),
@@ -184,14 +185,13 @@ class DeviceBatch:
                                  dp(self.Y) if want_mats else None,
                                  *[dp(self.sc[q]) for q in range(5)], *[dp(self.ic[q]) for q in range(3)])
 
-    def set_init(self, flag, xvec, X, Y):
+    def set_init(self, flag, xvec, X=None, Y=None, margin: float = 0.0):
+        """Device copies of an initial point (X, Y may be None for SDPAB_INIT_DUAL)."""
         import torch
         dev = self.xvec.device
-        self._init_t = [torch.as_tensor(np.ascontiguousarray(flag, np.int32), device=dev),
-                        torch.as_tensor(np.ascontiguousarray(xvec, np.float64), device=dev),
-                        torch.as_tensor(np.ascontiguousarray(X, np.float64), device=dev),
-                        torch.as_tensor(np.ascontiguousarray(Y, np.float64), device=dev)]
-        self.init = N.BatchInit(*[x.data_ptr() for x in self._init_t])
+        conv = lambda a, t: None if a is None else torch.as_tensor(np.ascontiguousarray(a, t), device=dev)
+        self._init_t = [conv(flag, np.int32), conv(xvec, np.float64), conv(X, np.float64), conv(Y, np.float64)]
+        self.init = N.BatchInit(*[None if x is None else x.data_ptr() for x in self._init_t], margin)
 
     def solve(self, params=None, precision=N.PREC_FP64, stream=None, ctas_per_sm=0):
         import torch

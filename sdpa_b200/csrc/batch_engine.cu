@@ -225,9 +225,11 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
     }
 
     // ---------------- initial point
-    bool warm = a.init.flag && a.init.flag[inst];
+    const int wmode = a.init.flag ? a.init.flag[inst] : SDPAB_INIT_NONE;
+    bool warm = false;
     int status = 0;
-    if (warm) {
+    if (wmode == SDPAB_INIT_POINT) {
+      warm = true;
       const double* Xu = a.init.X + a.p.dense_off[inst];
       const double* Yu = a.init.Y + a.p.dense_off[inst];
       const double* xv = a.init.xvec + a.p.vec_off[inst];
@@ -244,6 +246,73 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         cta::tri_inverse<NT>(n, W1, n, LZi, n, sD, gsm);
         cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
+    } else if (wmode == SDPAB_INIT_DUAL) {
+      // Proposed x only.  Applicable when the constraints are X_ii = b_i
+      // (F_i = e_i e_i^T, m = n, b > 0): then sum_i F_i = I, so shifting x by
+      // s adds s I to X = sum F_i x_i - F0, and Y = D X^{-1} D with
+      // D_ii = sqrt(b_i / (X^{-1})_ii) satisfies the constraints exactly.
+      int bad = (m != n);
+      for (int k = tid; k < m && !bad; k += NT) {
+        if (mp[k + 2] - mp[k + 1] != 1) { bad = 1; break; }
+        const long long e = mp[k + 1];
+        if (er[e] != ec[e] || ev[e] != 1.0 || !(bv[k] > 0.0)) bad = 1;
+      }
+      // every diagonal position covered exactly once
+      for (int t = tid; t < n; t += NT) W1[t] = 0.0;
+      __syncthreads();
+      for (int k = tid; k < m && !bad; k += NT) atomicAdd(&W1[er[mp[k + 1]]], 1.0);
+      __syncthreads();
+      for (int t = tid; t < n && !bad; t += NT) bad |= (W1[t] != 1.0);
+      bad = __syncthreads_or(bad);
+      if (!bad) {
+        const double* xv = a.init.xvec + a.p.vec_off[inst];
+        for (int k = tid; k < m; k += NT) vy[k] = -xv[k];
+        for (int t = tid; t < nn_i; t += NT) Z[t] = 0.0;
+        __syncthreads();
+        sp_axpy_block(er, ec, ev, mp[0], mp[1], -1.0, Z, n);  // C = -F0
+        __syncthreads();
+        double cs = 0.0;
+        for (int t = tid; t < n; t += NT) cs += fabs(Z[t + (size_t)n * t]);
+        cs = cta::block_sum<NT>(cs, RD) / n;
+        const double margin = ((a.init.init_margin > 0.0) ? a.init.init_margin : 0.02) * ((cs > 0.0) ? cs : 1.0);
+        sp_axpy_constraints(er, ec, ev, mp, m, vy, -1.0, Z, n);  // Z = C - sum y_k A_k
+        __syncthreads();
+        double lmin;
+        if (n > 20) lmin = lanczos_min_eig(n, Z, es);
+        else lmin = dense_min_eig(n, Z, es);
+        double shift = (lmin < margin) ? margin - lmin : 0.0;
+        int ok = 0;
+        for (int attempt = 0; attempt < 8 && !ok; ++attempt) {
+          for (int t = tid; t < nn_i; t += NT) W1[t] = Z[t] + (((t % n) == (t / n)) ? shift : 0.0);
+          __syncthreads();
+          if (cta::cholesky<NT>(n, W1, n, false, sD, gsm, &s_flag) == 0) ok = 1;
+          else shift = 2.0 * shift + margin;
+        }
+        if (ok) {
+          for (int k = tid; k < m; k += NT) vy[k] -= shift;
+          for (int t = tid; t < nn_i; t += NT) if ((t % n) == (t / n)) Z[t] += shift;
+          cta::tri_inverse<NT>(n, W1, n, LZi, n, sD, gsm);
+          cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
+          // X = D Z^-1 D with X_kk = b_k
+          for (int t = tid; t < n; t += NT) {
+            const int r = er[mp[t + 1]];
+            W1[r] = sqrt(bv[t] / Zi[r + (size_t)n * r]);
+          }
+          __syncthreads();
+          for (int t = tid; t < nn_i; t += NT) {
+            const int i = t % n, j = t / n;
+            X[t] = W1[i] * Zi[t] * W1[j];
+          }
+          __syncthreads();
+          for (int t = tid; t < nn_i; t += NT) W2[t] = X[t];
+          __syncthreads();
+          if (cta::cholesky<NT>(n, W2, n, false, sD, gsm, &s_flag) == 0) {
+            cta::tri_inverse<NT>(n, W2, n, LXi, n, sD, gsm);
+            warm = true;
+          }
+        }
+      }
+      if (!warm) status = 1;
     }
     if (!warm) {
       for (int t = tid; t < nn_i; t += NT) {

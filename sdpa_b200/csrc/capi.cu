@@ -166,6 +166,7 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
 {
   if (!hp || !prm || !hr || hp->count < 0) return set_error(SDPAB_EINVAL, "batch_solve_host: null argument");
   const int N = hp->count;
+  const bool want_init = hinit && hinit->flag;
   if (N == 0) return SDPAB_OK;
   if (!hp->n || !hp->m || !hp->vec_off || !hp->b || !hp->mat_off || !hp->mat_ptr || !hp->row ||
       !hp->col || !hp->val || !hp->dense_off || !hr->primal_obj || !hr->dual_obj || !hr->mu ||
@@ -184,6 +185,13 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
     nent = std::max(nent, hp->mat_ptr[hp->mat_off[i] + m + 1]);
     nden = std::max(nden, hp->dense_off[i] + (long long)n * n);
   }
+  if (want_init) {
+    bool need_xy = false;
+    for (int i = 0; i < N; ++i) need_xy |= (hinit->flag[i] == SDPAB_INIT_POINT);
+    if (!hinit->xvec) return set_error(SDPAB_EINVAL, "batch_solve_host: init xvec is NULL");
+    if (need_xy && (!hinit->X || !hinit->Y))
+      return set_error(SDPAB_EINVAL, "batch_solve_host: SDPAB_INIT_POINT needs init X and Y");
+  }
   std::vector<int> order(N);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(),
@@ -194,7 +202,6 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
   std::lock_guard<std::mutex> lk(g_stage_mu);
   Staging& S = g_stage[(dev >= 0 && dev < kMaxDevices) ? dev : 0];
   cudaStream_t st = 0;
-  const bool want_init = hinit && hinit->flag;
   struct Copy { int slot; const void* src; size_t bytes; };
   const Copy in[] = {
       {0, hp->n, N * sizeof(int)},          {1, hp->m, N * sizeof(int)},
@@ -246,6 +253,7 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
   sdpab_batch_init di;
   memset(&di, 0, sizeof(di));
   if (want_init) {
+    di.init_margin = hinit->init_margin;
     di.flag = (const int*)d[11];
     di.xvec = (const double*)d[12];
     di.X = (const double*)d[13];
