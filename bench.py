@@ -165,15 +165,47 @@ def run_reference(args):
     return 0
 
 
+def _events_time(fn, stream, steps, flush):
+    """Device time (ms) of fn() per step, CUDA events on `stream`, L2 flushed
+    (256 MB written) before every step."""
+    import torch
+    times = []
+    for _ in range(steps):
+        flush.add_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def _capture(fn, stream):
+    """CUDA graph of fn() on `stream` (None if capture is not possible)."""
+    import torch
+    try:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
+            fn()
+        return g
+    except Exception as e:  # capture unsupported: run eagerly
+        print(f"graph capture failed ({e}); timing eager launches", file=sys.stderr)
+        return None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--warm", type=int, default=1, help="learned warm start (1) or standard start (0)")
     ap.add_argument("--count", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -181,7 +213,8 @@ def main():
     import torch
     import torch.distributed as dist
     from sdpa_b200 import _native as N
-    from sdpa_b200 import batch
+    from sdpa_b200 import autotune, batch
+    from sdpa_b200 import warmstart as W
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -192,87 +225,156 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     prec = N.PREC_FP64 if args.precision == "fp64" else N.PREC_MIXED
 
-    insts, P = make_batch(args.count, rank * args.count)
-    db = batch.DeviceBatch(P)
+    seed0 = rank * args.count
+    graphs = [W.batch_graph(s, 20, 120) for s in range(seed0, seed0 + args.count)]
+    insts = [g.instance() for g in graphs]
+    P = batch.pack(insts)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
 
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        db.solve(precision=prec)
+    # ---- plain FP64 path (standard start): the denominator of the headline ratio
+    db0 = batch.DeviceBatch(P)
+    tune0 = autotune.tune(db0, N.PREC_FP64, stream=stream)
+    c0 = tune0["best"]
+    run0 = lambda: db0.solve(precision=N.PREC_FP64, stream=stream, ctas_per_sm=c0)
+    # ---- headline path: precision + learned warm start
+    dbh = batch.DeviceBatch(P)
+    pipe = W.WarmPipeline(W.default_model(), graphs, dbh) if args.warm else None
+    tuneh = autotune.tune(dbh, prec, stream=stream,
+                          run=(lambda c: pipe.run(precision=prec, stream=stream, ctas_per_sm=c)) if pipe else None)
+    ch = tuneh["best"]
+    if pipe is not None:
+        runh = lambda: pipe.run(precision=prec, stream=stream, ctas_per_sm=ch)
+    else:
+        runh = lambda: dbh.solve(precision=prec, stream=stream, ctas_per_sm=ch)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            run0()
+            runh()
     barrier()
-    times = []
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.add_(1.0)  # write 256 MB (> 126 MB L2) between timed steps
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            db.solve(precision=prec, stream=stream)
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
+    g0 = gh = None
+    if not args.no_graph:
+        g0 = _capture(run0, stream)
+        gh = _capture(runh, stream)
+    step0 = (lambda: g0.replay()) if g0 is not None else run0
+    steph = (lambda: gh.replay()) if gh is not None else runh
+    with torch.cuda.stream(stream):
+        step0()
+        steph()
+    barrier()
+
+    with torch.cuda.stream(stream):
+        t_plain = _events_time(step0, stream, args.steps, flush)
         barrier()
-    res = db.result()
+        with ClockSampler(local) as clk:
+            times = _events_time(steph, stream, args.steps, flush)
+        barrier()
+    # the other precision of the warm-started pipeline, same batch, same timing
+    alt = None
+    if pipe is not None:
+        aprec = N.PREC_FP64 if prec == N.PREC_MIXED else N.PREC_MIXED
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                pipe.run(precision=aprec, stream=stream, ctas_per_sm=ch)
+            ta = _events_time(lambda: pipe.run(precision=aprec, stream=stream, ctas_per_sm=ch), stream,
+                              args.steps, flush)
+        barrier()
+        ra = dbh.result()
+        alt = {"precision": "fp64" if aprec == N.PREC_FP64 else "mixed", "warm_start": True,
+               "value": args.count / (float(np.mean(ta)) / 1e3), "unit": "SDPs/s (this GPU)",
+               "ms_per_step": float(np.mean(ta)), "mean_iterations": float(ra.iterations.mean()),
+               "pdOPT": int(np.sum(ra.phase == 7)), "retried_in_fp64": int(np.sum(ra.status == 2))}
+        with torch.cuda.stream(stream):
+            steph()
+        barrier()
+    res = dbh.result()
+    res0 = db0.result()
     step_ms = float(np.mean(times))
-    t = torch.tensor([step_ms], device="cuda")
+    plain_ms = float(np.mean(t_plain))
+    t = torch.tensor([step_ms, plain_ms], device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms_max = float(t.item())
+    step_ms_max, plain_ms_max = float(t[0].item()), float(t[1].item())
     total = args.count * world
     value = total / (step_ms_max / 1e3)
+    plain_value = total / (plain_ms_max / 1e3)
 
-    # e2e through the host-pointer C ABI: H2D of the packed batch and D2H of
-    # the per-instance results inside the timed region, pinned host buffers.
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    import copy
-    Ph = copy.copy(P)
-    for k in ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col", "val", "dense_off"):
-        setattr(Ph, k, pin(getattr(P, k)))
-    batch.solve_host(Ph, precision=prec)
-    barrier()
+    # ---- e2e: host (pinned) inputs -> device, the same pipeline, results -> host
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    pairs = [(dbh.d[k], pin(getattr(P, k))) for k in dbh.d]
+    pairs.append((dbh.order, pin(dbh.order.cpu().numpy())))
+    if pipe is not None:
+        gb = pipe.dg.gb
+        pairs += [(pipe.dg.rowptr, pin(gb.rowptr)), (pipe.dg.col, pin(gb.col)), (pipe.dg.aval, pin(gb.aval)),
+                  (pipe.dg.aval_t, pin(gb.aval_t)), (pipe.dg.feat, pin(gb.feat)),
+                  (pipe.degree, pin(pipe.degree.cpu().numpy())), (pipe.fallback, pin(pipe.fallback.cpu().numpy()))]
+    h2d = sum(h.numel() * h.element_size() for _, h in pairs)
+    out_sc = torch.empty_like(dbh.sc, device="cpu").pin_memory()
+    out_ic = torch.empty_like(dbh.ic, device="cpu").pin_memory()
+    out_x = torch.empty_like(dbh.xvec, device="cpu").pin_memory()
+    d2h = out_sc.numel() * 8 + out_ic.numel() * 4 + out_x.numel() * 8
     e2e_t = []
     for _ in range(max(1, min(args.steps, 3))):
         flush.add_(1.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hr = batch.solve_host(Ph, precision=prec)
+        with torch.cuda.stream(stream):
+            for dev, host in pairs:
+                dev.copy_(host, non_blocking=True)
+            steph()
+            out_sc.copy_(dbh.sc, non_blocking=True)
+            out_ic.copy_(dbh.ic, non_blocking=True)
+            out_x.copy_(dbh.xvec, non_blocking=True)
+        stream.synchronize()
         e2e_t.append(time.perf_counter() - t0)
     barrier()
-    e2e_s = float(np.mean(e2e_t))
-    t = torch.tensor([e2e_s], device="cuda")
+    t = torch.tensor([float(np.mean(e2e_t))], device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_val = total / float(t.item())
-    d2h = hr.xvec.nbytes + 5 * 8 * P.count + 3 * 4 * P.count
 
-    # parity summary of this run
+    # ---- parity of this run (headline vs plain FP64) and roofline
     ok = int(np.sum(res.phase == 7))
+    relobj = np.abs(res.primal_obj - res0.primal_obj) / np.maximum(1.0, np.abs(res0.primal_obj))
+    xdiff = np.array([np.max(np.abs(res.x_of(P, q) - res0.x_of(P, q))) for q in range(P.count)])
     flops = sum(float(res.iterations[q]) * iter_flops(int(P.n[q]), int(P.m[q])) for q in range(P.count))
     hbm, bf16, src = peaks()
     achieved = flops / (step_ms / 1e3) / 1e12
+    launches_per_step = 9 if pipe is not None else 1  # 7 network + 1 proposal + 1 solver
     line = {"metric": METRIC, "value": value, "unit": "SDPs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == N.PREC_FP64 else "f32+f64",
             "data": "synthetic (seeded generator, no public suite)",
             "config": {"workload": WORKLOAD, "count_per_gpu": args.count, "precision": args.precision,
-                       "warm_start": False, "l2": "256 MB buffer written between timed steps",
+                       "warm_start": bool(args.warm), "cuda_graph": gh is not None,
+                       "ctas_per_sm": {"headline": ch, "plain_fp64": c0, "autotune_ms": tuneh["ms"]},
+                       "l2": "256 MB buffer written between timed steps",
                        "parallelism": f"replicas x{world} (independent instances per GPU)"},
-            "e2e": {"value": e2e_val, "unit": "SDPs/s", "h2d_bytes_per_step": int(P.h2d_bytes()),
-                    "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": args.steps,
+            "plain_fp64": {"value": plain_value, "unit": "SDPs/s", "ms_per_step": plain_ms_max,
+                           "mean_iterations": float(res0.iterations.mean()),
+                           "pdOPT": int(np.sum(res0.phase == 7))},
+            "speedup_vs_plain_fp64": value / plain_value,
+            "warm_other_precision": alt,
+            "e2e": {"value": e2e_val, "unit": "SDPs/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": args.steps * launches_per_step,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
                          "frac": achieved / bf16, "traffic": None,
                          "peak_source": f"{src} bf16 dense (MEASURED_PEAKS.json); the kernel computes "
-                                        "in FP64 on the SIMT pipe",
+                                        "on the FP64/FP32 SIMT pipes",
                          "fp64_nominal_tflops": 40.0, "frac_of_fp64_nominal": achieved / 40.0,
                          "flops_per_launch": flops, "kernel": "batch_ipm_fp64"},
             "clocks": clk.summary(),
-            "parity": {"pdOPT": ok, "count": int(P.count), "mean_iterations": float(res.iterations.mean())}}
+            "parity": {"pdOPT": ok, "count": int(P.count), "mean_iterations": float(res.iterations.mean()),
+                       "retried_in_fp64": int(np.sum(res.status == 2)),
+                       "max_rel_objective_diff_vs_plain_fp64": float(relobj.max()),
+                       "max_abs_x_diff_vs_plain_fp64": float(xdiff.max()),
+                       "x_diff_above_1e-5": int(np.sum(xdiff > 1e-5))}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         sample = min(args.count, max(64, 48 * cores))
@@ -280,6 +382,7 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": "SDPs/s", "cores": cores, "kind": "reference",
                                 "sample": f"first {sample} instances of this batch, one single-threaded "
                                           f"reference process per core; {det}"}
+    del g0, gh
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -121,10 +121,20 @@ SDPAB_API int sdpab_sdpa_input_problem(sdpab_sdpa* h, int m, int nblock, const i
  * block, a vector per LP block */
 SDPAB_API int sdpab_sdpa_set_init(sdpab_sdpa* h, const double* xvec, const double* const* X,
                                   const double* const* Y);
+/* Precision of the solve (no reference counterpart): SDPAB_PREC_FP64, or
+ * SDPAB_PREC_MIXED = FP32 products and FP32 Schur Cholesky with FP64
+ * iterative refinement of dy while the relative complementarity gap
+ * nDim * mu / max(1, (|objP| + |objD|) / 2) >= mu_switch (0 = 1e-2), FP64
+ * after. */
+SDPAB_API int sdpab_sdpa_set_precision(sdpab_sdpa* h, int mode, double mu_switch);
 /* SDPA::initializeSolve + SDPA::solve (sdpa_solve.cpp:10-43, :59-233) */
 SDPAB_API int sdpab_sdpa_solve(sdpab_sdpa* h);
 /* scalar getters (sdpa_call.cpp:719-847) */
 SDPAB_API int sdpab_sdpa_info(sdpab_sdpa* h, sdpab_sdpa_info_t* out);
+/* Device seconds per solver phase (the reference's ComputeTime categories,
+ * sdpa_parts.h:48-86): out8 = rMat+gVec, bMat, Cholesky, solves, dX/dZ,
+ * step length, update (inverses), residuals. */
+SDPAB_API int sdpab_sdpa_phase_times(sdpab_sdpa* h, double* out8);
 /* getResultXVec (sdpa_call.cpp:668-671), copied into out[m] */
 SDPAB_API int sdpab_sdpa_get_xvec(sdpab_sdpa* h, double* out);
 /* getResultXMat (which = 0) / getResultYMat (which = 1) of block l
@@ -178,14 +188,21 @@ SDPAB_API int sdpab_mpnn_adam(float* master, unsigned short* weights_bf16, const
                               float* m2, int step, float lr, float beta1, float beta2, float eps,
                               float weight_decay, void* stream);
 SDPAB_API int sdpab_mpnn_to_bf16(const float* master, unsigned short* weights_bf16, void* stream);
+/* proposed SDPA x vector from the network output: x_i = r_i d_i / 4 for nodes
+ * with edges, fallback_i for isolated nodes (node order = packed batch order) */
+SDPAB_API int sdpab_mpnn_propose_x(int num_nodes, const float* r, const double* degree, const double* fallback,
+                                   double* xvec, void* stream);
 
 /* ---------------------------------------------------------------- batched API */
 
 /* Precision modes of the batched solver. */
 #define SDPAB_PREC_FP64 0    /* every step in FP64 (the plain path) */
-#define SDPAB_PREC_MIXED 1   /* FP32 bulk products and Schur factorisation with
-                                FP64 refinement, FP64 residuals/gap/step length,
-                                FP64 everywhere once mu < mixed_mu_switch */
+#define SDPAB_PREC_MIXED 1   /* while nDim * mu / max(1, mean |objective|) >=
+                                mixed_switch_gap: bulk products in FP32 (FP32 accumulation), and in
+                                the host-driven solver the Schur Cholesky in FP32 with
+                                FP64 refinement of dy; FP64 residuals, gap, Lanczos step
+                                length and factorisations of X and Z; everything FP64
+                                once mu falls below that point */
 
 typedef struct sdpab_batch {
   int count;                   /* number of instances */
@@ -230,14 +247,18 @@ typedef struct sdpab_batch_result {
   double* dual_error;          /* [count] getDualError */
   int* iterations;             /* [count] getIteration */
   int* phase;                  /* [count] getPhaseValue code */
-  int* status;                 /* [count] 0 ok; 1 warm start not strictly interior
-                                  (standard start used); <0 instance rejected */
+  int* status;                 /* [count] 0 ok; 1 warm start not usable (standard start
+                                  used); 2 warm-started or mixed-precision solve ended
+                                  outside pdOPT and was solved again from the standard
+                                  start in FP64 (iterations count both attempts);
+                                  <0 instance rejected */
 } sdpab_batch_result;
 
 typedef struct sdpab_batch_config {
   int precision;               /* SDPAB_PREC_FP64 or SDPAB_PREC_MIXED */
   int ctas_per_sm;             /* resident solver blocks per SM (0 = auto) */
-  double mixed_mu_switch;      /* mixed mode: switch to FP64 below this mu (0 = 1e-6) */
+  double mixed_switch_gap;     /* mixed mode: FP64 once nDim * mu / max(1, mean
+                                  |objective|) < this (0 = 1e-2) */
 } sdpab_batch_config;
 
 /* Solves a batch whose arrays (problem, init, result) are all DEVICE pointers,

@@ -28,6 +28,7 @@
 
 namespace sdpab {
 struct SdpaImpl;
+struct SolveStats;
 }
 
 class SDPAB_CLASS_API SDPA {
@@ -137,9 +138,16 @@ class SDPAB_CLASS_API SDPA {
   void copyCurrentToInit();
   void setKappa(double KAPPA);
 
+  // not in the reference: precision mode (0 = FP64, 1 = mixed: FP32 bulk
+  // products and FP32 Schur factor with FP64 refinement while the relative
+  // complementarity gap n*mu / max(1, mean |objective|) >= mu_switch;
+  // 0 = default 1e-2)
+  void setPrecision(int mode, double mu_switch = 0.0);
   // not in the reference: the error channel that replaces its exit() calls
   int getErrorCode();
   const char* getErrorMessage();
+  // not in the reference: per-phase solver statistics (device seconds)
+  const sdpab::SolveStats& impl_solver_stats();
 
  private:
   sdpab::SdpaImpl* impl_;

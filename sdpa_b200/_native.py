@@ -50,7 +50,7 @@ class BatchResult(ctypes.Structure):
 
 
 class BatchConfig(ctypes.Structure):
-    _fields_ = [("precision", c_int), ("ctas_per_sm", c_int), ("mixed_mu_switch", c_double)]
+    _fields_ = [("precision", c_int), ("ctas_per_sm", c_int), ("mixed_switch_gap", c_double)]
 
 
 class SdpaInfo(ctypes.Structure):
@@ -82,6 +82,7 @@ SIGNATURES = [
     ("sdpab_mpnn_adam", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, ctypes.c_float,
                                 ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_void_p]),
     ("sdpab_mpnn_to_bf16", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("sdpab_mpnn_propose_x", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sdpab_sdpa_new", c_void_p, []),
     ("sdpab_sdpa_free", None, [c_void_p]),
     ("sdpab_sdpa_set_params", c_int, [c_void_p, POINTER(Params)]),
@@ -91,8 +92,10 @@ SIGNATURES = [
     ("sdpab_sdpa_input_problem", c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_longlong, c_void_p,
                                          c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sdpab_sdpa_set_init", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sdpab_sdpa_set_precision", c_int, [c_void_p, c_int, c_double]),
     ("sdpab_sdpa_solve", c_int, [c_void_p]),
     ("sdpab_sdpa_info", c_int, [c_void_p, POINTER(SdpaInfo)]),
+    ("sdpab_sdpa_phase_times", c_int, [c_void_p, c_void_p]),
     ("sdpab_sdpa_get_xvec", c_int, [c_void_p, c_void_p]),
     ("sdpab_sdpa_get_block", c_int, [c_void_p, c_int, c_int, c_void_p]),
     ("sdpab_sdpa_block_size", c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),

@@ -118,8 +118,8 @@ def _params(params):
     return p
 
 
-def _config(precision=N.PREC_FP64, ctas_per_sm=0, mixed_mu_switch=0.0):
-    return N.BatchConfig(precision, ctas_per_sm, mixed_mu_switch)
+def _config(precision=N.PREC_FP64, ctas_per_sm=0, mixed_switch_gap=0.0):
+    return N.BatchConfig(precision, ctas_per_sm, mixed_switch_gap)
 
 
 def solve_host(P: Packed, params=None, precision=N.PREC_FP64, want_x=True, want_mats=False,

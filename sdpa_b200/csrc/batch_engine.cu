@@ -45,6 +45,8 @@ struct BatchArgs {
   sdpab_batch_result r;
   Params prm;
   const int* order;
+  int mixed;             // SDPAB_PREC_MIXED: bulk GEMMs in FP32 while mixed_gap >= mu_switch
+  double mu_switch;
   double* ws;
   long long ws_stride;  // doubles per block
   int* queue;
@@ -217,6 +219,10 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         continue;
       }
     }
+    // all constraint entries on the diagonal?
+    int offdiag = 0;
+    for (long long e = mp[1] + tid; e < mp[m + 1]; e += NT) offdiag |= (er[e] != ec[e]);
+    const bool diag_cons = !__syncthreads_or(offdiag);
     // NonZeroEffect per constraint (diagonal 1, off-diagonal 2; sdpa_struct.cpp:1339-1341)
     for (int k = tid; k < m; k += NT) {
       int c = 0;
@@ -224,10 +230,44 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       s_nnz[k] = c;
     }
 
+    // A warm-started or mixed-precision solve that ends outside pdOPT is
+    // solved again from the standard start in FP64 (status 2); iterations
+    // count both attempts.
+    int status = 0, iter_total = 0;
+    double nrp, nrd;
+    // residuals: r_p = b - A.X, D = C - Z - sum y_k A_k (Residuals::compute)
+    auto residuals = [&](double& nrp, double& nrd) {
+      double mx = 0.0;
+      for (int k = tid; k < m; k += NT) {
+        double r = bv[k] - sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], X, n);
+        vrp[k] = r;
+        mx = fmax(mx, fabs(r));
+      }
+      nrp = cta::block_max<NT>(mx, RD);
+      for (int t = tid; t < nn_i; t += NT) D[t] = -Z[t];
+      __syncthreads();
+      sp_axpy_block(er, ec, ev, mp[0], mp[1], -1.0, D, n);  // C = -F0
+      sp_axpy_constraints(er, ec, ev, mp, m, vy, -1.0, D, n);
+      __syncthreads();
+      mx = 0.0;
+      for (int t = tid; t < nn_i; t += NT) mx = fmax(mx, fabs(D[t]));
+      nrd = cta::block_max<NT>(mx, RD);
+    };
+    // C . W with C = -F0
+    auto c_dot = [&](const double* W) {
+      double s = 0.0;
+      for (long long e = mp[0] + tid; e < mp[1]; e += NT) {
+        int r = er[e], c = ec[e];
+        double v = -ev[e];
+        s += (r == c) ? v * W[r + (size_t)n * r] : v * (W[r + (size_t)n * c] + W[c + (size_t)n * r]);
+      }
+      return cta::block_sum<NT>(s, RD);
+    };
+
+    for (int attempt = 0; attempt < 2; ++attempt) {
     // ---------------- initial point
-    const int wmode = a.init.flag ? a.init.flag[inst] : SDPAB_INIT_NONE;
+    const int wmode = (attempt == 0 && a.init.flag) ? a.init.flag[inst] : SDPAB_INIT_NONE;
     bool warm = false;
-    int status = 0;
     if (wmode == SDPAB_INIT_POINT) {
       warm = true;
       const double* Xu = a.init.X + a.p.dense_off[inst];
@@ -238,12 +278,12 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       __syncthreads();
       // strict interiority check (the reference ignores computeInverse's
       // failure here, sdpa_solve.cpp:63; this solver falls back instead)
-      int fx = cta::cholesky<NT>(n, W2, n, false, sD, gsm, &s_flag);
-      int fz = fx ? 1 : cta::cholesky<NT>(n, W1, n, false, sD, gsm, &s_flag);
+      int fx = cta::cholesky<NT, double>(n, W2, n, false, sD, gsm, &s_flag);
+      int fz = fx ? 1 : cta::cholesky<NT, double>(n, W1, n, false, sD, gsm, &s_flag);
       if (fx || fz) { warm = false; status = 1; }
       else {
-        cta::tri_inverse<NT>(n, W2, n, LXi, n, sD, gsm);
-        cta::tri_inverse<NT>(n, W1, n, LZi, n, sD, gsm);
+        cta::tri_inverse<NT, double>(n, W2, n, LXi, n, sD, gsm);
+        cta::tri_inverse<NT, double>(n, W1, n, LZi, n, sD, gsm);
         cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
     } else if (wmode == SDPAB_INIT_DUAL) {
@@ -285,13 +325,13 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         for (int attempt = 0; attempt < 8 && !ok; ++attempt) {
           for (int t = tid; t < nn_i; t += NT) W1[t] = Z[t] + (((t % n) == (t / n)) ? shift : 0.0);
           __syncthreads();
-          if (cta::cholesky<NT>(n, W1, n, false, sD, gsm, &s_flag) == 0) ok = 1;
+          if (cta::cholesky<NT, double>(n, W1, n, false, sD, gsm, &s_flag) == 0) ok = 1;
           else shift = 2.0 * shift + margin;
         }
         if (ok) {
           for (int k = tid; k < m; k += NT) vy[k] -= shift;
           for (int t = tid; t < nn_i; t += NT) if ((t % n) == (t / n)) Z[t] += shift;
-          cta::tri_inverse<NT>(n, W1, n, LZi, n, sD, gsm);
+          cta::tri_inverse<NT, double>(n, W1, n, LZi, n, sD, gsm);
           cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
           // X = D Z^-1 D with X_kk = b_k
           for (int t = tid; t < n; t += NT) {
@@ -306,8 +346,8 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
           __syncthreads();
           for (int t = tid; t < nn_i; t += NT) W2[t] = X[t];
           __syncthreads();
-          if (cta::cholesky<NT>(n, W2, n, false, sD, gsm, &s_flag) == 0) {
-            cta::tri_inverse<NT>(n, W2, n, LXi, n, sD, gsm);
+          if (cta::cholesky<NT, double>(n, W2, n, false, sD, gsm, &s_flag) == 0) {
+            cta::tri_inverse<NT, double>(n, W2, n, LXi, n, sD, gsm);
             warm = true;
           }
         }
@@ -331,36 +371,6 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       __syncthreads();
     }
 
-    // residuals: r_p = b - A.X, D = C - Z - sum y_k A_k (Residuals::compute)
-    auto residuals = [&](double& nrp, double& nrd) {
-      double mx = 0.0;
-      for (int k = tid; k < m; k += NT) {
-        double r = bv[k] - sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], X, n);
-        vrp[k] = r;
-        mx = fmax(mx, fabs(r));
-      }
-      nrp = cta::block_max<NT>(mx, RD);
-      for (int t = tid; t < nn_i; t += NT) D[t] = -Z[t];
-      __syncthreads();
-      sp_axpy_block(er, ec, ev, mp[0], mp[1], -1.0, D, n);  // C = -F0
-      sp_axpy_constraints(er, ec, ev, mp, m, vy, -1.0, D, n);
-      __syncthreads();
-      mx = 0.0;
-      for (int t = tid; t < nn_i; t += NT) mx = fmax(mx, fabs(D[t]));
-      nrd = cta::block_max<NT>(mx, RD);
-    };
-    // C . W with C = -F0
-    auto c_dot = [&](const double* W) {
-      double s = 0.0;
-      for (long long e = mp[0] + tid; e < mp[1]; e += NT) {
-        int r = er[e], c = ec[e];
-        double v = -ev[e];
-        s += (r == c) ? v * W[r + (size_t)n * r] : v * (W[r + (size_t)n * c] + W[c + (size_t)n * r]);
-      }
-      return cta::block_sum<NT>(s, RD);
-    };
-
-    double nrp, nrd;
     residuals(nrp, nrd);
     double mu0;
     if (warm) mu0 = cta::dot_mat<NT>(n, X, Z, RD) / n;
@@ -384,14 +394,20 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       __syncthreads();
       const bool dinf = dual_infeasible(S);
       const double bm = S.beta * S.mu;
+      // mixed precision: FP32 products while mu is above the switch point
+      const bool lowp = a.mixed && attempt == 0 && mixed_gap(S) >= a.mu_switch;
+      // every constraint diagonal and the point dual feasible: dZ is diagonal,
+      // so products with dZ are column scalings (exactly what the GEMM with a
+      // diagonal factor computes)
+      const bool dz_diag = diag_cons && !dinf;
 
       // ---- predictor: rMat and gVec (sdpa_newton.cpp:793-883)
       for (int t = tid; t < nn_i; t += NT) R[t] = bm * Zi[t] - X[t];
       __syncthreads();
       const double* G = R;
       if (dinf) {
-        cta::gemm<NT>(n, false, X, n, false, D, n, W1, n, 1.0, 0.0, gsm);
-        cta::gemm<NT>(n, false, W1, n, false, Zi, n, XDZ, n, 1.0, 0.0, gsm);
+        cta::gemm_prec<NT, double>(n, false, X, n, false, D, n, W1, n, 1.0, 0.0, gsm, lowp);
+        cta::gemm_prec<NT, double>(n, false, W1, n, false, Zi, n, XDZ, n, 1.0, 0.0, gsm, lowp);
         for (int t = tid; t < nn_i; t += NT) W2[t] = R[t] - XDZ[t];
         __syncthreads();
         G = W2;
@@ -408,10 +424,10 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       }
       __syncthreads();
       // ---- adjusted Cholesky and solve (compute_DyVec, sdpa_newton.cpp:2672-2716)
-      if (cta::cholesky<NT>(m, B, m, true, sD, gsm, &s_flag)) break;
+      if (cta::cholesky<NT, double>(m, B, m, true, sD, gsm, &s_flag)) break;
       for (int k = tid; k < m; k += NT) vdy[k] = vg[k];
       __syncthreads();
-      cta::chol_solve<NT>(m, B, m, vdy, sD);
+      cta::chol_solve<NT, double>(m, B, m, vdy, sD);
 
       // ---- dZ, dX (compute_DzMat / compute_DxMat, sdpa_newton.cpp:2718-2752)
       auto direction = [&]() {
@@ -419,8 +435,13 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         __syncthreads();
         sp_axpy_constraints(er, ec, ev, mp, m, vdy, -1.0, dZ, n);
         __syncthreads();
-        cta::gemm<NT>(n, false, X, n, false, dZ, n, W1, n, 1.0, 0.0, gsm);
-        cta::gemm<NT>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm);
+        if (dz_diag) {
+          for (int t = tid; t < nn_i; t += NT) W1[t] = X[t] * dZ[(t / n) * (n + 1)];
+          __syncthreads();
+        } else {
+          cta::gemm_prec<NT, double>(n, false, X, n, false, dZ, n, W1, n, 1.0, 0.0, gsm, lowp);
+        }
+        cta::gemm_prec<NT, double>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm, lowp);
         for (int t = tid; t < nn_i; t += NT) {
           const int i = t % n, j = t / n;
           if (i >= j) {
@@ -450,8 +471,13 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       // ---- corrector (Newton::Mehrotra(CORRECTOR))
       {
         const double bm2 = S.beta * S.mu;
-        cta::gemm<NT>(n, false, dX, n, false, dZ, n, W1, n, 1.0, 0.0, gsm);
-        cta::gemm<NT>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm);
+        if (dz_diag) {
+          for (int t = tid; t < nn_i; t += NT) W1[t] = dX[t] * dZ[(t / n) * (n + 1)];
+          __syncthreads();
+        } else {
+          cta::gemm_prec<NT, double>(n, false, dX, n, false, dZ, n, W1, n, 1.0, 0.0, gsm, lowp);
+        }
+        cta::gemm_prec<NT, double>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm, lowp);
         for (int t = tid; t < nn_i; t += NT) {
           double rr = bm2 * Zi[t] - X[t];
           rr = rr - W2[t];
@@ -461,7 +487,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         __syncthreads();
         for (int k = tid; k < m; k += NT) vdy[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], W1, n) + vrp[k];
         __syncthreads();
-        cta::chol_solve<NT>(m, B, m, vdy, sD);
+        cta::chol_solve<NT, double>(m, B, m, vdy, sD);
         direction();
       }
 
@@ -490,10 +516,10 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         for (int t = tid; t < nn_i; t += NT) { W2[t] = X[t]; W1[t] = Z[t]; }
         __syncthreads();
         if (cannot_move(S)) break;
-        if (cta::cholesky<NT>(n, W2, n, false, sD, gsm, &s_flag)) break;
-        cta::tri_inverse<NT>(n, W2, n, LXi, n, sD, gsm);
-        if (cta::cholesky<NT>(n, W1, n, false, sD, gsm, &s_flag)) break;
-        cta::tri_inverse<NT>(n, W1, n, LZi, n, sD, gsm);
+        if (cta::cholesky<NT, double>(n, W2, n, false, sD, gsm, &s_flag)) break;
+        cta::tri_inverse<NT, double>(n, W2, n, LXi, n, sD, gsm);
+        if (cta::cholesky<NT, double>(n, W1, n, false, sD, gsm, &s_flag)) break;
+        cta::tri_inverse<NT, double>(n, W1, n, LZi, n, sD, gsm);
         cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
       // ---- residuals and scalars
@@ -515,6 +541,14 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       }
       ++iter;
     }
+    iter_total += iter;
+    if (attempt == 0 && (warm || a.mixed) && S.phase != pdOPT) {
+      status = 2;
+      __syncthreads();
+      continue;
+    }
+    break;
+    }  // attempts
     // final residuals (sdpa_solve.cpp:204) and results
     residuals(nrp, nrd);
     if (tid == 0) {
@@ -523,7 +557,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       a.r.mu[inst] = S.mu;
       a.r.primal_error[inst] = nrd;
       a.r.dual_error[inst] = nrp;
-      a.r.iterations[inst] = iter;
+      a.r.iterations[inst] = iter_total;
       a.r.phase[inst] = user_phase(S.phase);
       a.r.status[inst] = status;
     }
@@ -597,6 +631,8 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.r = *res;
   memcpy(&a.prm, prm, sizeof(Params));
   a.order = order;
+  a.mixed = (cfg && cfg->precision == SDPAB_PREC_MIXED) ? 1 : 0;
+  a.mu_switch = (cfg && cfg->mixed_switch_gap > 0.0) ? cfg->mixed_switch_gap : 1.0e-2;
   a.ws = ws;
   a.ws_stride = stride;
   a.queue = queue;
@@ -679,6 +715,8 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.r = *res;
   memcpy(&a.prm, prm, sizeof(Params));
   a.order = order;
+  a.mixed = 0;
+  a.mu_switch = 1.0e-2;
   a.ws = base + head;
   a.ws_stride = stride;
   a.queue = queue;

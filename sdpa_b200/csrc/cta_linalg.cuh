@@ -85,27 +85,31 @@ __device__ double dot_vec(int n, const double* a, const double* b, Reducer& R)
 }
 
 // ------------------------------------------------------------ GEMM
-// C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C.
+// All GEMM / factorisation routines are templated on the matrix storage type
+// TM and the compute type TC (TC = float with TM = double is the mixed
+// precision path: operands are rounded to FP32 when staged in shared memory,
+// products accumulate in FP32, results are stored back in FP64).
+//
+// gemm_rect: C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C.
 // 64 x 64 output tiles, 256 threads as a 16 x 16 grid with 4 x 4 outputs each
-// (rows ty + 16 i, columns tx + 16 j), K staged in chunks of 32.
-// lower = true updates only entries with (row + diag_off >= col) and skips
-// tiles entirely above that diagonal (trailing updates of factorisations).
-// smem: 2 * 32 * 64 doubles.  Ends with a barrier.
+// (rows ty + 16 i, columns tx + 16 j), K staged in chunks of GK with the next
+// chunk prefetched into registers.  lower = true updates only entries with
+// (row + diag_off >= col) and skips tiles entirely above that diagonal
+// (trailing updates of factorisations).  smem: 2 * GK * GT elements of TC.
+// Ends with a barrier.
 constexpr int GT = 64, GK = 16;
-template <int NT>
-__device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const double* A, int lda, bool tB,
-                          const double* B, int ldb, double* C, int ldc, double alpha, double beta,
-                          double* smem, bool lower = false, int diag_off = 0)
+template <int NT, typename TM, typename TC>
+__device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const TM* A, int lda, bool tB,
+                                       const TM* B, int ldb, TM* C, int ldc, double alpha, double beta,
+                                       void* smem_v, bool lower = false, int diag_off = 0)
 {
   static_assert(NT == 256, "gemm tile mapping assumes 256 threads");
-  constexpr int PER = GK * GT / NT;  // staged elements per thread and operand (8)
-  double* As = smem;             // [GK][GT]  As[k*GT + r]
-  double* Bs = smem + GK * GT;   // [GK][GT]  Bs[k*GT + c]
+  constexpr int PER = GK * GT / NT;  // staged elements per thread and operand
+  TC* As = (TC*)smem_v;          // [GK][GT]  As[k*GT + r]
+  TC* Bs = As + GK * GT;         // [GK][GT]  Bs[k*GT + c]
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT;
-  double ra[PER], rb[PER];
-  // global -> registers for the chunk (r0, c0, k0); the loads of the next
-  // chunk are issued before the current chunk is multiplied.
+  TC ra[PER], rb[PER];
   auto fetch = [&](int r0, int c0, int k0) {
 #pragma unroll
     for (int u = 0; u < PER; ++u) {
@@ -113,11 +117,11 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const doubl
       int r, k;
       if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
       const int gr = r0 + r, gk = k0 + k;
-      ra[u] = (gr < M && gk < K) ? (tA ? A[gk + (size_t)lda * gr] : A[gr + (size_t)lda * gk]) : 0.0;
+      ra[u] = (gr < M && gk < K) ? (TC)(tA ? A[gk + (size_t)lda * gr] : A[gr + (size_t)lda * gk]) : (TC)0;
       int c;
       if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
       const int gc = c0 + c, gk2 = k0 + k;
-      rb[u] = (gc < N && gk2 < K) ? (tB ? B[gc + (size_t)ldb * gk2] : B[gk2 + (size_t)ldb * gc]) : 0.0;
+      rb[u] = (gc < N && gk2 < K) ? (TC)(tB ? B[gc + (size_t)ldb * gk2] : B[gk2 + (size_t)ldb * gc]) : (TC)0;
     }
   };
   auto store = [&]() {
@@ -132,7 +136,6 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const doubl
       Bs[k * GT + c] = rb[u];
     }
   };
-  // list of (tile, k0) steps, skipping tiles above the diagonal when lower
   auto tile_live = [&](int tile) {
     const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
     return !(lower && r0 + GT - 1 + diag_off < c0);
@@ -142,11 +145,11 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const doubl
   if (tile < tm * tn) fetch((tile % tm) * GT, (tile / tm) * GT, 0);
   while (tile < tm * tn) {
     const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
-    double acc[4][4];
+    TC acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+      for (int j = 0; j < 4; ++j) acc[i][j] = (TC)0;
     int next = tile + 1;
     while (next < tm * tn && !tile_live(next)) ++next;
     for (int k0 = 0; k0 < K; k0 += GK) {
@@ -156,7 +159,7 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const doubl
       else if (next < tm * tn) fetch((next % tm) * GT, (next / tm) * GT, 0);
       const int kmax = min(GK, K - k0);
       for (int k = 0; k < kmax; ++k) {
-        double a[4], b[4];
+        TC a[4], b[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) a[i] = As[k * GT + ty + 16 * i];
 #pragma unroll
@@ -177,8 +180,8 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const doubl
         const int gc = c0 + tx + 16 * j;
         if (gc >= N) continue;
         if (lower && gr + diag_off < gc) continue;
-        double* cp = C + gr + (size_t)ldc * gc;
-        *cp = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
+        TM* cp = C + gr + (size_t)ldc * gc;
+        *cp = (TM)((beta == 0.0) ? alpha * (double)acc[i][j] : alpha * (double)acc[i][j] + beta * (double)(*cp));
       }
     }
     tile = next;
@@ -189,35 +192,35 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const doubl
 // Square n x n product as ONE output tile of (16 R) x (16 R), R = ceil(n/16)
 // (n <= 96): thread (tx, ty) of the 16 x 16 grid owns rows ty + 16 i and
 // columns tx + 16 j, i, j < R, so no padding beyond the next multiple of 16
-// is computed.  K is staged in chunks of 16 (smem 2 * 16 * 16R doubles).
-template <int NT, int R>
-__device__ __noinline__ void gemm_tile(int n, bool tA, const double* A, int lda, bool tB, const double* B, int ldb,
-                          double* C, int ldc, double alpha, double beta, double* smem)
+// is computed.  K is staged in chunks of 16 (smem 2 * 16 * 16R elements of TC).
+template <int NT, int R, typename TM, typename TC>
+__device__ __noinline__ void gemm_tile(int n, bool tA, const TM* A, int lda, bool tB, const TM* B, int ldb,
+                                       TM* C, int ldc, double alpha, double beta, void* smem_v)
 {
   constexpr int T = 16 * R, KC = 16;
-  double* As = smem;            // [KC][T]
-  double* Bs = smem + KC * T;   // [KC][T]
+  TC* As = (TC*)smem_v;         // [KC][T]
+  TC* Bs = As + KC * T;         // [KC][T]
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[R][R];
+  TC acc[R][R];
 #pragma unroll
   for (int i = 0; i < R; ++i)
 #pragma unroll
-    for (int j = 0; j < R; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < R; ++j) acc[i][j] = (TC)0;
   for (int k0 = 0; k0 < n; k0 += KC) {
     for (int t = threadIdx.x; t < KC * T; t += NT) {
       int r, k;
       if (!tA) { r = t % T; k = t / T; } else { k = t % KC; r = t / KC; }
       const int gk = k0 + k;
-      As[k * T + r] = (r < n && gk < n) ? (tA ? A[gk + (size_t)lda * r] : A[r + (size_t)lda * gk]) : 0.0;
+      As[k * T + r] = (r < n && gk < n) ? (TC)(tA ? A[gk + (size_t)lda * r] : A[r + (size_t)lda * gk]) : (TC)0;
       int c;
       if (!tB) { k = t % KC; c = t / KC; } else { c = t % T; k = t / T; }
       const int gk2 = k0 + k;
-      Bs[k * T + c] = (c < n && gk2 < n) ? (tB ? B[c + (size_t)ldb * gk2] : B[gk2 + (size_t)ldb * c]) : 0.0;
+      Bs[k * T + c] = (c < n && gk2 < n) ? (TC)(tB ? B[c + (size_t)ldb * gk2] : B[gk2 + (size_t)ldb * c]) : (TC)0;
     }
     __syncthreads();
     const int kmax = min(KC, n - k0);
     for (int k = 0; k < kmax; ++k) {
-      double a[R], b[R];
+      TC a[R], b[R];
 #pragma unroll
       for (int i = 0; i < R; ++i) a[i] = As[k * T + ty + 16 * i];
 #pragma unroll
@@ -236,8 +239,8 @@ __device__ __noinline__ void gemm_tile(int n, bool tA, const double* A, int lda,
     for (int j = 0; j < R; ++j) {
       const int gc = tx + 16 * j;
       if (gr < n && gc < n) {
-        double* cp = C + gr + (size_t)ldc * gc;
-        *cp = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
+        TM* cp = C + gr + (size_t)ldc * gc;
+        *cp = (TM)((beta == 0.0) ? alpha * (double)acc[i][j] : alpha * (double)acc[i][j] + beta * (double)(*cp));
       }
     }
   }
@@ -245,51 +248,80 @@ __device__ __noinline__ void gemm_tile(int n, bool tA, const double* A, int lda,
 }
 
 // Square GEMM dispatch: one exact-size tile for n <= 96, 64 x 64 tiles above.
-// smem must hold 2 * 16 * 96 doubles.
-template <int NT>
-__device__ __forceinline__ void gemm(int n, bool tA, const double* A, int lda, bool tB, const double* B,
-                                     int ldb, double* C, int ldc, double alpha, double beta, double* smem)
+// smem must hold 2 * 16 * 96 doubles.  lowp = compute in FP32.
+template <int NT, typename TM>
+__device__ __forceinline__ void gemm_prec(int n, bool tA, const TM* A, int lda, bool tB, const TM* B, int ldb,
+                                          TM* C, int ldc, double alpha, double beta, void* smem, bool lowp)
 {
-  if (n <= 32) gemm_tile<NT, 2>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-  else if (n <= 48) gemm_tile<NT, 3>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-  else if (n <= 64) gemm_tile<NT, 4>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-  else if (n <= 80) gemm_tile<NT, 5>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-  else if (n <= 96) gemm_tile<NT, 6>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-  else gemm_rect<NT>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+  if (lowp) {
+    if (n <= 32) gemm_tile<NT, 2, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 48) gemm_tile<NT, 3, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 64) gemm_tile<NT, 4, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 80) gemm_tile<NT, 5, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 96) gemm_tile<NT, 6, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else gemm_rect<NT, TM, float>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+  } else {
+    if (n <= 32) gemm_tile<NT, 2, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 48) gemm_tile<NT, 3, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 64) gemm_tile<NT, 4, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 80) gemm_tile<NT, 5, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 96) gemm_tile<NT, 6, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else gemm_rect<NT, TM, TM>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void gemm(int n, bool tA, const double* A, int lda, bool tB, const double* B, int ldb,
+                                     double* C, int ldc, double alpha, double beta, double* smem)
+{
+  gemm_prec<NT, double>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem, false);
 }
 
 // ------------------------------------------------------------ warp Cholesky
+// Pivot rules: adjust = true is the reference's Schur-complement rule
+// (rATL_dpotrfL, sdpa_dpotrf.cpp:31-33): pivot < -1e-6 fails, pivot < 1e-14
+// is replaced by a huge value (1e100 in FP64; in FP32, where 1e100 is not
+// representable, 1e30, which likewise makes the column vanish).  adjust =
+// false is LAPACK dpotrf's rule (pivot <= 0 fails).  NaN fails under both.
+template <typename T>
+__device__ __forceinline__ T adjust_huge();
+template <>
+__device__ __forceinline__ double adjust_huge<double>() { return 1.0e100; }
+template <>
+__device__ __forceinline__ float adjust_huge<float>() { return 1.0e30f; }
+
 // Factors the bs x bs (bs <= 32) lower triangle held in sD (leading
 // dimension LDD) in place with one warp: lane r keeps row r in registers and
 // the column of each step is broadcast with shuffles (no shared-memory
-// traffic inside the factorisation).  Pivot rules as cholesky() below; kb is
-// the block's offset, used in the returned failing column (0 = success).
-static __device__ __noinline__ int warp_potrf32(int bs, double* sD, bool adjust, int kb)
+// traffic inside the factorisation).  kb is the block's offset, used in the
+// returned failing column (0 = success).
+template <typename T>
+static __device__ __noinline__ int warp_potrf32(int bs, T* sD, bool adjust, int kb)
 {
   const int lane = threadIdx.x & 31;
-  double a[32];
+  T a[32];
 #pragma unroll
-  for (int c = 0; c < 32; ++c) a[c] = (c <= lane && lane < bs) ? sD[lane + LDD * c] : 0.0;
+  for (int c = 0; c < 32; ++c) a[c] = (c <= lane && lane < bs) ? sD[lane + LDD * c] : (T)0;
   int fail = 0;
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     if (j < bs && !fail) {
-      double d = __shfl_sync(0xffffffffu, a[j], j);
+      T d = __shfl_sync(0xffffffffu, a[j], j);
       if (adjust) {
-        if (d < -1.0e-6 || d != d) fail = kb + j + 1;
-        else if (d < 1.0e-14) d = 1.0e100;
-      } else if (!(d > 0.0)) {
+        if (d < (T)-1.0e-6 || d != d) fail = kb + j + 1;
+        else if (d < (T)1.0e-14) d = adjust_huge<T>();
+      } else if (!(d > (T)0)) {
         fail = kb + j + 1;
       }
       if (!fail) {
-        const double ljj = sqrt(d);
-        const double inv = 1.0 / ljj;
+        const T ljj = sqrt(d);
+        const T inv = (T)1 / ljj;
         if (lane == j) a[j] = ljj;
         else if (lane > j) a[j] *= inv;
-        const double lrj = a[j];
+        const T lrj = a[j];
 #pragma unroll
         for (int c = j + 1; c < 32; ++c) {
-          const double lcj = __shfl_sync(0xffffffffu, lrj, c);
+          const T lcj = __shfl_sync(0xffffffffu, lrj, c);
           if (lane >= c) a[c] -= lrj * lcj;
         }
       }
@@ -304,29 +336,26 @@ static __device__ __noinline__ int warp_potrf32(int bs, double* sD, bool adjust,
 }
 
 // ------------------------------------------------------------ Cholesky
-// In-place lower Cholesky, right-looking, blocked by 32.  adjust = true is
-// the reference's Schur-complement rule (rATL_dpotrfL,
-// sdpa_dpotrf.cpp:31-33): pivot < -1e-6 fails, pivot < 1e-14 becomes 1e100.
-// adjust = false is LAPACK dpotrf's rule (pivot <= 0 or NaN fails).  NaN
-// pivots fail under both rules.  Returns 0 on success, else the failing
-// column + 1.  The strict upper triangle is zeroed on success.
-// sD: SD_DOUBLES doubles; smem: GEMM staging.
-template <int NT>
-__device__ int cholesky(int n, double* A, int lda, bool adjust, double* sD, double* smem, int* s_flag)
+// In-place lower Cholesky, right-looking, blocked by 32, pivot rules as
+// warp_potrf32.  Returns 0 on success, else the failing column + 1.  The
+// strict upper triangle is zeroed on success.  sD: SD_DOUBLES elements of T;
+// smem: GEMM staging.
+template <int NT, typename T>
+__device__ int cholesky(int n, T* A, int lda, bool adjust, T* sD, void* smem, int* s_flag)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   for (int kb = 0; kb < n; kb += NB) {
     const int bs = min(NB, n - kb);
-    // (a) diagonal block: staged by all threads, factored by warp 0 (lane r owns row r)
+    // (a) diagonal block: staged by all threads, factored by warp 0
     for (int t = tid; t < NB * NB; t += NT) {
       const int r = t % NB, c = t / NB;
       if (r < bs && c <= r) sD[r + LDD * c] = A[(kb + r) + (size_t)lda * (kb + c)];
     }
     __syncthreads();
     if (wid == 0) {
-      const int fail = warp_potrf32(bs, sD, adjust, kb);
+      const int fail = warp_potrf32<T>(bs, sD, adjust, kb);
       if (lane == 0) *s_flag = fail;
-      if (!fail && lane < bs) sD[NB * LDD + lane] = 1.0 / sD[lane + LDD * lane];
+      if (!fail && lane < bs) sD[NB * LDD + lane] = (T)1 / sD[lane + LDD * lane];
     }
     __syncthreads();
     const int f = *s_flag;
@@ -340,17 +369,17 @@ __device__ int cholesky(int n, double* A, int lda, bool adjust, double* sD, doub
       // (b) panel: A[r, kb:kb+bs] := A[r, kb:kb+bs] L_bb^{-T}; each warp solves
       //     four rows at a time (four independent shuffle chains)
       for (int rb = r0 + 4 * wid; rb < n; rb += 4 * (NT / 32)) {
-        double x[4];
+        T x[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-          x[u] = (lane < bs && rb + u < n) ? A[(rb + u) + (size_t)lda * (kb + lane)] : 0.0;
+          x[u] = (lane < bs && rb + u < n) ? A[(rb + u) + (size_t)lda * (kb + lane)] : (T)0;
         for (int c = 0; c < bs; ++c) {
-          const double dinv = sD[NB * LDD + c];
-          const double lc = (lane > c && lane < bs) ? sD[lane + LDD * c] : 0.0;
+          const T dinv = sD[NB * LDD + c];
+          const T lc = (lane > c && lane < bs) ? sD[lane + LDD * c] : (T)0;
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             if (lane == c) x[u] *= dinv;
-            const double xc = __shfl_sync(0xffffffffu, x[u], c);
+            const T xc = __shfl_sync(0xffffffffu, x[u], c);
             x[u] -= xc * lc;
           }
         }
@@ -360,29 +389,29 @@ __device__ int cholesky(int n, double* A, int lda, bool adjust, double* sD, doub
       }
       __syncthreads();
       // (c) trailing: A22 -= P P^T (lower triangle), P = A[r0:, kb:kb+bs]
-      const double* P = A + r0 + (size_t)lda * kb;
-      gemm_rect<NT>(rem, rem, bs, false, P, lda, true, P, lda, A + r0 + (size_t)lda * r0, lda, -1.0, 1.0,
-                    smem, true, 0);
+      const T* P = A + r0 + (size_t)lda * kb;
+      gemm_rect<NT, T, T>(rem, rem, bs, false, P, lda, true, P, lda, A + r0 + (size_t)lda * r0, lda, -1.0, 1.0,
+                          smem, true, 0);
     }
   }
   for (int t = tid; t < n * n; t += NT) {
     const int i = t % n, k = t / n;
-    if (i < k) A[i + (size_t)lda * k] = 0.0;
+    if (i < k) A[i + (size_t)lda * k] = (T)0;
   }
   __syncthreads();
   return 0;
 }
 
 // Li = L^{-1} for lower-triangular L: solves L Li = I blocked by 32
-// (diagonal block substitution one warp per column, trailing GEMM update).
+// (diagonal block substitution four columns per warp, trailing GEMM update).
 // Li must not alias L.
-template <int NT>
-__device__ void tri_inverse(int n, const double* L, int ldl, double* Li, int ldi, double* sD, double* smem)
+template <int NT, typename T>
+__device__ void tri_inverse(int n, const T* L, int ldl, T* Li, int ldi, T* sD, void* smem)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   for (int t = tid; t < n * n; t += NT) {
     const int i = t % n, j = t / n;
-    Li[i + (size_t)ldi * j] = (i == j) ? 1.0 : 0.0;
+    Li[i + (size_t)ldi * j] = (i == j) ? (T)1 : (T)0;
   }
   for (int kb = 0; kb < n; kb += NB) {
     const int bs = min(NB, n - kb);
@@ -390,21 +419,20 @@ __device__ void tri_inverse(int n, const double* L, int ldl, double* Li, int ldi
       const int r = t % NB, c = t / NB;
       if (r < bs && c <= r) sD[r + LDD * c] = L[(kb + r) + (size_t)ldl * (kb + c)];
     }
-    for (int r = tid; r < bs; r += NT) sD[NB * LDD + r] = 1.0 / L[(kb + r) + (size_t)ldl * (kb + r)];
+    for (int r = tid; r < bs; r += NT) sD[NB * LDD + r] = (T)1 / L[(kb + r) + (size_t)ldl * (kb + r)];
     __syncthreads();
-    // (a) Li[kb:kb+bs, 0:kb+bs] = L_bb^{-1} Li[kb:kb+bs, 0:kb+bs], four columns per warp
     for (int cb = 4 * wid; cb < kb + bs; cb += 4 * (NT / 32)) {
-      double x[4];
+      T x[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u)
-        x[u] = (lane < bs && cb + u < kb + bs) ? Li[(kb + lane) + (size_t)ldi * (cb + u)] : 0.0;
+        x[u] = (lane < bs && cb + u < kb + bs) ? Li[(kb + lane) + (size_t)ldi * (cb + u)] : (T)0;
       for (int p = 0; p < bs; ++p) {
-        const double dinv = sD[NB * LDD + p];
-        const double lp = (lane > p && lane < bs) ? sD[lane + LDD * p] : 0.0;
+        const T dinv = sD[NB * LDD + p];
+        const T lp = (lane > p && lane < bs) ? sD[lane + LDD * p] : (T)0;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           if (lane == p) x[u] *= dinv;
-          const double xp = __shfl_sync(0xffffffffu, x[u], p);
+          const T xp = __shfl_sync(0xffffffffu, x[u], p);
           x[u] -= lp * xp;
         }
       }
@@ -413,21 +441,20 @@ __device__ void tri_inverse(int n, const double* L, int ldl, double* Li, int ldi
         if (lane < bs && cb + u < kb + bs) Li[(kb + lane) + (size_t)ldi * (cb + u)] = x[u];
     }
     __syncthreads();
-    // (b) Li[kb+bs:, 0:kb+bs] -= L[kb+bs:, kb:kb+bs] Li[kb:kb+bs, 0:kb+bs]
     const int r0 = kb + bs, rem = n - r0;
     if (rem > 0)
-      gemm_rect<NT>(rem, kb + bs, bs, false, L + r0 + (size_t)ldl * kb, ldl, false, Li + kb, ldi,
-                    Li + r0, ldi, -1.0, 1.0, smem);
+      gemm_rect<NT, T, T>(rem, kb + bs, bs, false, L + r0 + (size_t)ldl * kb, ldl, false, Li + kb, ldi, Li + r0,
+                          ldi, -1.0, 1.0, smem);
   }
   __syncthreads();
 }
 
-// x = L^{-T} L^{-1} x for a Cholesky factor L (lower); x in shared memory.
-// Blocked by 32: each diagonal block is staged in shared memory by all
-// threads and solved by warp 0 with shuffles; the other rows are updated
-// block-wide.  sD: SD_DOUBLES doubles.
-template <int NT>
-__device__ void chol_solve(int n, const double* L, int ldl, double* x, double* sD)
+// x = L^{-T} L^{-1} x for a Cholesky factor L (lower).  Blocked by 32: each
+// diagonal block is staged in shared memory by all threads and solved by
+// warp 0 with shuffles; the other rows are updated block-wide.
+// sD: SD_DOUBLES elements of T.
+template <int NT, typename T>
+__device__ void chol_solve(int n, const T* L, int ldl, T* x, T* sD)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   auto stage = [&](int kb, int bs) {
@@ -435,48 +462,46 @@ __device__ void chol_solve(int n, const double* L, int ldl, double* x, double* s
       const int r = t % NB, c = t / NB;
       if (r < bs && c <= r) sD[r + LDD * c] = L[(kb + r) + (size_t)ldl * (kb + c)];
     }
-    for (int r = tid; r < bs; r += NT) sD[NB * LDD + r] = 1.0 / L[(kb + r) + (size_t)ldl * (kb + r)];
+    for (int r = tid; r < bs; r += NT) sD[NB * LDD + r] = (T)1 / L[(kb + r) + (size_t)ldl * (kb + r)];
     __syncthreads();
   };
-  // forward: L z = x
   for (int kb = 0; kb < n; kb += NB) {
     const int bs = min(NB, n - kb);
     stage(kb, bs);
     if (wid == 0) {
-      double v = (lane < bs) ? x[kb + lane] : 0.0;
+      T v = (lane < bs) ? x[kb + lane] : (T)0;
       for (int p = 0; p < bs; ++p) {
         if (lane == p) v *= sD[NB * LDD + p];
-        const double vp = __shfl_sync(0xffffffffu, v, p);
+        const T vp = __shfl_sync(0xffffffffu, v, p);
         if (lane > p && lane < bs) v -= sD[lane + LDD * p] * vp;
       }
       if (lane < bs) x[kb + lane] = v;
     }
     __syncthreads();
     for (int i = kb + bs + tid; i < n; i += NT) {
-      double s = 0.0;
+      T s = (T)0;
 #pragma unroll 8
       for (int p = 0; p < bs; ++p) s += L[i + (size_t)ldl * (kb + p)] * x[kb + p];
       x[i] -= s;
     }
     __syncthreads();
   }
-  // backward: L^T x = z
   const int nblk = (n + NB - 1) / NB;
   for (int b = nblk - 1; b >= 0; --b) {
     const int kb = b * NB, bs = min(NB, n - kb);
     stage(kb, bs);
     if (wid == 0) {
-      double v = (lane < bs) ? x[kb + lane] : 0.0;
+      T v = (lane < bs) ? x[kb + lane] : (T)0;
       for (int p = bs - 1; p >= 0; --p) {
         if (lane == p) v *= sD[NB * LDD + p];
-        const double vp = __shfl_sync(0xffffffffu, v, p);
+        const T vp = __shfl_sync(0xffffffffu, v, p);
         if (lane < p) v -= sD[p + LDD * lane] * vp;
       }
       if (lane < bs) x[kb + lane] = v;
     }
     __syncthreads();
     for (int i = wid; i < kb; i += NT / 32) {
-      double s = (lane < bs) ? L[(kb + lane) + (size_t)ldl * i] * x[kb + lane] : 0.0;
+      T s = (lane < bs) ? L[(kb + lane) + (size_t)ldl * i] * x[kb + lane] : (T)0;
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
       if (lane == 0) x[i] -= s;
     }

@@ -111,6 +111,18 @@ SDPAB_HD bool update_check(Scalars& s, const Params& p)
   return true;
 }
 
+// Complementarity gap nDim * mu relative to the objective scale
+// max(1, (|objP| + |objD|) / 2), the scale of the reference's gap test.  The
+// mixed-precision modes run their FP32 products while this is at least the
+// switch value (default 1e-2): the condition of X and Z grows like 1/mu, so
+// the switch is tied to how far the iterate is from optimal, not to mu0
+// (a warm start begins close to optimal).
+SDPAB_HD double mixed_gap(const Scalars& s)
+{
+  const double mean = (fabs(s.objP) + fabs(s.objD)) / 2.0;
+  return s.nDim * s.mu / (mean < 1.0 ? 1.0 : mean);
+}
+
 // Switch::MehrotraPredictor + DirectionParameter::MehrotraPredictor
 // (sdpa_parts.cpp:733-743, :653-666).
 SDPAB_HD void predictor_setup(Scalars& s, const Params& p)

@@ -217,6 +217,14 @@ __global__ void k_to_bf16(long long n, const float* w, __nv_bfloat16* wb)
 
 static inline int nb(long long n, int t = 256) { return (int)((n + t - 1) / t); }
 
+// x_i = r_i d_i / 4 (nodes with edges), fallback_i otherwise
+__global__ void k_propose(int n, const float* r, const double* degree, const double* fallback, double* x)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = (degree[i] > 1.0e-9) ? (double)r[i] * degree[i] * 0.25 : fallback[i];
+}
+
 // Activation layout inside act: per layer l: h_l (N x Fin_l), agg_l (N x Fin_l),
 // z_l (N x H); then h_L (N x H), r (N).
 struct Act {
@@ -330,6 +338,15 @@ SDPAB_API int sdpab_mpnn_adam(float* master, unsigned short* weights_bf16, const
                                                   beta1, beta2, eps, c1, c2, weight_decay);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? SDPAB_OK : cuda_error(e, "mpnn_adam");
+}
+
+SDPAB_API int sdpab_mpnn_propose_x(int num_nodes, const float* r, const double* degree, const double* fallback,
+                                   double* xvec, void* stream)
+{
+  if (num_nodes < 1 || !r || !degree || !fallback || !xvec) return set_error(SDPAB_EINVAL, "mpnn_propose_x: bad arguments");
+  k_propose<<<nb(num_nodes), 256, 0, (cudaStream_t)stream>>>(num_nodes, r, degree, fallback, xvec);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SDPAB_OK : cuda_error(e, "mpnn_propose_x");
 }
 
 SDPAB_API int sdpab_mpnn_to_bf16(const float* master, unsigned short* weights_bf16, void* stream)

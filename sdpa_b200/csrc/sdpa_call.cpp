@@ -623,9 +623,17 @@ void SDPA::printResultYMat(FILE* fp)
 {
   if (fp && impl_->solved) print_blocks(*impl_, impl_->Yres, impl_->YPrint, fp);
 }
+// ComputeTime::display (sdpa_parts.cpp:78-164) restated over the GPU phases
 void SDPA::printComputationTime(FILE* fp)
 {
-  if (fp) fprintf(fp, "    solve time = %.6f\n", getSolveTime());
+  if (!fp) return;
+  static const char* names[] = {"Make rMat+gVec", "Make bMat", "Cholesky bMat", "solve",
+                                "makedXdZ", "StepLength", "update (inverses)", "updateRes"};
+  const sdpab::SolveStats& s = impl_->solver.stats();
+  fprintf(fp, "                         Time(sec)\n");
+  for (size_t q = 0; q < s.phase_seconds.size() && q < 8; ++q)
+    fprintf(fp, " %-22s = %f\n", names[q], s.phase_seconds[q]);
+  fprintf(fp, " %-22s = %f\n", "Total (solve)", getSolveTime());
 }
 void SDPA::printParameters(FILE* fp)
 {
@@ -766,7 +774,9 @@ void SDPA::copyCurrentToInit()
   }
 }
 void SDPA::setKappa(double k) { impl_->kappa = k; }
+void SDPA::setPrecision(int mode, double mu_switch) { impl_->solver.set_precision(mode, mu_switch); }
 int SDPA::getErrorCode() { return impl_->err; }
+const sdpab::SolveStats& SDPA::impl_solver_stats() { return impl_->solver.stats(); }
 const char* SDPA::getErrorMessage() { return impl_->errmsg.c_str(); }
 
 // ------------------------------------------------------------------ C ABI
@@ -858,6 +868,13 @@ SDPAB_API int sdpab_sdpa_set_init(sdpab_sdpa* h, const double* xvec, const doubl
   }
   return status_of(p);
 }
+SDPAB_API int sdpab_sdpa_set_precision(sdpab_sdpa* h, int mode, double mu_switch)
+{
+  if (!h || (mode != SDPAB_PREC_FP64 && mode != SDPAB_PREC_MIXED))
+    return sdpab::set_error(SDPAB_EINVAL, "set_precision: bad arguments");
+  ((SDPA*)h)->setPrecision(mode, mu_switch);
+  return SDPAB_OK;
+}
 SDPAB_API int sdpab_sdpa_solve(sdpab_sdpa* h)
 {
   if (!h) return sdpab::set_error(SDPAB_EINVAL, "null argument");
@@ -882,6 +899,13 @@ SDPAB_API int sdpab_sdpa_info(sdpab_sdpa* h, sdpab_sdpa_info_t* out)
   out->phase = (int)p->getPhaseValue();
   out->m = p->getConstraintNumber();
   out->nblock = p->getBlockNumber();
+  return SDPAB_OK;
+}
+SDPAB_API int sdpab_sdpa_phase_times(sdpab_sdpa* h, double* out8)
+{
+  if (!h || !out8) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  const sdpab::SolveStats& s = ((SDPA*)h)->impl_solver_stats();
+  for (int q = 0; q < 8; ++q) out8[q] = (q < (int)s.phase_seconds.size()) ? s.phase_seconds[q] : 0.0;
   return SDPAB_OK;
 }
 SDPAB_API int sdpab_sdpa_get_xvec(sdpab_sdpa* h, double* out)

@@ -64,7 +64,8 @@ __global__ void k_sym_diff(int n, double* dX, const double* R, const double* W)
 }
 
 // rows x cols copy between leading dimensions
-__global__ void k_copy2d(int rows, int cols, const double* src, int lds, double* dst, int ldd)
+template <typename T>
+__global__ void k_copy2d_t(int rows, int cols, const T* src, int lds, T* dst, int ldd)
 {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)rows * cols) return;
@@ -315,9 +316,10 @@ __global__ void k_trace(int n, const double* A, double* out, double scale)
 
 // C = alpha op(A) op(B) + beta C over 64 x 64 output tiles, one tile per
 // block, z = batch (strided); lower skips tiles above the diagonal.
-__global__ void __launch_bounds__(NT) k_gemm(int M, int N, int K, int tA, const double* A, int lda,
-                                             long long sA, int tB, const double* B, int ldb, long long sB,
-                                             double* C, int ldc, long long sC, double alpha, double beta,
+template <typename TM, typename TC>
+__global__ void __launch_bounds__(NT) k_gemm(int M, int N, int K, int tA, const TM* A, int lda,
+                                             long long sA, int tB, const TM* B, int ldb, long long sB,
+                                             TM* C, int ldc, long long sC, double alpha, double beta,
                                              int lower)
 {
   extern __shared__ double smem[];
@@ -327,40 +329,114 @@ __global__ void __launch_bounds__(NT) k_gemm(int M, int N, int K, int tA, const 
   A += sA * z;
   B += sB * z;
   C += sC * z;
-  const double* Ap = tA ? A + (size_t)lda * r0 : A + r0;
-  const double* Bp = tB ? B + c0 : B + (size_t)ldb * c0;
-  cta::gemm_rect<NT>(min(cta::GT, M - r0), min(cta::GT, N - c0), K, tA, Ap, lda, tB, Bp, ldb,
-                     C + r0 + (size_t)ldc * c0, ldc, alpha, beta, smem, lower != 0, r0 - c0);
+  const TM* Ap = tA ? A + (size_t)lda * r0 : A + r0;
+  const TM* Bp = tB ? B + c0 : B + (size_t)ldb * c0;
+  cta::gemm_rect<NT, TM, TC>(min(cta::GT, M - r0), min(cta::GT, N - c0), K, tA, Ap, lda, tB, Bp, ldb,
+                             C + r0 + (size_t)ldc * c0, ldc, alpha, beta, smem, lower != 0, r0 - c0);
 }
 
 // Diagonal block of the blocked Cholesky: one block factors A[0:bs, 0:bs]
 // (leading dimension lda) with the chosen pivot rule; first failure (global
 // column + 1) is written to *flag if *flag is still 0.
-__global__ void __launch_bounds__(NT) k_chol_diag(int bs, double* A, int lda, int adjust, int col0, int* flag)
+template <typename T>
+__global__ void __launch_bounds__(NT) k_chol_diag(int bs, T* A, int lda, int adjust, int col0, int* flag)
 {
   extern __shared__ double smem[];
   __shared__ int s_flag;
-  double* sD = smem + 2 * cta::GK * cta::GT;
+  T* sD = (T*)(smem + 2 * cta::GK * cta::GT);
   if (*flag) return;
-  const int f = cta::cholesky<NT>(bs, A, lda, adjust != 0, sD, smem, &s_flag);
+  const int f = cta::cholesky<NT, T>(bs, A, lda, adjust != 0, sD, smem, &s_flag);
   if (f && threadIdx.x == 0) atomicCAS(flag, 0, col0 + f);
 }
 
 // Li = L^{-1} of a bs x bs lower-triangular block (lda) into Li (ld bs)
-__global__ void __launch_bounds__(NT) k_tri_inv(int bs, const double* L, int lda, double* Li, int ldi,
-                                                const int* flag)
+template <typename T>
+__global__ void __launch_bounds__(NT) k_tri_inv(int bs, const T* L, int lda, T* Li, int ldi, const int* flag)
 {
   extern __shared__ double smem[];
-  double* sD = smem + 2 * cta::GK * cta::GT;
+  T* sD = (T*)(smem + 2 * cta::GK * cta::GT);
   if (flag && *flag) return;
-  cta::tri_inverse<NT>(bs, L, lda, Li, ldi, sD, smem);
+  cta::tri_inverse<NT, T>(bs, L, lda, Li, ldi, sD, smem);
 }
 
 // x = L^{-T} L^{-1} x (Lal::solveSystems, sdpa_linear.cpp:843-862)
-__global__ void __launch_bounds__(NT) k_chol_solve(int m, const double* L, double* x)
+template <typename T>
+__global__ void __launch_bounds__(NT) k_chol_solve(int m, const T* L, T* x)
 {
   extern __shared__ double smem[];
-  cta::chol_solve<NT>(m, L, m, x, smem);
+  cta::chol_solve<NT, T>(m, L, m, x, (T*)smem);
+}
+
+// element-wise conversion between precisions
+template <typename TO, typename TI>
+__global__ void k_convert(long long n, TO* out, const TI* in)
+{
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < n) out[t] = (TO)in[t];
+}
+
+// Blocked triangular solves with the stored diagonal-block inverses of the
+// Cholesky factor (one block: x_b = Dinv_b x_b or Dinv_b^T x_b).
+template <typename T>
+__global__ void k_trsv_diag(int bs, const T* Dinv, T* x, int trans)
+{
+  __shared__ T xs[256];
+  for (int i = threadIdx.x; i < bs; i += blockDim.x) xs[i] = x[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < bs; i += blockDim.x) {
+    T s = (T)0;
+    if (!trans)
+      for (int p = 0; p <= i; ++p) s += Dinv[i + (size_t)bs * p] * xs[p];
+    else
+      for (int p = i; p < bs; ++p) s += Dinv[p + (size_t)bs * i] * xs[p];
+    x[i] = s;
+  }
+}
+
+// forward update: x[r] -= sum_p L[r, kb+p] x[kb+p] for the rows below the block
+template <typename T>
+__global__ void k_trsv_fwd_update(int rows, int bs, const T* Lp, int ld, const T* xb, T* xr)
+{
+  __shared__ T xs[256];
+  for (int i = threadIdx.x; i < bs; i += blockDim.x) xs[i] = xb[i];
+  __syncthreads();
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  T s = (T)0;
+  for (int p = 0; p < bs; ++p) s += Lp[r + (size_t)ld * p] * xs[p];
+  xr[r] -= s;
+}
+
+// backward update: x[i] -= sum_p L[kb+p, i] x[kb+p] for i < kb (one warp per i)
+template <typename T>
+__global__ void k_trsv_bwd_update(int kb, int bs, const T* Lrow, int ld, const T* xb, T* x)
+{
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= kb) return;
+  T s = (T)0;
+  for (int p = lane; p < bs; p += 32) s += Lrow[p + (size_t)ld * warp] * xb[p];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) x[warp] -= s;
+}
+
+// x += (double) v
+__global__ void k_add_f32(int m, double* x, const float* v)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < m) x[t] += (double)v[t];
+}
+
+// r = g - B x for the symmetric m x m FP64 Schur matrix (column i dotted with
+// x, one warp per i): the FP64 residual of the iterative refinement.
+__global__ void k_residual(int m, const double* B, const double* x, const double* g, double* r)
+{
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= m) return;
+  const double* col = B + (size_t)m * warp;
+  double s = 0.0;
+  for (int k = lane; k < m; k += 32) s += col[k] * x[k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) r[warp] = g[warp] - s;
 }
 
 // minimum eigenvalue of a formed M = L D L^T (n x n, global) into *out
@@ -431,6 +507,12 @@ struct DevState {
   double* Linv = nullptr;   // panel inverse scratch (NBG x NBG)
   double* T = nullptr;      // panel / F1 scratch
   size_t Tsize = 0;
+  float *B32 = nullptr, *Linv32 = nullptr, *T32 = nullptr, *v32 = nullptr;  // mixed-precision Schur
+  double* dinv = nullptr;   // diagonal-block inverses of the Schur factor (large m)
+  float* dinv32 = nullptr;
+  double* res = nullptr;    // refinement residual
+  int mixed = 0;
+  double mu_switch = 1.0e-2;
   double* part = nullptr;   // reduction partials
   double* sc = nullptr;     // scalar slots
   int* flag = nullptr;
@@ -461,41 +543,84 @@ struct DevState {
 
 static const int NBG = 128;        // panel width of the grid-level Cholesky
 static const int F1_CHUNK = 32;    // F1 constraints processed per batched GEMM
+static const int SMALL_SOLVE = 2048;  // Schur orders up to this use the one-block solve
 
 static size_t chol_smem() { return (2 * cta::GK * cta::GT + cta::SD_DOUBLES) * sizeof(double); }
 
-static void gemm(DevState& S, int M, int N, int K, bool tA, const double* A, int lda, bool tB,
-                 const double* B, int ldb, double* C, int ldc, double alpha, double beta, bool lower = false,
-                 int batch = 1, long long sA = 0, long long sB = 0, long long sC = 0)
+template <typename TM, typename TC>
+static void gemm_t(int M, int N, int K, bool tA, const TM* A, int lda, bool tB, const TM* B, int ldb, TM* C,
+                   int ldc, double alpha, double beta, bool lower = false, int batch = 1, long long sA = 0,
+                   long long sB = 0, long long sC = 0)
 {
   if (M <= 0 || N <= 0) return;
   dim3 grid((M + cta::GT - 1) / cta::GT, (N + cta::GT - 1) / cta::GT, batch);
-  k_gemm<<<grid, NT, 2 * cta::GK * cta::GT * sizeof(double)>>>(M, N, K, tA, A, lda, sA, tB, B, ldb, sB, C,
-                                                               ldc, sC, alpha, beta, lower ? 1 : 0);
+  k_gemm<TM, TC><<<grid, NT, 2 * cta::GK * cta::GT * sizeof(double)>>>(M, N, K, tA, A, lda, sA, tB, B, ldb, sB,
+                                                                       C, ldc, sC, alpha, beta, lower ? 1 : 0);
 }
 
-// Blocked right-looking Cholesky of an n x n matrix (lda = n) in place.
-// Returns 0 or the failing column + 1.
-static int cholesky_grid(DevState& S, double* A, int n, bool adjust)
+// FP64 matrices; lowp = FP32 products (mixed precision)
+static void gemm(DevState& S, int M, int N, int K, bool tA, const double* A, int lda, bool tB,
+                 const double* B, int ldb, double* C, int ldc, double alpha, double beta, bool lower = false,
+                 int batch = 1, long long sA = 0, long long sB = 0, long long sC = 0, bool lowp = false)
+{
+  if (lowp)
+    gemm_t<double, float>(M, N, K, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, lower, batch, sA, sB, sC);
+  else
+    gemm_t<double, double>(M, N, K, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, lower, batch, sA, sB, sC);
+}
+
+// Blocked right-looking Cholesky of an n x n matrix (lda = n) in place, in
+// the matrix's own precision T (FP32 for the mixed-precision Schur factor).
+// Linv: NBG x NBG scratch, Tb: n x NBG scratch.  Returns 0 or the failing
+// column + 1.
+template <typename T>
+static int cholesky_grid_t(DevState& S, T* A, int n, bool adjust, T* Linv, T* Tb, T* dinv_store = nullptr)
 {
   cudaMemset(S.flag, 0, sizeof(int));
   for (int kb = 0; kb < n; kb += NBG) {
     const int bs = std::min(NBG, n - kb);
-    double* Ad = A + kb + (size_t)n * kb;
-    k_chol_diag<<<1, NT, chol_smem()>>>(bs, Ad, n, adjust ? 1 : 0, kb, S.flag);
+    T* Ad = A + kb + (size_t)n * kb;
+    k_chol_diag<T><<<1, NT, chol_smem()>>>(bs, Ad, n, adjust ? 1 : 0, kb, S.flag);
     const int rem = n - kb - bs;
+    if (rem <= 0 && !dinv_store) continue;
+    T* Li = dinv_store ? dinv_store + (size_t)(kb / NBG) * NBG * NBG : Linv;
+    k_tri_inv<T><<<1, NT, chol_smem()>>>(bs, Ad, n, Li, bs, S.flag);
     if (rem <= 0) continue;
-    k_tri_inv<<<1, NT, chol_smem()>>>(bs, Ad, n, S.Linv, bs, S.flag);
-    double* P = A + (kb + bs) + (size_t)n * kb;
+    Linv = Li;
+    T* P = A + (kb + bs) + (size_t)n * kb;
     // panel: P <- P L_bb^{-T}
-    gemm(S, rem, bs, bs, false, P, n, true, S.Linv, bs, S.T, rem, 1.0, 0.0);
-    k_copy2d<<<nblk((long long)rem * bs), 256>>>(rem, bs, S.T, rem, P, n);
+    gemm_t<T, T>(rem, bs, bs, false, P, n, true, Linv, bs, Tb, rem, 1.0, 0.0);
+    k_copy2d_t<T><<<nblk((long long)rem * bs), 256>>>(rem, bs, Tb, rem, P, n);
     // trailing: A22 -= P P^T (lower)
-    gemm(S, rem, rem, bs, false, P, n, true, P, n, A + (kb + bs) + (size_t)n * (kb + bs), n, -1.0, 1.0, true);
+    gemm_t<T, T>(rem, rem, bs, false, P, n, true, P, n, A + (kb + bs) + (size_t)n * (kb + bs), n, -1.0, 1.0, true);
   }
   int f = 0;
   cudaMemcpy(&f, S.flag, sizeof(int), cudaMemcpyDeviceToHost);
   return f;
+}
+
+static int cholesky_grid(DevState& S, double* A, int n, bool adjust, double* dinv_store = nullptr)
+{
+  return cholesky_grid_t<double>(S, A, n, adjust, S.Linv, S.T, dinv_store);
+}
+
+// x = L^{-T} L^{-1} x with the factor of cholesky_grid_t and its stored
+// diagonal-block inverses (grid-wide updates between the block solves).
+template <typename T>
+static void chol_solve_grid(int m, const T* L, const T* dinv, T* x)
+{
+  const int nb = (m + NBG - 1) / NBG;
+  for (int b = 0; b < nb; ++b) {
+    const int kb = b * NBG, bs = std::min(NBG, m - kb), rem = m - kb - bs;
+    k_trsv_diag<T><<<1, 256>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 0);
+    if (rem > 0)
+      k_trsv_fwd_update<T><<<nblk(rem), 256>>>(rem, bs, L + (kb + bs) + (size_t)m * kb, m, x + kb, x + kb + bs);
+  }
+  for (int b = nb - 1; b >= 0; --b) {
+    const int kb = b * NBG, bs = std::min(NBG, m - kb);
+    k_trsv_diag<T><<<1, 256>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 1);
+    if (kb > 0) k_trsv_bwd_update<T><<<nblk((long long)kb * 32), 256>>>(kb, bs, L + kb, m, x + kb, x);
+  }
 }
 
 // Deterministic reduction of len elements into sc[slot]
@@ -752,6 +877,7 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
   S.ytmp = S.alloc(m);
   S.B = S.alloc((size_t)m * m);
   S.Linv = S.alloc((size_t)NBG * NBG);
+  if (m > SMALL_SOLVE) S.dinv = S.alloc((size_t)((m + NBG - 1) / NBG) * NBG * NBG);
   int nmaxb = 1;
   for (auto& B : S.sdp) nmaxb = std::max(nmaxb, B.n);
   Tneed = std::max(Tneed, (size_t)std::max(m, nmaxb) * NBG);
@@ -781,6 +907,27 @@ int Solver::solve(const InitPoint* init)
   auto t_start = std::chrono::steady_clock::now();
   stats_ = SolveStats();
   const int nsdp = (int)S.sdp.size();
+  S.mixed = (precision_ == SDPAB_PREC_MIXED) ? 1 : 0;
+  S.mu_switch = (mu_switch_ > 0.0) ? mu_switch_ : 1.0e-2;
+  if (S.mixed && !S.B32) {
+    void* p = nullptr;
+    const size_t fl = (size_t)m * m + (size_t)NBG * NBG + (size_t)m * NBG + m;
+    if (cudaMalloc(&p, fl * sizeof(float)) != cudaSuccess)
+      return set_error(SDPAB_ECUDA, "device allocation failed (FP32 Schur factor)");
+    S.allocs.push_back(p);
+    S.B32 = (float*)p;
+    S.Linv32 = S.B32 + (size_t)m * m;
+    S.T32 = S.Linv32 + (size_t)NBG * NBG;
+    S.v32 = S.T32 + (size_t)m * NBG;
+    S.res = S.alloc(2 * (size_t)m);
+    if (m > SMALL_SOLVE) {
+      void* q = nullptr;
+      if (cudaMalloc(&q, (size_t)((m + NBG - 1) / NBG) * NBG * NBG * sizeof(float)) != cudaSuccess)
+        return set_error(SDPAB_ECUDA, "device allocation failed (FP32 block inverses)");
+      S.allocs.push_back(q);
+      S.dinv32 = (float*)q;
+    }
+  }
 
   // ------------------------------------------------ initial point
   bool warm = init != nullptr;
@@ -818,10 +965,10 @@ int Solver::solve(const InitPoint* init)
       const long long nn = (long long)B.n * B.n;
       k_axpby<<<nblk(nn), 256>>>(nn, B.W1, 1.0, B.X, 0.0, nullptr);
       if (cholesky_grid(S, B.W1, B.n, false)) { ok = false; break; }
-      k_tri_inv<<<1, NT, chol_smem()>>>(B.n, B.W1, B.n, B.LXi, B.n, nullptr);
+      k_tri_inv<double><<<1, NT, chol_smem()>>>(B.n, B.W1, B.n, B.LXi, B.n, nullptr);
       k_axpby<<<nblk(nn), 256>>>(nn, B.W2, 1.0, B.Z, 0.0, nullptr);
       if (cholesky_grid(S, B.W2, B.n, false)) { ok = false; break; }
-      k_tri_inv<<<1, NT, chol_smem()>>>(B.n, B.W2, B.n, B.LZi, B.n, nullptr);
+      k_tri_inv<double><<<1, NT, chol_smem()>>>(B.n, B.W2, B.n, B.LZi, B.n, nullptr);
       gemm(S, B.n, B.n, B.n, true, B.LZi, B.n, false, B.LZi, B.n, B.Zi, B.n, 1.0, 0.0);
     }
     if (ok && nlp) {
@@ -950,19 +1097,33 @@ int Solver::solve(const InitPoint* init)
   init_scalars(sc, P, S.nDim, mu0, h[0], h[1], h[2], h[3]);
   update_check(sc, P);
 
+  // Per-phase device time (the reference's ComputeTime categories,
+  // sdpa_parts.h:48-86), recorded with CUDA events on the solver's stream.
+  enum { T_RMAT, T_BMAT, T_CHOL, T_SOLVE, T_DXDZ, T_STEP, T_UPDATE, T_RES, T_N };
+  std::vector<cudaEvent_t> evs;
+  std::vector<int> evphase;
+  auto mark = [&](int ph) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e);
+    evs.push_back(e);
+    evphase.push_back(ph);
+  };
   int iter = 0;
   while (true) {
     if (!update_check(sc, P) || iter >= P.maxIteration) break;
+    mark(T_RMAT);
     predictor_setup(sc, P);
     const bool dinf = dual_infeasible(sc);
+    const bool lowp = S.mixed && mixed_gap(sc) >= S.mu_switch;
     // ---- predictor rMat / gVec (Newton::compute_rMat, Make_gVec)
     std::vector<const double*> Wv;
     for (SdpBlock& B : S.sdp) {
       const long long nn = (long long)B.n * B.n;
       k_axpby<<<nblk(nn), 256>>>(nn, B.R, sc.beta * sc.mu, B.Zi, -1.0, B.X);
       if (dinf) {
-        gemm(S, B.n, B.n, B.n, false, B.X, B.n, false, B.D, B.n, B.W1, B.n, 1.0, 0.0);
-        gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.XDZ, B.n, 1.0, 0.0);
+        gemm(S, B.n, B.n, B.n, false, B.X, B.n, false, B.D, B.n, B.W1, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
+        gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.XDZ, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
         k_axpby<<<nblk(nn), 256>>>(nn, B.W2, 1.0, B.R, -1.0, B.XDZ);
         Wv.push_back(B.W2);
       } else {
@@ -979,6 +1140,7 @@ int Solver::solve(const InitPoint* init)
       }
     }
     a_dot(S.g, S.rp, -1.0, Wv, Wl);
+    mark(T_BMAT);
     // ---- Schur complement (Newton::Make_bMat)
     cudaMemset(S.B, 0, (size_t)m * m * sizeof(double));
     for (SdpBlock& B : S.sdp) {
@@ -992,18 +1154,55 @@ int Solver::solve(const InitPoint* init)
         double* T = S.T;
         double* G = S.T + (size_t)F1_CHUNK * nn;
         k_f1_left<<<dim3(B.n, cnt), 256>>>(B.n, q0, B.f1, B.csc_cptr, B.csc_ptr, B.csc_row, B.csc_val, B.X, T);
-        gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn);
+        gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn, lowp);
         k_f1_dot<<<dim3(cnt, 16), 256>>>(B.nc, q0, B.f1, B.cons, B.ptr, B.row, B.col, B.val, B.nnz, G, B.n, S.B, m);
       }
     }
     if (nlp) k_lp_bmat<<<nlp, 256>>>(S.lpT_ptr, S.lpT_k, S.lpT_v, S.lpx, S.lpzi, S.B, m);
-    // ---- Cholesky with adjustment + solve (Newton::compute_DyVec)
-    if (cholesky_grid(S, S.B, m, true)) {
+    mark(T_CHOL);
+    // ---- Cholesky with adjustment + solve (Newton::compute_DyVec).  Mixed
+    // precision while mixed_gap >= mu_switch: FP32 factor of the FP64 Schur matrix
+    // with FP64 iterative refinement of dy; FP64 factor otherwise (and when
+    // the FP32 factorisation fails).
+    bool fp32_factor = false;
+    if (lowp) {
+      k_convert<float, double><<<nblk((long long)m * m), 256>>>((long long)m * m, S.B32, S.B);
+      fp32_factor = cholesky_grid_t<float>(S, S.B32, m, true, S.Linv32, S.T32, S.dinv32) == 0;
+    }
+    if (!fp32_factor && cholesky_grid(S, S.B, m, true, S.dinv)) {
       stats_.cholesky_failed = 1;
       break;
     }
+    auto solve64 = [&](double* x) {
+      if (m > SMALL_SOLVE) chol_solve_grid<double>(m, S.B, S.dinv, x);
+      else k_chol_solve<double><<<1, NT, cta::SD_DOUBLES * sizeof(double)>>>(m, S.B, x);
+    };
+    auto solve32 = [&](float* x) {
+      if (m > SMALL_SOLVE) chol_solve_grid<float>(m, S.B32, S.dinv32, x);
+      else k_chol_solve<float><<<1, NT, cta::SD_DOUBLES * sizeof(float)>>>(m, S.B32, x);
+    };
+    auto schur_solve = [&](double* x) {
+      if (!fp32_factor) {
+        solve64(x);
+        return;
+      }
+      double* rhs = S.res;
+      double* r = S.res + m;
+      cudaMemcpy(rhs, x, m * sizeof(double), cudaMemcpyDeviceToDevice);
+      k_convert<float, double><<<nblk(m), 256>>>(m, S.v32, x);
+      solve32(S.v32);
+      k_convert<double, float><<<nblk(m), 256>>>(m, x, S.v32);
+      for (int it = 0; it < 2; ++it) {  // x += B^{-1} (rhs - B x), correction in FP32
+        k_residual<<<nblk((long long)m * 32), 256>>>(m, S.B, x, rhs, r);
+        k_convert<float, double><<<nblk(m), 256>>>(m, S.v32, r);
+        solve32(S.v32);
+        k_add_f32<<<nblk(m), 256>>>(m, x, S.v32);
+      }
+    };
+    mark(T_SOLVE);
     cudaMemcpy(S.dy, S.g, m * sizeof(double), cudaMemcpyDeviceToDevice);
-    k_chol_solve<<<1, NT, cta::SD_DOUBLES * sizeof(double)>>>(m, S.B, S.dy);
+    schur_solve(S.dy);
+    mark(T_DXDZ);
 
     // ---- dZ and dX (compute_DzMat / compute_DxMat)
     auto direction = [&]() {
@@ -1013,8 +1212,8 @@ int Solver::solve(const InitPoint* init)
         else cudaMemset(B.dZ, 0, nn * sizeof(double));
         if (B.nc) k_sp_scatter<<<nblk((long long)B.nc * 32), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val,
                                                                     S.dy, -1.0, B.dZ, B.n);
-        gemm(S, B.n, B.n, B.n, false, B.X, B.n, false, B.dZ, B.n, B.W1, B.n, 1.0, 0.0);
-        gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.W2, B.n, 1.0, 0.0);
+        gemm(S, B.n, B.n, B.n, false, B.X, B.n, false, B.dZ, B.n, B.W1, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
+        gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.W2, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
         k_sym_diff<<<nblk(nn), 256>>>(B.n, B.dX, B.R, B.W2);
       }
       if (nlp) {
@@ -1041,8 +1240,8 @@ int Solver::solve(const InitPoint* init)
     Wv.clear();
     for (SdpBlock& B : S.sdp) {
       const long long nn = (long long)B.n * B.n;
-      gemm(S, B.n, B.n, B.n, false, B.dX, B.n, false, B.dZ, B.n, B.W1, B.n, 1.0, 0.0);
-      gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.W2, B.n, 1.0, 0.0);
+      gemm(S, B.n, B.n, B.n, false, B.dX, B.n, false, B.dZ, B.n, B.W1, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
+      gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.W2, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
       k_axpby_sub<<<nblk(nn), 256>>>(nn, B.R, sc.beta * sc.mu, B.Zi, -1.0, B.X, B.W2);
       if (dinf) {
         k_axpby<<<nblk(nn), 256>>>(nn, B.W1, 1.0, B.R, -1.0, B.XDZ);
@@ -1060,8 +1259,11 @@ int Solver::solve(const InitPoint* init)
       }
     }
     a_dot(S.dy, S.rp, -1.0, Wv, Wl);
-    k_chol_solve<<<1, NT, cta::SD_DOUBLES * sizeof(double)>>>(m, S.B, S.dy);
+    mark(T_SOLVE);
+    schur_solve(S.dy);
+    mark(T_DXDZ);
     direction();
+    mark(T_STEP);
 
     // ---- step length (StepLength::MehrotraCorrector)
     double minX = 1.0e50, minZ = 1.0e50;
@@ -1098,6 +1300,7 @@ int Solver::solve(const InitPoint* init)
       stats_.trace.insert(stats_.trace.end(), row, row + 8);
     }
 
+    mark(T_UPDATE);
     // ---- update (Solutions::update)
     for (SdpBlock& B : S.sdp) {
       const long long nn = (long long)B.n * B.n;
@@ -1111,6 +1314,7 @@ int Solver::solve(const InitPoint* init)
     k_axpby<<<nblk(m), 256>>>(m, S.y, 1.0, S.y, sc.alphaD, S.dy);
     if (cannot_move(sc)) break;
     if (!compute_inverse()) break;
+    mark(T_RES);
     // ---- residuals, mu, objectives, rho
     residuals();
     ip(2, mats(4), mats(0), S.lpC, S.lpx);
@@ -1137,6 +1341,7 @@ int Solver::solve(const InitPoint* init)
     after_update(sc, P, h[4], h[0], h[1], h[2], h[3], x0zM, xMz0);
     ++iter;
   }
+  mark(T_N);
   // final residuals (sdpa_solve.cpp:204), results
   residuals();
   read_scalars(S, h, 2);
@@ -1179,6 +1384,13 @@ int Solver::solve(const InitPoint* init)
   }
   stats_.solve_seconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  stats_.phase_seconds.assign(T_N, 0.0);
+  for (size_t q = 0; q + 1 < evs.size(); ++q) {
+    float ms = 0.0f;
+    if (evphase[q] < T_N && cudaEventElapsedTime(&ms, evs[q], evs[q + 1]) == cudaSuccess)
+      stats_.phase_seconds[evphase[q]] += ms / 1e3;
+  }
+  for (cudaEvent_t e : evs) cudaEventDestroy(e);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "solve");
   return SDPAB_OK;

@@ -48,6 +48,9 @@ struct SolveStats {
   int cholesky_failed = 0;
   int warm_start_rejected = 0;
   std::vector<double> trace;  // per iteration: mu, thetaP, thetaD, objP, objD, alphaP, alphaD, beta
+  // device seconds per phase: rMat+gVec, bMat, Cholesky, solves, dX/dZ,
+  // step length, update (inverses), residuals
+  std::vector<double> phase_seconds;
 };
 
 struct DevState;  // device buffers (single_engine.cu)
@@ -66,6 +69,14 @@ class Solver {
   // SDPA::solve (sdpa_solve.cpp:59-233); init may be NULL.
   int solve(const InitPoint* init);
   void release();
+  // SDPAB_PREC_FP64 (default) or SDPAB_PREC_MIXED: FP32 products and FP32
+  // Schur factor with FP64 refinement while the relative complementarity
+  // gap n*mu / max(1, mean |objective|) >= mu_switch (0 = 1e-2).
+  void set_precision(int mode, double mu_switch)
+  {
+    precision_ = mode;
+    mu_switch_ = mu_switch;
+  }
 
   const SolveStats& stats() const { return stats_; }
   // Results in the reference getters' layout (file block order, 1-based l).
@@ -76,6 +87,8 @@ class Solver {
 
  private:
   DevState* d_ = nullptr;
+  int precision_ = 0;
+  double mu_switch_ = 0.0;
   SolveStats stats_;
   std::vector<double> xvec_;
   std::vector<std::vector<double>> Xres_, Yres_;

@@ -37,6 +37,12 @@ class SDPA:
         for k, v in kw.items():
             setattr(self.params, k, v)
 
+    def setPrecision(self, mode: int, mu_switch: float = 0.0):
+        """0 = FP64, 1 = mixed (FP32 products and Schur factor + FP64 refinement while
+        the relative complementarity gap n*mu / max(1, mean |objective|) >= mu_switch;
+        0 = default 1e-2)."""
+        N.check(self._lib.sdpab_sdpa_set_precision(self._h, mode, mu_switch), "setPrecision")
+
     def readParameter(self, path: str):
         self.params = N.read_params(path)
 
@@ -118,6 +124,14 @@ class SDPA:
 
     def getResultYMat(self, l: int) -> np.ndarray:
         return self._block(l, 1)
+
+    PHASE_NAMES = ["rMat+gVec", "bMat", "Cholesky", "solve", "dXdZ", "StepLength", "update", "residuals"]
+
+    def phaseTimes(self) -> dict:
+        """Device seconds per solver phase (ComputeTime categories)."""
+        out = np.zeros(8)
+        N.check(self._lib.sdpab_sdpa_phase_times(self._h, out.ctypes.data_as(ctypes.c_void_p)), "phaseTimes")
+        return dict(zip(self.PHASE_NAMES, out.tolist()))
 
     def getDimacsError(self) -> np.ndarray:
         out = np.zeros(7)

@@ -157,13 +157,15 @@ class MPNN:
     def _sync_bf16(self):
         N.check(self.L.sdpab_mpnn_to_bf16(self.master.data_ptr(), self.wb.data_ptr(), None), "mpnn_to_bf16")
 
-    def forward(self, dg: DeviceGraphs):
+    def forward(self, dg: DeviceGraphs, act=None, out=None, stream=None):
         import torch
         n = dg.gb.num_nodes
-        act = torch.empty(int(self.L.sdpab_mpnn_act_floats(n)), dtype=torch.float32, device="cuda")
-        out = torch.empty(n, dtype=torch.float32, device="cuda")
+        if act is None:
+            act = torch.empty(int(self.L.sdpab_mpnn_act_floats(n)), dtype=torch.float32, device="cuda")
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device="cuda")
         N.check(self.L.sdpab_mpnn_forward(ctypes.byref(dg.c), self.wb.data_ptr(), act.data_ptr(),
-                                          out.data_ptr(), None), "mpnn_forward")
+                                          out.data_ptr(), stream), "mpnn_forward")
         return out
 
     def loss_grad(self, dg: DeviceGraphs):
@@ -191,6 +193,50 @@ class MPNN:
         import torch
         self.master.copy_(torch.from_numpy(np.asarray(w, np.float32)))
         self._sync_bf16()
+
+
+class WarmPipeline:
+    """Device-resident warm-started batched solve: network forward, proposal
+    kernel and the persistent solver, all on one stream (capturable in a CUDA
+    graph).  The graphs must be in the order of the packed batch."""
+
+    def __init__(self, model: MPNN, graphs: list[Graph], db: "B.DeviceBatch", margin: float = 0.0):
+        import torch
+        self.model, self.db = model, db
+        gb = make_graph_batch(graphs)
+        self.dg = DeviceGraphs(gb)
+        n = gb.num_nodes
+        assert n == db.P.nvec, "graph nodes must match the packed constraints"
+        fb = np.empty(n)
+        for q, g in enumerate(graphs):
+            o = gb.offsets[q]
+            d = gb.degree[o:o + g.n]
+            fb[o:o + g.n] = 0.01 * max(d.mean() / 4.0, 1e-3)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        self.degree, self.fallback = t(gb.degree.astype(np.float64)), t(fb)
+        self.act = torch.empty(int(N.lib().sdpab_mpnn_act_floats(n)), dtype=torch.float32, device="cuda")
+        self.r = torch.empty(n, dtype=torch.float32, device="cuda")
+        self.xprop = torch.zeros(n, dtype=torch.float64, device="cuda")
+        self.flag = torch.full((db.P.count,), INIT_DUAL, dtype=torch.int32, device="cuda")
+        db.init = N.BatchInit(self.flag.data_ptr(), self.xprop.data_ptr(), None, None, margin)
+        self.n = n
+
+    def run(self, precision=N.PREC_FP64, stream=None, ctas_per_sm=0):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream()
+        self.model.forward(self.dg, self.act, self.r, s.cuda_stream)
+        N.check(N.lib().sdpab_mpnn_propose_x(self.n, self.r.data_ptr(), self.degree.data_ptr(),
+                                             self.fallback.data_ptr(), self.xprop.data_ptr(), s.cuda_stream),
+                "mpnn_propose_x")
+        self.db.solve(precision=precision, stream=s, ctas_per_sm=ctas_per_sm)
+
+
+def default_model() -> MPNN:
+    """The network trained by sdpa_b200.train_warmstart (weights in sdpa_b200/data)."""
+    import os
+    m = MPNN(seed=0)
+    m.load(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "mpnn_maxcut.npy")))
+    return m
 
 
 def solve_graphs(graphs: list[Graph], precision=N.PREC_FP64, init_x: list | None = None, margin: float = 0.0):
@@ -237,26 +283,30 @@ def propose_x(model: MPNN, graphs: list[Graph]) -> list[np.ndarray]:
 
 def train(model: MPNN, graphs: list[Graph], targets: np.ndarray, masks: np.ndarray, epochs: int = 30,
           batch_graphs: int = 256, lr: float = 2e-3, seed: int = 0, log=None):
-    """Minibatch Adam over graphs; returns the per-epoch mean loss."""
+    """Minibatch Adam over graphs (cosine learning-rate decay).  The graphs
+    are grouped into fixed batches once, kept on the device, and the batch
+    order is shuffled every epoch.  Returns the per-epoch mean loss."""
     rng = np.random.default_rng(seed)
     offs = np.concatenate([[0], np.cumsum([g.n for g in graphs])])
-    hist = []
     idx = np.arange(len(graphs))
+    rng.shuffle(idx)
+    dev_batches = []
+    for b0 in range(0, len(idx), batch_graphs):
+        sel = idx[b0:b0 + batch_graphs]
+        gb = make_graph_batch([graphs[s] for s in sel])
+        t = np.concatenate([targets[offs[s]:offs[s + 1]] for s in sel])
+        m = np.concatenate([masks[offs[s]:offs[s + 1]] for s in sel])
+        dev_batches.append(DeviceGraphs(gb, m, t))
+    hist = []
+    order = np.arange(len(dev_batches))
     for ep in range(epochs):
-        rng.shuffle(idx)
-        tot, cnt = 0.0, 0
-        for b0 in range(0, len(idx), batch_graphs):
-            sel = idx[b0:b0 + batch_graphs]
-            gb = make_graph_batch([graphs[s] for s in sel])
-            t = np.concatenate([targets[offs[s]:offs[s + 1]] for s in sel])
-            m = np.concatenate([masks[offs[s]:offs[s + 1]] for s in sel])
-            dg = DeviceGraphs(gb, m, t)
-            cur_lr = lr * (0.5 * (1 + np.cos(np.pi * ep / max(epochs, 1))))
-            loss = model.loss_grad(dg)
+        rng.shuffle(order)
+        cur_lr = lr * (0.5 * (1 + np.cos(np.pi * ep / max(epochs, 1))))
+        losses = []
+        for b in order:
+            losses.append(model.loss_grad(dev_batches[b]))
             model.adam(lr=float(cur_lr))
-            tot += float(loss.item())
-            cnt += 1
-        hist.append(tot / max(cnt, 1))
+        hist.append(float(sum(float(x.item()) for x in losses) / max(len(losses), 1)))
         if log:
             log(f"epoch {ep} loss {hist[-1]:.5f}")
     return hist

@@ -90,6 +90,18 @@ PARAM_1E8 = """200 maxIteration
 """
 
 
+# epsilonStar 1e-11: the reference's own solution polished far past the
+# default stopping test, the optimum that paths which leave the reference's
+# iterate sequence (warm start, mixed precision) are compared against.
+PARAM_TIGHT = PARAM_1E8.replace("1.0E-8 epsilonStar", "1.0E-11 epsilonStar").replace(
+    "1.0E-8 epsilonDash", "1.0E-9 epsilonDash")
+
+
+def heldout_cases(count=64):
+    """MaxCut SDPs of the warm-start held-out seeds (300000.., n ~ U{50..200})."""
+    return [(f"ws{s}", inst.batch_maxcut(s, 50, 200)) for s in range(300000, 300000 + count)]
+
+
 def run_ref(instances, tmp, param=None, trace=False, procs=1, threads=1):
     paths = []
     for q, it in enumerate(instances):
@@ -178,6 +190,25 @@ def main():
                                    "alphaP", "alphaD", "beta"], "rows": tr["trace"],
                        "iterations": tr["iterations"]}, f, indent=1)
 
+        # tight solutions (and default ones for the held-out set)
+        tpath = os.path.join(tmp, "param_tight.sdpa")
+        with open(tpath, "w") as f:
+            f.write(PARAM_TIGHT)
+        tcases = cases + heldout_cases()
+        rt = run_ref([c[1] for c in tcases], tmp, param=tpath, procs=8)
+        ho = heldout_cases()
+        rd = run_ref([c[1] for c in ho], tmp, procs=8)
+        meta, arrays = {"heldout_default": {}, "tight": {}}, {}
+        for (name, it), r in zip(tcases, rt):
+            meta["tight"][name] = {k: r[k] for k in ("iterations", "phase", "primal_obj", "dual_obj")}
+            arrays[name + ".tight"] = r["xvec"]
+        for (name, it), r in zip(ho, rd):
+            meta["heldout_default"][name] = {k: r[k] for k in ("iterations", "phase", "primal_obj", "dual_obj")}
+            arrays[name + ".xvec"] = r["xvec"]
+        with open(os.path.join(HERE, "tight.json"), "w") as f:
+            json.dump(meta, f, indent=1)
+        np.savez_compressed(os.path.join(HERE, "tight.npz"), **arrays)
+
         if large:
             big = [("lt200", inst.lovasz_theta(200, 0.5, 1)), ("rnd2000", inst.random_sdp(seed=1))]
             meta, arrays = {}, {}
@@ -187,6 +218,9 @@ def main():
                                                 "seconds")}
                 arrays[name + ".xvec"] = r["xvec"]
                 print(name, meta[name], flush=True)
+            r = run_ref([big[0][1]], tmp, param=tpath, threads=os.cpu_count() or 8)[0]
+            meta["lt200.tight"] = {k: r[k] for k in ("iterations", "phase", "primal_obj", "dual_obj")}
+            arrays["lt200.tight"] = r["xvec"]
             with open(os.path.join(HERE, "large.json"), "w") as f:
                 json.dump(meta, f, indent=1)
             np.savez_compressed(os.path.join(HERE, "large.npz"), **arrays)

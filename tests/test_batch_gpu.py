@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from golden_util import GOLDEN, rel, small
+from golden_util import GOLDEN, rel, small, tight, x_within_reference_accuracy
 
 pytestmark = pytest.mark.gpu
 
@@ -82,3 +82,19 @@ def test_empty_and_oversized_instances():
     P.n[0] = 5000  # larger than the supported block order: rejected with a code
     with pytest.raises(Exception):
         batch.solve_host(P)
+
+
+def test_batched_mixed_precision_matches_reference():
+    """Mixed precision leaves the reference's iterate sequence: objectives
+    within the parity tolerance, x at least as close to the reference's
+    tight optimum as the reference's own x."""
+    meta, arr = small()
+    _, tz = tight()
+    names = [f"bmc{s}" for s in range(64)] + ["mc100", "mc20", "mc50w", "lt20", "lt40"]
+    P, r = _solve(names, precision=1)
+    for q, nm in enumerate(names):
+        g = meta[nm]
+        assert r.phase[q] == 7, (nm, r.phase[q])
+        assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
+        assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL, nm
+        assert x_within_reference_accuracy(r.x_of(P, q), arr[nm + ".xvec"], tz[nm + ".tight"]), nm

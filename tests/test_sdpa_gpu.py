@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from golden_util import GOLDEN, known_answers, large, rel, small
+from golden_util import GOLDEN, known_answers, large, rel, small, tight, x_within_reference_accuracy
 
 pytestmark = pytest.mark.gpu
 
@@ -148,3 +148,45 @@ def test_large_configs_match_reference(name):
     assert rel(s.getPrimalObj(), g["primal_obj"]) < OBJ_TOL
     assert rel(s.getDualObj(), g["dual_obj"]) < OBJ_TOL
     assert np.max(np.abs(s.getResultXVec() - arr[name + ".xvec"])) < X_TOL
+
+
+@pytest.mark.parametrize("name", ["mc100", "lt40", "rnd120", "ex2"])
+def test_mixed_precision_small(name):
+    """FP32 products / FP32 Schur factor + FP64 refinement (mixed) reach the
+    same optimum as the reference within the parity tolerance."""
+    from sdpa_b200.sdpa import SDPA
+    meta, arr = small()
+    inst = dict(MG.small_cases())[name]
+    s = SDPA()
+    s.setPrecision(1)
+    s.inputProblem(inst)
+    s.solve()
+    g = meta[name]
+    assert s.getPhaseString() == "pdOPT"
+    assert rel(s.getPrimalObj(), g["primal_obj"]) < OBJ_TOL
+    assert rel(s.getDualObj(), g["dual_obj"]) < OBJ_TOL
+    _, tz = tight()
+    assert x_within_reference_accuracy(s.getResultXVec(), arr[name + ".xvec"], tz[name + ".tight"])
+
+
+@pytest.mark.parametrize("name", ["lt200", "rnd2000"])
+def test_mixed_precision_large(name):
+    from sdpa_b200 import instances
+    from sdpa_b200.sdpa import SDPA
+    meta, arr = large()
+    if meta is None:
+        pytest.skip("large fixtures not generated")
+    inst = instances.lovasz_theta(200, 0.5, 1) if name == "lt200" else instances.random_sdp(seed=1)
+    s = SDPA()
+    s.setPrecision(1)
+    s.inputProblem(inst)
+    s.solve()
+    g = meta[name]
+    assert s.getPhaseString() == "pdOPT"
+    assert rel(s.getPrimalObj(), g["primal_obj"]) < OBJ_TOL
+    assert rel(s.getDualObj(), g["dual_obj"]) < OBJ_TOL
+    x = s.getResultXVec()
+    if name + ".tight" in arr.files:
+        assert x_within_reference_accuracy(x, arr[name + ".xvec"], arr[name + ".tight"])
+    else:  # no tight solution stored: the reference's x itself
+        assert np.max(np.abs(x - arr[name + ".xvec"])) < X_TOL

@@ -78,3 +78,34 @@ def test_trained_network_reduces_iterations():
     for q in range(Pc.count):
         assert rel(warm.primal_obj[q], cold.primal_obj[q]) < 1e-6
     assert warm.iterations.mean() < cold.iterations.mean() - 1.0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_shipped_network_warm_start_parity_heldout(precision):
+    """The shipped network (sdpa_b200/data) through the device pipeline
+    (network -> proposal kernel -> batched solver) on the held-out seeds:
+    pdOPT everywhere, objectives within 1e-6 of the reference, x at least as
+    close to the reference's tight optimum as the reference's own x, and
+    fewer iterations than the reference needed."""
+    import torch
+    from sdpa_b200 import batch as B
+    from sdpa_b200 import warmstart as W
+    from golden_util import tight, x_within_reference_accuracy
+    meta, tz = tight()
+    names = sorted(meta["heldout_default"], key=lambda k: int(k[2:]))
+    graphs = [W.batch_graph(int(nm[2:]), 50, 200) for nm in names]
+    P = B.pack([g.instance() for g in graphs])
+    db = B.DeviceBatch(P)
+    pipe = W.WarmPipeline(W.default_model(), graphs, db)
+    pipe.run(precision=precision)
+    torch.cuda.synchronize()
+    r = db.result()
+    iters_ref = []
+    for q, nm in enumerate(names):
+        g = meta["heldout_default"][nm]
+        iters_ref.append(g["iterations"])
+        assert r.phase[q] == 7, nm
+        assert rel(r.primal_obj[q], g["primal_obj"]) < 1e-6, nm
+        assert rel(r.dual_obj[q], g["dual_obj"]) < 1e-6, nm
+        assert x_within_reference_accuracy(r.x_of(P, q), tz[nm + ".xvec"], tz[nm + ".tight"]), nm
+    assert r.iterations.mean() < np.mean(iters_ref) - 2.0
