@@ -259,6 +259,9 @@ typedef struct sdpab_batch_config {
   int ctas_per_sm;             /* resident solver blocks per SM (0 = auto) */
   double mixed_switch_gap;     /* mixed mode: FP64 once nDim * mu / max(1, mean
                                   |objective|) < this (0 = 1e-2) */
+  int staging_doubles;         /* shared-memory staging of GEMM tiles and Lanczos
+                                  matrices per solver block, in doubles (0 = auto;
+                                  raised to the GEMM minimum of 3072) */
 } sdpab_batch_config;
 
 /* Solves a batch whose arrays (problem, init, result) are all DEVICE pointers,

@@ -50,7 +50,8 @@ class BatchResult(ctypes.Structure):
 
 
 class BatchConfig(ctypes.Structure):
-    _fields_ = [("precision", c_int), ("ctas_per_sm", c_int), ("mixed_switch_gap", c_double)]
+    _fields_ = [("precision", c_int), ("ctas_per_sm", c_int), ("mixed_switch_gap", c_double),
+                ("staging_doubles", c_int)]
 
 
 class SdpaInfo(ctypes.Structure):

@@ -32,11 +32,35 @@
 
 namespace sdpab {
 
-__host__ __device__ __forceinline__ int big_doubles(int nmax)
+// Dynamic shared memory of the solver block, in doubles / bytes, given the
+// staging area `gsm` (doubles) for GEMM tiles and Lanczos matrices.
+static __host__ __device__ long long fixed_smem_doubles(int nmax, int mmax)
 {
-  const int g = 2 * 16 * 96;  // GEMM staging (largest single-tile GEMM, n <= 96)
-  const int m2 = nmax * nmax;
-  return (m2 <= LANCZOS_SMEM_DOUBLES && m2 > g) ? m2 : g;
+  return cta::SD_DOUBLES + 4 * (NT / 32) + 4LL * mmax + eig_scratch_doubles(nmax);
+}
+
+static size_t smem_bytes_for(int nmax, int mmax, long long gsm)
+{
+  return (size_t)(gsm + fixed_smem_doubles(nmax, mmax)) * sizeof(double) + (size_t)mmax * sizeof(int) + 64;
+}
+
+// Staging area: at least the largest single-tile GEMM (n <= 96).  `want`
+// doubles when given (capped at what one block can have); by default both
+// Lanczos matrices (2 n^2) when they fit in LANCZOS_SMEM_DOUBLES, else one,
+// else the GEMM minimum.
+static long long staging_doubles(int nmax, int mmax, int want)
+{
+  const long long g = 2 * 16 * 96;
+  const long long m2 = (long long)nmax * nmax;
+  long long s;
+  if (want > 0) s = want;
+  else if (2 * m2 <= LANCZOS_SMEM_DOUBLES) s = 2 * m2;
+  else if (m2 <= LANCZOS_SMEM_DOUBLES) s = m2;
+  else s = g;
+  const long long cap = (227LL * 1024 - 512 - (long long)smem_bytes_for(nmax, mmax, 0)) / (long long)sizeof(double);
+  if (s > cap) s = cap;
+  s = s / 32 * 32;
+  return s > g ? s : g;
 }
 
 struct BatchArgs {
@@ -45,6 +69,7 @@ struct BatchArgs {
   sdpab_batch_result r;
   Params prm;
   const int* order;
+  int gsm_doubles;        // staging area (doubles) at the head of dynamic shared memory
   int mixed;             // SDPAB_PREC_MIXED: bulk GEMMs in FP32 while mixed_gap >= mu_switch
   double mu_switch;
   double* ws;
@@ -141,28 +166,18 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 {
   extern __shared__ double smem[];
   const int nmax = a.p.nmax, mmax = a.p.mmax;
-  const int gsm_doubles = big_doubles(nmax);
+  const int gsm_doubles = a.gsm_doubles;
   double* gsm = smem;                                   // GEMM staging / Lanczos matrix
   double* sD = gsm + gsm_doubles;                       // diagonal block NB*LDD
-  double* redbuf = sD + cta::SD_DOUBLES;             // 2 * NT/32
-  double* vy = redbuf + 2 * (NT / 32);                  // y   (mmax)
+  double* redbuf = sD + cta::SD_DOUBLES;                // 4 * NT/32
+  double* vy = redbuf + 4 * (NT / 32);                  // y   (mmax)
   double* vdy = vy + mmax;                              // dy  (mmax)
   double* vg = vdy + mmax;                              // g   (mmax)
   double* vrp = vg + mmax;                              // r_p (mmax)
-  EigScratch es;
-  es.q = vrp + mmax;
-  es.qold = es.q + nmax;
-  es.r = es.qold + nmax;
-  es.w = es.r + nmax;
-  es.t = es.w + nmax;
-  es.d = es.t + nmax;
-  es.e = es.d + TRI_MAX;
-  es.work = es.e + TRI_MAX;
-  es.M = es.work + 6 * TRI_MAX;
-  es.s_val = es.M + 400;
   cta::Reducer RD{redbuf, 0};
-  es.R = &RD;
-  int* s_nnz = (int*)(es.s_val + 4);                     // mmax ints
+  EigScratch es;
+  eig_scratch_carve(es, vrp + mmax, nmax, &RD);          // eig_scratch_doubles(nmax)
+  int* s_nnz = (int*)(vrp + mmax + eig_scratch_doubles(nmax));  // mmax ints
 
   __shared__ int s_inst, s_flag;
   __shared__ Scalars S;
@@ -493,8 +508,10 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 
       // ---- step length (StepLength::MehrotraCorrector)
       {
-        const double minX = min_eig(n, LXi, dX, W1, W2, gsm, gsm_doubles, es);
-        const double minZ = min_eig(n, LZi, dZ, W1, W2, gsm, gsm_doubles, es);
+        // R and XDZ are free here (both are rebuilt by the next predictor)
+        double mins[2];
+        min_eig_pair(n, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins);
+        const double minX = mins[0], minZ = mins[1];
         double CdX = c_dot(dX);
         double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);
         double xdz = cta::dot_mat<NT>(n, X, dZ, RD);
@@ -579,13 +596,6 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 
 // Host side -----------------------------------------------------------------
 
-static size_t smem_bytes(int nmax, int mmax)
-{
-  size_t d = (size_t)big_doubles(nmax) + cta::SD_DOUBLES + 2 * (NT / 32) + 4 * (size_t)mmax + 5 * (size_t)nmax + 2 * TRI_MAX +
-             6 * TRI_MAX + 400 + 4;
-  return d * sizeof(double) + (size_t)mmax * sizeof(int) + 64;
-}
-
 static long long ws_doubles(int nmax, int mmax)
 {
   long long nn = (long long)nmax * nmax;
@@ -606,7 +616,8 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   if (cudaGetDevice(&dev) != cudaSuccess) return set_error(SDPAB_ENODEV, "no CUDA device");
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t shm = smem_bytes(prob->nmax, prob->mmax);
+  const long long gsm = staging_doubles(prob->nmax, prob->mmax, cfg ? cfg->staging_doubles : 0);
+  const size_t shm = smem_bytes_for(prob->nmax, prob->mmax, gsm);
   if (shm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(batch_ipm_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shm);
@@ -631,6 +642,7 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.r = *res;
   memcpy(&a.prm, prm, sizeof(Params));
   a.order = order;
+  a.gsm_doubles = (int)gsm;
   a.mixed = (cfg && cfg->precision == SDPAB_PREC_MIXED) ? 1 : 0;
   a.mu_switch = (cfg && cfg->mixed_switch_gap > 0.0) ? cfg->mixed_switch_gap : 1.0e-2;
   a.ws = ws;
@@ -694,7 +706,8 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   }
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t shm = smem_bytes(prob->nmax, prob->mmax);
+  const long long gsm = staging_doubles(prob->nmax, prob->mmax, 0);
+  const size_t shm = smem_bytes_for(prob->nmax, prob->mmax, gsm);
   if (shm > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(batch_ipm_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shm);
@@ -715,6 +728,7 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.r = *res;
   memcpy(&a.prm, prm, sizeof(Params));
   a.order = order;
+  a.gsm_doubles = (int)gsm;
   a.mixed = 0;
   a.mu_switch = 1.0e-2;
   a.ws = base + head;

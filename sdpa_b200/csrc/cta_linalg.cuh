@@ -26,7 +26,7 @@ constexpr int SD_DOUBLES = NB * LDD + NB;
 // a slot that a slow thread is still reading (that thread must first pass
 // the next reduction's barrier).  All threads must call in the same order.
 struct Reducer {
-  double* buf;  // 2 * (NT/32) doubles
+  double* buf;  // 4 * (NT/32) doubles: two parities of 2 * (NT/32) slots
   int parity;
 };
 
@@ -34,7 +34,7 @@ template <int NT>
 __device__ __forceinline__ double block_sum(double v, Reducer& R)
 {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  double* slot = R.buf + R.parity * (NT / 32);
+  double* slot = R.buf + R.parity * (2 * (NT / 32));
   R.parity ^= 1;
   if ((threadIdx.x & 31) == 0) slot[threadIdx.x >> 5] = v;
   __syncthreads();
@@ -44,11 +44,34 @@ __device__ __forceinline__ double block_sum(double v, Reducer& R)
   return s;
 }
 
+// K <= 2 sums with one barrier (same slot discipline as block_sum).
+template <int NT, int K>
+__device__ __forceinline__ void block_sum_n(const double* v, double* out, Reducer& R)
+{
+  static_assert(K >= 1 && K <= 2, "block_sum_n: K <= 2");
+  double* slot = R.buf + R.parity * (2 * (NT / 32));
+  R.parity ^= 1;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    double x = v[j];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) slot[j * (NT / 32) + (threadIdx.x >> 5)] = x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) s += slot[j * (NT / 32) + w];
+    out[j] = s;
+  }
+}
+
 template <int NT>
 __device__ __forceinline__ double block_max(double v, Reducer& R)
 {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  double* slot = R.buf + R.parity * (NT / 32);
+  double* slot = R.buf + R.parity * (2 * (NT / 32));
   R.parity ^= 1;
   if ((threadIdx.x & 31) == 0) slot[threadIdx.x >> 5] = v;
   __syncthreads();
@@ -525,8 +548,11 @@ __device__ __forceinline__ int sturm_count(int k, const double* d, const double*
     cnt += ((pn < 0.0) != (p < 0.0)) ? 1 : 0;
     pm = p;
     p = pn;
-    const int ex = ilogb(p);
-    if (ex > 400 || ex < -400) {
+    // rescale the pair when it leaves [1e-150, 1e150] (a compare per step;
+    // the exponent arithmetic only on the rare rescale)
+    const double big = fmax(fabs(p), fabs(pm));
+    if (big > 1.0e150 || big < 1.0e-150) {
+      const int ex = ilogb(big);
       p = scalbn(p, -ex);
       pm = scalbn(pm, -ex);
     }
@@ -534,13 +560,22 @@ __device__ __forceinline__ int sturm_count(int k, const double* d, const double*
   return cnt;
 }
 
-// Smallest eigenvalue of a symmetric tridiagonal (d, e) of order k.  Warp
-// multisection of the Gershgorin interval (33 parts per round) until the
-// bracket is narrow, then Newton steps on det(T - xI) (its smallest root is
-// approached monotonically from the left), each kept inside the bracket,
-// until the step is below one ulp.  Called by one full warp; every lane
-// returns the value.
-static __device__ double tridiag_min_eig_warp(int k, const double* d, const double* e)
+// Smallest eigenvalue of a symmetric tridiagonal (d, e) of order k, and the
+// magnitude of the last component of its unit eigenvector (the Lanczos error
+// estimate).  Warp multisection until the bracket is narrow, then Newton
+// steps on f(x) = det(T - xI) (its smallest root is approached monotonically
+// from the left), each kept inside the bracket, until the step is below one
+// ulp of the result (or of 1e-2 of the matrix scale for a result near zero).
+// The eigenvector component comes from the same recurrences: for an
+// eigenvalue lam of an unreduced tridiagonal, u_k^2 = -P_{k-1}(lam) / P_k'(lam)
+// with P_j the leading principal minors of T - lam I, which Newton has just
+// evaluated.  `upper` is a known upper bound of the result (the smallest Ritz
+// value of a leading principal submatrix, by interlacing; 1e300 for none):
+// the first round then probes geometrically spaced points below it, which
+// brackets the value in one round when it has moved little.  Called by one
+// full warp; every lane returns the same values.
+static __device__ double tridiag_min_eig_warp(int k, const double* d, const double* e, double upper,
+                                              double* ulast)
 {
   const int lane = threadIdx.x & 31;
   double lo = 1.0e300, hi = -1.0e300;
@@ -552,7 +587,24 @@ static __device__ double tridiag_min_eig_warp(int k, const double* d, const doub
   const double span = fmax(fabs(lo), fabs(hi));
   lo -= 1.0e-15 * span + 1.0e-300;
   hi += 1.0e-15 * span + 1.0e-300;
+  if (upper < hi && upper > lo) {
+    // probes p_0 = upper + h (above the value), p_l = upper + h - h 4^l
+    const double h = 1.0e-12 * fmax(fabs(upper), 1.0e-3 * span) + 1.0e-300;
+    const double x = (lane == 0) ? upper + h : upper + h - h * exp2(2.0 * lane);
+    const bool below = (x > lo) && sturm_count(k, d, e, x) >= 1;
+    const unsigned ball = __ballot_sync(0xffffffffu, below);
+    if (ball & 1u) {  // the bound holds: bracket between the last probe with
+                      // an eigenvalue below it and the next one
+      const int f = (ball == 0xffffffffu) ? 32 : __ffs(~ball) - 1;  // first probe without (32: none)
+      const double xhi = __shfl_sync(0xffffffffu, x, (f > 0 && f < 32) ? f - 1 : 31);
+      const double xlo = __shfl_sync(0xffffffffu, x, (f < 32) ? f : 31);
+      hi = fmin(hi, xhi);
+      if (f < 32) lo = fmax(lo, xlo);
+    }
+  }
+  const double floor_abs = 1.0e-12 * span + 1.0e-300;
   for (int round = 0; round < 24; ++round) {
+    if (hi - lo <= 1.0e-7 * fmax(fabs(lo), fabs(hi)) + floor_abs) break;
     const double w = (hi - lo) / 33.0;
     const double x = lo + w * (lane + 1);
     const int c = sturm_count(k, d, e, x);
@@ -562,12 +614,12 @@ static __device__ double tridiag_min_eig_warp(int k, const double* d, const doub
     const double nhi = (f < 32) ? lo + w * (f + 1) : hi;
     lo = nlo;
     hi = nhi;
-    if (hi - lo <= 1.0e-7 * fmax(fabs(lo), fabs(hi)) + 1.0e-300) break;
   }
   // Newton on f(x) = det(T - xI) from the left end of the bracket, with
   // P_{i+1} = (d_i - x) P_i - e^2 P_{i-1} and its derivative
   // D_{i+1} = -P_i + (d_i - x) D_i - e^2 D_{i-1}, rescaled together.
-  double x = lo;
+  double x = lo, Plast = 0.0, Dlast = 0.0;
+  const double tol_abs = 2.2e-18 * span;
   for (int it = 0; it < 20; ++it) {
     double Pm = 1.0, P = d[0] - x, Dm = 0.0, Dv = -1.0;
     for (int i = 1; i < k; ++i) {
@@ -576,80 +628,28 @@ static __device__ double tridiag_min_eig_warp(int k, const double* d, const doub
       const double Pn = dx * P - e2 * Pm;
       const double Dn = -P + dx * Dv - e2 * Dm;
       Pm = P; P = Pn; Dm = Dv; Dv = Dn;
-      const int ex = ilogb(fmax(fabs(P), fabs(Dv)));
-      if (ex > 400 || ex < -400) {
+      const double big = fmax(fmax(fabs(P), fabs(Dv)), fmax(fabs(Pm), fabs(Dm)));
+      if (big > 1.0e150 || big < 1.0e-150) {
+        const int ex = ilogb(big);
         P = scalbn(P, -ex); Pm = scalbn(Pm, -ex); Dv = scalbn(Dv, -ex); Dm = scalbn(Dm, -ex);
       }
     }
+    Plast = Pm;  // P_{k-1}(x) and P_k'(x), same scale
+    Dlast = Dv;
     if (!(Dv != 0.0) || P != P || Dv != Dv) break;
     const double xn = x - P / Dv;
     if (!(xn >= lo) || !(xn <= hi)) break;
-    if (fabs(xn - x) <= 2.2e-16 * fabs(xn)) { x = xn; break; }
+    if (fabs(xn - x) <= fmax(2.2e-16 * fabs(xn), tol_abs)) { x = xn; break; }
     x = xn;
   }
+  double u2 = 1.0;
+  if (k > 1) {
+    u2 = (Dlast != 0.0) ? -Plast / Dlast : 1.0;
+    if (!(u2 >= 0.0)) u2 = 0.0;  // rounding (or NaN) below zero
+    if (u2 > 1.0) u2 = 1.0;
+  }
+  *ulast = sqrt(u2);
   return x;
-}
-
-// Last component (index k-1) of the unit eigenvector of the tridiagonal (d, e)
-// for eigenvalue lam: two steps of inverse iteration on T - (lam - tiny) I
-// with partial pivoting (pivot reciprocals computed once).  Called by one
-// thread; work needs 6*k doubles; k <= 64.
-static __device__ double tridiag_evec_last(int k, const double* d, const double* e, double lam, double* work)
-{
-  if (k <= 1) return 1.0;
-  if (k > 64) k = 64;
-  double* a = work;           // sub-diagonal (row i, column i-1)
-  double* b = work + k;       // diagonal, then its reciprocal
-  double* c = work + 2 * k;   // first super-diagonal
-  double* c2 = work + 3 * k;  // second super-diagonal (fill-in of pivoting)
-  double* v = work + 4 * k;
-  double* pl = work + 5 * k;  // multipliers
-  unsigned long long swp = 0ull;
-  double span = 0.0;
-  for (int i = 0; i < k; ++i) span = fmax(span, fabs(d[i]) + ((i < k - 1) ? fabs(e[i]) : 0.0));
-  const double shift = lam - 1.0e-13 * (span + 1.0e-300);
-  for (int i = 0; i < k; ++i) {
-    a[i] = (i > 0) ? e[i - 1] : 0.0;
-    b[i] = d[i] - shift;
-    c[i] = (i < k - 1) ? e[i] : 0.0;
-    c2[i] = 0.0;
-    v[i] = 1.0;
-  }
-  for (int i = 0; i < k - 1; ++i) {
-    if (fabs(a[i + 1]) > fabs(b[i])) {  // swap rows i and i+1
-      double t;
-      t = b[i]; b[i] = a[i + 1]; a[i + 1] = t;
-      t = c[i]; c[i] = b[i + 1]; b[i + 1] = t;
-      t = c2[i]; c2[i] = c[i + 1]; c[i + 1] = t;
-      swp |= (1ull << i);
-    }
-    const double rinv = 1.0 / ((b[i] != 0.0) ? b[i] : 1.0e-300);
-    b[i] = rinv;
-    const double l = a[i + 1] * rinv;
-    pl[i] = l;
-    b[i + 1] -= l * c[i];
-    c[i + 1] -= l * c2[i];
-  }
-  b[k - 1] = 1.0 / ((b[k - 1] != 0.0) ? b[k - 1] : 1.0e-300);
-  for (int itn = 0; itn < 2; ++itn) {
-    for (int i = 0; i < k - 1; ++i) {
-      if (swp & (1ull << i)) { const double t = v[i]; v[i] = v[i + 1]; v[i + 1] = t; }
-      v[i + 1] -= pl[i] * v[i];
-    }
-    double nrm = 0.0;
-    for (int i = k - 1; i >= 0; --i) {
-      double s = v[i];
-      if (i + 1 < k) s -= c[i] * v[i + 1];
-      if (i + 2 < k) s -= c2[i] * v[i + 2];
-      v[i] = s * b[i];
-      nrm = fmax(nrm, fabs(v[i]));
-    }
-    const double inv = 1.0 / nrm;
-    for (int i = 0; i < k; ++i) v[i] *= inv;
-  }
-  double s2 = 0.0;
-  for (int i = 0; i < k; ++i) s2 += v[i] * v[i];
-  return v[k - 1] * rsqrt(s2);
 }
 
 }  // namespace cta

@@ -14,99 +14,208 @@ constexpr int TRI_MAX = 64;  // Lanczos tridiagonal order bound (sqrt(n)+11 for 
 // blocks run the Lanczos matvecs from global memory.
 constexpr int LANCZOS_SMEM_DOUBLES = 12288;
 
-struct EigScratch {
-  double *q, *qold, *r, *w, *t;   // Lanczos vectors (n)
-  double *d, *e, *work;           // tridiagonal (TRI_MAX), work 6*TRI_MAX
-  double* M;                      // dense n <= 20 matrix (400)
-  cta::Reducer* R;
-  double* s_val;                  // broadcast slot
+// One Lanczos process: vectors (n), tridiagonal (d, e), work (6 TRI_MAX;
+// the dense n <= 20 path keeps its Householder vectors there) and the slots
+// warp j publishes its Ritz results in.
+struct LanczosVec {
+  double *q, *qold, *r, *w;
+  double *d, *e, *work;
+  double* val;  // [0] Ritz minimum, [1] last eigenvector component, [2] fresh flag
 };
 
-// Lal::getMinEigen (sdpa_linear.cpp:29-143): Lanczos on M = L D L^T with
-// the reference's start vector (all ones), stopping rule and error
-// correction.  M is formed once by two GEMMs (the reference applies L^T, D, L
-// to each Lanczos vector; the products agree to rounding), so each step is a
-// single coalesced matvec.  The tridiagonal eigen-solve (dsteqr in the
-// reference) is a warp multisection for the smallest Ritz value plus inverse
-// iteration for the last component of its eigenvector.
-static __device__ double lanczos_min_eig(int n, const double* M, EigScratch& s)
+struct EigScratch {
+  LanczosVec v[2];  // up to two processes run in lockstep (X and Z)
+  double* M;        // dense n <= 20 matrix (400)
+  cta::Reducer* R;
+};
+
+// Shared-memory doubles of an EigScratch for blocks of order <= nmax;
+// `sets` = number of Lanczos processes that may run together (1 or 2).
+__host__ __device__ inline long long eig_scratch_doubles(int nmax, int sets = 2)
+{
+  return (long long)sets * (4LL * nmax + 8 * TRI_MAX + 4) + 400;
+}
+
+static __device__ inline void eig_scratch_carve(EigScratch& s, double* p, int nmax, cta::Reducer* R,
+                                                int sets = 2)
+{
+  s.v[1] = LanczosVec{};
+  for (int j = 0; j < sets; ++j) {
+    LanczosVec& v = s.v[j];
+    v.q = p; p += nmax;
+    v.qold = p; p += nmax;
+    v.r = p; p += nmax;
+    v.w = p; p += nmax;
+    v.d = p; p += TRI_MAX;
+    v.e = p; p += TRI_MAX;
+    v.work = p; p += 6 * TRI_MAX;
+    v.val = p; p += 4;
+  }
+  s.M = p;
+  s.R = R;
+}
+
+// Lal::getMinEigen (sdpa_linear.cpp:29-143) for NM independent matrices in
+// lockstep: Lanczos on each M_j = L D L^T with the reference's start vector
+// (all ones), stopping rule and error correction, each process advancing
+// only while its own stopping test says so.  Running the X and Z step-length
+// problems together shares every block barrier between them and lets warp j
+// solve process j's tridiagonal while warp 1-j solves the other's.  M_j is
+// formed beforehand by two GEMMs (the reference applies L^T, D, L to each
+// Lanczos vector; the products agree to rounding), so each step is one
+// coalesced matvec.  The tridiagonal eigen-solve (dsteqr in the reference) is
+// a warp multisection + Newton for the smallest Ritz value, which also yields
+// the last component of its eigenvector.
+template <int NM>
+static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, EigScratch& s,
+                                                          double* out)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  // every thread owns the vector entries i = tid, tid + NT, ...
-  for (int i = tid; i < n; i += NT) { s.q[i] = 0.0; s.r[i] = 1.0; }
-  if (wid == 0) {
-    for (int i = lane; i < TRI_MAX; i += 32) { s.d[i] = 1.0e50; s.e[i] = 0.0; }
-  }
-  double beta = sqrt((double)n);
-  double mn = 1.0e51, mn_old = 1.0e52, err = 1.0e10;
-  int k = 0, kk = 0;
+  constexpr int NW = NT / 32;
+  double beta[NM], mn[NM], mn_old[NM], err[NM];
+  int k[NM], kk[NM];
+  bool act[NM];
   const double sqn = sqrt((double)n);
-  while (k < n && k < sqn + 10 && k < TRI_MAX - 1 && beta > 1.0e-16 &&
-         (fabs(mn - mn_old) > 1.0e-5 * fabs(mn) + 1.0e-8 ||
-          fabs(err * beta) > 1.0e-2 * fabs(mn) + 1.0e-4)) {
-    const double ib = 1.0 / beta;
-    for (int i = tid; i < n; i += NT) { s.qold[i] = s.q[i]; s.q[i] = s.r[i] * ib; }
+#pragma unroll
+  for (int j = 0; j < NM; ++j) {
+    LanczosVec& v = s.v[j];
+    for (int i = tid; i < n; i += NT) { v.q[i] = 0.0; v.r[i] = 1.0; }
+    for (int i = tid; i < TRI_MAX; i += NT) { v.d[i] = 1.0e50; v.e[i] = 0.0; }
+    beta[j] = sqn;
+    mn[j] = 1.0e51;
+    mn_old[j] = 1.0e52;
+    err[j] = 1.0e10;
+    k[j] = kk[j] = 0;
+  }
+  for (;;) {
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      act[j] = k[j] < n && k[j] < sqn + 10 && k[j] < TRI_MAX - 1 && beta[j] > 1.0e-16 &&
+               (fabs(mn[j] - mn_old[j]) > 1.0e-5 * fabs(mn[j]) + 1.0e-8 ||
+                fabs(err[j] * beta[j]) > 1.0e-2 * fabs(mn[j]) + 1.0e-4);
+      any |= act[j];
+    }
+    if (!any) break;
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      if (!act[j]) continue;
+      LanczosVec& v = s.v[j];
+      const double ib = 1.0 / beta[j];
+      for (int i = tid; i < n; i += NT) { v.qold[i] = v.q[i]; v.q[i] = v.r[i] * ib; }
+    }
     __syncthreads();
-    // w = M q: each warp takes 4 columns at a time (M column i dotted with q)
-    double part = 0.0;
-    for (int i0 = wid * 4; i0 < n; i0 += NT / 8) {
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      const double* c0 = M + (size_t)n * i0;
-      for (int kx = lane; kx < n; kx += 32) {
-        const double qk = s.q[kx];
-        a0 += c0[kx] * qk;
-        if (i0 + 1 < n) a1 += c0[kx + n] * qk;
-        if (i0 + 2 < n) a2 += c0[kx + 2 * n] * qk;
-        if (i0 + 3 < n) a3 += c0[kx + 3 * n] * qk;
+    // w_j = M_j q_j: each warp takes CW columns of every active matrix per
+    // pass and issues all their loads (CW x 4 per lane and matrix for
+    // n <= 128) before the FMAs, so the latency of a column is paid once per
+    // pass.
+    constexpr int CW = (NM == 2) ? 2 : 4;
+    double part[NM];
+#pragma unroll
+    for (int j = 0; j < NM; ++j) part[j] = 0.0;
+    for (int i0 = wid * CW; i0 < n; i0 += CW * NW) {
+      double acc[NM][CW];
+#pragma unroll
+      for (int j = 0; j < NM; ++j)
+#pragma unroll
+        for (int c = 0; c < CW; ++c) acc[j][c] = 0.0;
+      for (int kx0 = 0; kx0 < n; kx0 += 128) {
+        double qv[NM][4], mv[NM][CW][4];
+#pragma unroll
+        for (int j = 0; j < NM; ++j) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int kx = kx0 + lane + 32 * u;
+            qv[j][u] = (act[j] && kx < n) ? s.v[j].q[kx] : 0.0;
+#pragma unroll
+            for (int c = 0; c < CW; ++c)
+              mv[j][c][u] = (act[j] && kx < n && i0 + c < n) ? Ms[j][kx + (size_t)n * (i0 + c)] : 0.0;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < NM; ++j)
+#pragma unroll
+          for (int c = 0; c < CW; ++c)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[j][c] += mv[j][c][u] * qv[j][u];
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
-        a3 += __shfl_xor_sync(0xffffffffu, a3, o);
-      }
-      if (lane < 4 && i0 + lane < n) {
-        const double wv = (lane == 0) ? a0 : (lane == 1) ? a1 : (lane == 2) ? a2 : a3;
-        s.w[i0 + lane] = wv;
-        part += s.q[i0 + lane] * wv;
+#pragma unroll
+      for (int j = 0; j < NM; ++j) {
+        double wv = 0.0;
+#pragma unroll
+        for (int c = 0; c < CW; ++c) {
+          for (int o = 16; o > 0; o >>= 1) acc[j][c] += __shfl_xor_sync(0xffffffffu, acc[j][c], o);
+          if (lane == c) wv = acc[j][c];
+        }
+        if (act[j] && lane < CW && i0 + lane < n) {
+          s.v[j].w[i0 + lane] = wv;
+          part[j] += s.v[j].q[i0 + lane] * wv;
+        }
       }
     }
-    const double alpha = cta::block_sum<NT>(part, *s.R);  // barrier also publishes w
-    double rpart = 0.0;
-    for (int i = tid; i < n; i += NT) {
-      const double rv = (s.w[i] - alpha * s.q[i]) - beta * s.qold[i];
-      s.r[i] = rv;
-      rpart += rv * rv;
+    double alpha[NM];
+    cta::block_sum_n<NT, NM>(part, alpha, *s.R);  // the barrier also publishes w
+    double rpart[NM];
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      rpart[j] = 0.0;
+      if (!act[j]) continue;
+      LanczosVec& v = s.v[j];
+      for (int i = tid; i < n; i += NT) {
+        const double rv = (v.w[i] - alpha[j] * v.q[i]) - beta[j] * v.qold[i];
+        v.r[i] = rv;
+        rpart[j] += rv * rv;
+      }
     }
-    if (wid == 0) {
-      if (lane == 0) s.d[k] = alpha;
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      if (wid != j || !act[j]) continue;
+      LanczosVec& v = s.v[j];
+      const int kj = k[j];
+      if (lane == 0) v.d[kj] = alpha[j];
       __syncwarp();
-      if (kk >= sqrt((double)k) || k == n - 1 || k > sqrt((double)n + 9)) {
-        const double lam = cta::tridiag_min_eig_warp(k + 1, s.d, s.e);
+      if (kk[j] >= sqrt((double)kj) || kj == n - 1 || kj > sqrt((double)n + 9)) {
+        double ul;
+        const double lam = cta::tridiag_min_eig_warp(kj + 1, v.d, v.e, mn[j], &ul);
         if (lane == 0) {
-          s.s_val[0] = lam;
-          s.s_val[1] = cta::tridiag_evec_last(k + 1, s.d, s.e, lam, s.work);
-          s.s_val[2] = 1.0;
+          v.val[0] = lam;
+          v.val[1] = ul;
+          v.val[2] = 1.0;
         }
       } else if (lane == 0) {
-        s.s_val[2] = 0.0;
+        v.val[2] = 0.0;
       }
     }
-    // the barrier of this reduction also publishes warp 0's eigen result
-    const double rr = cta::block_sum<NT>(rpart, *s.R);
-    if (s.s_val[2] != 0.0) {
-      kk = 0;
-      mn_old = mn;
-      mn = s.s_val[0];
-      err = s.s_val[1];
+    // the barrier of this reduction also publishes the warps' eigen results
+    double rr[NM];
+    cta::block_sum_n<NT, NM>(rpart, rr, *s.R);
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      if (!act[j]) continue;
+      LanczosVec& v = s.v[j];
+      if (v.val[2] != 0.0) {
+        kk[j] = 0;
+        mn_old[j] = mn[j];
+        mn[j] = v.val[0];
+        err[j] = v.val[1];
+      }
+      beta[j] = sqrt(rr[j]);
+      if (tid == 0) v.e[k[j]] = beta[j];
+      ++k[j];
+      ++kk[j];
     }
-    beta = sqrt(rr);
-    if (tid == 0) s.e[k] = beta;
-    ++k;
-    ++kk;
   }
   __syncthreads();
-  return mn - fabs(err * beta);
+#pragma unroll
+  for (int j = 0; j < NM; ++j) out[j] = mn[j] - fabs(err[j] * beta[j]);
+}
+
+static __device__ double lanczos_min_eig(int n, const double* M, EigScratch& s)
+{
+  const double* Ms[1] = {M};
+  double out[1];
+  lanczos_min_eig_multi<1>(n, Ms, s, out);
+  return out[0];
 }
 
 // n <= 20: minimum eigenvalue of the lower triangle of M = L D L^T
@@ -116,6 +225,7 @@ static __device__ double lanczos_min_eig(int n, const double* M, EigScratch& s)
 static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
 {
   const int tid = threadIdx.x, lane = tid & 31;
+  LanczosVec& lv = s.v[0];
   double* M = s.M;  // n x n symmetric copy of the lower triangle
   for (int t = tid; t < n * n; t += NT) {
     const int i = t % n, j = t / n;
@@ -123,8 +233,8 @@ static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
   }
   __syncthreads();
   if (tid < 32) {
-    double* v = s.work;        // n
-    double* p = s.work + 32;   // n
+    double* v = lv.work;        // n
+    double* p = lv.work + 32;   // n
     for (int k = 0; k + 2 < n; ++k) {
       const int len = n - k - 1;
       const double x = (lane < len) ? M[(k + 1 + lane) + n * k] : 0.0;
@@ -134,7 +244,7 @@ static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
       const double alpha = (x0 >= 0.0) ? -sqrt(nrm2) : sqrt(nrm2);
       const double vi = (lane == 0) ? x - alpha : x;
       const double vn2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
-      if (lane == 0) s.e[k] = (nrm2 > 0.0) ? alpha : 0.0;
+      if (lane == 0) lv.e[k] = (nrm2 > 0.0) ? alpha : 0.0;
       if (!(vn2 > 0.0)) { __syncwarp(); continue; }
       if (lane < len) v[lane] = vi;
       __syncwarp();
@@ -156,14 +266,15 @@ static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
       }
       __syncwarp();
     }
-    if (lane < n) s.d[lane] = M[lane + n * lane];
-    if (n >= 2 && lane == 0) s.e[n - 2] = M[(n - 1) + n * (n - 2)];
+    if (lane < n) lv.d[lane] = M[lane + n * lane];
+    if (n >= 2 && lane == 0) lv.e[n - 2] = M[(n - 1) + n * (n - 2)];
     __syncwarp();
-    const double lam = cta::tridiag_min_eig_warp(n, s.d, s.e);
-    if (lane == 0) s.s_val[0] = lam;
+    double ul;
+    const double lam = cta::tridiag_min_eig_warp(n, lv.d, lv.e, 1.0e300, &ul);
+    if (lane == 0) lv.val[0] = lam;
   }
   __syncthreads();
-  const double r = s.s_val[0];
+  const double r = lv.val[0];
   __syncthreads();
   return r;
 }
@@ -185,5 +296,37 @@ static __device__ double min_eig(int n, const double* L, const double* D, double
   return lanczos_min_eig(n, M, s);
 }
 
+
+// Both step-length eigenvalues of an iteration, lambda_min(Lx Dx Lx^T) and
+// lambda_min(Lz Dz Lz^T), with the two Lanczos processes in lockstep.
+// Wx1, Wx2, Wz1, Wz2: n x n scratch (Wx2 and Wz2 receive the formed
+// matrices).  The matrices are staged in shared memory while they fit.
+static __device__ void min_eig_pair(int n, const double* Lx, const double* Dx, const double* Lz,
+                                    const double* Dz, double* Wx1, double* Wx2, double* Wz1, double* Wz2,
+                                    double* gsm, int gsm_doubles, EigScratch& s, double* out)
+{
+  cta::gemm<NT>(n, false, Dx, n, true, Lx, n, Wx1, n, 1.0, 0.0, gsm);
+  cta::gemm<NT>(n, false, Lx, n, false, Wx1, n, Wx2, n, 1.0, 0.0, gsm);
+  cta::gemm<NT>(n, false, Dz, n, true, Lz, n, Wz1, n, 1.0, 0.0, gsm);
+  cta::gemm<NT>(n, false, Lz, n, false, Wz1, n, Wz2, n, 1.0, 0.0, gsm);
+  if (n <= 20) {
+    out[0] = dense_min_eig(n, Wx2, s);
+    out[1] = dense_min_eig(n, Wz2, s);
+    return;
+  }
+  const double* Ms[2] = {Wx2, Wz2};
+  const int nn = n * n;
+  if (2 * nn <= gsm_doubles) {
+    for (int t = threadIdx.x; t < nn; t += NT) { gsm[t] = Wx2[t]; gsm[nn + t] = Wz2[t]; }
+    __syncthreads();
+    Ms[0] = gsm;
+    Ms[1] = gsm + nn;
+  } else if (nn <= gsm_doubles) {
+    for (int t = threadIdx.x; t < nn; t += NT) gsm[t] = Wx2[t];
+    __syncthreads();
+    Ms[0] = gsm;
+  }
+  lanczos_min_eig_multi<2>(n, Ms, s, out);
+}
 
 }  // namespace sdpab

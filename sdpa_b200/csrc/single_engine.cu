@@ -443,20 +443,10 @@ __global__ void k_residual(int m, const double* B, const double* x, const double
 __global__ void __launch_bounds__(NT) k_min_eig(int n, const double* M, double* out)
 {
   extern __shared__ double smem[];
-  __shared__ double redbuf[2 * (NT / 32)];
+  __shared__ double redbuf[4 * (NT / 32)];
   cta::Reducer RD{redbuf, 0};
   EigScratch es;
-  es.q = smem;
-  es.qold = es.q + n;
-  es.r = es.qold + n;
-  es.w = es.r + n;
-  es.t = es.w + n;
-  es.d = es.t + n;
-  es.e = es.d + TRI_MAX;
-  es.work = es.e + TRI_MAX;
-  es.M = es.work + 6 * TRI_MAX;
-  es.s_val = es.M + 400;
-  es.R = &RD;
+  eig_scratch_carve(es, smem, n, &RD, 1);
   const double v = (n > 20) ? lanczos_min_eig(n, M, es) : dense_min_eig(n, M, es);
   if (threadIdx.x == 0) *out = v;
 }
@@ -1268,7 +1258,7 @@ int Solver::solve(const InitPoint* init)
     // ---- step length (StepLength::MehrotraCorrector)
     double minX = 1.0e50, minZ = 1.0e50;
     for (SdpBlock& B : S.sdp) {
-      const size_t shm = (size_t)(5 * B.n + 2 * TRI_MAX + 6 * TRI_MAX + 400 + 4) * sizeof(double);
+      const size_t shm = (size_t)eig_scratch_doubles(B.n, 1) * sizeof(double);
       gemm(S, B.n, B.n, B.n, false, B.dX, B.n, true, B.LXi, B.n, B.W1, B.n, 1.0, 0.0);
       gemm(S, B.n, B.n, B.n, false, B.LXi, B.n, false, B.W1, B.n, B.W2, B.n, 1.0, 0.0);
       k_min_eig<<<1, NT, shm>>>(B.n, B.W2, S.sc + 10);
