@@ -206,6 +206,7 @@ def main():
     ap.add_argument("--count", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--ctas-per-sm", type=int, default=0, help="fixed launch shape (0 = autotune)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -239,13 +240,14 @@ def main():
 
     # ---- plain FP64 path (standard start): the denominator of the headline ratio
     db0 = batch.DeviceBatch(P)
-    tune0 = autotune.tune(db0, N.PREC_FP64, stream=stream)
+    cand = (args.ctas_per_sm,) if args.ctas_per_sm > 0 else (1, 2)
+    tune0 = autotune.tune(db0, N.PREC_FP64, stream=stream, candidates=cand)
     c0 = tune0["best"]
     run0 = lambda: db0.solve(precision=N.PREC_FP64, stream=stream, ctas_per_sm=c0)
     # ---- headline path: precision + learned warm start
     dbh = batch.DeviceBatch(P)
     pipe = W.WarmPipeline(W.default_model(), graphs, dbh) if args.warm else None
-    tuneh = autotune.tune(dbh, prec, stream=stream,
+    tuneh = autotune.tune(dbh, prec, stream=stream, candidates=cand,
                           run=(lambda c: pipe.run(precision=prec, stream=stream, ctas_per_sm=c)) if pipe else None)
     ch = tuneh["best"]
     if pipe is not None:

@@ -1,4 +1,5 @@
-"""Builds the native library libsdpa_b200.so in-tree (sdpa_b200/_lib/).
+"""Builds the native library libsdpa_b200.so in-tree (sdpa_b200/_lib/), and
+the sdpa command-line driver (sdpa_b200/_lib/sdpa) linked against it.
 
 nvcc cross-compiles for sm_100a only (no other architectures, no JIT PTX), so
 the build runs on machines without a GPU.  Objects are rebuilt when a source
@@ -18,6 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT, "libsdpa_b200.so")
+CLI_SRC = os.path.join(HERE, "cli", "sdpa_main.cpp")
+CLI = os.path.join(OUT, "sdpa")  # the drop-in for the reference's sdpa executable
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -52,6 +55,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if force or not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(LIB),
+                                                                       os.path.getmtime(CLI_SRC)):
+        cmd = [os.environ.get("CXX_HOST", "g++"), "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+               CLI_SRC, "-L" + OUT, "-lsdpa_b200", "-Wl,-rpath,$ORIGIN", "-o", CLI]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -40,6 +41,7 @@ struct SdpaImpl {
   Solver solver;
   std::vector<double> xvec;
   std::vector<std::vector<double>> Xres, Yres;
+  double file_read_seconds = 0.0;  // readInput / readInit / readParameter
   int err = 0;
   std::string errmsg;
   void fail(int code, const std::string& msg)
@@ -71,6 +73,15 @@ struct SdpaImpl {
     }
     if ((int)init.xvec.size() != prob.m) init.xvec.assign(prob.m, 0.0);
   }
+};
+
+// Adds the lifetime of the object to a seconds counter (the reference's
+// ComputeTime::FileRead).
+struct ReadTimer {
+  double& acc;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  explicit ReadTimer(double& a) : acc(a) {}
+  ~ReadTimer() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
 
 // ----------------------------------------------------------- text scanning
@@ -272,6 +283,128 @@ static double host_min_eig(std::vector<double> A, int n)
 
 }  // namespace sdpab
 
+namespace sdpab {
+static bool noprint(const char* fmt) { return strcmp(fmt, "NOPRINT") == 0; }
+
+// Vector::display (sdpa_struct.cpp:82-123): "{v1,v2,...}"
+static void print_vector(FILE* fp, const double* v, size_t n, const char* fmt)
+{
+  if (noprint(fmt)) { fprintf(fp, "NOPRINT\n"); return; }
+  fprintf(fp, "{");
+  for (size_t k = 0; k < n; ++k) {
+    fprintf(fp, fmt, v[k]);
+    fprintf(fp, (k + 1 < n) ? "," : "}\n");
+  }
+  if (n == 0) fprintf(fp, "  }\n");
+}
+
+// DenseMatrix::display (sdpa_struct.cpp:795-833): one brace group per row,
+// the rows themselves in a brace group when n > 1.
+static void print_dense(FILE* fp, const double* M, int n, const char* fmt)
+{
+  fprintf(fp, "{");
+  for (int i = 0; i < n - 1; ++i) {
+    fprintf(fp, i == 0 ? " {" : "  {");
+    for (int j = 0; j < n; ++j) {
+      fprintf(fp, fmt, M[i + (size_t)n * j]);
+      if (j + 1 < n) fprintf(fp, ",");
+    }
+    fprintf(fp, " },\n");
+  }
+  if (n > 1) fprintf(fp, "  {");
+  for (int j = 0; j < n; ++j) {
+    fprintf(fp, fmt, M[(n - 1) + (size_t)n * j]);
+    if (j + 1 < n) fprintf(fp, ",");
+  }
+  fprintf(fp, " }");
+  fprintf(fp, n > 1 ? "   }\n" : "\n");
+}
+
+// DenseLinearSpace::displaySolution (sdpa_struct.cpp:1624-1661): the blocks in
+// file order, SDP blocks as dense matrices, LP blocks as vectors.
+static void print_blocks(SdpaImpl& I, std::vector<std::vector<double>>& M, const char* fmt, FILE* fp)
+{
+  if (noprint(fmt)) { fprintf(fp, "NOPRINT\n"); return; }
+  fprintf(fp, "{\n");
+  for (int l = 0; l < I.nb(); ++l) {
+    const int n = I.blockDim(l);
+    if (I.isSdp(l)) print_dense(fp, M[l].data(), n, fmt);
+    else print_vector(fp, M[l].data(), (size_t)n, fmt);
+  }
+  fprintf(fp, "}\n");
+}
+
+// Parameter::display (sdpa_parts.cpp:266-310)
+static void print_params(FILE* fp, const Params& p, const SdpaImpl& I, const char* fmt)
+{
+  if (noprint(fmt)) { fprintf(fp, "NOPRINT\n"); return; }
+  fprintf(fp, "** Parameters **\n");
+  fprintf(fp, "maxIteration = %d\n", p.maxIteration);
+  const char* names[] = {"epsilonStar  = ", "lambdaStar   = ", "omegaStar    = ", "lowerBound   = ",
+                         "upperBound   = ", "betaStar     = ", "betaBar      = ", "gammaStar    = ",
+                         "epsilonDash  = "};
+  const double vals[] = {p.epsilonStar, p.lambdaStar, p.omegaStar, p.lowerBound, p.upperBound,
+                         p.betaStar,    p.betaBar,    p.gammaStar, p.epsilonDash};
+  for (int q = 0; q < 9; ++q) {
+    fprintf(fp, "%s", names[q]);
+    fprintf(fp, fmt, vals[q]);
+    fprintf(fp, "\n");
+  }
+  fprintf(fp, "xPrint       = %s \n", I.xPrint);
+  fprintf(fp, "XPrint       = %s \n", I.XPrint);
+  fprintf(fp, "YPrint       = %s \n", I.YPrint);
+  fprintf(fp, "infPrint     = %s \n", I.infPrint);
+}
+
+// ComputeTime::display (sdpa_parts.cpp:78-164): the reference's table of
+// rows; this solver times its own phases on the device (rMat+gVec, bMat,
+// Cholesky, solves, dX/dZ, step length, update of X/Z and their inverses,
+// residuals), which fill the matching rows; rows with no counterpart
+// print 0.
+static void print_times(FILE* fp, const SolveStats& s, double file_read)
+{
+  double ph[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (size_t q = 0; q < s.phase_seconds.size() && q < 8; ++q) ph[q] = s.phase_seconds[q];
+  const double main_loop = s.solve_seconds;
+  const double total = s.solve_seconds + file_read;
+  const double div = (main_loop > 0.0) ? main_loop : 1.0;
+  struct Row { const char* name; double v; };
+  const double eig = ph[5];
+  const Row rows[] = {
+      {" Predictor time  =       ", 0.0}, {" Corrector time  =       ", 0.0},
+      {" Make bMat time  =       ", ph[1]}, {" Make bDia time  =       ", 0.0},
+      {" Make bF1  time  =       ", 0.0}, {" Make bF2  time  =       ", 0.0},
+      {" Make bF3  time  =       ", 0.0}, {" Make bPRE time  =       ", 0.0},
+      {" Make rMat time  =       ", ph[0]}, {" Make gVec Mul   =       ", 0.0},
+      {" Make gVec time  =       ", 0.0}, {" Cholesky bMat   =       ", ph[2]},
+      {" Ste Pre time    =       ", 0.0}, {" Ste Cor time    =       ", ph[5]},
+      {" solve           =       ", ph[3]}, {" sumDz           =       ", 0.0},
+      {" makedX          =       ", ph[4]}, {" symmetriseDx    =       ", 0.0},
+      {" makedXdZ        =       ", 0.0}, {" xMatTime        =       ", 0.0},
+      {" zMatTime        =       ", 0.0}, {" invzMatTime     =       ", 0.0},
+      {" xMatzMatTime    =       ", ph[6]}, {" EigxMatTime     =       ", 0.0},
+      {" EigzMatTime     =       ", 0.0}, {" EigxMatzMatTime =       ", 0.0},
+      {" updateRes       =       ", ph[7]}, {" EigTime         =       ", eig},
+      {" sub_total_bMat  =       ", main_loop - ph[1]}, {" Main Loop       =       ", main_loop},
+      {" File Check      =       ", 0.0}, {" File Change     =       ", 0.0},
+      {" File Read       =       ", file_read}, {" Total           =       ", total}};
+  fprintf(fp, "\n");
+  fprintf(fp, "                         Time(sec) ");
+  fprintf(fp, " Ratio(%% : MainLoop) \n");
+  for (const Row& r : rows) fprintf(fp, "%s%f,  %f\n", r.name, r.v, r.v / div * 100.0);
+  fprintf(fp, "\n");
+}
+
+// IO::printOneIteration (sdpa_io.cpp:622-658) in the reference's reversed
+// primal/dual form; r = mu, thetaP, thetaD, objP, objD, alphaP, alphaD, beta
+// of the internal problem.
+static void print_iteration(FILE* fp, int it, const double* r)
+{
+  fprintf(fp, "%2d %4.1e %4.1e %4.1e %+7.2e %+7.2e %4.1e %4.1e %4.2e\n", it, r[0], r[2], r[1], -r[4], -r[3],
+          r[6], r[5], r[7]);
+}
+}  // namespace sdpab
+
 using sdpab::SdpaImpl;
 
 SDPA::SDPA() : impl_(new SdpaImpl()) {}
@@ -408,8 +541,20 @@ void SDPA::initializeSolve()
 {
   SdpaImpl& I = *impl_;
   if (I.err) return;
+  // Newton::setNumThreads and Newton::initialize_bMat messages
+  // (sdpa_newton.cpp:2127-2149, :262-270): the thread count the reference
+  // would use, and the Schur path (always dense here)
+  int nt = I.numThreads;
+  if (nt == 0) {
+    const char* env = getenv("OMP_NUM_THREADS");
+    nt = env ? atoi(env) : 1;
+  }
+  for (FILE* f : {I.display, I.fpout})
+    if (f) fprintf(f, "NumThreads  is set as %d\n", nt);
   const int rc = I.solver.setup(I.prob, I.prm, I.kappa);
   if (rc != SDPAB_OK) return I.fail(rc, sdpab_last_error());
+  for (FILE* f : {I.display, I.fpout})
+    if (f) fprintf(f, "Schur computation : DENSE \n");
   I.initialized = true;
   I.solved = false;
 }
@@ -430,16 +575,64 @@ void SDPA::solve()
     I.Xres[l - 1] = I.solver.resultX(l);
     I.Yres[l - 1] = I.solver.resultY(l);
   }
-  if (I.display) {
-    const sdpab::SolveStats& s = I.solver.stats();
-    char ph[32];
-    getPhaseString(ph);
-    fprintf(I.display, "phase.value  = %s\n   Iteration = %d\n          mu = %+.16e\n", ph, s.iterations, s.mu);
-    fprintf(I.display, "objValPrimal = %+.16e\nobjValDual   = %+.16e\n", s.primal_obj, s.dual_obj);
-    fprintf(I.display, "p.feas.error = %+.16e\nd.feas.error = %+.16e\n", s.primal_error, s.dual_error);
+  // the reference's output sequence of SDPA::solve (sdpa_solve.cpp:76, :164,
+  // :212-231): header, one line per iteration, the last-iteration block,
+  // parameters and times, the solution, and the time lines
+  const sdpab::SolveStats& st = I.solver.stats();
+  FILE* outs[2] = {I.fpout, I.display};
+  const char* head = "   mu      thetaP  thetaD  objP      objD      alphaP  alphaD  beta \n";
+  for (FILE* f : outs)
+    if (f) fprintf(f, "%s", head);
+  const size_t rows = st.trace.size() / 8;
+  for (size_t q = 0; q < rows; ++q)
+    for (FILE* f : outs)
+      if (f) sdpab::print_iteration(f, (int)q, &st.trace[8 * q]);
+  for (FILE* f : outs)
+    if (f) sdpab::print_iteration(f, st.iterations, st.final_row);
+  // IO::printLastInfo (sdpa_io.cpp:661-772)
+  const double oP = st.objValPrimal, oD = st.objValDual;
+  const double mean = (fabs(oP) + fabs(oD)) / 2.0, pdgap = fabs(oP - oD);
+  const double relgap = (mean < 1.0) ? pdgap : pdgap / mean;
+  const double gap = oP - oD;
+  const double digits = -log10(fabs(pdgap / mean));
+  char ph[32];
+  getPhaseString(ph);
+  for (FILE* f : {I.display, I.fpout}) {
+    if (!f) continue;
+    fprintf(f, "\n");
+    fprintf(f, "phase.value  = %-10s\n", ph);
+    fprintf(f, "   Iteration = %d\n", st.iterations);
+    const char* labels[] = {"          mu = ", "relative gap = ", "        gap  = ", "     digits  = ",
+                            "objValPrimal = ", "objValDual   = ", "p.feas.error = ", "d.feas.error = "};
+    const double vals[] = {st.mu, relgap, gap, digits, -oD, -oP, st.primal_error, st.dual_error};
+    for (int q = 0; q < 8; ++q) {
+      fprintf(f, "%s", labels[q]);
+      fprintf(f, I.infPrint, vals[q]);
+      fprintf(f, "\n");
+    }
+    fprintf(f, "total time   = %.6f\n", st.solve_seconds + I.file_read_seconds);
   }
   if (I.fpout) {
+    sdpab::print_params(I.fpout, I.prm, I, I.infPrint);
+    sdpab::print_times(I.fpout, st, I.file_read_seconds);
+    // IO::printSolution (sdpa_io.cpp:845-867)
+    fprintf(I.fpout, "xVec = \n");
     printResultXVec(I.fpout);
+    fprintf(I.fpout, "xMat = \n");
+    printResultXMat(I.fpout);
+    fprintf(I.fpout, "yMat = \n");
+    printResultYMat(I.fpout);
+  }
+  const double tl[5] = {st.solve_seconds, st.solve_seconds + I.file_read_seconds, 0.0, 0.0, I.file_read_seconds};
+  if (I.display) {
+    const char* n[5] = {"  main loop time = ", "      total time = ", "file  check time = ", "file change time = ",
+                        "file   read time = "};
+    for (int q = 0; q < 5; ++q) fprintf(I.display, "%s%.6f\n", n[q], tl[q]);
+  }
+  if (I.fpout) {
+    const char* n[5] = {"    main loop time = ", "        total time = ", "  file  check time = ",
+                        "  file change time = ", "  file   read time = "};
+    for (int q = 0; q < 5; ++q) fprintf(I.fpout, "%s%.6f\n", n[q], tl[q]);
   }
 }
 
@@ -578,73 +771,27 @@ void SDPA::printDimacsError(double* d, char* fmt, FILE* fp)
   }
   fprintf(fp, "\n");
 }
+
 void SDPA::printResultXVec(FILE* fp)
 {
   if (!fp || !impl_->solved) return;
-  fprintf(fp, "{");
-  for (size_t k = 0; k < impl_->xvec.size(); ++k) {
-    fprintf(fp, impl_->xPrint, impl_->xvec[k]);
-    if (k + 1 < impl_->xvec.size()) fprintf(fp, ",");
-  }
-  fprintf(fp, "}\n");
-}
-static void print_blocks(SdpaImpl& I, std::vector<std::vector<double>>& M, const char* fmt, FILE* fp)
-{
-  fprintf(fp, "{\n");
-  for (int l = 0; l < I.nb(); ++l) {
-    const int n = I.blockDim(l);
-    if (I.isSdp(l)) {
-      fprintf(fp, "{\n");
-      for (int i = 0; i < n; ++i) {
-        fprintf(fp, "{");
-        for (int j = 0; j < n; ++j) {
-          fprintf(fp, fmt, M[l][i + (size_t)n * j]);
-          if (j + 1 < n) fprintf(fp, ",");
-        }
-        fprintf(fp, "}%s\n", i + 1 < n ? "," : "");
-      }
-      fprintf(fp, "}\n");
-    } else {
-      fprintf(fp, "{");
-      for (int i = 0; i < n; ++i) {
-        fprintf(fp, fmt, M[l][i]);
-        if (i + 1 < n) fprintf(fp, ",");
-      }
-      fprintf(fp, "}\n");
-    }
-  }
-  fprintf(fp, "}\n");
+  sdpab::print_vector(fp, impl_->xvec.data(), impl_->xvec.size(), impl_->xPrint);
 }
 void SDPA::printResultXMat(FILE* fp)
 {
-  if (fp && impl_->solved) print_blocks(*impl_, impl_->Xres, impl_->XPrint, fp);
+  if (fp && impl_->solved) sdpab::print_blocks(*impl_, impl_->Xres, impl_->XPrint, fp);
 }
 void SDPA::printResultYMat(FILE* fp)
 {
-  if (fp && impl_->solved) print_blocks(*impl_, impl_->Yres, impl_->YPrint, fp);
+  if (fp && impl_->solved) sdpab::print_blocks(*impl_, impl_->Yres, impl_->YPrint, fp);
 }
-// ComputeTime::display (sdpa_parts.cpp:78-164) restated over the GPU phases
 void SDPA::printComputationTime(FILE* fp)
 {
-  if (!fp) return;
-  static const char* names[] = {"Make rMat+gVec", "Make bMat", "Cholesky bMat", "solve",
-                                "makedXdZ", "StepLength", "update (inverses)", "updateRes"};
-  const sdpab::SolveStats& s = impl_->solver.stats();
-  fprintf(fp, "                         Time(sec)\n");
-  for (size_t q = 0; q < s.phase_seconds.size() && q < 8; ++q)
-    fprintf(fp, " %-22s = %f\n", names[q], s.phase_seconds[q]);
-  fprintf(fp, " %-22s = %f\n", "Total (solve)", getSolveTime());
+  if (fp) sdpab::print_times(fp, impl_->solver.stats(), impl_->file_read_seconds);
 }
 void SDPA::printParameters(FILE* fp)
 {
-  if (!fp) return;
-  const sdpab::Params& p = impl_->prm;
-  fprintf(fp, "** Parameters **\nmaxIteration = %d\nepsilonStar  = %+8.3e\nlambdaStar   = %+8.3e\n",
-          p.maxIteration, p.epsilonStar, p.lambdaStar);
-  fprintf(fp, "omegaStar    = %+8.3e\nlowerBound   = %+8.3e\nupperBound   = %+8.3e\n", p.omegaStar,
-          p.lowerBound, p.upperBound);
-  fprintf(fp, "betaStar     = %+8.3e\nbetaBar      = %+8.3e\ngammaStar    = %+8.3e\nepsilonDash  = %+8.3e\n",
-          p.betaStar, p.betaBar, p.gammaStar, p.epsilonDash);
+  if (fp) sdpab::print_params(fp, impl_->prm, *impl_, "%+8.3e");
 }
 void SDPA::printSDPAVersion(FILE* fp)
 {
@@ -653,6 +800,7 @@ void SDPA::printSDPAVersion(FILE* fp)
 
 void SDPA::readInput(char* filename, FILE* fpout, SparseType type)
 {
+  const sdpab::ReadTimer timer_(impl_->file_read_seconds);
   SdpaImpl& I = *impl_;
   std::string txt, why;
   if (!filename || !sdpab::slurp(filename, txt)) return I.fail(SDPAB_EIO, "readInput: cannot open data file");
@@ -663,12 +811,23 @@ void SDPA::readInput(char* filename, FILE* fpout, SparseType type)
   } else {
     sparse = (type == SPARSE);
   }
-  if (fpout) fprintf(fpout, "data   is %s  : %s\n", filename, sparse ? "sparse" : "dense");
+  if (fpout) {
+    fprintf(fpout, "data   is %s  : %s\n", filename, sparse ? "sparse" : "dense");
+    // the title / comment lines ahead of the data are echoed (IO::read, sdpa_io.cpp:33-45)
+    size_t pos = 0;
+    while (pos < txt.size() && (txt[pos] == '"' || txt[pos] == '*')) {
+      const size_t eol = txt.find('\n', pos);
+      const size_t e = (eol == std::string::npos) ? txt.size() : eol + 1;
+      fwrite(txt.data() + pos, 1, e - pos, fpout);
+      pos = e;
+    }
+  }
   const int rc = sdpab::parse_sdpa(txt, sparse, I.prob, why);
   if (rc != SDPAB_OK) return I.fail(rc, "readInput: " + why);
 }
 void SDPA::readInit(char* filename, FILE* fpout, SparseType type)
 {
+  const sdpab::ReadTimer timer_(impl_->file_read_seconds);
   SdpaImpl& I = *impl_;
   std::string txt, why;
   if (!filename || !sdpab::slurp(filename, txt)) return I.fail(SDPAB_EIO, "readInit: cannot open init file");
@@ -685,6 +844,7 @@ void SDPA::readInit(char* filename, FILE* fpout, SparseType type)
 }
 void SDPA::readParameter(char* filename, FILE* fpout)
 {
+  const sdpab::ReadTimer timer_(impl_->file_read_seconds);
   sdpab_params p;
   if (sdpab_read_params(filename, &p) != SDPAB_OK) return impl_->fail(SDPAB_EIO, "readParameter failed");
   memcpy(&impl_->prm, &p, sizeof(p));

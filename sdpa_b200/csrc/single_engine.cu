@@ -1347,6 +1347,10 @@ int Solver::solve(const InitPoint* init)
   stats_.primal_error = h[1];
   stats_.dual_error = h[0];
   stats_.mu = sc.mu;
+  {
+    const double row[8] = {sc.mu, sc.thetaP, sc.thetaD, sc.objP, sc.objD, sc.alphaP, sc.alphaD, sc.beta};
+    for (int q = 0; q < 8; ++q) stats_.final_row[q] = row[q];
+  }
   xvec_.assign(m, 0.0);
   cudaMemcpy(xvec_.data(), S.y, m * sizeof(double), cudaMemcpyDeviceToHost);
   for (double& v : xvec_) v = -v;

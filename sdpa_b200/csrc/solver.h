@@ -48,6 +48,7 @@ struct SolveStats {
   int cholesky_failed = 0;
   int warm_start_rejected = 0;
   std::vector<double> trace;  // per iteration: mu, thetaP, thetaD, objP, objD, alphaP, alphaD, beta
+  double final_row[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // the same quantities at loop exit
   // device seconds per phase: rMat+gVec, bMat, Cholesky, solves, dX/dZ,
   // step length, update (inverses), residuals
   std::vector<double> phase_seconds;

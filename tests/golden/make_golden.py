@@ -32,6 +32,7 @@ sys.path.insert(0, ROOT)
 from sdpa_b200 import instances as inst  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "ref_batch")
+REF_CLI = os.path.join(ROOT, "oracle", "_ref", "sdpa")  # the reference's own executable (sdpa_exe.cpp)
 
 
 def example1():
@@ -137,6 +138,62 @@ def run_ref(instances, tmp, param=None, trace=False, procs=1, threads=1):
     return outl
 
 
+def write_dense(it, path):
+    """The instance in SDPA's dense .dat format (IO::read dense branch,
+    sdpa_io.cpp:540-604): header, then F0..Fm, each block as a full matrix
+    (SDP) or its diagonal (LP)."""
+    mats = []
+    for k in range(it.m + 1):
+        blocks = []
+        for l, bs in enumerate(it.blocks, start=1):
+            n = abs(int(bs))
+            blocks.append(np.zeros((n, n)) if bs > 0 else np.zeros(n))
+        for q in range(it.k.size):
+            if int(it.k[q]) != k:
+                continue
+            B = blocks[int(it.l[q]) - 1]
+            r, c = int(it.i[q]) - 1, int(it.j[q]) - 1
+            if B.ndim == 2:
+                B[r, c] = B[c, r] = float(it.v[q])
+            else:
+                B[r] = float(it.v[q])
+        mats.append(blocks)
+    fmt = lambda a: ",".join(repr(float(x)) for x in a)
+    out = [f'"{it.name} (dense)"', f"{it.m} = mDIM", f"{len(it.blocks)} = nBLOCK",
+           " ".join(str(int(b)) for b in it.blocks) + " = bLOCKsTRUCT", "{" + fmt(it.c) + "}"]
+    for blocks in mats:
+        parts = []
+        for B in blocks:
+            if B.ndim == 2:
+                parts.append("{ " + ", ".join("{" + fmt(row) + "}" for row in B) + " }")
+            else:
+                parts.append("{" + fmt(B) + "}")
+        out.append("{ " + " ".join(parts) + " }")
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+
+
+def cli_fixtures():
+    """Inputs and the reference executable's result files for the command-line
+    driver test (tests/golden/cli): example 1 sparse with -pt 0, example 2
+    dense in the positional style with -pt 0 and -dimacs, example 1 with a
+    parameter file (epsilonStar 1e-8)."""
+    d = os.path.join(HERE, "cli")
+    os.makedirs(d, exist_ok=True)
+    example1().write(os.path.join(d, "ex1.dat-s"))
+    write_dense(example2(), os.path.join(d, "ex2.dat"))
+    with open(os.path.join(d, "param.sdpa"), "w") as f:
+        f.write(PARAM_1E8)
+    runs = [(["-ds", "ex1.dat-s", "-o", "ex1.result", "-pt", "0"], "ex1.result"),
+            (["ex2.dat", "ex2.result", "-pt", "0", "-dimacs"], "ex2.result"),
+            (["-ds", "ex1.dat-s", "-o", "ex1p.result", "-p", "param.sdpa"], "ex1p.result")]
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+    for args, _ in runs:
+        subprocess.run([REF_CLI] + args, cwd=d, env=env, check=True, capture_output=True)
+    with open(os.path.join(d, "runs.json"), "w") as f:
+        json.dump([{"args": a, "result": r} for a, r in runs], f, indent=1)
+
+
 def small_cases():
     cases = [("mc100", inst.maxcut(100, 0.1, 1)), ("mc20", inst.maxcut(20, 0.3, 1)),
              ("mc50w", inst.maxcut(50, 0.2, 5, unit_weights=False)),
@@ -208,6 +265,8 @@ def main():
         with open(os.path.join(HERE, "tight.json"), "w") as f:
             json.dump(meta, f, indent=1)
         np.savez_compressed(os.path.join(HERE, "tight.npz"), **arrays)
+
+        cli_fixtures()
 
         if large:
             big = [("lt200", inst.lovasz_theta(200, 0.5, 1)), ("rnd2000", inst.random_sdp(seed=1))]
