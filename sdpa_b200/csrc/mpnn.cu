@@ -7,8 +7,9 @@
 // A is the row-normalised weighted adjacency a_ij = w_ij / (d_i + 1).
 // Weights are used in BF16 (a master FP32 copy is kept for the optimiser);
 // every product accumulates in FP32.  Forward, backward (loss = mean squared
-// error over masked nodes) and Adam are hand-written SIMT kernels: the
-// per-node products are 64-wide, too small for tensor-core tiles to pay.
+// error over masked nodes) and Adam are hand-written SIMT kernels in FP32
+// (a layer over a 4096-graph batch is ~14 GFLOP and ~0.3 GB of activations,
+// a fraction of a millisecond either way).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -49,29 +50,56 @@ __global__ void k_spmm(int N, int F, const int* rowptr, const int* col, const fl
   Y[t] = s;
 }
 
-// z = h Ws^T + agg Wn^T + b; hout = relu(z).  Each block stages the layer's
-// weights once (as float) and covers NODES_PER_BLOCK nodes, 64 threads
-// (output features j) per node.
-constexpr int NODES_PER_BLOCK = 64;
-__global__ void k_dense_fwd(int N, int Fin, const float* h, const float* agg, const __nv_bfloat16* Ws,
-                            const __nv_bfloat16* Wn, const __nv_bfloat16* b, float* z, float* hout)
+// z = h Ws^T + agg Wn^T + b; hout = relu(z).  A block covers FWD_NODES
+// nodes: the layer's weights are staged transposed (k-major, so the 32
+// lanes of a warp read 32 consecutive output features: no bank conflicts)
+// and the nodes' h and agg rows are staged once; thread (j, g) computes
+// output feature j of nodes g, g + 4, ... from registers.  The products are
+// accumulated in the same order for every node (per k: agg term, then h
+// term), FP32 throughout.
+constexpr int FWD_NODES = 32;
+constexpr int FWD_PER = FWD_NODES / 4;  // nodes per thread (256 threads = 64 features x 4)
+__global__ void __launch_bounds__(256) k_dense_fwd(int N, int Fin, const float* h, const float* agg,
+                                                   const __nv_bfloat16* Ws, const __nv_bfloat16* Wn,
+                                                   const __nv_bfloat16* b, float* z, float* hout)
 {
-  __shared__ float sWs[H * H], sWn[H * H];
+  __shared__ float sWs[H * H], sWn[H * H];                        // [k][j]
+  __shared__ __align__(16) float sh[FWD_NODES * H], sa[FWD_NODES * H];  // [node][k]
   for (int t = threadIdx.x; t < H * Fin; t += blockDim.x) {
-    sWs[t] = __bfloat162float(Ws[t]);
-    sWn[t] = __bfloat162float(Wn[t]);
+    const int jj = t / Fin, k = t % Fin;  // source layout [j][k]
+    sWs[k * H + jj] = __bfloat162float(Ws[t]);
+    sWn[k * H + jj] = __bfloat162float(Wn[t]);
+  }
+  const int i0 = blockIdx.x * FWD_NODES;
+  const int cnt = min(FWD_NODES, N - i0);
+  for (int t = threadIdx.x; t < FWD_NODES * Fin; t += blockDim.x) {
+    const int r = t / Fin;
+    const bool ok = r < cnt;
+    sh[t] = ok ? h[(long long)i0 * Fin + t] : 0.0f;
+    sa[t] = ok ? agg[(long long)i0 * Fin + t] : 0.0f;
   }
   __syncthreads();
-  const int j = threadIdx.x % H;
+  const int j = threadIdx.x % H, g = threadIdx.x / H;
   const float bj = __bfloat162float(b[j]);
-  for (int i = blockIdx.x * NODES_PER_BLOCK + threadIdx.x / H; i < min(N, (blockIdx.x + 1) * NODES_PER_BLOCK);
-       i += blockDim.x / H) {
-    float s = bj;
-    const float* hi = h + (long long)i * Fin;
-    const float* ai = agg + (long long)i * Fin;
-    for (int k = 0; k < Fin; ++k) s = fmaf(hi[k], sWs[j * Fin + k], fmaf(ai[k], sWn[j * Fin + k], s));
-    z[(long long)i * H + j] = s;
-    hout[(long long)i * H + j] = s > 0.0f ? s : 0.0f;
+  float acc[FWD_PER];
+#pragma unroll
+  for (int u = 0; u < FWD_PER; ++u) acc[u] = bj;
+  for (int k = 0; k < Fin; ++k) {
+    const float ws = sWs[k * H + j], wn = sWn[k * H + j];
+#pragma unroll
+    for (int u = 0; u < FWD_PER; ++u) {
+      const int r = g + 4 * u;
+      acc[u] = fmaf(sh[r * Fin + k], ws, fmaf(sa[r * Fin + k], wn, acc[u]));
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < FWD_PER; ++u) {
+    const int r = g + 4 * u;
+    if (r < cnt) {
+      const long long o = (long long)(i0 + r) * H + j;
+      z[o] = acc[u];
+      hout[o] = acc[u] > 0.0f ? acc[u] : 0.0f;
+    }
   }
 }
 
@@ -260,7 +288,7 @@ static void forward(const sdpab_graph_batch* g, const __nv_bfloat16* wb, const A
   for (int l = 0; l < L; ++l) {
     const int Fin = fin_of(l);
     k_spmm<<<nb((long long)N * Fin), 256, 0, st>>>(N, Fin, g->rowptr, g->col, g->aval, a.h[l], a.agg[l]);
-    k_dense_fwd<<<nb(N, NODES_PER_BLOCK), 256, 0, st>>>(N, Fin, a.h[l], a.agg[l], wb + off_ws(l), wb + off_wn(l), wb + off_b(l),
+    k_dense_fwd<<<nb(N, FWD_NODES), 256, 0, st>>>(N, Fin, a.h[l], a.agg[l], wb + off_ws(l), wb + off_wn(l), wb + off_b(l),
                                           a.z[l], a.h[l + 1]);
   }
 }

@@ -163,3 +163,29 @@ def random_sdp(m: int = 2000, n: int = 500, nlp: int = 50, density: float = 0.01
     return Instance(m=m, blocks=[n, -nlp], c=b, k=np.concatenate(ks), l=np.concatenate(ls),
                     i=np.concatenate(is_), j=np.concatenate(js), v=np.concatenate(vs),
                     name=f"random sdp m={m} n={n} lp={nlp} seed {seed}")
+
+
+def main(argv=None):
+    """Writes a generated instance as an SDPA .dat-s file:
+
+        python -m sdpa_b200.instances mc1  OUT.dat-s   # MaxCut G(100, 0.1), seed 1
+        python -m sdpa_b200.instances lt   OUT.dat-s   # Lovasz theta G(200, 0.5), seed 1 (m = 9986)
+        python -m sdpa_b200.instances rnd  OUT.dat-s   # random m = 2000, blocks {500, -50}, seed 1
+        python -m sdpa_b200.instances mcb SEED OUT.dat-s  # one batched-MaxCut instance
+    """
+    import sys
+    a = list(sys.argv[1:] if argv is None else argv)
+    if len(a) == 2 and a[0] in ("mc1", "lt", "rnd"):
+        it = {"mc1": lambda: maxcut(100, 0.1, 1), "lt": lambda: lovasz_theta(200, 0.5, 1),
+              "rnd": lambda: random_sdp(seed=1)}[a[0]]()
+        it.write(a[1])
+    elif len(a) == 3 and a[0] == "mcb":
+        batch_maxcut(int(a[1])).write(a[2])
+    else:
+        print(main.__doc__)
+        return 2
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -93,6 +93,20 @@ def evaluate(model, graphs, label, precision=N.PREC_FP64):
     }
 
 
+def evaluate_all(model, args):
+    """Held-out set and the batched-MaxCut benchmark set, FP64 and mixed."""
+    test_g = [W.batch_graph(s, args.nmin, args.nmax) for s in range(300000, 300000 + args.test)]
+    mcb = [W.batch_graph(s, 20, 120) for s in range(4096)]
+    ev = []
+    for prec, name in ((N.PREC_FP64, "fp64"), (N.PREC_MIXED, "mixed")):
+        for graphs, label in ((test_g, f"held-out n~U{{{args.nmin}..{args.nmax}}} seeds 300000+"),
+                              (mcb, "batched MaxCut n~U{20..120} seeds 0..4095")):
+            e = evaluate(model, graphs, label, prec)
+            e["precision"] = name
+            ev.append(e)
+    return ev
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=20000)
@@ -104,17 +118,11 @@ def main():
     ap.add_argument("--nmax", type=int, default=200)
     ap.add_argument("--out", default=os.path.join(HERE, "data"))
     ap.add_argument("--eval-only", action="store_true", help="load mpnn_maxcut.npy and evaluate")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
-    prec = N.PREC_FP64 if args.precision == "fp64" else N.PREC_MIXED
     if args.eval_only:
         model = W.MPNN(seed=0)
         model.load(np.load(DEFAULT_WEIGHTS))
-        test_g = [W.batch_graph(s, args.nmin, args.nmax) for s in range(300000, 300000 + args.test)]
-        ev = [evaluate(model, test_g, f"held-out n~U{{{args.nmin}..{args.nmax}}} seeds 300000+", prec)]
-        mcb = [W.batch_graph(s, 20, 120) for s in range(4096)]
-        ev.append(evaluate(model, mcb, "batched MaxCut n~U{20..120} seeds 0..4095", prec))
-        print(json.dumps({"precision": args.precision, "eval": ev}, indent=1), flush=True)
+        print(json.dumps({"eval": evaluate_all(model, args)}, indent=1), flush=True)
         return
     os.makedirs(args.out, exist_ok=True)
     t0 = time.time()
@@ -135,10 +143,7 @@ def main():
                    log=lambda s: print(s, flush=True))
     train_s = time.time() - t1
     np.save(os.path.join(args.out, "mpnn_maxcut.npy"), model.state())
-    test_g = [W.batch_graph(s, args.nmin, args.nmax) for s in range(300000, 300000 + args.test)]
-    ev = [evaluate(model, test_g, f"held-out n~U{{{args.nmin}..{args.nmax}}} seeds 300000+")]
-    mcb = [W.batch_graph(s, 20, 120) for s in range(4096)]
-    ev.append(evaluate(model, mcb, "batched MaxCut n~U{20..120} seeds 0..4095"))
+    ev = evaluate_all(model, args)
     summary = {"train_instances": args.train, "train_pdOPT": ok, "epochs": args.epochs,
                "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "train_seconds": train_s,
                "params": model.P, "eval": ev}
