@@ -42,6 +42,14 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+# DRAM bytes (read + write) per instance of the solver launch, from one ncu
+# capture of a 592-instance launch at the bench's launch shape (2 blocks per
+# SM, warm start, FP64): 9.62 GB / 592.  The traffic is workspace eviction
+# (per-block workspaces of the instances in flight exceed L2), so it grows
+# with the instances processed.
+TRAFFIC_BYTES_PER_INSTANCE = 9.62e9 / 592
+
+
 def iter_flops(n: int, m: int) -> float:
     """Algorithmic flops of one IPM iteration in the reference's operation
     sequence for one dense block with single-entry constraints (F3 Schur):
@@ -366,7 +374,9 @@ def main():
             "e2e": {"value": e2e_val, "unit": "SDPs/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": args.steps * launches_per_step,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                         "frac": achieved / bf16, "traffic": None,
+                         "frac": achieved / bf16,
+                         "traffic": TRAFFIC_BYTES_PER_INSTANCE * P.count,
+                         "traffic_note": "ncu capture of 592 instances scaled by instances (bytes per launch)",
                          "peak_source": f"{src} bf16 dense (MEASURED_PEAKS.json); the kernel computes "
                                         "on the FP64/FP32 SIMT pipes",
                          "fp64_nominal_tflops": 40.0, "frac_of_fp64_nominal": achieved / 40.0,

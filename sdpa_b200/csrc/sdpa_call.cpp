@@ -432,7 +432,20 @@ void SDPA::setParameterPrintInformation(char* s) { snprintf(impl_->infPrint, 32,
 void SDPA::setDisplay(FILE* f) { impl_->display = f; }
 void SDPA::setResultFile(FILE* f) { impl_->fpout = f; }
 void SDPA::setInitPoint(bool b) { impl_->isInitPoint = b; }
-void SDPA::setNumThreads(SDPA_INT n) { impl_->numThreads = n; }
+// The solve runs on the GPU; the thread count is kept for getNumThreads and
+// reported like Newton::setNumThreads (sdpa_newton.cpp:2127-2149): the given
+// value, or OMP_NUM_THREADS, or 1.
+void SDPA::setNumThreads(SDPA_INT n)
+{
+  impl_->numThreads = n;
+  int nt = n;
+  if (nt == 0) {
+    const char* env = getenv("OMP_NUM_THREADS");
+    nt = env ? atoi(env) : 1;
+  }
+  for (FILE* f : {impl_->display, impl_->fpout})
+    if (f) fprintf(f, "NumThreads  is set as %d\n", nt);
+}
 
 SDPA::ParameterType SDPA::getParameterType() { return (ParameterType)impl_->ptype; }
 SDPA_INT SDPA::getParameterMaxIteration() { return impl_->prm.maxIteration; }
@@ -541,18 +554,10 @@ void SDPA::initializeSolve()
 {
   SdpaImpl& I = *impl_;
   if (I.err) return;
-  // Newton::setNumThreads and Newton::initialize_bMat messages
-  // (sdpa_newton.cpp:2127-2149, :262-270): the thread count the reference
-  // would use, and the Schur path (always dense here)
-  int nt = I.numThreads;
-  if (nt == 0) {
-    const char* env = getenv("OMP_NUM_THREADS");
-    nt = env ? atoi(env) : 1;
-  }
-  for (FILE* f : {I.display, I.fpout})
-    if (f) fprintf(f, "NumThreads  is set as %d\n", nt);
   const int rc = I.solver.setup(I.prob, I.prm, I.kappa);
   if (rc != SDPAB_OK) return I.fail(rc, sdpab_last_error());
+  // Newton::initialize_bMat's message (sdpa_newton.cpp:262-270): the Schur
+  // path, always dense here
   for (FILE* f : {I.display, I.fpout})
     if (f) fprintf(f, "Schur computation : DENSE \n");
   I.initialized = true;
@@ -565,7 +570,7 @@ void SDPA::solve()
   if (I.err) return;
   if (!I.initialized) return I.fail(SDPAB_ESTATE, "solve called before initializeSolve");
   if (I.isInitPoint) I.ensureInit();
-  const int rc = I.solver.solve(I.isInitPoint ? &I.init : nullptr);
+  const int rc = I.solver.solve(I.isInitPoint ? &I.init : nullptr, &I.prm);
   if (rc != SDPAB_OK) return I.fail(rc, sdpab_last_error());
   I.solved = true;
   I.xvec = I.solver.xvec();
@@ -789,9 +794,10 @@ void SDPA::printComputationTime(FILE* fp)
 {
   if (fp) sdpab::print_times(fp, impl_->solver.stats(), impl_->file_read_seconds);
 }
+// Parameter::display with its default format "%+10.16e" (sdpa_parts.h:119)
 void SDPA::printParameters(FILE* fp)
 {
-  if (fp) sdpab::print_params(fp, impl_->prm, *impl_, "%+8.3e");
+  if (fp) sdpab::print_params(fp, impl_->prm, *impl_, "%+10.16e");
 }
 void SDPA::printSDPAVersion(FILE* fp)
 {

@@ -887,8 +887,9 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
   return SDPAB_OK;
 }
 
-int Solver::solve(const InitPoint* init)
+int Solver::solve(const InitPoint* init, const Params* prm)
 {
+  if (d_ && prm) d_->prm = *prm;
   if (!d_) return set_error(SDPAB_ESTATE, "solve before initializeSolve");
   DevState& S = *d_;
   const Params& P = S.prm;

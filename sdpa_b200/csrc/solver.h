@@ -67,8 +67,11 @@ class Solver {
   // index, formula choice (computeFormula_SDP), device upload.  Returns an
   // SDPAB_* status.
   int setup(const ProblemData& p, const Params& prm, double kappa);
-  // SDPA::solve (sdpa_solve.cpp:59-233); init may be NULL.
-  int solve(const InitPoint* init);
+  // SDPA::solve (sdpa_solve.cpp:59-233); init may be NULL.  `prm` are the
+  // parameters in force at the call (the reference reads its Parameter
+  // object at solve time, so changes after initializeSolve apply); NULL
+  // keeps those given to setup.
+  int solve(const InitPoint* init, const Params* prm = nullptr);
   void release();
   // SDPAB_PREC_FP64 (default) or SDPAB_PREC_MIXED: FP32 products and FP32
   // Schur factor with FP64 refinement while the relative complementarity

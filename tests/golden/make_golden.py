@@ -184,6 +184,9 @@ def cli_fixtures():
     write_dense(example2(), os.path.join(d, "ex2.dat"))
     with open(os.path.join(d, "param.sdpa"), "w") as f:
         f.write(PARAM_1E8)
+    # an interior initial point for example 1 (x, then user X and Y entries)
+    with open(os.path.join(d, "ex1.ini-s"), "w") as f:
+        f.write("0.0 0.0 0.0\n1 1 1 1 10.0\n1 1 2 2 10.0\n2 1 1 1 10.0\n2 1 2 2 10.0\n")
     runs = [(["-ds", "ex1.dat-s", "-o", "ex1.result", "-pt", "0"], "ex1.result"),
             (["ex2.dat", "ex2.result", "-pt", "0", "-dimacs"], "ex2.result"),
             (["-ds", "ex1.dat-s", "-o", "ex1p.result", "-p", "param.sdpa"], "ex1p.result")]
