@@ -261,7 +261,7 @@ typedef struct sdpab_batch_config {
                                   |objective|) < this (0 = 1e-2) */
   int staging_doubles;         /* shared-memory staging of GEMM tiles and Lanczos
                                   matrices per solver block, in doubles (0 = auto;
-                                  raised to the GEMM minimum of 3072) */
+                                  raised to the GEMM minimum of 6144) */
 } sdpab_batch_config;
 
 /* Solves a batch whose arrays (problem, init, result) are all DEVICE pointers,

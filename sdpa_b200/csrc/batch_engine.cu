@@ -36,7 +36,7 @@ namespace sdpab {
 // staging area `gsm` (doubles) for GEMM tiles and Lanczos matrices.
 static __host__ __device__ long long fixed_smem_doubles(int nmax, int mmax)
 {
-  return cta::SD_DOUBLES + 4 * (NT / 32) + 4LL * mmax + eig_scratch_doubles(nmax);
+  return 2 * cta::SD_DOUBLES + 4 * (NT / 32) + 4LL * mmax + eig_scratch_doubles(nmax);
 }
 
 static size_t smem_bytes_for(int nmax, int mmax, long long gsm)
@@ -44,13 +44,13 @@ static size_t smem_bytes_for(int nmax, int mmax, long long gsm)
   return (size_t)(gsm + fixed_smem_doubles(nmax, mmax)) * sizeof(double) + (size_t)mmax * sizeof(int) + 64;
 }
 
-// Staging area: at least the largest single-tile GEMM (n <= 96).  `want`
+// Staging area: at least the double-buffered single-tile GEMM (n <= 96).  `want`
 // doubles when given (capped at what one block can have); by default both
 // Lanczos matrices (2 n^2) when they fit in LANCZOS_SMEM_DOUBLES, else one,
 // else the GEMM minimum.
 static long long staging_doubles(int nmax, int mmax, int want)
 {
-  const long long g = 2 * 16 * 96;
+  const long long g = 4 * 16 * 96;  // double-buffered single-tile GEMM (n <= 96)
   const long long m2 = (long long)nmax * nmax;
   long long s;
   if (want > 0) s = want;
@@ -169,7 +169,8 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
   const int gsm_doubles = a.gsm_doubles;
   double* gsm = smem;                                   // GEMM staging / Lanczos matrix
   double* sD = gsm + gsm_doubles;                       // diagonal block NB*LDD
-  double* redbuf = sD + cta::SD_DOUBLES;                // 4 * NT/32
+  double* sD2 = sD + cta::SD_DOUBLES;                   // second diagonal block (paired X / Z steps)
+  double* redbuf = sD2 + cta::SD_DOUBLES;               // 4 * NT/32
   double* vy = redbuf + 4 * (NT / 32);                  // y   (mmax)
   double* vdy = vy + mmax;                              // dy  (mmax)
   double* vg = vdy + mmax;                              // g   (mmax)
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
   eig_scratch_carve(es, vrp + mmax, nmax, &RD);          // eig_scratch_doubles(nmax)
   int* s_nnz = (int*)(vrp + mmax + eig_scratch_doubles(nmax));  // mmax ints
 
-  __shared__ int s_inst, s_flag;
+  __shared__ int s_inst, s_flag, s_flag2[2];
   __shared__ Scalars S;
   const int tid = threadIdx.x;
   const Params& P = a.prm;
@@ -533,10 +534,9 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         for (int t = tid; t < nn_i; t += NT) { W2[t] = X[t]; W1[t] = Z[t]; }
         __syncthreads();
         if (cannot_move(S)) break;
-        if (cta::cholesky<NT, double>(n, W2, n, false, sD, gsm, &s_flag)) break;
-        cta::tri_inverse<NT, double>(n, W2, n, LXi, n, sD, gsm);
-        if (cta::cholesky<NT, double>(n, W1, n, false, sD, gsm, &s_flag)) break;
-        cta::tri_inverse<NT, double>(n, W1, n, LZi, n, sD, gsm);
+        // X and Z factored and inverted in lockstep (either failing ends the loop)
+        if (cta::cholesky_pair<NT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2)) break;
+        cta::tri_inverse_pair<NT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
         cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
       // ---- residuals and scalars

@@ -270,8 +270,88 @@ __device__ __noinline__ void gemm_tile(int n, bool tA, const TM* A, int lda, boo
   __syncthreads();
 }
 
-// Square GEMM dispatch: one exact-size tile for n <= 96, 64 x 64 tiles above.
-// smem must hold 2 * 16 * 96 doubles.  lowp = compute in FP32.
+// Asynchronous global -> shared copy of one 8-byte element (cp.async, zero
+// fill when `valid` is false; the source pointer must still be a valid
+// address), and the group fences around it.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// FP64 gemm_tile with double-buffered staging: chunk k+1 is copied by
+// cp.async while chunk k is multiplied, so each chunk costs one barrier and
+// its load latency is hidden.  smem: 4 * 16 * 16R doubles.
+template <int NT, int R>
+__device__ __noinline__ void gemm_tile_db(int n, bool tA, const double* A, int lda, bool tB, const double* B,
+                                          int ldb, double* C, int ldc, double alpha, double beta, void* smem_v)
+{
+  constexpr int T = 16 * R, KC = 16;
+  double* buf = (double*)smem_v;  // [2][As: KC*T | Bs: KC*T]
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  auto issue = [&](int k0, int which) {
+    double* As = buf + which * 2 * KC * T;
+    double* Bs = As + KC * T;
+    for (int t = threadIdx.x; t < KC * T; t += NT) {
+      int r, k;
+      if (!tA) { r = t % T; k = t / T; } else { k = t % KC; r = t / KC; }
+      const int gk = k0 + k;
+      const bool va = r < n && gk < n;
+      cp_async8(&As[k * T + r], va ? (tA ? A + gk + (size_t)lda * r : A + r + (size_t)lda * gk) : A, va);
+      int c;
+      if (!tB) { k = t % KC; c = t / KC; } else { c = t % T; k = t / T; }
+      const int gk2 = k0 + k;
+      const bool vb = c < n && gk2 < n;
+      cp_async8(&Bs[k * T + c], vb ? (tB ? B + c + (size_t)ldb * gk2 : B + gk2 + (size_t)ldb * c) : B, vb);
+    }
+    cp_async_commit();
+  };
+  double acc[R][R];
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+#pragma unroll
+    for (int j = 0; j < R; ++j) acc[i][j] = 0.0;
+  const int nch = (n + KC - 1) / KC;
+  issue(0, 0);
+  for (int ch = 0; ch < nch; ++ch) {
+    cp_async_wait_all();
+    __syncthreads();  // chunk ch visible; every thread is done with chunk ch-1's buffer
+    if (ch + 1 < nch) issue((ch + 1) * KC, (ch + 1) & 1);
+    const double* As = buf + (ch & 1) * 2 * KC * T;
+    const double* Bs = As + KC * T;
+    const int kmax = min(KC, n - ch * KC);
+    for (int k = 0; k < kmax; ++k) {
+      double a[R], b[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) a[i] = As[k * T + ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < R; ++j) b[j] = Bs[k * T + tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < R; ++i)
+#pragma unroll
+        for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int gr = ty + 16 * i;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int gc = tx + 16 * j;
+      if (gr < n && gc < n) {
+        double* cp = C + gr + (size_t)ldc * gc;
+        *cp = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Square GEMM dispatch: one exact-size tile for n <= 96 (FP64: double-
+// buffered), 64 x 64 tiles above.  smem must hold 4 * 16 * 96 doubles.
+// lowp = compute in FP32.
 template <int NT, typename TM>
 __device__ __forceinline__ void gemm_prec(int n, bool tA, const TM* A, int lda, bool tB, const TM* B, int ldb,
                                           TM* C, int ldc, double alpha, double beta, void* smem, bool lowp)
@@ -284,11 +364,11 @@ __device__ __forceinline__ void gemm_prec(int n, bool tA, const TM* A, int lda, 
     else if (n <= 96) gemm_tile<NT, 6, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
     else gemm_rect<NT, TM, float>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
   } else {
-    if (n <= 32) gemm_tile<NT, 2, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 48) gemm_tile<NT, 3, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 64) gemm_tile<NT, 4, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 80) gemm_tile<NT, 5, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 96) gemm_tile<NT, 6, TM, TM>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    if (n <= 32) gemm_tile_db<NT, 2>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 48) gemm_tile_db<NT, 3>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 64) gemm_tile_db<NT, 4>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 80) gemm_tile_db<NT, 5>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 96) gemm_tile_db<NT, 6>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
     else gemm_rect<NT, TM, TM>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
   }
 }
@@ -468,6 +548,145 @@ __device__ void tri_inverse(int n, const T* L, int ldl, T* Li, int ldi, T* sD, v
     if (rem > 0)
       gemm_rect<NT, T, T>(rem, kb + bs, bs, false, L + r0 + (size_t)ldl * kb, ldl, false, Li + kb, ldi, Li + r0,
                           ldi, -1.0, 1.0, smem);
+  }
+  __syncthreads();
+}
+
+// Two independent Cholesky factorisations (LAPACK pivot rule, as cholesky
+// with adjust = false) in lockstep: the diagonal blocks of A0 and A1 are
+// factored concurrently by warps 0 and 1, the panels share one barrier, and
+// the trailing updates follow each other.  Used for X and Z in the update
+// step.  sD0, sD1: SD_DOUBLES elements of T each.  Returns 0 when both
+// succeed, else nonzero (both matrices are then left partially factored).
+template <int NT, typename T>
+__device__ int cholesky_pair(int n, T* A0, T* A1, int lda, T* sD0, T* sD1, void* smem, int* s_flag2)
+{
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  T* Am[2] = {A0, A1};
+  T* sDm[2] = {sD0, sD1};
+  for (int kb = 0; kb < n; kb += NB) {
+    const int bs = min(NB, n - kb);
+    for (int t = tid; t < 2 * NB * NB; t += NT) {
+      const int mtx = t / (NB * NB), u = t % (NB * NB);
+      const int r = u % NB, c = u / NB;
+      if (r < bs && c <= r) sDm[mtx][r + LDD * c] = Am[mtx][(kb + r) + (size_t)lda * (kb + c)];
+    }
+    __syncthreads();
+    if (wid < 2) {
+      T* sD = sDm[wid];
+      const int fail = warp_potrf32<T>(bs, sD, false, kb);
+      if (lane == 0) s_flag2[wid] = fail;
+      if (!fail && lane < bs) sD[NB * LDD + lane] = (T)1 / sD[lane + LDD * lane];
+    }
+    __syncthreads();
+    const int f = s_flag2[0] | s_flag2[1];
+    if (f) { __syncthreads(); return 1; }
+    for (int t = tid; t < 2 * NB * NB; t += NT) {
+      const int mtx = t / (NB * NB), u = t % (NB * NB);
+      const int r = u % NB, c = u / NB;
+      if (r < bs && c <= r) Am[mtx][(kb + r) + (size_t)lda * (kb + c)] = sDm[mtx][r + LDD * c];
+    }
+    const int r0 = kb + bs, rem = n - r0;
+    if (rem > 0) {
+      // panels of both matrices: A[r, kb:kb+bs] := A[r, kb:kb+bs] L_bb^{-T},
+      // four rows per warp at a time
+      const int rows4 = (rem + 3) / 4;
+      for (int job = wid; job < 2 * rows4; job += NT / 32) {
+        const int mtx = job / rows4, rb = r0 + 4 * (job % rows4);
+        T* A = Am[mtx];
+        const T* sD = sDm[mtx];
+        T x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          x[u] = (lane < bs && rb + u < n) ? A[(rb + u) + (size_t)lda * (kb + lane)] : (T)0;
+        for (int c = 0; c < bs; ++c) {
+          const T dinv = sD[NB * LDD + c];
+          const T lc = (lane > c && lane < bs) ? sD[lane + LDD * c] : (T)0;
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (lane == c) x[u] *= dinv;
+            const T xc = __shfl_sync(0xffffffffu, x[u], c);
+            x[u] -= xc * lc;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (lane < bs && rb + u < n) A[(rb + u) + (size_t)lda * (kb + lane)] = x[u];
+      }
+      __syncthreads();
+      for (int mtx = 0; mtx < 2; ++mtx) {
+        const T* P = Am[mtx] + r0 + (size_t)lda * kb;
+        gemm_rect<NT, T, T>(rem, rem, bs, false, P, lda, true, P, lda, Am[mtx] + r0 + (size_t)lda * r0, lda, -1.0,
+                            1.0, smem, true, 0);
+      }
+    }
+  }
+  for (int t = tid; t < 2 * n * n; t += NT) {
+    const int mtx = t / (n * n), u = t % (n * n);
+    const int i = u % n, k = u / n;
+    if (i < k) Am[mtx][i + (size_t)lda * k] = (T)0;
+  }
+  __syncthreads();
+  return 0;
+}
+
+// Li0 = L0^{-1} and Li1 = L1^{-1} in lockstep (tri_inverse for two lower
+// triangles): one staging barrier and one substitution barrier per block
+// column for both.  Li must not alias L.
+template <int NT, typename T>
+__device__ void tri_inverse_pair(int n, const T* L0, const T* L1, int ldl, T* Li0, T* Li1, int ldi, T* sD0, T* sD1,
+                                 void* smem)
+{
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const T* Lm[2] = {L0, L1};
+  T* Lim[2] = {Li0, Li1};
+  T* sDm[2] = {sD0, sD1};
+  for (int t = tid; t < 2 * n * n; t += NT) {
+    const int mtx = t / (n * n), u = t % (n * n);
+    const int i = u % n, j = u / n;
+    Lim[mtx][i + (size_t)ldi * j] = (i == j) ? (T)1 : (T)0;
+  }
+  for (int kb = 0; kb < n; kb += NB) {
+    const int bs = min(NB, n - kb);
+    for (int t = tid; t < 2 * NB * NB; t += NT) {
+      const int mtx = t / (NB * NB), u = t % (NB * NB);
+      const int r = u % NB, c = u / NB;
+      if (r < bs && c <= r) sDm[mtx][r + LDD * c] = Lm[mtx][(kb + r) + (size_t)ldl * (kb + c)];
+    }
+    for (int t = tid; t < 2 * NB; t += NT) {
+      const int mtx = t / NB, r = t % NB;
+      if (r < bs) sDm[mtx][NB * LDD + r] = (T)1 / Lm[mtx][(kb + r) + (size_t)ldl * (kb + r)];
+    }
+    __syncthreads();
+    const int cols4 = (kb + bs + 3) / 4;
+    for (int job = wid; job < 2 * cols4; job += NT / 32) {
+      const int mtx = job / cols4, cb = 4 * (job % cols4);
+      T* Li = Lim[mtx];
+      const T* sD = sDm[mtx];
+      T x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        x[u] = (lane < bs && cb + u < kb + bs) ? Li[(kb + lane) + (size_t)ldi * (cb + u)] : (T)0;
+      for (int p = 0; p < bs; ++p) {
+        const T dinv = sD[NB * LDD + p];
+        const T lp = (lane > p && lane < bs) ? sD[lane + LDD * p] : (T)0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (lane == p) x[u] *= dinv;
+          const T xp = __shfl_sync(0xffffffffu, x[u], p);
+          x[u] -= lp * xp;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (lane < bs && cb + u < kb + bs) Li[(kb + lane) + (size_t)ldi * (cb + u)] = x[u];
+    }
+    __syncthreads();
+    const int r0 = kb + bs, rem = n - r0;
+    if (rem > 0)
+      for (int mtx = 0; mtx < 2; ++mtx)
+        gemm_rect<NT, T, T>(rem, kb + bs, bs, false, Lm[mtx] + r0 + (size_t)ldl * kb, ldl, false, Lim[mtx] + kb,
+                            ldi, Lim[mtx] + r0, ldi, -1.0, 1.0, smem);
   }
   __syncthreads();
 }
