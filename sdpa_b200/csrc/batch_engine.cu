@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       {
         // R and XDZ are free here (both are rebuilt by the next predictor)
         double mins[2];
-        min_eig_pair(n, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins);
+        min_eig_pair(n, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins, dz_diag);
         const double minX = mins[0], minZ = mins[1];
         double CdX = c_dot(dX);
         double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);

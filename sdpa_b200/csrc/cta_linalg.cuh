@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <type_traits>
+
 namespace sdpab {
 namespace cta {
 
@@ -107,26 +109,160 @@ __device__ double dot_vec(int n, const double* a, const double* b, Reducer& R)
   return block_sum<NT>(s, R);
 }
 
+// Asynchronous global -> shared copy of one element of 4 or 8 bytes
+// (cp.async; zero fill when `valid` is false, the source pointer must still
+// be a valid address), and the group fences around it.
+template <typename T>
+__device__ __forceinline__ void cp_async_el(void* smem_dst, const T* gsrc, bool valid)
+{
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp_async_el: 4- or 8-byte elements");
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(valid ? 8 : 0));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gsrc), "r"(valid ? 4 : 0));
+}
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid)
+{
+  cp_async_el<double>(smem_dst, (const double*)gsrc, valid);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // ------------------------------------------------------------ GEMM
 // All GEMM / factorisation routines are templated on the matrix storage type
 // TM and the compute type TC (TC = float with TM = double is the mixed
 // precision path: operands are rounded to FP32 when staged in shared memory,
 // products accumulate in FP32, results are stored back in FP64).
 //
+// 64 x 64 output tiles, K staged in chunks of GK.
+constexpr int GT = 64, GK = 16;
+// shared memory (elements) a gemm_rect call may use: two stages of A and B
+constexpr int GEMM_RECT_SMEM = 4 * GK * GT;
+
+// gemm_rect with double-buffered cp.async staging (storage type = compute
+// type): the (tile, K chunk) steps form one pipeline, chunk s+1 (of this or
+// the next live tile) is copied while chunk s is multiplied, one barrier per
+// step.  smem: 4 * GK * GT elements of T.
+template <int NT, typename T>
+__device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T* A, int lda, bool tB, const T* B,
+                                          int ldb, T* C, int ldc, double alpha, double beta, void* smem_v,
+                                          bool lower, int diag_off)
+{
+  T* buf = (T*)smem_v;  // [2][As: GK*GT | Bs: GK*GT]
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT, ntile = tm * tn;
+  const int nk = (K + GK - 1) / GK;
+  auto live = [&](int tile) {
+    const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
+    return !(lower && r0 + GT - 1 + diag_off < c0);
+  };
+  auto next_live = [&](int tile) {
+    while (tile < ntile && !live(tile)) ++tile;
+    return tile;
+  };
+  auto issue = [&](int tile, int k0, int which) {
+    const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
+    T* As = buf + which * 2 * GK * GT;
+    T* Bs = As + GK * GT;
+    for (int t = threadIdx.x; t < GK * GT; t += NT) {
+      int r, k;
+      if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
+      const int gr = r0 + r, gk = k0 + k;
+      const bool va = gr < M && gk < K;
+      cp_async_el<T>(&As[k * GT + r], va ? (tA ? A + gk + (size_t)lda * gr : A + gr + (size_t)lda * gk) : A, va);
+      int c;
+      if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
+      const int gc = c0 + c, gk2 = k0 + k;
+      const bool vb = gc < N && gk2 < K;
+      cp_async_el<T>(&Bs[k * GT + c], vb ? (tB ? B + gc + (size_t)ldb * gk2 : B + gk2 + (size_t)ldb * gc) : B, vb);
+    }
+    cp_async_commit();
+  };
+  int tile = next_live(0);
+  if (tile >= ntile) {
+    __syncthreads();
+    return;
+  }
+  int it_tile = tile, it_k = 0;  // the next (tile, chunk) to copy
+  auto advance = [&]() {
+    if (++it_k == nk) {
+      it_k = 0;
+      it_tile = next_live(it_tile + 1);
+    }
+  };
+  issue(it_tile, 0, 0);
+  advance();
+  int which = 0;
+  while (tile < ntile) {
+    const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = (T)0;
+    for (int kc = 0; kc < nk; ++kc) {
+      cp_async_wait_all();
+      __syncthreads();  // this step's chunk is visible; the other buffer is free
+      if (it_tile < ntile) {
+        issue(it_tile, it_k * GK, which ^ 1);
+        advance();
+      }
+      const T* As = buf + which * 2 * GK * GT;
+      const T* Bs = As + GK * GT;
+      const int kmax = min(GK, K - kc * GK);
+      for (int k = 0; k < kmax; ++k) {
+        T a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[k * GT + ty + 16 * i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[k * GT + tx + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+      }
+      which ^= 1;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int gr = r0 + ty + 16 * i;
+      if (gr >= M) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int gc = c0 + tx + 16 * j;
+        if (gc >= N) continue;
+        if (lower && gr + diag_off < gc) continue;
+        T* cp = C + gr + (size_t)ldc * gc;
+        *cp = (T)((beta == 0.0) ? alpha * (double)acc[i][j] : alpha * (double)acc[i][j] + beta * (double)(*cp));
+      }
+    }
+    tile = next_live(tile + 1);
+  }
+  __syncthreads();
+}
+
 // gemm_rect: C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C.
 // 64 x 64 output tiles, 256 threads as a 16 x 16 grid with 4 x 4 outputs each
-// (rows ty + 16 i, columns tx + 16 j), K staged in chunks of GK with the next
-// chunk prefetched into registers.  lower = true updates only entries with
-// (row + diag_off >= col) and skips tiles entirely above that diagonal
-// (trailing updates of factorisations).  smem: 2 * GK * GT elements of TC.
-// Ends with a barrier.
-constexpr int GT = 64, GK = 16;
+// (rows ty + 16 i, columns tx + 16 j), K staged in chunks of GK.  When the
+// storage and compute types agree the staging is gemm_rect_db's (cp.async,
+// two stages); the mixed FP64-storage / FP32-compute form prefetches the
+// next chunk into registers and converts while storing.  lower = true
+// updates only entries with (row + diag_off >= col) and skips tiles
+// entirely above that diagonal (trailing updates of factorisations).
+// smem: GEMM_RECT_SMEM elements of TC.  Ends with a barrier.
 template <int NT, typename TM, typename TC>
 __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const TM* A, int lda, bool tB,
                                        const TM* B, int ldb, TM* C, int ldc, double alpha, double beta,
                                        void* smem_v, bool lower = false, int diag_off = 0)
 {
   static_assert(NT == 256, "gemm tile mapping assumes 256 threads");
+  if constexpr (std::is_same<TM, TC>::value) {
+    if (K > 0) {
+      gemm_rect_db<NT, TM>(M, N, K, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem_v, lower, diag_off);
+      return;
+    }
+  }
   constexpr int PER = GK * GT / NT;  // staged elements per thread and operand
   TC* As = (TC*)smem_v;          // [GK][GT]  As[k*GT + r]
   TC* Bs = As + GK * GT;         // [GK][GT]  Bs[k*GT + c]
@@ -269,17 +405,6 @@ __device__ __noinline__ void gemm_tile(int n, bool tA, const TM* A, int lda, boo
   }
   __syncthreads();
 }
-
-// Asynchronous global -> shared copy of one 8-byte element (cp.async, zero
-// fill when `valid` is false; the source pointer must still be a valid
-// address), and the group fences around it.
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid)
-{
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(valid ? 8 : 0));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // FP64 gemm_tile with double-buffered staging: chunk k+1 is copied by
 // cp.async while chunk k is multiplied, so each chunk costs one barrier and
@@ -752,65 +877,92 @@ __device__ void chol_solve(int n, const T* L, int ldl, T* x, T* sD)
 }
 
 // ------------------------------------------------------------ eigenvalues
-// Number of eigenvalues < x of the symmetric tridiagonal (d, e) of order k:
-// sign changes of the leading principal minors p_i(x) of T - xI (Sturm
-// sequence), by the division-free recurrence
-//   p_{i+1} = (d_i - x) p_i - e_{i-1}^2 p_{i-1},
-// rescaled by a power of two whenever |p_i| leaves [2^-400, 2^400].
-__device__ __forceinline__ int sturm_count(int k, const double* d, const double* e, double x)
+// Number of eigenvalues < x of a symmetric tridiagonal of order k given as
+// its diagonal ds and squared off-diagonal e2 (e2[i] couples i and i+1),
+// scaled so that every entry is at most 1 in magnitude: sign changes of the
+// leading principal minors p_i(x) of T - xI (Sturm sequence), by the
+// division-free recurrence p_{i+1} = (d_i - x) p_i - e_{i-1}^2 p_{i-1}.
+// With the scaling a minor grows at most 5x per step for x inside the
+// Gershgorin interval, so the pair is checked for rescaling every 8 steps
+// only; sign changes are counted from the sign bits.
+__device__ __forceinline__ int sturm_count(int k, const double* ds, const double* e2, double x)
 {
-  double pm = 1.0, p = d[0] - x;
+  double pm = 1.0, p = ds[0] - x;
   int cnt = (p < 0.0) ? 1 : 0;
   for (int i = 1; i < k; ++i) {
-    double pn = (d[i] - x) * p - e[i - 1] * e[i - 1] * pm;
+    double pn = fma(ds[i] - x, p, -e2[i - 1] * pm);
     if (pn == 0.0) pn = (p < 0.0) ? 1.0e-300 : -1.0e-300;  // a zero minor counts as a sign change
-    cnt += ((pn < 0.0) != (p < 0.0)) ? 1 : 0;
+    cnt += (int)(((unsigned)__double2hiint(pn) ^ (unsigned)__double2hiint(p)) >> 31);
     pm = p;
     p = pn;
-    // rescale the pair when it leaves [1e-150, 1e150] (a compare per step;
-    // the exponent arithmetic only on the rare rescale)
-    const double big = fmax(fabs(p), fabs(pm));
-    if (big > 1.0e150 || big < 1.0e-150) {
-      const int ex = ilogb(big);
-      p = scalbn(p, -ex);
-      pm = scalbn(pm, -ex);
+    if ((i & 7) == 0) {
+      const double big = fmax(fabs(p), fabs(pm));
+      if (big > 1.0e100 || big < 1.0e-100) {
+        const int ex = ilogb(big);
+        p = scalbn(p, -ex);
+        pm = scalbn(pm, -ex);
+      }
     }
   }
   return cnt;
 }
 
-// Smallest eigenvalue of a symmetric tridiagonal (d, e) of order k, and the
-// magnitude of the last component of its unit eigenvector (the Lanczos error
-// estimate).  Warp multisection until the bracket is narrow, then Newton
-// steps on f(x) = det(T - xI) (its smallest root is approached monotonically
-// from the left), each kept inside the bracket, until the step is below one
-// ulp of the result (or of 1e-2 of the matrix scale for a result near zero).
-// The eigenvector component comes from the same recurrences: for an
-// eigenvalue lam of an unreduced tridiagonal, u_k^2 = -P_{k-1}(lam) / P_k'(lam)
-// with P_j the leading principal minors of T - lam I, which Newton has just
-// evaluated.  `upper` is a known upper bound of the result (the smallest Ritz
-// value of a leading principal submatrix, by interlacing; 1e300 for none):
-// the first round then probes geometrically spaced points below it, which
-// brackets the value in one round when it has moved little.  Called by one
-// full warp; every lane returns the same values.
+// Smallest eigenvalue of a symmetric tridiagonal (d, e) of order k <= 64,
+// and the magnitude of the last component of its unit eigenvector (the
+// Lanczos error estimate).
+// * The matrix is scaled by its Gershgorin radius (lane-parallel bounds)
+//   into `work` (2 * 64 doubles: diagonal, squared off-diagonal).
+// * Warp multisection (33 points per round) until the bracket is narrow,
+//   then Newton steps on f(x) = det(T - xI), whose smallest root is
+//   approached monotonically from the left; each step is kept inside the
+//   bracket, until the step is below one ulp of the result (or of 1e-2 of
+//   the matrix scale for a result near zero).
+// * The eigenvector component comes from the same recurrences: for an
+//   eigenvalue lam of an unreduced tridiagonal,
+//   u_k^2 = -P_{k-1}(lam) / P_k'(lam), with P_j the leading principal minors
+//   of T - lam I, which Newton has just evaluated.
+// * `upper` is a known upper bound of the result (the smallest Ritz value of
+//   a leading principal submatrix, by interlacing; 1e300 for none).  The
+//   first round then probes geometrically spaced points below it, which
+//   brackets the value in one round when it has moved little.
+// Called by one full warp; every lane returns the same values.
 static __device__ double tridiag_min_eig_warp(int k, const double* d, const double* e, double upper,
-                                              double* ulast)
+                                              double* ulast, double* work)
 {
   const int lane = threadIdx.x & 31;
+  // Gershgorin interval, lane-parallel (k <= 64: two entries per lane)
   double lo = 1.0e300, hi = -1.0e300;
-  for (int i = 0; i < k; ++i) {
+  for (int i = lane; i < k; i += 32) {
     const double r = ((i > 0) ? fabs(e[i - 1]) : 0.0) + ((i < k - 1) ? fabs(e[i]) : 0.0);
     lo = fmin(lo, d[i] - r);
     hi = fmax(hi, d[i] + r);
   }
-  const double span = fmax(fabs(lo), fabs(hi));
-  lo -= 1.0e-15 * span + 1.0e-300;
-  hi += 1.0e-15 * span + 1.0e-300;
-  if (upper < hi && upper > lo) {
-    // probes p_0 = upper + h (above the value), p_l = upper + h - h 4^l
-    const double h = 1.0e-12 * fmax(fabs(upper), 1.0e-3 * span) + 1.0e-300;
-    const double x = (lane == 0) ? upper + h : upper + h - h * exp2(2.0 * lane);
-    const bool below = (x > lo) && sturm_count(k, d, e, x) >= 1;
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  const double sc = fmax(fabs(lo), fabs(hi));
+  if (!(sc > 0.0)) {  // the zero matrix
+    *ulast = (k > 1) ? 0.0 : 1.0;
+    return 0.0;
+  }
+  const double inv = 1.0 / sc;
+  double* ds = work;
+  double* e2 = work + 64;
+  for (int i = lane; i < k; i += 32) {
+    ds[i] = d[i] * inv;
+    const double es = (i < k - 1) ? e[i] * inv : 0.0;
+    e2[i] = es * es;
+  }
+  __syncwarp();
+  lo = lo * inv - 1.0e-15;  // |lo|, |hi| <= 1 after scaling
+  hi = hi * inv + 1.0e-15;
+  const double up = upper * inv;
+  if (up < hi && up > lo) {
+    // probes p_0 = up + h (above the value), p_l = up + h - h 4^l
+    const double h = 1.0e-12 * fmax(fabs(up), 1.0e-3) + 1.0e-300;
+    const double x = (lane == 0) ? up + h : up + h - h * exp2(2.0 * lane);
+    const bool below = (x > lo) && sturm_count(k, ds, e2, x) >= 1;
     const unsigned ball = __ballot_sync(0xffffffffu, below);
     if (ball & 1u) {  // the bound holds: bracket between the last probe with
                       // an eigenvalue below it and the next one
@@ -821,12 +973,11 @@ static __device__ double tridiag_min_eig_warp(int k, const double* d, const doub
       if (f < 32) lo = fmax(lo, xlo);
     }
   }
-  const double floor_abs = 1.0e-12 * span + 1.0e-300;
   for (int round = 0; round < 24; ++round) {
-    if (hi - lo <= 1.0e-7 * fmax(fabs(lo), fabs(hi)) + floor_abs) break;
+    if (hi - lo <= 1.0e-7 * fmax(fabs(lo), fabs(hi)) + 1.0e-12) break;
     const double w = (hi - lo) / 33.0;
     const double x = lo + w * (lane + 1);
-    const int c = sturm_count(k, d, e, x);
+    const int c = sturm_count(k, ds, e2, x);
     const unsigned ball = __ballot_sync(0xffffffffu, c >= 1);
     const int f = ball ? (__ffs(ball) - 1) : 32;  // first point with an eigenvalue below it
     const double nlo = lo + w * f;
@@ -838,19 +989,19 @@ static __device__ double tridiag_min_eig_warp(int k, const double* d, const doub
   // P_{i+1} = (d_i - x) P_i - e^2 P_{i-1} and its derivative
   // D_{i+1} = -P_i + (d_i - x) D_i - e^2 D_{i-1}, rescaled together.
   double x = lo, Plast = 0.0, Dlast = 0.0;
-  const double tol_abs = 2.2e-18 * span;
   for (int it = 0; it < 20; ++it) {
-    double Pm = 1.0, P = d[0] - x, Dm = 0.0, Dv = -1.0;
+    double Pm = 1.0, P = ds[0] - x, Dm = 0.0, Dv = -1.0;
     for (int i = 1; i < k; ++i) {
-      const double e2 = e[i - 1] * e[i - 1];
-      const double dx = d[i] - x;
-      const double Pn = dx * P - e2 * Pm;
-      const double Dn = -P + dx * Dv - e2 * Dm;
+      const double dx = ds[i] - x, ee = e2[i - 1];
+      const double Pn = fma(dx, P, -ee * Pm);
+      const double Dn = fma(dx, Dv, -fma(ee, Dm, P));
       Pm = P; P = Pn; Dm = Dv; Dv = Dn;
-      const double big = fmax(fmax(fabs(P), fabs(Dv)), fmax(fabs(Pm), fabs(Dm)));
-      if (big > 1.0e150 || big < 1.0e-150) {
-        const int ex = ilogb(big);
-        P = scalbn(P, -ex); Pm = scalbn(Pm, -ex); Dv = scalbn(Dv, -ex); Dm = scalbn(Dm, -ex);
+      if ((i & 7) == 0) {
+        const double big = fmax(fmax(fabs(P), fabs(Dv)), fmax(fabs(Pm), fabs(Dm)));
+        if (big > 1.0e100 || big < 1.0e-100) {
+          const int ex = ilogb(big);
+          P = scalbn(P, -ex); Pm = scalbn(Pm, -ex); Dv = scalbn(Dv, -ex); Dm = scalbn(Dm, -ex);
+        }
       }
     }
     Plast = Pm;  // P_{k-1}(x) and P_k'(x), same scale
@@ -858,7 +1009,7 @@ static __device__ double tridiag_min_eig_warp(int k, const double* d, const doub
     if (!(Dv != 0.0) || P != P || Dv != Dv) break;
     const double xn = x - P / Dv;
     if (!(xn >= lo) || !(xn <= hi)) break;
-    if (fabs(xn - x) <= fmax(2.2e-16 * fabs(xn), tol_abs)) { x = xn; break; }
+    if (fabs(xn - x) <= fmax(2.2e-16 * fabs(xn), 2.2e-18)) { x = xn; break; }
     x = xn;
   }
   double u2 = 1.0;
@@ -868,7 +1019,7 @@ static __device__ double tridiag_min_eig_warp(int k, const double* d, const doub
     if (u2 > 1.0) u2 = 1.0;
   }
   *ulast = sqrt(u2);
-  return x;
+  return x * sc;
 }
 
 }  // namespace cta

@@ -58,23 +58,29 @@ static __device__ inline void eig_scratch_carve(EigScratch& s, double* p, int nm
 // Lal::getMinEigen (sdpa_linear.cpp:29-143) for NM independent matrices in
 // lockstep: Lanczos on each M_j = L D L^T with the reference's start vector
 // (all ones), stopping rule and error correction, each process advancing
-// only while its own stopping test says so.  Running the X and Z step-length
-// problems together shares every block barrier between them and lets warp j
-// solve process j's tridiagonal while warp 1-j solves the other's.  M_j is
-// formed beforehand by two GEMMs (the reference applies L^T, D, L to each
-// Lanczos vector; the products agree to rounding), so each step is one
-// coalesced matvec.  The tridiagonal eigen-solve (dsteqr in the reference) is
-// a warp multisection + Newton for the smallest Ritz value, which also yields
-// the last component of its eigenvector.
+// only while its own stopping test says so.  M_j is formed beforehand by two
+// GEMMs (the reference applies L^T, D, L to each Lanczos vector; the
+// products agree to rounding), so each step is one coalesced matvec.  The
+// tridiagonal eigen-solve (dsteqr in the reference) is a warp multisection +
+// Newton for the smallest Ritz value, which also yields the last component
+// of its eigenvector.
+//
+// Schedule.  Running X and Z together shares every block barrier between
+// them.  The tridiagonal solve that step k calls for only decides whether
+// step k+1 happens, so it runs (warp j for process j) while the other warps
+// already compute step k+1's matvec; if the stopping test then ends the
+// process, that matvec is discarded.  The values computed and the decisions
+// taken are those of the plain sequence: per step, alpha = q.Mq, the
+// residual, beta, and at the steps the reference chooses (kk >= sqrt(k),
+// k = n-1 or k > sqrt(n+9)) the Ritz value and error of the tridiagonal.
 template <int NM>
-static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, EigScratch& s,
-                                                          double* out)
+static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, EigScratch& s, double* out)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   constexpr int NW = NT / 32;
   double beta[NM], mn[NM], mn_old[NM], err[NM];
   int k[NM], kk[NM];
-  bool act[NM];
+  bool act[NM], pend[NM];
   const double sqn = sqrt((double)n);
 #pragma unroll
   for (int j = 0; j < NM; ++j) {
@@ -86,17 +92,11 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
     mn_old[j] = 1.0e52;
     err[j] = 1.0e10;
     k[j] = kk[j] = 0;
+    act[j] = true;
+    pend[j] = false;
   }
   for (;;) {
-    bool any = false;
-#pragma unroll
-    for (int j = 0; j < NM; ++j) {
-      act[j] = k[j] < n && k[j] < sqn + 10 && k[j] < TRI_MAX - 1 && beta[j] > 1.0e-16 &&
-               (fabs(mn[j] - mn_old[j]) > 1.0e-5 * fabs(mn[j]) + 1.0e-8 ||
-                fabs(err[j] * beta[j]) > 1.0e-2 * fabs(mn[j]) + 1.0e-4);
-      any |= act[j];
-    }
-    if (!any) break;
+    // (a) start the next step of every running process: q = r / beta
 #pragma unroll
     for (int j = 0; j < NM; ++j) {
       if (!act[j]) continue;
@@ -105,56 +105,92 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
       for (int i = tid; i < n; i += NT) { v.qold[i] = v.q[i]; v.q[i] = v.r[i] * ib; }
     }
     __syncthreads();
-    // w_j = M_j q_j: each warp takes CW columns of every active matrix per
-    // pass and issues all their loads (CW x 4 per lane and matrix for
-    // n <= 128) before the FMAs, so the latency of a column is paid once per
-    // pass.
+    // (b) warps 0 / 1 solve the pending tridiagonals while the remaining
+    // warps multiply; CW columns of every running matrix per warp and pass,
+    // all loads of a pass issued before its FMAs
+    bool any_pend = false;
+#pragma unroll
+    for (int j = 0; j < NM; ++j) any_pend |= pend[j];
+    const int w0 = any_pend ? NM : 0;
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      if (wid != j || !pend[j]) continue;
+      LanczosVec& v = s.v[j];
+      double ul;
+      const double lam = cta::tridiag_min_eig_warp(k[j], v.d, v.e, mn[j], &ul, v.work);
+      if (lane == 0) {
+        v.val[0] = lam;
+        v.val[1] = ul;
+      }
+    }
     constexpr int CW = (NM == 2) ? 2 : 4;
     double part[NM];
 #pragma unroll
     for (int j = 0; j < NM; ++j) part[j] = 0.0;
-    for (int i0 = wid * CW; i0 < n; i0 += CW * NW) {
-      double acc[NM][CW];
-#pragma unroll
-      for (int j = 0; j < NM; ++j)
-#pragma unroll
-        for (int c = 0; c < CW; ++c) acc[j][c] = 0.0;
-      for (int kx0 = 0; kx0 < n; kx0 += 128) {
-        double qv[NM][4], mv[NM][CW][4];
-#pragma unroll
-        for (int j = 0; j < NM; ++j) {
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int kx = kx0 + lane + 32 * u;
-            qv[j][u] = (act[j] && kx < n) ? s.v[j].q[kx] : 0.0;
-#pragma unroll
-            for (int c = 0; c < CW; ++c)
-              mv[j][c][u] = (act[j] && kx < n && i0 + c < n) ? Ms[j][kx + (size_t)n * (i0 + c)] : 0.0;
-          }
-        }
+    if (wid >= w0) {
+      const int nwk = NW - w0;
+      for (int i0 = (wid - w0) * CW; i0 < n; i0 += CW * nwk) {
+        double acc[NM][CW];
 #pragma unroll
         for (int j = 0; j < NM; ++j)
 #pragma unroll
-          for (int c = 0; c < CW; ++c)
+          for (int c = 0; c < CW; ++c) acc[j][c] = 0.0;
+        for (int kx0 = 0; kx0 < n; kx0 += 128) {
+          double qv[NM][4], mv[NM][CW][4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) acc[j][c] += mv[j][c][u] * qv[j][u];
-      }
+          for (int j = 0; j < NM; ++j) {
 #pragma unroll
-      for (int j = 0; j < NM; ++j) {
-        double wv = 0.0;
+            for (int u = 0; u < 4; ++u) {
+              const int kx = kx0 + lane + 32 * u;
+              qv[j][u] = (act[j] && kx < n) ? s.v[j].q[kx] : 0.0;
 #pragma unroll
-        for (int c = 0; c < CW; ++c) {
-          for (int o = 16; o > 0; o >>= 1) acc[j][c] += __shfl_xor_sync(0xffffffffu, acc[j][c], o);
-          if (lane == c) wv = acc[j][c];
+              for (int c = 0; c < CW; ++c)
+                mv[j][c][u] = (act[j] && kx < n && i0 + c < n) ? Ms[j][kx + (size_t)n * (i0 + c)] : 0.0;
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < NM; ++j)
+#pragma unroll
+            for (int c = 0; c < CW; ++c)
+#pragma unroll
+              for (int u = 0; u < 4; ++u) acc[j][c] += mv[j][c][u] * qv[j][u];
         }
-        if (act[j] && lane < CW && i0 + lane < n) {
-          s.v[j].w[i0 + lane] = wv;
-          part[j] += s.v[j].q[i0 + lane] * wv;
+#pragma unroll
+        for (int j = 0; j < NM; ++j) {
+          double wv = 0.0;
+#pragma unroll
+          for (int c = 0; c < CW; ++c) {
+            for (int o = 16; o > 0; o >>= 1) acc[j][c] += __shfl_xor_sync(0xffffffffu, acc[j][c], o);
+            if (lane == c) wv = acc[j][c];
+          }
+          if (act[j] && lane < CW && i0 + lane < n) {
+            s.v[j].w[i0 + lane] = wv;
+            part[j] += s.v[j].q[i0 + lane] * wv;
+          }
         }
       }
     }
     double alpha[NM];
-    cta::block_sum_n<NT, NM>(part, alpha, *s.R);  // the barrier also publishes w
+    cta::block_sum_n<NT, NM>(part, alpha, *s.R);  // publishes w and the tridiagonal results
+    // (c) take in the Ritz values, then the reference's test for this step
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      if (pend[j]) {
+        mn_old[j] = mn[j];
+        mn[j] = s.v[j].val[0];
+        err[j] = s.v[j].val[1];
+        pend[j] = false;
+      }
+      if (act[j])
+        act[j] = k[j] < n && k[j] < sqn + 10 && k[j] < TRI_MAX - 1 && beta[j] > 1.0e-16 &&
+                 (fabs(mn[j] - mn_old[j]) > 1.0e-5 * fabs(mn[j]) + 1.0e-8 ||
+                  fabs(err[j] * beta[j]) > 1.0e-2 * fabs(mn[j]) + 1.0e-4);
+      any |= act[j];
+    }
+    if (!any) break;
+    // (d) finish the step: residual, its norm, and whether this step's
+    // tridiagonal (order k+1) is to be solved
     double rpart[NM];
 #pragma unroll
     for (int j = 0; j < NM; ++j) {
@@ -166,41 +202,20 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
         v.r[i] = rv;
         rpart[j] += rv * rv;
       }
-    }
-#pragma unroll
-    for (int j = 0; j < NM; ++j) {
-      if (wid != j || !act[j]) continue;
-      LanczosVec& v = s.v[j];
       const int kj = k[j];
-      if (lane == 0) v.d[kj] = alpha[j];
-      __syncwarp();
+      if (tid == 0) v.d[kj] = alpha[j];
       if (kk[j] >= sqrt((double)kj) || kj == n - 1 || kj > sqrt((double)n + 9)) {
-        double ul;
-        const double lam = cta::tridiag_min_eig_warp(kj + 1, v.d, v.e, mn[j], &ul);
-        if (lane == 0) {
-          v.val[0] = lam;
-          v.val[1] = ul;
-          v.val[2] = 1.0;
-        }
-      } else if (lane == 0) {
-        v.val[2] = 0.0;
+        pend[j] = true;
+        kk[j] = 0;
       }
     }
-    // the barrier of this reduction also publishes the warps' eigen results
     double rr[NM];
     cta::block_sum_n<NT, NM>(rpart, rr, *s.R);
 #pragma unroll
     for (int j = 0; j < NM; ++j) {
       if (!act[j]) continue;
-      LanczosVec& v = s.v[j];
-      if (v.val[2] != 0.0) {
-        kk[j] = 0;
-        mn_old[j] = mn[j];
-        mn[j] = v.val[0];
-        err[j] = v.val[1];
-      }
       beta[j] = sqrt(rr[j]);
-      if (tid == 0) v.e[k[j]] = beta[j];
+      if (tid == 0) s.v[j].e[k[j]] = beta[j];
       ++k[j];
       ++kk[j];
     }
@@ -270,7 +285,7 @@ static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
     if (n >= 2 && lane == 0) lv.e[n - 2] = M[(n - 1) + n * (n - 2)];
     __syncwarp();
     double ul;
-    const double lam = cta::tridiag_min_eig_warp(n, lv.d, lv.e, 1.0e300, &ul);
+    const double lam = cta::tridiag_min_eig_warp(n, lv.d, lv.e, 1.0e300, &ul, lv.work + 128);
     if (lane == 0) lv.val[0] = lam;
   }
   __syncthreads();
@@ -301,13 +316,22 @@ static __device__ double min_eig(int n, const double* L, const double* D, double
 // lambda_min(Lz Dz Lz^T), with the two Lanczos processes in lockstep.
 // Wx1, Wx2, Wz1, Wz2: n x n scratch (Wx2 and Wz2 receive the formed
 // matrices).  The matrices are staged in shared memory while they fit.
+// z_diag: Dz is diagonal, so Dz Lz^T is a row scaling of Lz^T (no GEMM).
 static __device__ void min_eig_pair(int n, const double* Lx, const double* Dx, const double* Lz,
                                     const double* Dz, double* Wx1, double* Wx2, double* Wz1, double* Wz2,
-                                    double* gsm, int gsm_doubles, EigScratch& s, double* out)
+                                    double* gsm, int gsm_doubles, EigScratch& s, double* out, bool z_diag = false)
 {
   cta::gemm<NT>(n, false, Dx, n, true, Lx, n, Wx1, n, 1.0, 0.0, gsm);
   cta::gemm<NT>(n, false, Lx, n, false, Wx1, n, Wx2, n, 1.0, 0.0, gsm);
-  cta::gemm<NT>(n, false, Dz, n, true, Lz, n, Wz1, n, 1.0, 0.0, gsm);
+  if (z_diag) {
+    for (int t = threadIdx.x; t < n * n; t += NT) {
+      const int i = t % n, j = t / n;
+      Wz1[t] = Dz[i + (size_t)n * i] * Lz[j + (size_t)n * i];
+    }
+    __syncthreads();
+  } else {
+    cta::gemm<NT>(n, false, Dz, n, true, Lz, n, Wz1, n, 1.0, 0.0, gsm);
+  }
   cta::gemm<NT>(n, false, Lz, n, false, Wz1, n, Wz2, n, 1.0, 0.0, gsm);
   if (n <= 20) {
     out[0] = dense_min_eig(n, Wx2, s);

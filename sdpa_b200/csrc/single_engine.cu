@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(NT) k_chol_diag(int bs, T* A, int lda, int adj
 {
   extern __shared__ double smem[];
   __shared__ int s_flag;
-  T* sD = (T*)(smem + 2 * cta::GK * cta::GT);
+  T* sD = (T*)(smem + cta::GEMM_RECT_SMEM);
   if (*flag) return;
   const int f = cta::cholesky<NT, T>(bs, A, lda, adjust != 0, sD, smem, &s_flag);
   if (f && threadIdx.x == 0) atomicCAS(flag, 0, col0 + f);
@@ -354,7 +354,7 @@ template <typename T>
 __global__ void __launch_bounds__(NT) k_tri_inv(int bs, const T* L, int lda, T* Li, int ldi, const int* flag)
 {
   extern __shared__ double smem[];
-  T* sD = (T*)(smem + 2 * cta::GK * cta::GT);
+  T* sD = (T*)(smem + cta::GEMM_RECT_SMEM);
   if (flag && *flag) return;
   cta::tri_inverse<NT, T>(bs, L, lda, Li, ldi, sD, smem);
 }
@@ -535,7 +535,7 @@ static const int NBG = 128;        // panel width of the grid-level Cholesky
 static const int F1_CHUNK = 32;    // F1 constraints processed per batched GEMM
 static const int SMALL_SOLVE = 2048;  // Schur orders up to this use the one-block solve
 
-static size_t chol_smem() { return (2 * cta::GK * cta::GT + cta::SD_DOUBLES) * sizeof(double); }
+static size_t chol_smem() { return (cta::GEMM_RECT_SMEM + cta::SD_DOUBLES) * sizeof(double); }
 
 template <typename TM, typename TC>
 static void gemm_t(int M, int N, int K, bool tA, const TM* A, int lda, bool tB, const TM* B, int ldb, TM* C,
@@ -544,7 +544,7 @@ static void gemm_t(int M, int N, int K, bool tA, const TM* A, int lda, bool tB, 
 {
   if (M <= 0 || N <= 0) return;
   dim3 grid((M + cta::GT - 1) / cta::GT, (N + cta::GT - 1) / cta::GT, batch);
-  k_gemm<TM, TC><<<grid, NT, 2 * cta::GK * cta::GT * sizeof(double)>>>(M, N, K, tA, A, lda, sA, tB, B, ldb, sB,
+  k_gemm<TM, TC><<<grid, NT, cta::GEMM_RECT_SMEM * sizeof(double)>>>(M, N, K, tA, A, lda, sA, tB, B, ldb, sB,
                                                                        C, ldc, sC, alpha, beta, lower ? 1 : 0);
 }
 
