@@ -197,6 +197,7 @@ SDPAB_API int sdpab_mpnn_propose_x(int num_nodes, const float* r, const double* 
 
 /* Precision modes of the batched solver. */
 #define SDPAB_PREC_FP64 0    /* every step in FP64 (the plain path) */
+#define SDPAB_PREC_MIXED_SIMT 2   /* host-driven solver: mixed without tensor cores (comparison) */
 #define SDPAB_PREC_MIXED 1   /* while nDim * mu / max(1, mean |objective|) >=
                                 mixed_switch_gap: bulk products in FP32 (FP32 accumulation), and in
                                 the host-driven solver the Schur Cholesky in FP32 with
@@ -263,6 +264,15 @@ typedef struct sdpab_batch_config {
                                   matrices per solver block, in doubles (0 = auto;
                                   raised to the GEMM minimum of 6144) */
 } sdpab_batch_config;
+
+/* Tensor-core lower update C -= P P^T of an M x M FP32 matrix, P M x K
+ * (column-major, device pointers), with split-TF32 MMAs (tcgen05) and FP32
+ * accumulation: the trailing update of the mixed-precision Schur factor,
+ * exposed stand-alone (no counterpart in the reference; the reference's is
+ * dsyrk inside rATL_dpotrfL, sdpa_dpotrf.cpp:218-265).  Synchronises
+ * `stream`. */
+SDPAB_API long long sdpab_tc_syrk_work_bytes(int M, int K);  /* device scratch of the call below */
+SDPAB_API int sdpab_tc_syrk(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, void* stream);
 
 /* Solves a batch whose arrays (problem, init, result) are all DEVICE pointers,
  * asynchronously on `stream` (a cudaStream_t, NULL = default stream).

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libsdpa_b200.so")
 
 # status codes
 OK, EINVAL, ECUDA, ESIZE, ENODEV, ESTATE, EIO = 0, -1, -2, -3, -4, -5, -6
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_SIMT = 0, 1, 2
 PHASES = ["noINFO", "pFEAS", "dFEAS", "pdFEAS", "pdINF", "pFEAS_dINF", "pINF_dFEAS", "pdOPT",
           "pUNBD", "dUNBD"]
 
@@ -104,6 +104,8 @@ SIGNATURES = [
     ("sdpab_sdpa_write_init", c_int, [c_void_p, c_char_p]),
     ("sdpab_sdpa_copy_current_to_init", c_int, [c_void_p]),
     ("sdpab_release_workspace", c_int, []),
+    ("sdpab_tc_syrk_work_bytes", c_longlong, [c_int, c_int]),
+    ("sdpab_tc_syrk", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
 ]
 
 _lib = None

@@ -294,26 +294,10 @@ static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
   return r;
 }
 
-// Minimum eigenvalue of L D L^T (Jal::getMinEigen, sdpa_jordan.cpp:58-109):
-// Lanczos for n > 20, dense for n <= 20.  W1, W2: n x n scratch.
-static __device__ double min_eig(int n, const double* L, const double* D, double* W1, double* W2,
-                          double* gsm, int gsm_doubles, EigScratch& s)
-{
-  cta::gemm<NT>(n, false, D, n, true, L, n, W1, n, 1.0, 0.0, gsm);   // D L^T
-  cta::gemm<NT>(n, false, L, n, false, W1, n, W2, n, 1.0, 0.0, gsm); // L (D L^T)
-  if (n <= 20) return dense_min_eig(n, W2, s);
-  const double* M = W2;
-  if (n * n <= gsm_doubles) {  // stage M in shared memory for the Lanczos steps
-    for (int t = threadIdx.x; t < n * n; t += NT) gsm[t] = W2[t];
-    __syncthreads();
-    M = gsm;
-  }
-  return lanczos_min_eig(n, M, s);
-}
-
-
-// Both step-length eigenvalues of an iteration, lambda_min(Lx Dx Lx^T) and
-// lambda_min(Lz Dz Lz^T), with the two Lanczos processes in lockstep.
+// Minimum eigenvalues of L D L^T for the step length (Jal::getMinEigen,
+// sdpa_jordan.cpp:58-109: Lanczos for n > 20, all eigenvalues for n <= 20),
+// for both of an iteration, lambda_min(Lx Dx Lx^T) and lambda_min(Lz Dz Lz^T),
+// with the two Lanczos processes in lockstep.
 // Wx1, Wx2, Wz1, Wz2: n x n scratch (Wx2 and Wz2 receive the formed
 // matrices).  The matrices are staged in shared memory while they fit.
 // z_diag: Dz is diagonal, so Dz Lz^T is a row scaling of Lz^T (no GEMM).

@@ -9,6 +9,12 @@
 namespace sdpab {
 
 int set_error(int code, const char* msg);
+// Tensor-core (tcgen05, split TF32) lower update C -= P P^T of an M x M FP32
+// matrix (tc_syrk.cu); `work` holds syrk_tf32x3_work_bytes(M, K) bytes.
+// Returns a cudaError_t value; *err (device) is set when a block gave up
+// waiting for its MMAs (the update is then incomplete).
+long long syrk_tf32x3_work_bytes(int M, int K);
+int syrk_tf32x3(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, int* err, cudaStream_t st);
 int cuda_error(cudaError_t e, const char* where);
 
 // Device memory kept between solver calls on the current device: the

@@ -506,6 +506,9 @@ struct DevState {
   double* part = nullptr;   // reduction partials
   double* sc = nullptr;     // scalar slots
   int* flag = nullptr;
+  int* tc_err = nullptr;    // tensor-core update time-out flag (inside the flag allocation)
+  bool tc = false;          // mixed mode: tensor-core trailing updates of the FP32 Schur factor
+  void* tc_work = nullptr;  // their split operands (syrk_tf32x3_work_bytes(m, NBG))
   std::vector<void*> allocs;
   double* alloc(size_t n)
   {
@@ -581,8 +584,13 @@ static int cholesky_grid_t(DevState& S, T* A, int n, bool adjust, T* Linv, T* Tb
     // panel: P <- P L_bb^{-T}
     gemm_t<T, T>(rem, bs, bs, false, P, n, true, Linv, bs, Tb, rem, 1.0, 0.0);
     k_copy2d_t<T><<<nblk((long long)rem * bs), 256>>>(rem, bs, Tb, rem, P, n);
-    // trailing: A22 -= P P^T (lower)
-    gemm_t<T, T>(rem, rem, bs, false, P, n, true, P, n, A + (kb + bs) + (size_t)n * (kb + bs), n, -1.0, 1.0, true);
+    // trailing: A22 -= P P^T (lower); FP32 with tensor cores in mixed mode
+    T* A22 = A + (kb + bs) + (size_t)n * (kb + bs);
+    bool done = false;
+    if constexpr (std::is_same<T, float>::value) {
+      if (S.tc && S.tc_work) done = syrk_tf32x3(rem, bs, P, n, A22, n, S.tc_work, S.tc_err, 0) == 0;
+    }
+    if (!done) gemm_t<T, T>(rem, rem, bs, false, P, n, true, P, n, A22, n, -1.0, 1.0, true);
   }
   int f = 0;
   cudaMemcpy(&f, S.flag, sizeof(int), cudaMemcpyDeviceToHost);
@@ -879,6 +887,7 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
   if (cudaMalloc(&fp, 256) != cudaSuccess) return set_error(SDPAB_ECUDA, "device allocation failed");
   S.allocs.push_back(fp);
   S.flag = (int*)fp;
+  S.tc_err = S.flag + 16;
   if (!S.B || !S.T || !S.b) return set_error(SDPAB_ECUDA, "device allocation failed (Schur matrix)");
   // shared memory limits of the block-level kernels
   cudaFuncSetAttribute(k_min_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -898,7 +907,9 @@ int Solver::solve(const InitPoint* init, const Params* prm)
   auto t_start = std::chrono::steady_clock::now();
   stats_ = SolveStats();
   const int nsdp = (int)S.sdp.size();
-  S.mixed = (precision_ == SDPAB_PREC_MIXED) ? 1 : 0;
+  S.mixed = (precision_ == SDPAB_PREC_MIXED || precision_ == SDPAB_PREC_MIXED_SIMT) ? 1 : 0;
+  // tensor-core trailing updates pay from a few panels on
+  S.tc = precision_ == SDPAB_PREC_MIXED && m >= 256;
   S.mu_switch = (mu_switch_ > 0.0) ? mu_switch_ : 1.0e-2;
   if (S.mixed && !S.B32) {
     void* p = nullptr;
@@ -907,6 +918,13 @@ int Solver::solve(const InitPoint* init, const Params* prm)
       return set_error(SDPAB_ECUDA, "device allocation failed (FP32 Schur factor)");
     S.allocs.push_back(p);
     S.B32 = (float*)p;
+    if (S.tc) {  // split operands of the tensor-core trailing updates
+      void* w = nullptr;
+      if (cudaMalloc(&w, (size_t)syrk_tf32x3_work_bytes(m, NBG)) == cudaSuccess) {
+        S.allocs.push_back(w);
+        S.tc_work = w;
+      }
+    }
     S.Linv32 = S.B32 + (size_t)m * m;
     S.T32 = S.Linv32 + (size_t)NBG * NBG;
     S.v32 = S.T32 + (size_t)m * NBG;
@@ -1158,7 +1176,16 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     bool fp32_factor = false;
     if (lowp) {
       k_convert<float, double><<<nblk((long long)m * m), 256>>>((long long)m * m, S.B32, S.B);
+      if (S.tc) cudaMemset(S.tc_err, 0, sizeof(int));
       fp32_factor = cholesky_grid_t<float>(S, S.B32, m, true, S.Linv32, S.T32, S.dinv32) == 0;
+      if (S.tc) {  // a tensor-core block that gave up leaves the factor incomplete: use FP64
+        int te = 0;
+        cudaMemcpy(&te, S.tc_err, sizeof(int), cudaMemcpyDeviceToHost);
+        if (te) {
+          fp32_factor = false;
+          stats_.tc_timeouts += 1;
+        }
+      }
     }
     if (!fp32_factor && cholesky_grid(S, S.B, m, true, S.dinv)) {
       stats_.cholesky_failed = 1;

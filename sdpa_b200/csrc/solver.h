@@ -47,6 +47,7 @@ struct SolveStats {
   double solve_seconds = 0;
   int cholesky_failed = 0;
   int warm_start_rejected = 0;
+  int tc_timeouts = 0;      // tensor-core Schur updates abandoned (FP64 factor used instead)
   std::vector<double> trace;  // per iteration: mu, thetaP, thetaD, objP, objD, alphaP, alphaD, beta
   double final_row[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // the same quantities at loop exit
   // device seconds per phase: rMat+gVec, bMat, Cholesky, solves, dX/dZ,
