@@ -13,20 +13,21 @@
 //
 // Two kernels:
 //  * k_split_tf32 writes P's hi and lo parts once per panel, already in the
-//    MMA's shared-memory layout: for every 128-row block and 32-wide K chunk
-//    a 16 KB tile in the canonical K-major no-swizzle layout (8-row x
+//    MMA's shared-memory layout: for every 128-row block and 16-wide K chunk
+//    an 8 KB tile in the canonical K-major no-swizzle layout (8-row x
 //    16-byte core matrices; core (row group g, K group q) at byte
 //    (q * 16 + g) * 128), hi and lo tiles side by side;
 //  * k_syrk_tf32x3: one 128-thread block per 128 x 128 tile of the lower
 //    triangle.  Thread 0 streams the four operand tiles of a K chunk into
-//    one of two shared-memory stages with bulk asynchronous copies that
-//    complete on the stage's "full" mbarrier, issues 3 x 4 MMAs
+//    one of two shared-memory stages (64 KB in all, so that three blocks
+//    share an SM) with bulk asynchronous copies that complete on the
+//    stage's "full" mbarrier, issues 3 x 2 MMAs
 //    (M = N = 128, K = 8 each) into a 128-column FP32 accumulator in tensor
 //    memory and commits them to the stage's "empty" mbarrier; once chunk
 //    k-1's MMAs are done its stage is refilled with chunk k+1 while chunk
 //    k's MMAs run.  The four warps then read the
 //    accumulator (warp w: lanes 32w..32w+31 = tile rows) and update C,
-//    32 columns per round of loads.
+//    16 columns per round of loads.
 // Every wait is bounded: on time-out the block records an error, waits
 // (bounded) for the MMAs it committed, frees its tensor memory and skips the
 // update; the caller then falls back.
@@ -40,9 +41,9 @@ namespace sdpab {
 namespace tc {
 
 constexpr int TILE = 128;        // M = N of the MMA and of a block's tile
-constexpr int KC = 32;           // K per stage
+constexpr int KC = 16;           // K per stage
 constexpr int THREADS = 128;
-constexpr int OPER_BYTES = TILE * KC * 4;          // one operand tile (16 KB)
+constexpr int OPER_BYTES = TILE * KC * 4;          // one operand tile (8 KB)
 constexpr int OPER_WORDS = OPER_BYTES / 4;
 constexpr int STAGE_BYTES = 4 * OPER_BYTES;        // A_hi, A_lo, B_hi, B_lo
 constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 128;  // two stages + barriers + TMEM address
@@ -120,7 +121,7 @@ __global__ void k_split_tf32(int M, int K, const float* __restrict__ P, int ldp,
     l[u] = to_tf32(a - __uint_as_float(h[u]));
   }
   uint32_t* base = S + ((size_t)b * nk + c) * 2 * OPER_WORDS;
-  const int w = (q * (TILE / 8) + (t >> 3)) * 32 + (t & 7) * 4;
+  const int w = (q * (TILE / 8) + (t >> 3)) * 32 + (t & 7) * 4;  // core (t / 8, q), row t % 8
   *reinterpret_cast<uint4*>(base + w) = make_uint4(h[0], h[1], h[2], h[3]);
   *reinterpret_cast<uint4*>(base + OPER_WORDS + w) = make_uint4(l[0], l[1], l[2], l[3]);
 }
@@ -134,7 +135,7 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
                : "memory");
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, 3)
 k_syrk_tf32x3(int M, int K, const uint32_t* __restrict__ S, float* __restrict__ C, int ldc, int* err)
 {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -241,17 +242,17 @@ k_syrk_tf32x3(int M, int K, const uint32_t* __restrict__ S, float* __restrict__ 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
     const int gr = r0 + 32 * wid + lane;
-    for (int grp = 0; grp < TILE / 32; ++grp) {
-      float cv[32];
+    for (int grp = 0; grp < TILE / 16; ++grp) {
+      float cv[16];
 #pragma unroll
-      for (int u = 0; u < 32; ++u) {
-        const int gc = c0 + 32 * grp + u;
+      for (int u = 0; u < 16; ++u) {
+        const int gc = c0 + 16 * grp + u;
         cv[u] = (gr < M && gc <= gr) ? C[gr + (size_t)ldc * gc] : 0.0f;
       }
-      uint32_t v[32];
+      uint32_t v[16];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const uint32_t taddr = tmem + ((uint32_t)(32 * wid) << 16) + (uint32_t)(32 * grp + 8 * j);
+      for (int j = 0; j < 2; ++j) {
+        const uint32_t taddr = tmem + ((uint32_t)(32 * wid) << 16) + (uint32_t)(16 * grp + 8 * j);
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                      : "=r"(v[8 * j + 0]), "=r"(v[8 * j + 1]), "=r"(v[8 * j + 2]), "=r"(v[8 * j + 3]),
                        "=r"(v[8 * j + 4]), "=r"(v[8 * j + 5]), "=r"(v[8 * j + 6]), "=r"(v[8 * j + 7])
@@ -259,8 +260,8 @@ k_syrk_tf32x3(int M, int K, const uint32_t* __restrict__ S, float* __restrict__ 
       }
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-      for (int u = 0; u < 32; ++u) {
-        const int gc = c0 + 32 * grp + u;
+      for (int u = 0; u < 16; ++u) {
+        const int gc = c0 + 16 * grp + u;
         if (gr < M && gc <= gr) C[gr + (size_t)ldc * gc] = cv[u] - __uint_as_float(v[u]);
       }
     }
