@@ -335,6 +335,98 @@ __global__ void __launch_bounds__(NT) k_gemm(int M, int N, int K, int tA, const 
                              C + r0 + (size_t)ldc * c0, ldc, alpha, beta, smem, lower != 0, r0 - c0);
 }
 
+// FP64 GEMM, C = alpha op(A) op(B) + beta C, one 128 x 64 output tile per
+// 256-thread block (z = batch, strided; lower skips tiles above the diagonal
+// and entries with row < column).  Thread (tx, ty) of the 16 x 16 grid owns
+// rows 8 ty .. 8 ty + 7 and columns 4 tx .. 4 tx + 3, read from shared
+// memory as 16-byte pairs: 32 FMAs per 6 shared loads.  K is staged in
+// chunks of 32 by cp.async into two stages (rows padded to 130 / 66 doubles
+// so transposed stores spread over the banks; 100 KB, two blocks per SM).
+constexpr int DG_M = 128, DG_N = 64, DG_K = 32, DG_AS = DG_M + 2, DG_BS = DG_N + 2;
+constexpr int DG_STAGE = DG_K * (DG_AS + DG_BS);
+constexpr size_t DG_SMEM = 2 * (size_t)DG_STAGE * sizeof(double);
+
+__global__ void __launch_bounds__(256, 2) k_dgemm(int M, int N, int K, int tA, const double* A, int lda,
+                                                  long long sA, int tB, const double* B, int ldb, long long sB,
+                                                  double* C, int ldc, long long sC, double alpha, double beta,
+                                                  int lower)
+{
+  extern __shared__ __align__(16) double dsm[];
+  const int r0 = blockIdx.x * DG_M, c0 = blockIdx.y * DG_N;
+  if (lower && r0 + DG_M - 1 < c0) return;
+  const int z = blockIdx.z;
+  A += sA * z;
+  B += sB * z;
+  C += sC * z;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  auto issue = [&](int k0, int st) {
+    double* As = dsm + st * DG_STAGE;
+    double* Bs = As + DG_K * DG_AS;
+    for (int t = tid; t < DG_K * DG_M; t += 256) {
+      int r, k;
+      if (!tA) { r = t % DG_M; k = t / DG_M; } else { k = t % DG_K; r = t / DG_K; }
+      const int gr = r0 + r, gk = k0 + k;
+      const bool v = gr < M && gk < K;
+      cta::cp_async_el<double>(&As[k * DG_AS + r], v ? (tA ? A + gk + (size_t)lda * gr : A + gr + (size_t)lda * gk) : A, v);
+    }
+    for (int t = tid; t < DG_K * DG_N; t += 256) {
+      int c, k;
+      if (!tB) { k = t % DG_K; c = t / DG_K; } else { c = t % DG_N; k = t / DG_N; }
+      const int gc = c0 + c, gk = k0 + k;
+      const bool v = gc < N && gk < K;
+      cta::cp_async_el<double>(&Bs[k * DG_BS + c], v ? (tB ? B + gc + (size_t)ldb * gk : B + gk + (size_t)ldb * gc) : B, v);
+    }
+    cta::cp_async_commit();
+  };
+  double acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  const int nch = (K + DG_K - 1) / DG_K;
+  if (nch > 0) issue(0, 0);
+  for (int ch = 0; ch < nch; ++ch) {
+    cta::cp_async_wait_all();
+    __syncthreads();  // chunk ch visible; every thread is done with the other stage
+    if (ch + 1 < nch) issue((ch + 1) * DG_K, (ch + 1) & 1);
+    const double* As = dsm + (ch & 1) * DG_STAGE;
+    const double* Bs = As + DG_K * DG_AS;
+    const int kmax = min(DG_K, K - ch * DG_K);
+#pragma unroll 4
+    for (int k = 0; k < kmax; ++k) {
+      double a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const double2 v = *reinterpret_cast<const double2*>(&As[k * DG_AS + 8 * ty + 2 * i]);
+        a[2 * i] = v.x;
+        a[2 * i + 1] = v.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const double2 v = *reinterpret_cast<const double2*>(&Bs[k * DG_BS + 4 * tx + 2 * j]);
+        b[2 * j] = v.x;
+        b[2 * j + 1] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gr = r0 + 8 * ty + i;
+    if (gr >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gc = c0 + 4 * tx + j;
+      if (gc >= N || (lower && gr < gc)) continue;
+      double* cp = C + gr + (size_t)ldc * gc;
+      *cp = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
+    }
+  }
+}
+
 // Diagonal block of the blocked Cholesky: one block factors A[0:bs, 0:bs]
 // (leading dimension lda) with the chosen pivot rule; first failure (global
 // column + 1) is written to *flag if *flag is still 0.
@@ -546,6 +638,18 @@ static void gemm_t(int M, int N, int K, bool tA, const TM* A, int lda, bool tB, 
                    long long sB = 0, long long sC = 0)
 {
   if (M <= 0 || N <= 0) return;
+  // The 128 x 64 tile pays off on the long-K products of the Schur build;
+  // the Cholesky's panel and trailing updates (K <= 128) stay on 64 x 64.
+  if constexpr (std::is_same<TM, double>::value && std::is_same<TC, double>::value) if (K > 128) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
+      attr = true;
+    }
+    dim3 g((M + DG_M - 1) / DG_M, (N + DG_N - 1) / DG_N, batch);
+    k_dgemm<<<g, 256, DG_SMEM>>>(M, N, K, tA, A, lda, sA, tB, B, ldb, sB, C, ldc, sC, alpha, beta, lower ? 1 : 0);
+    return;
+  }
   dim3 grid((M + cta::GT - 1) / cta::GT, (N + cta::GT - 1) / cta::GT, batch);
   k_gemm<TM, TC><<<grid, NT, cta::GEMM_RECT_SMEM * sizeof(double)>>>(M, N, K, tA, A, lda, sA, tB, B, ldb, sB,
                                                                        C, ldc, sC, alpha, beta, lower ? 1 : 0);
