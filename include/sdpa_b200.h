@@ -10,7 +10,8 @@
  *     of the same shape is declared in sdpa_call.h of this directory; these
  *     functions are its C binding for FFI callers (ctypes, MEX, cgo ...).
  *
- *  2. Batched API: thousands of single-block SDPs solved by one persistent
+ *  2. Batched API: thousands of small SDPs (one SDP block, or several SDP
+ *     blocks and LP blocks per instance) solved by one persistent
  *     kernel launch (no counterpart in the reference, which solves one problem
  *     per process; its per-problem semantics are those of SDPA::solve,
  *     sdpa_solve.cpp:59-233).
@@ -208,7 +209,7 @@ SDPAB_API int sdpab_mpnn_propose_x(int num_nodes, const float* r, const double* 
 typedef struct sdpab_batch {
   int count;                   /* number of instances */
   int nmax, mmax;              /* upper bounds of n and m over the batch */
-  const int* n;                /* [count] order of the single SDP block */
+  const int* n;                /* [count] matrix order (sum of the block orders) */
   const int* m;                /* [count] number of constraints */
   const long long* vec_off;    /* [count] offset of the instance's b / xvec (m doubles) */
   const double* b;             /* c vector of the .dat-s file (b of the internal problem) */
@@ -219,7 +220,19 @@ typedef struct sdpab_batch {
   const int* col;              /* entries: 0-based column */
   const double* val;           /* entries: value as written in the file */
   const long long* dense_off;  /* [count] offset of the instance's n*n blocks in X / Y arrays */
+  /* Block structure (optional; NULL nblock = one SDP block of order n).  An
+   * instance's blocks (bLOCKsTRUCT of the .dat-s file: positive = SDP block,
+   * negative = LP block of that many diagonal entries; order 1 counts as LP,
+   * sdpa_block.cpp:80-91) lie along the diagonal of its n x n matrices,
+   * n = sum |size|, in file order; row / col are those global indices.  An
+   * entry must lie inside one block, and inside an LP block on its diagonal.
+   * X / Y results are the block-diagonal n x n matrices. */
+  const int* nblock;           /* [count] number of blocks (1 .. SDPAB_BATCH_MAX_BLOCKS) */
+  const int* blk_off;          /* [count] offset of the instance's sizes in blk_size */
+  const int* blk_size;         /* signed block orders */
 } sdpab_batch;
+
+#define SDPAB_BATCH_MAX_BLOCKS 64  /* blocks per instance in a batch */
 
 #define SDPAB_INIT_NONE 0      /* standard start lambda* I */
 #define SDPAB_INIT_POINT 1     /* start from the given (x, X, Y) */

@@ -29,7 +29,11 @@ class Params(ctypes.Structure):
 class Batch(ctypes.Structure):
     _fields_ = [("count", c_int), ("nmax", c_int), ("mmax", c_int), ("n", c_void_p), ("m", c_void_p),
                 ("vec_off", c_void_p), ("b", c_void_p), ("mat_off", c_void_p), ("mat_ptr", c_void_p),
-                ("row", c_void_p), ("col", c_void_p), ("val", c_void_p), ("dense_off", c_void_p)]
+                ("row", c_void_p), ("col", c_void_p), ("val", c_void_p), ("dense_off", c_void_p),
+                ("nblock", c_void_p), ("blk_off", c_void_p), ("blk_size", c_void_p)]
+
+
+BATCH_MAX_BLOCKS = 64
 
 
 class BatchInit(ctypes.Structure):

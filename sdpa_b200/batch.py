@@ -1,8 +1,12 @@
-"""Batched solve of many single-block SDPs through the C ABI
+"""Batched solve of many small SDPs through the C ABI
 (sdpab_batch_solve / sdpab_batch_solve_host).
 
-`pack(instances)` turns `Instance`s (one SDP block each) into the flat arrays
-of `sdpab_batch`; `solve_host` runs the host-pointer entry point (copies
+`pack(instances)` turns `Instance`s into the flat arrays of `sdpab_batch`.
+An instance with several blocks (SDP blocks and an LP block, as in a .dat-s
+bLOCKsTRUCT) has its blocks laid along the diagonal of one n x n matrix,
+n = sum |size|, and carries the block orders; a batch whose instances are all
+one SDP block passes no block structure.  `solve_host` runs the host-pointer
+entry point (copies
 inside the call); `DeviceBatch` keeps a packed batch resident in device
 memory (torch tensors as allocation plumbing only) and solves it with the
 device-pointer entry point on a given stream.
@@ -35,10 +39,26 @@ class Packed:
     dense_off: np.ndarray  # int64
     nvec: int
     nden: int
+    nblock: np.ndarray | None = None    # int32 [count] (None: every instance is one SDP block)
+    blk_off: np.ndarray | None = None   # int32 [count] offset into blk_size
+    blk_size: np.ndarray | None = None  # int32 signed block orders (negative = LP)
+
+    def arrays(self):
+        """The sdpab_batch arrays in field order (None where absent)."""
+        return [getattr(self, k) for k in _ARRAYS]
 
     def h2d_bytes(self) -> int:
-        return sum(a.nbytes for a in (self.n, self.m, self.vec_off, self.b, self.mat_off, self.mat_ptr,
-                                      self.row, self.col, self.val, self.dense_off)) + 4 * self.count
+        return sum(a.nbytes for a in self.arrays() if a is not None) + 4 * self.count
+
+    def blocks_of(self, q: int) -> list[int]:
+        if self.nblock is None:
+            return [int(self.n[q])]
+        o = int(self.blk_off[q])
+        return [int(x) for x in self.blk_size[o:o + int(self.nblock[q])]]
+
+
+_ARRAYS = ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col", "val", "dense_off", "nblock", "blk_off",
+           "blk_size")
 
 
 def pack(instances: list[Instance]) -> Packed:
@@ -49,17 +69,26 @@ def pack(instances: list[Instance]) -> Packed:
     mat_off = np.zeros(cnt, np.int64)
     dense_off = np.zeros(cnt, np.int64)
     bs, ptrs, rows, cols, vals = [], [], [], [], []
+    structured = any(len(it.blocks) != 1 or int(it.blocks[0]) < 2 for it in instances)
+    nblock = np.zeros(cnt, np.int32)
+    blk_off = np.zeros(cnt, np.int32)
+    sizes = []
     nv = npn = ne = nd = 0
     for q, it in enumerate(instances):
-        if len(it.blocks) != 1 or it.blocks[0] < 2:
-            raise ValueError("batched solver takes one SDP block per instance")
-        nb = int(it.blocks[0])
+        blocks = [int(x) for x in it.blocks]
+        if not blocks or any(x == 0 for x in blocks) or len(blocks) > N.BATCH_MAX_BLOCKS:
+            raise ValueError(f"instance {q}: 1..{N.BATCH_MAX_BLOCKS} blocks of non-zero order are supported")
+        offs = np.concatenate([[0], np.cumsum(np.abs(blocks))]).astype(np.int64)
+        nb = int(offs[-1])
         n[q], m[q] = nb, it.m
+        nblock[q], blk_off[q] = len(blocks), len(sizes)
+        sizes.extend(blocks)
         vec_off[q], mat_off[q], dense_off[q] = nv, npn, nd
-        order = np.lexsort((it.j, it.i, it.k))
+        order = np.lexsort((it.j, it.i, it.l, it.k))
         k = it.k[order]
-        r = it.i[order] - 1
-        c = it.j[order] - 1
+        base = offs[it.l[order] - 1]
+        r = base + it.i[order] - 1
+        c = base + it.j[order] - 1
         v = it.v[order]
         # entries are stored upper-triangular
         sw = r > c
@@ -76,9 +105,12 @@ def pack(instances: list[Instance]) -> Packed:
         npn += it.m + 2
         ne += k.size
         nd += nb * nb
-    return Packed(cnt, int(n.max()), int(m.max()), n, m, vec_off, np.concatenate(bs), mat_off,
-                  np.concatenate(ptrs), np.concatenate(rows), np.concatenate(cols),
-                  np.concatenate(vals), dense_off, nv, nd)
+    P = Packed(cnt, int(n.max()), int(m.max()), n, m, vec_off, np.concatenate(bs), mat_off,
+               np.concatenate(ptrs), np.concatenate(rows), np.concatenate(cols),
+               np.concatenate(vals), dense_off, nv, nd)
+    if structured:
+        P.nblock, P.blk_off, P.blk_size = nblock, blk_off, np.asarray(sizes, np.int32)
+    return P
 
 
 @dataclass
@@ -101,6 +133,17 @@ class BatchResult:
     def mat_of(self, which: np.ndarray, P: Packed, q: int) -> np.ndarray:
         nb = int(P.n[q])
         return which[P.dense_off[q]:P.dense_off[q] + nb * nb].reshape(nb, nb, order="F")
+
+    def block_of(self, which: np.ndarray, P: Packed, q: int, l: int) -> np.ndarray:
+        """Block l (0-based) of instance q's X or Y, as getResultXMat(l+1) /
+        getResultYMat(l+1): the dense SDP block, or an LP block's vector."""
+        M = self.mat_of(which, P, q)
+        blocks = P.blocks_of(q)
+        o = int(np.sum(np.abs(blocks[:l])))
+        k = abs(blocks[l])
+        if blocks[l] < 0:
+            return np.diag(M)[o:o + k].copy()
+        return M[o:o + k, o:o + k].copy()
 
 
 def _ptr(a):
@@ -128,11 +171,8 @@ def solve_host(P: Packed, params=None, precision=N.PREC_FP64, want_x=True, want_
     the packed layouts (user X / Y as in SDPA::inputInitXMat / inputInitYMat)."""
     L = N.lib()
     cnt = P.count
-    arrs = {k: np.ascontiguousarray(getattr(P, k)) for k in
-            ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col", "val", "dense_off")}
-    bt = N.Batch(cnt, P.nmax, P.mmax, *[_ptr(arrs[k]) for k in
-                                         ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col",
-                                          "val", "dense_off")])
+    arrs = [None if a is None else np.ascontiguousarray(a) for a in P.arrays()]
+    bt = N.Batch(cnt, P.nmax, P.mmax, *[_ptr(a) for a in arrs])
     res = BatchResult(*[np.zeros(cnt) for _ in range(5)], *[np.zeros(cnt, np.int32) for _ in range(3)])
     res.xvec = np.zeros(P.nvec) if want_x else None
     res.X = np.zeros(P.nden) if want_mats else None
@@ -164,8 +204,7 @@ class DeviceBatch:
         import torch
         self.P = P
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
-        self.d = {k: t(getattr(P, k)) for k in
-                  ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col", "val", "dense_off")}
+        self.d = {k: t(a) for k, a in zip(_ARRAYS, P.arrays()) if a is not None}
         order = np.argsort(-(P.n.astype(np.int64) ** 2 + P.m), kind="stable").astype(np.int32)
         self.order = t(order)
         cnt = P.count
@@ -178,9 +217,7 @@ class DeviceBatch:
         self.Y = torch.zeros(P.nden, **f64) if want_mats else None
         self.init = None
         dp = lambda x: x.data_ptr()
-        self._bt = N.Batch(cnt, P.nmax, P.mmax, *[dp(self.d[k]) for k in
-                                                   ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row",
-                                                    "col", "val", "dense_off")])
+        self._bt = N.Batch(cnt, P.nmax, P.mmax, *[dp(self.d[k]) if k in self.d else None for k in _ARRAYS])
         self._br = N.BatchResult(dp(self.xvec), dp(self.X) if want_mats else None,
                                  dp(self.Y) if want_mats else None,
                                  *[dp(self.sc[q]) for q in range(5)], *[dp(self.ic[q]) for q in range(3)])

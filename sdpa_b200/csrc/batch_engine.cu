@@ -1,5 +1,10 @@
-// Batched persistent SDP solver: one launch solves a whole batch of
-// single-block SDPs.  Each thread block repeatedly takes the next instance
+// Batched persistent SDP solver: one launch solves a whole batch of small
+// SDPs.  An instance is one SDP block, or several SDP blocks and LP entries
+// laid along the diagonal of one n x n matrix: the HKM iterates of a
+// block-diagonal start stay block-diagonal (every product and inverse of
+// block-diagonal matrices is), so the dense steps run on the whole matrix,
+// and the step length takes each block's minimum eigenvalue as the
+// reference does.  Each thread block repeatedly takes the next instance
 // from a device work queue (atomic counter over a largest-first order) and
 // runs SDPA's complete Mehrotra predictor-corrector loop for it
 // (SDPA::solve, sdpa_solve.cpp:59-233), with every dense step executed
@@ -41,7 +46,8 @@ static __host__ __device__ long long fixed_smem_doubles(int nmax, int mmax)
 
 static size_t smem_bytes_for(int nmax, int mmax, long long gsm)
 {
-  return (size_t)(gsm + fixed_smem_doubles(nmax, mmax)) * sizeof(double) + (size_t)mmax * sizeof(int) + 64;
+  return (size_t)(gsm + fixed_smem_doubles(nmax, mmax)) * sizeof(double) + (size_t)(mmax + nmax) * sizeof(int) +
+         64;
 }
 
 // Staging area: at least the double-buffered single-tile GEMM (n <= 96).  `want`
@@ -57,7 +63,7 @@ static long long staging_doubles(int nmax, int mmax, int want)
   else if (2 * m2 <= LANCZOS_SMEM_DOUBLES) s = 2 * m2;
   else if (m2 <= LANCZOS_SMEM_DOUBLES) s = m2;
   else s = g;
-  const long long cap = (227LL * 1024 - 512 - (long long)smem_bytes_for(nmax, mmax, 0)) / (long long)sizeof(double);
+  const long long cap = (227LL * 1024 - 2048 - (long long)smem_bytes_for(nmax, mmax, 0)) / (long long)sizeof(double);
   if (s > cap) s = cap;
   s = s / 32 * 32;
   return s > g ? s : g;
@@ -162,6 +168,10 @@ __device__ __forceinline__ double f3_value(const int* row, const int* col, const
 
 // The solver -----------------------------------------------------------------
 
+// BLOCKS: the batch carries a block structure (sdpab_batch.nblock).  The
+// single-block instantiation has none of the block bookkeeping, so the
+// common case keeps its register allocation.
+template <bool BLOCKS>
 __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 {
   extern __shared__ double smem[];
@@ -179,8 +189,10 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
   EigScratch es;
   eig_scratch_carve(es, vrp + mmax, nmax, &RD);          // eig_scratch_doubles(nmax)
   int* s_nnz = (int*)(vrp + mmax + eig_scratch_doubles(nmax));  // mmax ints
+  int* s_bid = s_nnz + mmax;  // nmax ints: block of each row (-1 = LP entry)
 
   __shared__ int s_inst, s_flag, s_flag2[2];
+  __shared__ int s_nb, s_boff[SDPAB_BATCH_MAX_BLOCKS], s_bsz[SDPAB_BATCH_MAX_BLOCKS];
   __shared__ Scalars S;
   const int tid = threadIdx.x;
   const Params& P = a.prm;
@@ -223,12 +235,43 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
     const double lam = P.lambdaStar;
     const int nn_i = n * n;
 
-    // entries must index inside the block: reject the instance otherwise
+    // block structure (SDPA's bLOCKsTRUCT): blocks along the diagonal in
+    // file order; s_bid[t] = the SDP block holding row t, -1 for LP entries
+    bool blocked = false;
+    if constexpr (BLOCKS) {
+      if (tid == 0) {
+        const int nb = a.p.nblock[inst];
+        int bad = (nb < 1 || nb > SDPAB_BATCH_MAX_BLOCKS), off = 0;
+        for (int l = 0; l < nb && !bad; ++l) {
+          const int sz = a.p.blk_size[a.p.blk_off[inst] + l];
+          bad = (sz == 0);
+          s_boff[l] = off;
+          s_bsz[l] = (sz == 1) ? -1 : sz;  // order 1 is an LP entry (sdpa_block.cpp:80-91)
+          off += (sz < 0) ? -sz : sz;
+        }
+        s_nb = (bad || off != n) ? -1 : nb;
+      }
+      __syncthreads();
+      if (s_nb < 0) {
+        if (tid == 0) a.r.status[inst] = SDPAB_EINVAL;
+        continue;
+      }
+      for (int l = 0; l < s_nb; ++l) {
+        const int sz = s_bsz[l], cnt = (sz < 0) ? -sz : sz;
+        for (int t = tid; t < cnt; t += NT) s_bid[s_boff[l] + t] = (sz >= 2) ? l : -1;
+      }
+      __syncthreads();
+      blocked = !(s_nb == 1 && s_bsz[0] == n);
+    }
+    // entries must index inside one block (LP: its diagonal): reject the
+    // instance otherwise
     {
       int bad = 0;
       for (long long e = mp[0] + tid; e < mp[m + 1]; e += NT) {
         const int r = er[e], c = ec[e];
-        bad |= (r < 0 || c < 0 || r >= n || c >= n);
+        const bool out = (r < 0 || c < 0 || r >= n || c >= n);
+        bad |= out;
+        if (!out && blocked) bad |= (s_bid[r] != s_bid[c]) || (s_bid[r] < 0 && r != c);
       }
       if (__syncthreads_or(bad)) {
         if (tid == 0) a.r.status[inst] = SDPAB_EINVAL;
@@ -289,7 +332,13 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       const double* Xu = a.init.X + a.p.dense_off[inst];
       const double* Yu = a.init.Y + a.p.dense_off[inst];
       const double* xv = a.init.xvec + a.p.vec_off[inst];
-      for (int t = tid; t < nn_i; t += NT) { Z[t] = Xu[t]; X[t] = Yu[t]; W1[t] = Xu[t]; W2[t] = Yu[t]; }
+      // only the diagonal blocks of a block-structured point are used
+      for (int t = tid; t < nn_i; t += NT) {
+        const int i = t % n, j = t / n;
+        const bool keep = !blocked || (s_bid[i] == s_bid[j] && (s_bid[i] >= 0 || i == j));
+        const double xu = keep ? Xu[t] : 0.0, yu = keep ? Yu[t] : 0.0;
+        Z[t] = xu; X[t] = yu; W1[t] = xu; W2[t] = yu;
+      }
       for (int k = tid; k < m; k += NT) vy[k] = -xv[k];
       __syncthreads();
       // strict interiority check (the reference ignores computeInverse's
@@ -511,7 +560,11 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       {
         // R and XDZ are free here (both are rebuilt by the next predictor)
         double mins[2];
-        min_eig_pair(n, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins, dz_diag);
+        if (BLOCKS && blocked)
+          min_eig_pair_blocks(n, s_nb, s_boff, s_bsz, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es,
+                              mins, dz_diag);
+        else
+          min_eig_pair(n, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins, dz_diag);
         const double minX = mins[0], minZ = mins[1];
         double CdX = c_dot(dX);
         double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);
@@ -596,6 +649,12 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 
 // Host side -----------------------------------------------------------------
 
+// The instantiation for a batch: block-aware only when it carries a structure.
+static void* solver_kernel(const sdpab_batch* prob)
+{
+  return prob->nblock ? (void*)batch_ipm_fp64<true> : (void*)batch_ipm_fp64<false>;
+}
+
 static long long ws_doubles(int nmax, int mmax)
 {
   long long nn = (long long)nmax * nmax;
@@ -619,12 +678,12 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   const long long gsm = staging_doubles(prob->nmax, prob->mmax, cfg ? cfg->staging_doubles : 0);
   const size_t shm = smem_bytes_for(prob->nmax, prob->mmax, gsm);
   if (shm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(batch_ipm_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(solver_kernel(prob), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shm);
     if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
   }
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_ipm_fp64, NT, shm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solver_kernel(prob), NT, shm);
   if (per_sm < 1) return set_error(SDPAB_ESIZE, "batch_solve: kernel does not fit on an SM");
   int want = (cfg && cfg->ctas_per_sm > 0) ? cfg->ctas_per_sm : 2;
   per_sm = std::min(per_sm, want);
@@ -648,7 +707,8 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.ws = ws;
   a.ws_stride = stride;
   a.queue = queue;
-  batch_ipm_fp64<<<grid, NT, shm, stream>>>(a);
+  if (prob->nblock) batch_ipm_fp64<true><<<grid, NT, shm, stream>>>(a);
+  else batch_ipm_fp64<false><<<grid, NT, shm, stream>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "batch_ipm_fp64 launch");
   return SDPAB_OK;
@@ -709,12 +769,12 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   const long long gsm = staging_doubles(prob->nmax, prob->mmax, 0);
   const size_t shm = smem_bytes_for(prob->nmax, prob->mmax, gsm);
   if (shm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(batch_ipm_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(solver_kernel(prob), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shm);
     if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
   }
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_ipm_fp64, NT, shm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solver_kernel(prob), NT, shm);
   if (per_sm < 1) return set_error(SDPAB_ESIZE, "batch_solve_noalloc: kernel does not fit on an SM");
   per_sm = std::min(per_sm, 2);
   const long long grid = std::min<long long>(std::min<long long>(prob->count, (long long)sms * per_sm),
@@ -734,7 +794,8 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.ws = base + head;
   a.ws_stride = stride;
   a.queue = queue;
-  batch_ipm_fp64<<<(int)grid, NT, shm, stream>>>(a);
+  if (prob->nblock) batch_ipm_fp64<true><<<(int)grid, NT, shm, stream>>>(a);
+  else batch_ipm_fp64<false><<<(int)grid, NT, shm, stream>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "batch_solve_noalloc: launch");
   return SDPAB_OK;

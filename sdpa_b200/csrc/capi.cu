@@ -185,6 +185,24 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
     nent = std::max(nent, hp->mat_ptr[hp->mat_off[i] + m + 1]);
     nden = std::max(nden, hp->dense_off[i] + (long long)n * n);
   }
+  // block structure: extent of blk_size, and each instance's orders add up to n
+  long long nbs = 0;
+  if (hp->nblock) {
+    if (!hp->blk_off || !hp->blk_size) return set_error(SDPAB_EINVAL, "batch_solve_host: blk_off / blk_size NULL");
+    for (int i = 0; i < N; ++i) {
+      const int nb = hp->nblock[i];
+      if (nb < 1 || nb > SDPAB_BATCH_MAX_BLOCKS || hp->blk_off[i] < 0)
+        return set_error(SDPAB_EINVAL, "batch_solve_host: nblock out of range");
+      long long tot = 0;
+      for (int l = 0; l < nb; ++l) {
+        const int sz = hp->blk_size[hp->blk_off[i] + l];
+        if (sz == 0) return set_error(SDPAB_EINVAL, "batch_solve_host: block of order 0");
+        tot += (sz < 0) ? -(long long)sz : sz;
+      }
+      if (tot != hp->n[i]) return set_error(SDPAB_EINVAL, "batch_solve_host: block orders do not add up to n");
+      nbs = std::max(nbs, (long long)hp->blk_off[i] + nb);
+    }
+  }
   if (want_init) {
     bool need_xy = false;
     for (int i = 0; i < N; ++i) need_xy |= (hinit->flag[i] == SDPAB_INIT_POINT);
@@ -214,6 +232,9 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
       {12, want_init ? hinit->xvec : nullptr, want_init ? nvec * sizeof(double) : 0},
       {13, want_init ? hinit->X : nullptr, want_init ? nden * sizeof(double) : 0},
       {14, want_init ? hinit->Y : nullptr, want_init ? nden * sizeof(double) : 0},
+      {20, hp->nblock, hp->nblock ? N * sizeof(int) : 0},
+      {21, hp->nblock ? hp->blk_off : nullptr, hp->nblock ? N * sizeof(int) : 0},
+      {22, hp->nblock ? hp->blk_size : nullptr, nbs * sizeof(int)},
   };
   void* d[24] = {nullptr};
   for (const Copy& c : in) {
@@ -250,6 +271,9 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
   dp.col = (const int*)d[7];
   dp.val = (const double*)d[8];
   dp.dense_off = (const long long*)d[9];
+  dp.nblock = (const int*)d[20];
+  dp.blk_off = (const int*)d[21];
+  dp.blk_size = (const int*)d[22];
   sdpab_batch_init di;
   memset(&di, 0, sizeof(di));
   if (want_init) {

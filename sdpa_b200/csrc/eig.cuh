@@ -301,9 +301,10 @@ static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
 // Wx1, Wx2, Wz1, Wz2: n x n scratch (Wx2 and Wz2 receive the formed
 // matrices).  The matrices are staged in shared memory while they fit.
 // z_diag: Dz is diagonal, so Dz Lz^T is a row scaling of Lz^T (no GEMM).
-static __device__ void min_eig_pair(int n, const double* Lx, const double* Dx, const double* Lz,
-                                    const double* Dz, double* Wx1, double* Wx2, double* Wz1, double* Wz2,
-                                    double* gsm, int gsm_doubles, EigScratch& s, double* out, bool z_diag = false)
+// Wx2 = Lx Dx Lx^T and Wz2 = Lz Dz Lz^T (Wx1, Wz1 scratch).
+static __device__ void form_ldlt_pair(int n, const double* Lx, const double* Dx, const double* Lz,
+                                      const double* Dz, double* Wx1, double* Wx2, double* Wz1, double* Wz2,
+                                      double* gsm, bool z_diag)
 {
   cta::gemm<NT>(n, false, Dx, n, true, Lx, n, Wx1, n, 1.0, 0.0, gsm);
   cta::gemm<NT>(n, false, Lx, n, false, Wx1, n, Wx2, n, 1.0, 0.0, gsm);
@@ -317,6 +318,13 @@ static __device__ void min_eig_pair(int n, const double* Lx, const double* Dx, c
     cta::gemm<NT>(n, false, Dz, n, true, Lz, n, Wz1, n, 1.0, 0.0, gsm);
   }
   cta::gemm<NT>(n, false, Lz, n, false, Wz1, n, Wz2, n, 1.0, 0.0, gsm);
+}
+
+static __device__ void min_eig_pair(int n, const double* Lx, const double* Dx, const double* Lz,
+                                    const double* Dz, double* Wx1, double* Wx2, double* Wz1, double* Wz2,
+                                    double* gsm, int gsm_doubles, EigScratch& s, double* out, bool z_diag = false)
+{
+  form_ldlt_pair(n, Lx, Dx, Lz, Dz, Wx1, Wx2, Wz1, Wz2, gsm, z_diag);
   if (n <= 20) {
     out[0] = dense_min_eig(n, Wx2, s);
     out[1] = dense_min_eig(n, Wz2, s);
@@ -335,6 +343,63 @@ static __device__ void min_eig_pair(int n, const double* Lx, const double* Dx, c
     Ms[0] = gsm;
   }
   lanczos_min_eig_multi<2>(n, Ms, s, out);
+}
+
+// The same for block-diagonal X and Z: nb blocks of signed orders bsz at
+// offsets boff along the diagonal of the n x n matrices (order >= 2: SDP
+// block; otherwise LP entries, one per diagonal position).  As in
+// Jal::getMinEigen (sdpa_jordan.cpp:58-109) every SDP block gets its own
+// minimum eigenvalue (Lanczos for order > 20, all eigenvalues otherwise, on
+// a compact copy of the block), every LP entry contributes x_t l_t^2 (the
+// diagonal of L D L^T there), and the smallest value is the result.  Not
+// inlined: only block-structured instances take this path, and a second
+// inlined Lanczos would raise the register pressure of the whole solver.
+static __device__ __noinline__ void min_eig_pair_blocks(int n, int nb, const int* boff, const int* bsz,
+                                                        const double* Lx, const double* Dx, const double* Lz,
+                                                        const double* Dz, double* Wx1, double* Wx2, double* Wz1,
+                                                        double* Wz2, double* gsm, int gsm_doubles, EigScratch& s,
+                                                        double* out, bool z_diag)
+{
+  form_ldlt_pair(n, Lx, Dx, Lz, Dz, Wx1, Wx2, Wz1, Wz2, gsm, z_diag);
+  double mx = 1.0e50, mz = 1.0e50;
+  for (int l = 0; l < nb; ++l) {
+    if (bsz[l] >= 2) continue;
+    const int o = boff[l], cnt = bsz[l] < 0 ? -bsz[l] : bsz[l];
+    for (int t = threadIdx.x; t < cnt; t += NT) {
+      const size_t d = (size_t)(o + t) * (n + 1);
+      mx = fmin(mx, Wx2[d]);
+      mz = fmin(mz, Wz2[d]);
+    }
+  }
+  mx = -cta::block_max<NT>(-mx, *s.R);
+  mz = -cta::block_max<NT>(-mz, *s.R);
+  for (int l = 0; l < nb; ++l) {
+    const int k = bsz[l];
+    if (k < 2) continue;
+    const int o = boff[l];
+    const int kk = k * k;
+    double* Mx = (2 * kk <= gsm_doubles) ? gsm : Wx1;
+    double* Mz = (2 * kk <= gsm_doubles) ? gsm + kk : Wz1;
+    for (int t = threadIdx.x; t < kk; t += NT) {
+      const size_t g = (size_t)(o + t % k) + (size_t)n * (o + t / k);
+      Mx[t] = Wx2[g];
+      Mz[t] = Wz2[g];
+    }
+    __syncthreads();
+    double r[2];
+    if (k <= 20) {
+      r[0] = dense_min_eig(k, Mx, s);
+      r[1] = dense_min_eig(k, Mz, s);
+    } else {
+      const double* Ms[2] = {Mx, Mz};
+      lanczos_min_eig_multi<2>(k, Ms, s, r);
+    }
+    mx = fmin(mx, r[0]);
+    mz = fmin(mz, r[1]);
+    __syncthreads();
+  }
+  out[0] = mx;
+  out[1] = mz;
 }
 
 }  // namespace sdpab

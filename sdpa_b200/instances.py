@@ -14,6 +14,8 @@ The instance families are the workloads this solver is measured on:
   (file F0 = -C, c = b).
 * Batched MaxCut: per seed s, n ~ U{20..120}, p ~ U(0.05, 0.3), edge weights
   U(0, 1).  Warm-start sets use n ~ U{50..200}.
+* Batched multi-block: per seed, 2..4 SDP blocks of order U{6..40} and an LP
+  block, built like the random SDP (strictly feasible from X = Y = I).
 
 Indices in an `Instance` are 1-based exactly as in a .dat-s file (block l,
 row i <= column j; k = 0 is F0).
@@ -163,6 +165,78 @@ def random_sdp(m: int = 2000, n: int = 500, nlp: int = 50, density: float = 0.01
     return Instance(m=m, blocks=[n, -nlp], c=b, k=np.concatenate(ks), l=np.concatenate(ls),
                     i=np.concatenate(is_), j=np.concatenate(js), v=np.concatenate(vs),
                     name=f"random sdp m={m} n={n} lp={nlp} seed {seed}")
+
+
+def random_block_sdp(m: int, blocks: list, density: float = 0.1, lp_per_constraint: int = 1,
+                     seed: int = 1, name: str = "") -> Instance:
+    """Random strictly feasible SDP with the given signed block structure
+    (positive = SDP block, negative = LP block), built like `random_sdp`:
+    every A_i has floor(density * k(k+1)/2) (at least one) N(0,1) upper
+    entries in each SDP block of order k it touches (each block with
+    probability 0.7, at least one block) plus `lp_per_constraint` LP
+    entries; b_i = Tr(A_i), C = sum_i y0_i A_i + I, file F0 = -C, c = b."""
+    rng = np.random.default_rng(seed)
+    sdp = [(l + 1, int(k)) for l, k in enumerate(blocks) if k > 0]
+    lps = [(l + 1, -int(k)) for l, k in enumerate(blocks) if k < 0]
+    Cs = {l: np.eye(k) for l, k in sdp}
+    Cl = {l: np.ones(k) for l, k in lps}
+    y0 = rng.standard_normal(m)
+    b = np.zeros(m)
+    ks, ls, is_, js, vs = [], [], [], [], []
+
+    def add(a, l, r, c, v):
+        ks.append(np.full(r.size, a, np.int32))
+        ls.append(np.full(r.size, l, np.int32))
+        is_.append((r + 1).astype(np.int32))
+        js.append((c + 1).astype(np.int32))
+        vs.append(v)
+
+    for a in range(m):
+        touch = [t for t in range(len(sdp)) if rng.random() < 0.7] if sdp else []
+        if sdp and not touch:
+            touch = [int(rng.integers(len(sdp)))]
+        for t in touch:
+            l, k = sdp[t]
+            iu, ju = np.triu_indices(k)
+            per = max(1, int(np.floor(density * iu.size)))
+            pos = rng.choice(iu.size, size=per, replace=False)
+            val = rng.standard_normal(per)
+            r, c = iu[pos], ju[pos]
+            add(a + 1, l, r, c, val)
+            b[a] += val[r == c].sum()
+            np.add.at(Cs[l], (r, c), y0[a] * val)
+            off = r != c
+            np.add.at(Cs[l], (c[off], r[off]), y0[a] * val[off])
+        for l, k in lps:
+            cnt = min(lp_per_constraint, k)
+            idx = rng.choice(k, size=cnt, replace=False)
+            val = rng.standard_normal(cnt)
+            add(a + 1, l, idx, idx, val)
+            b[a] += val.sum()
+            np.add.at(Cl[l], idx, y0[a] * val)
+    for l, k in sdp:
+        iu, ju = np.triu_indices(k)
+        add(0, l, iu, ju, -Cs[l][iu, ju])
+    for l, k in lps:
+        add(0, l, np.arange(k), np.arange(k), -Cl[l])
+    return Instance(m=m, blocks=[int(x) for x in blocks], c=b, k=np.concatenate(ks), l=np.concatenate(ls),
+                    i=np.concatenate(is_), j=np.concatenate(js), v=np.concatenate(vs),
+                    name=name or f"random block sdp {blocks} m={m} seed {seed}")
+
+
+def batch_block_sdp(seed: int) -> Instance:
+    """One instance of the batched multi-block family: 2..4 SDP blocks of
+    order U{6..40}, an LP block of U{0..12} entries (none if 0), m ~ U{10..80},
+    density U(0.05, 0.2)."""
+    rng = np.random.default_rng(seed)
+    nsdp = int(rng.integers(2, 5))
+    blocks = [int(x) for x in rng.integers(6, 41, size=nsdp)]
+    nlp = int(rng.integers(0, 13))
+    if nlp:
+        blocks.append(-nlp)
+    m = int(rng.integers(10, 81))
+    dens = float(rng.uniform(0.05, 0.2))
+    return random_block_sdp(m, blocks, dens, seed=seed + 1000003, name=f"batched block sdp seed {seed}")
 
 
 def main(argv=None):

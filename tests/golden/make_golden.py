@@ -13,6 +13,9 @@ Fixtures (all from the reference's own output, never hand-written):
                        SDP with an LP block, batched-MaxCut seeds 0..63)
   mc100_trace.json     per-iteration (mu, objP, objD, alphaP, alphaD, beta)
                        of MaxCut G(100, 0.1) seed 1 at epsilonStar = 1e-7
+  blocks.json / blocks.npz  (also alone with --blocks) batched multi-block
+                       instances blk0..blk31: objectives, iterations, phase,
+                       x; every block of X and Y for blk0..blk7
   large.json / large.npz  (--large) Lovasz theta G(200, 0.5) seed 1 and the
                        random m=2000 SDP seed 1: objectives, iterations, x
 """
@@ -208,8 +211,36 @@ def small_cases():
     return cases
 
 
+def block_cases(count=32):
+    """Batched multi-block instances (several SDP blocks and an LP block)."""
+    return [(f"blk{s}", inst.batch_block_sdp(s)) for s in range(count)]
+
+
+def block_fixtures(tmp):
+    """blocks.json / blocks.npz: the reference's results (objectives,
+    iterations, phase, x; every block of X and Y for blk0..blk7) on
+    block_cases()."""
+    cases = block_cases()
+    res = run_ref([c[1] for c in cases], tmp, procs=8)
+    meta, arrays = {}, {}
+    for (name, it), r in zip(cases, res):
+        meta[name] = {k: r[k] for k in ("iterations", "phase", "primal_obj", "dual_obj")}
+        arrays[name + ".xvec"] = r["xvec"]
+        if int(name[3:]) < 8:
+            for l in range(len(it.blocks)):
+                arrays[name + f".X{l + 1}"] = r["X"][l]
+                arrays[name + f".Y{l + 1}"] = r["Y"][l]
+    with open(os.path.join(HERE, "blocks.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+    np.savez_compressed(os.path.join(HERE, "blocks.npz"), **arrays)
+
+
 def main():
     large = "--large" in sys.argv
+    if "--blocks" in sys.argv:
+        with tempfile.TemporaryDirectory() as tmp:
+            block_fixtures(tmp)
+        return
     with tempfile.TemporaryDirectory() as tmp:
         ppath = os.path.join(tmp, "param_1e-8.sdpa")
         with open(ppath, "w") as f:
@@ -270,6 +301,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, "tight.npz"), **arrays)
 
         cli_fixtures()
+        block_fixtures(tmp)
 
         if large:
             big = [("lt200", inst.lovasz_theta(200, 0.5, 1)), ("rnd2000", inst.random_sdp(seed=1))]

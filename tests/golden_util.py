@@ -14,6 +14,12 @@ def small():
     return meta, arr
 
 
+def blocks():
+    """Reference results of the batched multi-block instances blk0..blk31."""
+    meta = json.load(open(os.path.join(GOLDEN, "blocks.json")))
+    return meta, np.load(os.path.join(GOLDEN, "blocks.npz"))
+
+
 def known_answers():
     return json.load(open(os.path.join(GOLDEN, "known_answers.json")))
 

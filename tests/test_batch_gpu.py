@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from golden_util import GOLDEN, rel, small, tight, x_within_reference_accuracy
+from golden_util import GOLDEN, blocks, rel, small, tight, x_within_reference_accuracy
 
 pytestmark = pytest.mark.gpu
 
@@ -98,3 +98,115 @@ def test_batched_mixed_precision_matches_reference():
         assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
         assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL, nm
         assert x_within_reference_accuracy(r.x_of(P, q), arr[nm + ".xvec"], tz[nm + ".tight"]), nm
+
+
+def _block_batch():
+    """blk0..blk31, the small multi-block reference cases and two MaxCut
+    instances in one batch."""
+    from sdpa_b200 import batch
+    bc = dict(MG.block_cases())
+    sc = dict(MG.small_cases())
+    names = [f"blk{s}" for s in range(32)] + ["rnd40", "rnd120", "ex2", "bmc0", "bmc1"]
+    insts = [bc[n] if n.startswith("blk") else sc[n] for n in names]
+    return names, insts, batch.pack(insts)
+
+
+def _golden(nm):
+    meta, arr = blocks() if nm.startswith("blk") else small()
+    return meta[nm], arr
+
+
+def test_batched_block_instances_match_reference():
+    """Several SDP blocks and an LP block per instance (block-diagonal
+    layout, per-block step length) against the reference's results."""
+    from sdpa_b200 import batch
+    names, insts, P = _block_batch()
+    assert P.nblock is not None
+    r = batch.solve_host(P, want_mats=True)
+    iters_equal = 0
+    for q, nm in enumerate(names):
+        g, arr = _golden(nm)
+        assert r.status[q] == 0, (nm, r.status[q])
+        assert r.phase[q] == 7, (nm, r.phase[q])
+        assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
+        assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL, nm
+        assert np.max(np.abs(r.x_of(P, q) - arr[nm + ".xvec"])) < X_TOL, nm
+        iters_equal += int(r.iterations[q] == g["iterations"])
+        assert abs(int(r.iterations[q]) - g["iterations"]) <= 1, nm
+    assert iters_equal >= len(names) - 3
+    # every block of X (getResultXMat) and Y (getResultYMat); off-block zero
+    for q, nm in enumerate(names):
+        if nm not in [f"blk{s}" for s in range(8)] + ["rnd40", "ex2"]:
+            continue
+        _, arr = _golden(nm)
+        for l, b in enumerate(insts[q].blocks):
+            for which, key in ((r.X, "X"), (r.Y, "Y")):
+                ref = arr[f"{nm}.{key}{l + 1}"]
+                got = r.block_of(which, P, q, l).ravel(order="F")
+                assert np.max(np.abs(got - ref)) < 1e-4 * max(1.0, np.max(np.abs(ref))), (nm, key, l)
+        M = r.mat_of(r.Y, P, q)
+        mask = np.zeros(M.shape, bool)
+        o = 0
+        for b in insts[q].blocks:
+            k = abs(b)
+            if b > 0:
+                mask[o:o + k, o:o + k] = True
+            else:
+                mask[np.arange(o, o + k), np.arange(o, o + k)] = True
+            o += k
+        assert np.all(M[~mask] == 0.0), nm
+
+
+def test_block_device_path_equals_host_path():
+    import torch
+    from sdpa_b200 import batch
+    names, insts, P = _block_batch()
+    h = batch.solve_host(P)
+    db = batch.DeviceBatch(P)
+    db.solve()
+    torch.cuda.synchronize()
+    d = db.result()
+    # Entries of several constraints at one position are summed into the
+    # dense D and dZ by atomic adds, whose order varies between runs: equal
+    # iteration counts, objectives equal to rounding.
+    assert np.array_equal(h.iterations, d.iterations)
+    assert np.allclose(h.primal_obj, d.primal_obj, rtol=1e-9, atol=0)
+
+
+def test_block_warm_start_uses_diagonal_blocks_only():
+    """SDPAB_INIT_POINT on block instances: a point near the reference's
+    solution whose off-block entries are garbage; the solver keeps the
+    diagonal blocks only, starts there and reaches the reference's optimum."""
+    from sdpa_b200 import batch
+    names, insts, P = _block_batch()
+    sel = [q for q, nm in enumerate(names) if nm in [f"blk{s}" for s in range(8)]]
+    its = [insts[q] for q in sel]
+    P = batch.pack(its)
+    X = np.zeros(P.nden)
+    Y = np.zeros(P.nden)
+    xv = np.zeros(P.nvec)
+    for q, nm in enumerate([names[i] for i in sel]):
+        _, arr = _golden(nm)
+        n = int(P.n[q])
+        Xq = np.full((n, n), 0.37)
+        Yq = np.full((n, n), -0.21)
+        o = 0
+        for l, b in enumerate(its[q].blocks):
+            k = abs(b)
+            for M, key in ((Xq, "X"), (Yq, "Y")):
+                ref = arr[f"{nm}.{key}{l + 1}"]
+                blk = np.diag(ref) if b < 0 else ref.reshape(k, k, order="F")
+                M[o:o + k, o:o + k] = 0.9 * blk + 0.1 * np.eye(k)
+            o += k
+        X[P.dense_off[q]:P.dense_off[q] + n * n] = Xq.ravel(order="F")
+        Y[P.dense_off[q]:P.dense_off[q] + n * n] = Yq.ravel(order="F")
+        xv[P.vec_off[q]:P.vec_off[q] + P.m[q]] = arr[nm + ".xvec"]
+    flag = np.full(P.count, 1, np.int32)
+    r = batch.solve_host(P, init=(flag, xv, X, Y))
+    for q, nm in enumerate([names[i] for i in sel]):
+        g, _ = _golden(nm)
+        assert r.status[q] in (0, 2), (nm, r.status[q])
+        assert r.phase[q] == 7, nm
+        assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
+        assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL, nm
+    assert int(np.sum(r.status == 0)) >= len(sel) // 2

@@ -1,0 +1,81 @@
+"""Multi-block batches on the CPU: the oracle against the reference's
+results on the batched multi-block family (several SDP blocks and an LP
+block), the packed layout of sdpab_batch's block structure, and the host
+entry point's rejection of malformed structures (before any device call)."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from golden_util import GOLDEN, blocks, rel
+from oracle import sdpa_oracle as O
+
+_spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+MG = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(MG)
+
+
+def test_oracle_matches_reference_on_block_instances():
+    meta, arr = blocks()
+    cases = dict(MG.block_cases())
+    for name in ("blk0", "blk2", "blk3", "blk5"):
+        r = O.solve(O.parse_dats(cases[name].to_dats()))
+        g = meta[name]
+        assert O.PHASE_NAMES[r.phase] == g["phase"] == "pdOPT"
+        assert r.iterations == g["iterations"], name
+        assert rel(r.primal_obj, g["primal_obj"]) < 1e-8, name
+        assert rel(r.dual_obj, g["dual_obj"]) < 1e-8, name
+        assert np.max(np.abs(r.xvec - arr[name + ".xvec"])) < 1e-6, name
+
+
+def test_block_family_shapes():
+    from sdpa_b200 import instances
+    for s in range(32):
+        it = instances.batch_block_sdp(s)
+        sdp = [b for b in it.blocks if b > 0]
+        assert 2 <= len(sdp) <= 4 and all(6 <= b <= 40 for b in sdp)
+        assert all(-12 <= b < 0 for b in it.blocks if b < 0)
+        assert 10 <= it.m <= 80
+        # entries inside their block, LP entries diagonal
+        sz = np.abs(np.asarray(it.blocks))[it.l - 1]
+        assert np.all((it.i >= 1) & (it.j <= sz) & (it.i <= it.j))
+        lp = np.asarray(it.blocks)[it.l - 1] < 0
+        assert np.all(it.i[lp] == it.j[lp])
+
+
+def test_pack_lays_blocks_along_the_diagonal():
+    from sdpa_b200 import batch, instances
+    its = [instances.batch_block_sdp(2), instances.batch_maxcut(1)]
+    P = batch.pack(its)
+    assert P.nblock is not None and list(P.nblock) == [len(its[0].blocks), 1]
+    assert P.blocks_of(0) == its[0].blocks and P.blocks_of(1) == [its[1].m]
+    assert P.n[0] == sum(abs(b) for b in its[0].blocks)
+    offs = np.concatenate([[0], np.cumsum(np.abs(its[0].blocks))])
+    # every entry of instance 0 maps to its block's rows and columns
+    e0, e1 = P.mat_ptr[P.mat_off[0]], P.mat_ptr[P.mat_off[0] + its[0].m + 1]
+    r, c = P.row[e0:e1], P.col[e0:e1]
+    blk_r = np.searchsorted(offs, r, side="right") - 1
+    blk_c = np.searchsorted(offs, c, side="right") - 1
+    assert np.array_equal(blk_r, blk_c)
+    lp = np.asarray(its[0].blocks)[blk_r] < 0
+    assert np.all(r[lp] == c[lp])
+    # a batch of single SDP blocks carries no block structure
+    assert batch.pack([instances.batch_maxcut(s) for s in range(3)]).nblock is None
+
+
+@pytest.mark.parametrize("mutate", ["sum", "zero", "count"])
+def test_host_entry_rejects_malformed_structure(mutate):
+    from sdpa_b200 import _native as N
+    from sdpa_b200 import batch, instances
+    P = batch.pack([instances.batch_block_sdp(1)])
+    if mutate == "sum":
+        P.blk_size = P.blk_size.copy()
+        P.blk_size[0] += 1      # orders no longer add up to n
+    elif mutate == "zero":
+        P.blk_size = P.blk_size.copy()
+        P.blk_size[-1] = 0      # a block of order 0
+    else:
+        P.nblock = np.array([N.BATCH_MAX_BLOCKS + 1], np.int32)
+    with pytest.raises(N.SolverError, match="nblock|order|add up"):
+        batch.solve_host(P)
