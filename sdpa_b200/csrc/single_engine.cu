@@ -168,32 +168,92 @@ __global__ void k_f1_left(int n, int q0, const int* f1list, const long long* cpt
 }
 
 // F1 step 3 (calF1, sdpa_newton.cpp:885-889, driver :1868-1907):
-// B_ij += A_i . G_j for every i dominated by j.  Blocks (q, part): q is the
-// chunk entry, the constraints i are dealt to the warps of all parts.
-__global__ void k_f1_dot(int nc, int q0, const int* f1list, const int* cons, const long long* ptr,
-                         const int* row, const int* col, const double* val, const int* nnz,
-                         const double* G, int n, double* B, int m)
+// B_ij += A_i . G_j for every i dominated by j, for the (up to 32) j of a
+// chunk at once.  With A_i symmetric and stored as upper entries,
+// A_i . G_j = sum over entries (r <= c) of v * H_j(r, c), where
+// H_j(r, c) = G_j(r, c) + G_j(c, r) off the diagonal and G_j(r, r) on it.
+// k_f1_pack forms H for the whole chunk as rows of 32 doubles, one row per
+// upper position (packed index c (c + 1) / 2 + r, column q = chunk entry);
+// k_f1_spmm then reads one 256-byte row per entry of A_i for all j of the
+// chunk together (lane = q): each entry of A_i is read once per chunk, not
+// once per j, and every G read is coalesced.
+constexpr int F1_PACK_T = 16;                        // position tile (16 x 16)
+constexpr int F1_PACK_LD = 33;                       // padded q stride of the staged tile
+constexpr size_t F1_PACK_SMEM =
+    ((size_t)F1_PACK_T * F1_PACK_T * F1_PACK_LD + F1_PACK_T * (F1_PACK_T + 1)) * sizeof(double);
+
+__device__ __forceinline__ size_t f1_packed(int r, int c) { return (size_t)c * (c + 1) / 2 + r; }
+
+// One block per 16 x 16 tile on or above the diagonal (blockIdx.x indexes
+// those tiles row-major over the packed upper triangle of tiles).
+__global__ void __launch_bounds__(256) k_f1_pack(int n, int cnt, const double* G, double* H)
 {
-  const int q = blockIdx.x;
-  const int jl = f1list[q0 + q];
-  const int gj = cons[jl], jnz = nnz[jl];
-  const double* Gq = G + (size_t)q * n * n;
-  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int wid = blockIdx.y * nw + (threadIdx.x >> 5), stride = gridDim.y * nw;
-  for (int il = wid; il < nc; il += stride) {
-    const int gi = cons[il], inz = nnz[il];
-    if (jnz < inz || (inz == jnz && gi < gj)) continue;
-    double s = 0.0;
-    for (long long e = ptr[il] + lane; e < ptr[il + 1]; e += 32) {
-      const int r = row[e], c = col[e];
-      const double v = val[e];
-      s += (r == c) ? v * Gq[r + (size_t)n * r] : v * (Gq[r + (size_t)n * c] + Gq[c + (size_t)n * r]);
+  extern __shared__ double f1s[];
+  double* St = f1s;                                       // [256][33]
+  double* Tt = f1s + F1_PACK_T * F1_PACK_T * F1_PACK_LD;  // [16][17] transposed tile
+  // tile (tr, tc) with tr <= tc from the linear index
+  const long long k = blockIdx.x;
+  int tc = (int)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
+  while ((long long)tc * (tc + 1) / 2 > k) --tc;
+  while ((long long)(tc + 1) * (tc + 2) / 2 <= k) ++tc;
+  const int tr = (int)(k - (long long)tc * (tc + 1) / 2);
+  const int r0 = tr * F1_PACK_T, c0 = tc * F1_PACK_T;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int r = r0 + tx, c = c0 + ty;
+  const size_t nn = (size_t)n * n;
+  for (int q = 0; q < cnt; ++q) {
+    const double* Gq = G + q * nn;
+    Tt[ty * (F1_PACK_T + 1) + tx] = (c0 + tx < n && r0 + ty < n) ? Gq[(c0 + tx) + (size_t)n * (r0 + ty)] : 0.0;
+    const double a = (r < n && c < n) ? Gq[r + (size_t)n * c] : 0.0;
+    __syncthreads();
+    St[threadIdx.x * F1_PACK_LD + q] = (r == c) ? a : a + Tt[tx * (F1_PACK_T + 1) + ty];
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < F1_PACK_T * F1_PACK_T * cnt; t += blockDim.x) {
+    const int lp = t / cnt, q = t - lp * cnt;
+    const int rr = r0 + (lp & 15), cc = c0 + (lp >> 4);
+    if (rr > cc || cc >= n) continue;
+    H[f1_packed(rr, cc) * 32 + q] = St[lp * F1_PACK_LD + q];
+  }
+}
+
+// Warp (constraint il, part blockIdx.y of its entries); lane q = chunk entry.
+__global__ void __launch_bounds__(256) k_f1_spmm(int nc, int q0, int cnt, const int* f1list, const int* cons,
+                                                 const long long* ptr, const int* pos, const double* val,
+                                                 const int* nnz, const double* H, double* B, int m)
+{
+  const int lane = threadIdx.x & 31;
+  const int il = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (il >= nc) return;
+  const int gi = cons[il], inz = nnz[il];
+  int gj = 0;
+  bool dom = false;
+  if (lane < cnt) {
+    const int jl = f1list[q0 + lane];
+    gj = cons[jl];
+    const int jnz = nnz[jl];
+    dom = !(jnz < inz || (inz == jnz && gi < gj));
+  }
+  if (!__any_sync(0xffffffffu, dom)) return;
+  const long long beg = ptr[il], end = ptr[il + 1];
+  const int parts = gridDim.y;
+  double acc = 0.0;
+  for (long long e0 = beg + 32LL * blockIdx.y; e0 < end; e0 += 32LL * parts) {
+    const long long e = e0 + lane;
+    const int p = (e < end) ? pos[e] : 0;
+    const double v = (e < end) ? val[e] : 0.0;
+    const int ne = (int)min(32LL, end - e0);
+#pragma unroll 8
+    for (int u = 0; u < 32; ++u) {
+      if (u >= ne) break;
+      const int pu = __shfl_sync(0xffffffffu, p, u);
+      const double vu = __shfl_sync(0xffffffffu, v, u);
+      acc += vu * H[(size_t)pu * 32 + lane];
     }
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-      atomicAdd(&B[gi + (size_t)m * gj], s);
-      if (gi != gj) atomicAdd(&B[gj + (size_t)m * gi], s);
-    }
+  }
+  if (dom) {
+    atomicAdd(&B[gi + (size_t)m * gj], acc);
+    if (gi != gj) atomicAdd(&B[gj + (size_t)m * gi], acc);
   }
 }
 
@@ -561,6 +621,7 @@ struct SdpBlock {
   std::vector<int> hrow, hcol;
   std::vector<double> hval;
   int *cons = nullptr, *nnz = nullptr, *form = nullptr, *row = nullptr, *col = nullptr;
+  int* pos = nullptr;  // packed upper position c (c + 1) / 2 + r of each entry (F1 inner products)
   long long* ptr = nullptr;
   double* val = nullptr;
   // F1/F2 constraints (local indices) and their symmetric CSC
@@ -627,7 +688,7 @@ struct DevState {
 };
 
 static const int NBG = 128;        // panel width of the grid-level Cholesky
-static const int F1_CHUNK = 32;    // F1 constraints processed per batched GEMM
+static const int F1_CHUNK = 32;    // F1 constraints processed per batched GEMM (= warp lanes in k_f1_spmm)
 static const int SMALL_SOLVE = 2048;  // Schur orders up to this use the one-block solve
 
 static size_t chol_smem() { return (cta::GEMM_RECT_SMEM + cta::SD_DOUBLES) * sizeof(double); }
@@ -936,6 +997,14 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
       B.csc_ptr = S.upload(eptr);
       B.csc_row = S.upload(crow);
       B.csc_val = S.upload(cval);
+      std::vector<int> hpos(B.hrow.size());
+      for (size_t e = 0; e < hpos.size(); ++e) {
+        const long long r = std::min(B.hrow[e], B.hcol[e]), c = std::max(B.hrow[e], B.hcol[e]);
+        hpos[e] = (int)(c * (c + 1) / 2 + r);
+      }
+      B.pos = S.upload(hpos);
+      // T holds the chunk's X A_j and then its packed H (n(n+1)/2 rows of 32);
+      // G follows it
       Tneed = std::max(Tneed, (size_t)2 * F1_CHUNK * B.n * B.n);
     }
   }
@@ -1268,7 +1337,15 @@ int Solver::solve(const InitPoint* init, const Params* prm)
         double* G = S.T + (size_t)F1_CHUNK * nn;
         k_f1_left<<<dim3(B.n, cnt), 256>>>(B.n, q0, B.f1, B.csc_cptr, B.csc_ptr, B.csc_row, B.csc_val, B.X, T);
         gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn, lowp);
-        k_f1_dot<<<dim3(cnt, 16), 256>>>(B.nc, q0, B.f1, B.cons, B.ptr, B.row, B.col, B.val, B.nnz, G, B.n, S.B, m);
+        static bool pack_attr = false;
+        if (!pack_attr) {
+          cudaFuncSetAttribute(k_f1_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F1_PACK_SMEM);
+          pack_attr = true;
+        }
+        const long long nt = (B.n + F1_PACK_T - 1) / F1_PACK_T;
+        k_f1_pack<<<(unsigned)(nt * (nt + 1) / 2), 256, F1_PACK_SMEM>>>(B.n, cnt, G, T);
+        k_f1_spmm<<<dim3((B.nc + 7) / 8, 4), 256>>>(B.nc, q0, cnt, B.f1, B.cons, B.ptr, B.pos, B.val, B.nnz, T,
+                                                    S.B, m);
       }
     }
     if (nlp) k_lp_bmat<<<nlp, 256>>>(S.lpT_ptr, S.lpT_k, S.lpT_v, S.lpx, S.lpzi, S.B, m);
