@@ -7,7 +7,12 @@ epsilonStar = 1e-7, inputs resident in HBM, one persistent kernel launch.
 Synthetic seeded data (no public suite is named).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|mixed] [--count C]
+                    [--precision fp64|mixed] [--count C] [--workload maxcut|blocks]
+
+--workload blocks measures the batched multi-block family instead (one GPU,
+FP64, standard start): per seed 2..4 SDP blocks of order U{6..40} and an LP
+block of U{0..12} entries, m ~ U{10..80}, laid along the diagonal of one
+matrix per instance.
 
 Multi-GPU (torchrun): each rank solves its own 4096 instances (independent
 units, no collective in the data path): weak scaling; the timed region is the
@@ -32,6 +37,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "SDPs/sec to 1e-7 rel gap on 1 B200: mixed+warm-start vs plain FP64"
 WORKLOAD = "batched MaxCut: 4096 SDPs, n~U{20..120}, G(n,p~U(0.05,0.3)), w~U(0,1), m=n, eps*=1e-7"
+BLOCK_METRIC = "SDPs/sec to 1e-7 rel gap on 1 B200: batched multi-block SDPs, FP64"
+BLOCK_WORKLOAD = ("batched multi-block SDPs: 4096 instances, 2..4 SDP blocks of order U{6..40} + LP block "
+                  "U{0..12}, m~U{10..80}, eps*=1e-7")
 
 
 def peaks():
@@ -115,9 +123,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_batch(count: int, seed0: int):
+def make_batch(count: int, seed0: int, workload: str = "maxcut"):
     from sdpa_b200 import batch, instances
-    insts = [instances.batch_maxcut(s) for s in range(seed0, seed0 + count)]
+    gen = instances.batch_block_sdp if workload == "blocks" else instances.batch_maxcut
+    insts = [gen(s) for s in range(seed0, seed0 + count)]
     return insts, batch.pack(insts)
 
 
@@ -150,7 +159,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    insts, _ = make_batch(args.count, 0)
+    insts, _ = make_batch(args.count, 0, args.workload)
     cores = os.cpu_count() or 1
     sample = min(args.count, max(64, 48 * cores))
     for _ in range(args.warmup):
@@ -160,11 +169,12 @@ def run_reference(args):
         v, det = cpu_reference(insts, sample, cores)
         vals.append(v)
     value = float(np.median(vals))
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "SDPs/s",
+    blocks = args.workload == "blocks"
+    line = {"impl": "reference", "metric": BLOCK_METRIC if blocks else METRIC, "value": value, "unit": "SDPs/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * args.count / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "count": args.count},
+            "config": {"workload": BLOCK_WORKLOAD if blocks else WORKLOAD, "count": args.count},
             "cpu_baseline": {"value": value, "unit": "SDPs/s", "cores": cores, "kind": "reference",
                              "sample": f"first {sample} instances of the batch per step, one "
                                        f"single-threaded reference process per core; {det}"},
@@ -203,6 +213,77 @@ def _capture(fn, stream):
         return None
 
 
+def run_blocks(args):
+    """The batched multi-block family on one GPU: FP64 from the standard
+    start (the reference's own path), one persistent launch per step."""
+    import torch
+    from sdpa_b200 import _native as N
+    from sdpa_b200 import autotune, batch
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        raise SystemExit("--workload blocks runs on one GPU")
+    torch.cuda.set_device(0)
+    insts, P = make_batch(args.count, 0, "blocks")
+    db = batch.DeviceBatch(P)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    cand = (args.ctas_per_sm,) if args.ctas_per_sm > 0 else (1, 2)
+    tune = autotune.tune(db, N.PREC_FP64, stream=stream, candidates=cand)
+    c = tune["best"]
+    run = lambda: db.solve(precision=N.PREC_FP64, stream=stream, ctas_per_sm=c)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clk:
+            times = _events_time(run, stream, args.steps, flush)
+    torch.cuda.synchronize()
+    res = db.result()
+    step_ms = float(np.mean(times))
+    value = P.count / (step_ms / 1e3)
+    # e2e: host (pinned) inputs -> device, solve, results -> host
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    pairs = [(db.d[k], pin(getattr(P, k))) for k in db.d] + [(db.order, pin(db.order.cpu().numpy()))]
+    h2d = sum(h.numel() * h.element_size() for _, h in pairs)
+    out_sc = torch.empty_like(db.sc, device="cpu").pin_memory()
+    out_ic = torch.empty_like(db.ic, device="cpu").pin_memory()
+    out_x = torch.empty_like(db.xvec, device="cpu").pin_memory()
+    d2h = out_sc.numel() * 8 + out_ic.numel() * 4 + out_x.numel() * 8
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 3))):
+        flush.add_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for dev, host in pairs:
+                dev.copy_(host, non_blocking=True)
+            run()
+            out_sc.copy_(db.sc, non_blocking=True)
+            out_ic.copy_(db.ic, non_blocking=True)
+            out_x.copy_(db.xvec, non_blocking=True)
+        stream.synchronize()
+        e2e_t.append(time.perf_counter() - t0)
+    line = {"metric": BLOCK_METRIC, "value": value, "unit": "SDPs/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no public suite)",
+            "config": {"workload": BLOCK_WORKLOAD, "count_per_gpu": args.count, "precision": "fp64",
+                       "warm_start": False, "ctas_per_sm": c, "autotune_ms": tune["ms"],
+                       "l2": "256 MB buffer written between timed steps", "parallelism": "replicas x1"},
+            "e2e": {"value": P.count / float(np.mean(e2e_t)), "unit": "SDPs/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": args.steps, "clocks": clk.summary(),
+            "parity": {"pdOPT": int(np.sum(res.phase == 7)), "count": int(P.count),
+                       "mean_iterations": float(res.iterations.mean()), "status_nonzero": int(np.sum(res.status != 0))}}
+    if not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        sample = min(args.count, max(64, 48 * cores))
+        v, det = cpu_reference(insts, sample, cores)
+        line["cpu_baseline"] = {"value": v, "unit": "SDPs/s", "cores": cores, "kind": "reference",
+                                "sample": f"first {sample} instances of this batch, one single-threaded "
+                                          f"reference process per core; {det}"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,9 +296,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="fixed launch shape (0 = autotune)")
+    ap.add_argument("--workload", default="maxcut", choices=["maxcut", "blocks"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "blocks":
+        return run_blocks(args)
 
     import torch
     import torch.distributed as dist

@@ -220,7 +220,12 @@ typedef struct sdpab_batch {
   const int* col;              /* entries: 0-based column */
   const double* val;           /* entries: value as written in the file */
   const long long* dense_off;  /* [count] offset of the instance's n*n blocks in X / Y arrays */
-  /* Block structure (optional; NULL nblock = one SDP block of order n).  An
+  /* Block structure (optional; NULL nblock = one SDP block of order n, and
+   * every Schur entry by formula F3, the fast path for MaxCut-like
+   * constraints with one or two entries).  A batch that sets it runs the
+   * general solver: block structure, and per constraint the reference's
+   * choice between F1 and F3 (sdpa_newton.cpp:515-695); set it (one block of
+   * order n is allowed) for constraints with many entries.  An
    * instance's blocks (bLOCKsTRUCT of the .dat-s file: positive = SDP block,
    * negative = LP block of that many diagonal entries; order 1 counts as LP,
    * sdpa_block.cpp:80-91) lie along the diagonal of its n x n matrices,

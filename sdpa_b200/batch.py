@@ -4,8 +4,12 @@
 `pack(instances)` turns `Instance`s into the flat arrays of `sdpab_batch`.
 An instance with several blocks (SDP blocks and an LP block, as in a .dat-s
 bLOCKsTRUCT) has its blocks laid along the diagonal of one n x n matrix,
-n = sum |size|, and carries the block orders; a batch whose instances are all
-one SDP block passes no block structure.  `solve_host` runs the host-pointer
+n = sum |size|, and carries the block orders.  A batch carries a block
+structure (which selects the solver with block support and F1 Schur
+columns) when an instance has several blocks, or one block of order above
+200, or a constraint with more than 2n effective entries (the cases where
+the reference's formula choice can pick F1); a batch of MaxCut-like
+instances passes none and runs the F3-only solver.  `solve_host` runs the host-pointer
 entry point (copies
 inside the call); `DeviceBatch` keeps a packed batch resident in device
 memory (torch tensors as allocation plumbing only) and solves it with the
@@ -61,6 +65,19 @@ _ARRAYS = ("n", "m", "vec_off", "b", "mat_off", "mat_ptr", "row", "col", "val", 
            "blk_size")
 
 
+def _needs_general(it: Instance) -> bool:
+    """Several blocks, a block of order > 200, or a constraint whose
+    NonZeroEffect (diagonal 1, off-diagonal 2) exceeds 2n."""
+    if len(it.blocks) != 1 or int(it.blocks[0]) < 2:
+        return True
+    n = int(it.blocks[0])
+    if n > 200:
+        return True
+    sel = it.k > 0
+    eff = np.bincount(it.k[sel], weights=np.where(it.i[sel] == it.j[sel], 1.0, 2.0), minlength=it.m + 1)
+    return bool(eff.max(initial=0.0) > 2 * n)
+
+
 def pack(instances: list[Instance]) -> Packed:
     cnt = len(instances)
     n = np.zeros(cnt, np.int32)
@@ -69,7 +86,7 @@ def pack(instances: list[Instance]) -> Packed:
     mat_off = np.zeros(cnt, np.int64)
     dense_off = np.zeros(cnt, np.int64)
     bs, ptrs, rows, cols, vals = [], [], [], [], []
-    structured = any(len(it.blocks) != 1 or int(it.blocks[0]) < 2 for it in instances)
+    structured = any(_needs_general(it) for it in instances)
     nblock = np.zeros(cnt, np.int32)
     blk_off = np.zeros(cnt, np.int32)
     sizes = []

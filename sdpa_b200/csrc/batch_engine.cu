@@ -46,8 +46,8 @@ static __host__ __device__ long long fixed_smem_doubles(int nmax, int mmax)
 
 static size_t smem_bytes_for(int nmax, int mmax, long long gsm)
 {
-  return (size_t)(gsm + fixed_smem_doubles(nmax, mmax)) * sizeof(double) + (size_t)(mmax + nmax) * sizeof(int) +
-         64;
+  return (size_t)(gsm + fixed_smem_doubles(nmax, mmax)) * sizeof(double) +
+         (size_t)(2 * mmax + nmax) * sizeof(int) + 64;
 }
 
 // Staging area: at least the double-buffered single-tile GEMM (n <= 96).  `want`
@@ -166,12 +166,84 @@ __device__ __forceinline__ double f3_value(const int* row, const int* col, const
   return ret;
 }
 
+// F1 columns of the Schur complement (compute_bMat_dense_SDP with calF1,
+// sdpa_newton.cpp:885-889, :1827-1922): for every constraint j flagged in
+// `form`, G = X A_j Z^-1 and B_ij = A_i . G for each i that j dominates.
+// T, G: n x n scratch.  With a block structure (nb > 0 blocks at boff of
+// signed orders bsz) Z^-1 is block-diagonal, so G is formed one block at a
+// time (sum of k^3 instead of n^3) and LP entries as diagonal products.
+// Not inlined: only instances with F1 constraints call it.
+static __device__ __noinline__ void schur_f1(int n, int m, const long long* mp, const int* er, const int* ec,
+                                             const double* ev, const double* X, const double* Zi, double* T,
+                                             double* G, double* B, const int* nnz, const int* form, int nb,
+                                             const int* boff, const int* bsz, double* gsm)
+{
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int j = 0; j < m; ++j) {
+    if (!form[j]) continue;
+    const long long jb = mp[j + 1], je = mp[j + 2];
+    // T = X A_j: each thread owns rows of T (A_j symmetric, upper entries)
+    for (int i = tid; i < n; i += NT) {
+      for (int c = 0; c < n; ++c) T[i + (size_t)n * c] = 0.0;
+      for (long long e = jb; e < je; ++e) {
+        const int r = er[e], c = ec[e];
+        const double v = ev[e];
+        T[i + (size_t)n * c] += v * X[i + (size_t)n * r];
+        if (r != c) T[i + (size_t)n * r] += v * X[i + (size_t)n * c];
+      }
+    }
+    __syncthreads();
+    // G = T Z^-1; a block that A_j does not touch has T = 0 there, so its G
+    // block is zero without a product
+    if (nb <= 0) {
+      cta::gemm<NT>(n, false, T, n, false, Zi, n, G, n, 1.0, 0.0, gsm);
+    } else {
+      for (int l = 0; l < nb; ++l) {
+        const int k = bsz[l];
+        const size_t o = (size_t)boff[l] * (n + 1);
+        if (k >= 2) {
+          int hit = 0;
+          for (long long e = jb + tid; e < je; e += NT) hit |= (er[e] >= boff[l] && er[e] < boff[l] + k);
+          if (__syncthreads_or(hit)) {
+            cta::gemm<NT>(k, false, T + o, n, false, Zi + o, n, G + o, n, 1.0, 0.0, gsm);
+          } else {
+            for (int t = threadIdx.x; t < k * k; t += NT) G[o + (size_t)(t % k) + (size_t)n * (t / k)] = 0.0;
+          }
+        } else {
+          for (int t = tid; t < -k; t += NT) G[o + (size_t)t * (n + 1)] = T[o + (size_t)t * (n + 1)] * Zi[o + (size_t)t * (n + 1)];
+        }
+      }
+    }
+    __syncthreads();
+    // B_ij = A_i . G for the i dominated by j, one warp per i
+    const int jnz = nnz[j];
+    for (int i = wid; i < m; i += NT / 32) {
+      const int inz = nnz[i];
+      if (jnz < inz || (inz == jnz && i < j)) continue;
+      double s = 0.0;
+      for (long long e = mp[i + 1] + lane; e < mp[i + 2]; e += 32) {
+        const int r = er[e], c = ec[e];
+        const double v = ev[e];
+        s += (r == c) ? v * G[r + (size_t)n * r] : v * (G[r + (size_t)n * c] + G[c + (size_t)n * r]);
+      }
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) {
+        B[i + (size_t)m * j] = s;
+        B[j + (size_t)m * i] = s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // The solver -----------------------------------------------------------------
 
-// BLOCKS: the batch carries a block structure (sdpab_batch.nblock).  The
-// single-block instantiation has none of the block bookkeeping, so the
-// common case keeps its register allocation.
-template <bool BLOCKS>
+// GENERAL: the batch carries a block structure (sdpab_batch.nblock; one
+// block of order n counts), and the solver supports several blocks and F1
+// Schur columns for constraints with many entries.  The other instantiation
+// (single SDP block, every Schur entry by F3) has none of that bookkeeping,
+// so the MaxCut-like common case keeps its register allocation.
+template <bool GENERAL>
 __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 {
   extern __shared__ double smem[];
@@ -190,6 +262,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
   eig_scratch_carve(es, vrp + mmax, nmax, &RD);          // eig_scratch_doubles(nmax)
   int* s_nnz = (int*)(vrp + mmax + eig_scratch_doubles(nmax));  // mmax ints
   int* s_bid = s_nnz + mmax;  // nmax ints: block of each row (-1 = LP entry)
+  int* s_form = s_bid + nmax;  // mmax ints: 1 = constraint's Schur column by F1
 
   __shared__ int s_inst, s_flag, s_flag2[2];
   __shared__ int s_nb, s_boff[SDPAB_BATCH_MAX_BLOCKS], s_bsz[SDPAB_BATCH_MAX_BLOCKS];
@@ -238,7 +311,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
     // block structure (SDPA's bLOCKsTRUCT): blocks along the diagonal in
     // file order; s_bid[t] = the SDP block holding row t, -1 for LP entries
     bool blocked = false;
-    if constexpr (BLOCKS) {
+    if constexpr (GENERAL) {
       if (tid == 0) {
         const int nb = a.p.nblock[inst];
         int bad = (nb < 1 || nb > SDPAB_BATCH_MAX_BLOCKS), off = 0;
@@ -287,6 +360,38 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       int c = 0;
       for (long long e = mp[k + 1]; e < mp[k + 2]; ++e) c += (er[e] == ec[e]) ? 1 : 2;
       s_nnz[k] = c;
+    }
+    // Schur formula per constraint j, in the manner of the reference's
+    // choice (Newton::computeFormula_SDP, sdpa_newton.cpp:515-695) but with
+    // the costs of this solver's two implementations: F3 costs about four
+    // gathers per entry pair, 4 nnz_j up_j; F1 costs the block GEMMs of
+    // X A_j Z^-1 (sum of k^3), forming X A_j (2 n nnz_j) and one pass over
+    // the dominated entries (up_j), where up_j sums the NonZeroEffect of the
+    // constraints j dominates.  The formulas give the same values up to
+    // rounding.  Single-block batches (MaxCut-like) use F3 only.
+    bool any_f1 = false;
+    if constexpr (GENERAL) {
+      __syncthreads();
+      double kcube = 0.0;
+      if (blocked) {
+        for (int l = 0; l < s_nb; ++l)
+          if (s_bsz[l] >= 2) kcube += (double)s_bsz[l] * s_bsz[l] * s_bsz[l];
+      } else {
+        kcube = (double)n * n * n;
+      }
+      int anyf1 = 0;
+      for (int j = tid; j < m; j += NT) {
+        const int jnz = s_nnz[j];
+        double up = 0.0;
+        for (int i = 0; i < m; ++i) {
+          const int inz = s_nnz[i];
+          if (!(jnz < inz || (inz == jnz && i < j))) up += inz;
+        }
+        const int use = kcube + 2.0 * n * jnz + up < 4.0 * jnz * up;
+        s_form[j] = use;
+        anyf1 |= use;
+      }
+      any_f1 = __syncthreads_or(anyf1);
     }
 
     // A warm-started or mixed-precision solve that ends outside pdOPT is
@@ -479,15 +584,23 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       }
       for (int k = tid; k < m; k += NT) vg[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], G, n) + vrp[k];
       // ---- Schur complement by F3 (compute_bMat_dense_SDP3, sdpa_newton.cpp:2019-2125)
+      // for the pairs whose dominant constraint is F3, then the F1 columns
       for (int t = tid; t < m * m; t += NT) {
         const int i = t % m, j = t / m;
         const int inz = s_nnz[i], jnz = s_nnz[j];
         if (jnz < inz || (inz == jnz && i < j)) continue;
+        if (GENERAL && any_f1 && s_form[j]) continue;
         double v = f3_value(er, ec, ev, mp[j + 1], mp[j + 2], mp[i + 1], mp[i + 2], X, Zi, n);
         B[i + (size_t)m * j] = v;
         B[j + (size_t)m * i] = v;
       }
       __syncthreads();
+      if (GENERAL && any_f1) {
+        if (blocked)
+          schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, B, s_nnz, s_form, s_nb, s_boff, s_bsz, gsm);
+        else
+          schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, B, s_nnz, s_form, 0, nullptr, nullptr, gsm);
+      }
       // ---- adjusted Cholesky and solve (compute_DyVec, sdpa_newton.cpp:2672-2716)
       if (cta::cholesky<NT, double>(m, B, m, true, sD, gsm, &s_flag)) break;
       for (int k = tid; k < m; k += NT) vdy[k] = vg[k];
@@ -560,7 +673,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       {
         // R and XDZ are free here (both are rebuilt by the next predictor)
         double mins[2];
-        if (BLOCKS && blocked)
+        if (GENERAL && blocked)
           min_eig_pair_blocks(n, s_nb, s_boff, s_bsz, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es,
                               mins, dz_diag);
         else
