@@ -170,47 +170,98 @@ __device__ __forceinline__ double f3_value(const int* row, const int* col, const
 // sdpa_newton.cpp:885-889, :1827-1922): for every constraint j flagged in
 // `form`, G = X A_j Z^-1 and B_ij = A_i . G for each i that j dominates.
 // T, G: n x n scratch.  With a block structure (nb > 0 blocks at boff of
-// signed orders bsz) Z^-1 is block-diagonal, so G is formed one block at a
-// time (sum of k^3 instead of n^3) and LP entries as diagonal products.
-// Not inlined: only instances with F1 constraints call it.
+// signed orders bsz; bid = SDP block of each row, -1 for LP entries) X, A_j
+// and Z^-1 are block-diagonal, so T = X A_j and G are formed one block at a
+// time, only for the blocks A_j touches (G is zero elsewhere), and LP
+// entries are diagonal products.  Not inlined: only instances with F1
+// constraints call it.
+//
+// T = X A_j with A_j symmetric, stored as upper entries (r, c, v).  Blocks
+// of order <= 64: A_j's block is scattered into the scratch Ad as a dense
+// k x k matrix and T = X_b A_b is a tiled block product like G = T Z^-1.
+// Larger blocks and a single block: one thread per row of T, accumulating
+// over the entries.
+static __device__ void f1_rows(int n, int r0, int k, long long jb, long long je, const int* er, const int* ec,
+                               const double* ev, const double* X, double* T)
+{
+  for (int i = r0 + (int)threadIdx.x; i < r0 + k; i += NT) {
+    for (int c = r0; c < r0 + k; ++c) T[i + (size_t)n * c] = 0.0;
+    for (long long e = jb; e < je; ++e) {
+      const int r = er[e], c = ec[e];
+      if (r < r0 || r >= r0 + k) continue;
+      const double v = ev[e];
+      T[i + (size_t)n * c] += v * X[i + (size_t)n * r];
+      if (r != c) T[i + (size_t)n * r] += v * X[i + (size_t)n * c];
+    }
+  }
+}
+
 static __device__ __noinline__ void schur_f1(int n, int m, const long long* mp, const int* er, const int* ec,
                                              const double* ev, const double* X, const double* Zi, double* T,
-                                             double* G, double* B, const int* nnz, const int* form, int nb,
-                                             const int* boff, const int* bsz, double* gsm)
+                                             double* G, double* Ad, double* B, const int* nnz, const int* form,
+                                             int nb, const int* boff, const int* bsz, const int* bid, double* gsm)
 {
+  __shared__ unsigned long long s_touch;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   for (int j = 0; j < m; ++j) {
     if (!form[j]) continue;
     const long long jb = mp[j + 1], je = mp[j + 2];
-    // T = X A_j: each thread owns rows of T (A_j symmetric, upper entries)
-    for (int i = tid; i < n; i += NT) {
-      for (int c = 0; c < n; ++c) T[i + (size_t)n * c] = 0.0;
-      for (long long e = jb; e < je; ++e) {
-        const int r = er[e], c = ec[e];
-        const double v = ev[e];
-        T[i + (size_t)n * c] += v * X[i + (size_t)n * r];
-        if (r != c) T[i + (size_t)n * r] += v * X[i + (size_t)n * c];
-      }
-    }
-    __syncthreads();
-    // G = T Z^-1; a block that A_j does not touch has T = 0 there, so its G
-    // block is zero without a product
     if (nb <= 0) {
+      f1_rows(n, 0, n, jb, je, er, ec, ev, X, T);
+      __syncthreads();
       cta::gemm<NT>(n, false, T, n, false, Zi, n, G, n, 1.0, 0.0, gsm);
     } else {
+      // blocks touched by A_j
+      if (tid == 0) s_touch = 0ull;
+      __syncthreads();
+      unsigned long long mine = 0ull;
+      for (long long e = jb + tid; e < je; e += NT) {
+        const int b = bid[er[e]];
+        if (b >= 0) mine |= 1ull << b;
+      }
+      if (mine) atomicOr(&s_touch, mine);
+      __syncthreads();
+      const unsigned long long touch = s_touch;
+      for (int l = 0; l < nb; ++l) {
+        const int k = bsz[l], o = boff[l];
+        if (k >= 2) {
+          if (!((touch >> l) & 1ull)) continue;
+          if (k > 64) {
+            f1_rows(n, o, k, jb, je, er, ec, ev, X, T);
+            continue;
+          }
+          for (int t = tid; t < k * k; t += NT) Ad[t] = 0.0;
+          __syncthreads();
+          for (long long e = jb + tid; e < je; e += NT) {
+            const int r = er[e] - o, c = ec[e] - o;
+            if (r < 0 || r >= k) continue;
+            Ad[r + k * c] = ev[e];
+            Ad[c + k * r] = ev[e];
+          }
+          __syncthreads();
+          const size_t od = (size_t)o * (n + 1);
+          cta::gemm<NT>(k, false, X + od, n, false, Ad, k, T + od, n, 1.0, 0.0, gsm);
+        } else {
+          // LP entries: G_tt = (sum of A_j's entries at (t, t)) X_tt Z^-1_tt
+          for (int t = tid; t < -k; t += NT) {
+            const int d = o + t;
+            double a = 0.0;
+            for (long long e = jb; e < je; ++e) a += (er[e] == d) ? ev[e] : 0.0;
+            const size_t dd = (size_t)d * (n + 1);
+            G[dd] = a * X[dd] * Zi[dd];
+          }
+        }
+      }
+      __syncthreads();
+      // G = T Z^-1 block by block; zero where A_j does not reach
       for (int l = 0; l < nb; ++l) {
         const int k = bsz[l];
+        if (k < 2) continue;
         const size_t o = (size_t)boff[l] * (n + 1);
-        if (k >= 2) {
-          int hit = 0;
-          for (long long e = jb + tid; e < je; e += NT) hit |= (er[e] >= boff[l] && er[e] < boff[l] + k);
-          if (__syncthreads_or(hit)) {
-            cta::gemm<NT>(k, false, T + o, n, false, Zi + o, n, G + o, n, 1.0, 0.0, gsm);
-          } else {
-            for (int t = threadIdx.x; t < k * k; t += NT) G[o + (size_t)(t % k) + (size_t)n * (t / k)] = 0.0;
-          }
+        if ((touch >> l) & 1ull) {
+          cta::gemm<NT>(k, false, T + o, n, false, Zi + o, n, G + o, n, 1.0, 0.0, gsm);
         } else {
-          for (int t = tid; t < -k; t += NT) G[o + (size_t)t * (n + 1)] = T[o + (size_t)t * (n + 1)] * Zi[o + (size_t)t * (n + 1)];
+          for (int t = tid; t < k * k; t += NT) G[o + (size_t)(t % k) + (size_t)n * (t / k)] = 0.0;
         }
       }
     }
@@ -597,9 +648,9 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       __syncthreads();
       if (GENERAL && any_f1) {
         if (blocked)
-          schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, B, s_nnz, s_form, s_nb, s_boff, s_bsz, gsm);
+          schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, dX, B, s_nnz, s_form, s_nb, s_boff, s_bsz, s_bid, gsm);
         else
-          schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, B, s_nnz, s_form, 0, nullptr, nullptr, gsm);
+          schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, dX, B, s_nnz, s_form, 0, nullptr, nullptr, nullptr, gsm);
       }
       // ---- adjusted Cholesky and solve (compute_DyVec, sdpa_newton.cpp:2672-2716)
       if (cta::cholesky<NT, double>(m, B, m, true, sD, gsm, &s_flag)) break;
