@@ -689,7 +689,7 @@ struct DevState {
 
 static const int NBG = 128;        // panel width of the grid-level Cholesky
 static const int F1_CHUNK = 32;    // F1 constraints processed per batched GEMM (= warp lanes in k_f1_spmm)
-static const int SMALL_SOLVE = 2048;  // Schur orders up to this use the one-block solve
+static const int SMALL_SOLVE = 512;   // Schur orders up to this use the one-block solve
 
 static size_t chol_smem() { return (cta::GEMM_RECT_SMEM + cta::SD_DOUBLES) * sizeof(double); }
 
