@@ -9,11 +9,18 @@
  *    and make initializeSolve/solve return without solving;
  *  - setNumThreads is accepted and ignored (the solve runs on the GPU);
  *  - SOCP is rejected as in the reference.
- * SDPA_INT is int (the reference's LP64 configuration, sdpa_include.h:44-45).
+ * SDPA_INT is int by default (the reference's LP64 configuration,
+ * LP64/sdpa_include.h:43-45), with sdpa_b200/_lib/libsdpa_b200.so.  Callers
+ * built for the reference's ILP64 configuration (ILP64/sdpa_include.h:43-45,
+ * SDPA_INT = int64_t) compile with -DSDPA_INT=int64_t and link
+ * sdpa_b200/_lib/libsdpa_b200_ilp64.so, the same library with that integer
+ * type in the class's signatures.  Sizes and indices beyond the int range
+ * are rejected (the solver's dense Schur matrix limits m far below it).
  */
 #ifndef SDPA_B200_SDPA_CALL_H
 #define SDPA_B200_SDPA_CALL_H
 
+#include <cstdint>
 #include <cstdio>
 
 #ifndef SDPA_INT

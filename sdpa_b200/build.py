@@ -19,6 +19,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT, "libsdpa_b200.so")
+# The same library with SDPA_INT = int64_t in class SDPA's signatures, for
+# callers built against the reference's ILP64 configuration.
+LIB_ILP64 = os.path.join(OUT, "libsdpa_b200_ilp64.so")
 CLI_SRC = os.path.join(HERE, "cli", "sdpa_main.cpp")
 CLI = os.path.join(OUT, "sdpa")  # the drop-in for the reference's sdpa executable
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -55,6 +58,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    # ILP64: sdpa_call.cpp again with SDPA_INT = int64_t, the other objects shared
+    call_src = os.path.join(CSRC, "sdpa_call.cpp")
+    call64 = os.path.join(OUT, "sdpa_call.ilp64.o")
+    if (force or not os.path.exists(call64) or os.path.getmtime(call64) < os.path.getmtime(call_src)
+            or os.path.getmtime(call64) < hdr_time):
+        cmd = [NVCC] + ARCH + CFLAGS + ["-DSDPA_INT=int64_t", "-x", "c++", "-c", call_src, "-o", call64]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    objs64 = [o for o in objs if not o.endswith("sdpa_call.cpp.o")] + [call64]
+    if force or not os.path.exists(LIB_ILP64) or os.path.getmtime(LIB_ILP64) < max(os.path.getmtime(o)
+                                                                                   for o in objs64):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB_ILP64] + objs64 + ["-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -8,6 +8,7 @@
 #include "sdpa_call.h"
 
 #include <ctype.h>
+#include <limits.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -407,6 +408,14 @@ static void print_iteration(FILE* fp, int it, const double* r)
 
 using sdpab::SdpaImpl;
 
+// SDPA_INT may be int64_t (the ILP64 build of this file): sizes and indices
+// are checked against the int range the solver stores them in.
+template <class T>
+static bool in_int(T v)
+{
+  return (long long)v >= (long long)INT_MIN && (long long)v <= (long long)INT_MAX;
+}
+
 SDPA::SDPA() : impl_(new SdpaImpl()) {}
 SDPA::~SDPA() { delete impl_; }
 
@@ -415,7 +424,11 @@ void SDPA::setParameterType(ParameterType type)
   impl_->ptype = (int)type;
   impl_->prm = sdpab::default_params((int)type);
 }
-void SDPA::setParameterMaxIteration(SDPA_INT v) { impl_->prm.maxIteration = v; }
+void SDPA::setParameterMaxIteration(SDPA_INT v)
+{
+  if (!in_int(v)) return impl_->fail(SDPAB_EINVAL, "setParameterMaxIteration: value out of range");
+  impl_->prm.maxIteration = (int)v;
+}
 void SDPA::setParameterEpsilonStar(double v) { impl_->prm.epsilonStar = v; }
 void SDPA::setParameterLambdaStar(double v) { impl_->prm.lambdaStar = v; }
 void SDPA::setParameterOmegaStar(double v) { impl_->prm.omegaStar = v; }
@@ -437,8 +450,9 @@ void SDPA::setInitPoint(bool b) { impl_->isInitPoint = b; }
 // value, or OMP_NUM_THREADS, or 1.
 void SDPA::setNumThreads(SDPA_INT n)
 {
-  impl_->numThreads = n;
-  int nt = n;
+  if (!in_int(n)) return impl_->fail(SDPAB_EINVAL, "setNumThreads: value out of range");
+  impl_->numThreads = (int)n;
+  int nt = (int)n;
   if (nt == 0) {
     const char* env = getenv("OMP_NUM_THREADS");
     nt = env ? atoi(env) : 1;
@@ -469,18 +483,21 @@ SDPA_INT SDPA::getNumThreads() { return impl_->numThreads; }
 
 void SDPA::inputConstraintNumber(SDPA_INT m)
 {
-  impl_->prob.m = m;
-  impl_->prob.c.assign(m, 0.0);
+  if (m < 0 || !in_int(m)) return impl_->fail(SDPAB_EINVAL, "inputConstraintNumber: m out of range");
+  impl_->prob.m = (int)m;
+  impl_->prob.c.assign((size_t)m, 0.0);
 }
 void SDPA::inputBlockNumber(SDPA_INT nBlock)
 {
-  impl_->prob.blockStruct.assign(nBlock, 0);
-  impl_->prob.blockType.assign(nBlock, 0);
+  if (nBlock < 0 || !in_int(nBlock)) return impl_->fail(SDPAB_EINVAL, "inputBlockNumber: nBlock out of range");
+  impl_->prob.blockStruct.assign((size_t)nBlock, 0);
+  impl_->prob.blockType.assign((size_t)nBlock, 0);
 }
 void SDPA::inputBlockSize(SDPA_INT l, SDPA_INT size)
 {
   if (l < 1 || l > impl_->nb()) return impl_->fail(SDPAB_EINVAL, "inputBlockSize: l out of range");
-  impl_->prob.blockStruct[l - 1] = size;
+  if (!in_int(size)) return impl_->fail(SDPAB_EINVAL, "inputBlockSize: size out of range");
+  impl_->prob.blockStruct[l - 1] = (int)size;
   if (size < 0) impl_->prob.blockType[l - 1] = 2;
 }
 void SDPA::inputBlockType(SDPA_INT l, ConeType t)
@@ -504,7 +521,7 @@ void SDPA::inputElement(SDPA_INT k, SDPA_INT l, SDPA_INT i, SDPA_INT j, double v
     if (!I.isSdp(l - 1) && i != j) return I.fail(SDPAB_EINVAL, "inputElement: i != j in an LP block");
   }
   if (i > j) std::swap(i, j);
-  I.prob.entries.push_back({k, l, i, j, v});
+  I.prob.entries.push_back({(int)k, (int)l, (int)i, (int)j, v});
 }
 void SDPA::inputInitXVec(SDPA_INT k, double v)
 {
@@ -512,11 +529,11 @@ void SDPA::inputInitXVec(SDPA_INT k, double v)
   if (k < 1 || k > impl_->prob.m) return impl_->fail(SDPAB_EINVAL, "inputInitXVec: k out of range");
   impl_->init.xvec[k - 1] = v;
 }
-static void set_init(SdpaImpl& I, bool isX, int l, int i, int j, double v)
+static void set_init(SdpaImpl& I, bool isX, long long l, long long i, long long j, double v)
 {
   I.ensureInit();
   if (l < 1 || l > I.nb()) return I.fail(SDPAB_EINVAL, "inputInit: l out of range");
-  const int n = I.blockDim(l - 1);
+  const int n = I.blockDim((int)l - 1);
   if (i < 1 || j < 1 || i > n || j > n) return I.fail(SDPAB_EINVAL, "inputInit: i/j out of range");
   std::vector<double>& M = isX ? I.init.X[l - 1] : I.init.Y[l - 1];
   if (I.isSdp(l - 1)) {

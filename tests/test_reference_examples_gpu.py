@@ -4,7 +4,8 @@ with libsdpa_b200.so (oracle/Makefile `examples`), against the same
 programs linked with the reference library: the same printed layout line
 for line (numbers masked, the version banner excepted), the same phases and
 iteration counts, objectives within 1e-6 and printed solutions within the
-printed precision."""
+printed precision.  The ILP64 tree's copies of the same programs, compiled
+with SDPA_INT = int64_t against libsdpa_b200_ilp64.so, must print the same."""
 import os
 import re
 import shutil
@@ -36,10 +37,11 @@ def _values(text, key):
             if ln.split("=")[0].strip() == key and "=" in ln]
 
 
+@pytest.mark.parametrize("variant", ["b200", "b200_ilp64"])
 @pytest.mark.parametrize("e", sorted(ARGS))
-def test_reference_example_runs_unchanged_on_b200(e, tmp_path):
+def test_reference_example_runs_unchanged_on_b200(e, variant, tmp_path):
     ref_bin = os.path.join(EX, f"ref_example{e}")
-    ours_bin = os.path.join(EX, f"b200_example{e}")
+    ours_bin = os.path.join(EX, f"{variant}_example{e}")
     if not (os.path.exists(ref_bin) and os.path.exists(ours_bin)):
         pytest.skip("reference examples not built (make -C oracle examples needs the reference sources)")
     dirs = {}
