@@ -292,6 +292,17 @@ typedef struct sdpab_batch_config {
 SDPAB_API long long sdpab_tc_syrk_work_bytes(int M, int K);  /* device scratch of the call below */
 SDPAB_API int sdpab_tc_syrk(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, void* stream);
 
+/* Tensor-core product C_q = A_q B^T for q < batch, FP64 in and out
+ * (column-major device pointers; A_q M x K at A + q sA, B N x K shared, C_q
+ * M x N at C + q sC), in split TF32 with FP32 accumulation: the F1 products
+ * (X A_j) Z^-1 of the mixed-precision Schur assembly (Z^-1 symmetric, so
+ * B = Z^-1), exposed stand-alone (no counterpart in the reference, whose F1
+ * products are dgemm calls, sdpa_newton.cpp:885-889).  Synchronises
+ * `stream`. */
+SDPAB_API long long sdpab_tc_gemm_work_bytes(int M, int N, int K, int batch);
+SDPAB_API int sdpab_tc_gemm(int M, int N, int K, int batch, const double* A, int lda, long long sA, const double* B,
+                            int ldb, double* C, int ldc, long long sC, void* work, void* stream);
+
 /* Solves a batch whose arrays (problem, init, result) are all DEVICE pointers,
  * asynchronously on `stream` (a cudaStream_t, NULL = default stream).
  * `order` (device, optional) gives the processing order of the instances;

@@ -110,6 +110,9 @@ SIGNATURES = [
     ("sdpab_release_workspace", c_int, []),
     ("sdpab_tc_syrk_work_bytes", c_longlong, [c_int, c_int]),
     ("sdpab_tc_syrk", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
+    ("sdpab_tc_gemm_work_bytes", c_longlong, [c_int, c_int, c_int, c_int]),
+    ("sdpab_tc_gemm", c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_longlong, c_void_p, c_int, c_void_p,
+                              c_int, c_longlong, c_void_p, c_void_p]),
 ]
 
 _lib = None

@@ -15,6 +15,9 @@ int set_error(int code, const char* msg);
 // waiting for its MMAs (the update is then incomplete).
 long long syrk_tf32x3_work_bytes(int M, int K);
 int syrk_tf32x3(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, int* err, cudaStream_t st);
+long long gemm_tf32x3_work_bytes(int M, int N, int K, int batch);
+int gemm_tf32x3(int M, int N, int K, int batch, const double* A, int lda, long long sA, const double* B, int ldb,
+                double* C, int ldc, long long sC, void* work, int* err, cudaStream_t st);
 int cuda_error(cudaError_t e, const char* where);
 
 // Device memory kept between solver calls on the current device: the

@@ -662,6 +662,8 @@ struct DevState {
   int* tc_err = nullptr;    // tensor-core update time-out flag (inside the flag allocation)
   bool tc = false;          // mixed mode: tensor-core trailing updates of the FP32 Schur factor
   void* tc_work = nullptr;  // their split operands (syrk_tf32x3_work_bytes(m, NBG))
+  int* tc_f1_err = nullptr;   // time-out flag of the tensor-core F1 products
+  void* tc_f1_work = nullptr; // split operands of the tensor-core F1 products (mixed mode)
   std::vector<void*> allocs;
   double* alloc(size_t n)
   {
@@ -1061,6 +1063,7 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
   S.allocs.push_back(fp);
   S.flag = (int*)fp;
   S.tc_err = S.flag + 16;
+  S.tc_f1_err = S.flag + 20;
   if (!S.B || !S.T || !S.b) return set_error(SDPAB_ECUDA, "device allocation failed (Schur matrix)");
   // shared memory limits of the block-level kernels
   cudaFuncSetAttribute(k_min_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -1096,6 +1099,17 @@ int Solver::solve(const InitPoint* init, const Params* prm)
       if (cudaMalloc(&w, (size_t)syrk_tf32x3_work_bytes(m, NBG)) == cudaSuccess) {
         S.allocs.push_back(w);
         S.tc_work = w;
+      }
+    }
+    // split operands of the tensor-core F1 products (X A_j) Z^-1, one chunk
+    long long f1w = 0;
+    for (const SdpBlock& B : S.sdp)
+      if (!B.hf1.empty()) f1w = std::max(f1w, gemm_tf32x3_work_bytes(B.n, B.n, B.n, F1_CHUNK));
+    if (precision_ == SDPAB_PREC_MIXED && f1w > 0) {
+      void* w = nullptr;
+      if (cudaMalloc(&w, (size_t)f1w) == cudaSuccess) {
+        S.allocs.push_back(w);
+        S.tc_f1_work = w;
       }
     }
     S.Linv32 = S.B32 + (size_t)m * m;
@@ -1323,7 +1337,12 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     }
     a_dot(S.g, S.rp, -1.0, Wv, Wl);
     mark(T_BMAT);
-    // ---- Schur complement (Newton::Make_bMat)
+    // ---- Schur complement (Newton::Make_bMat).  In the FP32 phase of the
+    // mixed mode the F1 products (X A_j) Z^-1 run on the tensor cores in
+    // split TF32 (gemm_tf32x3); a tensor-core block that gave up waiting
+    // leaves its tile unwritten, and the matrix is then built again with the
+    // SIMT products.
+    auto build_bmat = [&](bool use_tc) {
     cudaMemset(S.B, 0, (size_t)m * m * sizeof(double));
     for (SdpBlock& B : S.sdp) {
       if (!B.nc) continue;
@@ -1336,7 +1355,10 @@ int Solver::solve(const InitPoint* init, const Params* prm)
         double* T = S.T;
         double* G = S.T + (size_t)F1_CHUNK * nn;
         k_f1_left<<<dim3(B.n, cnt), 256>>>(B.n, q0, B.f1, B.csc_cptr, B.csc_ptr, B.csc_row, B.csc_val, B.X, T);
-        gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn, lowp);
+        const bool tc_done = use_tc && gemm_tf32x3(B.n, B.n, B.n, cnt, T, B.n, nn, B.Zi, B.n, G, B.n, nn,
+                                                   S.tc_f1_work, S.tc_f1_err, 0) == 0;
+        if (!tc_done)
+          gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn, lowp);
         static bool pack_attr = false;
         if (!pack_attr) {
           cudaFuncSetAttribute(k_f1_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F1_PACK_SMEM);
@@ -1349,6 +1371,18 @@ int Solver::solve(const InitPoint* init, const Params* prm)
       }
     }
     if (nlp) k_lp_bmat<<<nlp, 256>>>(S.lpT_ptr, S.lpT_k, S.lpT_v, S.lpx, S.lpzi, S.B, m);
+    };
+    const bool tc_f1 = lowp && S.tc_f1_work;
+    if (tc_f1) cudaMemset(S.tc_f1_err, 0, sizeof(int));
+    build_bmat(tc_f1);
+    if (tc_f1) {
+      int te = 0;
+      cudaMemcpy(&te, S.tc_f1_err, sizeof(int), cudaMemcpyDeviceToHost);
+      if (te) {
+        stats_.tc_timeouts += 1;
+        build_bmat(false);
+      }
+    }
     mark(T_CHOL);
     // ---- Cholesky with adjustment + solve (Newton::compute_DyVec).  Mixed
     // precision while mixed_gap >= mu_switch: FP32 factor of the FP64 Schur matrix

@@ -1,7 +1,8 @@
-"""The tensor-core (tcgen05, split TF32) lower update C -= P P^T of the
-mixed-precision Schur factorisation against an FP64 numpy reference:
-partial tiles, K not a multiple of the staging width, the upper triangle
-untouched, FP32-level error."""
+"""The tensor-core (tcgen05, split TF32) kernels against FP64 numpy
+references: the lower update C -= P P^T of the mixed-precision Schur
+factorisation (partial tiles, K not a multiple of the staging width, the
+upper triangle untouched) and the batched F1 product C_q = A_q B^T, both
+with FP32-level error."""
 import numpy as np
 import pytest
 
@@ -30,3 +31,39 @@ def test_tc_syrk_matches_fp64(M, K):
     assert err <= 2e-6 * scale, (err, scale)
     np.testing.assert_array_equal(C[~low], C0[~low])  # strictly upper triangle untouched
     assert np.all(Cd[:, M:].cpu().numpy() == 0)  # nothing written outside M x M
+
+
+@pytest.mark.parametrize("M,N,K,batch", [(128, 128, 16, 1), (200, 300, 70, 3), (500, 500, 500, 2), (37, 129, 131, 4)])
+def test_tc_gemm_matches_fp64(M, N, K, batch):
+    """The split-TF32 product of the mixed-precision F1 assembly,
+    C_q = A_q B^T with FP64 operands: partial tiles, K not a multiple of the
+    staging width, a batch with strides, FP32-level error against FP64."""
+    import torch
+    from sdpa_b200 import _native as N_
+    rng = np.random.default_rng(M * 7 + N * 5 + K * 3 + batch)
+    A = rng.standard_normal((batch, M, K))
+    B = rng.standard_normal((N, K))
+    lda, ldb, ldc = M + 2, N + 1, M + 5
+    sA, sC = lda * K + 7, ldc * N + 3
+    Ad = torch.zeros(batch * sA, dtype=torch.float64, device="cuda")
+    Bd = torch.zeros(ldb * K, dtype=torch.float64, device="cuda")
+    Cd = torch.zeros(batch * sC, dtype=torch.float64, device="cuda")
+    for q in range(batch):
+        blk = np.zeros((K, lda))
+        blk[:, :M] = A[q].T
+        Ad[q * sA:q * sA + lda * K] = torch.from_numpy(blk.ravel()).cuda()
+    bb = np.zeros((K, ldb))
+    bb[:, :N] = B.T
+    Bd[:] = torch.from_numpy(bb.ravel()).cuda()
+    work = torch.empty(int(N_.lib().sdpab_tc_gemm_work_bytes(M, N, K, batch)) // 8 + 4, dtype=torch.float64,
+                       device="cuda")
+    N_.check(N_.lib().sdpab_tc_gemm(M, N, K, batch, Ad.data_ptr(), lda, sA, Bd.data_ptr(), ldb, Cd.data_ptr(), ldc,
+                                    sC, work.data_ptr(), None), "tc_gemm")
+    Ch = Cd.cpu().numpy()
+    for q in range(batch):
+        C = Ch[q * sC:q * sC + ldc * N].reshape(N, ldc)[:, :M].T
+        ref = A[q] @ B.T
+        bound = np.abs(A[q]) @ np.abs(B).T
+        assert np.all(np.abs(C - ref) <= 5e-6 * bound + 1e-300), np.max(np.abs(C - ref) / bound)
+        pad = Ch[q * sC:q * sC + ldc * N].reshape(N, ldc)[:, M:]
+        assert np.all(pad == 0)  # nothing written outside M x N
