@@ -529,34 +529,56 @@ __global__ void k_convert(long long n, TO* out, const TI* in)
 
 // Blocked triangular solves with the stored diagonal-block inverses of the
 // Cholesky factor (one block: x_b = Dinv_b x_b or Dinv_b^T x_b).
+// 512 threads: row i = threadIdx.x % 128 (bs <= 128), column group
+// g = threadIdx.x / 128 takes every fourth column; the four partial sums are
+// reduced in shared memory.  Rows read Dinv coalesced (consecutive i) in
+// the forward product; the transposed product reads row i's column
+// segment, contiguous per thread.
 template <typename T>
-__global__ void k_trsv_diag(int bs, const T* Dinv, T* x, int trans)
+__global__ void __launch_bounds__(512) k_trsv_diag(int bs, const T* Dinv, T* x, int trans)
 {
-  __shared__ T xs[256];
+  __shared__ T xs[128];
+  __shared__ T part[4][129];
   for (int i = threadIdx.x; i < bs; i += blockDim.x) xs[i] = x[i];
   __syncthreads();
-  for (int i = threadIdx.x; i < bs; i += blockDim.x) {
-    T s = (T)0;
+  const int i = threadIdx.x & 127, g = threadIdx.x >> 7;
+  T s = (T)0;
+  if (i < bs) {
     if (!trans)
-      for (int p = 0; p <= i; ++p) s += Dinv[i + (size_t)bs * p] * xs[p];
+      for (int p = g; p <= i; p += 4) s += Dinv[i + (size_t)bs * p] * xs[p];
     else
-      for (int p = i; p < bs; ++p) s += Dinv[p + (size_t)bs * i] * xs[p];
-    x[i] = s;
+      for (int p = i + ((g - i) & 3); p < bs; p += 4) s += Dinv[p + (size_t)bs * i] * xs[p];
   }
+  part[g][i] = s;
+  __syncthreads();
+  if (g == 0 && i < bs) x[i] = part[0][i] + part[1][i] + part[2][i] + part[3][i];
 }
 
-// forward update: x[r] -= sum_p L[r, kb+p] x[kb+p] for the rows below the block
+// forward update: x[r] -= sum_p L[r, kb+p] x[kb+p] for the rows below the
+// block.  256-thread blocks of 32 rows x 8 column groups (each column read
+// by 32 consecutive rows, 256 bytes in FP64), partial sums reduced in shared
+// memory: eight times the threads of one thread per row, so a panel of
+// ~10^4 rows spreads over a few hundred blocks.
 template <typename T>
-__global__ void k_trsv_fwd_update(int rows, int bs, const T* Lp, int ld, const T* xb, T* xr)
+__global__ void __launch_bounds__(256) k_trsv_fwd_update(int rows, int bs, const T* Lp, int ld, const T* xb, T* xr)
 {
   __shared__ T xs[256];
+  __shared__ T part[8][33];
   for (int i = threadIdx.x; i < bs; i += blockDim.x) xs[i] = xb[i];
   __syncthreads();
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= rows) return;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int r = blockIdx.x * 32 + tx;
   T s = (T)0;
-  for (int p = 0; p < bs; ++p) s += Lp[r + (size_t)ld * p] * xs[p];
-  xr[r] -= s;
+  if (r < rows)
+    for (int p = ty; p < bs; p += 8) s += Lp[r + (size_t)ld * p] * xs[p];
+  part[ty][tx] = s;
+  __syncthreads();
+  if (ty == 0 && r < rows) {
+    T t = part[0][tx];
+#pragma unroll
+    for (int g = 1; g < 8; ++g) t += part[g][tx];
+    xr[r] -= t;
+  }
 }
 
 // backward update: x[i] -= sum_p L[kb+p, i] x[kb+p] for i < kb (one warp per i)
@@ -777,13 +799,13 @@ static void chol_solve_grid(int m, const T* L, const T* dinv, T* x)
   const int nb = (m + NBG - 1) / NBG;
   for (int b = 0; b < nb; ++b) {
     const int kb = b * NBG, bs = std::min(NBG, m - kb), rem = m - kb - bs;
-    k_trsv_diag<T><<<1, 256>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 0);
+    k_trsv_diag<T><<<1, 512>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 0);
     if (rem > 0)
-      k_trsv_fwd_update<T><<<nblk(rem), 256>>>(rem, bs, L + (kb + bs) + (size_t)m * kb, m, x + kb, x + kb + bs);
+      k_trsv_fwd_update<T><<<(rem + 31) / 32, 256>>>(rem, bs, L + (kb + bs) + (size_t)m * kb, m, x + kb, x + kb + bs);
   }
   for (int b = nb - 1; b >= 0; --b) {
     const int kb = b * NBG, bs = std::min(NBG, m - kb);
-    k_trsv_diag<T><<<1, 256>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 1);
+    k_trsv_diag<T><<<1, 512>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 1);
     if (kb > 0) k_trsv_bwd_update<T><<<nblk((long long)kb * 32), 256>>>(kb, bs, L + kb, m, x + kb, x);
   }
 }
