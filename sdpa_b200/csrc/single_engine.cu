@@ -654,8 +654,18 @@ struct SdpBlock {
   double* csc_val = nullptr;
 };
 
+// A captured grid solve (chol_solve_graph).
+struct SolveGraph {
+  const void* L;
+  const void* dinv;
+  void* x;
+  int m;
+  cudaGraphExec_t exec;
+};
+
 struct DevState {
   int m = 0, nlp = 0, nDim = 0;
+  std::vector<SolveGraph> solve_graphs;
   Params prm;
   std::vector<int> blockStruct, blockKind, blockIndex;  // kind 0 SDP, 2 LP; index = SDP idx or LP offset
   std::vector<SdpBlock> sdp;
@@ -707,6 +717,7 @@ struct DevState {
   }
   ~DevState()
   {
+    for (SolveGraph& g : solve_graphs) cudaGraphExecDestroy(g.exec);
     for (void* p : allocs) cudaFree(p);
   }
 };
@@ -794,19 +805,57 @@ static int cholesky_grid(DevState& S, double* A, int n, bool adjust, double* din
 // x = L^{-T} L^{-1} x with the factor of cholesky_grid_t and its stored
 // diagonal-block inverses (grid-wide updates between the block solves).
 template <typename T>
-static void chol_solve_grid(int m, const T* L, const T* dinv, T* x)
+static void chol_solve_grid(int m, const T* L, const T* dinv, T* x, cudaStream_t st = 0)
 {
   const int nb = (m + NBG - 1) / NBG;
   for (int b = 0; b < nb; ++b) {
     const int kb = b * NBG, bs = std::min(NBG, m - kb), rem = m - kb - bs;
-    k_trsv_diag<T><<<1, 512>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 0);
+    k_trsv_diag<T><<<1, 512, 0, st>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 0);
     if (rem > 0)
-      k_trsv_fwd_update<T><<<(rem + 31) / 32, 256>>>(rem, bs, L + (kb + bs) + (size_t)m * kb, m, x + kb, x + kb + bs);
+      k_trsv_fwd_update<T><<<(rem + 31) / 32, 256, 0, st>>>(rem, bs, L + (kb + bs) + (size_t)m * kb, m, x + kb, x + kb + bs);
   }
   for (int b = nb - 1; b >= 0; --b) {
     const int kb = b * NBG, bs = std::min(NBG, m - kb);
-    k_trsv_diag<T><<<1, 512>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 1);
-    if (kb > 0) k_trsv_bwd_update<T><<<nblk((long long)kb * 32), 256>>>(kb, bs, L + kb, m, x + kb, x);
+    k_trsv_diag<T><<<1, 512, 0, st>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 1);
+    if (kb > 0) k_trsv_bwd_update<T><<<nblk((long long)kb * 32), 256, 0, st>>>(kb, bs, L + kb, m, x + kb, x);
+  }
+}
+
+// The grid solve is ~4 launches per 128-row block and direction (about 300
+// for m = 10^4), each a few microseconds of work: captured once as a CUDA
+// graph per (factor, diagonal inverses, right-hand side) and replayed on the
+// default stream.  Capture failures fall back to direct launches.
+template <typename T>
+static void chol_solve_graph(DevState& S, int m, const T* L, const T* dinv, T* x)
+{
+  for (const SolveGraph& g : S.solve_graphs)
+    if (g.L == (const void*)L && g.dinv == (const void*)dinv && g.x == (void*)x && g.m == m) {
+      if (cudaGraphLaunch(g.exec, 0) == cudaSuccess) return;
+      cudaGetLastError();
+      chol_solve_grid<T>(m, L, dinv, x);
+      return;
+    }
+  cudaStream_t cs = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    chol_solve_grid<T>(m, L, dinv, x, cs);
+    ok = cudaStreamEndCapture(cs, &graph) == cudaSuccess && graph != nullptr;
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  }
+  if (graph) cudaGraphDestroy(graph);
+  if (cs) cudaStreamDestroy(cs);
+  if (!ok) {
+    cudaGetLastError();
+    chol_solve_grid<T>(m, L, dinv, x);
+    return;
+  }
+  S.solve_graphs.push_back({(const void*)L, (const void*)dinv, (void*)x, m, exec});
+  if (cudaGraphLaunch(exec, 0) != cudaSuccess) {
+    cudaGetLastError();
+    chol_solve_grid<T>(m, L, dinv, x);
   }
 }
 
@@ -1429,11 +1478,11 @@ int Solver::solve(const InitPoint* init, const Params* prm)
       break;
     }
     auto solve64 = [&](double* x) {
-      if (m > SMALL_SOLVE) chol_solve_grid<double>(m, S.B, S.dinv, x);
+      if (m > SMALL_SOLVE) chol_solve_graph<double>(S, m, S.B, S.dinv, x);
       else k_chol_solve<double><<<1, NT, cta::SD_DOUBLES * sizeof(double)>>>(m, S.B, x);
     };
     auto solve32 = [&](float* x) {
-      if (m > SMALL_SOLVE) chol_solve_grid<float>(m, S.B32, S.dinv32, x);
+      if (m > SMALL_SOLVE) chol_solve_graph<float>(S, m, S.B32, S.dinv32, x);
       else k_chol_solve<float><<<1, NT, cta::SD_DOUBLES * sizeof(float)>>>(m, S.B32, x);
     };
     auto schur_solve = [&](double* x) {
