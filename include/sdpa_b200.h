@@ -280,7 +280,7 @@ typedef struct sdpab_batch_config {
                                   |objective|) < this (0 = 1e-2) */
   int staging_doubles;         /* shared-memory staging of GEMM tiles and Lanczos
                                   matrices per solver block, in doubles (0 = auto;
-                                  raised to the GEMM minimum of 6144) */
+                                  raised to the GEMM minimum of 6400) */
 } sdpab_batch_config;
 
 /* Tensor-core lower update C -= P P^T of an M x M FP32 matrix, P M x K

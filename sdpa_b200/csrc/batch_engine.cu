@@ -56,7 +56,7 @@ static size_t smem_bytes_for(int nmax, int mmax, long long gsm)
 // else the GEMM minimum.
 static long long staging_doubles(int nmax, int mmax, int want)
 {
-  const long long g = 4 * 16 * 96;  // double-buffered single-tile GEMM (n <= 96)
+  const long long g = 4 * 16 * 100;  // double-buffered single-tile GEMM (n <= 96, rows padded to 100)
   const long long m2 = (long long)nmax * nmax;
   long long s;
   if (want > 0) s = want;

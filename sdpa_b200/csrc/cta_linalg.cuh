@@ -406,76 +406,101 @@ __device__ __noinline__ void gemm_tile(int n, bool tA, const TM* A, int lda, boo
   __syncthreads();
 }
 
-// FP64 gemm_tile with double-buffered staging: chunk k+1 is copied by
-// cp.async while chunk k is multiplied, so each chunk costs one barrier and
-// its load latency is hidden.  smem: 4 * 16 * 16R doubles.
-template <int NT, int R>
-__device__ __noinline__ void gemm_tile_db(int n, bool tA, const double* A, int lda, bool tB, const double* B,
-                                          int ldb, double* C, int ldc, double alpha, double beta, void* smem_v)
+// FP64 tile GEMM for n <= 96 on the FP64 tensor-core MMA
+// (mma.sync m8n8k4 .f64: one 8 x 8 x 4 product, 256 FMAs, per warp
+// instruction): one exact-size tile T x T (T = 16 R >= n), 256 threads as
+// 2 x 4 warps, warp (wr, wc) owning the 8 x 8 blocks (wr + 2 i, wc + 4 j).
+// K is staged in chunks of 16 by cp.async into two buffers ([k][r] with a
+// row stride of T + 4 doubles, so each half-warp's fragment loads fall on
+// distinct banks); per step of 4 a warp loads R A fragments and up to
+// (R + 1) / 2 B fragments and issues R x (R + 1) / 2 MMAs.  Fragments
+// (PTX m8n8k4 .f64): lane l holds A(l / 4, l % 4), B(l % 4, l / 4) and
+// C(l / 4, 2 (l % 4) + {0, 1}).  smem: 4 * 16 * (T + 4) doubles.
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b)
 {
-  constexpr int T = 16 * R, KC = 16;
-  double* buf = (double*)smem_v;  // [2][As: KC*T | Bs: KC*T]
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <int NT, int R>
+__device__ __noinline__ void gemm_tile_mma(int n, bool tA, const double* A, int lda, bool tB, const double* B,
+                                           int ldb, double* C, int ldc, double alpha, double beta, void* smem_v)
+{
+  static_assert(NT == 256, "gemm_tile_mma: 8 warps");
+  constexpr int T = 16 * R, TP = T + 4, KC = 16, NB = T / 8, RB = R, CB = (R + 1) / 2;
+  double* buf = (double*)smem_v;  // [2][As: KC*TP | Bs: KC*TP]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wr = w & 1, wc = w >> 1;
+  const int q = lane & 3, p = lane >> 2;
   auto issue = [&](int k0, int which) {
-    double* As = buf + which * 2 * KC * T;
-    double* Bs = As + KC * T;
+    double* As = buf + which * 2 * KC * TP;
+    double* Bs = As + KC * TP;
     for (int t = threadIdx.x; t < KC * T; t += NT) {
       int r, k;
       if (!tA) { r = t % T; k = t / T; } else { k = t % KC; r = t / KC; }
       const int gk = k0 + k;
       const bool va = r < n && gk < n;
-      cp_async8(&As[k * T + r], va ? (tA ? A + gk + (size_t)lda * r : A + r + (size_t)lda * gk) : A, va);
+      cp_async8(&As[k * TP + r], va ? (tA ? A + gk + (size_t)lda * r : A + r + (size_t)lda * gk) : A, va);
       int c;
       if (!tB) { k = t % KC; c = t / KC; } else { c = t % T; k = t / T; }
       const int gk2 = k0 + k;
       const bool vb = c < n && gk2 < n;
-      cp_async8(&Bs[k * T + c], vb ? (tB ? B + c + (size_t)ldb * gk2 : B + gk2 + (size_t)ldb * c) : B, vb);
+      cp_async8(&Bs[k * TP + c], vb ? (tB ? B + c + (size_t)ldb * gk2 : B + gk2 + (size_t)ldb * c) : B, vb);
     }
     cp_async_commit();
   };
-  double acc[R][R];
+  double acc[RB][CB][2];
 #pragma unroll
-  for (int i = 0; i < R; ++i)
+  for (int i = 0; i < RB; ++i)
 #pragma unroll
-    for (int j = 0; j < R; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < CB; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int nch = (n + KC - 1) / KC;
   issue(0, 0);
   for (int ch = 0; ch < nch; ++ch) {
     cp_async_wait_all();
     __syncthreads();  // chunk ch visible; every thread is done with chunk ch-1's buffer
     if (ch + 1 < nch) issue((ch + 1) * KC, (ch + 1) & 1);
-    const double* As = buf + (ch & 1) * 2 * KC * T;
-    const double* Bs = As + KC * T;
+    const double* As = buf + (ch & 1) * 2 * KC * TP;
+    const double* Bs = As + KC * TP;
+    // rows k >= n of the last chunk are zero-filled: whole steps of 4
     const int kmax = min(KC, n - ch * KC);
-    for (int k = 0; k < kmax; ++k) {
-      double a[R], b[R];
+    for (int kk = 0; kk < kmax; kk += 4) {
+      double a[RB], b[CB];
 #pragma unroll
-      for (int i = 0; i < R; ++i) a[i] = As[k * T + ty + 16 * i];
+      for (int i = 0; i < RB; ++i) a[i] = As[(kk + q) * TP + (wr + 2 * i) * 8 + p];
 #pragma unroll
-      for (int j = 0; j < R; ++j) b[j] = Bs[k * T + tx + 16 * j];
+      for (int j = 0; j < CB; ++j) {
+        const int cb = wc + 4 * j;
+        b[j] = (cb < NB) ? Bs[(kk + q) * TP + cb * 8 + p] : 0.0;
+      }
 #pragma unroll
-      for (int i = 0; i < R; ++i)
+      for (int i = 0; i < RB; ++i)
 #pragma unroll
-        for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < CB; ++j)
+          if (wc + 4 * j < NB) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
   }
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int gr = ty + 16 * i;
+  for (int i = 0; i < RB; ++i) {
+    const int gr = (wr + 2 * i) * 8 + p;
 #pragma unroll
-    for (int j = 0; j < R; ++j) {
-      const int gc = tx + 16 * j;
-      if (gr < n && gc < n) {
-        double* cp = C + gr + (size_t)ldc * gc;
-        *cp = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
+    for (int j = 0; j < CB; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gc = (wc + 4 * j) * 8 + 2 * q + h;
+        if (wc + 4 * j < NB && gr < n && gc < n) {
+          double* cp = C + gr + (size_t)ldc * gc;
+          *cp = (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*cp);
+        }
       }
     }
   }
   __syncthreads();
 }
 
-// Square GEMM dispatch: one exact-size tile for n <= 96 (FP64: double-
-// buffered), 64 x 64 tiles above.  smem must hold 4 * 16 * 96 doubles.
+// Square GEMM dispatch: one exact-size tile for n <= 96 (FP64: on the FP64
+// MMA, double-buffered), 64 x 64 tiles above.  smem must hold 4 * 16 * 100
+// doubles.
 // lowp = compute in FP32.
 template <int NT, typename TM>
 __device__ __forceinline__ void gemm_prec(int n, bool tA, const TM* A, int lda, bool tB, const TM* B, int ldb,
@@ -489,11 +514,11 @@ __device__ __forceinline__ void gemm_prec(int n, bool tA, const TM* A, int lda, 
     else if (n <= 96) gemm_tile<NT, 6, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
     else gemm_rect<NT, TM, float>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
   } else {
-    if (n <= 32) gemm_tile_db<NT, 2>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 48) gemm_tile_db<NT, 3>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 64) gemm_tile_db<NT, 4>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 80) gemm_tile_db<NT, 5>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 96) gemm_tile_db<NT, 6>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    if (n <= 32) gemm_tile_mma<NT, 2>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 48) gemm_tile_mma<NT, 3>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 64) gemm_tile_mma<NT, 4>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 80) gemm_tile_mma<NT, 5>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else if (n <= 96) gemm_tile_mma<NT, 6>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
     else gemm_rect<NT, TM, TM>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
   }
 }
