@@ -138,7 +138,17 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // 64 x 64 output tiles, K staged in chunks of GK.
 constexpr int GT = 64, GK = 16;
 // shared memory (elements) a gemm_rect call may use: two stages of A and B
-constexpr int GEMM_RECT_SMEM = 4 * GK * GT;
+constexpr int GTP = GT + 4;  // staged row stride (bank spread of the FP64 MMA fragment loads)
+constexpr int GEMM_RECT_SMEM = 4 * GK * GTP;
+
+// One FP64 tensor-core MMA, D = A B + D with A 8 x 4, B 4 x 8, D 8 x 8
+// (mma.sync m8n8k4 .f64; per lane one element of A and of B, two of D).
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
 
 // gemm_rect with double-buffered cp.async staging (storage type = compute
 // type): the (tile, K chunk) steps form one pipeline, chunk s+1 (of this or
@@ -149,7 +159,7 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
                                           int ldb, T* C, int ldc, double alpha, double beta, void* smem_v,
                                           bool lower, int diag_off)
 {
-  T* buf = (T*)smem_v;  // [2][As: GK*GT | Bs: GK*GT]
+  T* buf = (T*)smem_v;  // [2][As: GK*GTP | Bs: GK*GTP]
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT, ntile = tm * tn;
   const int nk = (K + GK - 1) / GK;
@@ -163,19 +173,19 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
   };
   auto issue = [&](int tile, int k0, int which) {
     const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
-    T* As = buf + which * 2 * GK * GT;
-    T* Bs = As + GK * GT;
+    T* As = buf + which * 2 * GK * GTP;
+    T* Bs = As + GK * GTP;
     for (int t = threadIdx.x; t < GK * GT; t += NT) {
       int r, k;
       if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
       const int gr = r0 + r, gk = k0 + k;
       const bool va = gr < M && gk < K;
-      cp_async_el<T>(&As[k * GT + r], va ? (tA ? A + gk + (size_t)lda * gr : A + gr + (size_t)lda * gk) : A, va);
+      cp_async_el<T>(&As[k * GTP + r], va ? (tA ? A + gk + (size_t)lda * gr : A + gr + (size_t)lda * gk) : A, va);
       int c;
       if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
       const int gc = c0 + c, gk2 = k0 + k;
       const bool vb = gc < N && gk2 < K;
-      cp_async_el<T>(&Bs[k * GT + c], vb ? (tB ? B + gc + (size_t)ldb * gk2 : B + gk2 + (size_t)ldb * gc) : B, vb);
+      cp_async_el<T>(&Bs[k * GTP + c], vb ? (tB ? B + gc + (size_t)ldb * gk2 : B + gk2 + (size_t)ldb * gc) : B, vb);
     }
     cp_async_commit();
   };
@@ -196,6 +206,58 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
   int which = 0;
   while (tile < ntile) {
     const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
+    if constexpr (std::is_same<T, double>::value) {
+      // FP64 MMA (m8n8k4): warps as 2 x 4 over the 8 x 8 blocks of the
+      // tile, warp (wr, wc) owning blocks (wr + 2 i, wc + 4 j), i < 4, j < 2;
+      // lane l holds A(l / 4, l % 4), B(l % 4, l / 4), C(l / 4, 2 (l % 4) + h)
+      const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wr = w & 1, wc = w >> 1;
+      const int q = lane & 3, p = lane >> 2;
+      double acc[4][2][2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+      for (int kc = 0; kc < nk; ++kc) {
+        cp_async_wait_all();
+        __syncthreads();  // this step's chunk is visible; the other buffer is free
+        if (it_tile < ntile) {
+          issue(it_tile, it_k * GK, which ^ 1);
+          advance();
+        }
+        const double* As = buf + which * 2 * GK * GTP;
+        const double* Bs = As + GK * GTP;
+        // rows k >= K of the last chunk are zero-filled: whole steps of 4
+        const int kmax = min(GK, K - kc * GK);
+        for (int kk = 0; kk < kmax; kk += 4) {
+          double a[4], b[2];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) a[i] = As[(kk + q) * GTP + (wr + 2 * i) * 8 + p];
+#pragma unroll
+          for (int j = 0; j < 2; ++j) b[j] = Bs[(kk + q) * GTP + (wc + 4 * j) * 8 + p];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+        which ^= 1;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int gr = r0 + (wr + 2 * i) * 8 + p;
+        if (gr >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int gc = c0 + (wc + 4 * j) * 8 + 2 * q + h;
+            if (gc >= N) continue;
+            if (lower && gr + diag_off < gc) continue;
+            double* cp = C + gr + (size_t)ldc * gc;
+            *cp = (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*cp);
+          }
+        }
+      }
+    } else {
     T acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -208,15 +270,15 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
         issue(it_tile, it_k * GK, which ^ 1);
         advance();
       }
-      const T* As = buf + which * 2 * GK * GT;
-      const T* Bs = As + GK * GT;
+      const T* As = buf + which * 2 * GK * GTP;
+      const T* Bs = As + GK * GTP;
       const int kmax = min(GK, K - kc * GK);
       for (int k = 0; k < kmax; ++k) {
         T a[4], b[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[k * GT + ty + 16 * i];
+        for (int i = 0; i < 4; ++i) a[i] = As[k * GTP + ty + 16 * i];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = Bs[k * GT + tx + 16 * j];
+        for (int j = 0; j < 4; ++j) b[j] = Bs[k * GTP + tx + 16 * j];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -236,6 +298,7 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
         T* cp = C + gr + (size_t)ldc * gc;
         *cp = (T)((beta == 0.0) ? alpha * (double)acc[i][j] : alpha * (double)acc[i][j] + beta * (double)(*cp));
       }
+    }
     }
     tile = next_live(tile + 1);
   }
@@ -416,12 +479,6 @@ __device__ __noinline__ void gemm_tile(int n, bool tA, const TM* A, int lda, boo
 // (R + 1) / 2 B fragments and issues R x (R + 1) / 2 MMAs.  Fragments
 // (PTX m8n8k4 .f64): lane l holds A(l / 4, l % 4), B(l % 4, l / 4) and
 // C(l / 4, 2 (l % 4) + {0, 1}).  smem: 4 * 16 * (T + 4) doubles.
-__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b)
-{
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
 
 template <int NT, int R>
 __device__ __noinline__ void gemm_tile_mma(int n, bool tA, const double* A, int lda, bool tB, const double* B,
