@@ -397,12 +397,14 @@ __global__ void __launch_bounds__(NT) k_gemm(int M, int N, int K, int tA, const 
 
 // FP64 GEMM, C = alpha op(A) op(B) + beta C, one 128 x 64 output tile per
 // 256-thread block (z = batch, strided; lower skips tiles above the diagonal
-// and entries with row < column).  Thread (tx, ty) of the 16 x 16 grid owns
-// rows 8 ty .. 8 ty + 7 and columns 4 tx .. 4 tx + 3, read from shared
-// memory as 16-byte pairs: 32 FMAs per 6 shared loads.  K is staged in
-// chunks of 32 by cp.async into two stages (rows padded to 130 / 66 doubles
-// so transposed stores spread over the banks; 100 KB, two blocks per SM).
-constexpr int DG_M = 128, DG_N = 64, DG_K = 32, DG_AS = DG_M + 2, DG_BS = DG_N + 2;
+// and entries with row < column), on the FP64 MMA (mma.sync m8n8k4): the 8
+// warps as 4 x 2 over the tile's 16 x 8 blocks of 8 x 8, warp (wr, wc)
+// owning blocks (wr + 4 i, wc + 2 j), i, j < 4: 16 MMAs per K step of 4 from
+// 8 fragment loads.  K is staged in chunks of 32 by cp.async into two
+// stages, [k][row] with strides of 132 / 68 doubles (= 4 mod 16, so each
+// half-warp's fragment loads fall on distinct banks); 100 KB, two blocks
+// per SM.
+constexpr int DG_M = 128, DG_N = 64, DG_K = 32, DG_AS = DG_M + 4, DG_BS = DG_N + 4;
 constexpr int DG_STAGE = DG_K * (DG_AS + DG_BS);
 constexpr size_t DG_SMEM = 2 * (size_t)DG_STAGE * sizeof(double);
 
@@ -418,7 +420,8 @@ __global__ void __launch_bounds__(256, 2) k_dgemm(int M, int N, int K, int tA, c
   A += sA * z;
   B += sB * z;
   C += sC * z;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, w = tid >> 5, wr = w & 3, wc = w >> 2, q = lane & 3, p = lane >> 2;
   auto issue = [&](int k0, int st) {
     double* As = dsm + st * DG_STAGE;
     double* Bs = As + DG_K * DG_AS;
@@ -438,11 +441,11 @@ __global__ void __launch_bounds__(256, 2) k_dgemm(int M, int N, int K, int tA, c
     }
     cta::cp_async_commit();
   };
-  double acc[8][4];
+  double acc[4][4][2];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int nch = (K + DG_K - 1) / DG_K;
   if (nch > 0) issue(0, 0);
   for (int ch = 0; ch < nch; ++ch) {
@@ -451,38 +454,34 @@ __global__ void __launch_bounds__(256, 2) k_dgemm(int M, int N, int K, int tA, c
     if (ch + 1 < nch) issue((ch + 1) * DG_K, (ch + 1) & 1);
     const double* As = dsm + (ch & 1) * DG_STAGE;
     const double* Bs = As + DG_K * DG_AS;
+    // rows k >= K of the last chunk are zero-filled: whole steps of 4
     const int kmax = min(DG_K, K - ch * DG_K);
-#pragma unroll 4
-    for (int k = 0; k < kmax; ++k) {
-      double a[8], b[4];
+#pragma unroll 2
+    for (int kk = 0; kk < kmax; kk += 4) {
+      double a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const double2 v = *reinterpret_cast<const double2*>(&As[k * DG_AS + 8 * ty + 2 * i]);
-        a[2 * i] = v.x;
-        a[2 * i + 1] = v.y;
-      }
+      for (int i = 0; i < 4; ++i) a[i] = As[(kk + q) * DG_AS + (wr + 4 * i) * 8 + p];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const double2 v = *reinterpret_cast<const double2*>(&Bs[k * DG_BS + 4 * tx + 2 * j]);
-        b[2 * j] = v.x;
-        b[2 * j + 1] = v.y;
-      }
+      for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + q) * DG_BS + (wc + 2 * j) * 8 + p];
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 4; ++j) cta::dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
   }
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int gr = r0 + 8 * ty + i;
+  for (int i = 0; i < 4; ++i) {
+    const int gr = r0 + (wr + 4 * i) * 8 + p;
     if (gr >= M) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int gc = c0 + 4 * tx + j;
-      if (gc >= N || (lower && gr < gc)) continue;
-      double* cp = C + gr + (size_t)ldc * gc;
-      *cp = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gc = c0 + (wc + 2 * j) * 8 + 2 * q + h;
+        if (gc >= N || (lower && gr < gc)) continue;
+        double* cp = C + gr + (size_t)ldc * gc;
+        *cp = (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*cp);
+      }
     }
   }
 }
