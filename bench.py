@@ -52,10 +52,10 @@ def peaks():
 
 # DRAM bytes (read + write) per instance of the solver launch, from one ncu
 # capture of a 592-instance launch at the bench's launch shape (2 blocks per
-# SM, warm start, FP64): 9.62 GB / 592.  The traffic is workspace eviction
+# SM, warm start, FP64): 9.89 GB / 592.  The traffic is workspace eviction
 # (per-block workspaces of the instances in flight exceed L2), so it grows
 # with the instances processed.
-TRAFFIC_BYTES_PER_INSTANCE = 9.62e9 / 592
+TRAFFIC_BYTES_PER_INSTANCE = 9.89e9 / 592
 
 
 def iter_flops(n: int, m: int) -> float:
