@@ -665,6 +665,10 @@ struct SolveGraph {
 struct DevState {
   int m = 0, nlp = 0, nDim = 0;
   std::vector<SolveGraph> solve_graphs;
+  // look-ahead of the grid Cholesky: the next diagonal block is factored on
+  // `side` (non-blocking) while the trailing update runs on the default stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_next = nullptr, ev_diag = nullptr;
   Params prm;
   std::vector<int> blockStruct, blockKind, blockIndex;  // kind 0 SDP, 2 LP; index = SDP idx or LP offset
   std::vector<SdpBlock> sdp;
@@ -717,6 +721,9 @@ struct DevState {
   ~DevState()
   {
     for (SolveGraph& g : solve_graphs) cudaGraphExecDestroy(g.exec);
+    if (ev_next) cudaEventDestroy(ev_next);
+    if (ev_diag) cudaEventDestroy(ev_diag);
+    if (side) cudaStreamDestroy(side);
     for (void* p : allocs) cudaFree(p);
   }
 };
@@ -765,32 +772,76 @@ static void gemm(DevState& S, int M, int N, int K, bool tA, const double* A, int
 // the matrix's own precision T (FP32 for the mixed-precision Schur factor).
 // Linv: NBG x NBG scratch, Tb: n x NBG scratch.  Returns 0 or the failing
 // column + 1.
+//
+// Look-ahead: the diagonal factor and inverse of block k+1 are single-block
+// kernels on a chain that does not shrink with n.  After panel k is formed,
+// only block column k+1 is updated first; block k+1 is then factored and
+// inverted on the side stream while the trailing update of the remaining
+// columns runs on the default stream (the side stream has the higher
+// priority, so its blocks are scheduled first).  Events order the two streams; the
+// shared Linv scratch is overwritten only after panel k's product has read
+// it.
 template <typename T>
 static int cholesky_grid_t(DevState& S, T* A, int n, bool adjust, T* Linv, T* Tb, T* dinv_store = nullptr)
 {
   cudaMemset(S.flag, 0, sizeof(int));
-  for (int kb = 0; kb < n; kb += NBG) {
+  if (!S.side) {
+    // highest priority: its single-block kernels go ahead of the trailing
+    // update's queued blocks instead of waiting for its last wave
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (cudaStreamCreateWithPriority(&S.side, cudaStreamNonBlocking, hi) != cudaSuccess) S.side = nullptr;
+    if (S.side && (cudaEventCreateWithFlags(&S.ev_next, cudaEventDisableTiming) != cudaSuccess ||
+                   cudaEventCreateWithFlags(&S.ev_diag, cudaEventDisableTiming) != cudaSuccess)) {
+      cudaGetLastError();
+      cudaStreamDestroy(S.side);
+      S.side = nullptr;
+    }
+  }
+  auto Li_of = [&](int kb) { return dinv_store ? dinv_store + (size_t)(kb / NBG) * NBG * NBG : Linv; };
+  // factor (and, if a panel or the stored inverses need it, invert) the
+  // diagonal block at kb on stream st
+  auto diag = [&](int kb, cudaStream_t st) {
     const int bs = std::min(NBG, n - kb);
     T* Ad = A + kb + (size_t)n * kb;
-    k_chol_diag<T><<<1, NT, chol_smem()>>>(bs, Ad, n, adjust ? 1 : 0, kb, S.flag);
+    k_chol_diag<T><<<1, NT, chol_smem(), st>>>(bs, Ad, n, adjust ? 1 : 0, kb, S.flag);
+    if (n - kb - bs > 0 || dinv_store) k_tri_inv<T><<<1, NT, chol_smem(), st>>>(bs, Ad, n, Li_of(kb), bs, S.flag);
+  };
+  diag(0, 0);
+  for (int kb = 0; kb < n; kb += NBG) {
+    const int bs = std::min(NBG, n - kb);
     const int rem = n - kb - bs;
-    if (rem <= 0 && !dinv_store) continue;
-    T* Li = dinv_store ? dinv_store + (size_t)(kb / NBG) * NBG * NBG : Linv;
-    k_tri_inv<T><<<1, NT, chol_smem()>>>(bs, Ad, n, Li, bs, S.flag);
-    if (rem <= 0) continue;
-    Linv = Li;
+    if (rem <= 0) break;
+    if (kb > 0 && S.side) cudaStreamWaitEvent(0, S.ev_diag, 0);  // diagonal block kb (side stream)
+    T* Li = Li_of(kb);
     T* P = A + (kb + bs) + (size_t)n * kb;
     // panel: P <- P L_bb^{-T}
-    gemm_t<T, T>(rem, bs, bs, false, P, n, true, Linv, bs, Tb, rem, 1.0, 0.0);
+    gemm_t<T, T>(rem, bs, bs, false, P, n, true, Li, bs, Tb, rem, 1.0, 0.0);
     k_copy2d_t<T><<<nblk((long long)rem * bs), 256>>>(rem, bs, Tb, rem, P, n);
-    // trailing: A22 -= P P^T (lower); FP32 with tensor cores in mixed mode
+    // block column kb+1 first, then its diagonal block on the side stream
+    const int nb2 = std::min(NBG, rem);
     T* A22 = A + (kb + bs) + (size_t)n * (kb + bs);
+    gemm_t<T, T>(rem, nb2, bs, false, P, n, true, P, n, A22, n, -1.0, 1.0, true);
+    if (S.side) {
+      cudaEventRecord(S.ev_next, 0);
+      cudaStreamWaitEvent(S.side, S.ev_next, 0);
+      diag(kb + bs, S.side);
+      cudaEventRecord(S.ev_diag, S.side);
+    } else {
+      diag(kb + bs, 0);
+    }
+    // trailing: the columns after block kb+1 (FP32 with tensor cores in mixed mode)
+    const int rest = rem - nb2;
+    if (rest <= 0) continue;
+    T* P2 = P + nb2;
+    T* A33 = A22 + nb2 + (size_t)n * nb2;
     bool done = false;
     if constexpr (std::is_same<T, float>::value) {
-      if (S.tc && S.tc_work) done = syrk_tf32x3(rem, bs, P, n, A22, n, S.tc_work, S.tc_err, 0) == 0;
+      if (S.tc && S.tc_work) done = syrk_tf32x3(rest, bs, P2, n, A33, n, S.tc_work, S.tc_err, 0) == 0;
     }
-    if (!done) gemm_t<T, T>(rem, rem, bs, false, P, n, true, P, n, A22, n, -1.0, 1.0, true);
+    if (!done) gemm_t<T, T>(rest, rest, bs, false, P2, n, true, P2, n, A33, n, -1.0, 1.0, true);
   }
+  if (S.side) cudaStreamWaitEvent(0, S.ev_diag, 0);  // the last diagonal block
   int f = 0;
   cudaMemcpy(&f, S.flag, sizeof(int), cudaMemcpyDeviceToHost);
   return f;
