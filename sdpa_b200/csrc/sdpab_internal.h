@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include <atomic>
+
 #include "sdpa_b200.h"
 
 namespace sdpab {
@@ -19,6 +21,21 @@ long long gemm_tf32x3_work_bytes(int M, int N, int K, int batch);
 int gemm_tf32x3(int M, int N, int K, int batch, const double* A, int lda, long long sA, const double* B, int ldb,
                 double* C, int ldc, long long sC, void* work, int* err, cudaStream_t st);
 int cuda_error(cudaError_t e, const char* where);
+
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current
+// device, once per device (the attribute is per device; `done` holds one bit
+// per device ordinal, devices 64 and up are set on every call).
+inline cudaError_t smem_attr_per_device(const void* kernel, int bytes, std::atomic<unsigned long long>& done)
+{
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = (dev >= 0 && dev < 64) ? 1ull << dev : 0ull;
+  if (bit && (done.load() & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && bit) done.fetch_or(bit);
+  return e;
+}
 
 // Device memory kept between solver calls on the current device: the
 // per-block workspace of the batched solver plus a small counter page.

@@ -743,11 +743,8 @@ static void gemm_t(int M, int N, int K, bool tA, const TM* A, int lda, bool tB, 
   // The 128 x 64 tile pays off on the long-K products of the Schur build;
   // the Cholesky's panel and trailing updates (K <= 128) stay on 64 x 64.
   if constexpr (std::is_same<TM, double>::value && std::is_same<TC, double>::value) if (K > 128) {
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
-      attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    smem_attr_per_device((const void*)k_dgemm, (int)DG_SMEM, attr);
     dim3 g((M + DG_M - 1) / DG_M, (N + DG_N - 1) / DG_N, batch);
     k_dgemm<<<g, 256, DG_SMEM>>>(M, N, K, tA, A, lda, sA, tB, B, ldb, sB, C, ldc, sC, alpha, beta, lower ? 1 : 0);
     return;
@@ -1480,11 +1477,8 @@ int Solver::solve(const InitPoint* init, const Params* prm)
                                                    S.tc_f1_work, S.tc_f1_err, 0) == 0;
         if (!tc_done)
           gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn, lowp);
-        static bool pack_attr = false;
-        if (!pack_attr) {
-          cudaFuncSetAttribute(k_f1_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F1_PACK_SMEM);
-          pack_attr = true;
-        }
+        static std::atomic<unsigned long long> pack_attr{0};
+        smem_attr_per_device((const void*)k_f1_pack, (int)F1_PACK_SMEM, pack_attr);
         const long long nt = (B.n + F1_PACK_T - 1) / F1_PACK_T;
         k_f1_pack<<<(unsigned)(nt * (nt + 1) / 2), 256, F1_PACK_SMEM>>>(B.n, cnt, G, T);
         k_f1_spmm<<<dim3((B.nc + 7) / 8, 4), 256>>>(B.nc, q0, cnt, B.f1, B.cons, B.ptr, B.pos, B.val, B.nnz, T,

@@ -401,13 +401,9 @@ int gemm_tf32x3(int M, int N, int K, int batch, const double* A, int lda, long l
                 double* C, int ldc, long long sC, void* work, int* err, cudaStream_t st)
 {
   if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return 0;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(tc::k_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         tc::SMEM_BYTES);
-    if (e != cudaSuccess) return (int)e;
-    attr_set = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = smem_attr_per_device((const void*)tc::k_gemm_tf32x3, tc::SMEM_BYTES, attr);
+  if (e != cudaSuccess) return (int)e;
   uint32_t* Sa = (uint32_t*)work;
   uint32_t* Sb = Sa + (size_t)batch * tc::split_words(M, K);
   const long long nk = (K + tc::KC - 1) / tc::KC;
@@ -426,13 +422,9 @@ int gemm_tf32x3(int M, int N, int K, int batch, const double* A, int lda, long l
 int syrk_tf32x3(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, int* err, cudaStream_t st)
 {
   if (M <= 0 || K <= 0) return 0;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(tc::k_syrk_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         tc::SMEM_BYTES);
-    if (e != cudaSuccess) return (int)e;
-    attr_set = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = smem_attr_per_device((const void*)tc::k_syrk_tf32x3, tc::SMEM_BYTES, attr);
+  if (e != cudaSuccess) return (int)e;
   const long long T = (M + tc::TILE - 1) / tc::TILE, nk = (K + tc::KC - 1) / tc::KC;
   const long long threads = T * tc::TILE * nk * (tc::KC / 4);
   tc::k_split_tf32<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(M, K, P, ldp, (uint32_t*)work);
