@@ -14,8 +14,9 @@ Fixtures (all from the reference's own output, never hand-written):
   mc100_trace.json     per-iteration (mu, objP, objD, alphaP, alphaD, beta)
                        of MaxCut G(100, 0.1) seed 1 at epsilonStar = 1e-7
   blocks.json / blocks.npz  (also alone with --blocks) batched multi-block
-                       instances blk0..blk31: objectives, iterations, phase,
-                       x; every block of X and Y for blk0..blk7
+                       instances blk0..blk31 and the dense-constraint
+                       single-block instances dns0..dns7: objectives,
+                       iterations, phase, x; X and Y for blk0..blk7, dns*
   large.json / large.npz  (--large) Lovasz theta G(200, 0.5) seed 1 and the
                        random m=2000 SDP seed 1: objectives, iterations, x
 """
@@ -216,17 +217,28 @@ def block_cases(count=32):
     return [(f"blk{s}", inst.batch_block_sdp(s)) for s in range(count)]
 
 
+def dense_cases(count=8):
+    """Single-block instances whose constraints have many entries (more than
+    2n NonZeroEffect), which the batched solver assembles by F1."""
+    out = []
+    for s in range(count):
+        n = 16 + 4 * s
+        out.append((f"dns{s}", inst.random_block_sdp(m=12 + 2 * s, blocks=[n], density=0.5, seed=500 + s,
+                                                      name=f"dense-constraint sdp n={n} seed {500 + s}")))
+    return out
+
+
 def block_fixtures(tmp):
     """blocks.json / blocks.npz: the reference's results (objectives,
     iterations, phase, x; every block of X and Y for blk0..blk7) on
     block_cases()."""
-    cases = block_cases()
+    cases = block_cases() + dense_cases()
     res = run_ref([c[1] for c in cases], tmp, procs=8)
     meta, arrays = {}, {}
     for (name, it), r in zip(cases, res):
         meta[name] = {k: r[k] for k in ("iterations", "phase", "primal_obj", "dual_obj")}
         arrays[name + ".xvec"] = r["xvec"]
-        if int(name[3:]) < 8:
+        if name.startswith("dns") or int(name[3:]) < 8:
             for l in range(len(it.blocks)):
                 arrays[name + f".X{l + 1}"] = r["X"][l]
                 arrays[name + f".Y{l + 1}"] = r["Y"][l]

@@ -210,3 +210,23 @@ def test_block_warm_start_uses_diagonal_blocks_only():
         assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
         assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL, nm
     assert int(np.sum(r.status == 0)) >= len(sel) // 2
+
+
+def test_batched_dense_constraints_single_block_match_reference():
+    """The general solver on one SDP block with dense constraints (F1 columns
+    with a full-order product, no block structure to exploit)."""
+    from sdpa_b200 import batch
+    meta, arr = blocks()
+    cases = MG.dense_cases()
+    P = batch.pack([it for _, it in cases])
+    r = batch.solve_host(P, want_mats=True)
+    for q, (nm, it) in enumerate(cases):
+        g = meta[nm]
+        assert r.status[q] == 0 and r.phase[q] == 7, (nm, r.status[q], r.phase[q])
+        assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
+        assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL, nm
+        assert np.max(np.abs(r.x_of(P, q) - arr[nm + ".xvec"])) < X_TOL, nm
+        assert abs(int(r.iterations[q]) - g["iterations"]) <= 1, nm
+        Y = r.block_of(r.Y, P, q, 0).ravel(order="F")
+        ref = arr[nm + ".Y1"]
+        assert np.max(np.abs(Y - ref)) < 1e-4 * max(1.0, np.max(np.abs(ref))), nm

@@ -79,3 +79,20 @@ def test_host_entry_rejects_malformed_structure(mutate):
         P.nblock = np.array([N.BATCH_MAX_BLOCKS + 1], np.int32)
     with pytest.raises(N.SolverError, match="nblock|order|add up"):
         batch.solve_host(P)
+
+
+def test_dense_constraint_instances_take_the_general_solver():
+    """Single-block instances whose constraints have more than 2n effective
+    entries carry a block structure, which selects the solver with F1
+    columns; the oracle matches the reference on two of them."""
+    from sdpa_b200 import batch
+    meta, arr = blocks()
+    cases = MG.dense_cases()
+    P = batch.pack([it for _, it in cases])
+    assert P.nblock is not None and all(P.blocks_of(q) == it.blocks for q, (_, it) in enumerate(cases))
+    for name, it in cases[:2]:
+        r = O.solve(O.parse_dats(it.to_dats()))
+        g = meta[name]
+        assert r.iterations == g["iterations"], name
+        assert rel(r.primal_obj, g["primal_obj"]) < 1e-8, name
+        assert np.max(np.abs(r.xvec - arr[name + ".xvec"])) < 1e-6, name
