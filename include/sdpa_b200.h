@@ -136,6 +136,14 @@ SDPAB_API int sdpab_sdpa_info(sdpab_sdpa* h, sdpab_sdpa_info_t* out);
  * sdpa_parts.h:48-86): out8 = rMat+gVec, bMat, Cholesky, solves, dX/dZ,
  * step length, update (inverses), residuals. */
 SDPAB_API int sdpab_sdpa_phase_times(sdpab_sdpa* h, double* out8);
+/* Schur factorisation of the last solve (no counterpart in the reference,
+ * whose choice between the dense and the MUMPS sparse factorisation is
+ * internal, Chordal::ordering_bMat, sdpa_chordal.cpp:365-524): *sparse = 1
+ * when the factorisation skipped the 128 x 128 tiles its symbolic pattern
+ * leaves zero; pairs[0] / pairs[1] = trailing tile pairs updated / of the
+ * dense factorisation.  SDPAB_SCHUR=dense or =sparse in the environment
+ * forces the mode. */
+SDPAB_API int sdpab_sdpa_schur_pattern(sdpab_sdpa* h, int* sparse, long long* pairs);
 /* getResultXVec (sdpa_call.cpp:668-671), copied into out[m] */
 SDPAB_API int sdpab_sdpa_get_xvec(sdpab_sdpa* h, double* out);
 /* getResultXMat (which = 0) / getResultYMat (which = 1) of block l

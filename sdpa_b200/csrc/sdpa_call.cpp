@@ -1084,6 +1084,15 @@ SDPAB_API int sdpab_sdpa_info(sdpab_sdpa* h, sdpab_sdpa_info_t* out)
   out->nblock = p->getBlockNumber();
   return SDPAB_OK;
 }
+SDPAB_API int sdpab_sdpa_schur_pattern(sdpab_sdpa* h, int* sparse, long long* pairs)
+{
+  if (!h || !sparse || !pairs) return sdpab::set_error(SDPAB_EINVAL, "null argument");
+  const sdpab::SolveStats& s = ((SDPA*)h)->impl_solver_stats();
+  *sparse = s.schur_sparse;
+  pairs[0] = s.schur_sparse_pairs;
+  pairs[1] = s.schur_dense_pairs;
+  return SDPAB_OK;
+}
 SDPAB_API int sdpab_sdpa_phase_times(sdpab_sdpa* h, double* out8)
 {
   if (!h || !out8) return sdpab::set_error(SDPAB_EINVAL, "null argument");

@@ -7,11 +7,13 @@
 // cta_linalg.cuh / eig.cuh, everything else as grid kernels.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
 #include <chrono>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "cta_linalg.cuh"
@@ -486,6 +488,22 @@ __global__ void __launch_bounds__(256, 2) k_dgemm(int M, int N, int K, int tA, c
   }
 }
 
+// Tile-sparse trailing update of the blocked Cholesky: one block per listed
+// 128 x 128 tile pair (i, j) of the lower triangle, A_ij -= P_i P_j^T with
+// P the scaled panel (columns kb .. kb + bs), lower-triangular on i == j.
+// Tiles the symbolic factorisation leaves zero are not touched: they stay
+// exactly zero, as in the dense factorisation.
+template <typename T>
+__global__ void __launch_bounds__(NT) k_syrk_pairs(const int* pairs, int n, int kb, int bs, T* A)
+{
+  extern __shared__ double smem[];
+  const int i = pairs[2 * blockIdx.x], j = pairs[2 * blockIdx.x + 1];
+  const int r0 = i * 128, c0 = j * 128;
+  const int M = min(128, n - r0), N = min(128, n - c0);
+  cta::gemm_rect<NT, T, T>(M, N, bs, false, A + r0 + (size_t)n * kb, n, true, A + c0 + (size_t)n * kb, n,
+                           A + r0 + (size_t)n * c0, n, -1.0, 1.0, smem, i == j, 0);
+}
+
 // Diagonal block of the blocked Cholesky: one block factors A[0:bs, 0:bs]
 // (leading dimension lda) with the chosen pivot rule; first failure (global
 // column + 1) is written to *flag if *flag is still 0.
@@ -669,6 +687,13 @@ struct DevState {
   // `side` (non-blocking) while the trailing update runs on the default stream
   cudaStream_t side = nullptr;
   cudaEvent_t ev_next = nullptr, ev_diag = nullptr;
+  // tile-sparse Schur factorisation: for panel k, the trailing 128 x 128
+  // tile pairs (i, j), i >= j >= k + 2, that the symbolic factorisation
+  // marks nonzero, at pairs[2 pair_off[k] ..]
+  bool sparse = false;
+  std::vector<long long> pair_off;
+  int* pairs = nullptr;
+  long long dense_pairs = 0, sparse_pairs = 0;
   Params prm;
   std::vector<int> blockStruct, blockKind, blockIndex;  // kind 0 SDP, 2 LP; index = SDP idx or LP offset
   std::vector<SdpBlock> sdp;
@@ -827,9 +852,18 @@ static int cholesky_grid_t(DevState& S, T* A, int n, bool adjust, T* Linv, T* Tb
     } else {
       diag(kb + bs, 0);
     }
-    // trailing: the columns after block kb+1 (FP32 with tensor cores in mixed mode)
+    // trailing: the columns after block kb+1 (FP32 with tensor cores in mixed
+    // mode; only the nonzero tile pairs when the Schur pattern is sparse)
     const int rest = rem - nb2;
     if (rest <= 0) continue;
+    if (S.sparse) {
+      const int k = kb / NBG;
+      const long long cnt = S.pair_off[k + 1] - S.pair_off[k];
+      if (cnt > 0)
+        k_syrk_pairs<T><<<(unsigned)cnt, NT, cta::GEMM_RECT_SMEM * sizeof(double)>>>(S.pairs + 2 * S.pair_off[k], n,
+                                                                                     kb, bs, A);
+      continue;
+    }
     T* P2 = P + nb2;
     T* A33 = A22 + nb2 + (size_t)n * nb2;
     bool done = false;
@@ -1128,12 +1162,14 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
       Tneed = std::max(Tneed, (size_t)2 * F1_CHUNK * B.n * B.n);
     }
   }
-  // LP data
+  // LP data (lp_by_t: the constraints of each LP coordinate, kept for the
+  // Schur pattern below)
+  std::vector<std::vector<std::pair<int, double>>> lp_by_t(nlp);
   {
     std::vector<long long> ptr(m + 1, 0);
     std::vector<int> idx;
     std::vector<double> val;
-    std::vector<std::vector<std::pair<int, double>>> byT(nlp);
+    std::vector<std::vector<std::pair<int, double>>>& byT = lp_by_t;
     for (int k = 0; k < m; ++k) {
       for (auto& pr : lpk[k]) {
         idx.push_back(pr.first);
@@ -1159,6 +1195,58 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
     double** lps[] = {&S.lpx, &S.lpz, &S.lpzi, &S.lplx, &S.lplz, &S.lpD, &S.lpR, &S.lpXDZ, &S.lpdx,
                       &S.lpdz, &S.lpW, &S.lpx0, &S.lpz0, &S.lptmp};
     for (double** pp : lps) *pp = S.alloc(nlp);
+  }
+  // Schur pattern at the tile level (Chordal::ordering_bMat decides between
+  // the dense and the MUMPS sparse factorisation from the aggregate pattern,
+  // sdpa_chordal.cpp:365-524): B_ij is nonzero only if constraints i and j
+  // share an SDP block or an LP coordinate.  Tiles (128 x 128) that hold
+  // such pairs, closed under the fill of a symbolic tile Cholesky, give the
+  // trailing tile pairs of every panel; the factorisation skips the rest
+  // when they are few enough.  SDPAB_SCHUR=dense or =sparse forces a mode.
+  {
+    const int nt = (m + NBG - 1) / NBG;
+    std::vector<std::vector<char>> P(nt, std::vector<char>(nt, 0));
+    auto mark = [&](const std::vector<int>& cons) {
+      std::vector<int> t;
+      for (int k : cons) t.push_back(k / NBG);
+      std::sort(t.begin(), t.end());
+      t.erase(std::unique(t.begin(), t.end()), t.end());
+      for (size_t a = 0; a < t.size(); ++a)
+        for (size_t b = 0; b <= a; ++b) P[t[a]][t[b]] = 1;
+    };
+    for (const SdpBlock& B : S.sdp) mark(B.hcons);
+    for (int t = 0; t < nlp; ++t) {
+      std::vector<int> c;
+      for (auto& pr : lp_by_t[t]) c.push_back(pr.first);
+      mark(c);
+    }
+    for (int i = 0; i < nt; ++i) P[i][i] = 1;
+    S.pair_off.assign(nt + 1, 0);
+    std::vector<int> hp;
+    S.dense_pairs = S.sparse_pairs = 0;
+    for (int k = 0; k < nt; ++k) {
+      std::vector<int> R;
+      for (int i = k + 1; i < nt; ++i)
+        if (P[i][k]) R.push_back(i);
+      for (size_t a = 0; a < R.size(); ++a)
+        for (size_t b = 0; b <= a; ++b) {
+          P[R[a]][R[b]] = 1;  // fill
+          if (R[b] >= k + 2) {
+            hp.push_back(R[a]);
+            hp.push_back(R[b]);
+          }
+        }
+      S.pair_off[k + 1] = (long long)hp.size() / 2;
+      const long long rest = std::max(0, nt - k - 2);
+      S.dense_pairs += rest * (rest + 1) / 2;
+    }
+    S.sparse_pairs = S.pair_off[nt];
+    const char* env = getenv("SDPAB_SCHUR");
+    const std::string mode = env ? env : "";
+    if (mode == "dense" || nt < 3) S.sparse = false;
+    else if (mode == "sparse") S.sparse = true;
+    else S.sparse = nt >= 4 && (double)S.sparse_pairs < 0.6 * (double)S.dense_pairs;
+    if (S.sparse) S.pairs = S.upload(hp);
   }
   S.b = S.upload(p.c);
   S.y = S.alloc(m);
@@ -1200,6 +1288,9 @@ int Solver::solve(const InitPoint* init, const Params* prm)
   const double lam = P.lambdaStar;
   auto t_start = std::chrono::steady_clock::now();
   stats_ = SolveStats();
+  stats_.schur_sparse = S.sparse ? 1 : 0;
+  stats_.schur_sparse_pairs = S.sparse_pairs;
+  stats_.schur_dense_pairs = S.dense_pairs;
   const int nsdp = (int)S.sdp.size();
   S.mixed = (precision_ == SDPAB_PREC_MIXED || precision_ == SDPAB_PREC_MIXED_SIMT) ? 1 : 0;
   // tensor-core trailing updates pay from a few panels on

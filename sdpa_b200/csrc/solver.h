@@ -48,6 +48,8 @@ struct SolveStats {
   int cholesky_failed = 0;
   int warm_start_rejected = 0;
   int tc_timeouts = 0;      // tensor-core Schur updates abandoned (FP64 factor used instead)
+  int schur_sparse = 0;     // 1: the Schur factorisation skipped the tile pairs its pattern leaves zero
+  long long schur_sparse_pairs = 0, schur_dense_pairs = 0;  // trailing tile pairs: pattern / dense
   std::vector<double> trace;  // per iteration: mu, thetaP, thetaD, objP, objD, alphaP, alphaD, beta
   double final_row[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // the same quantities at loop exit
   // device seconds per phase: rMat+gVec, bMat, Cholesky, solves, dX/dZ,

@@ -168,12 +168,13 @@ def random_sdp(m: int = 2000, n: int = 500, nlp: int = 50, density: float = 0.01
 
 
 def random_block_sdp(m: int, blocks: list, density: float = 0.1, lp_per_constraint: int = 1,
-                     seed: int = 1, name: str = "") -> Instance:
+                     seed: int = 1, name: str = "", touch: list | None = None) -> Instance:
     """Random strictly feasible SDP with the given signed block structure
     (positive = SDP block, negative = LP block), built like `random_sdp`:
     every A_i has floor(density * k(k+1)/2) (at least one) N(0,1) upper
     entries in each SDP block of order k it touches (each block with
-    probability 0.7, at least one block) plus `lp_per_constraint` LP
+    probability 0.7, at least one block; or the SDP blocks listed in
+    touch[i], indices into the SDP blocks) plus `lp_per_constraint` LP
     entries; b_i = Tr(A_i), C = sum_i y0_i A_i + I, file F0 = -C, c = b."""
     rng = np.random.default_rng(seed)
     sdp = [(l + 1, int(k)) for l, k in enumerate(blocks) if k > 0]
@@ -192,10 +193,13 @@ def random_block_sdp(m: int, blocks: list, density: float = 0.1, lp_per_constrai
         vs.append(v)
 
     for a in range(m):
-        touch = [t for t in range(len(sdp)) if rng.random() < 0.7] if sdp else []
-        if sdp and not touch:
-            touch = [int(rng.integers(len(sdp)))]
-        for t in touch:
+        if touch is not None:
+            tl = list(touch[a])
+        else:
+            tl = [t for t in range(len(sdp)) if rng.random() < 0.7] if sdp else []
+            if sdp and not tl:
+                tl = [int(rng.integers(len(sdp)))]
+        for t in tl:
             l, k = sdp[t]
             iu, ju = np.triu_indices(k)
             per = max(1, int(np.floor(density * iu.size)))
@@ -222,6 +226,21 @@ def random_block_sdp(m: int, blocks: list, density: float = 0.1, lp_per_constrai
     return Instance(m=m, blocks=[int(x) for x in blocks], c=b, k=np.concatenate(ks), l=np.concatenate(ls),
                     i=np.concatenate(is_), j=np.concatenate(js), v=np.concatenate(vs),
                     name=name or f"random block sdp {blocks} m={m} seed {seed}")
+
+
+def block_arrow_sdp(nblk: int = 24, n: int = 8, m_per: int = 24, n_couple: int = 8, density: float = 0.3,
+                    seed: int = 1) -> Instance:
+    """Many SDP blocks with a sparse Schur complement: m_per constraints touch
+    only block b (b = 0 .. nblk-1, in order), then n_couple constraints touch
+    two random blocks each, so the Schur matrix is block-diagonal with a
+    dense border (an arrowhead).  Built like `random_block_sdp` (strictly
+    feasible from X = Y = I), no LP block."""
+    rng = np.random.default_rng(seed)
+    touch = [[b] for b in range(nblk) for _ in range(m_per)]
+    for _ in range(n_couple):
+        touch.append([int(x) for x in rng.choice(nblk, size=2, replace=False)])
+    return random_block_sdp(len(touch), [n] * nblk, density, lp_per_constraint=0, seed=seed + 7, touch=touch,
+                            name=f"block arrow sdp {nblk}x{n} m={len(touch)} seed {seed}")
 
 
 def batch_block_sdp(seed: int) -> Instance:

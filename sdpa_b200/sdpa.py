@@ -127,6 +127,15 @@ class SDPA:
 
     PHASE_NAMES = ["rMat+gVec", "bMat", "Cholesky", "solve", "dXdZ", "StepLength", "update", "residuals"]
 
+    def schurPattern(self):
+        """(sparse, pairs updated, pairs of the dense factorisation) of the
+        last solve's Schur factorisation (tiles of 128 x 128)."""
+        sp = ctypes.c_int(0)
+        pr = np.zeros(2, np.int64)
+        N.check(self._lib.sdpab_sdpa_schur_pattern(self._h, ctypes.byref(sp), pr.ctypes.data_as(ctypes.c_void_p)),
+                "schurPattern")
+        return bool(sp.value), int(pr[0]), int(pr[1])
+
     def phaseTimes(self) -> dict:
         """Device seconds per solver phase (ComputeTime categories)."""
         out = np.zeros(8)

@@ -17,6 +17,9 @@ Fixtures (all from the reference's own output, never hand-written):
                        instances blk0..blk31 and the dense-constraint
                        single-block instances dns0..dns7: objectives,
                        iterations, phase, x; X and Y for blk0..blk7, dns*
+  arrow.json / arrow.npz  (also alone with --arrow) a many-block SDP with a
+                       sparse Schur matrix, from the numpy restatement
+                       (the reference's sparse path needs MUMPS)
   large.json / large.npz  (--large) Lovasz theta G(200, 0.5) seed 1 and the
                        random m=2000 SDP seed 1: objectives, iterations, x
 """
@@ -247,8 +250,27 @@ def block_fixtures(tmp):
     np.savez_compressed(os.path.join(HERE, "blocks.npz"), **arrays)
 
 
+def arrow_fixtures():
+    """arrow.json / arrow.npz: a many-block SDP whose Schur matrix is sparse
+    (block-diagonal with a dense border).  The reference takes its MUMPS
+    sparse-Schur path on it, which is not built here (MUMPS is absent and
+    stubbed), so these values come from the numpy restatement
+    (oracle/sdpa_oracle.py) of the reference's algorithm."""
+    from oracle import sdpa_oracle as O
+    it = inst.block_arrow_sdp()
+    r = O.solve(O.parse_dats(it.to_dats()))
+    meta = {"arrow": {"iterations": r.iterations, "phase": O.PHASE_NAMES[r.phase], "primal_obj": r.primal_obj,
+                      "dual_obj": r.dual_obj, "source": "numpy restatement (oracle/sdpa_oracle.py)"}}
+    with open(os.path.join(HERE, "arrow.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+    np.savez_compressed(os.path.join(HERE, "arrow.npz"), **{"arrow.xvec": r.xvec})
+
+
 def main():
     large = "--large" in sys.argv
+    if "--arrow" in sys.argv:
+        arrow_fixtures()
+        return
     if "--blocks" in sys.argv:
         with tempfile.TemporaryDirectory() as tmp:
             block_fixtures(tmp)
@@ -314,6 +336,7 @@ def main():
 
         cli_fixtures()
         block_fixtures(tmp)
+        arrow_fixtures()
 
         if large:
             big = [("lt200", inst.lovasz_theta(200, 0.5, 1)), ("rnd2000", inst.random_sdp(seed=1))]

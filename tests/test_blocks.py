@@ -96,3 +96,21 @@ def test_dense_constraint_instances_take_the_general_solver():
         assert r.iterations == g["iterations"], name
         assert rel(r.primal_obj, g["primal_obj"]) < 1e-8, name
         assert np.max(np.abs(r.xvec - arr[name + ".xvec"])) < 1e-6, name
+
+
+def test_block_arrow_family_and_its_fixture():
+    """The block-arrow family: separable constraints grouped by block, then
+    coupling constraints on two blocks each; its fixture comes from the
+    numpy restatement (the reference itself needs MUMPS for it)."""
+    import json
+    from sdpa_b200 import instances
+    it = instances.block_arrow_sdp()
+    assert it.m == 24 * 24 + 8 and it.blocks == [8] * 24
+    blk_of = {}
+    for k, l in zip(it.k, it.l):
+        if k > 0:
+            blk_of.setdefault(int(k), set()).add(int(l))
+    assert all(blk_of[k] == {(k - 1) // 24 + 1} for k in range(1, 24 * 24 + 1))
+    assert all(len(blk_of[k]) == 2 for k in range(24 * 24 + 1, it.m + 1))
+    meta = json.load(open(os.path.join(GOLDEN, "arrow.json")))["arrow"]
+    assert meta["phase"] == "pdOPT" and "restatement" in meta["source"]

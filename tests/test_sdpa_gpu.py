@@ -190,3 +190,41 @@ def test_mixed_precision_large(name):
         assert x_within_reference_accuracy(x, arr[name + ".xvec"], arr[name + ".tight"])
     else:  # no tight solution stored: the reference's x itself
         assert np.max(np.abs(x - arr[name + ".xvec"])) < X_TOL
+
+
+def test_sparse_schur_on_a_block_arrow_problem(monkeypatch):
+    """Many SDP blocks whose Schur matrix is block-diagonal with a dense
+    border: the reference takes its sparse (MUMPS) Schur path here; this
+    solver skips the 128 x 128 tiles of the factor its symbolic pattern
+    leaves zero.  The automatic choice is the sparse path, the result
+    matches the numpy restatement of the reference's algorithm, and the
+    dense factorisation (SDPAB_SCHUR=dense) gives the same iterates to
+    rounding."""
+    import json
+    from sdpa_b200 import instances
+    from sdpa_b200.sdpa import SDPA
+    meta = json.load(open(os.path.join(GOLDEN, "arrow.json")))["arrow"]
+    xref = np.load(os.path.join(GOLDEN, "arrow.npz"))["arrow.xvec"]
+    inst = instances.block_arrow_sdp()
+    res = {}
+    for mode in ("auto", "dense"):
+        if mode == "dense":
+            monkeypatch.setenv("SDPAB_SCHUR", "dense")
+        else:
+            monkeypatch.delenv("SDPAB_SCHUR", raising=False)
+        s = SDPA()
+        s.inputProblem(inst)
+        s.solve()
+        res[mode] = (s.getPhaseString(), s.getIteration(), s.getPrimalObj(), s.getDualObj(),
+                     s.getResultXVec().copy(), s.schurPattern())
+    phase, iters, pobj, dobj, x, (sparse, pairs, dense_pairs) = res["auto"]
+    assert sparse and pairs < 0.6 * dense_pairs, (pairs, dense_pairs)
+    assert phase == "pdOPT"
+    assert abs(iters - meta["iterations"]) <= 1
+    assert rel(pobj, meta["primal_obj"]) < OBJ_TOL
+    assert rel(dobj, meta["dual_obj"]) < OBJ_TOL
+    assert np.max(np.abs(x - xref)) < X_TOL
+    phase2, iters2, pobj2, dobj2, x2, (sparse2, _, _) = res["dense"]
+    assert not sparse2 and phase2 == "pdOPT" and iters2 == iters
+    assert rel(pobj2, pobj) < 1e-9 and rel(dobj2, dobj) < 1e-9
+    assert np.max(np.abs(x2 - x)) < 1e-7
