@@ -432,14 +432,16 @@ __global__ void __launch_bounds__(256, 2) k_dgemm(int M, int N, int K, int tA, c
       if (!tA) { r = t % DG_M; k = t / DG_M; } else { k = t % DG_K; r = t / DG_K; }
       const int gr = r0 + r, gk = k0 + k;
       const bool v = gr < M && gk < K;
-      cta::cp_async_el<double>(&As[k * DG_AS + r], v ? (tA ? A + gk + (size_t)lda * gr : A + gr + (size_t)lda * gk) : A, v);
+      cta::cp_async_el<double>(&As[k * DG_AS + r],
+                               v ? (tA ? A + gk + (size_t)lda * gr : A + gr + (size_t)lda * gk) : A, v);
     }
     for (int t = tid; t < DG_K * DG_N; t += 256) {
       int c, k;
       if (!tB) { k = t % DG_K; c = t / DG_K; } else { c = t % DG_N; k = t / DG_N; }
       const int gc = c0 + c, gk = k0 + k;
       const bool v = gc < N && gk < K;
-      cta::cp_async_el<double>(&Bs[k * DG_BS + c], v ? (tB ? B + gc + (size_t)ldb * gk : B + gk + (size_t)ldb * gc) : B, v);
+      cta::cp_async_el<double>(&Bs[k * DG_BS + c],
+                               v ? (tB ? B + gc + (size_t)ldb * gk : B + gk + (size_t)ldb * gc) : B, v);
     }
     cta::cp_async_commit();
   };
@@ -893,7 +895,8 @@ static void chol_solve_grid(int m, const T* L, const T* dinv, T* x, cudaStream_t
     const int kb = b * NBG, bs = std::min(NBG, m - kb), rem = m - kb - bs;
     k_trsv_diag<T><<<1, 512, 0, st>>>(bs, dinv + (size_t)b * NBG * NBG, x + kb, 0);
     if (rem > 0)
-      k_trsv_fwd_update<T><<<(rem + 31) / 32, 256, 0, st>>>(rem, bs, L + (kb + bs) + (size_t)m * kb, m, x + kb, x + kb + bs);
+      k_trsv_fwd_update<T><<<(rem + 31) / 32, 256, 0, st>>>(rem, bs, L + (kb + bs) + (size_t)m * kb, m, x + kb,
+                                                            x + kb + bs);
   }
   for (int b = nb - 1; b >= 0; --b) {
     const int kb = b * NBG, bs = std::min(NBG, m - kb);
@@ -1552,31 +1555,31 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     // leaves its tile unwritten, and the matrix is then built again with the
     // SIMT products.
     auto build_bmat = [&](bool use_tc) {
-    cudaMemset(S.B, 0, (size_t)m * m * sizeof(double));
-    for (SdpBlock& B : S.sdp) {
-      if (!B.nc) continue;
-      k_f3<<<nblk((long long)B.nc * B.nc), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val, B.nnz, B.form,
-                                                  B.X, B.Zi, B.n, S.B, m);
-      const int nf = (int)B.hf1.size();
-      for (int q0 = 0; q0 < nf; q0 += F1_CHUNK) {
-        const int cnt = std::min(F1_CHUNK, nf - q0);
-        const size_t nn = (size_t)B.n * B.n;
-        double* T = S.T;
-        double* G = S.T + (size_t)F1_CHUNK * nn;
-        k_f1_left<<<dim3(B.n, cnt), 256>>>(B.n, q0, B.f1, B.csc_cptr, B.csc_ptr, B.csc_row, B.csc_val, B.X, T);
-        const bool tc_done = use_tc && gemm_tf32x3(B.n, B.n, B.n, cnt, T, B.n, nn, B.Zi, B.n, G, B.n, nn,
-                                                   S.tc_f1_work, S.tc_f1_err, 0) == 0;
-        if (!tc_done)
-          gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn, lowp);
-        static std::atomic<unsigned long long> pack_attr{0};
-        smem_attr_per_device((const void*)k_f1_pack, (int)F1_PACK_SMEM, pack_attr);
-        const long long nt = (B.n + F1_PACK_T - 1) / F1_PACK_T;
-        k_f1_pack<<<(unsigned)(nt * (nt + 1) / 2), 256, F1_PACK_SMEM>>>(B.n, cnt, G, T);
-        k_f1_spmm<<<dim3((B.nc + 7) / 8, 4), 256>>>(B.nc, q0, cnt, B.f1, B.cons, B.ptr, B.pos, B.val, B.nnz, T,
-                                                    S.B, m);
+      cudaMemset(S.B, 0, (size_t)m * m * sizeof(double));
+      for (SdpBlock& B : S.sdp) {
+        if (!B.nc) continue;
+        k_f3<<<nblk((long long)B.nc * B.nc), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val, B.nnz, B.form,
+                                                    B.X, B.Zi, B.n, S.B, m);
+        const int nf = (int)B.hf1.size();
+        for (int q0 = 0; q0 < nf; q0 += F1_CHUNK) {
+          const int cnt = std::min(F1_CHUNK, nf - q0);
+          const size_t nn = (size_t)B.n * B.n;
+          double* T = S.T;
+          double* G = S.T + (size_t)F1_CHUNK * nn;
+          k_f1_left<<<dim3(B.n, cnt), 256>>>(B.n, q0, B.f1, B.csc_cptr, B.csc_ptr, B.csc_row, B.csc_val, B.X, T);
+          const bool tc_done = use_tc && gemm_tf32x3(B.n, B.n, B.n, cnt, T, B.n, nn, B.Zi, B.n, G, B.n, nn,
+                                                     S.tc_f1_work, S.tc_f1_err, 0) == 0;
+          if (!tc_done)
+            gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn, lowp);
+          static std::atomic<unsigned long long> pack_attr{0};
+          smem_attr_per_device((const void*)k_f1_pack, (int)F1_PACK_SMEM, pack_attr);
+          const long long nt = (B.n + F1_PACK_T - 1) / F1_PACK_T;
+          k_f1_pack<<<(unsigned)(nt * (nt + 1) / 2), 256, F1_PACK_SMEM>>>(B.n, cnt, G, T);
+          k_f1_spmm<<<dim3((B.nc + 7) / 8, 4), 256>>>(B.nc, q0, cnt, B.f1, B.cons, B.ptr, B.pos, B.val, B.nnz, T,
+                                                      S.B, m);
+        }
       }
-    }
-    if (nlp) k_lp_bmat<<<nlp, 256>>>(S.lpT_ptr, S.lpT_k, S.lpT_v, S.lpx, S.lpzi, S.B, m);
+      if (nlp) k_lp_bmat<<<nlp, 256>>>(S.lpT_ptr, S.lpT_k, S.lpT_v, S.lpx, S.lpzi, S.B, m);
     };
     const bool tc_f1 = lowp && S.tc_f1_work;
     if (tc_f1) cudaMemset(S.tc_f1_err, 0, sizeof(int));
