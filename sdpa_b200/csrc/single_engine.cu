@@ -644,6 +644,68 @@ __global__ void __launch_bounds__(NT) k_min_eig(int n, const double* M, double* 
   if (threadIdx.x == 0) *out = v;
 }
 
+// Many small SDP blocks: one 256-thread block per SDP block of order <= 96
+// runs the per-block steps with the block-level routines of the batched
+// engine, in one launch for all of them (instead of several launches and a
+// host read-back per block).
+constexpr int SMALL_BLOCK = 96;
+constexpr int SB_GSM = 4 * 16 * 100;  // GEMM staging: the double-buffered n <= 96 MMA tile
+
+struct BlockPtrs {
+  double *X, *Z, *Zi, *LXi, *LZi, *W1, *W2, *R, *XDZ, *dX, *dZ;
+  int n;
+};
+
+static size_t small_block_smem(int nmax)
+{
+  return (size_t)(SB_GSM + 2 * cta::SD_DOUBLES + eig_scratch_doubles(nmax, 2)) * sizeof(double);
+}
+
+// Solutions::update's inverses (sdpa_dataset.cpp:117-171) per block: the
+// Cholesky factors of X and Z in lockstep (LAPACK's pivot rule), their
+// inverses L_X^-1, L_Z^-1 and Z^-1 = L_Z^-T L_Z^-1; *flag = 1 if a factor fails.
+__global__ void __launch_bounds__(NT) k_blocks_inverse(const BlockPtrs* bp, int* flag)
+{
+  extern __shared__ double smem[];
+  __shared__ int s_flag2[2];
+  double* gsm = smem;
+  double* sD = gsm + SB_GSM;
+  double* sD2 = sD + cta::SD_DOUBLES;
+  const BlockPtrs b = bp[blockIdx.x];
+  const int n = b.n, nn = n * n;
+  for (int t = threadIdx.x; t < nn; t += NT) {
+    b.W1[t] = b.X[t];
+    b.W2[t] = b.Z[t];
+  }
+  __syncthreads();
+  if (cta::cholesky_pair<NT, double>(n, b.W1, b.W2, n, sD, sD2, gsm, s_flag2)) {
+    if (threadIdx.x == 0) atomicExch(flag, 1);
+    return;
+  }
+  cta::tri_inverse_pair<NT, double>(n, b.W1, b.W2, n, b.LXi, b.LZi, n, sD, sD2, gsm);
+  cta::gemm<NT>(n, true, b.LZi, n, false, b.LZi, n, b.Zi, n, 1.0, 0.0, gsm);
+}
+
+// Step length per block (Jal::getMinEigen, sdpa_jordan.cpp:58-109): the
+// minimum eigenvalues of L_X^-1 dX L_X^-T and L_Z^-1 dZ L_Z^-T, with the
+// two Lanczos processes in lockstep; out[2 b], out[2 b + 1].  R and XDZ are
+// scratch here (rebuilt by the next predictor).
+__global__ void __launch_bounds__(NT) k_blocks_step(const BlockPtrs* bp, int nmax, double* out)
+{
+  extern __shared__ double smem[];
+  __shared__ double redbuf[4 * (NT / 32)];
+  cta::Reducer RD{redbuf, 0};
+  EigScratch es;
+  eig_scratch_carve(es, smem + SB_GSM + 2 * cta::SD_DOUBLES, nmax, &RD, 2);
+  const BlockPtrs b = bp[blockIdx.x];
+  double mins[2];
+  min_eig_pair(b.n, b.LXi, b.dX, b.LZi, b.dZ, b.W1, b.W2, b.R, b.XDZ, smem, SB_GSM, es, mins, false);
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = mins[0];
+    out[2 * blockIdx.x + 1] = mins[1];
+  }
+}
+
 // ------------------------------------------------------------------ host side
 
 static inline int nblk(long long n, int t = 256) { return (int)((n + t - 1) / t); }
@@ -692,6 +754,12 @@ struct DevState {
   // tile-sparse Schur factorisation: for panel k, the trailing 128 x 128
   // tile pairs (i, j), i >= j >= k + 2, that the symbolic factorisation
   // marks nonzero, at pairs[2 pair_off[k] ..]
+  // SDP blocks of order <= SMALL_BLOCK, handled by k_blocks_* (device
+  // descriptors), the others one by one; per-block step-length minima
+  std::vector<int> small_idx, large_idx;
+  BlockPtrs* small_ptrs = nullptr;
+  int small_nmax = 0;
+  double* blk_mins = nullptr;
   bool sparse = false;
   std::vector<long long> pair_off;
   int* pairs = nullptr;
@@ -1267,6 +1335,33 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
   S.Tsize = Tneed;
   S.part = S.alloc(256);
   S.sc = S.alloc(64);
+  {
+    std::vector<BlockPtrs> hb;
+    S.small_idx.clear();
+    S.large_idx.clear();
+    for (int q = 0; q < nsdp; ++q) {
+      SdpBlock& B = S.sdp[q];
+      if (B.n <= SMALL_BLOCK) {
+        S.small_idx.push_back(q);
+        hb.push_back({B.X, B.Z, B.Zi, B.LXi, B.LZi, B.W1, B.W2, B.R, B.XDZ, B.dX, B.dZ, B.n});
+        S.small_nmax = std::max(S.small_nmax, B.n);
+      } else {
+        S.large_idx.push_back(q);
+      }
+    }
+    if (!hb.empty()) {
+      void* pp = nullptr;
+      if (cudaMalloc(&pp, hb.size() * sizeof(BlockPtrs)) != cudaSuccess)
+        return set_error(SDPAB_ECUDA, "device allocation failed (block descriptors)");
+      S.allocs.push_back(pp);
+      cudaMemcpy(pp, hb.data(), hb.size() * sizeof(BlockPtrs), cudaMemcpyHostToDevice);
+      S.small_ptrs = (BlockPtrs*)pp;
+      const int sm = (int)small_block_smem(S.small_nmax);
+      cudaFuncSetAttribute(k_blocks_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      cudaFuncSetAttribute(k_blocks_step, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    }
+    S.blk_mins = S.alloc(2 * (size_t)std::max(nsdp, 1));
+  }
   void* fp = nullptr;
   if (cudaMalloc(&fp, 256) != cudaSuccess) return set_error(SDPAB_ECUDA, "device allocation failed");
   S.allocs.push_back(fp);
@@ -1369,7 +1464,16 @@ int Solver::solve(const InitPoint* init, const Params* prm)
   // Solutions::computeInverse (sdpa_dataset.cpp:117-142); returns false on failure
   auto compute_inverse = [&]() -> bool {
     bool ok = true;
-    for (SdpBlock& B : S.sdp) {
+    if (!S.small_idx.empty()) {
+      cudaMemset(S.flag + 28, 0, sizeof(int));
+      k_blocks_inverse<<<(unsigned)S.small_idx.size(), NT, small_block_smem(S.small_nmax)>>>(S.small_ptrs,
+                                                                                          S.flag + 28);
+      int bad = 0;
+      cudaMemcpy(&bad, S.flag + 28, sizeof(int), cudaMemcpyDeviceToHost);
+      if (bad) return false;
+    }
+    for (int q : S.large_idx) {
+      SdpBlock& B = S.sdp[q];
       const long long nn = (long long)B.n * B.n;
       k_axpby<<<nblk(nn), 256>>>(nn, B.W1, 1.0, B.X, 0.0, nullptr);
       if (cholesky_grid(S, B.W1, B.n, false)) { ok = false; break; }
@@ -1709,18 +1813,28 @@ int Solver::solve(const InitPoint* init, const Params* prm)
 
     // ---- step length (StepLength::MehrotraCorrector)
     double minX = 1.0e50, minZ = 1.0e50;
-    for (SdpBlock& B : S.sdp) {
+    const int nsmall = (int)S.small_idx.size();
+    if (nsmall)
+      k_blocks_step<<<(unsigned)nsmall, NT, small_block_smem(S.small_nmax)>>>(S.small_ptrs, S.small_nmax,
+                                                                              S.blk_mins);
+    for (size_t u = 0; u < S.large_idx.size(); ++u) {
+      SdpBlock& B = S.sdp[S.large_idx[u]];
+      double* out = S.blk_mins + 2 * (nsmall + u);
       const size_t shm = (size_t)eig_scratch_doubles(B.n, 1) * sizeof(double);
       gemm(S, B.n, B.n, B.n, false, B.dX, B.n, true, B.LXi, B.n, B.W1, B.n, 1.0, 0.0);
       gemm(S, B.n, B.n, B.n, false, B.LXi, B.n, false, B.W1, B.n, B.W2, B.n, 1.0, 0.0);
-      k_min_eig<<<1, NT, shm>>>(B.n, B.W2, S.sc + 10);
+      k_min_eig<<<1, NT, shm>>>(B.n, B.W2, out);
       gemm(S, B.n, B.n, B.n, false, B.dZ, B.n, true, B.LZi, B.n, B.W1, B.n, 1.0, 0.0);
       gemm(S, B.n, B.n, B.n, false, B.LZi, B.n, false, B.W1, B.n, B.W2, B.n, 1.0, 0.0);
-      k_min_eig<<<1, NT, shm>>>(B.n, B.W2, S.sc + 11);
-      double mm[2];
-      cudaMemcpy(mm, S.sc + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost);
-      minX = std::min(minX, mm[0]);
-      minZ = std::min(minZ, mm[1]);
+      k_min_eig<<<1, NT, shm>>>(B.n, B.W2, out + 1);
+    }
+    if (nsdp) {
+      std::vector<double> mm(2 * (size_t)nsdp);
+      cudaMemcpy(mm.data(), S.blk_mins, mm.size() * sizeof(double), cudaMemcpyDeviceToHost);
+      for (int q = 0; q < nsdp; ++q) {
+        minX = std::min(minX, mm[2 * q]);
+        minZ = std::min(minZ, mm[2 * q + 1]);
+      }
     }
     if (nlp) {
       // LP part of Jal::getMinEigen (sdpa_jordan.cpp:99-105): dx_t / x_t
