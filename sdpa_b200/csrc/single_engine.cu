@@ -652,8 +652,13 @@ constexpr int SMALL_BLOCK = 96;
 constexpr int SB_GSM = 4 * 16 * 100;  // GEMM staging: the double-buffered n <= 96 MMA tile
 
 struct BlockPtrs {
-  double *X, *Z, *Zi, *LXi, *LZi, *W1, *W2, *R, *XDZ, *dX, *dZ;
-  int n;
+  double *X, *Z, *Zi, *LXi, *LZi, *W1, *W2, *R, *XDZ, *dX, *dZ, *D;
+  // the constraints touching the block: global index, entry ranges, entries
+  const int* cons;
+  const long long* ptr;
+  const int *row, *col;
+  const double* val;
+  int n, nc;
 };
 
 static size_t small_block_smem(int nmax)
@@ -684,6 +689,58 @@ __global__ void __launch_bounds__(NT) k_blocks_inverse(const BlockPtrs* bp, int*
   }
   cta::tri_inverse_pair<NT, double>(n, b.W1, b.W2, n, b.LXi, b.LZi, n, sD, sD2, gsm);
   cta::gemm<NT>(n, true, b.LZi, n, false, b.LZi, n, b.Zi, n, 1.0, 0.0, gsm);
+}
+
+// Newton direction per block (compute_DzMat / compute_DxMat,
+// sdpa_newton.cpp:2718-2752): dZ = D (dual infeasible) or 0, minus
+// sum_k dy_k A_k; dX = sym(R - X dZ Z^-1) (Lal::getSymmetrize); the products
+// in FP32 when lowp (mixed precision).
+__global__ void __launch_bounds__(NT) k_blocks_direction(const BlockPtrs* bp, const double* dy, int dinf, int lowp)
+{
+  extern __shared__ double smem[];
+  const BlockPtrs b = bp[blockIdx.x];
+  const int n = b.n, nn = n * n;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int t = threadIdx.x; t < nn; t += NT) b.dZ[t] = dinf ? b.D[t] : 0.0;
+  __syncthreads();
+  for (int k = wid; k < b.nc; k += NT / 32) {
+    const double sc = -dy[b.cons[k]];
+    for (long long e = b.ptr[k] + lane; e < b.ptr[k + 1]; e += 32) {
+      const int r = b.row[e], c = b.col[e];
+      const double v = sc * b.val[e];
+      atomicAdd(&b.dZ[r + (size_t)n * c], v);
+      if (r != c) atomicAdd(&b.dZ[c + (size_t)n * r], v);
+    }
+  }
+  __syncthreads();
+  cta::gemm_prec<NT, double>(n, false, b.X, n, false, b.dZ, n, b.W1, n, 1.0, 0.0, smem, lowp != 0);
+  cta::gemm_prec<NT, double>(n, false, b.W1, n, false, b.Zi, n, b.W2, n, 1.0, 0.0, smem, lowp != 0);
+  for (int t = threadIdx.x; t < nn; t += NT) {
+    const int i = t % n, j = t / n;
+    if (i < j) continue;
+    const double lo = b.R[i + (size_t)n * j] - b.W2[i + (size_t)n * j];
+    const double up = b.R[j + (size_t)n * i] - b.W2[j + (size_t)n * i];
+    const double v = 0.5 * (lo + up);
+    b.dX[i + (size_t)n * j] = v;
+    b.dX[j + (size_t)n * i] = v;
+  }
+}
+
+// Corrector right-hand side per block (Newton::Mehrotra(CORRECTOR),
+// sdpa_newton.cpp:2755-2809): R = (beta mu Z^-1 - X) - dX dZ Z^-1 and, when
+// the point is dual infeasible, W1 = R - X D Z^-1.
+__global__ void __launch_bounds__(NT) k_blocks_corrector(const BlockPtrs* bp, double bmu, int dinf, int lowp)
+{
+  extern __shared__ double smem[];
+  const BlockPtrs b = bp[blockIdx.x];
+  const int n = b.n, nn = n * n;
+  cta::gemm_prec<NT, double>(n, false, b.dX, n, false, b.dZ, n, b.W1, n, 1.0, 0.0, smem, lowp != 0);
+  cta::gemm_prec<NT, double>(n, false, b.W1, n, false, b.Zi, n, b.W2, n, 1.0, 0.0, smem, lowp != 0);
+  for (int t = threadIdx.x; t < nn; t += NT) {
+    const double r = (bmu * b.Zi[t] + -1.0 * b.X[t]) - b.W2[t];
+    b.R[t] = r;
+    if (dinf) b.W1[t] = 1.0 * r + -1.0 * b.XDZ[t];
+  }
 }
 
 // Step length per block (Jal::getMinEigen, sdpa_jordan.cpp:58-109): the
@@ -1343,7 +1400,13 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
       SdpBlock& B = S.sdp[q];
       if (B.n <= SMALL_BLOCK) {
         S.small_idx.push_back(q);
-        hb.push_back({B.X, B.Z, B.Zi, B.LXi, B.LZi, B.W1, B.W2, B.R, B.XDZ, B.dX, B.dZ, B.n});
+        BlockPtrs d{};
+        d.X = B.X; d.Z = B.Z; d.Zi = B.Zi; d.LXi = B.LXi; d.LZi = B.LZi; d.W1 = B.W1; d.W2 = B.W2;
+        d.R = B.R; d.XDZ = B.XDZ; d.dX = B.dX; d.dZ = B.dZ; d.D = B.D;
+        d.cons = B.cons; d.ptr = B.ptr; d.row = B.row; d.col = B.col; d.val = B.val;
+        d.n = B.n;
+        d.nc = B.nc;
+        hb.push_back(d);
         S.small_nmax = std::max(S.small_nmax, B.n);
       } else {
         S.large_idx.push_back(q);
@@ -1359,6 +1422,8 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
       const int sm = (int)small_block_smem(S.small_nmax);
       cudaFuncSetAttribute(k_blocks_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
       cudaFuncSetAttribute(k_blocks_step, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      cudaFuncSetAttribute(k_blocks_direction, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      cudaFuncSetAttribute(k_blocks_corrector, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     }
     S.blk_mins = S.alloc(2 * (size_t)std::max(nsdp, 1));
   }
@@ -1752,7 +1817,11 @@ int Solver::solve(const InitPoint* init, const Params* prm)
 
     // ---- dZ and dX (compute_DzMat / compute_DxMat)
     auto direction = [&]() {
-      for (SdpBlock& B : S.sdp) {
+      if (!S.small_idx.empty())
+        k_blocks_direction<<<(unsigned)S.small_idx.size(), NT, small_block_smem(S.small_nmax)>>>(
+            S.small_ptrs, S.dy, dinf ? 1 : 0, lowp ? 1 : 0);
+      for (int q : S.large_idx) {
+        SdpBlock& B = S.sdp[q];
         const long long nn = (long long)B.n * B.n;
         if (dinf) k_axpby<<<nblk(nn), 256>>>(nn, B.dZ, 1.0, B.D, 0.0, nullptr);
         else cudaMemset(B.dZ, 0, nn * sizeof(double));
@@ -1784,8 +1853,15 @@ int Solver::solve(const InitPoint* init, const Params* prm)
 
     // ---- corrector
     Wv.clear();
+    if (!S.small_idx.empty())
+      k_blocks_corrector<<<(unsigned)S.small_idx.size(), NT, small_block_smem(S.small_nmax)>>>(
+          S.small_ptrs, sc.beta * sc.mu, dinf ? 1 : 0, lowp ? 1 : 0);
     for (SdpBlock& B : S.sdp) {
       const long long nn = (long long)B.n * B.n;
+      if (B.n <= SMALL_BLOCK) {
+        Wv.push_back(dinf ? B.W1 : B.R);
+        continue;
+      }
       gemm(S, B.n, B.n, B.n, false, B.dX, B.n, false, B.dZ, B.n, B.W1, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
       gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.W2, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
       k_axpby_sub<<<nblk(nn), 256>>>(nn, B.R, sc.beta * sc.mu, B.Zi, -1.0, B.X, B.W2);
