@@ -75,24 +75,6 @@ __global__ void k_copy2d_t(int rows, int cols, const T* src, int lds, T* dst, in
   dst[i + (size_t)ldd * j] = src[i + (size_t)lds * j];
 }
 
-// Per-constraint inner products out[cons[q]] += sign * (A_q . W) over the
-// entries a block holds (Lal::getInnerProduct(Sparse, Dense),
-// sdpa_linear.cpp:318-460).  One warp per constraint.
-__global__ void k_sp_dot(int nc, const int* cons, const long long* ptr, const int* row, const int* col,
-                         const double* val, const double* W, int n, double sign, double* out)
-{
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= nc) return;
-  double s = 0.0;
-  for (long long e = ptr[warp] + lane; e < ptr[warp + 1]; e += 32) {
-    const int r = row[e], c = col[e];
-    const double v = val[e];
-    s += (r == c) ? v * W[r + (size_t)n * r] : v * (W[r + (size_t)n * c] + W[c + (size_t)n * r]);
-  }
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) atomicAdd(&out[cons[warp]], sign * s);
-}
-
 // W += scale * sum_q coef[cons[q]] A_q (InputData::multi_plusToA,
 // sdpa_dataset.cpp:427-433).  One warp per constraint, atomics for shared
 // positions.
@@ -114,13 +96,11 @@ __global__ void k_sp_scatter(int nc, const int* cons, const long long* ptr, cons
 // Schur complement by formula F3 for every pair whose dominant constraint
 // uses F3 (compute_bMat_dense_SDP3 + calF3_thread_2, sdpa_newton.cpp:2019-2125,
 // :1319-1403).  One thread per ordered (i, j) pair of the block's constraints.
-__global__ void k_f3(int nc, const int* cons, const long long* ptr, const int* row, const int* col,
-                     const double* val, const int* nnz, const int* formula, const double* X,
-                     const double* Zi, int n, double* B, int m)
+__device__ __forceinline__ void f3_pair(long long t, int nc, const int* cons, const long long* ptr, const int* row,
+                                        const int* col, const double* val, const int* nnz, const int* formula,
+                                        const double* X, const double* Zi, int n, double* B, int m)
 {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)nc * nc) return;
-  const int il = t % nc, jl = t / nc;
+  const int il = (int)(t % nc), jl = (int)(t / nc);
   if (formula[jl] != F3) return;
   const int gi = cons[il], gj = cons[jl];
   const int inz = nnz[il], jnz = nnz[jl];
@@ -148,6 +128,32 @@ __global__ void k_f3(int nc, const int* cons, const long long* ptr, const int* r
   }
   atomicAdd(&B[gi + (size_t)m * gj], ret);
   if (gi != gj) atomicAdd(&B[gj + (size_t)m * gi], ret);
+}
+
+// The F3 pairs of every SDP block in one launch: block b owns the flat pair
+// indices [off[b], off[b + 1]) (nc_b^2 of them), found by binary search.
+struct F3Desc {
+  const int* cons;
+  const long long* ptr;
+  const int *row, *col;
+  const double* val;
+  const int *nnz, *form;
+  const double *X, *Zi;
+  int nc, n;
+};
+
+__global__ void k_f3_all(const F3Desc* d, const long long* off, int nb, double* B, int m)
+{
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (off[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const F3Desc& q = d[lo];
+  f3_pair(t - off[lo], q.nc, q.cons, q.ptr, q.row, q.col, q.val, q.nnz, q.form, q.X, q.Zi, q.n, B, m);
 }
 
 // F1 step 1 (Lal::let(work1,'=',xMat,'*',Aj), sdpa_newton.cpp:1859-1863):
@@ -259,6 +265,80 @@ __global__ void __launch_bounds__(256) k_f1_spmm(int nc, int q0, int cnt, const 
   }
 }
 
+// F1/F2 columns of every SDP block of order <= SMALL_F1 in one launch (the
+// same products as k_f1_left + gemm + k_f1_pack + k_f1_spmm, which a block
+// of order 10 would otherwise pay four launches per chunk for).  One thread
+// block per (SDP block, F1 constraint j), found by binary search over off:
+// T = X A_j and G = T Z^-1 in shared memory, then one warp per constraint i
+// of the block that j dominates: B_ij += A_i . G (upper entries of A_i,
+// G(r, c) + G(c, r) off the diagonal).
+constexpr int SMALL_F1 = 64;
+
+struct F1Desc {
+  const int* f1;
+  const long long *cptr, *csc_ptr;
+  const int* csc_row;
+  const double* csc_val;
+  const int* cons;
+  const long long* ptr;
+  const int *row, *col;
+  const double* val;
+  const int* nnz;
+  const double *X, *Zi;
+  int nc, n;
+};
+
+__global__ void __launch_bounds__(256) k_f1_small(const F1Desc* d, const long long* off, int nb, double* B, int m)
+{
+  extern __shared__ double f1sm[];
+  const long long t = blockIdx.x;
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (off[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const F1Desc& q = d[lo];
+  const int n = q.n, nn = n * n;
+  const int jl = q.f1[t - off[lo]];
+  double* T = f1sm;
+  double* G = f1sm + nn;
+  const long long* cp = q.cptr + (size_t)jl * (n + 1);
+  const long long base = q.csc_ptr[jl];
+  for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+    const int i = idx % n, c = idx / n;
+    double s = 0.0;
+    for (long long e = base + cp[c]; e < base + cp[c + 1]; ++e) s += q.X[i + (size_t)n * q.csc_row[e]] * q.csc_val[e];
+    T[idx] = s;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+    const int i = idx % n, c = idx / n;
+    const double* zc = q.Zi + (size_t)n * c;
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += T[i + n * k] * __ldg(zc + k);
+    G[idx] = s;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gj = q.cons[jl], jnz = q.nnz[jl];
+  for (int il = warp; il < q.nc; il += blockDim.x >> 5) {
+    const int gi = q.cons[il], inz = q.nnz[il];
+    if (jnz < inz || (inz == jnz && gi < gj)) continue;
+    double acc = 0.0;
+    for (long long e = q.ptr[il] + lane; e < q.ptr[il + 1]; e += 32) {
+      const int r = q.row[e], c = q.col[e];
+      const double h = (r == c) ? G[r + n * c] : G[r + n * c] + G[c + n * r];
+      acc += q.val[e] * h;
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      atomicAdd(&B[gi + (size_t)m * gj], acc);
+      if (gi != gj) atomicAdd(&B[gj + (size_t)m * gi], acc);
+    }
+  }
+}
+
 // LP part of the Schur complement (compute_bMat_dense_LP,
 // sdpa_newton.cpp:2562-2602): B_ij += x_t z_t^-1 a_it a_jt for each LP
 // coordinate t and each pair of constraints touching it.  One block per t.
@@ -360,19 +440,134 @@ __global__ void k_dot_final(int np, const double* part, double* out, int mode, i
   else *out = r;
 }
 
-// trace of an n x n matrix into out (accumulate)
-__global__ void k_trace(int n, const double* A, double* out, double scale)
+// ---- all SDP blocks in one launch.  The n_q x n_q matrices of the blocks
+// form one flat range (block q at [eoff[q], eoff[q + 1])); which matrix of a
+// block is meant is a kind, looked up in tab[kind * nb + q].  A problem of
+// 200 blocks of order 10 would otherwise pay one or two launches per block
+// for every inner product, residual and update.
+enum { MB_X, MB_Z, MB_DX, MB_DZ, MB_C, MB_X0, MB_Z0, MB_D, MB_R, MB_W1, MB_W2, MB_ZI, MB_KINDS };
+
+// walks the part [c0, c1) of the flat range: f(q, local index, n_q, flat index)
+template <typename F>
+__device__ __forceinline__ void mb_walk(const long long* eoff, const int* nq, int nb, long long c0, long long c1,
+                                        F f)
 {
-  __shared__ double w[32];
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (eoff[mid] <= c0) lo = mid;
+    else hi = mid - 1;
+  }
+  for (int q = lo; q < nb && eoff[q] < c1; ++q) {
+    const long long b = max(c0, eoff[q]), e = min(c1, eoff[q + 1]);
+    for (long long t = b + threadIdx.x; t < e; t += blockDim.x) f(q, t - eoff[q], nq[q], t);
+  }
+}
+
+// Deterministic reduction over every block (mode 0: sum of a .* b, mode 1:
+// max |a|, mode 2: sum of the diagonals of a); block c of the grid takes the
+// c-th chunk and writes part[c] (combined by k_dot_final).
+__global__ void k_mb_reduce(const double* const* tab, int ka, int kb, const long long* eoff, const int* nq, int nb,
+                            long long chunk, double* part, int mode)
+{
+  const double* const* A = tab + (size_t)ka * nb;
+  const double* const* Bv = tab + (size_t)kb * nb;
+  const long long c0 = blockIdx.x * chunk, c1 = min(eoff[nb], c0 + chunk);
   double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += A[i + (size_t)n * i];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  mb_walk(eoff, nq, nb, c0, c1, [&](int q, long long l, int n, long long) {
+    const double a = A[q][l];
+    if (mode == 0) s += a * Bv[q][l];
+    else if (mode == 1) s = fmax(s, fabs(a));
+    else if (l % (n + 1) == 0) s += a;
+  });
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v = __shfl_xor_sync(0xffffffffu, s, o);
+    s = (mode == 1) ? fmax(s, v) : s + v;
+  }
+  __shared__ double w[32];
   if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
     double r = 0.0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) r += w[q];
-    *out += scale * r;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) r = (mode == 1) ? fmax(r, w[q]) : r + w[q];
+    part[blockIdx.x] = r;
+  }
+}
+
+// out = a x + b y over every block (ky < 0: out = a x)
+__global__ void k_mb_axpby(double* const* tab, int ko, double a, int kx, double b, int ky, const long long* eoff,
+                           const int* nq, int nb, long long chunk)
+{
+  double* const* O = tab + (size_t)ko * nb;
+  double* const* Xv = tab + (size_t)kx * nb;
+  double* const* Yv = ky >= 0 ? tab + (size_t)ky * nb : nullptr;
+  const long long c0 = blockIdx.x * chunk, c1 = min(eoff[nb], c0 + chunk);
+  mb_walk(eoff, nq, nb, c0, c1, [&](int q, long long l, int, long long) {
+    O[q][l] = a * Xv[q][l] + (Yv ? b * Yv[q][l] : 0.0);
+  });
+}
+
+// The constraint entries of every block: block q's constraints are warps
+// [coff[q], coff[q + 1]).
+struct MbSparse {
+  const int* cons;
+  const long long* ptr;
+  const int *row, *col;
+  const double* val;
+  int n, q;
+};
+
+__device__ __forceinline__ int mb_find(const long long* off, int nb, long long t)
+{
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (off[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Per-constraint inner products out[cons] += sign * (A_k . W) over the
+// entries each block holds (Lal::getInnerProduct(Sparse, Dense),
+// sdpa_linear.cpp:318-460), W = tab[kw]; one warp per (block, constraint).
+__global__ void k_mb_sp_dot(const MbSparse* d, const long long* coff, int ns, const double* const* tab, int kw,
+                            int nb, double sign, double* out)
+{
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= coff[ns]) return;
+  const MbSparse& B = d[mb_find(coff, ns, warp)];
+  const int k = (int)(warp - coff[&B - d]);
+  const double* W = tab[(size_t)kw * nb + B.q];
+  const int n = B.n;
+  double s = 0.0;
+  for (long long e = B.ptr[k] + lane; e < B.ptr[k + 1]; e += 32) {
+    const int r = B.row[e], c = B.col[e];
+    const double v = B.val[e];
+    s += (r == c) ? v * W[r + (size_t)n * r] : v * (W[r + (size_t)n * c] + W[c + (size_t)n * r]);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) atomicAdd(&out[B.cons[k]], sign * s);
+}
+
+// k_sp_scatter over every block: W += scale * sum_k coef[cons] A_k, W = tab[kw]
+__global__ void k_mb_sp_scatter(const MbSparse* d, const long long* coff, int ns, double* const* tab, int kw, int nb,
+                                const double* coef, double scale)
+{
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= coff[ns]) return;
+  const MbSparse& B = d[mb_find(coff, ns, warp)];
+  const int k = (int)(warp - coff[&B - d]);
+  double* W = tab[(size_t)kw * nb + B.q];
+  const int n = B.n;
+  const double s = scale * (coef ? coef[B.cons[k]] : 1.0);
+  for (long long e = B.ptr[k] + lane; e < B.ptr[k + 1]; e += 32) {
+    const int r = B.row[e], c = B.col[e];
+    const double v = s * B.val[e];
+    atomicAdd(&W[r + (size_t)n * c], v);
+    if (r != c) atomicAdd(&W[c + (size_t)n * r], v);
   }
 }
 
@@ -817,6 +1012,26 @@ struct DevState {
   BlockPtrs* small_ptrs = nullptr;
   int small_nmax = 0;
   double* blk_mins = nullptr;
+  // F3 assembly of all blocks in one launch (k_f3_all)
+  F3Desc* f3_desc = nullptr;
+  long long* f3_off = nullptr;
+  long long f3_total = 0;
+  int f3_nb = 0;
+  // F1 columns of the blocks of order <= SMALL_F1 in one launch (k_f1_small)
+  F1Desc* f1_desc = nullptr;
+  long long* f1_off = nullptr;
+  long long f1_total = 0;
+  int f1_nb = 0, f1_nmax = 0;
+  // every SDP block as one flat range (k_mb_*): matrix table
+  // [kind * nsdp + q], offsets and orders, constraint descriptors
+  double** mb_tab = nullptr;
+  long long* mb_eoff = nullptr;
+  int* mb_nq = nullptr;
+  long long mb_total = 0;
+  MbSparse* mb_sp = nullptr;
+  long long* mb_coff = nullptr;
+  long long mb_ctotal = 0;
+  int mb_ns = 0;
   bool sparse = false;
   std::vector<long long> pair_off;
   int* pairs = nullptr;
@@ -1426,6 +1641,73 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
       cudaFuncSetAttribute(k_blocks_corrector, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     }
     S.blk_mins = S.alloc(2 * (size_t)std::max(nsdp, 1));
+    std::vector<F3Desc> fd;
+    std::vector<long long> fo(1, 0);
+    for (SdpBlock& B : S.sdp) {
+      if (!B.nc) continue;
+      fd.push_back({B.cons, B.ptr, B.row, B.col, B.val, B.nnz, B.form, B.X, B.Zi, B.nc, B.n});
+      fo.push_back(fo.back() + (long long)B.nc * B.nc);
+    }
+    S.f3_total = fo.back();
+    S.f3_nb = (int)fd.size();
+    if (!fd.empty()) {
+      void* pp = nullptr;
+      if (cudaMalloc(&pp, fd.size() * sizeof(F3Desc)) != cudaSuccess)
+        return set_error(SDPAB_ECUDA, "device allocation failed (F3 descriptors)");
+      S.allocs.push_back(pp);
+      cudaMemcpy(pp, fd.data(), fd.size() * sizeof(F3Desc), cudaMemcpyHostToDevice);
+      S.f3_desc = (F3Desc*)pp;
+      S.f3_off = S.upload(fo);
+    }
+    std::vector<F1Desc> f1d;
+    std::vector<long long> f1o(1, 0);
+    for (SdpBlock& B : S.sdp) {
+      if (!B.nc || B.hf1.empty() || B.n > SMALL_F1) continue;
+      f1d.push_back({B.f1, B.csc_cptr, B.csc_ptr, B.csc_row, B.csc_val, B.cons, B.ptr, B.row, B.col, B.val, B.nnz,
+                     B.X, B.Zi, B.nc, B.n});
+      f1o.push_back(f1o.back() + (long long)B.hf1.size());
+      S.f1_nmax = std::max(S.f1_nmax, B.n);
+    }
+    S.f1_total = f1o.back();
+    S.f1_nb = (int)f1d.size();
+    if (!f1d.empty()) {
+      void* pp = nullptr;
+      if (cudaMalloc(&pp, f1d.size() * sizeof(F1Desc)) != cudaSuccess)
+        return set_error(SDPAB_ECUDA, "device allocation failed (F1 descriptors)");
+      S.allocs.push_back(pp);
+      cudaMemcpy(pp, f1d.data(), f1d.size() * sizeof(F1Desc), cudaMemcpyHostToDevice);
+      S.f1_desc = (F1Desc*)pp;
+      S.f1_off = S.upload(f1o);
+      cudaFuncSetAttribute(k_f1_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(2 * (size_t)S.f1_nmax * S.f1_nmax * sizeof(double)));
+    }
+    if (nsdp) {
+      std::vector<double*> tab((size_t)MB_KINDS * nsdp);
+      std::vector<long long> eoff(1, 0), coff(1, 0);
+      std::vector<int> nq;
+      std::vector<MbSparse> sp;
+      for (int q = 0; q < nsdp; ++q) {
+        SdpBlock& B = S.sdp[q];
+        double* k[MB_KINDS] = {B.X, B.Z, B.dX, B.dZ, B.C, B.X0, B.Z0, B.D, B.R, B.W1, B.W2, B.Zi};
+        for (int u = 0; u < MB_KINDS; ++u) tab[(size_t)u * nsdp + q] = k[u];
+        eoff.push_back(eoff.back() + (long long)B.n * B.n);
+        nq.push_back(B.n);
+        if (B.nc) {
+          sp.push_back({B.cons, B.ptr, B.row, B.col, B.val, B.n, q});
+          coff.push_back(coff.back() + B.nc);
+        }
+      }
+      S.mb_tab = S.upload(tab);
+      S.mb_eoff = S.upload(eoff);
+      S.mb_nq = S.upload(nq);
+      S.mb_total = eoff.back();
+      S.mb_sp = S.upload(sp);
+      S.mb_coff = S.upload(coff);
+      S.mb_ctotal = coff.back();
+      S.mb_ns = (int)sp.size();
+      if (!S.mb_tab || !S.mb_eoff || !S.mb_nq || !S.mb_sp || !S.mb_coff)
+        return set_error(SDPAB_ECUDA, "device allocation failed (block tables)");
+    }
   }
   void* fp = nullptr;
   if (cudaMalloc(&fp, 256) != cudaSuccess) return set_error(SDPAB_ECUDA, "device allocation failed");
@@ -1600,32 +1882,40 @@ int Solver::solve(const InitPoint* init, const Params* prm)
   }
 
   // ------------------------------------------------ helpers
-  // out[k] = base[k] + sign * sum_blocks A_k . W   (W per block; LP vector wl)
-  auto a_dot = [&](double* out, const double* base, double sign, std::vector<const double*> W,
-                   const double* wl) {
+  // reductions and element-wise updates over every SDP block at once
+  // (k_mb_*; kinds MB_*): sc[slot] (+)= scale * reduction, mode as k_mb_reduce
+  auto mb_reduce = [&](int ka, int kb, int mode, int slot, bool acc, double scale) {
+    const int g = (int)std::min<long long>(256, std::max<long long>(1, (S.mb_total + 2047) / 2048));
+    const long long chunk = (S.mb_total + g - 1) / g;
+    k_mb_reduce<<<g, 256>>>(S.mb_tab, ka, kb, S.mb_eoff, S.mb_nq, nsdp, chunk, S.part, mode);
+    k_dot_final<<<1, 32>>>(g, S.part, S.sc + slot, mode == 1 ? 1 : 0, acc ? 1 : 0, scale);
+  };
+  auto mb_axpby = [&](int ko, double a, int kx, double b, int ky) {
+    const long long chunk = 2048;
+    k_mb_axpby<<<(unsigned)((S.mb_total + chunk - 1) / chunk), 256>>>(S.mb_tab, ko, a, kx, b, ky, S.mb_eoff,
+                                                                        S.mb_nq, nsdp, chunk);
+  };
+  // out[k] = base[k] + sign * sum_blocks A_k . W   (W = matrix kind kw of
+  // each block; LP vector wl)
+  auto a_dot = [&](double* out, const double* base, double sign, int kw, const double* wl) {
     if (base) cudaMemcpy(out, base, m * sizeof(double), cudaMemcpyDeviceToDevice);
     else cudaMemset(out, 0, m * sizeof(double));
-    for (int q = 0; q < nsdp; ++q) {
-      SdpBlock& B = S.sdp[q];
-      if (B.nc) k_sp_dot<<<nblk((long long)B.nc * 32), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val,
-                                                              W[q], B.n, sign, out);
-    }
+    if (S.mb_ctotal)
+      k_mb_sp_dot<<<nblk(S.mb_ctotal * 32), 256>>>(S.mb_sp, S.mb_coff, S.mb_ns, S.mb_tab, kw, nsdp, sign, out);
     if (nlp) k_lp_dot<<<nblk(m), 256>>>(m, S.lp_ptr, S.lp_idx, S.lp_val, wl, sign, out);
   };
   // residuals (Residuals::compute, sdpa_dataset.cpp:585-608): rp = b - A.X,
   // D = C - Z - sum y_k A_k; sc[0] = |rp|max, sc[1] = |D|max
   auto residuals = [&]() {
-    std::vector<const double*> Xs;
-    for (auto& B : S.sdp) Xs.push_back(B.X);
-    a_dot(S.rp, S.b, -1.0, Xs, S.lpx);
+    a_dot(S.rp, S.b, -1.0, MB_X, S.lpx);
     dot(S, m, S.rp, nullptr, 0, false, 1);
     bool first = true;
-    for (SdpBlock& B : S.sdp) {
-      const long long nn = (long long)B.n * B.n;
-      k_axpby<<<nblk(nn), 256>>>(nn, B.D, 1.0, B.C, -1.0, B.Z);
-      if (B.nc) k_sp_scatter<<<nblk((long long)B.nc * 32), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val,
-                                                                  S.y, -1.0, B.D, B.n);
-      dot(S, nn, B.D, nullptr, 1, !first, 1);
+    if (nsdp) {
+      mb_axpby(MB_D, 1.0, MB_C, -1.0, MB_Z);
+      if (S.mb_ctotal)
+        k_mb_sp_scatter<<<nblk(S.mb_ctotal * 32), 256>>>(S.mb_sp, S.mb_coff, S.mb_ns, S.mb_tab, MB_D, nsdp, S.y,
+                                                         -1.0);
+      mb_reduce(MB_D, MB_D, 1, 1, false, 1.0);
       first = false;
     }
     if (nlp) {
@@ -1637,36 +1927,20 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     if (first) cudaMemset(S.sc + 1, 0, sizeof(double));
   };
   // sum over blocks of <A, B> (full Frobenius) + LP into sc[slot]
-  auto ip = [&](int slot, std::vector<const double*> A, std::vector<const double*> Bm, const double* al,
-                const double* bl) {
+  auto ip = [&](int slot, int ka, int kb, const double* al, const double* bl) {
     bool acc = false;
-    for (int q = 0; q < nsdp; ++q) {
-      dot(S, (long long)S.sdp[q].n * S.sdp[q].n, A[q], Bm[q], slot, acc);
+    if (nsdp) {
+      mb_reduce(ka, kb, 0, slot, false, 1.0);
       acc = true;
     }
     if (nlp) { dot(S, nlp, al, bl, slot, acc); acc = true; }
     if (!acc) cudaMemset(S.sc + slot, 0, sizeof(double));
   };
-  auto mats = [&](int which) {
-    std::vector<const double*> v;
-    for (auto& B : S.sdp) {
-      switch (which) {
-        case 0: v.push_back(B.X); break;
-        case 1: v.push_back(B.Z); break;
-        case 2: v.push_back(B.dX); break;
-        case 3: v.push_back(B.dZ); break;
-        case 4: v.push_back(B.C); break;
-        case 5: v.push_back(B.X0); break;
-        case 6: v.push_back(B.Z0); break;
-      }
-    }
-    return v;
-  };
 
   residuals();
-  ip(2, mats(4), mats(0), S.lpC, S.lpx);  // objP = C.X
+  ip(2, MB_C, MB_X, S.lpC, S.lpx);  // objP = C.X
   dot(S, m, S.b, S.y, 3, false);          // objD = b.y
-  if (warm) ip(4, mats(0), mats(1), S.lpx, S.lpz);  // X.Z
+  if (warm) ip(4, MB_X, MB_Z, S.lpx, S.lpz);  // X.Z
   double h[16];
   read_scalars(S, h, 5);
   Scalars sc;
@@ -1694,17 +1968,13 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     const bool dinf = dual_infeasible(sc);
     const bool lowp = S.mixed && mixed_gap(sc) >= S.mu_switch;
     // ---- predictor rMat / gVec (Newton::compute_rMat, Make_gVec)
-    std::vector<const double*> Wv;
-    for (SdpBlock& B : S.sdp) {
-      const long long nn = (long long)B.n * B.n;
-      k_axpby<<<nblk(nn), 256>>>(nn, B.R, sc.beta * sc.mu, B.Zi, -1.0, B.X);
-      if (dinf) {
+    if (nsdp) mb_axpby(MB_R, sc.beta * sc.mu, MB_ZI, -1.0, MB_X);
+    if (dinf) {
+      for (SdpBlock& B : S.sdp) {
+        const long long nn = (long long)B.n * B.n;
         gemm(S, B.n, B.n, B.n, false, B.X, B.n, false, B.D, B.n, B.W1, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
         gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.XDZ, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
         k_axpby<<<nblk(nn), 256>>>(nn, B.W2, 1.0, B.R, -1.0, B.XDZ);
-        Wv.push_back(B.W2);
-      } else {
-        Wv.push_back(B.R);
       }
     }
     const double* Wl = S.lpR;
@@ -1716,7 +1986,7 @@ int Solver::solve(const InitPoint* init, const Params* prm)
         Wl = S.lpW;
       }
     }
-    a_dot(S.g, S.rp, -1.0, Wv, Wl);
+    a_dot(S.g, S.rp, -1.0, dinf ? MB_W2 : MB_R, Wl);
     mark(T_BMAT);
     // ---- Schur complement (Newton::Make_bMat).  In the FP32 phase of the
     // mixed mode the F1 products (X A_j) Z^-1 run on the tensor cores in
@@ -1725,10 +1995,13 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     // SIMT products.
     auto build_bmat = [&](bool use_tc) {
       cudaMemset(S.B, 0, (size_t)m * m * sizeof(double));
+      if (S.f3_total > 0)
+        k_f3_all<<<(unsigned)nblk(S.f3_total), 256>>>(S.f3_desc, S.f3_off, S.f3_nb, S.B, m);
+      if (S.f1_total > 0)
+        k_f1_small<<<(unsigned)S.f1_total, 256, 2 * (size_t)S.f1_nmax * S.f1_nmax * sizeof(double)>>>(
+            S.f1_desc, S.f1_off, S.f1_nb, S.B, m);
       for (SdpBlock& B : S.sdp) {
-        if (!B.nc) continue;
-        k_f3<<<nblk((long long)B.nc * B.nc), 256>>>(B.nc, B.cons, B.ptr, B.row, B.col, B.val, B.nnz, B.form,
-                                                    B.X, B.Zi, B.n, S.B, m);
+        if (!B.nc || B.n <= SMALL_F1) continue;
         const int nf = (int)B.hf1.size();
         for (int q0 = 0; q0 < nf; q0 += F1_CHUNK) {
           const int cnt = std::min(F1_CHUNK, nf - q0);
@@ -1840,11 +2113,11 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     };
     direction();
     auto step_products = [&]() {
-      ip(5, mats(4), mats(2), S.lpC, S.lpdx);   // C.dX
+      ip(5, MB_C, MB_DX, S.lpC, S.lpdx);   // C.dX
       dot(S, m, S.b, S.dy, 6, false);            // b.dy
-      ip(7, mats(0), mats(3), S.lpx, S.lpdz);   // X.dZ
-      ip(8, mats(2), mats(1), S.lpdx, S.lpz);   // dX.Z
-      ip(9, mats(2), mats(3), S.lpdx, S.lpdz);  // dX.dZ
+      ip(7, MB_X, MB_DZ, S.lpx, S.lpdz);   // X.dZ
+      ip(8, MB_DX, MB_Z, S.lpdx, S.lpz);   // dX.Z
+      ip(9, MB_DX, MB_DZ, S.lpdx, S.lpdz);  // dX.dZ
     };
     step_products();
     read_scalars(S, h, 10);
@@ -1852,25 +2125,16 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     corrector_beta(sc, P, h[7], h[8], h[9]);
 
     // ---- corrector
-    Wv.clear();
     if (!S.small_idx.empty())
       k_blocks_corrector<<<(unsigned)S.small_idx.size(), NT, small_block_smem(S.small_nmax)>>>(
           S.small_ptrs, sc.beta * sc.mu, dinf ? 1 : 0, lowp ? 1 : 0);
     for (SdpBlock& B : S.sdp) {
       const long long nn = (long long)B.n * B.n;
-      if (B.n <= SMALL_BLOCK) {
-        Wv.push_back(dinf ? B.W1 : B.R);
-        continue;
-      }
+      if (B.n <= SMALL_BLOCK) continue;
       gemm(S, B.n, B.n, B.n, false, B.dX, B.n, false, B.dZ, B.n, B.W1, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
       gemm(S, B.n, B.n, B.n, false, B.W1, B.n, false, B.Zi, B.n, B.W2, B.n, 1.0, 0.0, false, 1, 0, 0, 0, lowp);
       k_axpby_sub<<<nblk(nn), 256>>>(nn, B.R, sc.beta * sc.mu, B.Zi, -1.0, B.X, B.W2);
-      if (dinf) {
-        k_axpby<<<nblk(nn), 256>>>(nn, B.W1, 1.0, B.R, -1.0, B.XDZ);
-        Wv.push_back(B.W1);
-      } else {
-        Wv.push_back(B.R);
-      }
+      if (dinf) k_axpby<<<nblk(nn), 256>>>(nn, B.W1, 1.0, B.R, -1.0, B.XDZ);
     }
     Wl = S.lpR;
     if (nlp) {
@@ -1880,7 +2144,7 @@ int Solver::solve(const InitPoint* init, const Params* prm)
         Wl = S.lpW;
       }
     }
-    a_dot(S.dy, S.rp, -1.0, Wv, Wl);
+    a_dot(S.dy, S.rp, -1.0, dinf ? MB_W1 : MB_R, Wl);
     mark(T_SOLVE);
     schur_solve(S.dy);
     mark(T_DXDZ);
@@ -1934,10 +2198,9 @@ int Solver::solve(const InitPoint* init, const Params* prm)
 
     mark(T_UPDATE);
     // ---- update (Solutions::update)
-    for (SdpBlock& B : S.sdp) {
-      const long long nn = (long long)B.n * B.n;
-      k_axpby<<<nblk(nn), 256>>>(nn, B.X, 1.0, B.X, sc.alphaP, B.dX);
-      k_axpby<<<nblk(nn), 256>>>(nn, B.Z, 1.0, B.Z, sc.alphaD, B.dZ);
+    if (nsdp) {
+      mb_axpby(MB_X, 1.0, MB_X, sc.alphaP, MB_DX);
+      mb_axpby(MB_Z, 1.0, MB_Z, sc.alphaD, MB_DZ);
     }
     if (nlp) {
       k_axpby<<<nblk(nlp), 256>>>(nlp, S.lpx, 1.0, S.lpx, sc.alphaP, S.lpdx);
@@ -1949,17 +2212,18 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     mark(T_RES);
     // ---- residuals, mu, objectives, rho
     residuals();
-    ip(2, mats(4), mats(0), S.lpC, S.lpx);
+    ip(2, MB_C, MB_X, S.lpC, S.lpx);
     dot(S, m, S.b, S.y, 3, false);
-    ip(4, mats(0), mats(1), S.lpx, S.lpz);
+    ip(4, MB_X, MB_Z, S.lpx, S.lpz);
     if (warm) {
-      ip(13, mats(5), mats(1), S.lpx0, S.lpz);
-      ip(14, mats(0), mats(6), S.lpx, S.lpz0);
+      ip(13, MB_X0, MB_Z, S.lpx0, S.lpz);
+      ip(14, MB_X, MB_Z0, S.lpx, S.lpz0);
     } else {
-      cudaMemset(S.sc + 13, 0, 2 * sizeof(double));
-      for (SdpBlock& B : S.sdp) {
-        k_trace<<<1, 256>>>(B.n, B.Z, S.sc + 13, lam);
-        k_trace<<<1, 256>>>(B.n, B.X, S.sc + 14, lam);
+      if (nsdp) {
+        mb_reduce(MB_Z, MB_Z, 2, 13, false, lam);
+        mb_reduce(MB_X, MB_X, 2, 14, false, lam);
+      } else {
+        cudaMemset(S.sc + 13, 0, 2 * sizeof(double));
       }
     }
     read_scalars(S, h, 16);
