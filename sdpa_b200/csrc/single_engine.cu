@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "cta_linalg.cuh"
+#include "diag_block.cuh"
 #include "eig.cuh"
 #include "ipm_control.h"
 #include "sdpa_b200.h"
@@ -701,20 +702,6 @@ __global__ void __launch_bounds__(NT) k_syrk_pairs(const int* pairs, int n, int 
                            A + r0 + (size_t)n * c0, n, -1.0, 1.0, smem, i == j, 0);
 }
 
-// Diagonal block of the blocked Cholesky: one block factors A[0:bs, 0:bs]
-// (leading dimension lda) with the chosen pivot rule; first failure (global
-// column + 1) is written to *flag if *flag is still 0.
-template <typename T>
-__global__ void __launch_bounds__(NT) k_chol_diag(int bs, T* A, int lda, int adjust, int col0, int* flag)
-{
-  extern __shared__ double smem[];
-  __shared__ int s_flag;
-  T* sD = (T*)(smem + cta::GEMM_RECT_SMEM);
-  if (*flag) return;
-  const int f = cta::cholesky<NT, T>(bs, A, lda, adjust != 0, sD, smem, &s_flag);
-  if (f && threadIdx.x == 0) atomicCAS(flag, 0, col0 + f);
-}
-
 // Li = L^{-1} of a bs x bs lower-triangular block (lda) into Li (ld bs)
 template <typename T>
 __global__ void __launch_bounds__(NT) k_tri_inv(int bs, const T* L, int lda, T* Li, int ldi, const int* flag)
@@ -1162,14 +1149,17 @@ static int cholesky_grid_t(DevState& S, T* A, int n, bool adjust, T* Linv, T* Tb
       S.side = nullptr;
     }
   }
+  static_assert(NBG == DB_MAX, "diagonal blocks of the grid Cholesky are factored by k_chol_inv_diag");
+  static std::atomic<unsigned long long> diag_attr{0};
+  smem_attr_per_device((const void*)k_chol_inv_diag<T>, (int)diag_block_smem<T>(), diag_attr);
   auto Li_of = [&](int kb) { return dinv_store ? dinv_store + (size_t)(kb / NBG) * NBG * NBG : Linv; };
   // factor (and, if a panel or the stored inverses need it, invert) the
   // diagonal block at kb on stream st
   auto diag = [&](int kb, cudaStream_t st) {
     const int bs = std::min(NBG, n - kb);
     T* Ad = A + kb + (size_t)n * kb;
-    k_chol_diag<T><<<1, NT, chol_smem(), st>>>(bs, Ad, n, adjust ? 1 : 0, kb, S.flag);
-    if (n - kb - bs > 0 || dinv_store) k_tri_inv<T><<<1, NT, chol_smem(), st>>>(bs, Ad, n, Li_of(kb), bs, S.flag);
+    T* Li = (n - kb - bs > 0 || dinv_store) ? Li_of(kb) : nullptr;
+    k_chol_inv_diag<T><<<1, DB_NT, diag_block_smem<T>(), st>>>(bs, Ad, n, adjust ? 1 : 0, kb, S.flag, Li, bs);
   };
   diag(0, 0);
   for (int kb = 0; kb < n; kb += NBG) {
