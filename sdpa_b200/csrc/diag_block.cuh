@@ -31,6 +31,8 @@ constexpr size_t diag_block_smem()
   return ((size_t)DB_MAX * DB_LDS + (size_t)DB_WLD * 32 + DB_MAX) * sizeof(T);
 }
 
+static_assert(diag_block_smem<double>() <= 227 * 1024, "the resident block must fit one block's shared memory");
+
 template <typename T>
 struct DbPair;
 template <>
