@@ -56,6 +56,7 @@ def peaks():
 # (per-block workspaces of the instances in flight exceed L2), so it grows
 # with the instances processed.
 TRAFFIC_BYTES_PER_INSTANCE = 9.89e9 / 592
+TRAFFIC_NOTE = "ncu dram__bytes of a 592-instance FP64 warm-start launch, scaled by instances"
 
 
 def iter_flops(n: int, m: int) -> float:
@@ -130,57 +131,92 @@ def make_batch(count: int, seed0: int, workload: str = "maxcut"):
     return insts, batch.pack(insts)
 
 
-def cpu_reference(insts, sample: int, procs: int):
+def cpu_reference(insts, procs: int, tight: bool = False):
     """The reference solver (oracle/_ref/ref_batch, compiled from the reference
-    sources) on `sample` instances, one single-threaded process per core.
-    Returns (SDPs/s over the summed solve time of the slowest worker, detail)."""
-    exe = os.path.join(ROOT, "oracle", "_ref", "ref_batch")
-    if not os.path.exists(exe):
-        return None, "oracle/_ref/ref_batch not built"
-    with tempfile.TemporaryDirectory() as tmp:
-        paths = []
-        for q, it in enumerate(insts[:sample]):
-            p = os.path.join(tmp, f"i{q}.dat-s")
-            it.write(p)
-            paths.append(p)
-        lst = os.path.join(tmp, "list.txt")
-        open(lst, "w").write("\n".join(paths))
-        env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
-        t0 = time.time()
-        out = subprocess.run([exe, "--procs", str(procs), "--list", lst], capture_output=True, text=True,
-                             env=env, check=True).stdout
-        wall = time.time() - t0
-    solve_wall = [float(l.split()[1]) for l in out.splitlines() if l.startswith("WALL")][0]
-    ok = sum(1 for l in out.splitlines() if l.startswith("RESULT") and " pdOPT " in l)
-    return sample / solve_wall, {"solve_wall_s": solve_wall, "process_wall_s": wall, "pdOPT": ok}
+    sources) on every instance of the batch, one single-threaded process per
+    core.  Returns (SDPs/s over the slowest worker's summed solve time,
+    detail, RefRun with per-instance objectives and x, RefRun at epsilonStar
+    1e-11 or None)."""
+    from oracle import ref_runner as R
+    if not R.available():
+        return None, "oracle/_ref/ref_batch not built", None, None
+    import shutil
+    tmp = tempfile.mkdtemp()
+    try:
+        R.write_instances(insts, tmp)
+        run = R.run(procs=procs, tmp=tmp, count=len(insts))
+        trun = R.run(procs=procs, tmp=tmp, count=len(insts), param=R.PARAM_TIGHT) if tight else None
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    det = {"solve_wall_s": run.wall_s, "process_wall_s": run.process_wall_s,
+           "pdOPT": int(np.sum(run.phase == 7)), "mean_iterations": float(run.iterations.mean())}
+    return len(insts) / run.wall_s, det, run, trun
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU solver on the whole batch
+    (all `count` instances every step), one single-threaded process per host
+    core.  Under torchrun only rank 0 runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    from oracle import ref_runner as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_batch is not built"}), flush=True)
+        return 0
     insts, _ = make_batch(args.count, 0, args.workload)
     cores = os.cpu_count() or 1
-    sample = min(args.count, max(64, 48 * cores))
-    for _ in range(args.warmup):
-        cpu_reference(insts, min(sample, 2 * cores), cores)
-    vals = []
-    for _ in range(args.steps):
-        v, det = cpu_reference(insts, sample, cores)
-        vals.append(v)
-    value = float(np.median(vals))
+    import shutil
+    tmp = tempfile.mkdtemp()
+    try:
+        R.write_instances(insts, tmp)
+        for _ in range(args.warmup):
+            R.run(procs=cores, tmp=tmp, count=len(insts))
+        runs = [R.run(procs=cores, tmp=tmp, count=len(insts)) for _ in range(args.steps)]
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    walls = [r.wall_s for r in runs]
+    value = args.count / float(np.mean(walls))
+    last = runs[-1]
     blocks = args.workload == "blocks"
+    det = {"solve_wall_s_mean": float(np.mean(walls)), "process_wall_s_mean": float(np.mean([r.process_wall_s for r in runs])),
+           "pdOPT": int(np.sum(last.phase == 7)), "mean_iterations": float(last.iterations.mean())}
     line = {"impl": "reference", "metric": BLOCK_METRIC if blocks else METRIC, "value": value, "unit": "SDPs/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * args.count / value, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * float(np.mean(walls)), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
             "config": {"workload": BLOCK_WORKLOAD if blocks else WORKLOAD, "count": args.count},
             "cpu_baseline": {"value": value, "unit": "SDPs/s", "cores": cores, "kind": "reference",
-                             "sample": f"first {sample} instances of the batch per step, one "
+                             "sample": f"all {args.count} instances of the batch every step, one "
                                        f"single-threaded reference process per core; {det}"},
             "e2e": {"value": value, "unit": "SDPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def fp64_peak():
+    """Measured FP64 GEMM throughput of this GPU (TFLOP/s): torch.matmul on
+    float64 8192^3 (cuBLAS DGEMM on the FP64 tensor cores), best of 5 after a
+    warm-up, CUDA events.  The batched solver's products run on the same FP64
+    MMA and its other steps on the FP64 SIMT pipe."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = torch.empty_like(a)
+    torch.matmul(a, b, out=c)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
 
 
 def _events_time(fn, stream, steps, flush):
@@ -275,11 +311,14 @@ def run_blocks(args):
                        "mean_iterations": float(res.iterations.mean()), "status_nonzero": int(np.sum(res.status != 0))}}
     if not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        sample = min(args.count, max(64, 48 * cores))
-        v, det = cpu_reference(insts, sample, cores)
+        v, det, ref, _ = cpu_reference(insts, cores)
         line["cpu_baseline"] = {"value": v, "unit": "SDPs/s", "cores": cores, "kind": "reference",
-                                "sample": f"first {sample} instances of this batch, one single-threaded "
+                                "sample": f"all {P.count} instances of this batch, one single-threaded "
                                           f"reference process per core; {det}"}
+        if ref is not None:
+            from oracle import ref_runner as R
+            line["reference_parity"] = R.parity_counts(res.primal_obj, res.dual_obj,
+                                                       [res.x_of(P, q) for q in range(P.count)], ref)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -433,14 +472,18 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_val = total / float(t.item())
 
-    # ---- parity of this run (headline vs plain FP64) and roofline
-    ok = int(np.sum(res.phase == 7))
-    relobj = np.abs(res.primal_obj - res0.primal_obj) / np.maximum(1.0, np.abs(res0.primal_obj))
-    xdiff = np.array([np.max(np.abs(res.x_of(P, q) - res0.x_of(P, q))) for q in range(P.count)])
+    # ---- roofline of the solver launch: algorithmic flops of the iterations
+    # each instance ran (reference operation sequence) / device time, against
+    # the measured FP64 GEMM peak (the kernel's products run on the FP64 MMA,
+    # the rest on the FP64 / FP32 SIMT pipes) and, for scale, the bf16 peak
     flops = sum(float(res.iterations[q]) * iter_flops(int(P.n[q]), int(P.m[q])) for q in range(P.count))
     hbm, bf16, src = peaks()
+    fp64 = fp64_peak()
     achieved = flops / (step_ms / 1e3) / 1e12
+    traffic = TRAFFIC_BYTES_PER_INSTANCE * P.count
     launches_per_step = 9 if pipe is not None else 1  # 7 network + 1 proposal + 1 solver
+    relobj = np.abs(res.primal_obj - res0.primal_obj) / np.maximum(1.0, np.abs(res0.primal_obj))
+    xdiff = np.array([np.max(np.abs(res.x_of(P, q) - res0.x_of(P, q))) for q in range(P.count)])
     line = {"metric": METRIC, "value": value, "unit": "SDPs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == N.PREC_FP64 else "f32+f64",
@@ -457,27 +500,36 @@ def main():
             "warm_other_precision": alt,
             "e2e": {"value": e2e_val, "unit": "SDPs/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": args.steps * launches_per_step,
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                         "frac": achieved / bf16,
-                         "traffic": TRAFFIC_BYTES_PER_INSTANCE * P.count,
-                         "traffic_note": "ncu capture of 592 instances scaled by instances (bytes per launch)",
-                         "peak_source": f"{src} bf16 dense (MEASURED_PEAKS.json); the kernel computes "
-                                        "on the FP64/FP32 SIMT pipes",
-                         "fp64_nominal_tflops": 40.0, "frac_of_fp64_nominal": achieved / 40.0,
+            "roofline": {"bound": "tensor", "pipe": "FP64 MMA (mma.sync .f64) + FP64/FP32 SIMT",
+                         "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
+                         "peak_source": "FP64 GEMM measured in this run (torch.matmul float64 8192^3, "
+                                        "cuBLAS DGEMM, best of 5)",
+                         "traffic": traffic, "traffic_note": TRAFFIC_NOTE,
+                         "bf16_peak": bf16, "frac_of_bf16": achieved / bf16,
+                         "bf16_peak_source": f"{src} (MEASURED_PEAKS.json)",
                          "flops_per_launch": flops, "kernel": "batch_ipm_fp64"},
             "clocks": clk.summary(),
-            "parity": {"pdOPT": ok, "count": int(P.count), "mean_iterations": float(res.iterations.mean()),
+            "parity": {"pdOPT": int(np.sum(res.phase == 7)), "count": int(P.count),
+                       "mean_iterations": float(res.iterations.mean()),
                        "retried_in_fp64": int(np.sum(res.status == 2)),
                        "max_rel_objective_diff_vs_plain_fp64": float(relobj.max()),
                        "max_abs_x_diff_vs_plain_fp64": float(xdiff.max()),
-                       "x_diff_above_1e-5": int(np.sum(xdiff > 1e-5))}}
+                       "x_diff_above_1e-5_vs_plain_fp64": int(np.sum(xdiff > 1e-5))}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        sample = min(args.count, max(64, 48 * cores))
-        v, det = cpu_reference(insts, sample, cores)
+        v, det, ref, tref = cpu_reference(insts, cores, tight=True)
         line["cpu_baseline"] = {"value": v, "unit": "SDPs/s", "cores": cores, "kind": "reference",
-                                "sample": f"first {sample} instances of this batch, one single-threaded "
+                                "sample": f"all {P.count} instances of this batch, one single-threaded "
                                           f"reference process per core; {det}"}
+        if ref is not None:
+            # the headline run's every instance against the reference's own
+            # results on the same input (objectives 1e-6, x 1e-5, and the
+            # reference-accuracy bar against its epsilonStar 1e-11 solution)
+            from oracle import ref_runner as R
+            xs = [res.x_of(P, q) for q in range(P.count)]
+            line["reference_parity"] = R.parity_counts(res.primal_obj, res.dual_obj, xs, ref, tref)
+            xs0 = [res0.x_of(P, q) for q in range(P.count)]
+            line["plain_fp64"]["reference_parity"] = R.parity_counts(res0.primal_obj, res0.dual_obj, xs0, ref)
     del g0, gh
     if world > 1:
         dist.barrier()

@@ -5,13 +5,15 @@
 // sequence as the reference CLI main (sdpa_exe.cpp:224-343).
 //
 // Usage:
-//   ref_batch [--param FILE] [--procs P] [--dump DIR] [--trace] FILE.dat-s ...
+//   ref_batch [--param FILE] [--procs P] [--dump DIR] [--trace] [--xvec] FILE.dat-s ...
 //
 // One line per instance on stdout:
 //   RESULT <file> <iterations> <phase> <primalObj> <dualObj> <solve_seconds>
 // With --trace, each iteration's (mu, objP, objD, alphaP, alphaD, beta) line
 // from the reference's own display output is echoed as
 //   TRACE <file> <reference iteration line>
+// With --xvec, the instance's xVec (getResultXVec) follows as
+//   XVEC <file> <m> <x_1> ... <x_m>
 // With --dump DIR, xVec (SDPA's x), and every block of X (getResultXMat) and
 // Y (getResultYMat) are written as raw little-endian float64 files.
 // --procs P forks P workers (instances dealt round-robin); the parent prints
@@ -70,7 +72,7 @@ static std::string base_name(const std::string& f)
 
 // Solves one file; returns initializeSolve+solve seconds.
 static double solve_one(const std::string& file, const char* param, const char* dumpdir,
-                        bool trace, FILE* out)
+                        bool trace, bool xvec, FILE* out)
 {
   SDPA p;
   char tracefile[64] = {0};
@@ -97,6 +99,21 @@ static double solve_one(const std::string& file, const char* param, const char* 
   double t1 = now_s();
   fprintf(out, "RESULT %s %d %s %.17e %.17e %.9f\n", file.c_str(), (int)p.getIteration(),
           phase_name(p.getPhaseValue()), p.getPrimalObj(), p.getDualObj(), t1 - t0);
+  if (xvec) {
+    // one write per line: workers share the output pipe, and writes of up to
+    // PIPE_BUF bytes (m up to about 160) do not interleave
+    const int m = (int)p.getConstraintNumber();
+    const double* x = p.getResultXVec();
+    std::string line = "XVEC " + file + " " + std::to_string(m);
+    char num[40];
+    for (int k = 0; k < m; ++k) {
+      snprintf(num, sizeof(num), " %.17e", x[k]);
+      line += num;
+    }
+    line += "\n";
+    fflush(out);
+    fwrite(line.data(), 1, line.size(), out);
+  }
   if (trace && disp) {
     fflush(disp);
     rewind(disp);
@@ -131,7 +148,7 @@ int main(int argc, char** argv)
 {
   const char* param = NULL;
   const char* dumpdir = NULL;
-  bool trace = false;
+  bool trace = false, xvec = false;
   int procs = 1;
   std::vector<std::string> files;
   for (int a = 1; a < argc; ++a) {
@@ -139,6 +156,7 @@ int main(int argc, char** argv)
     else if (!strcmp(argv[a], "--dump") && a + 1 < argc) dumpdir = argv[++a];
     else if (!strcmp(argv[a], "--procs") && a + 1 < argc) procs = atoi(argv[++a]);
     else if (!strcmp(argv[a], "--trace")) trace = true;
+    else if (!strcmp(argv[a], "--xvec")) xvec = true;
     else if (!strcmp(argv[a], "--list") && a + 1 < argc) {
       FILE* f = fopen(argv[++a], "r");
       if (!f) { perror(argv[a]); return 2; }
@@ -152,12 +170,12 @@ int main(int argc, char** argv)
     } else files.push_back(argv[a]);
   }
   if (files.empty()) {
-    fprintf(stderr, "usage: ref_batch [--param F] [--procs P] [--dump DIR] [--trace] [--list F] FILE...\n");
+    fprintf(stderr, "usage: ref_batch [--param F] [--procs P] [--dump DIR] [--trace] [--xvec] [--list F] FILE...\n");
     return 2;
   }
   if (procs <= 1) {
     double tot = 0.0;
-    for (size_t i = 0; i < files.size(); ++i) tot += solve_one(files[i], param, dumpdir, trace, stdout);
+    for (size_t i = 0; i < files.size(); ++i) tot += solve_one(files[i], param, dumpdir, trace, xvec, stdout);
     printf("WALL %.9f %zu\n", tot, files.size());
     return 0;
   }
@@ -172,7 +190,7 @@ int main(int argc, char** argv)
     if (pid[r] == 0) {
       close(fds[0]);
       double tot = 0.0;
-      for (size_t i = r; i < files.size(); i += procs) tot += solve_one(files[i], param, dumpdir, trace, stdout);
+      for (size_t i = r; i < files.size(); i += procs) tot += solve_one(files[i], param, dumpdir, trace, xvec, stdout);
       if (write(fds[1], &tot, sizeof(tot)) != (ssize_t)sizeof(tot)) _exit(3);
       close(fds[1]);
       fflush(stdout);

@@ -22,6 +22,11 @@ Fixtures (all from the reference's own output, never hand-written):
                        (the reference's sparse path needs MUMPS)
   large.json / large.npz  (--large) Lovasz theta G(200, 0.5) seed 1 and the
                        random m=2000 SDP seed 1: objectives, iterations, x
+  headline.json / headline.npz  (also alone with --headline) the first 512
+                       instances of the 4096-instance batched MaxCut benchmark
+                       (seeds 0..511, n ~ U{20..120}): objectives, iterations,
+                       phase and x at the default parameters, and x at
+                       epsilonStar 1e-11 (x* of the reference-accuracy bar)
 """
 from __future__ import annotations
 
@@ -266,8 +271,35 @@ def arrow_fixtures():
     np.savez_compressed(os.path.join(HERE, "arrow.npz"), **{"arrow.xvec": r.xvec})
 
 
+HEADLINE_SEEDS = 512
+
+
+def headline_fixtures():
+    """Reference results for the benchmark's batched MaxCut seeds 0..511:
+    the headline configuration (learned warm start, mixed precision) is
+    compared with these in tests/test_headline_parity_gpu.py."""
+    from oracle import ref_runner as R
+    its = [inst.batch_maxcut(s, 20, 120) for s in range(HEADLINE_SEEDS)]
+    rd = R.run(its)
+    rt = R.run(its, param=R.PARAM_TIGHT)
+    meta = {"seeds": [0, HEADLINE_SEEDS], "generator": "sdpa_b200.instances.batch_maxcut(seed, 20, 120)",
+            "iterations": rd.iterations.tolist(), "phase": rd.phase.tolist(),
+            "primal_obj": rd.primal_obj.tolist(), "dual_obj": rd.dual_obj.tolist(),
+            "tight_phase": rt.phase.tolist(), "tight_param": "epsilonStar 1e-11, epsilonDash 1e-9"}
+    arrays = {}
+    for s in range(HEADLINE_SEEDS):
+        arrays[f"bmc{s}.xvec"] = rd.x[s]
+        arrays[f"bmc{s}.tight"] = rt.x[s]
+    with open(os.path.join(HERE, "headline.json"), "w") as f:
+        json.dump(meta, f)
+    np.savez_compressed(os.path.join(HERE, "headline.npz"), **arrays)
+
+
 def main():
     large = "--large" in sys.argv
+    if "--headline" in sys.argv:
+        headline_fixtures()
+        return
     if "--arrow" in sys.argv:
         arrow_fixtures()
         return
@@ -337,6 +369,7 @@ def main():
         cli_fixtures()
         block_fixtures(tmp)
         arrow_fixtures()
+        headline_fixtures()
 
         if large:
             big = [("lt200", inst.lovasz_theta(200, 0.5, 1)), ("rnd2000", inst.random_sdp(seed=1))]

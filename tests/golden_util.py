@@ -5,6 +5,8 @@ import os
 
 import numpy as np
 
+from oracle.ref_runner import x_within_reference_accuracy  # noqa: F401  (the parity bar on x)
+
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
@@ -36,16 +38,6 @@ def tight():
     default-parameter results of the warm-start held-out set."""
     meta = json.load(open(os.path.join(GOLDEN, "tight.json")))
     return meta, np.load(os.path.join(GOLDEN, "tight.npz"))
-
-
-def x_within_reference_accuracy(x, x_ref, x_tight, tol=1e-5):
-    """Parity bar on x for paths that leave the reference's iterate sequence
-    (warm start, mixed precision).  At the default stopping test the
-    reference's own x is determined only to |x_ref - x*| (x* its solution at
-    epsilonStar 1e-11; up to 1.5e-4 on batched MaxCut, more where the optimal
-    face is not a point), so such a path must land at least as close to x*
-    as the reference does, up to `tol`."""
-    return float(np.max(np.abs(x - x_tight))) <= float(np.max(np.abs(x_ref - x_tight))) + tol
 
 
 def rel(a, b):

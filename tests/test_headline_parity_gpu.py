@@ -1,0 +1,91 @@
+"""The benchmark's headline configuration pinned to the reference.
+
+The first 512 instances of the 4096-instance batched MaxCut benchmark (seeds
+0..511, n ~ U{20..120}) are solved on the GPU exactly as the benchmark solves
+them: learned warm start (network forward, proposal kernel, SDPAB_INIT_DUAL)
+and mixed precision, through WarmPipeline.  Every instance is compared with
+the reference SDPA's own results on the same input (tests/golden/headline.*,
+made by the reference build):
+
+* phase pdOPT and both objectives within 1e-6 relative, for every instance;
+* x (SDPA's xVec) within 1e-5 of the reference's, or, where the warm/mixed
+  path ends elsewhere on the reference's own uncertainty, at least as close
+  to the reference's epsilonStar = 1e-11 solution x* as the reference's x is
+  (plus 1e-5): oracle.ref_runner.x_within_reference_accuracy.
+
+The plain FP64 path from the standard start follows the reference's iterate
+sequence, so it must meet the strict bar (x within 1e-5) on all 512.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from golden_util import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+SEEDS = 512
+
+
+def _fixture():
+    meta = json.load(open(os.path.join(GOLDEN, "headline.json")))
+    arr = np.load(os.path.join(GOLDEN, "headline.npz"))
+    assert meta["seeds"] == [0, SEEDS]
+    return meta, arr
+
+
+def _classify(res, P, meta, arr):
+    from oracle.ref_runner import x_within_reference_accuracy
+    rel = lambda a, b: abs(a - b) / max(1.0, abs(b))
+    obj_bad, x_strict, x_acc, x_bad = [], 0, 0, []
+    for q in range(SEEDS):
+        if (res.phase[q] != 7 or rel(res.primal_obj[q], meta["primal_obj"][q]) > 1e-6
+                or rel(res.dual_obj[q], meta["dual_obj"][q]) > 1e-6):
+            obj_bad.append(q)
+        x = res.x_of(P, q)
+        xr, xt = arr[f"bmc{q}.xvec"], arr[f"bmc{q}.tight"]
+        if np.max(np.abs(x - xr)) <= 1e-5:
+            x_strict += 1
+        elif x_within_reference_accuracy(x, xr, xt):
+            x_acc += 1
+        else:
+            x_bad.append(q)
+    return obj_bad, x_strict, x_acc, x_bad
+
+
+def test_headline_configuration_matches_reference():
+    """Warm start + mixed precision, the benchmark's pipeline."""
+    import torch
+    from sdpa_b200 import _native as N
+    from sdpa_b200 import batch
+    from sdpa_b200 import warmstart as W
+    meta, arr = _fixture()
+    graphs = [W.batch_graph(s, 20, 120) for s in range(SEEDS)]
+    P = batch.pack([g.instance() for g in graphs])
+    db = batch.DeviceBatch(P)
+    pipe = W.WarmPipeline(W.default_model(), graphs, db)
+    pipe.run(precision=N.PREC_MIXED)
+    torch.cuda.synchronize()
+    res = db.result()
+    obj_bad, x_strict, x_acc, x_bad = _classify(res, P, meta, arr)
+    print(f"headline vs reference ({SEEDS}): objectives off {len(obj_bad)}, x within 1e-5 {x_strict}, "
+          f"x only within the reference's accuracy {x_acc}, x outside both {len(x_bad)}; "
+          f"iterations {res.iterations.mean():.2f} (reference {np.mean(meta['iterations']):.2f})")
+    assert not obj_bad, f"objective or phase differs from the reference: instances {obj_bad[:10]}"
+    assert not x_bad, f"x outside both bars: instances {x_bad[:10]}"
+    assert res.iterations.mean() < np.mean(meta["iterations"]) - 3
+
+
+def test_plain_fp64_matches_reference_strictly():
+    """Standard start, FP64: the reference's iterate sequence, x within 1e-5."""
+    from sdpa_b200 import batch, instances
+    meta, arr = _fixture()
+    P = batch.pack([instances.batch_maxcut(s, 20, 120) for s in range(SEEDS)])
+    res = batch.solve_host(P)
+    obj_bad, x_strict, x_acc, x_bad = _classify(res, P, meta, arr)
+    assert not obj_bad
+    assert x_strict == SEEDS, f"{SEEDS - x_strict} instances outside x within 1e-5"
+    it_diff = np.abs(res.iterations - np.asarray(meta["iterations"]))
+    assert it_diff.max() <= 1

@@ -59,3 +59,31 @@ def test_dats_roundtrip():
     P = O.parse_dats(inst.to_dats())
     assert P.m == 5 and P.blocks == [2, 3, -2]
     assert len(P.entries[0]) == len([1 for k in inst.k if k == 0])
+
+
+def test_headline_fixture_matches_oracle_and_runner():
+    """The headline fixture (reference results for the benchmark's seeds
+    0..511) agrees with the numpy restatement on a few seeds, and, where the
+    reference build is present, with a fresh reference run through
+    oracle.ref_runner (the path bench.py's reference arm takes)."""
+    import json
+    from oracle import ref_runner as R
+    from sdpa_b200 import instances as I
+    meta = json.load(open(os.path.join(GOLDEN, "headline.json")))
+    arr = np.load(os.path.join(GOLDEN, "headline.npz"))
+    seeds = [0, 1, 7, 300]
+    its = [I.batch_maxcut(s, 20, 120) for s in seeds]
+    for s, it in zip(seeds, its[:2]):
+        r = O.solve(O.parse_dats(it.to_dats()))
+        assert r.iterations == meta["iterations"][s]
+        assert rel(r.primal_obj, meta["primal_obj"][s]) < 1e-10
+        assert np.max(np.abs(r.xvec - arr[f"bmc{s}.xvec"])) < 1e-7
+    if not R.available():
+        pytest.skip("oracle/_ref/ref_batch not built")
+    run = R.run(its, procs=2)
+    for q, s in enumerate(seeds):
+        assert run.phase[q] == 7 and run.iterations[q] == meta["iterations"][s]
+        assert run.primal_obj[q] == meta["primal_obj"][s] and run.dual_obj[q] == meta["dual_obj"][s]
+        assert np.array_equal(run.x[q], arr[f"bmc{s}.xvec"])
+    pc = R.parity_counts(run.primal_obj, run.dual_obj, run.x, run, run)
+    assert pc["objectives_within_1e-6"] == len(seeds) and pc["x_failing_both_bars"] == 0
