@@ -50,13 +50,14 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
-# DRAM bytes (read + write) per instance of the solver launch, from one ncu
-# capture of a 592-instance launch at the bench's launch shape (2 blocks per
-# SM, warm start, FP64): 9.89 GB / 592.  The traffic is workspace eviction
-# (per-block workspaces of the instances in flight exceed L2), so it grows
-# with the instances processed.
-TRAFFIC_BYTES_PER_INSTANCE = 9.89e9 / 592
-TRAFFIC_NOTE = "ncu dram__bytes of a 592-instance FP64 warm-start launch, scaled by instances"
+# DRAM bytes (read + write) of the headline solver launch (learned warm
+# start, mixed precision, 4096 instances), from one ncu capture of that
+# launch (profiles/batch_ipm_headline_maxcut4096.md): 34.64 GB read +
+# 41.22 GB written.  Other batch sizes are scaled by instances.
+TRAFFIC_BYTES_HEADLINE = 75.86e9
+TRAFFIC_COUNT = 4096
+TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4096-instance headline launch "
+                "(mixed + warm start), profiles/batch_ipm_headline_maxcut4096.md")
 
 
 def iter_flops(n: int, m: int) -> float:
@@ -336,6 +337,8 @@ def main():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="fixed launch shape (0 = autotune)")
     ap.add_argument("--workload", default="maxcut", choices=["maxcut", "blocks"])
+    ap.add_argument("--profile", action="store_true",
+                    help="only launch the headline pipeline warmup + steps times, untimed (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -368,6 +371,26 @@ def main():
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
+
+    if args.profile:
+        # the headline pipeline alone, launched warmup + steps times (one
+        # solver launch each), for a profiler: nothing is timed or printed
+        # but the instances' outcome
+        dbp = batch.DeviceBatch(P)
+        pp = W.WarmPipeline(W.default_model(), graphs, dbp) if args.warm else None
+        for _ in range(args.warmup + args.steps):
+            if pp is not None:
+                pp.run(precision=prec, stream=stream, ctas_per_sm=args.ctas_per_sm)
+            else:
+                dbp.solve(precision=prec, stream=stream, ctas_per_sm=args.ctas_per_sm)
+        barrier()
+        r = dbp.result()
+        if rank == 0:
+            print(json.dumps({"profile": True, "count": args.count, "launches": args.warmup + args.steps,
+                              "pdOPT": int(np.sum(r.phase == 7)), "mean_iterations": float(r.iterations.mean())}))
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
 
     # ---- plain FP64 path (standard start): the denominator of the headline ratio
     db0 = batch.DeviceBatch(P)
@@ -480,7 +503,7 @@ def main():
     hbm, bf16, src = peaks()
     fp64 = fp64_peak()
     achieved = flops / (step_ms / 1e3) / 1e12
-    traffic = TRAFFIC_BYTES_PER_INSTANCE * P.count
+    traffic = TRAFFIC_BYTES_HEADLINE * P.count / TRAFFIC_COUNT
     launches_per_step = 9 if pipe is not None else 1  # 7 network + 1 proposal + 1 solver
     relobj = np.abs(res.primal_obj - res0.primal_obj) / np.maximum(1.0, np.abs(res0.primal_obj))
     xdiff = np.array([np.max(np.abs(res.x_of(P, q) - res0.x_of(P, q))) for q in range(P.count)])

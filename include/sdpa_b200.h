@@ -128,6 +128,14 @@ SDPAB_API int sdpab_sdpa_set_init(sdpab_sdpa* h, const double* xvec, const doubl
  * nDim * mu / max(1, (|objP| + |objD|) / 2) >= mu_switch (0 = 1e-2), FP64
  * after. */
 SDPAB_API int sdpab_sdpa_set_precision(sdpab_sdpa* h, int mode, double mu_switch);
+/* Bound on the polls of every wait in the mixed mode's tensor-core pipelines
+ * (no reference counterpart; < 0: the default bound).  A pipeline that gives
+ * up makes that iteration use the FP64 Schur factor or the SIMT products; a
+ * small bound exercises that fall-back in tests. */
+SDPAB_API int sdpab_sdpa_set_tc_wait(sdpab_sdpa* h, long long polls);
+/* Tensor-core pipelines that gave up during the last solve (their
+ * iterations fell back as above). */
+SDPAB_API int sdpab_sdpa_tc_timeouts(sdpab_sdpa* h, int* out);
 /* SDPA::initializeSolve + SDPA::solve (sdpa_solve.cpp:10-43, :59-233) */
 SDPAB_API int sdpab_sdpa_solve(sdpab_sdpa* h);
 /* scalar getters (sdpa_call.cpp:719-847) */
@@ -151,8 +159,14 @@ SDPAB_API int sdpab_sdpa_get_xvec(sdpab_sdpa* h, double* out);
 SDPAB_API int sdpab_sdpa_get_block(sdpab_sdpa* h, int l, int which, double* out);
 /* getBlockSize / getBlockType (sdpa_call.cpp:813-847) */
 SDPAB_API int sdpab_sdpa_block_size(sdpab_sdpa* h, int l, int* size, int* is_sdp);
-/* SDPA::getDimacsError (IO::computeDimacs, sdpa_io.cpp:775-813): err7[1..6] */
+/* SDPA::getDimacsError (IO::computeDimacs, sdpa_io.cpp:775-813): err7[1..6];
+ * the norms, X . Z and the minimum eigenvalues are computed on the GPU. */
 SDPAB_API int sdpab_sdpa_dimacs(sdpab_sdpa* h, double* err7);
+/* Minimum eigenvalue of a symmetric n x n matrix (DEVICE pointer, column-major,
+ * lower triangle referenced) into *out (host), computed on the GPU: the
+ * dsyev minimum of Lal::getMinEigenValue (sdpa_linear.cpp:145-182) that
+ * IO::computeDimacs takes of X and Z.  Synchronises `stream`. */
+SDPAB_API int sdpab_min_eigenvalue(int n, const double* A, double* out, void* stream);
 /* SDPA::writeInitSparse (sdpa_call.cpp:1199-1220) */
 SDPAB_API int sdpab_sdpa_write_init(sdpab_sdpa* h, const char* path);
 /* SDPA::copyCurrentToInit (sdpa_call.cpp:1238-1245) + setInitPoint(true) */
@@ -296,9 +310,13 @@ typedef struct sdpab_batch_config {
  * accumulation: the trailing update of the mixed-precision Schur factor,
  * exposed stand-alone (no counterpart in the reference; the reference's is
  * dsyrk inside rATL_dpotrfL, sdpa_dpotrf.cpp:218-265).  Synchronises
- * `stream`. */
+ * `stream`.  Every wait of the MMA pipeline is bounded: wait_polls < 0 keeps
+ * the default bound, wait_polls >= 0 gives up after that many polls (for
+ * tests of the fall-back: the call then returns SDPAB_ECUDA and leaves the
+ * tiles whose block gave up unchanged). */
 SDPAB_API long long sdpab_tc_syrk_work_bytes(int M, int K);  /* device scratch of the call below */
-SDPAB_API int sdpab_tc_syrk(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, void* stream);
+SDPAB_API int sdpab_tc_syrk(int M, int K, const float* P, int ldp, float* C, int ldc, void* work,
+                            long long wait_polls, void* stream);
 
 /* Tensor-core product C_q = A_q B^T for q < batch, FP64 in and out
  * (column-major device pointers; A_q M x K at A + q sA, B N x K shared, C_q
@@ -306,10 +324,11 @@ SDPAB_API int sdpab_tc_syrk(int M, int K, const float* P, int ldp, float* C, int
  * (X A_j) Z^-1 of the mixed-precision Schur assembly (Z^-1 symmetric, so
  * B = Z^-1), exposed stand-alone (no counterpart in the reference, whose F1
  * products are dgemm calls, sdpa_newton.cpp:885-889).  Synchronises
- * `stream`. */
+ * `stream`.  wait_polls as for sdpab_tc_syrk. */
 SDPAB_API long long sdpab_tc_gemm_work_bytes(int M, int N, int K, int batch);
 SDPAB_API int sdpab_tc_gemm(int M, int N, int K, int batch, const double* A, int lda, long long sA, const double* B,
-                            int ldb, double* C, int ldc, long long sC, void* work, void* stream);
+                            int ldb, double* C, int ldc, long long sC, void* work, long long wait_polls,
+                            void* stream);
 
 /* Solves a batch whose arrays (problem, init, result) are all DEVICE pointers,
  * asynchronously on `stream` (a cudaStream_t, NULL = default stream).
@@ -332,15 +351,17 @@ SDPAB_API int sdpab_batch_solve_host(const sdpab_batch* prob, const sdpab_batch_
  * service that must not allocate after start-up because cudaMalloc
  * synchronises the device and may fail under memory pressure.  Arguments are
  * those of sdpab_batch_solve (all DEVICE pointers; the caller owns inputs and
- * outputs).  The solver's scratch is a fixed region of
+ * outputs), except that it takes no sdpab_batch_config: it always solves in
+ * FP64 with the default launch shape.  The solver's scratch is a fixed region of
  * SDPAB_NOALLOC_SCRATCH_BYTES inside this library, held on every GPU that
  * loads it until the process exits; one solver block needs
  * 8 * (14 * nmax^2 + mmax^2) bytes of it (nmax = mmax = 120 fits 19 blocks,
  * the largest accepted size is about nmax = mmax = 528), larger batches run
  * with fewer concurrent blocks, and sizes whose single block does not fit are
- * rejected with SDPAB_ESIZE.  The first call on a device looks up the
- * region's device address; make that first call before any stream capture.
- * Calls share the region (it keeps the last call's contents; the queue
+ * rejected with SDPAB_ESIZE.  Every call looks up the region's device
+ * address on the current device (the first call on a device also loads the
+ * module there; make that first call before any stream capture).  Calls
+ * share the region (it keeps the last call's contents; the queue
  * counter is cleared each call): calls that overlap on the GPU race. */
 #define SDPAB_NOALLOC_SCRATCH_BYTES (32ull * 1024ull * 1024ull)
 SDPAB_API int sdpab_batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,

@@ -150,6 +150,11 @@ class SDPAB_CLASS_API SDPA {
   // complementarity gap n*mu / max(1, mean |objective|) >= mu_switch;
   // 0 = default 1e-2)
   void setPrecision(int mode, double mu_switch = 0.0);
+  // not in the reference: bound on the polls of each wait of the mixed
+  // mode's tensor-core pipelines (< 0: the default bound).  A pipeline that
+  // gives up falls back to the FP64 factor / SIMT products for that
+  // iteration; tests use a small bound to exercise that path.
+  void setTensorCoreWaitLimit(long long polls);
   // not in the reference: the error channel that replaces its exit() calls
   int getErrorCode();
   const char* getErrorMessage();

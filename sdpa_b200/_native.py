@@ -98,6 +98,8 @@ SIGNATURES = [
                                          c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sdpab_sdpa_set_init", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sdpab_sdpa_set_precision", c_int, [c_void_p, c_int, c_double]),
+    ("sdpab_sdpa_set_tc_wait", c_int, [c_void_p, c_longlong]),
+    ("sdpab_sdpa_tc_timeouts", c_int, [c_void_p, POINTER(c_int)]),
     ("sdpab_sdpa_solve", c_int, [c_void_p]),
     ("sdpab_sdpa_info", c_int, [c_void_p, POINTER(SdpaInfo)]),
     ("sdpab_sdpa_phase_times", c_int, [c_void_p, c_void_p]),
@@ -106,14 +108,15 @@ SIGNATURES = [
     ("sdpab_sdpa_get_block", c_int, [c_void_p, c_int, c_int, c_void_p]),
     ("sdpab_sdpa_block_size", c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),
     ("sdpab_sdpa_dimacs", c_int, [c_void_p, c_void_p]),
+    ("sdpab_min_eigenvalue", c_int, [c_int, c_void_p, POINTER(c_double), c_void_p]),
     ("sdpab_sdpa_write_init", c_int, [c_void_p, c_char_p]),
     ("sdpab_sdpa_copy_current_to_init", c_int, [c_void_p]),
     ("sdpab_release_workspace", c_int, []),
     ("sdpab_tc_syrk_work_bytes", c_longlong, [c_int, c_int]),
-    ("sdpab_tc_syrk", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
+    ("sdpab_tc_syrk", c_int, [c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_longlong, c_void_p]),
     ("sdpab_tc_gemm_work_bytes", c_longlong, [c_int, c_int, c_int, c_int]),
     ("sdpab_tc_gemm", c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_longlong, c_void_p, c_int, c_void_p,
-                              c_int, c_longlong, c_void_p, c_void_p]),
+                              c_int, c_longlong, c_void_p, c_longlong, c_void_p]),
 ]
 
 _lib = None

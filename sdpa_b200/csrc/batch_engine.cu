@@ -23,9 +23,9 @@
 // There are no inter-block waits: the only synchronisation is __syncthreads.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
 #include <algorithm>
-#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -888,15 +888,14 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
 // instead of the growable workspace.  The region is a file-scope device
 // array, so every GPU that loads the library holds it until the process
 // exits.  Host code must not use the array's name as a device address: the
-// address is fetched once per device with cudaGetSymbolAddress (the first
-// call on a device does this set-up, so make that first call before any
-// stream capture).  All calls share the one region and it keeps the previous
+// address is looked up with cudaGetSymbolAddress on every call, on the
+// device that is current (a cached address would go stale after
+// cudaDeviceReset; the lookup allocates nothing), and the first call on a
+// device also loads the module there, so make that first call before any
+// stream capture.  All calls share the one region and it keeps the previous
 // call's contents; the work-queue counter is cleared on every call, and two
 // calls that overlap on the GPU race on the region.
 static __device__ __align__(256) double g_noalloc_scratch[SDPAB_NOALLOC_SCRATCH_BYTES / sizeof(double)];
-
-static std::mutex g_noalloc_mu;
-static double* g_noalloc_base[64] = {nullptr};
 
 int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
                         const sdpab_params* prm, sdpab_batch_result* res, const int* order,
@@ -910,24 +909,22 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   const long long stride = ws_doubles(prob->nmax, prob->mmax);
   const long long head = 32;  // doubles reserved for the work-queue counter
   const long long capacity = ((long long)(SDPAB_NOALLOC_SCRATCH_BYTES / sizeof(double)) - head) / stride;
-  if (capacity < 1)
-    return set_error(SDPAB_ESIZE,
-                     "batch_solve_noalloc: one block's workspace (14*nmax^2 + mmax^2 doubles) "
-                     "exceeds the 32 MiB scratch region; use sdpab_batch_solve");
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
-    return set_error(SDPAB_ENODEV, "batch_solve_noalloc: no CUDA device");
-  double* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_base[dev]) {
-      void* p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess) return cuda_error(e, "batch_solve_noalloc: cudaGetSymbolAddress");
-      g_noalloc_base[dev] = (double*)p;
-    }
-    base = g_noalloc_base[dev];
+  if (capacity < 1) {
+    char msg[200];
+    snprintf(msg, sizeof(msg),
+             "batch_solve_noalloc: one block's workspace (14*nmax^2 + mmax^2 doubles) exceeds the "
+             "%llu MiB scratch region; use sdpab_batch_solve",
+             (unsigned long long)(SDPAB_NOALLOC_SCRATCH_BYTES >> 20));
+    return set_error(SDPAB_ESIZE, msg);
   }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(SDPAB_ENODEV, "batch_solve_noalloc: no CUDA device");
+  void* sym = nullptr;
+  {
+    cudaError_t e = cudaGetSymbolAddress(&sym, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "batch_solve_noalloc: cudaGetSymbolAddress");
+  }
+  double* base = (double*)sym;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long gsm = staging_doubles(prob->nmax, prob->mmax, 0);

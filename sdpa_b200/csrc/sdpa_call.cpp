@@ -248,40 +248,6 @@ int parse_init(const std::string& text, bool sparse, SdpaImpl& I, std::string& w
   return SDPAB_OK;
 }
 
-// Smallest eigenvalue of a small symmetric matrix (host, cyclic Jacobi), for
-// the DIMACS errors.
-static double host_min_eig(std::vector<double> A, int n)
-{
-  for (int sweep = 0; sweep < 60; ++sweep) {
-    double off = 0.0;
-    for (int j = 0; j < n; ++j)
-      for (int i = 0; i < j; ++i) off += A[i + (size_t)n * j] * A[i + (size_t)n * j];
-    if (off < 1e-30) break;
-    for (int p = 0; p < n; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = A[p + (size_t)n * q];
-        if (fabs(apq) < 1e-300) continue;
-        const double app = A[p + (size_t)n * p], aqq = A[q + (size_t)n * q];
-        const double th = (aqq - app) / (2 * apq);
-        const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
-        const double c = 1 / sqrt(t * t + 1), s = t * c;
-        for (int k = 0; k < n; ++k) {
-          const double akp = A[k + (size_t)n * p], akq = A[k + (size_t)n * q];
-          A[k + (size_t)n * p] = c * akp - s * akq;
-          A[k + (size_t)n * q] = s * akp + c * akq;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double apk = A[p + (size_t)n * k], aqk = A[q + (size_t)n * k];
-          A[p + (size_t)n * k] = c * apk - s * aqk;
-          A[q + (size_t)n * k] = s * apk + c * aqk;
-        }
-      }
-  }
-  double mn = 1e300;
-  for (int i = 0; i < n; ++i) mn = std::min(mn, A[i + (size_t)n * i]);
-  return mn;
-}
-
 }  // namespace sdpab
 
 namespace sdpab {
@@ -717,67 +683,33 @@ SDPA::ConeType SDPA::getBlockType(SDPA_INT l)
   return impl_->isSdp(l - 1) ? SDP : LP;
 }
 
-// IO::computeDimacs (sdpa_io.cpp:775-813), on the host from the results.
+// IO::computeDimacs (sdpa_io.cpp:775-813).  The input norms ||b||_1 and
+// ||C||_1 (Lal::getOneNorm: largest absolute entry, sdpa_linear.cpp:184-235)
+// come from the input data; the residual norms, X . Z and the minimum
+// eigenvalues of X and Z are computed on the GPU from the final point.
 void SDPA::getDimacsError(double* d)
 {
   SdpaImpl& I = *impl_;
   for (int q = 0; q <= 6; ++q) d[q] = 0.0;
   if (!I.solved) return;
-  const int m = I.prob.m, nb = I.nb();
-  // internal X = Y result, Z = X result, y = -x
-  std::vector<double> rp(I.prob.c);
-  std::vector<std::vector<double>> Dm(nb);
   double b1 = 0.0, c1 = 0.0;
   for (double v : I.prob.c) b1 = std::max(b1, fabs(v));
-  for (int l = 0; l < nb; ++l) {
-    Dm[l].assign(I.Xres[l].size(), 0.0);
-    for (size_t t = 0; t < Dm[l].size(); ++t) Dm[l][t] = -I.Xres[l][t];
+  for (const sdpab::Entry& e : I.prob.entries)
+    if (e.k == 0) c1 = std::max(c1, fabs(e.v));
+  double dev[5];
+  const int rc = I.solver.dimacs(dev);
+  if (rc != SDPAB_OK) {
+    I.fail(rc, sdpab_last_error());
+    return;
   }
-  for (const sdpab::Entry& e : I.prob.entries) {
-    const int l = e.l - 1;
-    const int n = I.blockDim(l);
-    const bool sdp = I.isSdp(l);
-    auto Y = [&](int i, int j) { return sdp ? I.Yres[l][(i - 1) + (size_t)n * (j - 1)] : I.Yres[l][i - 1]; };
-    auto addD = [&](int i, int j, double v) {
-      if (sdp) {
-        Dm[l][(i - 1) + (size_t)n * (j - 1)] += v;
-        if (i != j) Dm[l][(j - 1) + (size_t)n * (i - 1)] += v;
-      } else {
-        Dm[l][i - 1] += v;
-      }
-    };
-    if (e.k == 0) {
-      c1 = std::max(c1, fabs(e.v));
-      addD(e.i, e.j, -e.v);  // C = -F0
-    } else {
-      const double a = (e.i == e.j || !sdp) ? e.v * Y(e.i, e.j) : e.v * (Y(e.i, e.j) + Y(e.j, e.i));
-      rp[e.k - 1] -= a;
-      addD(e.i, e.j, e.v * I.xvec[e.k - 1]);  // -A_k y_k with y = -x
-    }
-  }
-  double pn = 0.0, dn = 0.0, xz = 0.0;
-  for (double v : rp) pn += v * v;
-  double xmin = 1e300, zmin = 1e300;
-  for (int l = 0; l < nb; ++l) {
-    for (double v : Dm[l]) dn += v * v;
-    for (size_t t = 0; t < I.Xres[l].size(); ++t) xz += I.Xres[l][t] * I.Yres[l][t];
-    if (I.isSdp(l)) {
-      xmin = std::min(xmin, sdpab::host_min_eig(I.Yres[l], I.blockDim(l)));
-      zmin = std::min(zmin, sdpab::host_min_eig(I.Xres[l], I.blockDim(l)));
-    } else {
-      for (double v : I.Yres[l]) xmin = std::min(xmin, v);
-      for (double v : I.Xres[l]) zmin = std::min(zmin, v);
-    }
-  }
-  (void)m;
   const sdpab::SolveStats& s = I.solver.stats();
   const double ctx = s.objValPrimal, bty = s.objValDual;
-  d[1] = sqrt(pn) / (1 + b1);
-  d[2] = std::max(0.0, -xmin / (1 + b1));
-  d[3] = sqrt(dn) / (1 + c1);
-  d[4] = std::max(0.0, -zmin / (1 + c1));
+  d[1] = sqrt(dev[0]) / (1 + b1);
+  d[2] = std::max(0.0, -dev[2] / (1 + b1));
+  d[3] = sqrt(dev[1]) / (1 + c1);
+  d[4] = std::max(0.0, -dev[3] / (1 + c1));
   d[5] = (ctx - bty) / (1 + fabs(ctx) + fabs(bty));
-  d[6] = xz / (1 + fabs(ctx) + fabs(bty));
+  d[6] = dev[4] / (1 + fabs(ctx) + fabs(bty));
 }
 void SDPA::printDimacsError(double* d, char* fmt, FILE* fp)
 {
@@ -958,6 +890,7 @@ void SDPA::copyCurrentToInit()
 }
 void SDPA::setKappa(double k) { impl_->kappa = k; }
 void SDPA::setPrecision(int mode, double mu_switch) { impl_->solver.set_precision(mode, mu_switch); }
+void SDPA::setTensorCoreWaitLimit(long long polls) { impl_->solver.set_tc_wait(polls); }
 int SDPA::getErrorCode() { return impl_->err; }
 const sdpab::SolveStats& SDPA::impl_solver_stats() { return impl_->solver.stats(); }
 const char* SDPA::getErrorMessage() { return impl_->errmsg.c_str(); }
@@ -1058,6 +991,18 @@ SDPAB_API int sdpab_sdpa_set_precision(sdpab_sdpa* h, int mode, double mu_switch
   ((SDPA*)h)->setPrecision(mode, mu_switch);
   return SDPAB_OK;
 }
+SDPAB_API int sdpab_sdpa_set_tc_wait(sdpab_sdpa* h, long long polls)
+{
+  if (!h) return sdpab::set_error(SDPAB_EINVAL, "set_tc_wait: null handle");
+  ((SDPA*)h)->setTensorCoreWaitLimit(polls);
+  return SDPAB_OK;
+}
+SDPAB_API int sdpab_sdpa_tc_timeouts(sdpab_sdpa* h, int* out)
+{
+  if (!h || !out) return sdpab::set_error(SDPAB_EINVAL, "tc_timeouts: null argument");
+  *out = ((SDPA*)h)->impl_solver_stats().tc_timeouts;
+  return SDPAB_OK;
+}
 SDPAB_API int sdpab_sdpa_solve(sdpab_sdpa* h)
 {
   if (!h) return sdpab::set_error(SDPAB_EINVAL, "null argument");
@@ -1130,8 +1075,11 @@ SDPAB_API int sdpab_sdpa_block_size(sdpab_sdpa* h, int l, int* size, int* is_sdp
 SDPAB_API int sdpab_sdpa_dimacs(sdpab_sdpa* h, double* err7)
 {
   if (!h || !err7) return sdpab::set_error(SDPAB_EINVAL, "null argument");
-  ((SDPA*)h)->getDimacsError(err7);
-  return SDPAB_OK;
+  SDPA* p = (SDPA*)h;
+  const int before = p->getErrorCode();
+  p->getDimacsError(err7);
+  const int e = p->getErrorCode();
+  return (e != before) ? e : SDPAB_OK;
 }
 SDPAB_API int sdpab_sdpa_write_init(sdpab_sdpa* h, const char* path)
 {

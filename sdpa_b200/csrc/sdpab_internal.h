@@ -14,12 +14,15 @@ int set_error(int code, const char* msg);
 // Tensor-core (tcgen05, split TF32) lower update C -= P P^T of an M x M FP32
 // matrix (tc_syrk.cu); `work` holds syrk_tf32x3_work_bytes(M, K) bytes.
 // Returns a cudaError_t value; *err (device) is set when a block gave up
-// waiting for its MMAs (the update is then incomplete).
+// waiting for its MMAs (the update is then incomplete).  wait_polls < 0: the
+// default bound of the pipeline's waits; >= 0: that many polls (tests of
+// the fall-back paths).
 long long syrk_tf32x3_work_bytes(int M, int K);
-int syrk_tf32x3(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, int* err, cudaStream_t st);
+int syrk_tf32x3(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, int* err, cudaStream_t st,
+                long long wait_polls = -1);
 long long gemm_tf32x3_work_bytes(int M, int N, int K, int batch);
 int gemm_tf32x3(int M, int N, int K, int batch, const double* A, int lda, long long sA, const double* B, int ldb,
-                double* C, int ldc, long long sC, void* work, int* err, cudaStream_t st);
+                double* C, int ldc, long long sC, void* work, int* err, cudaStream_t st, long long wait_polls = -1);
 int cuda_error(cudaError_t e, const char* where);
 
 // Raises a kernel's dynamic shared-memory limit to `bytes` on the current
@@ -54,6 +57,26 @@ class Workspace {
 };
 
 Workspace& workspace();
+
+// IO::computeDimacs (sdpa_io.cpp:775-813) on the device: the final primal
+// residual vector, dual residual matrices, X and Z of a finished solve
+// (device pointers; SDP blocks as n x n column-major, LP blocks as vectors).
+struct DimacsInput {
+  int m;
+  const double* rp;
+  int nsdp;
+  const int* n;
+  const double* const* X;
+  const double* const* Z;
+  const double* const* D;
+  int nlp;
+  const double *lpx, *lpz, *lpD;
+};
+// out = {||rp||^2, ||D||^2, lambda_min(X), lambda_min(Z), X . Z} (dimacs.cu)
+int dimacs_device(const DimacsInput& in, double* out, cudaStream_t st);
+// Minimum eigenvalue of each of `count` symmetric matrices (device pointers,
+// lower triangles referenced) into out_host (dimacs.cu)
+int min_eigenvalues_device(int count, const int* n, const double* const* A, double* out_host, cudaStream_t st);
 
 int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
                        const sdpab_params* prm, const sdpab_batch_config* cfg,

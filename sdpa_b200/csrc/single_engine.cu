@@ -1053,6 +1053,7 @@ struct DevState {
   void* tc_work = nullptr;  // their split operands (syrk_tf32x3_work_bytes(m, NBG))
   int* tc_f1_err = nullptr;   // time-out flag of the tensor-core F1 products
   void* tc_f1_work = nullptr; // split operands of the tensor-core F1 products (mixed mode)
+  long long tc_wait = -1;     // polls per wait of the tensor-core pipelines (< 0: their default)
   std::vector<void*> allocs;
   double* alloc(size_t n)
   {
@@ -1200,7 +1201,7 @@ static int cholesky_grid_t(DevState& S, T* A, int n, bool adjust, T* Linv, T* Tb
     T* A33 = A22 + nb2 + (size_t)n * nb2;
     bool done = false;
     if constexpr (std::is_same<T, float>::value) {
-      if (S.tc && S.tc_work) done = syrk_tf32x3(rest, bs, P2, n, A33, n, S.tc_work, S.tc_err, 0) == 0;
+      if (S.tc && S.tc_work) done = syrk_tf32x3(rest, bs, P2, n, A33, n, S.tc_work, S.tc_err, 0, S.tc_wait) == 0;
     }
     if (!done) gemm_t<T, T>(rest, rest, bs, false, P2, n, true, P2, n, A33, n, -1.0, 1.0, true);
   }
@@ -1294,6 +1295,23 @@ void Solver::release()
 {
   delete d_;
   d_ = nullptr;
+}
+
+int Solver::dimacs(double* out)
+{
+  if (!d_) return set_error(SDPAB_ESTATE, "dimacs: no solve");
+  DevState& S = *d_;
+  std::vector<int> n;
+  std::vector<const double*> X, Z, D;
+  for (const SdpBlock& B : S.sdp) {
+    n.push_back(B.n);
+    X.push_back(B.X);
+    Z.push_back(B.Z);
+    D.push_back(B.D);
+  }
+  DimacsInput in{S.m, S.rp, (int)S.sdp.size(), n.data(), X.data(), Z.data(), D.data(),
+                 S.nlp, S.lpx, S.lpz, S.lpD};
+  return dimacs_device(in, out, 0);
 }
 
 int Solver::formula_count(int f) const
@@ -1731,6 +1749,7 @@ int Solver::solve(const InitPoint* init, const Params* prm)
   // tensor-core trailing updates pay from a few panels on
   S.tc = precision_ == SDPAB_PREC_MIXED && m >= 256;
   S.mu_switch = (mu_switch_ > 0.0) ? mu_switch_ : 1.0e-2;
+  S.tc_wait = tc_wait_;
   if (S.mixed && !S.B32) {
     void* p = nullptr;
     const size_t fl = (size_t)m * m + (size_t)NBG * NBG + (size_t)m * NBG + m;
@@ -2000,7 +2019,7 @@ int Solver::solve(const InitPoint* init, const Params* prm)
           double* G = S.T + (size_t)F1_CHUNK * nn;
           k_f1_left<<<dim3(B.n, cnt), 256>>>(B.n, q0, B.f1, B.csc_cptr, B.csc_ptr, B.csc_row, B.csc_val, B.X, T);
           const bool tc_done = use_tc && gemm_tf32x3(B.n, B.n, B.n, cnt, T, B.n, nn, B.Zi, B.n, G, B.n, nn,
-                                                     S.tc_f1_work, S.tc_f1_err, 0) == 0;
+                                                     S.tc_f1_work, S.tc_f1_err, 0, S.tc_wait) == 0;
           if (!tc_done)
             gemm(S, B.n, B.n, B.n, false, T, B.n, false, B.Zi, B.n, G, B.n, 1.0, 0.0, false, cnt, nn, 0, nn, lowp);
           static std::atomic<unsigned long long> pack_attr{0};

@@ -84,6 +84,8 @@ class Solver {
     precision_ = mode;
     mu_switch_ = mu_switch;
   }
+  // polls per wait of the tensor-core pipelines (< 0: their default bound)
+  void set_tc_wait(long long polls) { tc_wait_ = polls; }
 
   const SolveStats& stats() const { return stats_; }
   // Results in the reference getters' layout (file block order, 1-based l).
@@ -91,11 +93,16 @@ class Solver {
   const std::vector<double>& resultX(int l) const { return Xres_[l - 1]; }  // getResultXMat
   const std::vector<double>& resultY(int l) const { return Yres_[l - 1]; }  // getResultYMat
   int formula_count(int f) const;  // number of (constraint, block) pairs using F1/F2/F3
+  // The device part of IO::computeDimacs (sdpa_io.cpp:775-813) for the last
+  // solve: out = {||rp||^2, ||D||^2, lambda_min(X), lambda_min(Z), X . Z} of
+  // the final point (internal X, Z; D and rp the final residuals).
+  int dimacs(double* out);
 
  private:
   DevState* d_ = nullptr;
   int precision_ = 0;
   double mu_switch_ = 0.0;
+  long long tc_wait_ = -1;
   SolveStats stats_;
   std::vector<double> xvec_;
   std::vector<std::vector<double>> Xres_, Yres_;

@@ -80,9 +80,11 @@ __device__ __forceinline__ uint32_t to_tf32(float a)
   return r;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+// Polls an mbarrier phase at most `limit` times (limit <= 0: none); true once
+// the phase has completed.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = WAIT_LIMIT)
 {
-  for (long long it = 0; it < WAIT_LIMIT; ++it) {
+  for (long long it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -183,9 +185,13 @@ __device__ __forceinline__ Pipe pipe_open(unsigned char* smem)
 // Thread 0: streams the nk chunks of the A row block `a` and the B row block
 // `b` (hi and lo tiles adjacent per chunk) through the two stages and issues
 // 3 x 2 MMAs per chunk into the accumulator; a stage is refilled with chunk
-// k+1 once chunk k-1's MMAs have completed.  Every wait is bounded.
+// k+1 once chunk k-1's MMAs have completed.  Every wait is bounded: the
+// waits that advance the pipeline give up after `limit` polls (the caller's
+// choice; WAIT_LIMIT in normal use, small in the tests of the fall-back),
+// the waits that drain copies still in flight after giving up use
+// WAIT_LIMIT, so the block's shared memory is quiet when it is released.
 __device__ __forceinline__ void pipe_issue(const Pipe& p, unsigned char* smem, const uint32_t* a, const uint32_t* b,
-                                           int nk)
+                                           int nk, long long limit)
 {
   const uint32_t st0 = (uint32_t)__cvta_generic_to_shared(smem);
   auto load_stage = [&](int s, int c) {
@@ -204,7 +210,7 @@ __device__ __forceinline__ void pipe_issue(const Pipe& p, unsigned char* smem, c
   }
   for (int kc = 0; kc < nk && ok; ++kc) {
     const int s = kc & 1;
-    ok = mbar_wait(p.full[s], (kc >> 1) & 1);
+    ok = mbar_wait(p.full[s], (kc >> 1) & 1, limit);
     if (!ok) break;
     in_flight[s] = -1;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -228,7 +234,7 @@ __device__ __forceinline__ void pipe_issue(const Pipe& p, unsigned char* smem, c
     // (chunk kc's MMAs keep the tensor cores busy meanwhile)
     if (kc >= 1 && kc + 1 < nk) {
       const int sp = (kc - 1) & 1;
-      ok = mbar_wait(p.empty[sp], ((kc - 1) >> 1) & 1);
+      ok = mbar_wait(p.empty[sp], ((kc - 1) >> 1) & 1, limit);
       if (ok) {
         load_stage(sp, kc + 1);
         in_flight[sp] = kc + 1;
@@ -243,7 +249,9 @@ __device__ __forceinline__ void pipe_issue(const Pipe& p, unsigned char* smem, c
 }
 
 // All threads: true when every chunk's MMAs completed (the last commit
-// completes after all of them); on failure the error flag is set.
+// completes after all of them, and is waited for with WAIT_LIMIT also after
+// a give-up, so no MMA still writes the accumulator when it is freed); on
+// failure the error flag is set.
 __device__ __forceinline__ bool pipe_wait(const Pipe& p, int nk, int* err)
 {
   __syncthreads();
@@ -281,7 +289,8 @@ __device__ __forceinline__ void pipe_close(const Pipe& p)
 }
 
 __global__ void __launch_bounds__(THREADS, 3)
-k_syrk_tf32x3(int M, int K, const uint32_t* __restrict__ S, float* __restrict__ C, int ldc, int* err)
+k_syrk_tf32x3(int M, int K, const uint32_t* __restrict__ S, float* __restrict__ C, int ldc, int* err,
+              long long limit)
 {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
@@ -296,7 +305,7 @@ k_syrk_tf32x3(int M, int K, const uint32_t* __restrict__ S, float* __restrict__ 
 
   const Pipe p = pipe_open(smem);
   if (tid == 0)
-    pipe_issue(p, smem, S + (size_t)ti * nk * 2 * OPER_WORDS, S + (size_t)tj * nk * 2 * OPER_WORDS, nk);
+    pipe_issue(p, smem, S + (size_t)ti * nk * 2 * OPER_WORDS, S + (size_t)tj * nk * 2 * OPER_WORDS, nk, limit);
   if (pipe_wait(p, nk, err)) {
     const int gr = r0 + 32 * wid + lane;
     for (int grp = 0; grp < TILE / 16; ++grp) {
@@ -353,7 +362,7 @@ __global__ void k_split_tf32_f64(int M, int K, const double* __restrict__ P, int
 // shared by the batch.  Block (tile of M x N, q).
 __global__ void __launch_bounds__(THREADS, 3)
 k_gemm_tf32x3(int M, int N, int K, const uint32_t* __restrict__ Sa, const uint32_t* __restrict__ Sb,
-              double* __restrict__ C, int ldc, long long sC, int* err)
+              double* __restrict__ C, int ldc, long long sC, int* err, long long limit)
 {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
@@ -366,7 +375,7 @@ k_gemm_tf32x3(int M, int N, int K, const uint32_t* __restrict__ Sa, const uint32
   double* Cq = C + (size_t)blockIdx.y * sC;
 
   const Pipe p = pipe_open(smem);
-  if (tid == 0) pipe_issue(p, smem, a, b, nk);
+  if (tid == 0) pipe_issue(p, smem, a, b, nk, limit);
   if (pipe_wait(p, nk, err)) {
     const int gr = r0 + 32 * wid + lane;
     for (int grp = 0; grp < TILE / 16; ++grp) {
@@ -398,8 +407,9 @@ long long gemm_tf32x3_work_bytes(int M, int N, int K, int batch)
 // (16-byte aligned).  Returns a CUDA status; *err (device) is set when a
 // block timed out waiting.
 int gemm_tf32x3(int M, int N, int K, int batch, const double* A, int lda, long long sA, const double* B, int ldb,
-                double* C, int ldc, long long sC, void* work, int* err, cudaStream_t st)
+                double* C, int ldc, long long sC, void* work, int* err, cudaStream_t st, long long wait_polls)
 {
+  const long long limit = (wait_polls < 0) ? tc::WAIT_LIMIT : wait_polls;
   if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return 0;
   static std::atomic<unsigned long long> attr{0};
   cudaError_t e = smem_attr_per_device((const void*)tc::k_gemm_tf32x3, tc::SMEM_BYTES, attr);
@@ -412,15 +422,17 @@ int gemm_tf32x3(int M, int N, int K, int batch, const double* A, int lda, long l
   tc::k_split_tf32_f64<<<dim3((unsigned)((ta + 255) / 256), (unsigned)batch), 256, 0, st>>>(M, K, A, lda, sA, Sa);
   tc::k_split_tf32_f64<<<dim3((unsigned)((tb + 255) / 256), 1), 256, 0, st>>>(N, K, B, ldb, 0, Sb);
   tc::k_gemm_tf32x3<<<dim3((unsigned)(TMt * TNt), (unsigned)batch), tc::THREADS, tc::SMEM_BYTES, st>>>(
-      M, N, K, Sa, Sb, C, ldc, sC, err);
+      M, N, K, Sa, Sb, C, ldc, sC, err, limit);
   return (int)cudaGetLastError();
 }
 
 // C -= P P^T on the lower triangle (M x M, FP32), P M x K; `work` holds
 // syrk_tf32x3_work_bytes(M, K) bytes (16-byte aligned).  Returns a CUDA
 // status; *err (device) is set when a block timed out waiting.
-int syrk_tf32x3(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, int* err, cudaStream_t st)
+int syrk_tf32x3(int M, int K, const float* P, int ldp, float* C, int ldc, void* work, int* err, cudaStream_t st,
+                long long wait_polls)
 {
+  const long long limit = (wait_polls < 0) ? tc::WAIT_LIMIT : wait_polls;
   if (M <= 0 || K <= 0) return 0;
   static std::atomic<unsigned long long> attr{0};
   cudaError_t e = smem_attr_per_device((const void*)tc::k_syrk_tf32x3, tc::SMEM_BYTES, attr);
@@ -430,7 +442,7 @@ int syrk_tf32x3(int M, int K, const float* P, int ldp, float* C, int ldc, void* 
   tc::k_split_tf32<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(M, K, P, ldp, (uint32_t*)work);
   const long long tiles = T * (T + 1) / 2;
   tc::k_syrk_tf32x3<<<(unsigned)tiles, tc::THREADS, tc::SMEM_BYTES, st>>>(M, K, (const uint32_t*)work, C, ldc,
-                                                                          err);
+                                                                          err, limit);
   return (int)cudaGetLastError();
 }
 
@@ -444,9 +456,11 @@ extern "C" SDPAB_API long long sdpab_tc_syrk_work_bytes(int M, int K) { return s
 
 // Stand-alone form (device pointers; no counterpart in the reference): the
 // tensor-core update on `stream`, synchronised, with SDPAB_ECUDA when a
-// block gave up waiting for its MMAs.
+// block gave up waiting for its MMAs.  wait_polls < 0: the default bound of
+// the pipeline's waits; >= 0: that many polls (a block that runs out leaves
+// its tile of C unchanged).
 extern "C" SDPAB_API int sdpab_tc_syrk(int M, int K, const float* P, int ldp, float* C, int ldc, void* work,
-                                       void* stream)
+                                       long long wait_polls, void* stream)
 {
   if (M < 0 || K < 0 || !P || !C || !work || ldp < M || ldc < M)
     return sdpab::set_error(SDPAB_EINVAL, "tc_syrk: bad arguments");
@@ -457,7 +471,7 @@ extern "C" SDPAB_API int sdpab_tc_syrk(int M, int K, const float* P, int ldp, fl
   cudaStream_t st = (cudaStream_t)stream;
   e = cudaMemsetAsync(err, 0, sizeof(int), st);
   if (e != cudaSuccess) return sdpab::cuda_error(e, "tc_syrk: cudaMemsetAsync");
-  const int rc = sdpab::syrk_tf32x3(M, K, P, ldp, C, ldc, work, err, st);
+  const int rc = sdpab::syrk_tf32x3(M, K, P, ldp, C, ldc, work, err, st, wait_polls);
   if (rc != 0) return sdpab::cuda_error((cudaError_t)rc, "tc_syrk: launch");
   int h = 0;
   e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -474,10 +488,10 @@ extern "C" SDPAB_API long long sdpab_tc_gemm_work_bytes(int M, int N, int K, int
 // Stand-alone form of the F1 product kernel (device pointers; no counterpart
 // in the reference, whose F1 products are dgemm calls, sdpa_newton.cpp:
 // 885-889): C_q = A_q B^T on `stream`, synchronised, SDPAB_ECUDA when a block
-// gave up waiting for its MMAs.
+// gave up waiting for its MMAs (wait_polls as for sdpab_tc_syrk).
 extern "C" SDPAB_API int sdpab_tc_gemm(int M, int N, int K, int batch, const double* A, int lda, long long sA,
                                        const double* B, int ldb, double* C, int ldc, long long sC, void* work,
-                                       void* stream)
+                                       long long wait_polls, void* stream)
 {
   if (M < 0 || N < 0 || K < 0 || batch < 0 || !A || !B || !C || !work || lda < M || ldb < N || ldc < M)
     return sdpab::set_error(SDPAB_EINVAL, "tc_gemm: bad arguments");
@@ -488,7 +502,7 @@ extern "C" SDPAB_API int sdpab_tc_gemm(int M, int N, int K, int batch, const dou
   cudaStream_t st = (cudaStream_t)stream;
   e = cudaMemsetAsync(err, 0, sizeof(int), st);
   if (e != cudaSuccess) return sdpab::cuda_error(e, "tc_gemm: cudaMemsetAsync");
-  const int rc = sdpab::gemm_tf32x3(M, N, K, batch, A, lda, sA, B, ldb, C, ldc, sC, work, err, st);
+  const int rc = sdpab::gemm_tf32x3(M, N, K, batch, A, lda, sA, B, ldb, C, ldc, sC, work, err, st, wait_polls);
   if (rc != 0) return sdpab::cuda_error((cudaError_t)rc, "tc_gemm: launch");
   int h = 0;
   e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st);

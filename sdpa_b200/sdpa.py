@@ -43,6 +43,17 @@ class SDPA:
         0 = default 1e-2)."""
         N.check(self._lib.sdpab_sdpa_set_precision(self._h, mode, mu_switch), "setPrecision")
 
+    def setTensorCoreWaitLimit(self, polls: int):
+        """Polls per wait of the mixed mode's tensor-core pipelines (< 0: the
+        default bound); a pipeline that gives up falls back for that iteration."""
+        N.check(self._lib.sdpab_sdpa_set_tc_wait(self._h, int(polls)), "setTensorCoreWaitLimit")
+
+    def tensorCoreTimeouts(self) -> int:
+        """Tensor-core pipelines that gave up during the last solve."""
+        out = ctypes.c_int()
+        N.check(self._lib.sdpab_sdpa_tc_timeouts(self._h, ctypes.byref(out)), "tensorCoreTimeouts")
+        return out.value
+
     def readParameter(self, path: str):
         self.params = N.read_params(path)
 

@@ -21,6 +21,13 @@ def cost(n: int, m: int) -> float:
     return float(m) ** 3 / 3.0 + 14.0 * float(n) ** 3
 
 
+def instance_size(it) -> tuple[int, int]:
+    """(n, m) of an instance for cost(): the batched engine lays all its
+    blocks (SDP and LP) along the diagonal of one matrix of order
+    sum |size| and runs its dense steps on that whole matrix."""
+    return int(sum(abs(int(b)) for b in it.blocks)), int(it.m)
+
+
 def assign(sizes: list[tuple[int, int]], world: int) -> list[list[int]]:
     """Instance indices per rank: longest-processing-time-first dealing by
     cost(n, m).  Deterministic (ties broken by index), so every rank computes
@@ -58,7 +65,7 @@ def solve_sharded(instances, solve_fn=None, group=None, **solve_kw) -> ShardResu
     import torch.distributed as dist
     world = dist.get_world_size(group) if dist.is_initialized() else 1
     rank = dist.get_rank(group) if dist.is_initialized() else 0
-    sizes = [(int(it.blocks[0]), int(it.m)) for it in instances]
+    sizes = [instance_size(it) for it in instances]
     mine = assign(sizes, world)[rank]
     if solve_fn is None:
         from . import batch

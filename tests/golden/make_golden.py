@@ -27,6 +27,9 @@ Fixtures (all from the reference's own output, never hand-written):
                        (seeds 0..511, n ~ U{20..120}): objectives, iterations,
                        phase and x at the default parameters, and x at
                        epsilonStar 1e-11 (x* of the reference-accuracy bar)
+  tcfb.json / tcfb.npz  (also alone with --tcfb) a random SDP with m = 300 and
+                       an order-80 block (the mixed mode's tensor-core paths):
+                       objectives, x, and x at epsilonStar 1e-11
 """
 from __future__ import annotations
 
@@ -295,8 +298,28 @@ def headline_fixtures():
     np.savez_compressed(os.path.join(HERE, "headline.npz"), **arrays)
 
 
+def tc_fallback_fixtures():
+    """Reference results (default and epsilonStar 1e-11 x) of a random SDP
+    large enough for the mixed mode's tensor-core paths (m >= 256, F1
+    constraints in a block of order > 64): the fall-back test of those
+    paths compares with these."""
+    from oracle import ref_runner as R
+    it = inst.random_sdp(m=300, n=80, nlp=6, density=0.1, seed=11)
+    rd = R.run([it], procs=1)
+    rt = R.run([it], procs=1, param=R.PARAM_TIGHT)
+    meta = {"rnd300": {"iterations": int(rd.iterations[0]), "phase": int(rd.phase[0]),
+                       "primal_obj": float(rd.primal_obj[0]), "dual_obj": float(rd.dual_obj[0]),
+                       "generator": "sdpa_b200.instances.random_sdp(m=300, n=80, nlp=6, density=0.1, seed=11)"}}
+    with open(os.path.join(HERE, "tcfb.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+    np.savez_compressed(os.path.join(HERE, "tcfb.npz"), **{"rnd300.xvec": rd.x[0], "rnd300.tight": rt.x[0]})
+
+
 def main():
     large = "--large" in sys.argv
+    if "--tcfb" in sys.argv:
+        tc_fallback_fixtures()
+        return
     if "--headline" in sys.argv:
         headline_fixtures()
         return
@@ -370,6 +393,7 @@ def main():
         block_fixtures(tmp)
         arrow_fixtures()
         headline_fixtures()
+        tc_fallback_fixtures()
 
         if large:
             big = [("lt200", inst.lovasz_theta(200, 0.5, 1)), ("rnd2000", inst.random_sdp(seed=1))]

@@ -78,4 +78,16 @@ def test_result_file_matches_reference_executable(workdir, case):
         assert a.shape == b.shape, key
         assert np.all(np.abs(a - b) <= 2e-3 * np.abs(b) + 1e-5), key
     if ref["dimacs"]:
+        # IO::computeDimacs values, computed on the GPU here
         assert set(ours["dimacs"]) == set(ref["dimacs"])
+        od, rd = ours["dimacs"], ref["dimacs"]
+        # err1, err3: residual norms at the rounding level on both sides
+        for k in ("err1", "err3"):
+            assert od[k] <= 1e-12 and rd[k] <= 1e-12, (k, od[k], rd[k])
+        # err2, err4: zero while X and Z are positive definite
+        for k in ("err2", "err4"):
+            assert abs(od[k] - rd[k]) <= 1e-12, (k, od[k], rd[k])
+        # err5, err6: relative gap and X.Z (= nDim mu) at the final iterate,
+        # within the iteration table's own mu tolerance
+        for k in ("err5", "err6"):
+            assert abs(od[k] - rd[k]) <= 0.02 * abs(rd[k]) + 1e-13, (k, od[k], rd[k])

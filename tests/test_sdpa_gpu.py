@@ -132,6 +132,29 @@ def test_dimacs_errors_small():
     assert d[1] < 1e-7 and d[3] < 1e-7 and abs(d[5]) < 1e-6 and d[2] == 0.0 and d[4] == 0.0
 
 
+@pytest.mark.parametrize("n", [1, 2, 3, 20, 21, 64, 200, 501])
+def test_min_eigenvalue_matches_dense_solver(n):
+    """sdpab_min_eigenvalue (the dsyev minimum of Lal::getMinEigenValue that
+    the DIMACS errors take, computed on the GPU) against numpy's eigvalsh, on
+    random symmetric matrices and on a positive semidefinite one of rank
+    n - 1 (smallest eigenvalue 0)."""
+    import ctypes
+    import torch
+    from sdpa_b200 import _native as N
+    rng = np.random.default_rng(n)
+    G = rng.standard_normal((n, n))
+    V = rng.standard_normal((n, max(n - 1, 1)))
+    for A in (0.5 * (G + G.T), V @ V.T if n > 1 else np.zeros((1, 1))):
+        ref = np.linalg.eigvalsh(A)[0]
+        # only the lower triangle is referenced: spoil the strict upper one
+        Ad = np.tril(A) + np.triu(np.full((n, n), 7.0), 1)
+        dev = torch.from_numpy(np.asfortranarray(Ad).ravel(order="F").copy()).cuda()
+        out = ctypes.c_double()
+        N.check(N.lib().sdpab_min_eigenvalue(n, dev.data_ptr(), ctypes.byref(out), None), "min_eigenvalue")
+        scale = max(1.0, np.abs(np.linalg.eigvalsh(A)).max())
+        assert abs(out.value - ref) <= 1e-12 * scale, (n, out.value, ref)
+
+
 @pytest.mark.parametrize("name", ["lt200", "rnd2000"])
 def test_large_configs_match_reference(name):
     """Lovasz theta G(200, 0.5) (m = 9986, F3, dense 9986^2 Schur) and the random

@@ -65,6 +65,14 @@ def test_assignment_balances_and_covers():
     assert shard.assign(sizes, 3) == a  # deterministic
 
 
+def test_cost_counts_every_block():
+    from sdpa_b200 import instances as I
+    from sdpa_b200 import shard
+    it = I.batch_block_sdp(3)
+    n, m = shard.instance_size(it)
+    assert n == sum(abs(int(b)) for b in it.blocks) and n > abs(int(it.blocks[0])) and m == it.m
+
+
 def test_two_gloo_ranks_match_single_process(tmp_path):
     import torch.multiprocessing as mp
     from sdpa_b200 import shard

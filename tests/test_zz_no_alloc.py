@@ -29,6 +29,12 @@ def test_noalloc_matches_allocating_entry_point():
     ref = db.result()
     assert np.all(ref.phase == 7)
 
+    # drop the allocating path's workspace: the calls below must not grow it
+    # again, nor take any other device memory
+    N.check(N.lib().sdpab_release_workspace(), "sdpab_release_workspace")
+    torch.cuda.synchronize()
+    assert N.lib().sdpab_workspace_bytes() == 0
+    free_before = torch.cuda.mem_get_info()[0]
     prm = N.default_params(0)
     stream = torch.cuda.current_stream().cuda_stream
     for call in range(2):
@@ -47,6 +53,8 @@ def test_noalloc_matches_allocating_entry_point():
         rd = np.abs(got.dual_obj - ref.dual_obj) / np.maximum(1.0, np.abs(ref.dual_obj))
         assert rp.max() < OBJ_TOL and rd.max() < OBJ_TOL, call
         assert np.max(np.abs(got.xvec - ref.xvec)) < X_TOL, call
+    assert N.lib().sdpab_workspace_bytes() == 0
+    assert torch.cuda.mem_get_info()[0] >= free_before
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
