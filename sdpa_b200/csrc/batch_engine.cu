@@ -41,7 +41,7 @@ namespace sdpab {
 // staging area `gsm` (doubles) for GEMM tiles and Lanczos matrices.
 static __host__ __device__ long long fixed_smem_doubles(int nmax, int mmax)
 {
-  return 2 * cta::SD_DOUBLES + 4 * (NT / 32) + 4LL * mmax + eig_scratch_doubles(nmax);
+  return 2 * cta::SD_DOUBLES + 4 * (NT / 32) + 4LL * mmax + (long long)nmax + eig_scratch_doubles(nmax);
 }
 
 static size_t smem_bytes_for(int nmax, int mmax, long long gsm)
@@ -308,10 +308,11 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
   double* vdy = vy + mmax;                              // dy  (mmax)
   double* vg = vdy + mmax;                              // g   (mmax)
   double* vrp = vg + mmax;                              // r_p (mmax)
+  double* vdz = vrp + mmax;                             // dZ when it is diagonal (nmax)
   cta::Reducer RD{redbuf, 0};
   EigScratch es;
-  eig_scratch_carve(es, vrp + mmax, nmax, &RD);          // eig_scratch_doubles(nmax)
-  int* s_nnz = (int*)(vrp + mmax + eig_scratch_doubles(nmax));  // mmax ints
+  eig_scratch_carve(es, vdz + nmax, nmax, &RD);          // eig_scratch_doubles(nmax)
+  int* s_nnz = (int*)(vdz + nmax + eig_scratch_doubles(nmax));  // mmax ints
   int* s_bid = s_nnz + mmax;  // nmax ints: block of each row (-1 = LP entry)
   int* s_form = s_bid + nmax;  // mmax ints: 1 = constraint's Schur column by F1
 
@@ -653,21 +654,32 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
           schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, dX, B, s_nnz, s_form, 0, nullptr, nullptr, nullptr, gsm);
       }
       // ---- adjusted Cholesky and solve (compute_DyVec, sdpa_newton.cpp:2672-2716)
-      if (cta::cholesky<NT, double>(m, B, m, true, sD, gsm, &s_flag)) break;
+      if (cta::cholesky<NT, double>(m, B, m, true, sD, gsm, &s_flag, false)) break;  // solves read the lower triangle
       for (int k = tid; k < m; k += NT) vdy[k] = vg[k];
       __syncthreads();
       cta::chol_solve<NT, double>(m, B, m, vdy, sD);
 
-      // ---- dZ, dX (compute_DzMat / compute_DxMat, sdpa_newton.cpp:2718-2752)
+      // ---- dZ, dX (compute_DzMat / compute_DxMat, sdpa_newton.cpp:2718-2752).
+      // With every constraint diagonal and the point dual feasible, dZ =
+      // -sum dy_k A_k is diagonal: it is kept as the vector vdz (the full
+      // matrix dZ is not written), X dZ is a column scaling, and the inner
+      // products and the update with dZ touch the diagonal only.
       auto direction = [&]() {
-        for (int t = tid; t < nn_i; t += NT) dZ[t] = dinf ? D[t] : 0.0;
-        __syncthreads();
-        sp_axpy_constraints(er, ec, ev, mp, m, vdy, -1.0, dZ, n);
-        __syncthreads();
         if (dz_diag) {
-          for (int t = tid; t < nn_i; t += NT) W1[t] = X[t] * dZ[(t / n) * (n + 1)];
+          for (int t = tid; t < n; t += NT) vdz[t] = 0.0;
+          __syncthreads();
+          for (int k = tid; k < m; k += NT) {
+            const double s = -vdy[k];
+            for (long long e = mp[k + 1]; e < mp[k + 2]; ++e) atomicAdd(&vdz[er[e]], s * ev[e]);
+          }
+          __syncthreads();
+          for (int t = tid; t < nn_i; t += NT) W1[t] = X[t] * vdz[t / n];
           __syncthreads();
         } else {
+          for (int t = tid; t < nn_i; t += NT) dZ[t] = dinf ? D[t] : 0.0;
+          __syncthreads();
+          sp_axpy_constraints(er, ec, ev, mp, m, vdy, -1.0, dZ, n);
+          __syncthreads();
           cta::gemm_prec<NT, double>(n, false, X, n, false, dZ, n, W1, n, 1.0, 0.0, gsm, lowp);
         }
         cta::gemm_prec<NT, double>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm, lowp);
@@ -683,13 +695,20 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         }
         __syncthreads();
       };
+      // A . dZ (A = X or dX): the diagonal only when dZ is diagonal
+      auto dot_dz = [&](const double* A) {
+        if (!dz_diag) return cta::dot_mat<NT>(n, A, dZ, RD);
+        double s = 0.0;
+        for (int t = tid; t < n; t += NT) s += A[t * (n + 1)] * vdz[t];
+        return cta::block_sum<NT>(s, RD);
+      };
       direction();
       {
         double CdX = c_dot(dX);
         double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);
-        double xdz = cta::dot_mat<NT>(n, X, dZ, RD);
+        double xdz = dot_dz(X);
         double dxz = cta::dot_mat<NT>(n, dX, Z, RD);
-        double dxdz = cta::dot_mat<NT>(n, dX, dZ, RD);
+        double dxdz = dot_dz(dX);
         if (tid == 0) {
           predictor_step(S, CdX, bdy);
           corrector_beta(S, P, xdz, dxz, dxdz);
@@ -701,7 +720,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       {
         const double bm2 = S.beta * S.mu;
         if (dz_diag) {
-          for (int t = tid; t < nn_i; t += NT) W1[t] = dX[t] * dZ[(t / n) * (n + 1)];
+          for (int t = tid; t < nn_i; t += NT) W1[t] = dX[t] * vdz[t / n];
           __syncthreads();
         } else {
           cta::gemm_prec<NT, double>(n, false, dX, n, false, dZ, n, W1, n, 1.0, 0.0, gsm, lowp);
@@ -724,17 +743,18 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       {
         // R and XDZ are free here (both are rebuilt by the next predictor)
         double mins[2];
+        const double* DZ = dz_diag ? vdz : dZ;  // the diagonal vector when dZ is diagonal
         if (GENERAL && blocked)
-          min_eig_pair_blocks(n, s_nb, s_boff, s_bsz, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es,
+          min_eig_pair_blocks(n, s_nb, s_boff, s_bsz, LXi, dX, LZi, DZ, W1, W2, R, XDZ, gsm, gsm_doubles, es,
                               mins, dz_diag);
         else
-          min_eig_pair(n, LXi, dX, LZi, dZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins, dz_diag);
+          min_eig_pair(n, LXi, dX, LZi, DZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins, dz_diag);
         const double minX = mins[0], minZ = mins[1];
         double CdX = c_dot(dX);
         double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);
-        double xdz = cta::dot_mat<NT>(n, X, dZ, RD);
+        double xdz = dot_dz(X);
         double dxz = cta::dot_mat<NT>(n, dX, Z, RD);
-        double dxdz = cta::dot_mat<NT>(n, dX, dZ, RD);
+        double dxdz = dot_dz(dX);
         if (tid == 0) corrector_step(S, P, minX, minZ, CdX, bdy, xdz, dxz, dxdz, S.objD, S.objP);
         __syncthreads();
       }
@@ -742,17 +762,22 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       // ---- update (Solutions::update, sdpa_dataset.cpp:145-171)
       {
         const double ap = S.alphaP, ad = S.alphaD;
+        // X += ap dX, Z += ad dZ, and the copies the factorisations work on
         for (int t = tid; t < nn_i; t += NT) {
-          X[t] += ap * dX[t];
-          Z[t] += ad * dZ[t];
+          const double x = X[t] + ap * dX[t];
+          double z = Z[t];
+          if (!dz_diag) z += ad * dZ[t];
+          else if ((t % n) == (t / n)) z += ad * vdz[t / n];
+          X[t] = x;
+          Z[t] = z;
+          W2[t] = x;
+          W1[t] = z;
         }
         for (int k = tid; k < m; k += NT) vy[k] += ad * vdy[k];
         __syncthreads();
-        for (int t = tid; t < nn_i; t += NT) { W2[t] = X[t]; W1[t] = Z[t]; }
-        __syncthreads();
         if (cannot_move(S)) break;
         // X and Z factored and inverted in lockstep (either failing ends the loop)
-        if (cta::cholesky_pair<NT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2)) break;
+        if (cta::cholesky_pair<NT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false)) break;  // inverses read the lower triangles
         cta::tri_inverse_pair<NT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
         cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }

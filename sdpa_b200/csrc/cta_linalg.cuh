@@ -648,10 +648,11 @@ static __device__ __noinline__ int warp_potrf32(int bs, T* sD, bool adjust, int 
 // ------------------------------------------------------------ Cholesky
 // In-place lower Cholesky, right-looking, blocked by 32, pivot rules as
 // warp_potrf32.  Returns 0 on success, else the failing column + 1.  The
-// strict upper triangle is zeroed on success.  sD: SD_DOUBLES elements of T;
-// smem: GEMM staging.
+// strict upper triangle is zeroed on success when zero_upper is set (callers
+// that only read the lower triangle skip that pass).  sD: SD_DOUBLES
+// elements of T; smem: GEMM staging.
 template <int NT, typename T>
-__device__ int cholesky(int n, T* A, int lda, bool adjust, T* sD, void* smem, int* s_flag)
+__device__ int cholesky(int n, T* A, int lda, bool adjust, T* sD, void* smem, int* s_flag, bool zero_upper = true)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   for (int kb = 0; kb < n; kb += NB) {
@@ -704,11 +705,13 @@ __device__ int cholesky(int n, T* A, int lda, bool adjust, T* sD, void* smem, in
                           smem, true, 0);
     }
   }
-  for (int t = tid; t < n * n; t += NT) {
-    const int i = t % n, k = t / n;
-    if (i < k) A[i + (size_t)lda * k] = (T)0;
+  if (zero_upper) {
+    for (int t = tid; t < n * n; t += NT) {
+      const int i = t % n, k = t / n;
+      if (i < k) A[i + (size_t)lda * k] = (T)0;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   return 0;
 }
 
@@ -765,8 +768,10 @@ __device__ void tri_inverse(int n, const T* L, int ldl, T* Li, int ldi, T* sD, v
 // the trailing updates follow each other.  Used for X and Z in the update
 // step.  sD0, sD1: SD_DOUBLES elements of T each.  Returns 0 when both
 // succeed, else nonzero (both matrices are then left partially factored).
+// The strict upper triangles are zeroed when zero_upper is set.
 template <int NT, typename T>
-__device__ int cholesky_pair(int n, T* A0, T* A1, int lda, T* sD0, T* sD1, void* smem, int* s_flag2)
+__device__ int cholesky_pair(int n, T* A0, T* A1, int lda, T* sD0, T* sD1, void* smem, int* s_flag2,
+                             bool zero_upper = true)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   T* Am[2] = {A0, A1};
@@ -828,12 +833,14 @@ __device__ int cholesky_pair(int n, T* A0, T* A1, int lda, T* sD0, T* sD1, void*
       }
     }
   }
-  for (int t = tid; t < 2 * n * n; t += NT) {
-    const int mtx = t / (n * n), u = t % (n * n);
-    const int i = u % n, k = u / n;
-    if (i < k) Am[mtx][i + (size_t)lda * k] = (T)0;
+  if (zero_upper) {
+    for (int t = tid; t < 2 * n * n; t += NT) {
+      const int mtx = t / (n * n), u = t % (n * n);
+      const int i = u % n, k = u / n;
+      if (i < k) Am[mtx][i + (size_t)lda * k] = (T)0;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   return 0;
 }
 

@@ -300,7 +300,8 @@ static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
 // with the two Lanczos processes in lockstep.
 // Wx1, Wx2, Wz1, Wz2: n x n scratch (Wx2 and Wz2 receive the formed
 // matrices).  The matrices are staged in shared memory while they fit.
-// z_diag: Dz is diagonal, so Dz Lz^T is a row scaling of Lz^T (no GEMM).
+// z_diag: Dz is diagonal and given as the vector of its diagonal (n values),
+// so Dz Lz^T is a row scaling of Lz^T (no GEMM).
 // Wx2 = Lx Dx Lx^T and Wz2 = Lz Dz Lz^T (Wx1, Wz1 scratch).
 static __device__ void form_ldlt_pair(int n, const double* Lx, const double* Dx, const double* Lz,
                                       const double* Dz, double* Wx1, double* Wx2, double* Wz1, double* Wz2,
@@ -311,7 +312,7 @@ static __device__ void form_ldlt_pair(int n, const double* Lx, const double* Dx,
   if (z_diag) {
     for (int t = threadIdx.x; t < n * n; t += NT) {
       const int i = t % n, j = t / n;
-      Wz1[t] = Dz[i + (size_t)n * i] * Lz[j + (size_t)n * i];
+      Wz1[t] = Dz[i] * Lz[j + (size_t)n * i];
     }
     __syncthreads();
   } else {
