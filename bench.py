@@ -220,6 +220,11 @@ def fp64_peak():
     return 2.0 * n ** 3 / (best / 1e3) / 1e12
 
 
+def fixed_shape(args) -> dict:
+    """The launch shape given on the command line (0 = the library default)."""
+    return {"ctas_per_sm": args.ctas_per_sm, "block_threads": args.block_threads}
+
+
 def _events_time(fn, stream, steps, flush):
     """Device time (ms) of fn() per step, CUDA events on `stream`, L2 flushed
     (256 MB written) before every step."""
@@ -263,10 +268,10 @@ def run_blocks(args):
     db = batch.DeviceBatch(P)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.Stream()
-    cand = (args.ctas_per_sm,) if args.ctas_per_sm > 0 else (1, 2)
+    cand = [fixed_shape(args)] if (args.ctas_per_sm > 0 or args.block_threads > 0) else None
     tune = autotune.tune(db, N.PREC_FP64, stream=stream, candidates=cand)
     c = tune["best"]
-    run = lambda: db.solve(precision=N.PREC_FP64, stream=stream, ctas_per_sm=c)
+    run = lambda: db.solve(precision=N.PREC_FP64, stream=stream, **c)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             run()
@@ -303,7 +308,7 @@ def run_blocks(args):
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no public suite)",
             "config": {"workload": BLOCK_WORKLOAD, "count_per_gpu": args.count, "precision": "fp64",
-                       "warm_start": False, "ctas_per_sm": c, "autotune_ms": tune["ms"],
+                       "warm_start": False, "launch_shape": c, "autotune_ms": tune["ms"],
                        "l2": "256 MB buffer written between timed steps", "parallelism": "replicas x1"},
             "e2e": {"value": P.count / float(np.mean(e2e_t)), "unit": "SDPs/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
@@ -336,6 +341,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--ctas-per-sm", type=int, default=0, help="fixed launch shape (0 = autotune)")
+    ap.add_argument("--block-threads", type=int, default=0, help="fixed threads per instance, 256 or 128 (0 = autotune)")
     ap.add_argument("--workload", default="maxcut", choices=["maxcut", "blocks"])
     ap.add_argument("--profile", action="store_true",
                     help="only launch the headline pipeline warmup + steps times, untimed (for ncu captures)")
@@ -380,9 +386,9 @@ def main():
         pp = W.WarmPipeline(W.default_model(), graphs, dbp) if args.warm else None
         for _ in range(args.warmup + args.steps):
             if pp is not None:
-                pp.run(precision=prec, stream=stream, ctas_per_sm=args.ctas_per_sm)
+                pp.run(precision=prec, stream=stream, **fixed_shape(args))
             else:
-                dbp.solve(precision=prec, stream=stream, ctas_per_sm=args.ctas_per_sm)
+                dbp.solve(precision=prec, stream=stream, **fixed_shape(args))
         barrier()
         r = dbp.result()
         if rank == 0:
@@ -394,20 +400,20 @@ def main():
 
     # ---- plain FP64 path (standard start): the denominator of the headline ratio
     db0 = batch.DeviceBatch(P)
-    cand = (args.ctas_per_sm,) if args.ctas_per_sm > 0 else (1, 2)
+    cand = [fixed_shape(args)] if (args.ctas_per_sm > 0 or args.block_threads > 0) else None
     tune0 = autotune.tune(db0, N.PREC_FP64, stream=stream, candidates=cand)
     c0 = tune0["best"]
-    run0 = lambda: db0.solve(precision=N.PREC_FP64, stream=stream, ctas_per_sm=c0)
+    run0 = lambda: db0.solve(precision=N.PREC_FP64, stream=stream, **c0)
     # ---- headline path: precision + learned warm start
     dbh = batch.DeviceBatch(P)
     pipe = W.WarmPipeline(W.default_model(), graphs, dbh) if args.warm else None
     tuneh = autotune.tune(dbh, prec, stream=stream, candidates=cand,
-                          run=(lambda c: pipe.run(precision=prec, stream=stream, ctas_per_sm=c)) if pipe else None)
+                          run=(lambda c: pipe.run(precision=prec, stream=stream, **c)) if pipe else None)
     ch = tuneh["best"]
     if pipe is not None:
-        runh = lambda: pipe.run(precision=prec, stream=stream, ctas_per_sm=ch)
+        runh = lambda: pipe.run(precision=prec, stream=stream, **ch)
     else:
-        runh = lambda: dbh.solve(precision=prec, stream=stream, ctas_per_sm=ch)
+        runh = lambda: dbh.solve(precision=prec, stream=stream, **ch)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -435,10 +441,11 @@ def main():
     alt = None
     if pipe is not None:
         aprec = N.PREC_FP64 if prec == N.PREC_MIXED else N.PREC_MIXED
+        ach = {k: v for k, v in ch.items() if k != "mixed_products"}
         with torch.cuda.stream(stream):
             for _ in range(2):
-                pipe.run(precision=aprec, stream=stream, ctas_per_sm=ch)
-            ta = _events_time(lambda: pipe.run(precision=aprec, stream=stream, ctas_per_sm=ch), stream,
+                pipe.run(precision=aprec, stream=stream, **ach)
+            ta = _events_time(lambda: pipe.run(precision=aprec, stream=stream, **ach), stream,
                               args.steps, flush)
         barrier()
         ra = dbh.result()
@@ -513,7 +520,8 @@ def main():
             "data": "synthetic (seeded generator, no public suite)",
             "config": {"workload": WORKLOAD, "count_per_gpu": args.count, "precision": args.precision,
                        "warm_start": bool(args.warm), "cuda_graph": gh is not None,
-                       "ctas_per_sm": {"headline": ch, "plain_fp64": c0, "autotune_ms": tuneh["ms"]},
+                       "launch_shape": {"headline": ch, "plain_fp64": c0, "autotune_ms_headline": tuneh["ms"],
+                                        "autotune_ms_plain_fp64": tune0["ms"]},
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": f"replicas x{world} (independent instances per GPU)"},
             "plain_fp64": {"value": plain_value, "unit": "SDPs/s", "ms_per_step": plain_ms_max,

@@ -222,11 +222,15 @@ SDPAB_API int sdpab_mpnn_propose_x(int num_nodes, const float* r, const double* 
 #define SDPAB_PREC_FP64 0    /* every step in FP64 (the plain path) */
 #define SDPAB_PREC_MIXED_SIMT 2   /* host-driven solver: mixed without tensor cores (comparison) */
 #define SDPAB_PREC_MIXED 1   /* while nDim * mu / max(1, mean |objective|) >=
-                                mixed_switch_gap: bulk products in FP32 (FP32 accumulation), and in
-                                the host-driven solver the Schur Cholesky in FP32 with
-                                FP64 refinement of dy; FP64 residuals, gap, Lanczos step
+                                mixed_switch_gap: the Schur Cholesky in FP32 with FP64
+                                iterative refinement of dy (predictor and corrector
+                                solves), and bulk products in FP32 (FP32 accumulation;
+                                in the batched solver only with mixed_products = 1, else
+                                on the FP64 MMA); FP64 residuals, gap, Lanczos step
                                 length and factorisations of X and Z; everything FP64
-                                once mu falls below that point */
+                                once mu falls below that point, and in the batched
+                                solver also once an FP32 factor fails or a refinement
+                                does not converge in three steps */
 
 typedef struct sdpab_batch {
   int count;                   /* number of instances */
@@ -297,12 +301,18 @@ typedef struct sdpab_batch_result {
 
 typedef struct sdpab_batch_config {
   int precision;               /* SDPAB_PREC_FP64 or SDPAB_PREC_MIXED */
-  int ctas_per_sm;             /* resident solver blocks per SM (0 = auto) */
+  int ctas_per_sm;             /* resident solver blocks per SM (0 = 2 of 256 threads,
+                                  4 of 128) */
   double mixed_switch_gap;     /* mixed mode: FP64 once nDim * mu / max(1, mean
                                   |objective|) < this (0 = 1e-2) */
   int staging_doubles;         /* shared-memory staging of GEMM tiles and Lanczos
                                   matrices per solver block, in doubles (0 = auto;
                                   raised to the GEMM minimum of 6400) */
+  int mixed_products;          /* mixed mode: the n^3 products of the FP32 phase in
+                                  FP32 (1) or on the FP64 MMA (0) */
+  int block_threads;           /* threads per solver block (one instance in flight
+                                  each): 256 (0 = default) or 128; with 128, four
+                                  blocks share an SM by default */
 } sdpab_batch_config;
 
 /* Tensor-core lower update C -= P P^T of an M x M FP32 matrix, P M x K

@@ -37,33 +37,46 @@
 
 namespace sdpab {
 
-// Dynamic shared memory of the solver block, in doubles / bytes, given the
-// staging area `gsm` (doubles) for GEMM tiles and Lanczos matrices.
-static __host__ __device__ long long fixed_smem_doubles(int nmax, int mmax)
+// Dynamic shared memory of the solver block (bt threads), in doubles /
+// bytes, given the staging area `gsm` (doubles) for GEMM tiles, Lanczos
+// matrices and the diagonal blocks of the factorisations.
+static __host__ __device__ long long fixed_smem_doubles(int nmax, int mmax, int bt)
 {
-  return 2 * cta::SD_DOUBLES + 4 * (NT / 32) + 4LL * mmax + (long long)nmax + eig_scratch_doubles(nmax);
+  return 4 * (bt / 32) + 6LL * mmax + (long long)nmax + eig_scratch_doubles(nmax);
 }
 
-static size_t smem_bytes_for(int nmax, int mmax, long long gsm)
+static size_t smem_bytes_for(int nmax, int mmax, long long gsm, int bt)
 {
-  return (size_t)(gsm + fixed_smem_doubles(nmax, mmax)) * sizeof(double) +
+  return (size_t)(gsm + fixed_smem_doubles(nmax, mmax, bt)) * sizeof(double) +
          (size_t)(2 * mmax + nmax) * sizeof(int) + 64;
 }
 
-// Staging area: at least the double-buffered single-tile GEMM (n <= 96).  `want`
-// doubles when given (capped at what one block can have); by default both
-// Lanczos matrices (2 n^2) when they fit in LANCZOS_SMEM_DOUBLES, else one,
-// else the GEMM minimum.
-static long long staging_doubles(int nmax, int mmax, int want)
+// Shared memory of one SM and what the system reserves per resident block.
+constexpr long long SM_SMEM_BYTES = 228LL * 1024, BLOCK_RESERVED_BYTES = 1024;
+
+// Staging area for `per_sm` resident blocks of bt threads: at least the
+// square GEMM's double-buffered tiles (cta::gemm_smem_min) and the two
+// diagonal blocks; `want` doubles when given, by default both Lanczos
+// matrices (2 n^2) when they fit in LANCZOS_SMEM_DOUBLES, else one, else
+// the minimum; capped at what per_sm blocks of this size can have.
+static long long staging_min(int bt)
 {
-  const long long g = 4 * 16 * 100;  // double-buffered single-tile GEMM (n <= 96, rows padded to 100)
+  const long long g = (bt >= 256) ? cta::gemm_smem_min<256>() : cta::gemm_smem_min<128>();
+  return std::max<long long>(g, 2 * cta::SD_DOUBLES);
+}
+
+static long long staging_doubles(int nmax, int mmax, int want, int bt, int per_sm)
+{
+  const long long g = staging_min(bt);
   const long long m2 = (long long)nmax * nmax;
   long long s;
   if (want > 0) s = want;
   else if (2 * m2 <= LANCZOS_SMEM_DOUBLES) s = 2 * m2;
   else if (m2 <= LANCZOS_SMEM_DOUBLES) s = m2;
   else s = g;
-  const long long cap = (227LL * 1024 - 2048 - (long long)smem_bytes_for(nmax, mmax, 0)) / (long long)sizeof(double);
+  const long long per_block = std::min<long long>(227LL * 1024, SM_SMEM_BYTES / std::max(per_sm, 1) -
+                                                                    BLOCK_RESERVED_BYTES);
+  const long long cap = (per_block - (long long)smem_bytes_for(nmax, mmax, 0, bt)) / (long long)sizeof(double);
   if (s > cap) s = cap;
   s = s / 32 * 32;
   return s > g ? s : g;
@@ -76,7 +89,8 @@ struct BatchArgs {
   Params prm;
   const int* order;
   int gsm_doubles;        // staging area (doubles) at the head of dynamic shared memory
-  int mixed;             // SDPAB_PREC_MIXED: bulk GEMMs in FP32 while mixed_gap >= mu_switch
+  int mixed;             // SDPAB_PREC_MIXED: FP32 Schur factor + FP64 refinement while mixed_gap >= mu_switch
+  int mixed_products;    // mixed mode: the n^3 products in FP32 as well (else on the FP64 MMA)
   double mu_switch;
   double* ws;
   long long ws_stride;  // doubles per block
@@ -100,11 +114,12 @@ __device__ __forceinline__ double sp_dot(const int* row, const int* col, const d
 }
 
 // W += scale * A (both triangles), block-parallel over entries.
+template <int BT>
 __device__ __forceinline__ void sp_axpy_block(const int* row, const int* col, const double* val,
                                               long long beg, long long end, double scale, double* W,
                                               int ld)
 {
-  for (long long e = beg + threadIdx.x; e < end; e += NT) {
+  for (long long e = beg + threadIdx.x; e < end; e += BT) {
     int r = row[e], c = col[e];
     double v = scale * val[e];
     atomicAdd(&W[r + (size_t)ld * c], v);
@@ -115,12 +130,13 @@ __device__ __forceinline__ void sp_axpy_block(const int* row, const int* col, co
 // W += scale * sum_k coef[k] A_k, one thread per constraint
 // (InputData::multi_plusToA, sdpa_dataset.cpp:427-433).  mp points at the
 // instance's F0 pointer; A_k is matrix k+1.
+template <int BT>
 __device__ __forceinline__ void sp_axpy_constraints(const int* row, const int* col,
                                                     const double* val, const long long* mp, int m,
                                                     const double* coef, double scale, double* W,
                                                     int ld)
 {
-  for (int k = threadIdx.x; k < m; k += NT) {
+  for (int k = threadIdx.x; k < m; k += BT) {
     const double s = scale * coef[k];
     for (long long e = mp[k + 1]; e < mp[k + 2]; ++e) {
       int r = row[e], c = col[e];
@@ -181,10 +197,11 @@ __device__ __forceinline__ double f3_value(const int* row, const int* col, const
 // k x k matrix and T = X_b A_b is a tiled block product like G = T Z^-1.
 // Larger blocks and a single block: one thread per row of T, accumulating
 // over the entries.
+template <int BT>
 static __device__ void f1_rows(int n, int r0, int k, long long jb, long long je, const int* er, const int* ec,
                                const double* ev, const double* X, double* T)
 {
-  for (int i = r0 + (int)threadIdx.x; i < r0 + k; i += NT) {
+  for (int i = r0 + (int)threadIdx.x; i < r0 + k; i += BT) {
     for (int c = r0; c < r0 + k; ++c) T[i + (size_t)n * c] = 0.0;
     for (long long e = jb; e < je; ++e) {
       const int r = er[e], c = ec[e];
@@ -196,6 +213,7 @@ static __device__ void f1_rows(int n, int r0, int k, long long jb, long long je,
   }
 }
 
+template <int BT>
 static __device__ __noinline__ void schur_f1(int n, int m, const long long* mp, const int* er, const int* ec,
                                              const double* ev, const double* X, const double* Zi, double* T,
                                              double* G, double* Ad, double* B, const int* nnz, const int* form,
@@ -207,15 +225,15 @@ static __device__ __noinline__ void schur_f1(int n, int m, const long long* mp, 
     if (!form[j]) continue;
     const long long jb = mp[j + 1], je = mp[j + 2];
     if (nb <= 0) {
-      f1_rows(n, 0, n, jb, je, er, ec, ev, X, T);
+      f1_rows<BT>(n, 0, n, jb, je, er, ec, ev, X, T);
       __syncthreads();
-      cta::gemm<NT>(n, false, T, n, false, Zi, n, G, n, 1.0, 0.0, gsm);
+      cta::gemm<BT>(n, false, T, n, false, Zi, n, G, n, 1.0, 0.0, gsm);
     } else {
       // blocks touched by A_j
       if (tid == 0) s_touch = 0ull;
       __syncthreads();
       unsigned long long mine = 0ull;
-      for (long long e = jb + tid; e < je; e += NT) {
+      for (long long e = jb + tid; e < je; e += BT) {
         const int b = bid[er[e]];
         if (b >= 0) mine |= 1ull << b;
       }
@@ -227,12 +245,12 @@ static __device__ __noinline__ void schur_f1(int n, int m, const long long* mp, 
         if (k >= 2) {
           if (!((touch >> l) & 1ull)) continue;
           if (k > 64) {
-            f1_rows(n, o, k, jb, je, er, ec, ev, X, T);
+            f1_rows<BT>(n, o, k, jb, je, er, ec, ev, X, T);
             continue;
           }
-          for (int t = tid; t < k * k; t += NT) Ad[t] = 0.0;
+          for (int t = tid; t < k * k; t += BT) Ad[t] = 0.0;
           __syncthreads();
-          for (long long e = jb + tid; e < je; e += NT) {
+          for (long long e = jb + tid; e < je; e += BT) {
             const int r = er[e] - o, c = ec[e] - o;
             if (r < 0 || r >= k) continue;
             Ad[r + k * c] = ev[e];
@@ -240,10 +258,10 @@ static __device__ __noinline__ void schur_f1(int n, int m, const long long* mp, 
           }
           __syncthreads();
           const size_t od = (size_t)o * (n + 1);
-          cta::gemm<NT>(k, false, X + od, n, false, Ad, k, T + od, n, 1.0, 0.0, gsm);
+          cta::gemm<BT>(k, false, X + od, n, false, Ad, k, T + od, n, 1.0, 0.0, gsm);
         } else {
           // LP entries: G_tt = (sum of A_j's entries at (t, t)) X_tt Z^-1_tt
-          for (int t = tid; t < -k; t += NT) {
+          for (int t = tid; t < -k; t += BT) {
             const int d = o + t;
             double a = 0.0;
             for (long long e = jb; e < je; ++e) a += (er[e] == d) ? ev[e] : 0.0;
@@ -259,16 +277,16 @@ static __device__ __noinline__ void schur_f1(int n, int m, const long long* mp, 
         if (k < 2) continue;
         const size_t o = (size_t)boff[l] * (n + 1);
         if ((touch >> l) & 1ull) {
-          cta::gemm<NT>(k, false, T + o, n, false, Zi + o, n, G + o, n, 1.0, 0.0, gsm);
+          cta::gemm<BT>(k, false, T + o, n, false, Zi + o, n, G + o, n, 1.0, 0.0, gsm);
         } else {
-          for (int t = tid; t < k * k; t += NT) G[o + (size_t)(t % k) + (size_t)n * (t / k)] = 0.0;
+          for (int t = tid; t < k * k; t += BT) G[o + (size_t)(t % k) + (size_t)n * (t / k)] = 0.0;
         }
       }
     }
     __syncthreads();
     // B_ij = A_i . G for the i dominated by j, one warp per i
     const int jnz = nnz[j];
-    for (int i = wid; i < m; i += NT / 32) {
+    for (int i = wid; i < m; i += BT / 32) {
       const int inz = nnz[i];
       if (jnz < inz || (inz == jnz && i < j)) continue;
       double s = 0.0;
@@ -294,25 +312,30 @@ static __device__ __noinline__ void schur_f1(int n, int m, const long long* mp, 
 // Schur columns for constraints with many entries.  The other instantiation
 // (single SDP block, every Schur entry by F3) has none of that bookkeeping,
 // so the MaxCut-like common case keeps its register allocation.
-template <bool GENERAL>
-__global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
+template <bool GENERAL, int BT>
+__global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
 {
   extern __shared__ double smem[];
   const int nmax = a.p.nmax, mmax = a.p.mmax;
   const int gsm_doubles = a.gsm_doubles;
-  double* gsm = smem;                                   // GEMM staging / Lanczos matrix
-  double* sD = gsm + gsm_doubles;                       // diagonal block NB*LDD
+  // GEMM staging / Lanczos matrices; the diagonal blocks of the blocked
+  // factorisations and solves share it (they are dead while a GEMM or a
+  // Lanczos process uses it: every such call starts and ends at a barrier)
+  double* gsm = smem;
+  double* sD = gsm;                                     // diagonal block NB*LDD
   double* sD2 = sD + cta::SD_DOUBLES;                   // second diagonal block (paired X / Z steps)
-  double* redbuf = sD2 + cta::SD_DOUBLES;               // 4 * NT/32
-  double* vy = redbuf + 4 * (NT / 32);                  // y   (mmax)
+  double* redbuf = gsm + gsm_doubles;                   // 4 * BT/32
+  double* vy = redbuf + 4 * (BT / 32);                  // y   (mmax)
   double* vdy = vy + mmax;                              // dy  (mmax)
   double* vg = vdy + mmax;                              // g   (mmax)
   double* vrp = vg + mmax;                              // r_p (mmax)
   double* vdz = vrp + mmax;                             // dZ when it is diagonal (nmax)
+  double* vres = vdz + nmax;                            // refinement residual (mmax)
+  float* x32 = (float*)(vres + mmax);                   // FP32 solve vector (mmax floats)
   cta::Reducer RD{redbuf, 0};
   EigScratch es;
-  eig_scratch_carve(es, vdz + nmax, nmax, &RD);          // eig_scratch_doubles(nmax)
-  int* s_nnz = (int*)(vdz + nmax + eig_scratch_doubles(nmax));  // mmax ints
+  eig_scratch_carve(es, vres + 2 * mmax, nmax, &RD);     // eig_scratch_doubles(nmax)
+  int* s_nnz = (int*)(vres + 2 * mmax + eig_scratch_doubles(nmax));  // mmax ints
   int* s_bid = s_nnz + mmax;  // nmax ints: block of each row (-1 = LP entry)
   int* s_form = s_bid + nmax;  // mmax ints: 1 = constraint's Schur column by F1
 
@@ -339,6 +362,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
   double* X0 = W2 + nn;
   double* Z0 = X0 + nn;
   double* B = Z0 + nn;  // mmax * mmax
+  float* B32 = (float*)(B + (size_t)mmax * mmax);  // mixed mode: FP32 factor of B (mmax * mmax floats)
 
   for (;;) {
     if (tid == 0) s_inst = atomicAdd(a.queue, 1);
@@ -383,7 +407,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       }
       for (int l = 0; l < s_nb; ++l) {
         const int sz = s_bsz[l], cnt = (sz < 0) ? -sz : sz;
-        for (int t = tid; t < cnt; t += NT) s_bid[s_boff[l] + t] = (sz >= 2) ? l : -1;
+        for (int t = tid; t < cnt; t += BT) s_bid[s_boff[l] + t] = (sz >= 2) ? l : -1;
       }
       __syncthreads();
       blocked = !(s_nb == 1 && s_bsz[0] == n);
@@ -392,7 +416,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
     // instance otherwise
     {
       int bad = 0;
-      for (long long e = mp[0] + tid; e < mp[m + 1]; e += NT) {
+      for (long long e = mp[0] + tid; e < mp[m + 1]; e += BT) {
         const int r = er[e], c = ec[e];
         const bool out = (r < 0 || c < 0 || r >= n || c >= n);
         bad |= out;
@@ -405,10 +429,10 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
     }
     // all constraint entries on the diagonal?
     int offdiag = 0;
-    for (long long e = mp[1] + tid; e < mp[m + 1]; e += NT) offdiag |= (er[e] != ec[e]);
+    for (long long e = mp[1] + tid; e < mp[m + 1]; e += BT) offdiag |= (er[e] != ec[e]);
     const bool diag_cons = !__syncthreads_or(offdiag);
     // NonZeroEffect per constraint (diagonal 1, off-diagonal 2; sdpa_struct.cpp:1339-1341)
-    for (int k = tid; k < m; k += NT) {
+    for (int k = tid; k < m; k += BT) {
       int c = 0;
       for (long long e = mp[k + 1]; e < mp[k + 2]; ++e) c += (er[e] == ec[e]) ? 1 : 2;
       s_nnz[k] = c;
@@ -432,7 +456,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         kcube = (double)n * n * n;
       }
       int anyf1 = 0;
-      for (int j = tid; j < m; j += NT) {
+      for (int j = tid; j < m; j += BT) {
         const int jnz = s_nnz[j];
         double up = 0.0;
         for (int i = 0; i < m; ++i) {
@@ -454,30 +478,30 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
     // residuals: r_p = b - A.X, D = C - Z - sum y_k A_k (Residuals::compute)
     auto residuals = [&](double& nrp, double& nrd) {
       double mx = 0.0;
-      for (int k = tid; k < m; k += NT) {
+      for (int k = tid; k < m; k += BT) {
         double r = bv[k] - sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], X, n);
         vrp[k] = r;
         mx = fmax(mx, fabs(r));
       }
-      nrp = cta::block_max<NT>(mx, RD);
-      for (int t = tid; t < nn_i; t += NT) D[t] = -Z[t];
+      nrp = cta::block_max<BT>(mx, RD);
+      for (int t = tid; t < nn_i; t += BT) D[t] = -Z[t];
       __syncthreads();
-      sp_axpy_block(er, ec, ev, mp[0], mp[1], -1.0, D, n);  // C = -F0
-      sp_axpy_constraints(er, ec, ev, mp, m, vy, -1.0, D, n);
+      sp_axpy_block<BT>(er, ec, ev, mp[0], mp[1], -1.0, D, n);  // C = -F0
+      sp_axpy_constraints<BT>(er, ec, ev, mp, m, vy, -1.0, D, n);
       __syncthreads();
       mx = 0.0;
-      for (int t = tid; t < nn_i; t += NT) mx = fmax(mx, fabs(D[t]));
-      nrd = cta::block_max<NT>(mx, RD);
+      for (int t = tid; t < nn_i; t += BT) mx = fmax(mx, fabs(D[t]));
+      nrd = cta::block_max<BT>(mx, RD);
     };
     // C . W with C = -F0
     auto c_dot = [&](const double* W) {
       double s = 0.0;
-      for (long long e = mp[0] + tid; e < mp[1]; e += NT) {
+      for (long long e = mp[0] + tid; e < mp[1]; e += BT) {
         int r = er[e], c = ec[e];
         double v = -ev[e];
         s += (r == c) ? v * W[r + (size_t)n * r] : v * (W[r + (size_t)n * c] + W[c + (size_t)n * r]);
       }
-      return cta::block_sum<NT>(s, RD);
+      return cta::block_sum<BT>(s, RD);
     };
 
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -490,23 +514,23 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       const double* Yu = a.init.Y + a.p.dense_off[inst];
       const double* xv = a.init.xvec + a.p.vec_off[inst];
       // only the diagonal blocks of a block-structured point are used
-      for (int t = tid; t < nn_i; t += NT) {
+      for (int t = tid; t < nn_i; t += BT) {
         const int i = t % n, j = t / n;
         const bool keep = !blocked || (s_bid[i] == s_bid[j] && (s_bid[i] >= 0 || i == j));
         const double xu = keep ? Xu[t] : 0.0, yu = keep ? Yu[t] : 0.0;
         Z[t] = xu; X[t] = yu; W1[t] = xu; W2[t] = yu;
       }
-      for (int k = tid; k < m; k += NT) vy[k] = -xv[k];
+      for (int k = tid; k < m; k += BT) vy[k] = -xv[k];
       __syncthreads();
       // strict interiority check (the reference ignores computeInverse's
       // failure here, sdpa_solve.cpp:63; this solver falls back instead)
-      int fx = cta::cholesky<NT, double>(n, W2, n, false, sD, gsm, &s_flag);
-      int fz = fx ? 1 : cta::cholesky<NT, double>(n, W1, n, false, sD, gsm, &s_flag);
+      int fx = cta::cholesky<BT, double>(n, W2, n, false, sD, gsm, &s_flag);
+      int fz = fx ? 1 : cta::cholesky<BT, double>(n, W1, n, false, sD, gsm, &s_flag);
       if (fx || fz) { warm = false; status = 1; }
       else {
-        cta::tri_inverse<NT, double>(n, W2, n, LXi, n, sD, gsm);
-        cta::tri_inverse<NT, double>(n, W1, n, LZi, n, sD, gsm);
-        cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
+        cta::tri_inverse<BT, double>(n, W2, n, LXi, n, sD, gsm);
+        cta::tri_inverse<BT, double>(n, W1, n, LZi, n, sD, gsm);
+        cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
     } else if (wmode == SDPAB_INIT_DUAL) {
       // Proposed x only.  Applicable when the constraints are X_ii = b_i
@@ -514,62 +538,62 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       // s adds s I to X = sum F_i x_i - F0, and Y = D X^{-1} D with
       // D_ii = sqrt(b_i / (X^{-1})_ii) satisfies the constraints exactly.
       int bad = (m != n);
-      for (int k = tid; k < m && !bad; k += NT) {
+      for (int k = tid; k < m && !bad; k += BT) {
         if (mp[k + 2] - mp[k + 1] != 1) { bad = 1; break; }
         const long long e = mp[k + 1];
         if (er[e] != ec[e] || ev[e] != 1.0 || !(bv[k] > 0.0)) bad = 1;
       }
       // every diagonal position covered exactly once
-      for (int t = tid; t < n; t += NT) W1[t] = 0.0;
+      for (int t = tid; t < n; t += BT) W1[t] = 0.0;
       __syncthreads();
-      for (int k = tid; k < m && !bad; k += NT) atomicAdd(&W1[er[mp[k + 1]]], 1.0);
+      for (int k = tid; k < m && !bad; k += BT) atomicAdd(&W1[er[mp[k + 1]]], 1.0);
       __syncthreads();
-      for (int t = tid; t < n && !bad; t += NT) bad |= (W1[t] != 1.0);
+      for (int t = tid; t < n && !bad; t += BT) bad |= (W1[t] != 1.0);
       bad = __syncthreads_or(bad);
       if (!bad) {
         const double* xv = a.init.xvec + a.p.vec_off[inst];
-        for (int k = tid; k < m; k += NT) vy[k] = -xv[k];
-        for (int t = tid; t < nn_i; t += NT) Z[t] = 0.0;
+        for (int k = tid; k < m; k += BT) vy[k] = -xv[k];
+        for (int t = tid; t < nn_i; t += BT) Z[t] = 0.0;
         __syncthreads();
-        sp_axpy_block(er, ec, ev, mp[0], mp[1], -1.0, Z, n);  // C = -F0
+        sp_axpy_block<BT>(er, ec, ev, mp[0], mp[1], -1.0, Z, n);  // C = -F0
         __syncthreads();
         double cs = 0.0;
-        for (int t = tid; t < n; t += NT) cs += fabs(Z[t + (size_t)n * t]);
-        cs = cta::block_sum<NT>(cs, RD) / n;
+        for (int t = tid; t < n; t += BT) cs += fabs(Z[t + (size_t)n * t]);
+        cs = cta::block_sum<BT>(cs, RD) / n;
         const double margin = ((a.init.init_margin > 0.0) ? a.init.init_margin : 0.02) * ((cs > 0.0) ? cs : 1.0);
-        sp_axpy_constraints(er, ec, ev, mp, m, vy, -1.0, Z, n);  // Z = C - sum y_k A_k
+        sp_axpy_constraints<BT>(er, ec, ev, mp, m, vy, -1.0, Z, n);  // Z = C - sum y_k A_k
         __syncthreads();
         double lmin;
-        if (n > 20) lmin = lanczos_min_eig(n, Z, es);
-        else lmin = dense_min_eig(n, Z, es);
+        if (n > 20) lmin = lanczos_min_eig<BT>(n, Z, es);
+        else lmin = dense_min_eig<BT>(n, Z, es);
         double shift = (lmin < margin) ? margin - lmin : 0.0;
         int ok = 0;
         for (int attempt = 0; attempt < 8 && !ok; ++attempt) {
-          for (int t = tid; t < nn_i; t += NT) W1[t] = Z[t] + (((t % n) == (t / n)) ? shift : 0.0);
+          for (int t = tid; t < nn_i; t += BT) W1[t] = Z[t] + (((t % n) == (t / n)) ? shift : 0.0);
           __syncthreads();
-          if (cta::cholesky<NT, double>(n, W1, n, false, sD, gsm, &s_flag) == 0) ok = 1;
+          if (cta::cholesky<BT, double>(n, W1, n, false, sD, gsm, &s_flag) == 0) ok = 1;
           else shift = 2.0 * shift + margin;
         }
         if (ok) {
-          for (int k = tid; k < m; k += NT) vy[k] -= shift;
-          for (int t = tid; t < nn_i; t += NT) if ((t % n) == (t / n)) Z[t] += shift;
-          cta::tri_inverse<NT, double>(n, W1, n, LZi, n, sD, gsm);
-          cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
+          for (int k = tid; k < m; k += BT) vy[k] -= shift;
+          for (int t = tid; t < nn_i; t += BT) if ((t % n) == (t / n)) Z[t] += shift;
+          cta::tri_inverse<BT, double>(n, W1, n, LZi, n, sD, gsm);
+          cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
           // X = D Z^-1 D with X_kk = b_k
-          for (int t = tid; t < n; t += NT) {
+          for (int t = tid; t < n; t += BT) {
             const int r = er[mp[t + 1]];
             W1[r] = sqrt(bv[t] / Zi[r + (size_t)n * r]);
           }
           __syncthreads();
-          for (int t = tid; t < nn_i; t += NT) {
+          for (int t = tid; t < nn_i; t += BT) {
             const int i = t % n, j = t / n;
             X[t] = W1[i] * Zi[t] * W1[j];
           }
           __syncthreads();
-          for (int t = tid; t < nn_i; t += NT) W2[t] = X[t];
+          for (int t = tid; t < nn_i; t += BT) W2[t] = X[t];
           __syncthreads();
-          if (cta::cholesky<NT, double>(n, W2, n, false, sD, gsm, &s_flag) == 0) {
-            cta::tri_inverse<NT, double>(n, W2, n, LXi, n, sD, gsm);
+          if (cta::cholesky<BT, double>(n, W2, n, false, sD, gsm, &s_flag) == 0) {
+            cta::tri_inverse<BT, double>(n, W2, n, LXi, n, sD, gsm);
             warm = true;
           }
         }
@@ -577,7 +601,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       if (!warm) status = 1;
     }
     if (!warm) {
-      for (int t = tid; t < nn_i; t += NT) {
+      for (int t = tid; t < nn_i; t += BT) {
         bool dg = (t % n) == (t / n);
         X[t] = dg ? lam : 0.0;
         Z[t] = dg ? lam : 0.0;
@@ -585,21 +609,21 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         LZi[t] = dg ? 1.0 / sqrt(lam) : 0.0;
         Zi[t] = dg ? 1.0 / lam : 0.0;
       }
-      for (int k = tid; k < m; k += NT) vy[k] = 0.0;
+      for (int k = tid; k < m; k += BT) vy[k] = 0.0;
     }
     __syncthreads();
     if (warm) {
-      for (int t = tid; t < nn_i; t += NT) { X0[t] = X[t]; Z0[t] = Z[t]; }
+      for (int t = tid; t < nn_i; t += BT) { X0[t] = X[t]; Z0[t] = Z[t]; }
       __syncthreads();
     }
 
     residuals(nrp, nrd);
     double mu0;
-    if (warm) mu0 = cta::dot_mat<NT>(n, X, Z, RD) / n;
+    if (warm) mu0 = cta::dot_mat<BT>(n, X, Z, RD) / n;
     else mu0 = lam * lam;
     {
       double objP = c_dot(X);
-      double objD = cta::dot_vec<NT>(m, bv, vy, RD);
+      double objD = cta::dot_vec<BT>(m, bv, vy, RD);
       if (tid == 0) {
         init_scalars(S, P, n, mu0, nrp, nrd, objP, objD);
         update_check(S, P);
@@ -607,6 +631,52 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
     }
     __syncthreads();
 
+    // mixed mode: once an FP32 factor fails or its refinement stalls, the
+    // rest of the solve factors in FP64
+    bool fp64_only = false;
+    // x = B^-1 rhs with the FP32 factor in B32 and FP64 iterative refinement
+    // against B (full, FP64): x <- x + L32^-T L32^-1 (rhs - B x) until the
+    // correction is below 1e-10 |x| (the error left is then that times the
+    // FP32 solve's own contraction, cond(B) 6e-8); at most REFINE steps, so
+    // a B too ill-conditioned for the FP32 factor returns false (x is then
+    // not used) and the solve continues with the FP64 factor.
+    auto solve_refined = [&](const double* rhs, double* x) -> bool {
+      constexpr int REFINE = 3;
+      for (int k = tid; k < m; k += BT) x32[k] = (float)rhs[k];
+      __syncthreads();
+      cta::chol_solve<BT, float>(m, B32, m, x32, (float*)sD);
+      for (int k = tid; k < m; k += BT) x[k] = (double)x32[k];
+      __syncthreads();
+      const int lane = tid & 31, wid = tid >> 5;
+      for (int step = 0; step < REFINE; ++step) {
+        // residual rhs - B x, one warp per row (B symmetric: row i = column i)
+        for (int i = wid; i < m; i += BT / 32) {
+          double acc = 0.0;
+          for (int j = lane; j < m; j += 32) acc += B[j + (size_t)m * i] * x[j];
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+          if (lane == 0) {
+            const double r = rhs[i] - acc;
+            vres[i] = r;
+            x32[i] = (float)r;
+          }
+        }
+        __syncthreads();
+        cta::chol_solve<BT, float>(m, B32, m, x32, (float*)sD);
+        double cmax = 0.0, xmax = 0.0;
+        for (int k = tid; k < m; k += BT) {
+          const double c = (double)x32[k];
+          const double xn = x[k] + c;
+          x[k] = xn;
+          cmax = fmax(cmax, fabs(c));
+          xmax = fmax(xmax, fabs(xn));
+        }
+        double v2[2] = {cmax, xmax}, mx2[2];
+        cta::block_max_n<BT, 2>(v2, mx2, RD);
+        if (!(mx2[0] == mx2[0])) return false;  // NaN
+        if (mx2[0] <= 1.0e-10 * mx2[1]) return true;
+      }
+      return false;
+    };
     int iter = 0;
     for (;;) {
       if (tid == 0) s_flag = update_check(S, P) ? 1 : 0;
@@ -617,27 +687,28 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       const bool dinf = dual_infeasible(S);
       const double bm = S.beta * S.mu;
       // mixed precision: FP32 products while mu is above the switch point
-      const bool lowp = a.mixed && attempt == 0 && mixed_gap(S) >= a.mu_switch;
+      const bool lowp = a.mixed && attempt == 0 && !fp64_only && mixed_gap(S) >= a.mu_switch;
+      const bool lowp_prod = lowp && a.mixed_products;
       // every constraint diagonal and the point dual feasible: dZ is diagonal,
       // so products with dZ are column scalings (exactly what the GEMM with a
       // diagonal factor computes)
       const bool dz_diag = diag_cons && !dinf;
 
       // ---- predictor: rMat and gVec (sdpa_newton.cpp:793-883)
-      for (int t = tid; t < nn_i; t += NT) R[t] = bm * Zi[t] - X[t];
+      for (int t = tid; t < nn_i; t += BT) R[t] = bm * Zi[t] - X[t];
       __syncthreads();
       const double* G = R;
       if (dinf) {
-        cta::gemm_prec<NT, double>(n, false, X, n, false, D, n, W1, n, 1.0, 0.0, gsm, lowp);
-        cta::gemm_prec<NT, double>(n, false, W1, n, false, Zi, n, XDZ, n, 1.0, 0.0, gsm, lowp);
-        for (int t = tid; t < nn_i; t += NT) W2[t] = R[t] - XDZ[t];
+        cta::gemm_prec<BT, double>(n, false, X, n, false, D, n, W1, n, 1.0, 0.0, gsm, lowp_prod);
+        cta::gemm_prec<BT, double>(n, false, W1, n, false, Zi, n, XDZ, n, 1.0, 0.0, gsm, lowp_prod);
+        for (int t = tid; t < nn_i; t += BT) W2[t] = R[t] - XDZ[t];
         __syncthreads();
         G = W2;
       }
-      for (int k = tid; k < m; k += NT) vg[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], G, n) + vrp[k];
+      for (int k = tid; k < m; k += BT) vg[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], G, n) + vrp[k];
       // ---- Schur complement by F3 (compute_bMat_dense_SDP3, sdpa_newton.cpp:2019-2125)
       // for the pairs whose dominant constraint is F3, then the F1 columns
-      for (int t = tid; t < m * m; t += NT) {
+      for (int t = tid; t < m * m; t += BT) {
         const int i = t % m, j = t / m;
         const int inz = s_nnz[i], jnz = s_nnz[j];
         if (jnz < inz || (inz == jnz && i < j)) continue;
@@ -649,15 +720,29 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       __syncthreads();
       if (GENERAL && any_f1) {
         if (blocked)
-          schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, dX, B, s_nnz, s_form, s_nb, s_boff, s_bsz, s_bid, gsm);
+          schur_f1<BT>(n, m, mp, er, ec, ev, X, Zi, W1, W2, dX, B, s_nnz, s_form, s_nb, s_boff, s_bsz, s_bid, gsm);
         else
-          schur_f1(n, m, mp, er, ec, ev, X, Zi, W1, W2, dX, B, s_nnz, s_form, 0, nullptr, nullptr, nullptr, gsm);
+          schur_f1<BT>(n, m, mp, er, ec, ev, X, Zi, W1, W2, dX, B, s_nnz, s_form, 0, nullptr, nullptr, nullptr, gsm);
       }
-      // ---- adjusted Cholesky and solve (compute_DyVec, sdpa_newton.cpp:2672-2716)
-      if (cta::cholesky<NT, double>(m, B, m, true, sD, gsm, &s_flag, false)) break;  // solves read the lower triangle
-      for (int k = tid; k < m; k += NT) vdy[k] = vg[k];
-      __syncthreads();
-      cta::chol_solve<NT, double>(m, B, m, vdy, sD);
+      // ---- adjusted Cholesky and solve (compute_DyVec, sdpa_newton.cpp:2672-2716).
+      // Mixed mode (FP32 phase): the factor in FP32 (the same adjust rule) of
+      // an FP32 copy of B, each solve refined in FP64 against B; a factor
+      // that fails, or a solve whose refinement does not converge, sends this
+      // iteration and the rest of the solve to the FP64 factor.
+      bool f32 = false;
+      if (lowp) {
+        for (int t = tid; t < m * m; t += BT) B32[t] = (float)B[t];
+        __syncthreads();
+        f32 = cta::cholesky<BT, float>(m, B32, m, true, (float*)sD, gsm, &s_flag, false) == 0;
+        if (f32) f32 = solve_refined(vg, vdy);
+        if (!f32) fp64_only = true;
+      }
+      if (!f32) {
+        if (cta::cholesky<BT, double>(m, B, m, true, sD, gsm, &s_flag, false)) break;  // solves read the lower triangle
+        for (int k = tid; k < m; k += BT) vdy[k] = vg[k];
+        __syncthreads();
+        cta::chol_solve<BT, double>(m, B, m, vdy, sD);
+      }
 
       // ---- dZ, dX (compute_DzMat / compute_DxMat, sdpa_newton.cpp:2718-2752).
       // With every constraint diagonal and the point dual feasible, dZ =
@@ -666,24 +751,24 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       // products and the update with dZ touch the diagonal only.
       auto direction = [&]() {
         if (dz_diag) {
-          for (int t = tid; t < n; t += NT) vdz[t] = 0.0;
+          for (int t = tid; t < n; t += BT) vdz[t] = 0.0;
           __syncthreads();
-          for (int k = tid; k < m; k += NT) {
+          for (int k = tid; k < m; k += BT) {
             const double s = -vdy[k];
             for (long long e = mp[k + 1]; e < mp[k + 2]; ++e) atomicAdd(&vdz[er[e]], s * ev[e]);
           }
           __syncthreads();
-          for (int t = tid; t < nn_i; t += NT) W1[t] = X[t] * vdz[t / n];
+          for (int t = tid; t < nn_i; t += BT) W1[t] = X[t] * vdz[t / n];
           __syncthreads();
         } else {
-          for (int t = tid; t < nn_i; t += NT) dZ[t] = dinf ? D[t] : 0.0;
+          for (int t = tid; t < nn_i; t += BT) dZ[t] = dinf ? D[t] : 0.0;
           __syncthreads();
-          sp_axpy_constraints(er, ec, ev, mp, m, vdy, -1.0, dZ, n);
+          sp_axpy_constraints<BT>(er, ec, ev, mp, m, vdy, -1.0, dZ, n);
           __syncthreads();
-          cta::gemm_prec<NT, double>(n, false, X, n, false, dZ, n, W1, n, 1.0, 0.0, gsm, lowp);
+          cta::gemm_prec<BT, double>(n, false, X, n, false, dZ, n, W1, n, 1.0, 0.0, gsm, lowp_prod);
         }
-        cta::gemm_prec<NT, double>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm, lowp);
-        for (int t = tid; t < nn_i; t += NT) {
+        cta::gemm_prec<BT, double>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm, lowp_prod);
+        for (int t = tid; t < nn_i; t += BT) {
           const int i = t % n, j = t / n;
           if (i >= j) {
             double lo = R[i + n * j] - W2[i + n * j];
@@ -697,17 +782,17 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       };
       // A . dZ (A = X or dX): the diagonal only when dZ is diagonal
       auto dot_dz = [&](const double* A) {
-        if (!dz_diag) return cta::dot_mat<NT>(n, A, dZ, RD);
+        if (!dz_diag) return cta::dot_mat<BT>(n, A, dZ, RD);
         double s = 0.0;
-        for (int t = tid; t < n; t += NT) s += A[t * (n + 1)] * vdz[t];
-        return cta::block_sum<NT>(s, RD);
+        for (int t = tid; t < n; t += BT) s += A[t * (n + 1)] * vdz[t];
+        return cta::block_sum<BT>(s, RD);
       };
       direction();
       {
         double CdX = c_dot(dX);
-        double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);
+        double bdy = cta::dot_vec<BT>(m, bv, vdy, RD);
         double xdz = dot_dz(X);
-        double dxz = cta::dot_mat<NT>(n, dX, Z, RD);
+        double dxz = cta::dot_mat<BT>(n, dX, Z, RD);
         double dxdz = dot_dz(dX);
         if (tid == 0) {
           predictor_step(S, CdX, bdy);
@@ -720,22 +805,33 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       {
         const double bm2 = S.beta * S.mu;
         if (dz_diag) {
-          for (int t = tid; t < nn_i; t += NT) W1[t] = dX[t] * vdz[t / n];
+          for (int t = tid; t < nn_i; t += BT) W1[t] = dX[t] * vdz[t / n];
           __syncthreads();
         } else {
-          cta::gemm_prec<NT, double>(n, false, dX, n, false, dZ, n, W1, n, 1.0, 0.0, gsm, lowp);
+          cta::gemm_prec<BT, double>(n, false, dX, n, false, dZ, n, W1, n, 1.0, 0.0, gsm, lowp_prod);
         }
-        cta::gemm_prec<NT, double>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm, lowp);
-        for (int t = tid; t < nn_i; t += NT) {
+        cta::gemm_prec<BT, double>(n, false, W1, n, false, Zi, n, W2, n, 1.0, 0.0, gsm, lowp_prod);
+        for (int t = tid; t < nn_i; t += BT) {
           double rr = bm2 * Zi[t] - X[t];
           rr = rr - W2[t];
           R[t] = rr;
           W1[t] = dinf ? rr - XDZ[t] : rr;
         }
         __syncthreads();
-        for (int k = tid; k < m; k += NT) vdy[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], W1, n) + vrp[k];
+        for (int k = tid; k < m; k += BT) vg[k] = -sp_dot(er, ec, ev, mp[k + 1], mp[k + 2], W1, n) + vrp[k];
         __syncthreads();
-        cta::chol_solve<NT, double>(m, B, m, vdy, sD);
+        bool refined = f32 && solve_refined(vg, vdy);
+        if (f32 && !refined) {
+          // the FP32 factor does not carry this right-hand side: FP64 factor
+          // (B is intact: the FP32 path never factors it in place)
+          fp64_only = true;
+          if (cta::cholesky<BT, double>(m, B, m, true, sD, gsm, &s_flag, false)) break;
+        }
+        if (!refined) {
+          for (int k = tid; k < m; k += BT) vdy[k] = vg[k];
+          __syncthreads();
+          cta::chol_solve<BT, double>(m, B, m, vdy, sD);
+        }
         direction();
       }
 
@@ -745,15 +841,15 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
         double mins[2];
         const double* DZ = dz_diag ? vdz : dZ;  // the diagonal vector when dZ is diagonal
         if (GENERAL && blocked)
-          min_eig_pair_blocks(n, s_nb, s_boff, s_bsz, LXi, dX, LZi, DZ, W1, W2, R, XDZ, gsm, gsm_doubles, es,
+          min_eig_pair_blocks<BT>(n, s_nb, s_boff, s_bsz, LXi, dX, LZi, DZ, W1, W2, R, XDZ, gsm, gsm_doubles, es,
                               mins, dz_diag);
         else
-          min_eig_pair(n, LXi, dX, LZi, DZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins, dz_diag);
+          min_eig_pair<BT>(n, LXi, dX, LZi, DZ, W1, W2, R, XDZ, gsm, gsm_doubles, es, mins, dz_diag);
         const double minX = mins[0], minZ = mins[1];
         double CdX = c_dot(dX);
-        double bdy = cta::dot_vec<NT>(m, bv, vdy, RD);
+        double bdy = cta::dot_vec<BT>(m, bv, vdy, RD);
         double xdz = dot_dz(X);
-        double dxz = cta::dot_mat<NT>(n, dX, Z, RD);
+        double dxz = cta::dot_mat<BT>(n, dX, Z, RD);
         double dxdz = dot_dz(dX);
         if (tid == 0) corrector_step(S, P, minX, minZ, CdX, bdy, xdz, dxz, dxdz, S.objD, S.objP);
         __syncthreads();
@@ -763,7 +859,7 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
       {
         const double ap = S.alphaP, ad = S.alphaD;
         // X += ap dX, Z += ad dZ, and the copies the factorisations work on
-        for (int t = tid; t < nn_i; t += NT) {
+        for (int t = tid; t < nn_i; t += BT) {
           const double x = X[t] + ap * dX[t];
           double z = Z[t];
           if (!dz_diag) z += ad * dZ[t];
@@ -773,27 +869,27 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
           W2[t] = x;
           W1[t] = z;
         }
-        for (int k = tid; k < m; k += NT) vy[k] += ad * vdy[k];
+        for (int k = tid; k < m; k += BT) vy[k] += ad * vdy[k];
         __syncthreads();
         if (cannot_move(S)) break;
         // X and Z factored and inverted in lockstep (either failing ends the loop)
-        if (cta::cholesky_pair<NT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false)) break;  // inverses read the lower triangles
-        cta::tri_inverse_pair<NT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
-        cta::gemm<NT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
+        if (cta::cholesky_pair<BT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false)) break;  // inverses read the lower triangles
+        cta::tri_inverse_pair<BT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
+        cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
       // ---- residuals and scalars
       {
-        double xz = cta::dot_mat<NT>(n, X, Z, RD);
+        double xz = cta::dot_mat<BT>(n, X, Z, RD);
         residuals(nrp, nrd);
         double objP = c_dot(X);
-        double objD = cta::dot_vec<NT>(m, bv, vy, RD);
+        double objD = cta::dot_vec<BT>(m, bv, vy, RD);
         double x0zM, xMz0;
         if (warm) {
-          x0zM = cta::dot_mat<NT>(n, X0, Z, RD);
-          xMz0 = cta::dot_mat<NT>(n, X, Z0, RD);
+          x0zM = cta::dot_mat<BT>(n, X0, Z, RD);
+          xMz0 = cta::dot_mat<BT>(n, X, Z0, RD);
         } else {
-          x0zM = lam * cta::trace<NT>(n, Z, RD);
-          xMz0 = lam * cta::trace<NT>(n, X, RD);
+          x0zM = lam * cta::trace<BT>(n, Z, RD);
+          xMz0 = lam * cta::trace<BT>(n, X, RD);
         }
         if (tid == 0) after_update(S, P, xz, nrp, nrd, objP, objD, x0zM, xMz0);
         __syncthreads();
@@ -822,15 +918,15 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
     }
     if (a.r.xvec) {
       double* xo = a.r.xvec + a.p.vec_off[inst];
-      for (int k = tid; k < m; k += NT) xo[k] = -vy[k];
+      for (int k = tid; k < m; k += BT) xo[k] = -vy[k];
     }
     if (a.r.X) {
       double* o = a.r.X + a.p.dense_off[inst];
-      for (int t = tid; t < nn_i; t += NT) o[t] = Z[t];
+      for (int t = tid; t < nn_i; t += BT) o[t] = Z[t];
     }
     if (a.r.Y) {
       double* o = a.r.Y + a.p.dense_off[inst];
-      for (int t = tid; t < nn_i; t += NT) o[t] = X[t];
+      for (int t = tid; t < nn_i; t += BT) o[t] = X[t];
     }
     __syncthreads();
   }
@@ -838,16 +934,69 @@ __global__ void __launch_bounds__(NT, 2) batch_ipm_fp64(BatchArgs a)
 
 // Host side -----------------------------------------------------------------
 
-// The instantiation for a batch: block-aware only when it carries a structure.
-static void* solver_kernel(const sdpab_batch* prob)
+// The instantiation for a batch: block-aware only when it carries a
+// structure; 256 or 128 threads per instance.
+static void* solver_kernel(const sdpab_batch* prob, int bt)
 {
-  return prob->nblock ? (void*)batch_ipm_fp64<true> : (void*)batch_ipm_fp64<false>;
+  if (bt == 128)
+    return prob->nblock ? (void*)batch_ipm_fp64<true, 128> : (void*)batch_ipm_fp64<false, 128>;
+  return prob->nblock ? (void*)batch_ipm_fp64<true, 256> : (void*)batch_ipm_fp64<false, 256>;
+}
+
+// Launch shape of the solver: threads per block (instance), resident blocks
+// per SM, staging doubles and dynamic shared memory bytes.
+struct LaunchShape {
+  int bt, per_sm;
+  long long gsm;
+  size_t shm;
+};
+
+// Threads per block from the configuration (256 by default, or 128), and
+// the blocks per SM it asks for (default: 2 of 256 threads, 4 of 128); the
+// staging area is sized for that many, and the occupancy the device reports
+// caps it.
+static int launch_shape(const sdpab_batch* prob, int want_bt, int want_per_sm, int want_staging, int dev,
+                        LaunchShape& L, const char* who)
+{
+  L.bt = (want_bt == 128) ? 128 : 256;
+  const int per_sm_req = (want_per_sm > 0) ? want_per_sm : (L.bt == 128 ? 4 : 2);
+  L.gsm = staging_doubles(prob->nmax, prob->mmax, want_staging, L.bt, per_sm_req);
+  L.shm = smem_bytes_for(prob->nmax, prob->mmax, L.gsm, L.bt);
+  void* k = solver_kernel(prob, L.bt);
+  if (L.shm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.shm);
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, L.bt, L.shm);
+  if (e != cudaSuccess) return cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (per_sm < 1) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "%s: the solver block does not fit on an SM", who);
+    return set_error(SDPAB_ESIZE, msg);
+  }
+  L.per_sm = std::min(per_sm, per_sm_req);
+  (void)dev;
+  return SDPAB_OK;
+}
+
+static void launch_solver(const sdpab_batch* prob, const LaunchShape& L, int grid, const BatchArgs& a,
+                          cudaStream_t stream)
+{
+  if (L.bt == 128) {
+    if (prob->nblock) batch_ipm_fp64<true, 128><<<grid, 128, L.shm, stream>>>(a);
+    else batch_ipm_fp64<false, 128><<<grid, 128, L.shm, stream>>>(a);
+  } else {
+    if (prob->nblock) batch_ipm_fp64<true, 256><<<grid, 256, L.shm, stream>>>(a);
+    else batch_ipm_fp64<false, 256><<<grid, 256, L.shm, stream>>>(a);
+  }
 }
 
 static long long ws_doubles(int nmax, int mmax)
 {
   long long nn = (long long)nmax * nmax;
-  long long s = 14 * nn + (long long)mmax * mmax;
+  const long long mm = (long long)mmax * mmax;
+  long long s = 14 * nn + mm + (mm + 1) / 2;  // 14 n x n, the Schur matrix, its FP32 factor
   return (s + 31) / 32 * 32;  // 256-byte aligned per block
 }
 
@@ -864,19 +1013,11 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   if (cudaGetDevice(&dev) != cudaSuccess) return set_error(SDPAB_ENODEV, "no CUDA device");
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long gsm = staging_doubles(prob->nmax, prob->mmax, cfg ? cfg->staging_doubles : 0);
-  const size_t shm = smem_bytes_for(prob->nmax, prob->mmax, gsm);
-  if (shm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(solver_kernel(prob), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)shm);
-    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
-  }
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solver_kernel(prob), NT, shm);
-  if (per_sm < 1) return set_error(SDPAB_ESIZE, "batch_solve: kernel does not fit on an SM");
-  int want = (cfg && cfg->ctas_per_sm > 0) ? cfg->ctas_per_sm : 2;
-  per_sm = std::min(per_sm, want);
-  int grid = std::min(prob->count, sms * per_sm);
+  LaunchShape L;
+  int rc = launch_shape(prob, cfg ? cfg->block_threads : 0, cfg ? cfg->ctas_per_sm : 0,
+                        cfg ? cfg->staging_doubles : 0, dev, L, "batch_solve");
+  if (rc != SDPAB_OK) return rc;
+  int grid = std::min(prob->count, sms * L.per_sm);
   const long long stride = ws_doubles(prob->nmax, prob->mmax);
   Workspace& W = workspace();
   double* ws = (double*)W.get((size_t)grid * stride * sizeof(double) + 256);
@@ -890,14 +1031,14 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.r = *res;
   memcpy(&a.prm, prm, sizeof(Params));
   a.order = order;
-  a.gsm_doubles = (int)gsm;
+  a.gsm_doubles = (int)L.gsm;
   a.mixed = (cfg && cfg->precision == SDPAB_PREC_MIXED) ? 1 : 0;
+  a.mixed_products = (cfg && cfg->mixed_products) ? 1 : 0;
   a.mu_switch = (cfg && cfg->mixed_switch_gap > 0.0) ? cfg->mixed_switch_gap : 1.0e-2;
   a.ws = ws;
   a.ws_stride = stride;
   a.queue = queue;
-  if (prob->nblock) batch_ipm_fp64<true><<<grid, NT, shm, stream>>>(a);
-  else batch_ipm_fp64<false><<<grid, NT, shm, stream>>>(a);
+  launch_solver(prob, L, grid, a, stream);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "batch_ipm_fp64 launch");
   return SDPAB_OK;
@@ -952,18 +1093,10 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   double* base = (double*)sym;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long gsm = staging_doubles(prob->nmax, prob->mmax, 0);
-  const size_t shm = smem_bytes_for(prob->nmax, prob->mmax, gsm);
-  if (shm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(solver_kernel(prob), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)shm);
-    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
-  }
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solver_kernel(prob), NT, shm);
-  if (per_sm < 1) return set_error(SDPAB_ESIZE, "batch_solve_noalloc: kernel does not fit on an SM");
-  per_sm = std::min(per_sm, 2);
-  const long long grid = std::min<long long>(std::min<long long>(prob->count, (long long)sms * per_sm),
+  LaunchShape L;
+  int rc = launch_shape(prob, 256, 2, 0, dev, L, "batch_solve_noalloc");
+  if (rc != SDPAB_OK) return rc;
+  const long long grid = std::min<long long>(std::min<long long>(prob->count, (long long)sms * L.per_sm),
                                              capacity);
   int* queue = (int*)base;
   cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
@@ -974,14 +1107,14 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.r = *res;
   memcpy(&a.prm, prm, sizeof(Params));
   a.order = order;
-  a.gsm_doubles = (int)gsm;
+  a.gsm_doubles = (int)L.gsm;
   a.mixed = 0;
+  a.mixed_products = 0;
   a.mu_switch = 1.0e-2;
   a.ws = base + head;
   a.ws_stride = stride;
   a.queue = queue;
-  if (prob->nblock) batch_ipm_fp64<true><<<(int)grid, NT, shm, stream>>>(a);
-  else batch_ipm_fp64<false><<<(int)grid, NT, shm, stream>>>(a);
+  launch_solver(prob, L, (int)grid, a, stream);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "batch_solve_noalloc: launch");
   return SDPAB_OK;

@@ -69,6 +69,29 @@ __device__ __forceinline__ void block_sum_n(const double* v, double* out, Reduce
   }
 }
 
+// K <= 2 maxima with one barrier (same slot discipline as block_sum).
+template <int NT, int K>
+__device__ __forceinline__ void block_max_n(const double* v, double* out, Reducer& R)
+{
+  static_assert(K >= 1 && K <= 2, "block_max_n: K <= 2");
+  double* slot = R.buf + R.parity * (2 * (NT / 32));
+  R.parity ^= 1;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    double x = v[j];
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if ((threadIdx.x & 31) == 0) slot[j * (NT / 32) + (threadIdx.x >> 5)] = x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    double s = slot[j * (NT / 32)];
+#pragma unroll
+    for (int w = 1; w < NT / 32; ++w) s = fmax(s, slot[j * (NT / 32) + w]);
+    out[j] = s;
+  }
+}
+
 template <int NT>
 __device__ __forceinline__ double block_max(double v, Reducer& R)
 {
@@ -133,13 +156,20 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // All GEMM / factorisation routines are templated on the matrix storage type
 // TM and the compute type TC (TC = float with TM = double is the mixed
 // precision path: operands are rounded to FP32 when staged in shared memory,
-// products accumulate in FP32, results are stored back in FP64).
+// products accumulate in FP32, results are stored back in FP64), and on the
+// number of threads NT of the calling block (256 or 128; 8 or 4 warps).
 //
-// 64 x 64 output tiles, K staged in chunks of GK.
+// 64 x 64 output tiles, K staged in chunks of gk<NT>() (16 with 256
+// threads, 8 with 128: a 128-thread block shares its SM with three others
+// and stages half as much).
 constexpr int GT = 64, GK = 16;
+template <int NT>
+__host__ __device__ constexpr int gk() { return NT >= 256 ? 16 : 8; }
 // shared memory (elements) a gemm_rect call may use: two stages of A and B
 constexpr int GTP = GT + 4;  // staged row stride (bank spread of the FP64 MMA fragment loads)
-constexpr int GEMM_RECT_SMEM = 4 * GK * GTP;
+constexpr int GEMM_RECT_SMEM = 4 * GK * GTP;  // 256 threads
+template <int NT>
+__host__ __device__ constexpr int gemm_rect_smem() { return 4 * gk<NT>() * GTP; }
 
 // One FP64 tensor-core MMA, D = A B + D with A 8 x 4, B 4 x 8, D 8 x 8
 // (mma.sync m8n8k4 .f64; per lane one element of A and of B, two of D).
@@ -153,16 +183,18 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
 // gemm_rect with double-buffered cp.async staging (storage type = compute
 // type): the (tile, K chunk) steps form one pipeline, chunk s+1 (of this or
 // the next live tile) is copied while chunk s is multiplied, one barrier per
-// step.  smem: 4 * GK * GT elements of T.
+// step.  FP64: the warps as 2 x (NT / 64) over the 8 x 8 blocks of the tile
+// on the FP64 MMA; FP32: the threads as 16 x (NT / 16), each 64 / (NT / 16)
+// rows x 4 columns.  smem: 4 * gk<NT>() * GTP elements of T.
 template <int NT, typename T>
 __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T* A, int lda, bool tB, const T* B,
                                           int ldb, T* C, int ldc, double alpha, double beta, void* smem_v,
                                           bool lower, int diag_off)
 {
-  T* buf = (T*)smem_v;  // [2][As: GK*GTP | Bs: GK*GTP]
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  constexpr int G = gk<NT>();
+  T* buf = (T*)smem_v;  // [2][As: G*GTP | Bs: G*GTP]
   const int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT, ntile = tm * tn;
-  const int nk = (K + GK - 1) / GK;
+  const int nk = (K + G - 1) / G;
   auto live = [&](int tile) {
     const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
     return !(lower && r0 + GT - 1 + diag_off < c0);
@@ -173,19 +205,19 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
   };
   auto issue = [&](int tile, int k0, int which) {
     const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
-    T* As = buf + which * 2 * GK * GTP;
-    T* Bs = As + GK * GTP;
-    for (int t = threadIdx.x; t < GK * GT; t += NT) {
+    T* As = buf + which * 2 * G * GTP;
+    T* Bs = As + G * GTP;
+    for (int t = threadIdx.x; t < G * GT; t += NT) {
       int r, k;
-      if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
-      const int gr = r0 + r, gk = k0 + k;
-      const bool va = gr < M && gk < K;
-      cp_async_el<T>(&As[k * GTP + r], va ? (tA ? A + gk + (size_t)lda * gr : A + gr + (size_t)lda * gk) : A, va);
+      if (!tA) { r = t % GT; k = t / GT; } else { k = t % G; r = t / G; }
+      const int gr = r0 + r, gk2 = k0 + k;
+      const bool va = gr < M && gk2 < K;
+      cp_async_el<T>(&As[k * GTP + r], va ? (tA ? A + gk2 + (size_t)lda * gr : A + gr + (size_t)lda * gk2) : A, va);
       int c;
-      if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
-      const int gc = c0 + c, gk2 = k0 + k;
-      const bool vb = gc < N && gk2 < K;
-      cp_async_el<T>(&Bs[k * GTP + c], vb ? (tB ? B + gc + (size_t)ldb * gk2 : B + gk2 + (size_t)ldb * gc) : B, vb);
+      if (!tB) { k = t % G; c = t / G; } else { c = t % GT; k = t / GT; }
+      const int gc = c0 + c, gk3 = k0 + k;
+      const bool vb = gc < N && gk3 < K;
+      cp_async_el<T>(&Bs[k * GTP + c], vb ? (tB ? B + gc + (size_t)ldb * gk3 : B + gk3 + (size_t)ldb * gc) : B, vb);
     }
     cp_async_commit();
   };
@@ -207,37 +239,39 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
   while (tile < ntile) {
     const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
     if constexpr (std::is_same<T, double>::value) {
-      // FP64 MMA (m8n8k4): warps as 2 x 4 over the 8 x 8 blocks of the
-      // tile, warp (wr, wc) owning blocks (wr + 2 i, wc + 4 j), i < 4, j < 2;
-      // lane l holds A(l / 4, l % 4), B(l % 4, l / 4), C(l / 4, 2 (l % 4) + h)
+      // FP64 MMA (m8n8k4): warps as 2 x WC over the 8 x 8 blocks of the
+      // tile, warp (wr, wc) owning blocks (wr + 2 i, wc + WC j), i < 4,
+      // j < 8 / WC; lane l holds A(l / 4, l % 4), B(l % 4, l / 4),
+      // C(l / 4, 2 (l % 4) + h)
+      constexpr int WC = NT / 64, JB = 8 / WC;
       const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wr = w & 1, wc = w >> 1;
       const int q = lane & 3, p = lane >> 2;
-      double acc[4][2][2];
+      double acc[4][JB][2];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < JB; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
       for (int kc = 0; kc < nk; ++kc) {
         cp_async_wait_all();
         __syncthreads();  // this step's chunk is visible; the other buffer is free
         if (it_tile < ntile) {
-          issue(it_tile, it_k * GK, which ^ 1);
+          issue(it_tile, it_k * G, which ^ 1);
           advance();
         }
-        const double* As = buf + which * 2 * GK * GTP;
-        const double* Bs = As + GK * GTP;
+        const double* As = buf + which * 2 * G * GTP;
+        const double* Bs = As + G * GTP;
         // rows k >= K of the last chunk are zero-filled: whole steps of 4
-        const int kmax = min(GK, K - kc * GK);
+        const int kmax = min(G, K - kc * G);
         for (int kk = 0; kk < kmax; kk += 4) {
-          double a[4], b[2];
+          double a[4], b[JB];
 #pragma unroll
           for (int i = 0; i < 4; ++i) a[i] = As[(kk + q) * GTP + (wr + 2 * i) * 8 + p];
 #pragma unroll
-          for (int j = 0; j < 2; ++j) b[j] = Bs[(kk + q) * GTP + (wc + 4 * j) * 8 + p];
+          for (int j = 0; j < JB; ++j) b[j] = Bs[(kk + q) * GTP + (wc + WC * j) * 8 + p];
 #pragma unroll
           for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+            for (int j = 0; j < JB; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
         which ^= 1;
       }
@@ -246,10 +280,10 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
         const int gr = r0 + (wr + 2 * i) * 8 + p;
         if (gr >= M) continue;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < JB; ++j) {
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const int gc = c0 + (wc + 4 * j) * 8 + 2 * q + h;
+            const int gc = c0 + (wc + WC * j) * 8 + 2 * q + h;
             if (gc >= N) continue;
             if (lower && gr + diag_off < gc) continue;
             double* cp = C + gr + (size_t)ldc * gc;
@@ -258,37 +292,39 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
         }
       }
     } else {
-    T acc[4][4];
+    constexpr int TY = NT / 16, IR = GT / TY;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    T acc[IR][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < IR; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[i][j] = (T)0;
     for (int kc = 0; kc < nk; ++kc) {
       cp_async_wait_all();
       __syncthreads();  // this step's chunk is visible; the other buffer is free
       if (it_tile < ntile) {
-        issue(it_tile, it_k * GK, which ^ 1);
+        issue(it_tile, it_k * G, which ^ 1);
         advance();
       }
-      const T* As = buf + which * 2 * GK * GTP;
-      const T* Bs = As + GK * GTP;
-      const int kmax = min(GK, K - kc * GK);
+      const T* As = buf + which * 2 * G * GTP;
+      const T* Bs = As + G * GTP;
+      const int kmax = min(G, K - kc * G);
       for (int k = 0; k < kmax; ++k) {
-        T a[4], b[4];
+        T a[IR], b[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[k * GTP + ty + 16 * i];
+        for (int i = 0; i < IR; ++i) a[i] = As[k * GTP + ty + TY * i];
 #pragma unroll
         for (int j = 0; j < 4; ++j) b[j] = Bs[k * GTP + tx + 16 * j];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < IR; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
       }
       which ^= 1;
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int gr = r0 + ty + 16 * i;
+    for (int i = 0; i < IR; ++i) {
+      const int gr = r0 + ty + TY * i;
       if (gr >= M) continue;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -306,29 +342,32 @@ __device__ __noinline__ void gemm_rect_db(int M, int N, int K, bool tA, const T*
 }
 
 // gemm_rect: C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C.
-// 64 x 64 output tiles, 256 threads as a 16 x 16 grid with 4 x 4 outputs each
-// (rows ty + 16 i, columns tx + 16 j), K staged in chunks of GK.  When the
-// storage and compute types agree the staging is gemm_rect_db's (cp.async,
-// two stages); the mixed FP64-storage / FP32-compute form prefetches the
-// next chunk into registers and converts while storing.  lower = true
-// updates only entries with (row + diag_off >= col) and skips tiles
-// entirely above that diagonal (trailing updates of factorisations).
-// smem: GEMM_RECT_SMEM elements of TC.  Ends with a barrier.
+// 64 x 64 output tiles, K staged in chunks of gk<NT>().  When the storage
+// and compute types agree the staging is gemm_rect_db's (cp.async, two
+// stages); the mixed FP64-storage / FP32-compute form prefetches the next
+// chunk into registers and converts while storing, with the threads as
+// 16 x (NT / 16), each 64 / (NT / 16) rows x 4 columns (rows ty + (NT / 16) i,
+// columns tx + 16 j).  lower = true updates only entries with
+// (row + diag_off >= col) and skips tiles entirely above that diagonal
+// (trailing updates of factorisations).  smem: gemm_rect_smem<NT>()
+// elements of TC.  Ends with a barrier.
 template <int NT, typename TM, typename TC>
 __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const TM* A, int lda, bool tB,
                                        const TM* B, int ldb, TM* C, int ldc, double alpha, double beta,
                                        void* smem_v, bool lower = false, int diag_off = 0)
 {
-  static_assert(NT == 256, "gemm tile mapping assumes 256 threads");
+  static_assert(NT == 256 || NT == 128, "gemm tile mappings for 256 or 128 threads");
   if constexpr (std::is_same<TM, TC>::value) {
     if (K > 0) {
       gemm_rect_db<NT, TM>(M, N, K, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem_v, lower, diag_off);
       return;
     }
   }
-  constexpr int PER = GK * GT / NT;  // staged elements per thread and operand
-  TC* As = (TC*)smem_v;          // [GK][GT]  As[k*GT + r]
-  TC* Bs = As + GK * GT;         // [GK][GT]  Bs[k*GT + c]
+  constexpr int G = gk<NT>();
+  constexpr int PER = G * GT / NT;  // staged elements per thread and operand
+  constexpr int TY = NT / 16, IR = GT / TY;
+  TC* As = (TC*)smem_v;          // [G][GT]  As[k*GT + r]
+  TC* Bs = As + G * GT;          // [G][GT]  Bs[k*GT + c]
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT;
   TC ra[PER], rb[PER];
@@ -337,13 +376,13 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const TM* A
     for (int u = 0; u < PER; ++u) {
       const int t = threadIdx.x + u * NT;
       int r, k;
-      if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
-      const int gr = r0 + r, gk = k0 + k;
-      ra[u] = (gr < M && gk < K) ? (TC)(tA ? A[gk + (size_t)lda * gr] : A[gr + (size_t)lda * gk]) : (TC)0;
+      if (!tA) { r = t % GT; k = t / GT; } else { k = t % G; r = t / G; }
+      const int gr = r0 + r, gk2 = k0 + k;
+      ra[u] = (gr < M && gk2 < K) ? (TC)(tA ? A[gk2 + (size_t)lda * gr] : A[gr + (size_t)lda * gk2]) : (TC)0;
       int c;
-      if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
-      const int gc = c0 + c, gk2 = k0 + k;
-      rb[u] = (gc < N && gk2 < K) ? (TC)(tB ? B[gc + (size_t)ldb * gk2] : B[gk2 + (size_t)ldb * gc]) : (TC)0;
+      if (!tB) { k = t % G; c = t / G; } else { c = t % GT; k = t / GT; }
+      const int gc = c0 + c, gk3 = k0 + k;
+      rb[u] = (gc < N && gk3 < K) ? (TC)(tB ? B[gc + (size_t)ldb * gk3] : B[gk3 + (size_t)ldb * gc]) : (TC)0;
     }
   };
   auto store = [&]() {
@@ -351,10 +390,10 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const TM* A
     for (int u = 0; u < PER; ++u) {
       const int t = threadIdx.x + u * NT;
       int r, k;
-      if (!tA) { r = t % GT; k = t / GT; } else { k = t % GK; r = t / GK; }
+      if (!tA) { r = t % GT; k = t / GT; } else { k = t % G; r = t / G; }
       As[k * GT + r] = ra[u];
       int c;
-      if (!tB) { k = t % GK; c = t / GK; } else { c = t % GT; k = t / GT; }
+      if (!tB) { k = t % G; c = t / G; } else { c = t % GT; k = t / GT; }
       Bs[k * GT + c] = rb[u];
     }
   };
@@ -367,35 +406,35 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const TM* A
   if (tile < tm * tn) fetch((tile % tm) * GT, (tile / tm) * GT, 0);
   while (tile < tm * tn) {
     const int r0 = (tile % tm) * GT, c0 = (tile / tm) * GT;
-    TC acc[4][4];
+    TC acc[IR][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < IR; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[i][j] = (TC)0;
     int next = tile + 1;
     while (next < tm * tn && !tile_live(next)) ++next;
-    for (int k0 = 0; k0 < K; k0 += GK) {
+    for (int k0 = 0; k0 < K; k0 += G) {
       store();
       __syncthreads();
-      if (k0 + GK < K) fetch(r0, c0, k0 + GK);
+      if (k0 + G < K) fetch(r0, c0, k0 + G);
       else if (next < tm * tn) fetch((next % tm) * GT, (next / tm) * GT, 0);
-      const int kmax = min(GK, K - k0);
+      const int kmax = min(G, K - k0);
       for (int k = 0; k < kmax; ++k) {
-        TC a[4], b[4];
+        TC a[IR], b[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[k * GT + ty + 16 * i];
+        for (int i = 0; i < IR; ++i) a[i] = As[k * GT + ty + TY * i];
 #pragma unroll
         for (int j = 0; j < 4; ++j) b[j] = Bs[k * GT + tx + 16 * j];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < IR; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
       }
       __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int gr = r0 + ty + 16 * i;
+    for (int i = 0; i < IR; ++i) {
+      const int gr = r0 + ty + TY * i;
       if (gr >= M) continue;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -412,51 +451,52 @@ __device__ __noinline__ void gemm_rect(int M, int N, int K, bool tA, const TM* A
 }
 
 // Square n x n product as ONE output tile of (16 R) x (16 R), R = ceil(n/16)
-// (n <= 96): thread (tx, ty) of the 16 x 16 grid owns rows ty + 16 i and
-// columns tx + 16 j, i, j < R, so no padding beyond the next multiple of 16
-// is computed.  K is staged in chunks of 16 (smem 2 * 16 * 16R elements of TC).
+// (n <= 96): the threads as 16 x (NT / 16); thread (tx, ty) owns rows
+// ty + (NT / 16) i and columns tx + 16 j, so no padding beyond the next
+// multiple of 16 is computed.  K is staged in chunks of 16 (smem
+// 2 * 16 * 16R elements of TC).
 template <int NT, int R, typename TM, typename TC>
 __device__ __noinline__ void gemm_tile(int n, bool tA, const TM* A, int lda, bool tB, const TM* B, int ldb,
                                        TM* C, int ldc, double alpha, double beta, void* smem_v)
 {
-  constexpr int T = 16 * R, KC = 16;
+  constexpr int T = 16 * R, KC = 16, TY = NT / 16, RI = T / TY;
   TC* As = (TC*)smem_v;         // [KC][T]
   TC* Bs = As + KC * T;         // [KC][T]
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  TC acc[R][R];
+  TC acc[RI][R];
 #pragma unroll
-  for (int i = 0; i < R; ++i)
+  for (int i = 0; i < RI; ++i)
 #pragma unroll
     for (int j = 0; j < R; ++j) acc[i][j] = (TC)0;
   for (int k0 = 0; k0 < n; k0 += KC) {
     for (int t = threadIdx.x; t < KC * T; t += NT) {
       int r, k;
       if (!tA) { r = t % T; k = t / T; } else { k = t % KC; r = t / KC; }
-      const int gk = k0 + k;
-      As[k * T + r] = (r < n && gk < n) ? (TC)(tA ? A[gk + (size_t)lda * r] : A[r + (size_t)lda * gk]) : (TC)0;
+      const int gk2 = k0 + k;
+      As[k * T + r] = (r < n && gk2 < n) ? (TC)(tA ? A[gk2 + (size_t)lda * r] : A[r + (size_t)lda * gk2]) : (TC)0;
       int c;
       if (!tB) { k = t % KC; c = t / KC; } else { c = t % T; k = t / T; }
-      const int gk2 = k0 + k;
-      Bs[k * T + c] = (c < n && gk2 < n) ? (TC)(tB ? B[c + (size_t)ldb * gk2] : B[gk2 + (size_t)ldb * c]) : (TC)0;
+      const int gk3 = k0 + k;
+      Bs[k * T + c] = (c < n && gk3 < n) ? (TC)(tB ? B[c + (size_t)ldb * gk3] : B[gk3 + (size_t)ldb * c]) : (TC)0;
     }
     __syncthreads();
     const int kmax = min(KC, n - k0);
     for (int k = 0; k < kmax; ++k) {
-      TC a[R], b[R];
+      TC a[RI], b[R];
 #pragma unroll
-      for (int i = 0; i < R; ++i) a[i] = As[k * T + ty + 16 * i];
+      for (int i = 0; i < RI; ++i) a[i] = As[k * T + ty + TY * i];
 #pragma unroll
       for (int j = 0; j < R; ++j) b[j] = Bs[k * T + tx + 16 * j];
 #pragma unroll
-      for (int i = 0; i < R; ++i)
+      for (int i = 0; i < RI; ++i)
 #pragma unroll
         for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int gr = ty + 16 * i;
+  for (int i = 0; i < RI; ++i) {
+    const int gr = ty + TY * i;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
       const int gc = tx + 16 * j;
@@ -471,94 +511,115 @@ __device__ __noinline__ void gemm_tile(int n, bool tA, const TM* A, int lda, boo
 
 // FP64 tile GEMM for n <= 96 on the FP64 tensor-core MMA
 // (mma.sync m8n8k4 .f64: one 8 x 8 x 4 product, 256 FMAs, per warp
-// instruction): one exact-size tile T x T (T = 16 R >= n), 256 threads as
-// 2 x 4 warps, warp (wr, wc) owning the 8 x 8 blocks (wr + 2 i, wc + 4 j).
-// K is staged in chunks of 16 by cp.async into two buffers ([k][r] with a
-// row stride of T + 4 doubles, so each half-warp's fragment loads fall on
-// distinct banks); per step of 4 a warp loads R A fragments and up to
-// (R + 1) / 2 B fragments and issues R x (R + 1) / 2 MMAs.  Fragments
-// (PTX m8n8k4 .f64): lane l holds A(l / 4, l % 4), B(l % 4, l / 4) and
-// C(l / 4, 2 (l % 4) + {0, 1}).  smem: 4 * 16 * (T + 4) doubles.
+// instruction): one exact-size tile T x T (T = 16 R >= n) of 2R x 2R blocks
+// of 8 x 8.  The warps as 2 x WC (WC = NT / 64), warp (wr, wc) owning the
+// row blocks wr + 2 i (i < R) and, in each of NPASS column passes (1 with
+// 256 threads, 2 with 128, so that a warp's accumulators stay at
+// R x ceil(R / 2) blocks), the column blocks pbase + wc + WC j of the pass.
+// K is staged in chunks of KC (16 with 256 threads, 8 with 128) by cp.async
+// into two buffers ([k][r] with a row stride of T + 4 doubles, so each
+// half-warp's fragment loads fall on distinct banks); a pass stages A
+// whole and B's columns of the pass.  Fragments (PTX m8n8k4 .f64): lane l
+// holds A(l / 4, l % 4), B(l % 4, l / 4) and C(l / 4, 2 (l % 4) + {0, 1}).
+// smem: 4 * KC * (T + 4) doubles.
+template <int NT>
+__host__ __device__ constexpr int mma_kc() { return NT >= 256 ? 16 : 8; }
 
 template <int NT, int R>
 __device__ __noinline__ void gemm_tile_mma(int n, bool tA, const double* A, int lda, bool tB, const double* B,
                                            int ldb, double* C, int ldc, double alpha, double beta, void* smem_v)
 {
-  static_assert(NT == 256, "gemm_tile_mma: 8 warps");
-  constexpr int T = 16 * R, TP = T + 4, KC = 16, NB = T / 8, RB = R, CB = (R + 1) / 2;
+  static_assert(NT == 256 || NT == 128, "gemm_tile_mma: 8 or 4 warps");
+  constexpr int T = 16 * R, TP = T + 4, KC = mma_kc<NT>(), NB = T / 8;
+  constexpr int WC = NT / 64, NPASS = (NT == 256) ? 1 : 2;
+  constexpr int PB = (NB + NPASS - 1) / NPASS;  // column blocks per pass
+  constexpr int CB = (PB + WC - 1) / WC;        // column blocks per warp and pass
   double* buf = (double*)smem_v;  // [2][As: KC*TP | Bs: KC*TP]
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wr = w & 1, wc = w >> 1;
   const int q = lane & 3, p = lane >> 2;
-  auto issue = [&](int k0, int which) {
-    double* As = buf + which * 2 * KC * TP;
-    double* Bs = As + KC * TP;
-    for (int t = threadIdx.x; t < KC * T; t += NT) {
-      int r, k;
-      if (!tA) { r = t % T; k = t / T; } else { k = t % KC; r = t / KC; }
-      const int gk = k0 + k;
-      const bool va = r < n && gk < n;
-      cp_async8(&As[k * TP + r], va ? (tA ? A + gk + (size_t)lda * r : A + r + (size_t)lda * gk) : A, va);
-      int c;
-      if (!tB) { k = t % KC; c = t / KC; } else { c = t % T; k = t / T; }
-      const int gk2 = k0 + k;
-      const bool vb = c < n && gk2 < n;
-      cp_async8(&Bs[k * TP + c], vb ? (tB ? B + c + (size_t)ldb * gk2 : B + gk2 + (size_t)ldb * c) : B, vb);
-    }
-    cp_async_commit();
-  };
-  double acc[RB][CB][2];
-#pragma unroll
-  for (int i = 0; i < RB; ++i)
-#pragma unroll
-    for (int j = 0; j < CB; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int nch = (n + KC - 1) / KC;
-  issue(0, 0);
-  for (int ch = 0; ch < nch; ++ch) {
-    cp_async_wait_all();
-    __syncthreads();  // chunk ch visible; every thread is done with chunk ch-1's buffer
-    if (ch + 1 < nch) issue((ch + 1) * KC, (ch + 1) & 1);
-    const double* As = buf + (ch & 1) * 2 * KC * TP;
-    const double* Bs = As + KC * TP;
-    // rows k >= n of the last chunk are zero-filled: whole steps of 4
-    const int kmax = min(KC, n - ch * KC);
-    for (int kk = 0; kk < kmax; kk += 4) {
-      double a[RB], b[CB];
+  for (int pass = 0; pass < NPASS; ++pass) {
+    const int pbase = pass * PB;
+    const int pcols = min(PB, NB - pbase) * 8;  // columns of this pass
+    const int c0 = pbase * 8;
+    auto issue = [&](int k0, int which) {
+      double* As = buf + which * 2 * KC * TP;
+      double* Bs = As + KC * TP;
+      for (int t = threadIdx.x; t < KC * T; t += NT) {
+        int r, k;
+        if (!tA) { r = t % T; k = t / T; } else { k = t % KC; r = t / KC; }
+        const int gk2 = k0 + k;
+        const bool va = r < n && gk2 < n;
+        cp_async8(&As[k * TP + r], va ? (tA ? A + gk2 + (size_t)lda * r : A + r + (size_t)lda * gk2) : A, va);
+      }
+      for (int t = threadIdx.x; t < KC * pcols; t += NT) {
+        int c, k;
+        if (!tB) { k = t % KC; c = t / KC; } else { c = t % pcols; k = t / pcols; }
+        const int gc = c0 + c, gk3 = k0 + k;
+        const bool vb = gc < n && gk3 < n;
+        cp_async8(&Bs[k * TP + c], vb ? (tB ? B + gc + (size_t)ldb * gk3 : B + gk3 + (size_t)ldb * gc) : B, vb);
+      }
+      cp_async_commit();
+    };
+    double acc[R][CB][2];
 #pragma unroll
-      for (int i = 0; i < RB; ++i) a[i] = As[(kk + q) * TP + (wr + 2 * i) * 8 + p];
+    for (int i = 0; i < R; ++i)
+#pragma unroll
+      for (int j = 0; j < CB; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    issue(0, 0);
+    for (int ch = 0; ch < nch; ++ch) {
+      cp_async_wait_all();
+      __syncthreads();  // chunk ch visible; every thread is done with chunk ch-1's buffer
+      if (ch + 1 < nch) issue((ch + 1) * KC, (ch + 1) & 1);
+      const double* As = buf + (ch & 1) * 2 * KC * TP;
+      const double* Bs = As + KC * TP;
+      // rows k >= n of the last chunk are zero-filled: whole steps of 4
+      const int kmax = min(KC, n - ch * KC);
+      for (int kk = 0; kk < kmax; kk += 4) {
+        double a[R], b[CB];
+#pragma unroll
+        for (int i = 0; i < R; ++i) a[i] = As[(kk + q) * TP + (wr + 2 * i) * 8 + p];
+#pragma unroll
+        for (int j = 0; j < CB; ++j) {
+          const int lb = wc + WC * j;  // column block within the pass
+          b[j] = (lb < PB && pbase + lb < NB) ? Bs[(kk + q) * TP + lb * 8 + p] : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+          for (int j = 0; j < CB; ++j)
+            if (wc + WC * j < PB && pbase + wc + WC * j < NB) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int gr = (wr + 2 * i) * 8 + p;
 #pragma unroll
       for (int j = 0; j < CB; ++j) {
-        const int cb = wc + 4 * j;
-        b[j] = (cb < NB) ? Bs[(kk + q) * TP + cb * 8 + p] : 0.0;
-      }
+        const int lb = wc + WC * j;
 #pragma unroll
-      for (int i = 0; i < RB; ++i)
-#pragma unroll
-        for (int j = 0; j < CB; ++j)
-          if (wc + 4 * j < NB) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < RB; ++i) {
-    const int gr = (wr + 2 * i) * 8 + p;
-#pragma unroll
-    for (int j = 0; j < CB; ++j) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int gc = (wc + 4 * j) * 8 + 2 * q + h;
-        if (wc + 4 * j < NB && gr < n && gc < n) {
-          double* cp = C + gr + (size_t)ldc * gc;
-          *cp = (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*cp);
+        for (int h = 0; h < 2; ++h) {
+          const int gc = (pbase + lb) * 8 + 2 * q + h;
+          if (lb < PB && pbase + lb < NB && gr < n && gc < n) {
+            double* cp = C + gr + (size_t)ldc * gc;
+            *cp = (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*cp);
+          }
         }
       }
     }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
+// Shared memory (doubles) the square GEMM dispatch below needs with NT threads.
+template <int NT>
+__host__ __device__ constexpr int gemm_smem_min() { return 4 * mma_kc<NT>() * (96 + 4); }
+
 // Square GEMM dispatch: one exact-size tile for n <= 96 (FP64: on the FP64
-// MMA, double-buffered), 64 x 64 tiles above.  smem must hold 4 * 16 * 100
+// MMA, double-buffered), 64 x 64 tiles above.  The FP32 form (lowp) with
+// 128 threads keeps the exact tile to n <= 64 (the accumulators of larger
+// ones would not stay in registers).  smem must hold gemm_smem_min<NT>()
 // doubles.
-// lowp = compute in FP32.
 template <int NT, typename TM>
 __device__ __forceinline__ void gemm_prec(int n, bool tA, const TM* A, int lda, bool tB, const TM* B, int ldb,
                                           TM* C, int ldc, double alpha, double beta, void* smem, bool lowp)
@@ -567,9 +628,19 @@ __device__ __forceinline__ void gemm_prec(int n, bool tA, const TM* A, int lda, 
     if (n <= 32) gemm_tile<NT, 2, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
     else if (n <= 48) gemm_tile<NT, 3, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
     else if (n <= 64) gemm_tile<NT, 4, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 80) gemm_tile<NT, 5, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else if (n <= 96) gemm_tile<NT, 6, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
-    else gemm_rect<NT, TM, float>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    else {
+      if constexpr (NT == 256) {
+        if (n <= 80) {
+          gemm_tile<NT, 5, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+          return;
+        }
+        if (n <= 96) {
+          gemm_tile<NT, 6, TM, float>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+          return;
+        }
+      }
+      gemm_rect<NT, TM, float>(n, n, n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
+    }
   } else {
     if (n <= 32) gemm_tile_mma<NT, 2>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);
     else if (n <= 48) gemm_tile_mma<NT, 3>(n, tA, A, lda, tB, B, ldb, C, ldc, alpha, beta, smem);

@@ -1,8 +1,9 @@
 // Minimum eigenvalue of L D L^T for the step length (Jal::getMinEigen,
 // sdpa_jordan.cpp:58-109): Lanczos for n > 20 (Lal::getMinEigen,
 // sdpa_linear.cpp:29-143), all eigenvalues for n <= 20 (dsyev branch,
-// sdpa_linear.cpp:145-182).  Executed by one 256-thread block; shared by the
-// batched persistent solver and the host-driven solver.
+// sdpa_linear.cpp:145-182).  Executed by one block of BT threads (256, the
+// default NT, or 128); shared by the batched persistent solver and the
+// host-driven solver.
 #pragma once
 #include "cta_linalg.cuh"
 
@@ -73,11 +74,11 @@ static __device__ inline void eig_scratch_carve(EigScratch& s, double* p, int nm
 // taken are those of the plain sequence: per step, alpha = q.Mq, the
 // residual, beta, and at the steps the reference chooses (kk >= sqrt(k),
 // k = n-1 or k > sqrt(n+9)) the Ritz value and error of the tridiagonal.
-template <int NM>
+template <int NM, int BT = NT>
 static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, EigScratch& s, double* out)
 {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  constexpr int NW = NT / 32;
+  constexpr int NW = BT / 32;
   double beta[NM], mn[NM], mn_old[NM], err[NM];
   int k[NM], kk[NM];
   bool act[NM], pend[NM];
@@ -85,8 +86,8 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
 #pragma unroll
   for (int j = 0; j < NM; ++j) {
     LanczosVec& v = s.v[j];
-    for (int i = tid; i < n; i += NT) { v.q[i] = 0.0; v.r[i] = 1.0; }
-    for (int i = tid; i < TRI_MAX; i += NT) { v.d[i] = 1.0e50; v.e[i] = 0.0; }
+    for (int i = tid; i < n; i += BT) { v.q[i] = 0.0; v.r[i] = 1.0; }
+    for (int i = tid; i < TRI_MAX; i += BT) { v.d[i] = 1.0e50; v.e[i] = 0.0; }
     beta[j] = sqn;
     mn[j] = 1.0e51;
     mn_old[j] = 1.0e52;
@@ -102,7 +103,7 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
       if (!act[j]) continue;
       LanczosVec& v = s.v[j];
       const double ib = 1.0 / beta[j];
-      for (int i = tid; i < n; i += NT) { v.qold[i] = v.q[i]; v.q[i] = v.r[i] * ib; }
+      for (int i = tid; i < n; i += BT) { v.qold[i] = v.q[i]; v.q[i] = v.r[i] * ib; }
     }
     __syncthreads();
     // (b) warps 0 / 1 solve the pending tridiagonals while the remaining
@@ -171,7 +172,7 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
       }
     }
     double alpha[NM];
-    cta::block_sum_n<NT, NM>(part, alpha, *s.R);  // publishes w and the tridiagonal results
+    cta::block_sum_n<BT, NM>(part, alpha, *s.R);  // publishes w and the tridiagonal results
     // (c) take in the Ritz values, then the reference's test for this step
     bool any = false;
 #pragma unroll
@@ -197,7 +198,7 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
       rpart[j] = 0.0;
       if (!act[j]) continue;
       LanczosVec& v = s.v[j];
-      for (int i = tid; i < n; i += NT) {
+      for (int i = tid; i < n; i += BT) {
         const double rv = (v.w[i] - alpha[j] * v.q[i]) - beta[j] * v.qold[i];
         v.r[i] = rv;
         rpart[j] += rv * rv;
@@ -210,7 +211,7 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
       }
     }
     double rr[NM];
-    cta::block_sum_n<NT, NM>(rpart, rr, *s.R);
+    cta::block_sum_n<BT, NM>(rpart, rr, *s.R);
 #pragma unroll
     for (int j = 0; j < NM; ++j) {
       if (!act[j]) continue;
@@ -225,11 +226,12 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
   for (int j = 0; j < NM; ++j) out[j] = mn[j] - fabs(err[j] * beta[j]);
 }
 
+template <int BT = NT>
 static __device__ double lanczos_min_eig(int n, const double* M, EigScratch& s)
 {
   const double* Ms[1] = {M};
   double out[1];
-  lanczos_min_eig_multi<1>(n, Ms, s, out);
+  lanczos_min_eig_multi<1, BT>(n, Ms, s, out);
   return out[0];
 }
 
@@ -237,12 +239,13 @@ static __device__ double lanczos_min_eig(int n, const double* M, EigScratch& s)
 // (Jal::getMinEigen QR branch + dsyev, sdpa_jordan.cpp:81-89,
 // sdpa_linear.cpp:145-182) via Householder tridiagonalisation (warp 0) and
 // multisection.
+template <int BT = NT>
 static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
 {
   const int tid = threadIdx.x, lane = tid & 31;
   LanczosVec& lv = s.v[0];
   double* M = s.M;  // n x n symmetric copy of the lower triangle
-  for (int t = tid; t < n * n; t += NT) {
+  for (int t = tid; t < n * n; t += BT) {
     const int i = t % n, j = t / n;
     M[i + n * j] = (i >= j) ? W2[i + (size_t)n * j] : W2[j + (size_t)n * i];
   }
@@ -303,47 +306,49 @@ static __device__ double dense_min_eig(int n, const double* W2, EigScratch& s)
 // z_diag: Dz is diagonal and given as the vector of its diagonal (n values),
 // so Dz Lz^T is a row scaling of Lz^T (no GEMM).
 // Wx2 = Lx Dx Lx^T and Wz2 = Lz Dz Lz^T (Wx1, Wz1 scratch).
+template <int BT = NT>
 static __device__ void form_ldlt_pair(int n, const double* Lx, const double* Dx, const double* Lz,
                                       const double* Dz, double* Wx1, double* Wx2, double* Wz1, double* Wz2,
                                       double* gsm, bool z_diag)
 {
-  cta::gemm<NT>(n, false, Dx, n, true, Lx, n, Wx1, n, 1.0, 0.0, gsm);
-  cta::gemm<NT>(n, false, Lx, n, false, Wx1, n, Wx2, n, 1.0, 0.0, gsm);
+  cta::gemm<BT>(n, false, Dx, n, true, Lx, n, Wx1, n, 1.0, 0.0, gsm);
+  cta::gemm<BT>(n, false, Lx, n, false, Wx1, n, Wx2, n, 1.0, 0.0, gsm);
   if (z_diag) {
-    for (int t = threadIdx.x; t < n * n; t += NT) {
+    for (int t = threadIdx.x; t < n * n; t += BT) {
       const int i = t % n, j = t / n;
       Wz1[t] = Dz[i] * Lz[j + (size_t)n * i];
     }
     __syncthreads();
   } else {
-    cta::gemm<NT>(n, false, Dz, n, true, Lz, n, Wz1, n, 1.0, 0.0, gsm);
+    cta::gemm<BT>(n, false, Dz, n, true, Lz, n, Wz1, n, 1.0, 0.0, gsm);
   }
-  cta::gemm<NT>(n, false, Lz, n, false, Wz1, n, Wz2, n, 1.0, 0.0, gsm);
+  cta::gemm<BT>(n, false, Lz, n, false, Wz1, n, Wz2, n, 1.0, 0.0, gsm);
 }
 
+template <int BT = NT>
 static __device__ void min_eig_pair(int n, const double* Lx, const double* Dx, const double* Lz,
                                     const double* Dz, double* Wx1, double* Wx2, double* Wz1, double* Wz2,
                                     double* gsm, int gsm_doubles, EigScratch& s, double* out, bool z_diag = false)
 {
-  form_ldlt_pair(n, Lx, Dx, Lz, Dz, Wx1, Wx2, Wz1, Wz2, gsm, z_diag);
+  form_ldlt_pair<BT>(n, Lx, Dx, Lz, Dz, Wx1, Wx2, Wz1, Wz2, gsm, z_diag);
   if (n <= 20) {
-    out[0] = dense_min_eig(n, Wx2, s);
-    out[1] = dense_min_eig(n, Wz2, s);
+    out[0] = dense_min_eig<BT>(n, Wx2, s);
+    out[1] = dense_min_eig<BT>(n, Wz2, s);
     return;
   }
   const double* Ms[2] = {Wx2, Wz2};
   const int nn = n * n;
   if (2 * nn <= gsm_doubles) {
-    for (int t = threadIdx.x; t < nn; t += NT) { gsm[t] = Wx2[t]; gsm[nn + t] = Wz2[t]; }
+    for (int t = threadIdx.x; t < nn; t += BT) { gsm[t] = Wx2[t]; gsm[nn + t] = Wz2[t]; }
     __syncthreads();
     Ms[0] = gsm;
     Ms[1] = gsm + nn;
   } else if (nn <= gsm_doubles) {
-    for (int t = threadIdx.x; t < nn; t += NT) gsm[t] = Wx2[t];
+    for (int t = threadIdx.x; t < nn; t += BT) gsm[t] = Wx2[t];
     __syncthreads();
     Ms[0] = gsm;
   }
-  lanczos_min_eig_multi<2>(n, Ms, s, out);
+  lanczos_min_eig_multi<2, BT>(n, Ms, s, out);
 }
 
 // The same for block-diagonal X and Z: nb blocks of signed orders bsz at
@@ -355,25 +360,26 @@ static __device__ void min_eig_pair(int n, const double* Lx, const double* Dx, c
 // diagonal of L D L^T there), and the smallest value is the result.  Not
 // inlined: only block-structured instances take this path, and a second
 // inlined Lanczos would raise the register pressure of the whole solver.
+template <int BT = NT>
 static __device__ __noinline__ void min_eig_pair_blocks(int n, int nb, const int* boff, const int* bsz,
                                                         const double* Lx, const double* Dx, const double* Lz,
                                                         const double* Dz, double* Wx1, double* Wx2, double* Wz1,
                                                         double* Wz2, double* gsm, int gsm_doubles, EigScratch& s,
                                                         double* out, bool z_diag)
 {
-  form_ldlt_pair(n, Lx, Dx, Lz, Dz, Wx1, Wx2, Wz1, Wz2, gsm, z_diag);
+  form_ldlt_pair<BT>(n, Lx, Dx, Lz, Dz, Wx1, Wx2, Wz1, Wz2, gsm, z_diag);
   double mx = 1.0e50, mz = 1.0e50;
   for (int l = 0; l < nb; ++l) {
     if (bsz[l] >= 2) continue;
     const int o = boff[l], cnt = bsz[l] < 0 ? -bsz[l] : bsz[l];
-    for (int t = threadIdx.x; t < cnt; t += NT) {
+    for (int t = threadIdx.x; t < cnt; t += BT) {
       const size_t d = (size_t)(o + t) * (n + 1);
       mx = fmin(mx, Wx2[d]);
       mz = fmin(mz, Wz2[d]);
     }
   }
-  mx = -cta::block_max<NT>(-mx, *s.R);
-  mz = -cta::block_max<NT>(-mz, *s.R);
+  mx = -cta::block_max<BT>(-mx, *s.R);
+  mz = -cta::block_max<BT>(-mz, *s.R);
   for (int l = 0; l < nb; ++l) {
     const int k = bsz[l];
     if (k < 2) continue;
@@ -381,7 +387,7 @@ static __device__ __noinline__ void min_eig_pair_blocks(int n, int nb, const int
     const int kk = k * k;
     double* Mx = (2 * kk <= gsm_doubles) ? gsm : Wx1;
     double* Mz = (2 * kk <= gsm_doubles) ? gsm + kk : Wz1;
-    for (int t = threadIdx.x; t < kk; t += NT) {
+    for (int t = threadIdx.x; t < kk; t += BT) {
       const size_t g = (size_t)(o + t % k) + (size_t)n * (o + t / k);
       Mx[t] = Wx2[g];
       Mz[t] = Wz2[g];
@@ -389,11 +395,11 @@ static __device__ __noinline__ void min_eig_pair_blocks(int n, int nb, const int
     __syncthreads();
     double r[2];
     if (k <= 20) {
-      r[0] = dense_min_eig(k, Mx, s);
-      r[1] = dense_min_eig(k, Mz, s);
+      r[0] = dense_min_eig<BT>(k, Mx, s);
+      r[1] = dense_min_eig<BT>(k, Mz, s);
     } else {
       const double* Ms[2] = {Mx, Mz};
-      lanczos_min_eig_multi<2>(k, Ms, s, r);
+      lanczos_min_eig_multi<2, BT>(k, Ms, s, r);
     }
     mx = fmin(mx, r[0]);
     mz = fmin(mz, r[1]);

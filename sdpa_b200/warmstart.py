@@ -221,14 +221,15 @@ class WarmPipeline:
         db.init = N.BatchInit(self.flag.data_ptr(), self.xprop.data_ptr(), None, None, margin)
         self.n = n
 
-    def run(self, precision=N.PREC_FP64, stream=None, ctas_per_sm=0, staging=0):
+    def run(self, precision=N.PREC_FP64, stream=None, **shape):
+        """shape: launch shape and mixed-mode options of DeviceBatch.solve."""
         import torch
         s = stream if stream is not None else torch.cuda.current_stream()
         self.model.forward(self.dg, self.act, self.r, s.cuda_stream)
         N.check(N.lib().sdpab_mpnn_propose_x(self.n, self.r.data_ptr(), self.degree.data_ptr(),
                                              self.fallback.data_ptr(), self.xprop.data_ptr(), s.cuda_stream),
                 "mpnn_propose_x")
-        self.db.solve(precision=precision, stream=s, ctas_per_sm=ctas_per_sm, staging=staging)
+        self.db.solve(precision=precision, stream=s, **shape)
 
 
 def default_model() -> MPNN:

@@ -230,3 +230,55 @@ def test_batched_dense_constraints_single_block_match_reference():
         Y = r.block_of(r.Y, P, q, 0).ravel(order="F")
         ref = arr[nm + ".Y1"]
         assert np.max(np.abs(Y - ref)) < 1e-4 * max(1.0, np.max(np.abs(ref))), nm
+
+
+@pytest.mark.parametrize("shape", [{"block_threads": 128, "ctas_per_sm": 4}, {"block_threads": 128, "ctas_per_sm": 3},
+                                   {"block_threads": 256, "ctas_per_sm": 1}])
+def test_launch_shapes_match_reference(shape):
+    """Every launch shape the autotuner may pick (128-thread blocks, whose
+    products run as two-pass exact tiles with K chunks of 8, or fewer
+    256-thread blocks per SM) solves to the same results: FP64 single-block
+    and multi-block batches against the reference (strict bar), and mixed
+    precision with either product precision (reference-accuracy bar)."""
+    from sdpa_b200 import batch
+    meta, arr = small()
+    _, tz = tight()
+    names = [f"bmc{s}" for s in range(64)] + ["mc100", "mc20", "mc50w"]
+    P, r = _solve(names, **shape)
+    for q, nm in enumerate(names):
+        g = meta[nm]
+        assert r.status[q] == 0 and r.phase[q] == 7, (nm, r.phase[q])
+        assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
+        assert np.max(np.abs(r.x_of(P, q) - arr[nm + ".xvec"])) < X_TOL, nm
+        assert abs(int(r.iterations[q]) - g["iterations"]) <= 1
+    bnames, insts, BP = _block_batch()
+    rb = batch.solve_host(BP, **shape)
+    for q, nm in enumerate(bnames):
+        g, garr = _golden(nm)
+        assert rb.status[q] == 0 and rb.phase[q] == 7, (nm, rb.status[q], rb.phase[q])
+        assert rel(rb.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
+        assert np.max(np.abs(rb.x_of(BP, q) - garr[nm + ".xvec"])) < X_TOL, nm
+    mnames = names + ["lt20", "lt40"]
+    for mp in (0, 1):
+        P2, r2 = _solve(mnames, precision=1, mixed_products=mp, **shape)
+        for q, nm in enumerate(mnames):
+            g = meta[nm]
+            assert r2.phase[q] == 7, (nm, mp, r2.phase[q])
+            assert rel(r2.primal_obj[q], g["primal_obj"]) < OBJ_TOL, (nm, mp)
+            assert rel(r2.dual_obj[q], g["dual_obj"]) < OBJ_TOL, (nm, mp)
+            assert x_within_reference_accuracy(r2.x_of(P2, q), arr[nm + ".xvec"], tz[nm + ".tight"]), (nm, mp)
+
+
+def test_mixed_precision_refines_in_fp32_phase():
+    """Mixed precision with the FP32 Schur factor and FP64 refinement over a
+    wide FP32 phase (switch at relative gap 1e-5): the solve still reaches
+    pdOPT with the reference's objectives on every instance."""
+    meta, arr = small()
+    _, tz = tight()
+    names = [f"bmc{s}" for s in range(64)]
+    P, r = _solve(names, precision=1, mixed_switch_gap=1e-5)
+    for q, nm in enumerate(names):
+        g = meta[nm]
+        assert r.phase[q] == 7, (nm, r.phase[q])
+        assert rel(r.primal_obj[q], g["primal_obj"]) < OBJ_TOL, nm
+        assert rel(r.dual_obj[q], g["dual_obj"]) < OBJ_TOL, nm
