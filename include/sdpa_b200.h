@@ -313,6 +313,9 @@ typedef struct sdpab_batch_config {
   int block_threads;           /* threads per solver block (one instance in flight
                                   each): 256 (0 = default) or 128; with 128, four
                                   blocks share an SM by default */
+  double refine_tol;           /* mixed mode: the FP64 refinement of a solve with the
+                                  FP32 Schur factor stops once the correction is below
+                                  this times |dy| (0 = 1e-8; three steps at most) */
 } sdpab_batch_config;
 
 /* Tensor-core lower update C -= P P^T of an M x M FP32 matrix, P M x K

@@ -92,6 +92,7 @@ struct BatchArgs {
   int mixed;             // SDPAB_PREC_MIXED: FP32 Schur factor + FP64 refinement while mixed_gap >= mu_switch
   int mixed_products;    // mixed mode: the n^3 products in FP32 as well (else on the FP64 MMA)
   double mu_switch;
+  double refine_tol;     // mixed mode: refinement stops once the correction is below this times |dy|
   double* ws;
   long long ws_stride;  // doubles per block
   int* queue;
@@ -636,10 +637,10 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
     bool fp64_only = false;
     // x = B^-1 rhs with the FP32 factor in B32 and FP64 iterative refinement
     // against B (full, FP64): x <- x + L32^-T L32^-1 (rhs - B x) until the
-    // correction is below 1e-10 |x| (the error left is then that times the
-    // FP32 solve's own contraction, cond(B) 6e-8); at most REFINE steps, so
-    // a B too ill-conditioned for the FP32 factor returns false (x is then
-    // not used) and the solve continues with the FP64 factor.
+    // correction is below REFINE_TOL |x| (the error left is then that times
+    // the FP32 solve's own contraction, about cond(B) 6e-8); at most REFINE
+    // steps, so a B too ill-conditioned for the FP32 factor returns false (x
+    // is then not used) and the solve continues with the FP64 factor.
     auto solve_refined = [&](const double* rhs, double* x) -> bool {
       constexpr int REFINE = 3;
       for (int k = tid; k < m; k += BT) x32[k] = (float)rhs[k];
@@ -673,7 +674,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
         double v2[2] = {cmax, xmax}, mx2[2];
         cta::block_max_n<BT, 2>(v2, mx2, RD);
         if (!(mx2[0] == mx2[0])) return false;  // NaN
-        if (mx2[0] <= 1.0e-10 * mx2[1]) return true;
+        if (mx2[0] <= a.refine_tol * mx2[1]) return true;
       }
       return false;
     };
@@ -1035,6 +1036,7 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.mixed = (cfg && cfg->precision == SDPAB_PREC_MIXED) ? 1 : 0;
   a.mixed_products = (cfg && cfg->mixed_products) ? 1 : 0;
   a.mu_switch = (cfg && cfg->mixed_switch_gap > 0.0) ? cfg->mixed_switch_gap : 1.0e-2;
+  a.refine_tol = (cfg && cfg->refine_tol > 0.0) ? cfg->refine_tol : 1.0e-8;
   a.ws = ws;
   a.ws_stride = stride;
   a.queue = queue;
@@ -1111,6 +1113,7 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.mixed = 0;
   a.mixed_products = 0;
   a.mu_switch = 1.0e-2;
+  a.refine_tol = 1.0e-8;
   a.ws = base + head;
   a.ws_stride = stride;
   a.queue = queue;

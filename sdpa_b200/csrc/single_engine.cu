@@ -131,6 +131,79 @@ __device__ __forceinline__ void f3_pair(long long t, int nc, const int* cons, co
   if (gi != gj) atomicAdd(&B[gj + (size_t)m * gi], ret);
 }
 
+// Tr(A_i X A_j Z^-1) of one constraint pair by formula F3 (calF3_thread_2,
+// sdpa_newton.cpp:1319-1403), the constraint with more entries as the outer
+// loop (the value is symmetric in i and j).
+__device__ __forceinline__ double f3_value_pair(int i, int j, const long long* ptr, const int* row, const int* col,
+                                                const double* val, const int* nnz, const double* X, const double* Zi,
+                                                int n)
+{
+  const int o = (nnz[j] >= nnz[i]) ? j : i, in = (o == j) ? i : j;
+  double ret = 0.0;
+  for (long long e1 = ptr[o]; e1 < ptr[o + 1]; ++e1) {
+    const int al = row[e1], be = col[e1];
+    const double* Xa = X + (size_t)n * al;
+    const double* Xb = X + (size_t)n * be;
+    const double* Za = Zi + (size_t)n * al;
+    const double* Zb = Zi + (size_t)n * be;
+    double sum = 0.0;
+    for (long long e2 = ptr[in]; e2 < ptr[in + 1]; ++e2) {
+      const int ga = row[e2], de = col[e2];
+      double plu;
+      if (al != be) {
+        plu = (ga != de) ? Zb[de] * Xa[ga] + Zb[ga] * Xa[de] + Za[de] * Xb[ga] + Za[ga] * Xb[de]
+                         : Zb[de] * Xa[ga] + Za[de] * Xb[ga];
+      } else {
+        plu = (ga != de) ? Zb[de] * Xa[ga] + Zb[ga] * Xa[de] : Zb[de] * Xa[ga];
+      }
+      sum += val[e2] * plu;
+    }
+    ret += val[e1] * sum;
+  }
+  return ret;
+}
+
+// The whole Schur matrix by F3 when it has one source: one SDP block that
+// every constraint touches, every constraint F3, no LP block (Lovasz theta,
+// MaxCut).  Each entry is then written once, so B needs no zero fill and no
+// atomics.  One block of threads per 32 x 32 tile on or below the diagonal
+// (tile rows i, columns j of the constraint index); the tile's values go
+// through shared memory, and both the tile and its mirror above the
+// diagonal are stored with consecutive threads on consecutive rows
+// (coalesced).  Threads as 32 x 8, four pairs each.
+constexpr int F3T = 32;
+__global__ void __launch_bounds__(256) k_f3_tiles(int m, const long long* ptr, const int* row, const int* col,
+                                                  const double* val, const int* nnz, const double* X,
+                                                  const double* Zi, int n, double* B)
+{
+  __shared__ double tile[F3T][F3T + 1];
+  const long long t = blockIdx.x;
+  int ti = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((long long)(ti + 1) * (ti + 2) / 2 <= t) ++ti;
+  while ((long long)ti * (ti + 1) / 2 > t) --ti;
+  const int tj = (int)(t - (long long)ti * (ti + 1) / 2);
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int i = ti * F3T + tx;
+#pragma unroll
+  for (int k = 0; k < F3T / 8; ++k) {
+    const int jl = ty + 8 * k, j = tj * F3T + jl;
+    double v = 0.0;
+    if (i < m && j < m && (ti > tj || tx >= jl)) v = f3_value_pair(i, j, ptr, row, col, val, nnz, X, Zi, n);
+    tile[tx][jl] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < F3T / 8; ++k) {
+    const int jl = ty + 8 * k, j = tj * F3T + jl;
+    if (i < m && j < m && (ti > tj || tx >= jl)) B[i + (size_t)m * j] = tile[tx][jl];
+  }
+#pragma unroll
+  for (int k = 0; k < F3T / 8; ++k) {
+    const int il = ty + 8 * k, i2 = ti * F3T + il, j2 = tj * F3T + tx;
+    if (i2 < m && j2 < m && (ti > tj || il >= tx)) B[j2 + (size_t)m * i2] = tile[il][tx];
+  }
+}
+
 // The F3 pairs of every SDP block in one launch: block b owns the flat pair
 // indices [off[b], off[b + 1]) (nc_b^2 of them), found by binary search.
 struct F3Desc {
@@ -1004,6 +1077,9 @@ struct DevState {
   long long* f3_off = nullptr;
   long long f3_total = 0;
   int f3_nb = 0;
+  // the Schur matrix has one source (k_f3_tiles): the SDP block of index
+  // f3_direct_block, touched by every constraint, all F3, no LP block
+  int f3_direct_block = -1;
   // F1 columns of the blocks of order <= SMALL_F1 in one launch (k_f1_small)
   F1Desc* f1_desc = nullptr;
   long long* f1_off = nullptr;
@@ -1658,6 +1734,13 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
     }
     S.f3_total = fo.back();
     S.f3_nb = (int)fd.size();
+    S.f3_direct_block = -1;
+    if (nsdp == 1 && nlp == 0 && S.sdp[0].nc == m) {
+      const SdpBlock& B0 = S.sdp[0];
+      bool direct = true;
+      for (int l = 0; l < B0.nc && direct; ++l) direct = B0.hcons[l] == l && B0.hform[l] == F3;
+      if (direct) S.f3_direct_block = 0;
+    }
     if (!fd.empty()) {
       void* pp = nullptr;
       if (cudaMalloc(&pp, fd.size() * sizeof(F3Desc)) != cudaSuccess)
@@ -2003,6 +2086,14 @@ int Solver::solve(const InitPoint* init, const Params* prm)
     // leaves its tile unwritten, and the matrix is then built again with the
     // SIMT products.
     auto build_bmat = [&](bool use_tc) {
+      if (S.f3_direct_block >= 0) {
+        // one source: every entry written once, no zero fill, no atomics
+        const SdpBlock& B0 = S.sdp[S.f3_direct_block];
+        const long long T = (m + F3T - 1) / F3T;
+        k_f3_tiles<<<(unsigned)(T * (T + 1) / 2), 256>>>(m, B0.ptr, B0.row, B0.col, B0.val, B0.nnz, B0.X, B0.Zi,
+                                                          B0.n, S.B);
+        return;
+      }
       cudaMemset(S.B, 0, (size_t)m * m * sizeof(double));
       if (S.f3_total > 0)
         k_f3_all<<<(unsigned)nblk(S.f3_total), 256>>>(S.f3_desc, S.f3_off, S.f3_nb, S.B, m);
