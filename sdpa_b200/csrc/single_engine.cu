@@ -133,14 +133,16 @@ __device__ __forceinline__ void f3_pair(long long t, int nc, const int* cons, co
 
 // Tr(A_i X A_j Z^-1) of one constraint pair by formula F3 (calF3_thread_2,
 // sdpa_newton.cpp:1319-1403), the constraint with more entries as the outer
-// loop (the value is symmetric in i and j).
-__device__ __forceinline__ double f3_value_pair(int i, int j, const long long* ptr, const int* row, const int* col,
-                                                const double* val, const int* nnz, const double* X, const double* Zi,
-                                                int n)
+// loop (the value is symmetric in i and j).  The outer entries
+// [e_beg, e_end) with stride e_step (a slice of the outer constraint's
+// entries when several threads share one pair).
+constexpr long long F3_HEAVY = 1024;  // entry pairs above which one pair gets a block of threads
+__device__ __forceinline__ double f3_value_slice(int o, int in, long long e_beg, long long e_step,
+                                                 const long long* ptr, const int* row, const int* col,
+                                                 const double* val, const double* X, const double* Zi, int n)
 {
-  const int o = (nnz[j] >= nnz[i]) ? j : i, in = (o == j) ? i : j;
   double ret = 0.0;
-  for (long long e1 = ptr[o]; e1 < ptr[o + 1]; ++e1) {
+  for (long long e1 = ptr[o] + e_beg; e1 < ptr[o + 1]; e1 += e_step) {
     const int al = row[e1], be = col[e1];
     const double* Xa = X + (size_t)n * al;
     const double* Xb = X + (size_t)n * be;
@@ -188,7 +190,14 @@ __global__ void __launch_bounds__(256) k_f3_tiles(int m, const long long* ptr, c
   for (int k = 0; k < F3T / 8; ++k) {
     const int jl = ty + 8 * k, j = tj * F3T + jl;
     double v = 0.0;
-    if (i < m && j < m && (ti > tj || tx >= jl)) v = f3_value_pair(i, j, ptr, row, col, val, nnz, X, Zi, n);
+    if (i < m && j < m && (ti > tj || tx >= jl)) {
+      const long long ci = ptr[i + 1] - ptr[i], cj = ptr[j + 1] - ptr[j];
+      // heavy pairs are left to k_f3_heavy (stored as 0 here, overwritten there)
+      if (ci * cj <= F3_HEAVY) {
+        const int o = (nnz[j] >= nnz[i]) ? j : i, in = (o == j) ? i : j;
+        v = f3_value_slice(o, in, 0, 1, ptr, row, col, val, X, Zi, n);
+      }
+    }
     tile[tx][jl] = v;
   }
   __syncthreads();
@@ -201,6 +210,29 @@ __global__ void __launch_bounds__(256) k_f3_tiles(int m, const long long* ptr, c
   for (int k = 0; k < F3T / 8; ++k) {
     const int il = ty + 8 * k, i2 = ti * F3T + il, j2 = tj * F3T + tx;
     if (i2 < m && j2 < m && (ti > tj || il >= tx)) B[j2 + (size_t)m * i2] = tile[il][tx];
+  }
+}
+
+// The heavy pairs of the one-source F3 assembly (entry pairs above
+// F3_HEAVY, e.g. the trace constraint of Lovasz theta with itself): one
+// block of threads per pair, the outer constraint's entries dealt over the
+// threads, a fixed-order block reduction; runs after k_f3_tiles.
+__global__ void __launch_bounds__(256) k_f3_heavy(int m, const int* pairs, const long long* ptr, const int* row,
+                                                  const int* col, const double* val, const int* nnz,
+                                                  const double* X, const double* Zi, int n, double* B)
+{
+  __shared__ double red[8];
+  const int i = pairs[2 * blockIdx.x], j = pairs[2 * blockIdx.x + 1];
+  const int o = (nnz[j] >= nnz[i]) ? j : i, in = (o == j) ? i : j;
+  double v = f3_value_slice(o, in, threadIdx.x, 256, ptr, row, col, val, X, Zi, n);
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += red[w];
+    B[i + (size_t)m * j] = s;
+    B[j + (size_t)m * i] = s;
   }
 }
 
@@ -1080,6 +1112,8 @@ struct DevState {
   // the Schur matrix has one source (k_f3_tiles): the SDP block of index
   // f3_direct_block, touched by every constraint, all F3, no LP block
   int f3_direct_block = -1;
+  int* f3_heavy = nullptr;   // its heavy pairs (i, j), i >= j (k_f3_heavy)
+  int f3_nheavy = 0;
   // F1 columns of the blocks of order <= SMALL_F1 in one launch (k_f1_small)
   F1Desc* f1_desc = nullptr;
   long long* f1_off = nullptr;
@@ -1739,7 +1773,25 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
       const SdpBlock& B0 = S.sdp[0];
       bool direct = true;
       for (int l = 0; l < B0.nc && direct; ++l) direct = B0.hcons[l] == l && B0.hform[l] == F3;
-      if (direct) S.f3_direct_block = 0;
+      if (direct) {
+        S.f3_direct_block = 0;
+        // every pair whose entry counts multiply to more than F3_HEAVY (the
+        // test k_f3_tiles applies): one of the two has more than
+        // sqrt(F3_HEAVY) = 32 entries, so only those need pairing with all
+        auto cnt = [&](int l) { return B0.hptr[l + 1] - B0.hptr[l]; };
+        std::vector<int> hp;
+        for (int a = 0; a < B0.nc; ++a) {
+          if (cnt(a) <= 32) continue;
+          for (int j = 0; j < B0.nc; ++j) {
+            if (cnt(a) * cnt(j) <= F3_HEAVY) continue;
+            if (cnt(j) > 32 && j > a) continue;  // listed once, from the larger index
+            hp.push_back(a);
+            hp.push_back(j);
+          }
+        }
+        S.f3_nheavy = (int)(hp.size() / 2);
+        if (S.f3_nheavy) S.f3_heavy = S.upload(hp);
+      }
     }
     if (!fd.empty()) {
       void* pp = nullptr;
@@ -2092,6 +2144,9 @@ int Solver::solve(const InitPoint* init, const Params* prm)
         const long long T = (m + F3T - 1) / F3T;
         k_f3_tiles<<<(unsigned)(T * (T + 1) / 2), 256>>>(m, B0.ptr, B0.row, B0.col, B0.val, B0.nnz, B0.X, B0.Zi,
                                                           B0.n, S.B);
+        if (S.f3_nheavy)
+          k_f3_heavy<<<(unsigned)S.f3_nheavy, 256>>>(m, S.f3_heavy, B0.ptr, B0.row, B0.col, B0.val, B0.nnz, B0.X,
+                                                     B0.Zi, B0.n, S.B);
         return;
       }
       cudaMemset(S.B, 0, (size_t)m * m * sizeof(double));
