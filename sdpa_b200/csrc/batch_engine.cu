@@ -56,9 +56,9 @@ constexpr long long SM_SMEM_BYTES = 228LL * 1024, BLOCK_RESERVED_BYTES = 1024;
 
 // Staging area for `per_sm` resident blocks of bt threads: at least the
 // square GEMM's double-buffered tiles (cta::gemm_smem_min) and the two
-// diagonal blocks; `want` doubles when given, by default both Lanczos
-// matrices (2 n^2) when they fit in LANCZOS_SMEM_DOUBLES, else one, else
-// the minimum; capped at what per_sm blocks of this size can have.
+// diagonal blocks; `want` doubles when given, by default all the shared
+// memory per_sm blocks of this size can have (more of it keeps the Lanczos
+// matrices and the Schur factorisation in shared memory for larger n).
 static long long staging_min(int bt)
 {
   const long long g = (bt >= 256) ? cta::gemm_smem_min<256>() : cta::gemm_smem_min<128>();
@@ -69,11 +69,8 @@ static long long staging_doubles(int nmax, int mmax, int want, int bt, int per_s
 {
   const long long g = staging_min(bt);
   const long long m2 = (long long)nmax * nmax;
-  long long s;
-  if (want > 0) s = want;
-  else if (2 * m2 <= LANCZOS_SMEM_DOUBLES) s = 2 * m2;
-  else if (m2 <= LANCZOS_SMEM_DOUBLES) s = m2;
-  else s = g;
+  // nothing uses more than both Lanczos matrices or the FP64 factorisation
+  long long s = (want > 0) ? want : std::max(2 * m2, cta::cholesky_smem_elems(mmax));
   const long long per_block = std::min<long long>(227LL * 1024, SM_SMEM_BYTES / std::max(per_sm, 1) -
                                                                     BLOCK_RESERVED_BYTES);
   const long long cap = (per_block - (long long)smem_bytes_for(nmax, mmax, 0, bt)) / (long long)sizeof(double);
@@ -678,6 +675,13 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
       }
       return false;
     };
+    // adjusted FP64 Cholesky of B in place (solves read the lower triangle):
+    // in shared memory when the staging area holds it, else blocked from L2
+    auto factor_fp64 = [&]() -> int {
+      if (cta::cholesky_smem_elems(m) <= (long long)gsm_doubles)
+        return cta::cholesky_smem<BT, double, double>(m, B, m, B, m, true, gsm, &s_flag);
+      return cta::cholesky<BT, double>(m, B, m, true, sD, gsm, &s_flag, false);
+    };
     int iter = 0;
     for (;;) {
       if (tid == 0) s_flag = update_check(S, P) ? 1 : 0;
@@ -732,14 +736,18 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
       // iteration and the rest of the solve to the FP64 factor.
       bool f32 = false;
       if (lowp) {
-        for (int t = tid; t < m * m; t += BT) B32[t] = (float)B[t];
-        __syncthreads();
-        f32 = cta::cholesky<BT, float>(m, B32, m, true, (float*)sD, gsm, &s_flag, false) == 0;
+        if (cta::cholesky_smem_elems(m) <= 2LL * gsm_doubles) {
+          f32 = cta::cholesky_smem<BT, float, double>(m, B, m, B32, m, true, (float*)gsm, &s_flag) == 0;
+        } else {
+          for (int t = tid; t < m * m; t += BT) B32[t] = (float)B[t];
+          __syncthreads();
+          f32 = cta::cholesky<BT, float>(m, B32, m, true, (float*)sD, gsm, &s_flag, false) == 0;
+        }
         if (f32) f32 = solve_refined(vg, vdy);
         if (!f32) fp64_only = true;
       }
       if (!f32) {
-        if (cta::cholesky<BT, double>(m, B, m, true, sD, gsm, &s_flag, false)) break;  // solves read the lower triangle
+        if (factor_fp64()) break;
         for (int k = tid; k < m; k += BT) vdy[k] = vg[k];
         __syncthreads();
         cta::chol_solve<BT, double>(m, B, m, vdy, sD);
@@ -826,7 +834,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
           // the FP32 factor does not carry this right-hand side: FP64 factor
           // (B is intact: the FP32 path never factors it in place)
           fp64_only = true;
-          if (cta::cholesky<BT, double>(m, B, m, true, sD, gsm, &s_flag, false)) break;
+          if (factor_fp64()) break;
         }
         if (!refined) {
           for (int k = tid; k < m; k += BT) vdy[k] = vg[k];

@@ -672,17 +672,17 @@ template <>
 __device__ __forceinline__ float adjust_huge<float>() { return 1.0e30f; }
 
 // Factors the bs x bs (bs <= 32) lower triangle held in sD (leading
-// dimension LDD) in place with one warp: lane r keeps row r in registers and
-// the column of each step is broadcast with shuffles (no shared-memory
-// traffic inside the factorisation).  kb is the block's offset, used in the
-// returned failing column (0 = success).
+// dimension ld, LDD by default) in place with one warp: lane r keeps row r in
+// registers and the column of each step is broadcast with shuffles (no
+// shared-memory traffic inside the factorisation).  kb is the block's
+// offset, used in the returned failing column (0 = success).
 template <typename T>
-static __device__ __noinline__ int warp_potrf32(int bs, T* sD, bool adjust, int kb)
+static __device__ __noinline__ int warp_potrf32(int bs, T* sD, bool adjust, int kb, int ld = LDD)
 {
   const int lane = threadIdx.x & 31;
   T a[32];
 #pragma unroll
-  for (int c = 0; c < 32; ++c) a[c] = (c <= lane && lane < bs) ? sD[lane + LDD * c] : (T)0;
+  for (int c = 0; c < 32; ++c) a[c] = (c <= lane && lane < bs) ? sD[lane + ld * c] : (T)0;
   int fail = 0;
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
@@ -711,12 +711,106 @@ static __device__ __noinline__ int warp_potrf32(int bs, T* sD, bool adjust, int 
   if (!fail && lane < bs) {
 #pragma unroll
     for (int c = 0; c < 32; ++c)
-      if (c <= lane) sD[lane + LDD * c] = a[c];
+      if (c <= lane) sD[lane + ld * c] = a[c];
   }
   return fail;
 }
 
 // ------------------------------------------------------------ Cholesky
+// Shared memory (elements of T) cholesky_smem needs for order n.
+__host__ __device__ constexpr long long cholesky_smem_elems(int n) { return (long long)n * (n + 1) + NB; }
+
+// Lower Cholesky of an n x n matrix factored entirely in shared memory: the
+// lower triangle of A (type TA) is loaded once into S (column-major, leading
+// dimension n + 1, so the rows of a column and the columns of a row spread
+// over the banks), factored in place blocked by 32 (the diagonal block by
+// one warp with shuffles, the panel by the warps four rows at a time, the
+// trailing update by all threads in 2 x 2 register tiles from shared
+// memory), and the factor is stored to the lower triangle of Out (type T).
+// No global traffic between the load and the store, and three barriers per
+// block column.  Pivot rules, return value and failure behaviour as
+// cholesky (Out is then not written).  S: cholesky_smem_elems(n) elements
+// of T.
+template <int NT, typename T, typename TA>
+__device__ int cholesky_smem(int n, const TA* A, int lda, T* Out, int ldo, bool adjust, T* S, int* s_flag)
+{
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int ld = n + 1;
+  T* rcp = S + (size_t)n * ld;  // reciprocals of the current diagonal block
+  for (int t = tid; t < n * n; t += NT) {
+    const int i = t % n, j = t / n;
+    if (i >= j) S[i + ld * j] = (T)A[i + (size_t)lda * j];
+  }
+  __syncthreads();
+  for (int kb = 0; kb < n; kb += NB) {
+    const int bs = min(NB, n - kb);
+    T* Dg = S + kb * (ld + 1);
+    if (wid == 0) {
+      const int fail = warp_potrf32<T>(bs, Dg, adjust, kb, ld);
+      if (lane == 0) *s_flag = fail;
+      if (!fail && lane < bs) rcp[lane] = (T)1 / Dg[lane + ld * lane];
+    }
+    __syncthreads();
+    const int f = *s_flag;
+    if (f) { __syncthreads(); return f; }
+    const int r0 = kb + bs, rem = n - r0;
+    if (rem <= 0) break;
+    // panel: S[r, kb:kb+bs] := S[r, kb:kb+bs] L_bb^{-T}, four rows per warp
+    for (int rb = r0 + 4 * wid; rb < n; rb += 4 * (NT / 32)) {
+      T x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = (lane < bs && rb + u < n) ? S[(rb + u) + ld * (kb + lane)] : (T)0;
+      for (int c = 0; c < bs; ++c) {
+        const T dinv = rcp[c];
+        const T lc = (lane > c && lane < bs) ? Dg[lane + ld * c] : (T)0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (lane == c) x[u] *= dinv;
+          const T xc = __shfl_sync(0xffffffffu, x[u], c);
+          x[u] -= xc * lc;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (lane < bs && rb + u < n) S[(rb + u) + ld * (kb + lane)] = x[u];
+    }
+    __syncthreads();
+    // trailing: S22 -= P P^T on and below the diagonal, P = S[r0:, kb:kb+bs],
+    // in 2 x 2 tiles (tile rows I >= tile columns J)
+    const int T2 = (rem + 1) / 2;
+    const int ntile = T2 * (T2 + 1) / 2;
+    for (int q = tid; q < ntile; q += NT) {
+      int I = (int)((sqrtf(8.0f * (float)q + 1.0f) - 1.0f) * 0.5f);
+      while ((I + 1) * (I + 2) / 2 <= q) ++I;
+      while (I * (I + 1) / 2 > q) --I;
+      const int J = q - I * (I + 1) / 2;
+      const int i0 = r0 + 2 * I, j0 = r0 + 2 * J;
+      const bool i1ok = i0 + 1 < n, j1ok = j0 + 1 < n;
+      T s00 = 0, s01 = 0, s10 = 0, s11 = 0;
+      const T* P = S + ld * kb;
+      for (int k = 0; k < bs; ++k) {
+        const T a0 = P[i0 + ld * k], a1 = i1ok ? P[i0 + 1 + ld * k] : (T)0;
+        const T b0 = P[j0 + ld * k], b1 = j1ok ? P[j0 + 1 + ld * k] : (T)0;
+        s00 += a0 * b0;
+        s01 += a0 * b1;
+        s10 += a1 * b0;
+        s11 += a1 * b1;
+      }
+      S[i0 + ld * j0] -= s00;
+      if (i1ok) S[i0 + 1 + ld * j0] -= s10;
+      if (j1ok && i0 >= j0 + 1) S[i0 + ld * (j0 + 1)] -= s01;
+      if (i1ok && j1ok) S[i0 + 1 + ld * (j0 + 1)] -= s11;
+    }
+    __syncthreads();
+  }
+  for (int t = tid; t < n * n; t += NT) {
+    const int i = t % n, j = t / n;
+    if (i >= j) Out[i + (size_t)ldo * j] = S[i + ld * j];
+  }
+  __syncthreads();
+  return 0;
+}
+
 // In-place lower Cholesky, right-looking, blocked by 32, pivot rules as
 // warp_potrf32.  Returns 0 on success, else the failing column + 1.  The
 // strict upper triangle is zeroed on success when zero_upper is set (callers

@@ -174,27 +174,69 @@ __device__ __forceinline__ double f3_value_slice(int o, int in, long long e_beg,
 // diagonal are stored with consecutive threads on consecutive rows
 // (coalesced).  Threads as 32 x 8, four pairs each.
 constexpr int F3T = 32;
+// F3 value of a pair of single-entry constraints (r1, c1, v1), (r2, c2, v2)
+// (the one-entry case of f3_value_slice; the first as the outer loop).
+__device__ __forceinline__ double f3_value_11(int al, int be, double v1, int ga, int de, double v2, const double* X,
+                                              const double* Zi, int n)
+{
+  const double* Xa = X + (size_t)n * al;
+  const double* Xb = X + (size_t)n * be;
+  const double* Za = Zi + (size_t)n * al;
+  const double* Zb = Zi + (size_t)n * be;
+  double plu;
+  if (al != be) {
+    plu = (ga != de) ? Zb[de] * Xa[ga] + Zb[ga] * Xa[de] + Za[de] * Xb[ga] + Za[ga] * Xb[de]
+                     : Zb[de] * Xa[ga] + Za[de] * Xb[ga];
+  } else {
+    plu = (ga != de) ? Zb[de] * Xa[ga] + Zb[ga] * Xa[de] : Zb[de] * Xa[ga];
+  }
+  return v1 * (v2 * plu);
+}
+
 __global__ void __launch_bounds__(256) k_f3_tiles(int m, const long long* ptr, const int* row, const int* col,
                                                   const double* val, const int* nnz, const double* X,
                                                   const double* Zi, int n, double* B)
 {
   __shared__ double tile[F3T][F3T + 1];
+  // the tile's row and column constraints: entry count, NonZeroEffect and
+  // (for single-entry constraints) the entry itself, loaded once per tile
+  __shared__ long long s_cnt[2][F3T];
+  __shared__ int s_nnz[2][F3T], s_r[2][F3T], s_c[2][F3T];
+  __shared__ double s_v[2][F3T];
   const long long t = blockIdx.x;
   int ti = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
   while ((long long)(ti + 1) * (ti + 2) / 2 <= t) ++ti;
   while ((long long)ti * (ti + 1) / 2 > t) --ti;
   const int tj = (int)(t - (long long)ti * (ti + 1) / 2);
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  if (ty < 2) {
+    const int q = (ty == 0 ? ti : tj) * F3T + tx;
+    if (q < m) {
+      const long long b0 = ptr[q], c = ptr[q + 1] - b0;
+      s_cnt[ty][tx] = c;
+      s_nnz[ty][tx] = nnz[q];
+      s_r[ty][tx] = (c > 0) ? row[b0] : 0;
+      s_c[ty][tx] = (c > 0) ? col[b0] : 0;
+      s_v[ty][tx] = (c > 0) ? val[b0] : 0.0;
+    }
+  }
+  __syncthreads();
   const int i = ti * F3T + tx;
 #pragma unroll
   for (int k = 0; k < F3T / 8; ++k) {
     const int jl = ty + 8 * k, j = tj * F3T + jl;
     double v = 0.0;
     if (i < m && j < m && (ti > tj || tx >= jl)) {
-      const long long ci = ptr[i + 1] - ptr[i], cj = ptr[j + 1] - ptr[j];
-      // heavy pairs are left to k_f3_heavy (stored as 0 here, overwritten there)
-      if (ci * cj <= F3_HEAVY) {
-        const int o = (nnz[j] >= nnz[i]) ? j : i, in = (o == j) ? i : j;
+      const long long ci = s_cnt[0][tx], cj = s_cnt[1][jl];
+      if (ci == 1 && cj == 1) {
+        // j outer when it dominates (equal NonZeroEffect: either order)
+        if (s_nnz[1][jl] >= s_nnz[0][tx])
+          v = f3_value_11(s_r[1][jl], s_c[1][jl], s_v[1][jl], s_r[0][tx], s_c[0][tx], s_v[0][tx], X, Zi, n);
+        else
+          v = f3_value_11(s_r[0][tx], s_c[0][tx], s_v[0][tx], s_r[1][jl], s_c[1][jl], s_v[1][jl], X, Zi, n);
+      } else if (ci * cj <= F3_HEAVY) {
+        // heavy pairs are left to k_f3_heavy (stored as 0 here, overwritten there)
+        const int o = (s_nnz[1][jl] >= s_nnz[0][tx]) ? j : i, in = (o == j) ? i : j;
         v = f3_value_slice(o, in, 0, 1, ptr, row, col, val, X, Zi, n);
       }
     }
@@ -215,22 +257,29 @@ __global__ void __launch_bounds__(256) k_f3_tiles(int m, const long long* ptr, c
 
 // The heavy pairs of the one-source F3 assembly (entry pairs above
 // F3_HEAVY, e.g. the trace constraint of Lovasz theta with itself): one
-// block of threads per pair, the outer constraint's entries dealt over the
-// threads, a fixed-order block reduction; runs after k_f3_tiles.
-__global__ void __launch_bounds__(256) k_f3_heavy(int m, const int* pairs, const long long* ptr, const int* row,
-                                                  const int* col, const double* val, const int* nnz,
-                                                  const double* X, const double* Zi, int n, double* B)
+// block of 1024 threads per pair, the (outer, inner) entry pairs dealt over
+// the threads, a fixed-order block reduction; runs after k_f3_tiles.
+__global__ void __launch_bounds__(1024) k_f3_heavy(int m, const int* pairs, const long long* ptr, const int* row,
+                                                   const int* col, const double* val, const int* nnz,
+                                                   const double* X, const double* Zi, int n, double* B)
 {
-  __shared__ double red[8];
+  __shared__ double red[32];
   const int i = pairs[2 * blockIdx.x], j = pairs[2 * blockIdx.x + 1];
   const int o = (nnz[j] >= nnz[i]) ? j : i, in = (o == j) ? i : j;
-  double v = f3_value_slice(o, in, threadIdx.x, 256, ptr, row, col, val, X, Zi, n);
+  // the (outer, inner) entry pairs dealt over the threads
+  const long long ob = ptr[o], ib = ptr[in], ci = ptr[in + 1] - ib;
+  const long long tot = (ptr[o + 1] - ob) * ci;
+  double v = 0.0;
+  for (long long f = threadIdx.x; f < tot; f += 1024) {
+    const long long e1 = ob + f / ci, e2 = ib + f % ci;
+    v += f3_value_11(row[e1], col[e1], val[e1], row[e2], col[e2], val[e2], X, Zi, n);
+  }
   for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0.0;
-    for (int w = 0; w < 8; ++w) s += red[w];
+    for (int w = 0; w < 32; ++w) s += red[w];
     B[i + (size_t)m * j] = s;
     B[j + (size_t)m * i] = s;
   }
@@ -2145,7 +2194,7 @@ int Solver::solve(const InitPoint* init, const Params* prm)
         k_f3_tiles<<<(unsigned)(T * (T + 1) / 2), 256>>>(m, B0.ptr, B0.row, B0.col, B0.val, B0.nnz, B0.X, B0.Zi,
                                                           B0.n, S.B);
         if (S.f3_nheavy)
-          k_f3_heavy<<<(unsigned)S.f3_nheavy, 256>>>(m, S.f3_heavy, B0.ptr, B0.row, B0.col, B0.val, B0.nnz, B0.X,
+          k_f3_heavy<<<(unsigned)S.f3_nheavy, 1024>>>(m, S.f3_heavy, B0.ptr, B0.row, B0.col, B0.val, B0.nnz, B0.X,
                                                      B0.Zi, B0.n, S.B);
         return;
       }
