@@ -51,8 +51,9 @@ static size_t smem_bytes_for(int nmax, int mmax, long long gsm, int bt)
          (size_t)(2 * mmax + nmax) * sizeof(int) + 64;
 }
 
-// Shared memory of one SM and what the system reserves per resident block.
-constexpr long long SM_SMEM_BYTES = 228LL * 1024, BLOCK_RESERVED_BYTES = 1024;
+// Shared memory of one SM, what the system reserves per resident block, and
+// an allowance for the solver kernel's static shared memory (under 1 KB).
+constexpr long long SM_SMEM_BYTES = 228LL * 1024, BLOCK_RESERVED_BYTES = 1024, STATIC_SMEM_BYTES = 1024;
 
 // Staging area for `per_sm` resident blocks of bt threads: at least the
 // square GEMM's double-buffered tiles (cta::gemm_smem_min) and the two
@@ -72,7 +73,8 @@ static long long staging_doubles(int nmax, int mmax, int want, int bt, int per_s
   // nothing uses more than both Lanczos matrices or the FP64 factorisation
   long long s = (want > 0) ? want : std::max(2 * m2, cta::cholesky_smem_elems(mmax));
   const long long per_block = std::min<long long>(227LL * 1024, SM_SMEM_BYTES / std::max(per_sm, 1) -
-                                                                    BLOCK_RESERVED_BYTES);
+                                                                    BLOCK_RESERVED_BYTES) -
+                              STATIC_SMEM_BYTES;
   const long long cap = (per_block - (long long)smem_bytes_for(nmax, mmax, 0, bt)) / (long long)sizeof(double);
   if (s > cap) s = cap;
   s = s / 32 * 32;
@@ -867,7 +869,11 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
       // ---- update (Solutions::update, sdpa_dataset.cpp:145-171)
       {
         const double ap = S.alphaP, ad = S.alphaD;
-        // X += ap dX, Z += ad dZ, and the copies the factorisations work on
+        // the factorisations run in shared memory when the staging area
+        // holds one n x n matrix (X, then Z, read straight from X and Z);
+        // else in lockstep on copies in W2, W1
+        const bool xz_smem = cta::cholesky_smem_elems(n) <= (long long)gsm_doubles;
+        // X += ap dX, Z += ad dZ (and the copies the L2 factorisations work on)
         for (int t = tid; t < nn_i; t += BT) {
           const double x = X[t] + ap * dX[t];
           double z = Z[t];
@@ -875,14 +881,21 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
           else if ((t % n) == (t / n)) z += ad * vdz[t / n];
           X[t] = x;
           Z[t] = z;
-          W2[t] = x;
-          W1[t] = z;
+          if (!xz_smem) {
+            W2[t] = x;
+            W1[t] = z;
+          }
         }
         for (int k = tid; k < m; k += BT) vy[k] += ad * vdy[k];
         __syncthreads();
         if (cannot_move(S)) break;
         // X and Z factored and inverted in lockstep (either failing ends the loop)
-        if (cta::cholesky_pair<BT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false)) break;  // inverses read the lower triangles
+        if (xz_smem) {
+          if (cta::cholesky_smem<BT, double, double>(n, X, n, W2, n, false, gsm, &s_flag)) break;
+          if (cta::cholesky_smem<BT, double, double>(n, Z, n, W1, n, false, gsm, &s_flag)) break;
+        } else if (cta::cholesky_pair<BT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false)) {
+          break;  // the inverses read the lower triangles only
+        }
         cta::tri_inverse_pair<BT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
         cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
@@ -970,15 +983,22 @@ static int launch_shape(const sdpab_batch* prob, int want_bt, int want_per_sm, i
   L.bt = (want_bt == 128) ? 128 : 256;
   const int per_sm_req = (want_per_sm > 0) ? want_per_sm : (L.bt == 128 ? 4 : 2);
   L.gsm = staging_doubles(prob->nmax, prob->mmax, want_staging, L.bt, per_sm_req);
-  L.shm = smem_bytes_for(prob->nmax, prob->mmax, L.gsm, L.bt);
   void* k = solver_kernel(prob, L.bt);
-  if (L.shm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.shm);
-    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
-  }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, L.bt, L.shm);
-  if (e != cudaSuccess) return cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  // the default staging is the budget of per_sm_req blocks; should the
+  // device fit fewer of that size, it shrinks (1 KB at a time) to the size
+  // that fits them
+  for (;;) {
+    L.shm = smem_bytes_for(prob->nmax, prob->mmax, L.gsm, L.bt);
+    if (L.shm > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.shm);
+      if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
+    }
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, L.bt, L.shm);
+    if (e != cudaSuccess) return cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm >= per_sm_req || want_staging > 0 || L.gsm - 128 < staging_min(L.bt)) break;
+    L.gsm -= 128;
+  }
   if (per_sm < 1) {
     char msg[160];
     snprintf(msg, sizeof(msg), "%s: the solver block does not fit on an SM", who);
