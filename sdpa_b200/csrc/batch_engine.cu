@@ -872,7 +872,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
         // the factorisations run in shared memory when the staging area
         // holds one n x n matrix (X, then Z, read straight from X and Z);
         // else in lockstep on copies in W2, W1
-        const bool xz_smem = cta::cholesky_smem_elems(n) <= (long long)gsm_doubles;
+        const bool xz_smem = cta::cholesky_smem_elems(n) <= (long long)gsm_doubles && n <= 160;
         // X += ap dX, Z += ad dZ (and the copies the L2 factorisations work on)
         for (int t = tid; t < nn_i; t += BT) {
           const double x = X[t] + ap * dX[t];
@@ -891,13 +891,23 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
         if (cannot_move(S)) break;
         // X and Z factored and inverted in lockstep (either failing ends the loop)
         if (xz_smem) {
-          if (cta::cholesky_smem<BT, double, double>(n, X, n, W2, n, false, gsm, &s_flag)) break;
-          if (cta::cholesky_smem<BT, double, double>(n, Z, n, W1, n, false, gsm, &s_flag)) break;
-        } else if (cta::cholesky_pair<BT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false)) {
-          break;  // the inverses read the lower triangles only
+          // in shared memory, X then Z: factor, invert the factor in place,
+          // store it (and Z^-1 = L_Z^-T L_Z^-1, formed from shared memory)
+          cta::smem_load_lower<BT, double, double>(n, X, n, gsm);
+          if (cta::smem_potrf<BT, double>(n, gsm, false, &s_flag)) break;
+          cta::smem_trtri<BT>(n, gsm);
+          cta::smem_store_lower<BT, double>(n, gsm, LXi, n, true);
+          cta::smem_load_lower<BT, double, double>(n, Z, n, gsm);
+          if (cta::smem_potrf<BT, double>(n, gsm, false, &s_flag)) break;
+          cta::smem_trtri<BT>(n, gsm);
+          cta::smem_store_lower<BT, double>(n, gsm, LZi, n, true);
+          cta::smem_ltl<BT>(n, gsm, Zi, n);
+        } else {
+          if (cta::cholesky_pair<BT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false))
+            break;  // the inverses read the lower triangles only
+          cta::tri_inverse_pair<BT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
+          cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
         }
-        cta::tri_inverse_pair<BT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
-        cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
       // ---- residuals and scalars
       {

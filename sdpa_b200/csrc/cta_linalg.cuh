@@ -720,28 +720,47 @@ static __device__ __noinline__ int warp_potrf32(int bs, T* sD, bool adjust, int 
 // Shared memory (elements of T) cholesky_smem needs for order n.
 __host__ __device__ constexpr long long cholesky_smem_elems(int n) { return (long long)n * (n + 1) + NB; }
 
-// Lower Cholesky of an n x n matrix factored entirely in shared memory: the
-// lower triangle of A (type TA) is loaded once into S (column-major, leading
-// dimension n + 1, so the rows of a column and the columns of a row spread
-// over the banks), factored in place blocked by 32 (the diagonal block by
-// one warp with shuffles, the panel by the warps four rows at a time, the
-// trailing update by all threads in 2 x 2 register tiles from shared
-// memory), and the factor is stored to the lower triangle of Out (type T).
-// No global traffic between the load and the store, and three barriers per
-// block column.  Pivot rules, return value and failure behaviour as
-// cholesky (Out is then not written).  S: cholesky_smem_elems(n) elements
-// of T.
+// The pieces of a factorisation held entirely in shared memory: S is the
+// n x n matrix column-major with leading dimension n + 1 (so the rows of a
+// column and the columns of a row spread over the banks), followed by NB
+// elements of scratch (the reciprocals of the current diagonal block).
+
+// S = lower triangle of A (type TA, converted to T).  Ends with a barrier.
 template <int NT, typename T, typename TA>
-__device__ int cholesky_smem(int n, const TA* A, int lda, T* Out, int ldo, bool adjust, T* S, int* s_flag)
+__device__ void smem_load_lower(int n, const TA* A, int lda, T* S)
 {
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int ld = n + 1;
-  T* rcp = S + (size_t)n * ld;  // reciprocals of the current diagonal block
-  for (int t = tid; t < n * n; t += NT) {
+  for (int t = threadIdx.x; t < n * n; t += NT) {
     const int i = t % n, j = t / n;
     if (i >= j) S[i + ld * j] = (T)A[i + (size_t)lda * j];
   }
   __syncthreads();
+}
+
+// Out = lower triangle of S (strict upper zeroed when zero_upper).  Ends
+// with a barrier.
+template <int NT, typename T>
+__device__ void smem_store_lower(int n, const T* S, T* Out, int ldo, bool zero_upper)
+{
+  const int ld = n + 1;
+  for (int t = threadIdx.x; t < n * n; t += NT) {
+    const int i = t % n, j = t / n;
+    if (i >= j) Out[i + (size_t)ldo * j] = S[i + ld * j];
+    else if (zero_upper) Out[i + (size_t)ldo * j] = (T)0;
+  }
+  __syncthreads();
+}
+
+// In-place lower Cholesky of S, blocked by 32 (the diagonal block by one
+// warp with shuffles, the panel by the warps four rows at a time, the
+// trailing update by all threads in 2 x 2 register tiles), three barriers
+// per block column.  Pivot rules and return value as cholesky.
+template <int NT, typename T>
+__device__ int smem_potrf(int n, T* S, bool adjust, int* s_flag)
+{
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int ld = n + 1;
+  T* rcp = S + (size_t)n * ld;  // reciprocals of the current diagonal block
   for (int kb = 0; kb < n; kb += NB) {
     const int bs = min(NB, n - kb);
     T* Dg = S + kb * (ld + 1);
@@ -803,12 +822,126 @@ __device__ int cholesky_smem(int n, const TA* A, int lda, T* Out, int ldo, bool 
     }
     __syncthreads();
   }
-  for (int t = tid; t < n * n; t += NT) {
+  return 0;
+}
+
+// Lower Cholesky of an n x n matrix factored entirely in shared memory: the
+// lower triangle of A (type TA) is loaded once into S, factored in place
+// (smem_potrf), and the factor is stored to the lower triangle of Out (type
+// T); no global traffic between the load and the store.  Pivot rules,
+// return value and failure behaviour as cholesky (Out is then not written).
+// S: cholesky_smem_elems(n) elements of T.
+template <int NT, typename T, typename TA>
+__device__ int cholesky_smem(int n, const TA* A, int lda, T* Out, int ldo, bool adjust, T* S, int* s_flag)
+{
+  smem_load_lower<NT, T, TA>(n, A, lda, S);
+  const int f = smem_potrf<NT, T>(n, S, adjust, s_flag);
+  if (f) return f;
+  smem_store_lower<NT, T>(n, S, Out, ldo, false);
+  return 0;
+}
+
+// In-place inverse of the lower-triangular factor in S (LAPACK trtri's
+// blocked lower algorithm): the block columns are taken from the last to
+// the first; with J the current block, T the rows below it (whose block
+// S[T, T] already holds L_TT^{-1}):
+//   S[J, J] <- L_JJ^{-1}                       (one warp, column per lane)
+//   S[T, J] <- -L_TT^{-1} (L_TJ L_JJ^{-1})    (two products, all threads)
+// Each product is computed into registers (up to PER outputs per thread),
+// then written after a barrier, so it can overwrite its own operand.
+// Requires n <= NT * PER / NB rows below any block (n <= 544 with 256
+// threads).
+template <int NT>
+__device__ void smem_trtri(int n, double* S)
+{
+  constexpr int PER = 16;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int ld = n + 1;
+  const int nblk = (n + NB - 1) / NB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int kb = b * NB, bs = min(NB, n - kb);
+    double* D = S + kb * (ld + 1);
+    // (1) diagonal block: lane c computes column c of L_JJ^{-1} by forward
+    // substitution, reading the rows of L_JJ from shared memory (broadcast)
+    if (wid == 0) {
+      double x[NB];
+#pragma unroll
+      for (int r = 0; r < NB; ++r) {
+        double v = 0.0;
+        if (r < bs) {
+          double acc = (r == lane) ? 1.0 : 0.0;
+#pragma unroll
+          for (int k = 0; k < r; ++k)
+            if (k >= lane) acc -= D[r + ld * k] * x[k];
+          if (lane < bs && r >= lane) v = acc / D[r + ld * r];
+        }
+        x[r] = v;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int r = 0; r < NB; ++r)
+        if (r < bs && lane < bs && r >= lane) D[r + ld * lane] = x[r];
+    }
+    __syncthreads();
+    const int r0 = kb + bs, rem = n - r0;
+    if (rem <= 0) continue;
+    // (2) W = L_TJ L_JJ^{-1}: w[t, c] = sum_{k >= c} L[t, k] Linv[k, c]
+    double o[PER];
+    const int tot = rem * bs;
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * NT;
+      double acc = 0.0;
+      if (e < tot) {
+        const int t = r0 + e % rem, c = e / rem;
+        for (int k = c; k < bs; ++k) acc += S[t + ld * (kb + k)] * D[k + ld * c];
+      }
+      o[u] = acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * NT;
+      if (e < tot) S[(r0 + e % rem) + ld * (kb + e / rem)] = o[u];
+    }
+    __syncthreads();
+    // (3) S[T, J] = -L_TT^{-1} W: y[t, c] = -sum_{r0 <= k <= t} M[t, k] W[k, c]
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * NT;
+      double acc = 0.0;
+      if (e < tot) {
+        const int t = r0 + e % rem, c = kb + e / rem;
+        for (int k = r0; k <= t; ++k) acc += S[t + ld * k] * S[k + ld * c];
+      }
+      o[u] = -acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * NT;
+      if (e < tot) S[(r0 + e % rem) + ld * (kb + e / rem)] = o[u];
+    }
+    __syncthreads();
+  }
+}
+
+// Zi = Li^T Li for the lower-triangular Li in S (the inverse of Z from the
+// inverse of its Cholesky factor), written in full (both triangles) to Zi:
+// Zi[i, j] = sum_{k >= max(i, j)} Li[k, i] Li[k, j].  Ends with a barrier.
+template <int NT>
+__device__ void smem_ltl(int n, const double* S, double* Zi, int ldz)
+{
+  const int ld = n + 1;
+  for (int t = threadIdx.x; t < n * n; t += NT) {
     const int i = t % n, j = t / n;
-    if (i >= j) Out[i + (size_t)ldo * j] = S[i + ld * j];
+    if (i < j) continue;
+    double acc = 0.0;
+    for (int k = i; k < n; ++k) acc += S[k + ld * i] * S[k + ld * j];
+    Zi[i + (size_t)ldz * j] = acc;
+    Zi[j + (size_t)ldz * i] = acc;
   }
   __syncthreads();
-  return 0;
 }
 
 // In-place lower Cholesky, right-looking, blocked by 32, pivot rules as
