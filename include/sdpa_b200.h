@@ -316,6 +316,9 @@ typedef struct sdpab_batch_config {
   double refine_tol;           /* mixed mode: the FP64 refinement of a solve with the
                                   FP32 Schur factor stops once the correction is below
                                   this times |dy| (0 = 1e-8; three steps at most) */
+  int factor_smem;             /* 1: the Schur factorisation runs in shared memory
+                                  when the staging area holds it (m (m + 1) + 32
+                                  elements), 0: blocked from L2 */
 } sdpab_batch_config;
 
 /* Tensor-core lower update C -= P P^T of an M x M FP32 matrix, P M x K

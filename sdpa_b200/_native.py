@@ -56,7 +56,7 @@ class BatchResult(ctypes.Structure):
 class BatchConfig(ctypes.Structure):
     _fields_ = [("precision", c_int), ("ctas_per_sm", c_int), ("mixed_switch_gap", c_double),
                 ("staging_doubles", c_int), ("mixed_products", c_int), ("block_threads", c_int),
-                ("refine_tol", c_double)]
+                ("refine_tol", c_double), ("factor_smem", c_int)]
 
 
 class SdpaInfo(ctypes.Structure):

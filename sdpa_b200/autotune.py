@@ -13,6 +13,9 @@ decides how its dense steps map onto the SM:
 * ctas_per_sm: resident blocks per SM (the staging area is sized to fit
   them); more blocks also put more per-block workspace (about 15 n^2 doubles
   each) into L2.
+* factor_smem: the Schur factorisation in shared memory (the whole m x m
+  matrix loaded once, factored there, stored once) when the staging area
+  holds it, or blocked from L2 with the GEMM tiles on the FP64 MMA.
 * mixed_products (mixed precision only): the n^3 products of the FP32 phase
   on the FP64 MMA (0) or in FP32 on the SIMT pipe (1).
 
@@ -45,8 +48,8 @@ def label(shape: dict) -> str:
 
 def tune(db, precision: int = 0, candidates=None, reps: int = 2, run=None, stream=None) -> dict:
     """Times one solve step for each candidate shape (dicts of DeviceBatch.solve
-    keyword arguments; default SHAPES, and for mixed precision both product
-    precisions on the fastest shape); returns {"best": shape, "ms": {label:
+    keyword arguments; default SHAPES, then on the fastest the shared-memory
+    Schur factorisation and, for mixed precision, FP32 products); returns {"best": shape, "ms": {label:
     ms}, "class": nmax class} and caches the choice.  `run(shape)` issues the
     step (default: db.solve with that shape) on `stream`."""
     import torch
@@ -73,9 +76,12 @@ def tune(db, precision: int = 0, candidates=None, reps: int = 2, run=None, strea
 
     for shape in (candidates or SHAPES):
         time(shape)
-    if precision == N.PREC_MIXED and candidates is None:
+    if candidates is None:
         top = dict(shapes[min(res, key=res.get)])
-        time(dict(top, mixed_products=1))
+        time(dict(top, factor_smem=1))
+        if precision == N.PREC_MIXED:
+            top = dict(shapes[min(res, key=res.get)])
+            time(dict(top, mixed_products=1))
     choice = shapes[min(res, key=res.get)]
     _cache[key] = choice
     return {"best": choice, "ms": res, "class": key[0]}

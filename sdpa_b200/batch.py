@@ -179,14 +179,14 @@ def _params(params):
 
 
 def _config(precision=N.PREC_FP64, ctas_per_sm=0, mixed_switch_gap=0.0, staging=0, mixed_products=0,
-            block_threads=0, refine_tol=0.0):
+            block_threads=0, refine_tol=0.0, factor_smem=0):
     return N.BatchConfig(precision, ctas_per_sm, mixed_switch_gap, staging, mixed_products, block_threads,
-                         refine_tol)
+                         refine_tol, factor_smem)
 
 
 def solve_host(P: Packed, params=None, precision=N.PREC_FP64, want_x=True, want_mats=False,
                init=None, ctas_per_sm=0, staging=0, block_threads=0, mixed_products=0,
-               mixed_switch_gap=0.0, refine_tol=0.0) -> BatchResult:
+               mixed_switch_gap=0.0, refine_tol=0.0, factor_smem=0) -> BatchResult:
     """sdpab_batch_solve_host on host arrays.  init = (flag, xvec, X, Y) in
     the packed layouts (user X / Y as in SDPA::inputInitXMat / inputInitYMat).
     The launch shape (block_threads, ctas_per_sm, staging) and the mixed
@@ -211,7 +211,8 @@ def solve_host(P: Packed, params=None, precision=N.PREC_FP64, want_x=True, want_
         keep = [flag, xv, Xu, Yu]
         bi = ctypes.byref(N.BatchInit(_ptr(flag), _ptr(xv), _ptr(Xu), _ptr(Yu), margin))
     prm = _params(params)
-    cfg = _config(precision, ctas_per_sm, mixed_switch_gap, staging, mixed_products, block_threads, refine_tol)
+    cfg = _config(precision, ctas_per_sm, mixed_switch_gap, staging, mixed_products, block_threads, refine_tol,
+                  factor_smem)
     N.check(L.sdpab_batch_solve_host(ctypes.byref(bt), bi, ctypes.byref(prm), ctypes.byref(cfg),
                                      ctypes.byref(br)), "sdpab_batch_solve_host")
     del keep
@@ -253,13 +254,14 @@ class DeviceBatch:
         self.init = N.BatchInit(*[None if x is None else x.data_ptr() for x in self._init_t], margin)
 
     def solve(self, params=None, precision=N.PREC_FP64, stream=None, ctas_per_sm=0, staging=0, block_threads=0,
-              mixed_products=0, mixed_switch_gap=0.0, refine_tol=0.0):
+              mixed_products=0, mixed_switch_gap=0.0, refine_tol=0.0, factor_smem=0):
         """block_threads / ctas_per_sm / staging: launch shape (0 = defaults;
         see sdpa_b200.autotune); mixed_products / mixed_switch_gap: options of
         the mixed mode (sdpab_batch_config)."""
         import torch
         prm = _params(params)
-        cfg = _config(precision, ctas_per_sm, mixed_switch_gap, staging, mixed_products, block_threads, refine_tol)
+        cfg = _config(precision, ctas_per_sm, mixed_switch_gap, staging, mixed_products, block_threads, refine_tol,
+                      factor_smem)
         s = stream if stream is not None else torch.cuda.current_stream()
         N.check(N.lib().sdpab_batch_solve(ctypes.byref(self._bt),
                                           ctypes.byref(self.init) if self.init is not None else None,

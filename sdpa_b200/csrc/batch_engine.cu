@@ -57,9 +57,10 @@ constexpr long long SM_SMEM_BYTES = 228LL * 1024, BLOCK_RESERVED_BYTES = 1024, S
 
 // Staging area for `per_sm` resident blocks of bt threads: at least the
 // square GEMM's double-buffered tiles (cta::gemm_smem_min) and the two
-// diagonal blocks; `want` doubles when given, by default all the shared
-// memory per_sm blocks of this size can have (more of it keeps the Lanczos
-// matrices and the Schur factorisation in shared memory for larger n).
+// diagonal blocks; `want` doubles when given, by default both Lanczos
+// matrices (2 n^2) when they fit in LANCZOS_SMEM_DOUBLES, else one, else
+// the minimum; capped at what per_sm blocks of this size can have.  (Shared
+// memory beyond that is taken from the L1 cache the workspace loads use.)
 static long long staging_min(int bt)
 {
   const long long g = (bt >= 256) ? cta::gemm_smem_min<256>() : cta::gemm_smem_min<128>();
@@ -70,8 +71,11 @@ static long long staging_doubles(int nmax, int mmax, int want, int bt, int per_s
 {
   const long long g = staging_min(bt);
   const long long m2 = (long long)nmax * nmax;
-  // nothing uses more than both Lanczos matrices or the FP64 factorisation
-  long long s = (want > 0) ? want : std::max(2 * m2, cta::cholesky_smem_elems(mmax));
+  long long s;
+  if (want > 0) s = want;
+  else if (2 * m2 <= LANCZOS_SMEM_DOUBLES) s = 2 * m2;
+  else if (m2 <= LANCZOS_SMEM_DOUBLES) s = m2;
+  else s = g;
   const long long per_block = std::min<long long>(227LL * 1024, SM_SMEM_BYTES / std::max(per_sm, 1) -
                                                                     BLOCK_RESERVED_BYTES) -
                               STATIC_SMEM_BYTES;
@@ -92,6 +96,7 @@ struct BatchArgs {
   int mixed_products;    // mixed mode: the n^3 products in FP32 as well (else on the FP64 MMA)
   double mu_switch;
   double refine_tol;     // mixed mode: refinement stops once the correction is below this times |dy|
+  int factor_smem;       // the Schur factorisation in shared memory when the staging area holds it
   double* ws;
   long long ws_stride;  // doubles per block
   int* queue;
@@ -680,7 +685,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
     // adjusted FP64 Cholesky of B in place (solves read the lower triangle):
     // in shared memory when the staging area holds it, else blocked from L2
     auto factor_fp64 = [&]() -> int {
-      if (cta::cholesky_smem_elems(m) <= (long long)gsm_doubles)
+      if (a.factor_smem && cta::cholesky_smem_elems(m) <= (long long)gsm_doubles)
         return cta::cholesky_smem<BT, double, double>(m, B, m, B, m, true, gsm, &s_flag);
       return cta::cholesky<BT, double>(m, B, m, true, sD, gsm, &s_flag, false);
     };
@@ -738,7 +743,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
       // iteration and the rest of the solve to the FP64 factor.
       bool f32 = false;
       if (lowp) {
-        if (cta::cholesky_smem_elems(m) <= 2LL * gsm_doubles) {
+        if (a.factor_smem && cta::cholesky_smem_elems(m) <= 2LL * gsm_doubles) {
           f32 = cta::cholesky_smem<BT, float, double>(m, B, m, B32, m, true, (float*)gsm, &s_flag) == 0;
         } else {
           for (int t = tid; t < m * m; t += BT) B32[t] = (float)B[t];
@@ -869,11 +874,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
       // ---- update (Solutions::update, sdpa_dataset.cpp:145-171)
       {
         const double ap = S.alphaP, ad = S.alphaD;
-        // the factorisations run in shared memory when the staging area
-        // holds one n x n matrix (X, then Z, read straight from X and Z);
-        // else in lockstep on copies in W2, W1
-        const bool xz_smem = cta::cholesky_smem_elems(n) <= (long long)gsm_doubles && n <= 160;
-        // X += ap dX, Z += ad dZ (and the copies the L2 factorisations work on)
+        // X += ap dX, Z += ad dZ, and the copies the factorisations work on
         for (int t = tid; t < nn_i; t += BT) {
           const double x = X[t] + ap * dX[t];
           double z = Z[t];
@@ -881,33 +882,17 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
           else if ((t % n) == (t / n)) z += ad * vdz[t / n];
           X[t] = x;
           Z[t] = z;
-          if (!xz_smem) {
-            W2[t] = x;
-            W1[t] = z;
-          }
+          W2[t] = x;
+          W1[t] = z;
         }
         for (int k = tid; k < m; k += BT) vy[k] += ad * vdy[k];
         __syncthreads();
         if (cannot_move(S)) break;
         // X and Z factored and inverted in lockstep (either failing ends the loop)
-        if (xz_smem) {
-          // in shared memory, X then Z: factor, invert the factor in place,
-          // store it (and Z^-1 = L_Z^-T L_Z^-1, formed from shared memory)
-          cta::smem_load_lower<BT, double, double>(n, X, n, gsm);
-          if (cta::smem_potrf<BT, double>(n, gsm, false, &s_flag)) break;
-          cta::smem_trtri<BT>(n, gsm);
-          cta::smem_store_lower<BT, double>(n, gsm, LXi, n, true);
-          cta::smem_load_lower<BT, double, double>(n, Z, n, gsm);
-          if (cta::smem_potrf<BT, double>(n, gsm, false, &s_flag)) break;
-          cta::smem_trtri<BT>(n, gsm);
-          cta::smem_store_lower<BT, double>(n, gsm, LZi, n, true);
-          cta::smem_ltl<BT>(n, gsm, Zi, n);
-        } else {
-          if (cta::cholesky_pair<BT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false))
-            break;  // the inverses read the lower triangles only
-          cta::tri_inverse_pair<BT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
-          cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
-        }
+        if (cta::cholesky_pair<BT, double>(n, W2, W1, n, sD, sD2, gsm, s_flag2, false))
+          break;  // the inverses read the lower triangles only
+        cta::tri_inverse_pair<BT, double>(n, W2, W1, n, LXi, LZi, n, sD, sD2, gsm);
+        cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
       }
       // ---- residuals and scalars
       {
@@ -1075,6 +1060,7 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.mixed_products = (cfg && cfg->mixed_products) ? 1 : 0;
   a.mu_switch = (cfg && cfg->mixed_switch_gap > 0.0) ? cfg->mixed_switch_gap : 1.0e-2;
   a.refine_tol = (cfg && cfg->refine_tol > 0.0) ? cfg->refine_tol : 1.0e-8;
+  a.factor_smem = (cfg && cfg->factor_smem) ? 1 : 0;
   a.ws = ws;
   a.ws_stride = stride;
   a.queue = queue;
@@ -1152,6 +1138,7 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   a.mixed_products = 0;
   a.mu_switch = 1.0e-2;
   a.refine_tol = 1.0e-8;
+  a.factor_smem = 0;
   a.ws = base + head;
   a.ws_stride = stride;
   a.queue = queue;

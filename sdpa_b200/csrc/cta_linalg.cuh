@@ -841,109 +841,6 @@ __device__ int cholesky_smem(int n, const TA* A, int lda, T* Out, int ldo, bool 
   return 0;
 }
 
-// In-place inverse of the lower-triangular factor in S (LAPACK trtri's
-// blocked lower algorithm): the block columns are taken from the last to
-// the first; with J the current block, T the rows below it (whose block
-// S[T, T] already holds L_TT^{-1}):
-//   S[J, J] <- L_JJ^{-1}                       (one warp, column per lane)
-//   S[T, J] <- -L_TT^{-1} (L_TJ L_JJ^{-1})    (two products, all threads)
-// Each product is computed into registers (up to PER outputs per thread),
-// then written after a barrier, so it can overwrite its own operand.
-// Requires n <= NT * PER / NB rows below any block (n <= 544 with 256
-// threads).
-template <int NT>
-__device__ void smem_trtri(int n, double* S)
-{
-  constexpr int PER = 16;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const int ld = n + 1;
-  const int nblk = (n + NB - 1) / NB;
-  for (int b = nblk - 1; b >= 0; --b) {
-    const int kb = b * NB, bs = min(NB, n - kb);
-    double* D = S + kb * (ld + 1);
-    // (1) diagonal block: lane c computes column c of L_JJ^{-1} by forward
-    // substitution, reading the rows of L_JJ from shared memory (broadcast)
-    if (wid == 0) {
-      double x[NB];
-#pragma unroll
-      for (int r = 0; r < NB; ++r) {
-        double v = 0.0;
-        if (r < bs) {
-          double acc = (r == lane) ? 1.0 : 0.0;
-#pragma unroll
-          for (int k = 0; k < r; ++k)
-            if (k >= lane) acc -= D[r + ld * k] * x[k];
-          if (lane < bs && r >= lane) v = acc / D[r + ld * r];
-        }
-        x[r] = v;
-      }
-      __syncwarp();
-#pragma unroll
-      for (int r = 0; r < NB; ++r)
-        if (r < bs && lane < bs && r >= lane) D[r + ld * lane] = x[r];
-    }
-    __syncthreads();
-    const int r0 = kb + bs, rem = n - r0;
-    if (rem <= 0) continue;
-    // (2) W = L_TJ L_JJ^{-1}: w[t, c] = sum_{k >= c} L[t, k] Linv[k, c]
-    double o[PER];
-    const int tot = rem * bs;
-#pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int e = tid + u * NT;
-      double acc = 0.0;
-      if (e < tot) {
-        const int t = r0 + e % rem, c = e / rem;
-        for (int k = c; k < bs; ++k) acc += S[t + ld * (kb + k)] * D[k + ld * c];
-      }
-      o[u] = acc;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int e = tid + u * NT;
-      if (e < tot) S[(r0 + e % rem) + ld * (kb + e / rem)] = o[u];
-    }
-    __syncthreads();
-    // (3) S[T, J] = -L_TT^{-1} W: y[t, c] = -sum_{r0 <= k <= t} M[t, k] W[k, c]
-#pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int e = tid + u * NT;
-      double acc = 0.0;
-      if (e < tot) {
-        const int t = r0 + e % rem, c = kb + e / rem;
-        for (int k = r0; k <= t; ++k) acc += S[t + ld * k] * S[k + ld * c];
-      }
-      o[u] = -acc;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int e = tid + u * NT;
-      if (e < tot) S[(r0 + e % rem) + ld * (kb + e / rem)] = o[u];
-    }
-    __syncthreads();
-  }
-}
-
-// Zi = Li^T Li for the lower-triangular Li in S (the inverse of Z from the
-// inverse of its Cholesky factor), written in full (both triangles) to Zi:
-// Zi[i, j] = sum_{k >= max(i, j)} Li[k, i] Li[k, j].  Ends with a barrier.
-template <int NT>
-__device__ void smem_ltl(int n, const double* S, double* Zi, int ldz)
-{
-  const int ld = n + 1;
-  for (int t = threadIdx.x; t < n * n; t += NT) {
-    const int i = t % n, j = t / n;
-    if (i < j) continue;
-    double acc = 0.0;
-    for (int k = i; k < n; ++k) acc += S[k + ld * i] * S[k + ld * j];
-    Zi[i + (size_t)ldz * j] = acc;
-    Zi[j + (size_t)ldz * i] = acc;
-  }
-  __syncthreads();
-}
-
 // In-place lower Cholesky, right-looking, blocked by 32, pivot rules as
 // warp_potrf32.  Returns 0 on success, else the failing column + 1.  The
 // strict upper triangle is zeroed on success when zero_upper is set (callers

@@ -233,11 +233,13 @@ def test_batched_dense_constraints_single_block_match_reference():
 
 
 @pytest.mark.parametrize("shape", [{"block_threads": 128, "ctas_per_sm": 4}, {"block_threads": 128, "ctas_per_sm": 3},
-                                   {"block_threads": 256, "ctas_per_sm": 1}])
+                                   {"block_threads": 256, "ctas_per_sm": 1}, {"factor_smem": 1},
+                                   {"factor_smem": 1, "block_threads": 128}])
 def test_launch_shapes_match_reference(shape):
     """Every launch shape the autotuner may pick (128-thread blocks, whose
-    products run as two-pass exact tiles with K chunks of 8, or fewer
-    256-thread blocks per SM) solves to the same results: FP64 single-block
+    products run as two-pass exact tiles with K chunks of 8; fewer
+    256-thread blocks per SM; the Schur factorisation in shared memory)
+    solves to the same results: FP64 single-block
     and multi-block batches against the reference (strict bar), and mixed
     precision with either product precision (reference-accuracy bar)."""
     from sdpa_b200 import batch
