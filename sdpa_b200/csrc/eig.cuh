@@ -86,7 +86,7 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
 #pragma unroll
   for (int j = 0; j < NM; ++j) {
     LanczosVec& v = s.v[j];
-    for (int i = tid; i < n; i += BT) { v.q[i] = 0.0; v.r[i] = 1.0; }
+    for (int i = tid; i < n; i += BT) { v.qold[i] = 0.0; v.r[i] = 1.0; }
     for (int i = tid; i < TRI_MAX; i += BT) { v.d[i] = 1.0e50; v.e[i] = 0.0; }
     beta[j] = sqn;
     mn[j] = 1.0e51;
@@ -96,16 +96,14 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
     act[j] = true;
     pend[j] = false;
   }
+  __syncthreads();
   for (;;) {
-    // (a) start the next step of every running process: q = r / beta
+    // (a) the next step of every running process works on q = r / beta,
+    // formed where it is read (r is published by the previous step's last
+    // barrier), so the step has two barriers
+    double ib[NM];
 #pragma unroll
-    for (int j = 0; j < NM; ++j) {
-      if (!act[j]) continue;
-      LanczosVec& v = s.v[j];
-      const double ib = 1.0 / beta[j];
-      for (int i = tid; i < n; i += BT) { v.qold[i] = v.q[i]; v.q[i] = v.r[i] * ib; }
-    }
-    __syncthreads();
+    for (int j = 0; j < NM; ++j) ib[j] = 1.0 / beta[j];
     // (b) warps 0 / 1 solve the pending tridiagonals while the remaining
     // warps multiply; CW columns of every running matrix per warp and pass,
     // all loads of a pass issued before its FMAs
@@ -117,6 +115,7 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
     for (int j = 0; j < NM; ++j) {
       if (wid != j || !pend[j]) continue;
       LanczosVec& v = s.v[j];
+      __syncwarp();  // e[k] was written by this warp's lane 0
       double ul;
       const double lam = cta::tridiag_min_eig_warp(k[j], v.d, v.e, mn[j], &ul, v.work);
       if (lane == 0) {
@@ -143,7 +142,7 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
               const int kx = kx0 + lane + 32 * u;
-              qv[j][u] = (act[j] && kx < n) ? s.v[j].q[kx] : 0.0;
+              qv[j][u] = (act[j] && kx < n) ? s.v[j].r[kx] * ib[j] : 0.0;
 #pragma unroll
               for (int c = 0; c < CW; ++c)
                 mv[j][c][u] = (act[j] && kx < n && i0 + c < n) ? Ms[j][kx + (size_t)n * (i0 + c)] : 0.0;
@@ -166,7 +165,7 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
           }
           if (act[j] && lane < CW && i0 + lane < n) {
             s.v[j].w[i0 + lane] = wv;
-            part[j] += s.v[j].q[i0 + lane] * wv;
+            part[j] += (s.v[j].r[i0 + lane] * ib[j]) * wv;
           }
         }
       }
@@ -199,7 +198,9 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
       if (!act[j]) continue;
       LanczosVec& v = s.v[j];
       for (int i = tid; i < n; i += BT) {
-        const double rv = (v.w[i] - alpha[j] * v.q[i]) - beta[j] * v.qold[i];
+        const double qi = v.r[i] * ib[j];
+        const double rv = (v.w[i] - alpha[j] * qi) - beta[j] * v.qold[i];
+        v.qold[i] = qi;
         v.r[i] = rv;
         rpart[j] += rv * rv;
       }
@@ -216,7 +217,8 @@ static __device__ void lanczos_min_eig_multi(int n, const double* const* Ms, Eig
     for (int j = 0; j < NM; ++j) {
       if (!act[j]) continue;
       beta[j] = sqrt(rr[j]);
-      if (tid == 0) s.v[j].e[k[j]] = beta[j];
+      // written by the lane that later solves this process's tridiagonal
+      if (wid == j && lane == 0) s.v[j].e[k[j]] = beta[j];
       ++k[j];
       ++kk[j];
     }
