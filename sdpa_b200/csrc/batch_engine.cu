@@ -42,7 +42,7 @@ namespace sdpab {
 // matrices and the diagonal blocks of the factorisations.
 static __host__ __device__ long long fixed_smem_doubles(int nmax, int mmax, int bt)
 {
-  return 4 * (bt / 32) + 6LL * mmax + (long long)nmax + eig_scratch_doubles(nmax);
+  return 4 * (bt / 32) + 6LL * mmax + 4LL * nmax + eig_scratch_doubles(nmax);
 }
 
 static size_t smem_bytes_for(int nmax, int mmax, long long gsm, int bt)
@@ -337,10 +337,13 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
   double* vdz = vrp + mmax;                             // dZ when it is diagonal (nmax)
   double* vres = vdz + nmax;                            // refinement residual (mmax)
   float* x32 = (float*)(vres + mmax);                   // FP32 solve vector (mmax floats)
+  double* vX0d = vres + 2 * mmax;                       // diagonals of X0, Z0 and C (nmax each)
+  double* vZ0d = vX0d + nmax;
+  double* vCd = vZ0d + nmax;
   cta::Reducer RD{redbuf, 0};
   EigScratch es;
-  eig_scratch_carve(es, vres + 2 * mmax, nmax, &RD);     // eig_scratch_doubles(nmax)
-  int* s_nnz = (int*)(vres + 2 * mmax + eig_scratch_doubles(nmax));  // mmax ints
+  eig_scratch_carve(es, vCd + nmax, nmax, &RD);          // eig_scratch_doubles(nmax)
+  int* s_nnz = (int*)(vCd + nmax + eig_scratch_doubles(nmax));  // mmax ints
   int* s_bid = s_nnz + mmax;  // nmax ints: block of each row (-1 = LP entry)
   int* s_form = s_bid + nmax;  // mmax ints: 1 = constraint's Schur column by F1
 
@@ -480,7 +483,10 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
     // count both attempts.
     int status = 0, iter_total = 0;
     double nrp, nrd;
-    // residuals: r_p = b - A.X, D = C - Z - sum y_k A_k (Residuals::compute)
+    // residuals: r_p = b - A.X, D = C - Z - sum y_k A_k (Residuals::compute).
+    // D is formed in the scratch W1 (free wherever this runs) and kept (in D)
+    // only when the point is dual infeasible, the one case in which the next
+    // iteration reads it; a dual-feasible solve never touches D's slot.
     auto residuals = [&](double& nrp, double& nrd) {
       double mx = 0.0;
       for (int k = tid; k < m; k += BT) {
@@ -489,14 +495,18 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
         mx = fmax(mx, fabs(r));
       }
       nrp = cta::block_max<BT>(mx, RD);
-      for (int t = tid; t < nn_i; t += BT) D[t] = -Z[t];
+      for (int t = tid; t < nn_i; t += BT) W1[t] = -Z[t];
       __syncthreads();
-      sp_axpy_block<BT>(er, ec, ev, mp[0], mp[1], -1.0, D, n);  // C = -F0
-      sp_axpy_constraints<BT>(er, ec, ev, mp, m, vy, -1.0, D, n);
+      sp_axpy_block<BT>(er, ec, ev, mp[0], mp[1], -1.0, W1, n);  // C = -F0
+      sp_axpy_constraints<BT>(er, ec, ev, mp, m, vy, -1.0, W1, n);
       __syncthreads();
       mx = 0.0;
-      for (int t = tid; t < nn_i; t += BT) mx = fmax(mx, fabs(D[t]));
+      for (int t = tid; t < nn_i; t += BT) mx = fmax(mx, fabs(W1[t]));
       nrd = cta::block_max<BT>(mx, RD);
+      if (nrd > P.epsilonDash) {  // dual infeasible (Phase::updateCheck): the next predictor reads D
+        for (int t = tid; t < nn_i; t += BT) D[t] = W1[t];
+        __syncthreads();
+      }
     };
     // C . W with C = -F0
     auto c_dot = [&](const double* W) {
@@ -621,11 +631,35 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
       for (int t = tid; t < nn_i; t += BT) { X0[t] = X[t]; Z0[t] = Z[t]; }
       __syncthreads();
     }
+    // A start from a proposed x (SDPAB_INIT_DUAL) has Z0 = C - sum y0_k A_k
+    // with every A_k diagonal; while every step's dZ stays diagonal, Z - Z0
+    // is diagonal and Z0's off-diagonal is C's, so the inner products with
+    // the initial point reduce to diagonals:
+    //   X0 . Z = X0 . Z0 + sum_i X0_ii (Z_ii - Z0_ii),
+    //   X . Z0 = C . X + sum_i X_ii (Z0_ii - C_ii),
+    // and X0, Z0 are not read again (their slots leave L2).
+    bool diag_track = warm && wmode == SDPAB_INIT_DUAL;
+    double x0z0 = 0.0;
+    if (diag_track) {
+      for (int t = tid; t < n; t += BT) {
+        vX0d[t] = X[t * (n + 1)];
+        vZ0d[t] = Z[t * (n + 1)];
+        vCd[t] = 0.0;
+      }
+      __syncthreads();
+      for (long long e = mp[0] + tid; e < mp[1]; e += BT)
+        if (er[e] == ec[e]) atomicAdd(&vCd[er[e]], -ev[e]);  // C = -F0
+      __syncthreads();
+    }
 
     residuals(nrp, nrd);
     double mu0;
-    if (warm) mu0 = cta::dot_mat<BT>(n, X, Z, RD) / n;
-    else mu0 = lam * lam;
+    if (warm) {
+      x0z0 = cta::dot_mat<BT>(n, X, Z, RD);
+      mu0 = x0z0 / n;
+    } else {
+      mu0 = lam * lam;
+    }
     {
       double objP = c_dot(X);
       double objD = cta::dot_vec<BT>(m, bv, vy, RD);
@@ -874,6 +908,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
       // ---- update (Solutions::update, sdpa_dataset.cpp:145-171)
       {
         const double ap = S.alphaP, ad = S.alphaD;
+        diag_track = diag_track && dz_diag;
         // X += ap dX, Z += ad dZ, and the copies the factorisations work on
         for (int t = tid; t < nn_i; t += BT) {
           const double x = X[t] + ap * dX[t];
@@ -901,7 +936,17 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
         double objP = c_dot(X);
         double objD = cta::dot_vec<BT>(m, bv, vy, RD);
         double x0zM, xMz0;
-        if (warm) {
+        if (diag_track) {
+          double v2[2] = {0.0, 0.0};
+          for (int t = tid; t < n; t += BT) {
+            v2[0] += vX0d[t] * (Z[t * (n + 1)] - vZ0d[t]);
+            v2[1] += X[t * (n + 1)] * (vZ0d[t] - vCd[t]);
+          }
+          double s2[2];
+          cta::block_sum_n<BT, 2>(v2, s2, RD);
+          x0zM = x0z0 + s2[0];
+          xMz0 = objP + s2[1];
+        } else if (warm) {
           x0zM = cta::dot_mat<BT>(n, X0, Z, RD);
           xMz0 = cta::dot_mat<BT>(n, X, Z0, RD);
         } else {
