@@ -52,9 +52,9 @@ def peaks():
 
 # DRAM bytes (read + write) of the headline solver launch (learned warm
 # start, mixed precision, 4096 instances), from one ncu capture of that
-# launch (profiles/batch_ipm_headline_maxcut4096.md): 34.68 GB read +
-# 41.20 GB written.  Other batch sizes are scaled by instances.
-TRAFFIC_BYTES_HEADLINE = 75.88e9
+# launch (profiles/batch_ipm_headline_maxcut4096.md): 25.96 GB read +
+# 34.63 GB written.  Other batch sizes are scaled by instances.
+TRAFFIC_BYTES_HEADLINE = 60.59e9
 TRAFFIC_COUNT = 4096
 TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4096-instance headline launch "
                 "(mixed + warm start), profiles/batch_ipm_headline_maxcut4096.md")
