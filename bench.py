@@ -317,14 +317,15 @@ def run_blocks(args):
                        "mean_iterations": float(res.iterations.mean()), "status_nonzero": int(np.sum(res.status != 0))}}
     if not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        v, det, ref, _ = cpu_reference(insts, cores)
+        v, det, ref, tref = cpu_reference(insts, cores, tight=True)
         line["cpu_baseline"] = {"value": v, "unit": "SDPs/s", "cores": cores, "kind": "reference",
                                 "sample": f"all {P.count} instances of this batch, one single-threaded "
                                           f"reference process per core; {det}"}
         if ref is not None:
             from oracle import ref_runner as R
             line["reference_parity"] = R.parity_counts(res.primal_obj, res.dual_obj,
-                                                       [res.x_of(P, q) for q in range(P.count)], ref)
+                                                       [res.x_of(P, q) for q in range(P.count)], ref, tref,
+                                                       phase=res.phase)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -558,9 +559,10 @@ def main():
             # reference-accuracy bar against its epsilonStar 1e-11 solution)
             from oracle import ref_runner as R
             xs = [res.x_of(P, q) for q in range(P.count)]
-            line["reference_parity"] = R.parity_counts(res.primal_obj, res.dual_obj, xs, ref, tref)
+            line["reference_parity"] = R.parity_counts(res.primal_obj, res.dual_obj, xs, ref, tref, phase=res.phase)
             xs0 = [res0.x_of(P, q) for q in range(P.count)]
-            line["plain_fp64"]["reference_parity"] = R.parity_counts(res0.primal_obj, res0.dual_obj, xs0, ref)
+            line["plain_fp64"]["reference_parity"] = R.parity_counts(res0.primal_obj, res0.dual_obj, xs0, ref,
+                                                                      phase=res0.phase)
     del g0, gh
     if world > 1:
         dist.barrier()

@@ -149,11 +149,16 @@ def x_within_reference_accuracy(x, x_ref, x_tight, tol=1e-5) -> bool:
     return float(np.max(np.abs(x - x_tight))) <= float(np.max(np.abs(x_ref - x_tight))) + tol
 
 
-def parity_counts(primal, dual, xs, ref: RefRun, tight: RefRun | None = None) -> dict:
+def parity_counts(primal, dual, xs, ref: RefRun, tight: RefRun | None = None, phase=None) -> dict:
     """Per-instance comparison with the reference's results on the same
     inputs: objectives within 1e-6 relative (both), x within 1e-5 (max abs),
     and, for the instances outside 1e-5, whether x passes the reference-
-    accuracy bar against the tight solution."""
+    accuracy bar against the tight solution.  With `phase` (the solver's
+    phase codes) also the phase agreement, and the objective and x counts
+    over the instances that both solvers end at pdOPT: an instance that the
+    reference stops short of optimal (pdFEAS after a step too short to
+    continue) ends where rounding decides, for the reference's own build as
+    for any other, and its x is not determined."""
     n = len(xs)
     rel = lambda a, b: np.abs(a - b) / np.maximum(1.0, np.abs(b))
     rp = rel(np.asarray(primal), ref.primal_obj)
@@ -170,4 +175,15 @@ def parity_counts(primal, dual, xs, ref: RefRun, tight: RefRun | None = None) ->
                         for q in range(n)])
         out["x_only_within_reference_accuracy"] = int(np.sum(acc & ~x_ok))
         out["x_failing_both_bars"] = int(np.sum(~acc))
+    if phase is not None:
+        ph = np.asarray(phase)
+        both = (ph == 7) & (ref.phase == 7)
+        out["phase_equal"] = int(np.sum(ph == ref.phase))
+        out["both_pdOPT"] = int(both.sum())
+        out["objectives_within_1e-6_both_pdOPT"] = int(np.sum(obj_ok & both))
+        out["x_within_1e-5_both_pdOPT"] = int(np.sum(x_ok & both))
+        if both.any():
+            out["max_abs_x_diff_both_pdOPT"] = float(dx[both].max())
+        if tight is not None:
+            out["x_failing_both_bars_both_pdOPT"] = int(np.sum(~acc & both))
     return out

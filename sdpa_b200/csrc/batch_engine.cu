@@ -1061,11 +1061,12 @@ static void launch_solver(const sdpab_batch* prob, const LaunchShape& L, int gri
   }
 }
 
-static long long ws_doubles(int nmax, int mmax)
+static long long ws_doubles(int nmax, int mmax, bool mixed)
 {
   long long nn = (long long)nmax * nmax;
   const long long mm = (long long)mmax * mmax;
-  long long s = 14 * nn + mm + (mm + 1) / 2;  // 14 n x n, the Schur matrix, its FP32 factor
+  // 14 n x n, the Schur matrix and, in mixed precision, its FP32 factor (last)
+  long long s = 14 * nn + mm + (mixed ? (mm + 1) / 2 : 0);
   return (s + 31) / 32 * 32;  // 256-byte aligned per block
 }
 
@@ -1087,7 +1088,7 @@ int batch_solve_device(const sdpab_batch* prob, const sdpab_batch_init* init,
                         cfg ? cfg->staging_doubles : 0, dev, L, "batch_solve");
   if (rc != SDPAB_OK) return rc;
   int grid = std::min(prob->count, sms * L.per_sm);
-  const long long stride = ws_doubles(prob->nmax, prob->mmax);
+  const long long stride = ws_doubles(prob->nmax, prob->mmax, cfg && cfg->precision == SDPAB_PREC_MIXED);
   Workspace& W = workspace();
   double* ws = (double*)W.get((size_t)grid * stride * sizeof(double) + 256);
   if (!ws) return set_error(SDPAB_ECUDA, "workspace allocation failed");
@@ -1143,7 +1144,7 @@ int batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
   if (prob->count == 0) return SDPAB_OK;
   if (prob->nmax > 1024 || prob->mmax > 2048)
     return set_error(SDPAB_ESIZE, "batch_solve_noalloc: nmax <= 1024 and mmax <= 2048 are supported");
-  const long long stride = ws_doubles(prob->nmax, prob->mmax);
+  const long long stride = ws_doubles(prob->nmax, prob->mmax, false);  // FP64 only: no FP32 factor
   const long long head = 32;  // doubles reserved for the work-queue counter
   const long long capacity = ((long long)(SDPAB_NOALLOC_SCRATCH_BYTES / sizeof(double)) - head) / stride;
   if (capacity < 1) {

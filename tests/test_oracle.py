@@ -87,3 +87,21 @@ def test_headline_fixture_matches_oracle_and_runner():
         assert np.array_equal(run.x[q], arr[f"bmc{s}.xvec"])
     pc = R.parity_counts(run.primal_obj, run.dual_obj, run.x, run, run)
     assert pc["objectives_within_1e-6"] == len(seeds) and pc["x_failing_both_bars"] == 0
+
+
+def test_parity_counts_split_by_phase():
+    """Instances the reference stops short of pdOPT are counted apart: their
+    x is not determined, so a large x difference there is reported but does
+    not enter the both-pdOPT counts."""
+    from oracle import ref_runner as R
+    ref = R.RefRun(wall_s=1.0, process_wall_s=1.0, iterations=np.array([9, 9, 9]),
+                   phase=np.array([7, 7, 3]), primal_obj=np.array([1.0, 2.0, 3.0]),
+                   dual_obj=np.array([1.0, 2.0, 3.0]),
+                   x=[np.array([0.5, 0.25]), np.array([1.0, 2.0]), np.array([1.0, 1.0])])
+    ours_x = [np.array([0.5, 0.25 + 4e-6]), np.array([1.0, 2.0 + 3e-5]), np.array([1.0, 900.0])]
+    pc = R.parity_counts([1.0, 2.0, 3.0 + 1e-3], [1.0, 2.0, 3.0], ours_x, ref, phase=[7, 7, 7])
+    assert pc["objectives_within_1e-6"] == 2 and pc["x_within_1e-5"] == 1
+    assert pc["phase_equal"] == 2 and pc["both_pdOPT"] == 2
+    assert pc["objectives_within_1e-6_both_pdOPT"] == 2 and pc["x_within_1e-5_both_pdOPT"] == 1
+    assert pc["max_abs_x_diff"] == pytest.approx(899.0)
+    assert pc["max_abs_x_diff_both_pdOPT"] == pytest.approx(3e-5)
