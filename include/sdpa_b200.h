@@ -272,6 +272,21 @@ typedef struct sdpab_batch {
                                   X = sum F_i x_i - F0 is positive definite with margin
                                   init_margin * mean |F0_ii|, and sets
                                   Y = D X^-1 D with unit-scaled diagonal */
+#define SDPAB_INIT_FACTOR 3    /* start from a low-rank factor V of the user Y (constraints
+                                  X_ii = b_i as for SDPAB_INIT_DUAL; row i of V has norm
+                                  sqrt(b_i)), e.g. from sdpab_lowrank_factor.  The solver forms
+                                  Y = V V^T, the multipliers x_i = (F0 Y)_ii / b_i and
+                                  X = sum F_i x_i - F0, and starts on the central path's
+                                  equation Y0 X0 = mu I at
+                                    mu = max(init_mu, 3 rho) s,  s = mean |F0_ii|,
+                                    rho = |X V|_F / (|V|_F s) (the factor's stationarity
+                                    residual, 0 at the optimum),  tau = 0.3 sqrt(mu s):
+                                    X0 = X + mu (Y + tau I)^-1 + delta I,  Y0 = mu X0^-1,
+                                  delta the first of 0, mu/n, 4 mu/n, 16 mu/n, ... that makes X0
+                                  positive definite (x shifted by delta to match).  No
+                                  counterpart in the reference, which starts only from a given
+                                  point or lambda* I.  Instances not of this form take the
+                                  standard start (status 1). */
 
 typedef struct sdpab_batch_init {
   const int* flag;             /* [count] SDPAB_INIT_* per instance */
@@ -279,6 +294,11 @@ typedef struct sdpab_batch_init {
   const double* X;             /* user X (dense_off layout), as inputInitXMat */
   const double* Y;             /* user Y (dense_off layout), as inputInitYMat */
   double init_margin;          /* SDPAB_INIT_DUAL interiority margin (0 = 0.02) */
+  const double* V;             /* SDPAB_INIT_FACTOR: instance q's factor, n x rank row-major, at
+                                  V + vec_off[q] * rank (may be NULL otherwise) */
+  int rank;                    /* columns of V */
+  double init_mu;              /* SDPAB_INIT_FACTOR: the smallest start mu relative to
+                                  mean |F0_ii| (0 = 3e-5) */
 } sdpab_batch_init;
 
 typedef struct sdpab_batch_result {
@@ -383,6 +403,34 @@ SDPAB_API int sdpab_batch_solve_host(const sdpab_batch* prob, const sdpab_batch_
 SDPAB_API int sdpab_batch_solve_noalloc(const sdpab_batch* prob, const sdpab_batch_init* init,
                                         const sdpab_params* prm, sdpab_batch_result* res,
                                         const int* order, void* stream);
+
+/* Low-rank factor for SDPAB_INIT_FACTOR (no counterpart in the reference).
+ * For every instance whose constraints are X_ii = b_i (one SDP block, m = n,
+ * F_i = e_i e_i^T, b > 0: MaxCut-type relaxations), an approximate solution
+ * of the user's dual problem  max <F0, Y>  s.t.  Y_ii = b_i, Y >= 0  in the
+ * factored form Y = V V^T (Burer-Monteiro), by block-coordinate ascent over
+ * the rows of V (the mixing method of Wang, Chang and Kolter, 2017):
+ *   v_i <- sqrt(b_i) g_i / |g_i|,  g_i = sum_{j != i} F0_ij v_j,
+ * rows in order, from a seeded pseudo-random V.  Instance q uses
+ * r_q = min(rank, ceil(sqrt(2 n_q)) + 1) columns (its other columns are
+ * written as 0) and stops when a sweep changes sum_i <v_i, g_i> by at most
+ * tol relative, or after max_sweeps sweeps.
+ *   prob: DEVICE batch; num_entries: length of its row / col / val arrays;
+ *   rank: columns of V, 1..32 (0 = ceil(sqrt(2 nmax)) + 1, at most 32);
+ *   V: DEVICE, [nvec * rank] doubles (instance q at V + vec_off[q] * rank);
+ *   sweeps: DEVICE, [count] ints out: sweeps run, -1 for an instance not of
+ *   this form (its V is not written);
+ *   order: DEVICE, [count] instance indices in the order warps take them
+ *   (largest first balances the launch), or NULL for 0..count-1.
+ * One warp per instance, taken from a work queue; F0's off-diagonal entries are laid out by rows in a
+ * library-owned scratch (2 * num_entries entries, kept between calls, freed
+ * by sdpab_release_workspace).  SDPAB_ESIZE when one instance's factor does
+ * not fit in shared memory (nmax * rank above about 24,000). */
+SDPAB_API int sdpab_lowrank_factor(const sdpab_batch* prob, long long num_entries, int rank, int max_sweeps,
+                                   double tol, unsigned long long seed, double* V, int* sweeps,
+                                   const int* order, void* stream);
+/* The rank sdpab_lowrank_factor uses for rank = 0. */
+SDPAB_API int sdpab_lowrank_default_rank(int nmax);
 
 /* Device memory the batched solver keeps between calls (workspace, staging). */
 SDPAB_API long long sdpab_workspace_bytes(void);

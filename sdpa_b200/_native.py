@@ -38,7 +38,7 @@ BATCH_MAX_BLOCKS = 64
 
 class BatchInit(ctypes.Structure):
     _fields_ = [("flag", c_void_p), ("xvec", c_void_p), ("X", c_void_p), ("Y", c_void_p),
-                ("init_margin", c_double)]
+                ("init_margin", c_double), ("V", c_void_p), ("rank", c_int), ("init_mu", c_double)]
 
 
 class GraphBatch(ctypes.Structure):
@@ -79,6 +79,9 @@ SIGNATURES = [
     ("sdpab_batch_solve_noalloc", c_int, [POINTER(Batch), POINTER(BatchInit), POINTER(Params),
                                           POINTER(BatchResult), c_void_p, c_void_p]),
     ("sdpab_workspace_bytes", c_longlong, []),
+    ("sdpab_lowrank_factor", c_int, [POINTER(Batch), c_longlong, c_int, c_int, c_double, ctypes.c_ulonglong,
+                                     c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sdpab_lowrank_default_rank", c_int, [c_int]),
     ("sdpab_mpnn_num_params", c_longlong, []),
     ("sdpab_mpnn_act_floats", c_longlong, [c_int]),
     ("sdpab_mpnn_scratch_floats", c_longlong, [c_int]),

@@ -187,8 +187,10 @@ def _config(precision=N.PREC_FP64, ctas_per_sm=0, mixed_switch_gap=0.0, staging=
 def solve_host(P: Packed, params=None, precision=N.PREC_FP64, want_x=True, want_mats=False,
                init=None, ctas_per_sm=0, staging=0, block_threads=0, mixed_products=0,
                mixed_switch_gap=0.0, refine_tol=0.0, factor_smem=0) -> BatchResult:
-    """sdpab_batch_solve_host on host arrays.  init = (flag, xvec, X, Y) in
-    the packed layouts (user X / Y as in SDPA::inputInitXMat / inputInitYMat).
+    """sdpab_batch_solve_host on host arrays.  init = (flag, xvec, X, Y
+    [, margin [, V, rank [, init_mu]]]) in the packed layouts (user X / Y as in
+    SDPA::inputInitXMat / inputInitYMat; V: the SDPAB_INIT_FACTOR factors,
+    instance q's n x rank rows at vec_off[q] * rank).
     The launch shape (block_threads, ctas_per_sm, staging) and the mixed
     mode's options are those of sdpab_batch_config (0 = defaults)."""
     L = N.lib()
@@ -208,8 +210,11 @@ def solve_host(P: Packed, params=None, precision=N.PREC_FP64, want_x=True, want_
         conv = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
         flag, xv, Xu, Yu = np.ascontiguousarray(init[0], np.int32), conv(init[1]), conv(init[2]), conv(init[3])
         margin = float(init[4]) if len(init) > 4 else 0.0
-        keep = [flag, xv, Xu, Yu]
-        bi = ctypes.byref(N.BatchInit(_ptr(flag), _ptr(xv), _ptr(Xu), _ptr(Yu), margin))
+        Vf = conv(init[5]) if len(init) > 5 else None
+        rank = int(init[6]) if len(init) > 6 else 0
+        init_mu = float(init[7]) if len(init) > 7 else 0.0
+        keep = [flag, xv, Xu, Yu, Vf]
+        bi = ctypes.byref(N.BatchInit(_ptr(flag), _ptr(xv), _ptr(Xu), _ptr(Yu), margin, _ptr(Vf), rank, init_mu))
     prm = _params(params)
     cfg = _config(precision, ctas_per_sm, mixed_switch_gap, staging, mixed_products, block_threads, refine_tol,
                   factor_smem)

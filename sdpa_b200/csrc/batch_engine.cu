@@ -614,6 +614,142 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
         }
       }
       if (!warm) status = 1;
+    } else if (wmode == SDPAB_INIT_FACTOR) {
+      // A low-rank factor V of the user Y (row i of norm sqrt(b_i)) for
+      // constraints X_ii = b_i: Y = V V^T, multipliers x_i = (F0 Y)_ii / b_i,
+      // internal Z = sum F_i x_i - F0 (Z Y = 0 at the optimum), and a start
+      // on the central path's equation X Z = mu I: with s = mean |F0_ii|,
+      // mu = max(init_mu, 3 |Z V| / (|V| s)) s and tau = 0.3 sqrt(mu s)
+      //   Z0 = Z + mu (Y + tau I)^-1 + delta I,   X0 = mu Z0^-1,
+      // delta the first of 0, mu/n, 4 mu/n, ... that makes Z0 positive
+      // definite (X0 = Y + mu (Z + tau I)^-1 instead when delta > 0).  Near
+      // the path, Z ~ Z* + mu Y*^+ and X ~ Y* + mu Z*^+: the added term is the
+      // first-order correction on the range of Y, where it makes mu Z0^-1 ~ Y;
+      // tau keeps it bounded in the directions where Y is (nearly) singular
+      // and is far above the factor's own error.  X0 is primal feasible to
+      // O(mu), Z0 dual feasible to O(mu / tau).
+      const int R = a.init.rank;
+      int bad = (m != n || blocked || !a.init.V || R < 1 || R > 32 || R > nmax) ? 1 : 0;  // n x R scratch in nmax^2 slots
+      for (int k = tid; k < m && !bad; k += BT) {
+        if (mp[k + 2] - mp[k + 1] != 1) { bad = 1; break; }
+        const long long e = mp[k + 1];
+        if (er[e] != ec[e] || ev[e] != 1.0 || !(bv[k] > 0.0)) bad = 1;
+      }
+      for (int t = tid; t < n; t += BT) W1[t] = 0.0;
+      __syncthreads();
+      for (int k = tid; k < m && !bad; k += BT) atomicAdd(&W1[er[mp[k + 1]]], 1.0);
+      __syncthreads();
+      for (int t = tid; t < n && !bad; t += BT) bad |= (W1[t] != 1.0);
+      bad = __syncthreads_or(bad);
+      if (!bad) {
+        const double* Vq = a.init.V + a.p.vec_off[inst] * R;
+        // X = Y = V V^T (V row-major n x R = column-major R x n, ld R)
+        cta::gemm_rect<BT, double, double>(n, n, R, true, Vq, R, false, Vq, R, X, n, 1.0, 0.0, gsm);
+        // C = -F0, its scale s and mu, tau
+        for (int t = tid; t < nn_i; t += BT) Z[t] = 0.0;
+        __syncthreads();
+        sp_axpy_block<BT>(er, ec, ev, mp[0], mp[1], -1.0, Z, n);
+        __syncthreads();
+        double cs = 0.0;
+        for (int t = tid; t < n; t += BT) cs += fabs(Z[t + (size_t)n * t]);
+        cs = cta::block_sum<BT>(cs, RD) / n;
+        if (!(cs > 0.0)) cs = 1.0;
+        // (F0 Y)_ii = -sum_j C_ij Y_ij, one warp per row; y_k = -x_{row(k)}
+        {
+          const int lane = tid & 31, wid = tid >> 5;
+          for (int i = wid; i < n; i += BT / 32) {
+            double acc = 0.0;
+            for (int j = lane; j < n; j += 32) acc += Z[j + (size_t)n * i] * X[j + (size_t)n * i];
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) W2[i] = -acc;
+          }
+          __syncthreads();
+          for (int k = tid; k < m; k += BT) {
+            const int r = er[mp[k + 1]];
+            vy[k] = -W2[r] / bv[k];
+          }
+          __syncthreads();
+        }
+        sp_axpy_constraints<BT>(er, ec, ev, mp, m, vy, -1.0, Z, n);  // Z = C - sum y_k A_k
+        __syncthreads();
+        // the factor's stationarity residual rho = |Z V| / (|V| s) (0 at the
+        // optimum) sets mu: a start closer than the factor's own error stalls
+        cta::gemm_rect<BT, double, double>(n, R, n, false, Z, n, true, Vq, R, dX, n, 1.0, 0.0, gsm);
+        double zv = 0.0, vv = 0.0;
+        for (int t = tid; t < n * R; t += BT) {
+          zv += dX[t] * dX[t];
+          vv += Vq[t] * Vq[t];
+        }
+        zv = cta::block_sum<BT>(zv, RD);
+        vv = cta::block_sum<BT>(vv, RD);
+        const double rho = (vv > 0.0) ? sqrt(zv / vv) / cs : 0.0;
+        const double mu_s = fmax((a.init.init_mu > 0.0) ? a.init.init_mu : 3.0e-5, 3.0 * rho) * cs;
+        const double tau = 0.3 * sqrt(mu_s * cs);
+        // (Y + tau I)^-1 = (I - V M^-1 V^T) / tau, M = tau I + V^T V (R x R):
+        // M = L L^T in W1, Li = L^-1 in LXi, U = V Li^T (n x R) in dX,
+        // Z0 = Z + (mu / tau) (I - U U^T)
+        cta::gemm_rect<BT, double, double>(R, R, n, false, Vq, R, true, Vq, R, W1, R, 1.0, 0.0, gsm);
+        for (int t = tid; t < R; t += BT) W1[t + R * t] += tau;
+        __syncthreads();
+        if (cta::cholesky<BT, double>(R, W1, R, false, sD, gsm, &s_flag) == 0) {
+          cta::tri_inverse<BT, double>(R, W1, R, LXi, R, sD, gsm);
+          cta::gemm_rect<BT, double, double>(n, R, R, true, Vq, R, true, LXi, R, dX, n, 1.0, 0.0, gsm);
+          cta::gemm_rect<BT, double, double>(n, n, R, false, dX, n, true, dX, n, W2, n, 1.0, 0.0, gsm);
+          const double sc = mu_s / tau;
+          for (int t = tid; t < nn_i; t += BT) Z[t] += sc * ((((t % n) == (t / n)) ? 1.0 : 0.0) - W2[t]);
+          __syncthreads();
+          // the smallest shift of the ladder that leaves Z0 positive definite
+          double delta = 0.0;
+          int ok = 0;
+          for (int step = 0; step < 12 && !ok; ++step) {
+            for (int t = tid; t < nn_i; t += BT) W1[t] = Z[t] + (((t % n) == (t / n)) ? delta : 0.0);
+            __syncthreads();
+            if (cta::cholesky<BT, double>(n, W1, n, false, sD, gsm, &s_flag) == 0) ok = 1;
+            else delta = mu_s / n * (double)(1 << (2 * step));
+          }
+          if (ok) {
+            // Z0 shifted by delta (x with it) and Z0^-1.  X0 = mu Z0^-1 (X0 Z0
+            // = mu I, the central path's equation) when no shift was needed;
+            // a shift means Z has negative curvature beyond the factor's
+            // correction, where mu Z0^-1 would be large, and then
+            // X0 = Y + mu (Z + tau I)^-1, bounded by tau, with Y = V V^T.
+            for (int k = tid; k < m; k += BT) vy[k] -= delta;
+            for (int t = tid; t < nn_i; t += BT) if ((t % n) == (t / n)) Z[t] += delta;
+            cta::tri_inverse<BT, double>(n, W1, n, LZi, n, sD, gsm);
+            cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
+            if (delta == 0.0) {
+              for (int t = tid; t < nn_i; t += BT) {
+                X[t] = mu_s * Zi[t];
+                W2[t] = X[t];
+              }
+            } else {
+              // Z + tau I = (Z0 - delta I - mu (Y + tau I)^-1) + tau I, from
+              // the unshifted parts still at hand: W2 = U U^T, sc = mu / tau
+              for (int t = tid; t < nn_i; t += BT) {
+                const bool dg = (t % n) == (t / n);
+                W1[t] = Z[t] - sc * ((dg ? 1.0 : 0.0) - W2[t]) + (dg ? tau - delta : 0.0);
+              }
+              __syncthreads();
+              if (cta::cholesky<BT, double>(n, W1, n, false, sD, gsm, &s_flag) != 0) ok = 0;
+              if (ok) {
+                cta::tri_inverse<BT, double>(n, W1, n, LXi, n, sD, gsm);
+                cta::gemm<BT>(n, true, LXi, n, false, LXi, n, D, n, 1.0, 0.0, gsm);
+                cta::gemm_rect<BT, double, double>(n, n, R, true, Vq, R, false, Vq, R, X, n, 1.0, 0.0, gsm);
+                for (int t = tid; t < nn_i; t += BT) {
+                  X[t] += mu_s * D[t];
+                  W2[t] = X[t];
+                }
+              }
+            }
+            __syncthreads();
+            if (ok && cta::cholesky<BT, double>(n, W2, n, false, sD, gsm, &s_flag) == 0) {
+              cta::tri_inverse<BT, double>(n, W2, n, LXi, n, sD, gsm);
+              warm = true;
+            }
+          }
+        }
+      }
+      if (!warm) status = 1;
     }
     if (!warm) {
       for (int t = tid; t < nn_i; t += BT) {

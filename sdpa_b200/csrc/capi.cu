@@ -155,6 +155,7 @@ int sdpab_release_workspace(void)
   int dev = 0;
   cudaGetDevice(&dev);
   workspace().release();
+  lowrank_release();
   std::lock_guard<std::mutex> lk(g_stage_mu);
   if (dev >= 0 && dev < kMaxDevices) g_stage[dev].release();
   return SDPAB_OK;
@@ -203,12 +204,19 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
       nbs = std::max(nbs, (long long)hp->blk_off[i] + nb);
     }
   }
+  bool need_x = false, need_v = false;
   if (want_init) {
     bool need_xy = false;
-    for (int i = 0; i < N; ++i) need_xy |= (hinit->flag[i] == SDPAB_INIT_POINT);
-    if (!hinit->xvec) return set_error(SDPAB_EINVAL, "batch_solve_host: init xvec is NULL");
+    for (int i = 0; i < N; ++i) {
+      need_xy |= (hinit->flag[i] == SDPAB_INIT_POINT);
+      need_x |= (hinit->flag[i] == SDPAB_INIT_POINT || hinit->flag[i] == SDPAB_INIT_DUAL);
+      need_v |= (hinit->flag[i] == SDPAB_INIT_FACTOR);
+    }
+    if (need_x && !hinit->xvec) return set_error(SDPAB_EINVAL, "batch_solve_host: init xvec is NULL");
     if (need_xy && (!hinit->X || !hinit->Y))
       return set_error(SDPAB_EINVAL, "batch_solve_host: SDPAB_INIT_POINT needs init X and Y");
+    if (need_v && (!hinit->V || hinit->rank < 1 || hinit->rank > 32))
+      return set_error(SDPAB_EINVAL, "batch_solve_host: SDPAB_INIT_FACTOR needs V and a rank of 1..32");
   }
   std::vector<int> order(N);
   std::iota(order.begin(), order.end(), 0);
@@ -229,12 +237,13 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
       {8, hp->val, nent * sizeof(double)},   {9, hp->dense_off, N * sizeof(long long)},
       {10, order.data(), N * sizeof(int)},
       {11, want_init ? hinit->flag : nullptr, want_init ? N * sizeof(int) : 0},
-      {12, want_init ? hinit->xvec : nullptr, want_init ? nvec * sizeof(double) : 0},
+      {12, (want_init && hinit->xvec) ? hinit->xvec : nullptr, want_init ? nvec * sizeof(double) : 0},
       {13, want_init ? hinit->X : nullptr, want_init ? nden * sizeof(double) : 0},
       {14, want_init ? hinit->Y : nullptr, want_init ? nden * sizeof(double) : 0},
       {20, hp->nblock, hp->nblock ? N * sizeof(int) : 0},
       {21, hp->nblock ? hp->blk_off : nullptr, hp->nblock ? N * sizeof(int) : 0},
       {22, hp->nblock ? hp->blk_size : nullptr, nbs * sizeof(int)},
+      {23, need_v ? hinit->V : nullptr, need_v ? nvec * hinit->rank * sizeof(double) : 0},
   };
   void* d[24] = {nullptr};
   for (const Copy& c : in) {
@@ -282,6 +291,9 @@ int sdpab_batch_solve_host(const sdpab_batch* hp, const sdpab_batch_init* hinit,
     di.xvec = (const double*)d[12];
     di.X = (const double*)d[13];
     di.Y = (const double*)d[14];
+    di.V = (const double*)d[23];
+    di.rank = hinit->rank;
+    di.init_mu = hinit->init_mu;
   }
   sdpab_batch_result dr;
   double* sc = (double*)d[18];

@@ -58,6 +58,9 @@ class Workspace {
 
 Workspace& workspace();
 
+// Frees the low-rank factor routine's scratch on the current device.
+void lowrank_release();
+
 // IO::computeDimacs (sdpa_io.cpp:775-813) on the device: the final primal
 // residual vector, dual residual matrices, X and Z of a finished solve
 // (device pointers; SDP blocks as n x n column-major, LP blocks as vectors).
