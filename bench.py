@@ -3,11 +3,17 @@
 Workload (one "step"): solve a batch of 4096 MaxCut SDP relaxations (seeds
 0..4095 per rank, n ~ U{20..120}, G(n, p ~ U(0.05, 0.3)), edge weights
 U(0, 1), one n x n block, m = n) to SDPA's pdOPT stopping test with
-epsilonStar = 1e-7, inputs resident in HBM, one persistent kernel launch.
+epsilonStar = 1e-7, inputs resident in HBM.  The headline step is the warm
+start and the solve: the low-rank factor of every instance (mixing-method
+kernel) and the persistent solver from the SDPAB_INIT_FACTOR start (--start
+factor, default), or the learned network's proposal and the solver (--start
+learned), or the solver alone from the standard start (--start none).  The
+plain FP64 solve from the standard start is timed in the same run.
 Synthetic seeded data (no public suite is named).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|mixed] [--count C] [--workload maxcut|blocks]
+                    [--precision fp64|mixed] [--start factor|learned|none]
+                    [--count C] [--workload maxcut|blocks]
 
 --workload blocks measures the batched multi-block family instead (one GPU,
 FP64, standard start): per seed 2..4 SDP blocks of order U{6..40} and an LP
@@ -50,14 +56,14 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
-# DRAM bytes (read + write) of the headline solver launch (learned warm
-# start, mixed precision, 4096 instances), from one ncu capture of that
-# launch (profiles/batch_ipm_headline_maxcut4096.md): 25.96 GB read +
-# 34.63 GB written.  Other batch sizes are scaled by instances.
-TRAFFIC_BYTES_HEADLINE = 60.59e9
+# DRAM bytes (read + write) of the headline solver launch (factor start,
+# mixed precision, 4096 instances), from one ncu capture of that launch
+# (profiles/batch_ipm_headline_maxcut4096.md): 15.75 GB read + 18.74 GB
+# written.  Other batch sizes are scaled by instances.
+TRAFFIC_BYTES_HEADLINE = 34.49e9
 TRAFFIC_COUNT = 4096
-TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4096-instance headline launch "
-                "(mixed + warm start), profiles/batch_ipm_headline_maxcut4096.md")
+TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4096-instance headline solver launch "
+                "(factor start, mixed), profiles/batch_ipm_headline_maxcut4096.md")
 
 
 def iter_flops(n: int, m: int) -> float:
@@ -337,7 +343,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--warm", type=int, default=1, help="learned warm start (1) or standard start (0)")
+    ap.add_argument("--start", default="factor", choices=["factor", "learned", "none"],
+                    help="headline start: low-rank factor (mixing method + SDPAB_INIT_FACTOR), the learned "
+                         "network's proposal (SDPAB_INIT_DUAL), or the standard start")
+    ap.add_argument("--warm", type=int, default=None, help="0: same as --start none (kept for old commands)")
     ap.add_argument("--count", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
@@ -347,6 +356,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="only launch the headline pipeline warmup + steps times, untimed (for ncu captures)")
     args = ap.parse_args()
+    if args.warm == 0:
+        args.start = "none"
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "blocks":
@@ -355,7 +366,7 @@ def main():
     import torch
     import torch.distributed as dist
     from sdpa_b200 import _native as N
-    from sdpa_b200 import autotune, batch
+    from sdpa_b200 import autotune, batch, lowrank
     from sdpa_b200 import warmstart as W
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -379,12 +390,19 @@ def main():
         if world > 1:
             dist.barrier()
 
+    def make_pipe(start, db):
+        if start == "factor":
+            return lowrank.FactorPipeline(db)
+        if start == "learned":
+            return W.WarmPipeline(W.default_model(), graphs, db)
+        return None
+
     if args.profile:
         # the headline pipeline alone, launched warmup + steps times (one
         # solver launch each), for a profiler: nothing is timed or printed
         # but the instances' outcome
         dbp = batch.DeviceBatch(P)
-        pp = W.WarmPipeline(W.default_model(), graphs, dbp) if args.warm else None
+        pp = make_pipe(args.start, dbp)
         for _ in range(args.warmup + args.steps):
             if pp is not None:
                 pp.run(precision=prec, stream=stream, **fixed_shape(args))
@@ -405,9 +423,9 @@ def main():
     tune0 = autotune.tune(db0, N.PREC_FP64, stream=stream, candidates=cand)
     c0 = tune0["best"]
     run0 = lambda: db0.solve(precision=N.PREC_FP64, stream=stream, **c0)
-    # ---- headline path: precision + learned warm start
+    # ---- headline path: precision + warm start
     dbh = batch.DeviceBatch(P)
-    pipe = W.WarmPipeline(W.default_model(), graphs, dbh) if args.warm else None
+    pipe = make_pipe(args.start, dbh)
     tuneh = autotune.tune(dbh, prec, stream=stream, candidates=cand,
                           run=(lambda c: pipe.run(precision=prec, stream=stream, **c)) if pipe else None)
     ch = tuneh["best"]
@@ -438,25 +456,37 @@ def main():
         with ClockSampler(local) as clk:
             times = _events_time(steph, stream, args.steps, flush)
         barrier()
-    # the other precision of the warm-started pipeline, same batch, same timing
+    # the pipeline's two stages timed apart (factor: the mixing kernel;
+    # solve: the persistent solver from the start), and the learned network's
+    # start in the same precision, same batch, same timing
+    stages = None
+    if isinstance(pipe, lowrank.FactorPipeline):
+        with torch.cuda.stream(stream):
+            tf = _events_time(lambda: pipe.factor(stream), stream, args.steps, flush)
+            ts = _events_time(lambda: dbh.solve(precision=prec, stream=stream, **ch), stream, args.steps, flush)
+        barrier()
+        stages = {"factor_ms": float(np.mean(tf)), "solve_ms": float(np.mean(ts)),
+                  "mean_sweeps": float(pipe.sweeps.float().mean().item()),
+                  "max_sweeps": int(pipe.sweeps.max().item())}
     alt = None
-    if pipe is not None:
-        aprec = N.PREC_FP64 if prec == N.PREC_MIXED else N.PREC_MIXED
+    if args.start != "learned":
+        dbl = batch.DeviceBatch(P)
+        lp = W.WarmPipeline(W.default_model(), graphs, dbl)
         ach = {k: v for k, v in ch.items() if k != "mixed_products"}
         with torch.cuda.stream(stream):
             for _ in range(2):
-                pipe.run(precision=aprec, stream=stream, **ach)
-            ta = _events_time(lambda: pipe.run(precision=aprec, stream=stream, **ach), stream,
-                              args.steps, flush)
+                lp.run(precision=prec, stream=stream, **ach)
+            ta = _events_time(lambda: lp.run(precision=prec, stream=stream, **ach), stream, args.steps, flush)
         barrier()
-        ra = dbh.result()
-        alt = {"precision": "fp64" if aprec == N.PREC_FP64 else "mixed", "warm_start": True,
+        ra = dbl.result()
+        alt = {"start": "learned network proposal (SDPAB_INIT_DUAL)", "precision": args.precision,
                "value": args.count / (float(np.mean(ta)) / 1e3), "unit": "SDPs/s (this GPU)",
                "ms_per_step": float(np.mean(ta)), "mean_iterations": float(ra.iterations.mean()),
                "pdOPT": int(np.sum(ra.phase == 7)), "retried_in_fp64": int(np.sum(ra.status == 2))}
-        with torch.cuda.stream(stream):
-            steph()
-        barrier()
+        del lp, dbl
+    with torch.cuda.stream(stream):
+        steph()
+    barrier()
     res = dbh.result()
     res0 = db0.result()
     step_ms = float(np.mean(times))
@@ -473,7 +503,7 @@ def main():
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     pairs = [(dbh.d[k], pin(getattr(P, k))) for k in dbh.d]
     pairs.append((dbh.order, pin(dbh.order.cpu().numpy())))
-    if pipe is not None:
+    if isinstance(pipe, W.WarmPipeline):
         gb = pipe.dg.gb
         pairs += [(pipe.dg.rowptr, pin(gb.rowptr)), (pipe.dg.col, pin(gb.col)), (pipe.dg.aval, pin(gb.aval)),
                   (pipe.dg.aval_t, pin(gb.aval_t)), (pipe.dg.feat, pin(gb.feat)),
@@ -510,9 +540,12 @@ def main():
     flops = sum(float(res.iterations[q]) * iter_flops(int(P.n[q]), int(P.m[q])) for q in range(P.count))
     hbm, bf16, src = peaks()
     fp64 = fp64_peak()
-    achieved = flops / (step_ms / 1e3) / 1e12
+    # the solver launch's own time when the step also runs the factor kernel
+    solver_ms = stages["solve_ms"] if stages else step_ms
+    achieved = flops / (solver_ms / 1e3) / 1e12
     traffic = TRAFFIC_BYTES_HEADLINE * P.count / TRAFFIC_COUNT
-    launches_per_step = 9 if pipe is not None else 1  # 7 network + 1 proposal + 1 solver
+    # factor: mixing kernel + solver; learned: 7 network + 1 proposal + 1 solver
+    launches_per_step = {"factor": 2, "learned": 9, "none": 1}[args.start]
     relobj = np.abs(res.primal_obj - res0.primal_obj) / np.maximum(1.0, np.abs(res0.primal_obj))
     xdiff = np.array([np.max(np.abs(res.x_of(P, q) - res0.x_of(P, q))) for q in range(P.count)])
     line = {"metric": METRIC, "value": value, "unit": "SDPs/s", "n_gpus": world, "steps": args.steps,
@@ -520,7 +553,10 @@ def main():
             "vs_baseline": None, "dtype": "f64" if prec == N.PREC_FP64 else "f32+f64",
             "data": "synthetic (seeded generator, no public suite)",
             "config": {"workload": WORKLOAD, "count_per_gpu": args.count, "precision": args.precision,
-                       "warm_start": bool(args.warm), "cuda_graph": gh is not None,
+                       "start": {"factor": "low-rank factor (mixing method) + SDPAB_INIT_FACTOR",
+                                 "learned": "learned network proposal (SDPAB_INIT_DUAL)",
+                                 "none": "standard start lambda* I"}[args.start],
+                       "cuda_graph": gh is not None,
                        "launch_shape": {"headline": ch, "plain_fp64": c0, "autotune_ms_headline": tuneh["ms"],
                                         "autotune_ms_plain_fp64": tune0["ms"]},
                        "l2": "256 MB buffer written between timed steps",
@@ -529,7 +565,8 @@ def main():
                            "mean_iterations": float(res0.iterations.mean()),
                            "pdOPT": int(np.sum(res0.phase == 7))},
             "speedup_vs_plain_fp64": value / plain_value,
-            "warm_other_precision": alt,
+            "stages": stages,
+            "learned_warm_start": alt,
             "e2e": {"value": e2e_val, "unit": "SDPs/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": args.steps * launches_per_step,
             "roofline": {"bound": "tensor", "pipe": "FP64 MMA (mma.sync .f64) + FP64/FP32 SIMT",
@@ -539,7 +576,7 @@ def main():
                          "traffic": traffic, "traffic_note": TRAFFIC_NOTE,
                          "bf16_peak": bf16, "frac_of_bf16": achieved / bf16,
                          "bf16_peak_source": f"{src} (MEASURED_PEAKS.json)",
-                         "flops_per_launch": flops, "kernel": "batch_ipm_fp64"},
+                         "flops_per_launch": flops, "kernel": "batch_ipm_fp64", "kernel_ms": solver_ms},
             "clocks": clk.summary(),
             "parity": {"pdOPT": int(np.sum(res.phase == 7)), "count": int(P.count),
                        "mean_iterations": float(res.iterations.mean()),
