@@ -1,9 +1,10 @@
-"""The benchmark's headline configuration pinned to the reference.
+"""The learned warm start pinned to the reference.
 
 The first 512 instances of the 4096-instance batched MaxCut benchmark (seeds
-0..511, n ~ U{20..120}) are solved on the GPU exactly as the benchmark solves
-them: learned warm start (network forward, proposal kernel, SDPAB_INIT_DUAL)
-and mixed precision, through WarmPipeline.  Every instance is compared with
+0..511, n ~ U{20..120}) are solved on the GPU from the learned network's
+proposal (network forward, proposal kernel, SDPAB_INIT_DUAL) in mixed
+precision, through WarmPipeline, the benchmark's `learned_warm_start` leg
+(the headline's factor start is pinned the same way in test_lowrank_gpu).  Every instance is compared with
 the reference SDPA's own results on the same input (tests/golden/headline.*,
 made by the reference build):
 
@@ -67,8 +68,8 @@ def _classify(res, P, meta, arr):
     return obj_bad, x_strict, x_acc, x_bad, np.array(e_ours), np.array(e_ref)
 
 
-def test_headline_configuration_matches_reference():
-    """Warm start + mixed precision, the benchmark's pipeline."""
+def test_learned_start_matches_reference():
+    """Learned warm start + mixed precision."""
     import torch
     from sdpa_b200 import _native as N
     from sdpa_b200 import batch
@@ -82,7 +83,7 @@ def test_headline_configuration_matches_reference():
     torch.cuda.synchronize()
     res = db.result()
     obj_bad, x_strict, x_acc, x_bad, eo, er = _classify(res, P, meta, arr)
-    print(f"headline vs reference ({SEEDS}): objectives off {len(obj_bad)}, x within 1e-5 {x_strict}, "
+    print(f"learned start vs reference ({SEEDS}): objectives off {len(obj_bad)}, x within 1e-5 {x_strict}, "
           f"x only within the reference's accuracy {x_acc}, x outside both {len(x_bad)}; |x - x*| median "
           f"{np.median(eo):.2e} max {eo.max():.2e} (reference {np.median(er):.2e} / {er.max():.2e}); "
           f"iterations {res.iterations.mean():.2f} (reference {np.mean(meta['iterations']):.2f})")
