@@ -718,10 +718,18 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
             cta::tri_inverse<BT, double>(n, W1, n, LZi, n, sD, gsm);
             cta::gemm<BT>(n, true, LZi, n, false, LZi, n, Zi, n, 1.0, 0.0, gsm);
             if (delta == 0.0) {
+              // X0 = mu Z0^-1 = (sqrt(mu) L^-T)(sqrt(mu) L^-T)^T with Z0 = L L^T
+              // (L in W1), so L^T / sqrt(mu) is the inverse of a factor of X0:
+              // upper triangular, which serves as LXi (the step length's
+              // L^-1 dX L^-T has the same spectrum for any factor of X)
+              const double ism = 1.0 / sqrt(mu_s);
               for (int t = tid; t < nn_i; t += BT) {
+                const int i = t % n, j = t / n;
                 X[t] = mu_s * Zi[t];
-                W2[t] = X[t];
+                LXi[t] = W1[j + (size_t)n * i] * ism;
               }
+              __syncthreads();
+              warm = true;
             } else {
               // Z + tau I = (Z0 - delta I - mu (Y + tau I)^-1) + tau I, from
               // the unshifted parts still at hand: W2 = U U^T, sc = mu / tau
@@ -742,7 +750,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
               }
             }
             __syncthreads();
-            if (ok && cta::cholesky<BT, double>(n, W2, n, false, sD, gsm, &s_flag) == 0) {
+            if (!warm && ok && cta::cholesky<BT, double>(n, W2, n, false, sD, gsm, &s_flag) == 0) {
               cta::tri_inverse<BT, double>(n, W2, n, LXi, n, sD, gsm);
               warm = true;
             }
