@@ -68,11 +68,11 @@ constexpr int LR_RING = 32 * LR_SLOTS;
 
 // Shared memory of one warp for instances of order <= nmax with RL-wide
 // rows: V (nmax RL doubles), the ring (LR_RING records), sqrt(b) per row
-// (nmax doubles), row pointers and fill cursors (2 (nmax + 1) ints, rounded
-// up to 16 bytes).
+// (nmax doubles), row pointers, fill cursors and the flags of neighbouring
+// consecutive rows (3 (nmax + 1) ints, rounded up to 16 bytes).
 __host__ __device__ inline size_t lr_warp_bytes(int nmax, int RL)
 {
-  const size_t ints = (2 * ((size_t)nmax + 1) + 3) / 4 * 4;
+  const size_t ints = (3 * ((size_t)nmax + 1) + 3) / 4 * 4;
   return ((size_t)nmax * RL + nmax) * sizeof(double) + LR_RING * sizeof(LrRec) + ints * sizeof(int);
 }
 
@@ -129,6 +129,7 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
   double* sb = (double*)(ring + LR_RING);        // sqrt(b_i) by row
   int* rp = (int*)(sb + p.nmax);                 // row pointers (n + 1)
   int* cur = rp + p.nmax + 1;                    // counts, then fill cursors
+  int* adjn = cur + p.nmax + 1;                  // row i is a neighbour of row i + 1
   for (;;) {
     int qi = 0;
     if (lane == 0) qi = atomicAdd(queue, 1);
@@ -193,7 +194,10 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
     }
     if (lane == 0) rp[n] = carry;
     __syncwarp();
-    for (int i = lane; i < n; i += 32) cur[i] = rp[i];
+    for (int i = lane; i < n; i += 32) {
+      cur[i] = rp[i];
+      adjn[i] = 0;
+    }
     __syncwarp();
     // each 32-entry chunk places its entries in lane order (ranks among the
     // lanes with the same target row), so the layout does not depend on timing
@@ -220,6 +224,7 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
           rec.pad = 0;
           rec.w = v;
           crec[cur[key] + __popc(peers & lt)] = rec;
+          if (other == key + 1) adjn[key] = 1;
         }
         __syncwarp();
         if (ok && (peers & lt) == 0) cur[key] += __popc(peers);
@@ -266,62 +271,108 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
       while (src >= L) src -= L;
       while (issued < LR_SLOTS) issue();
     }
+    // one row's neighbours from the ring, records from stream position p0
+    auto acc_ring = [&](int p0, int deg, double& a0, double& a1, double& b0, double& b1) {
+      int t = h;
+      for (; t + H < deg; t += 2 * H) {
+        const LrRec r0 = ring[(p0 + t) & (LR_RING - 1)];
+        const LrRec r1 = ring[(p0 + t + H) & (LR_RING - 1)];
+        const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
+        const double2 v1 = *(const double2*)(Vs + r1.off + 2 * kk);
+        a0 = fma(r0.w, v0.x, a0);
+        a1 = fma(r0.w, v0.y, a1);
+        b0 = fma(r1.w, v1.x, b0);
+        b1 = fma(r1.w, v1.y, b1);
+      }
+      if (t < deg) {
+        const LrRec r0 = ring[(p0 + t) & (LR_RING - 1)];
+        const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
+        a0 = fma(r0.w, v0.x, a0);
+        a1 = fma(r0.w, v0.y, a1);
+      }
+    };
+    // the row's new value from its partial sums: group sums, norm, scale
+    auto finish = [&](int i, double g0, double g1, double& f) {
+#pragma unroll
+      for (int o = LPV; o < 32; o <<= 1) {
+        g0 += __shfl_xor_sync(FULL, g0, o);
+        g1 += __shfl_xor_sync(FULL, g1, o);
+      }
+      double ss = g0 * g0 + g1 * g1;
+#pragma unroll
+      for (int o = LPV / 2; o > 0; o >>= 1) ss += __shfl_xor_sync(FULL, ss, o);
+      if (ss > 0.0) {
+        const double sc = sb[i] * lr_rsqrt(ss);
+        if (h == 0) {
+          if (act0) Vs[i * RL + 2 * kk] = g0 * sc;
+          if (act1) Vs[i * RL + 2 * kk + 1] = g1 * sc;
+        }
+        f += sc * ss;
+      }
+    };
     double fold = 0.0;
     int s = 0;
     while (s < max_sweeps) {
       double f = 0.0;
-      for (int i = 0; i < n; ++i) {
+      for (int i = 0; i < n;) {
         const int deg = rp[i + 1] - rp[i];
-        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-        if (deg > 0 && deg <= LR_RING - 32) {
-          lr_wait(issued - 1 - ((pos + deg - 1) >> 5));  // the chunk of the row's last record
+        const int deg2 = (i + 1 < n) ? rp[i + 2] - rp[i + 1] : 0;
+        if (i + 1 < n && !adjn[i] && deg > 0 && deg2 > 0 && deg + deg2 <= LR_RING - 32) {
+          // rows i and i + 1 are not neighbours, so the update of i + 1 does
+          // not read row i: both update at once, with the results of the
+          // updates one after the other
+          lr_wait(issued - 1 - ((pos + deg + deg2 - 1) >> 5));
           __syncwarp();
-          int t = h;
-          for (; t + H < deg; t += 2 * H) {
-            const LrRec r0 = ring[(pos + t) & (LR_RING - 1)];
-            const LrRec r1 = ring[(pos + t + H) & (LR_RING - 1)];
-            const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
-            const double2 v1 = *(const double2*)(Vs + r1.off + 2 * kk);
-            a0 = fma(r0.w, v0.x, a0);
-            a1 = fma(r0.w, v0.y, a1);
-            b0 = fma(r1.w, v1.x, b0);
-            b1 = fma(r1.w, v1.y, b1);
-          }
-          if (t < deg) {
-            const LrRec r0 = ring[(pos + t) & (LR_RING - 1)];
-            const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
-            a0 = fma(r0.w, v0.x, a0);
-            a1 = fma(r0.w, v0.y, a1);
-          }
-        } else if (deg > 0) {
-          const LrRec* rr = crec + rp[i];
-          for (int t = h; t < deg; t += H) {
-            const LrRec r0 = rr[t];
-            const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
-            a0 = fma(r0.w, v0.x, a0);
-            a1 = fma(r0.w, v0.y, a1);
-          }
-        }
-        double g0 = act0 ? a0 + b0 : 0.0, g1 = act1 ? a1 + b1 : 0.0;
+          double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0, c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
+          acc_ring(pos, deg, a0, a1, b0, b1);
+          acc_ring(pos + deg, deg2, c0, c1, d0, d1);
+          double g0 = act0 ? a0 + b0 : 0.0, g1 = act1 ? a1 + b1 : 0.0;
+          double e0 = act0 ? c0 + d0 : 0.0, e1 = act1 ? c1 + d1 : 0.0;
 #pragma unroll
-        for (int o = LPV; o < 32; o <<= 1) {
-          g0 += __shfl_xor_sync(FULL, g0, o);
-          g1 += __shfl_xor_sync(FULL, g1, o);
-        }
-        double ss = g0 * g0 + g1 * g1;
+          for (int o = LPV; o < 32; o <<= 1) {
+            g0 += __shfl_xor_sync(FULL, g0, o);
+            g1 += __shfl_xor_sync(FULL, g1, o);
+            e0 += __shfl_xor_sync(FULL, e0, o);
+            e1 += __shfl_xor_sync(FULL, e1, o);
+          }
+          double ss = g0 * g0 + g1 * g1, tt = e0 * e0 + e1 * e1;
 #pragma unroll
-        for (int o = LPV / 2; o > 0; o >>= 1) ss += __shfl_xor_sync(FULL, ss, o);
-        if (ss > 0.0) {
-          const double rs = lr_rsqrt(ss);
-          const double sc = sb[i] * rs;
+          for (int o = LPV / 2; o > 0; o >>= 1) {
+            ss += __shfl_xor_sync(FULL, ss, o);
+            tt += __shfl_xor_sync(FULL, tt, o);
+          }
+          const double rs = lr_rsqrt(ss > 0.0 ? ss : 1.0), rt = lr_rsqrt(tt > 0.0 ? tt : 1.0);
+          const double sc = sb[i] * rs, sd = sb[i + 1] * rt;
           if (h == 0) {
-            if (act0) Vs[i * RL + 2 * kk] = g0 * sc;
-            if (act1) Vs[i * RL + 2 * kk + 1] = g1 * sc;
+            if (ss > 0.0 && act0) Vs[i * RL + 2 * kk] = g0 * sc;
+            if (ss > 0.0 && act1) Vs[i * RL + 2 * kk + 1] = g1 * sc;
+            if (tt > 0.0 && act0) Vs[(i + 1) * RL + 2 * kk] = e0 * sd;
+            if (tt > 0.0 && act1) Vs[(i + 1) * RL + 2 * kk + 1] = e1 * sd;
           }
-          f += sc * ss;
+          if (ss > 0.0) f += sc * ss;
+          if (tt > 0.0) f += sd * tt;
+          pos += deg + deg2;
+          i += 2;
+        } else {
+          double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+          if (deg > 0 && deg <= LR_RING - 32) {
+            lr_wait(issued - 1 - ((pos + deg - 1) >> 5));  // the chunk of the row's last record
+            __syncwarp();
+            acc_ring(pos, deg, a0, a1, b0, b1);
+          } else if (deg > 0) {
+            const LrRec* rr = crec + rp[i];
+            for (int t = h; t < deg; t += H) {
+              const LrRec r0 = rr[t];
+              const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
+              a0 = fma(r0.w, v0.x, a0);
+              a1 = fma(r0.w, v0.y, a1);
+            }
+          }
+          finish(i, act0 ? a0 + b0 : 0.0, act1 ? a1 + b1 : 0.0, f);
+          pos += deg;
+          i += 1;
         }
-        pos += deg;
-        __syncwarp();  // the row's ring records are read, its V row written
+        __syncwarp();  // the rows' ring records are read, their V rows written
         while (issued < (pos >> 5) + LR_SLOTS) issue();
       }
       ++s;

@@ -18,6 +18,8 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
+
 from . import _native as N
 
 INIT_FACTOR = 3
@@ -44,6 +46,12 @@ class FactorPipeline:
         self.sweeps = torch.zeros(P.count, dtype=torch.int32, device=dev)
         self.flag = torch.full((P.count,), INIT_FACTOR, dtype=torch.int32, device=dev)
         self.num_entries = int(db.d["val"].numel())
+        # the mixing kernel's queue order: most work per sweep first (rows
+        # plus neighbour records), so the longest instances start first
+        f0 = P.mat_ptr[P.mat_off + 1] - P.mat_ptr[P.mat_off]
+        cost = P.n.astype(np.int64) + 2 * f0.astype(np.int64)
+        order = np.argsort(-cost, kind="stable").astype(np.int32)
+        self.order = torch.from_numpy(order).to(dev)
         db.init = N.BatchInit(self.flag.data_ptr(), None, None, None, 0.0, self.V.data_ptr(), self.rank,
                               float(init_mu))
 
@@ -52,7 +60,7 @@ class FactorPipeline:
         s = stream if stream is not None else torch.cuda.current_stream()
         N.check(N.lib().sdpab_lowrank_factor(ctypes.byref(self.db._bt), self.num_entries, self.rank,
                                              self.max_sweeps, self.tol, self.seed, self.V.data_ptr(),
-                                             self.sweeps.data_ptr(), self.db.order.data_ptr(), s.cuda_stream),
+                                             self.sweeps.data_ptr(), self.order.data_ptr(), s.cuda_stream),
                 "sdpab_lowrank_factor")
 
     def run(self, precision=N.PREC_FP64, stream=None, **shape):
