@@ -63,16 +63,17 @@ struct __align__(16) LrRec {
 };
 
 // The ring: LR_SLOTS chunks of 32 records.
-constexpr int LR_SLOTS = 4;
+constexpr int LR_SLOTS = 8;
 constexpr int LR_RING = 32 * LR_SLOTS;
 
 // Shared memory of one warp for instances of order <= nmax with RL-wide
 // rows: V (nmax RL doubles), the ring (LR_RING records), sqrt(b) per row
-// (nmax doubles), row pointers, fill cursors and the flags of neighbouring
-// consecutive rows (3 (nmax + 1) ints, rounded up to 16 bytes).
+// (nmax doubles), record offsets by row, fill cursors / colours, the update
+// order, the group starts and the record offsets by position (5 (nmax + 1)
+// ints, rounded up to 16 bytes).
 __host__ __device__ inline size_t lr_warp_bytes(int nmax, int RL)
 {
-  const size_t ints = (3 * ((size_t)nmax + 1) + 3) / 4 * 4;
+  const size_t ints = (5 * ((size_t)nmax + 1) + 3) / 4 * 4;
   return ((size_t)nmax * RL + nmax) * sizeof(double) + LR_RING * sizeof(LrRec) + ints * sizeof(int);
 }
 
@@ -86,7 +87,11 @@ __device__ __forceinline__ void lr_commit() { asm volatile("cp.async.commit_grou
 // recent copy groups are still in flight.
 __device__ __forceinline__ void lr_wait(int pending)
 {
-  if (pending >= 3) asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+  if (pending >= 7) asm volatile("cp.async.wait_group 7;\n" ::: "memory");
+  else if (pending == 6) asm volatile("cp.async.wait_group 6;\n" ::: "memory");
+  else if (pending == 5) asm volatile("cp.async.wait_group 5;\n" ::: "memory");
+  else if (pending == 4) asm volatile("cp.async.wait_group 4;\n" ::: "memory");
+  else if (pending == 3) asm volatile("cp.async.wait_group 3;\n" ::: "memory");
   else if (pending == 2) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
   else if (pending == 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
   else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -121,15 +126,16 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
   extern __shared__ __align__(16) unsigned char lr_smem[];
   constexpr unsigned FULL = 0xffffffffu;
   constexpr int LPV = RL / 2;   // lanes per row vector, two components each
-  constexpr int H = 32 / LPV;   // lane groups, each taking every H-th neighbour
+  constexpr int H = 32 / LPV;   // lane groups: one row of a group each
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  double* Vs = (double*)lr_smem;                 // n x RL
+  double* Vs = (double*)lr_smem;                 // n x RL, rows in the instance's order
   LrRec* ring = (LrRec*)(Vs + (size_t)p.nmax * RL);
   double* sb = (double*)(ring + LR_RING);        // sqrt(b_i) by row
-  int* rp = (int*)(sb + p.nmax);                 // row pointers (n + 1)
-  int* cur = rp + p.nmax + 1;                    // counts, then fill cursors
-  int* adjn = cur + p.nmax + 1;                  // row i is a neighbour of row i + 1
+  int* rp = (int*)(sb + p.nmax);                 // record offsets (n + 1): by row, then by position
+  int* cur = rp + p.nmax + 1;                    // counts, fill cursors, then colours (n + 1)
+  int* perm = cur + p.nmax + 1;                  // the rows in update order (n)
+  int* gs = perm + p.nmax;                       // group starts, in positions (n + 1)
   for (;;) {
     int qi = 0;
     if (lane == 0) qi = atomicAdd(queue, 1);
@@ -179,29 +185,33 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
       continue;
     }
     __syncwarp();
-    int carry = 0;
-    for (int i0 = 0; i0 < n; i0 += 32) {
-      const int i = i0 + lane;
-      const int v = (i < n) ? cur[i] : 0;
-      int s = v;
+    // exclusive scan of cur[0 .. cnt) into dst[0 .. cnt], the total in dst[cnt]
+    auto scan = [&](const int* src, int* dst, int cnt) {
+      int carry = 0;
+      for (int i0 = 0; i0 < cnt; i0 += 32) {
+        const int i = i0 + lane;
+        const int v = (i < cnt) ? src[i] : 0;
+        int s = v;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(FULL, s, o);
-        if (lane >= o) s += t;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(FULL, s, o);
+          if (lane >= o) s += t;
+        }
+        if (i < cnt) dst[i] = carry + s - v;
+        carry += __shfl_sync(FULL, s, 31);
       }
-      if (i < n) rp[i] = carry + s - v;
-      carry += __shfl_sync(FULL, s, 31);
-    }
-    if (lane == 0) rp[n] = carry;
-    __syncwarp();
-    for (int i = lane; i < n; i += 32) {
-      cur[i] = rp[i];
-      adjn[i] = 0;
-    }
+      if (lane == 0) dst[cnt] = carry;
+      __syncwarp();
+    };
+    scan(cur, rp, n);
+    for (int i = lane; i < n; i += 32) cur[i] = rp[i];
     __syncwarp();
     // each 32-entry chunk places its entries in lane order (ranks among the
-    // lanes with the same target row), so the layout does not depend on timing
-    LrRec* crec = csr + 2 * f0;
+    // lanes with the same target row), so the layout does not depend on
+    // timing; records by row go to region A (2 f0 ..), by update position to
+    // region B (2 num_entries + 2 f0 ..)
+    LrRec* recA = csr + 2 * f0;
+    LrRec* recB = csr + 2 * num_entries + 2 * f0;
     for (long long c0 = f0; c0 < f1; c0 += 32) {
       const long long e = c0 + lane;
       int r = -1, c = -1;
@@ -223,14 +233,76 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
           rec.off = other * RL;
           rec.pad = 0;
           rec.w = v;
-          crec[cur[key] + __popc(peers & lt)] = rec;
-          if (other == key + 1) adjn[key] = 1;
+          recA[cur[key] + __popc(peers & lt)] = rec;
         }
         __syncwarp();
         if (ok && (peers & lt) == 0) cur[key] += __popc(peers);
         __syncwarp();
       }
     }
+    __threadfence_block();
+    // ---- greedy colouring in row order: row i takes the smallest colour
+    // below 64 that no neighbour coloured before it has (64 + i when none is
+    // free); rows of one colour are not neighbours, so their updates commute
+    int* col = cur;
+    for (int i = lane; i < n; i += 32) col[i] = -1;
+    __syncwarp();
+    for (int i = 0; i < n; ++i) {
+      unsigned lo = 0, hi = 0;
+      for (int t = rp[i] + lane; t < rp[i + 1]; t += 32) {
+        const int cj = col[recA[t].off / RL];
+        if (cj >= 0 && cj < 32) lo |= 1u << cj;
+        else if (cj >= 32 && cj < 64) hi |= 1u << (cj - 32);
+      }
+      lo = __reduce_or_sync(FULL, lo);
+      hi = __reduce_or_sync(FULL, hi);
+      const int c = (~lo) ? __ffs(~lo) - 1 : ((~hi) ? 31 + __ffs(~hi) : 64 + i);
+      if (lane == 0) col[i] = c;
+      __syncwarp();
+    }
+    // ---- update order: the rows by colour, in row order within a colour
+    {
+      int np = 0;
+      for (int c = 0; c < 65 && np < n; ++c) {
+        for (int i0 = 0; i0 < n; i0 += 32) {
+          const int i = i0 + lane;
+          const bool in = i < n && (c < 64 ? col[i] == c : col[i] >= 64);
+          const unsigned bal = __ballot_sync(FULL, in);
+          if (in) perm[np + __popc(bal & lt)] = i;
+          np += __popc(bal);
+        }
+      }
+    }
+    __syncwarp();
+    // ---- records in update order (region B) and their offsets pp by position
+    int* pp = gs + p.nmax + 1;
+    for (int k = lane; k < n; k += 32) pp[k] = rp[perm[k] + 1] - rp[perm[k]];
+    __syncwarp();
+    scan(pp, pp, n);
+    for (int k = 0; k < n; ++k) {
+      const int src = rp[perm[k]], dst = pp[k], cnt = pp[k + 1] - pp[k];
+      for (int t = lane; t < cnt; t += 32) recB[dst + t] = recA[src + t];
+    }
+    // ---- groups of up to H consecutive positions of one colour whose
+    // records fit the ring together (a longer row is a group of its own)
+    int ng = 0;
+    if (lane == 0) {
+      int k = 0;
+      while (k < n) {
+        const int start = k, c = col[perm[k]];
+        int tot = pp[k + 1] - pp[k];
+        ++k;
+        while (k < n && k - start < H && col[perm[k]] == c && tot + pp[k + 1] - pp[k] <= LR_RING - 32) {
+          tot += pp[k + 1] - pp[k];
+          ++k;
+        }
+        gs[ng++] = start;
+      }
+      gs[ng] = n;
+    }
+    ng = __shfl_sync(FULL, ng, 0);
+    __threadfence_block();
+    __syncwarp();
     // ---- seeded start, rows scaled to norm sqrt(b_i)
     const int rq = lr_rank_for(n, R);
     for (int t = lane; t < n * RL; t += 32) {
@@ -245,139 +317,100 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
       for (int k = 0; k < rq; ++k) Vs[i * RL + k] *= sc;
     }
     __syncwarp();
-    // ---- sweeps.  Lane (h, kk) holds components 2kk, 2kk + 1 of the row
-    // vector and takes the neighbours t = h, h + H, ... of each row.  The
-    // rows' records, sweep after sweep, are one periodic stream of L = rp[n]
-    // records; the warp copies it 32 records at a time into the ring, up to
-    // LR_SLOTS chunks ahead of the row being updated.  A row longer than the
-    // ring reads its records from global memory.
+    // ---- sweeps, one group of rows at a time: lane group h (LPV lanes, two
+    // components each) updates the group's h-th row.  The groups' records,
+    // sweep after sweep, are one periodic stream of L = pp[n] records; the
+    // warp copies it 32 records at a time into the ring, up to LR_SLOTS
+    // chunks ahead of the group being updated.
     const int h = lane / LPV, kk = lane % LPV;
     const bool act0 = 2 * kk < rq, act1 = 2 * kk + 1 < rq;
-    const int L = rp[n];
+    const int L = pp[n];
     int issued = 0;   // chunks of the stream issued
-    int pos = 0;      // stream position of the current row's first record
+    int pos = 0;      // stream position of the current group's first record
     int src = 0;      // this lane's record of the next chunk: (32 issued + lane) mod L
     auto issue = [&]() {
       if (L > 0) {
-        lr_cp16(&ring[(issued & (LR_SLOTS - 1)) * 32 + lane], crec + src);
+        lr_cp16(&ring[(issued & (LR_SLOTS - 1)) * 32 + lane], recB + src);
         src += 32;
         while (src >= L) src -= L;
       }
       lr_commit();
       ++issued;
     };
+    __threadfence();  // region B's records are written before the ring copies read them
+    __syncwarp();
     if (L > 0) {
       src = lane;
       while (src >= L) src -= L;
       while (issued < LR_SLOTS) issue();
     }
-    // one row's neighbours from the ring, records from stream position p0
-    auto acc_ring = [&](int p0, int deg, double& a0, double& a1, double& b0, double& b1) {
-      int t = h;
-      for (; t + H < deg; t += 2 * H) {
-        const LrRec r0 = ring[(p0 + t) & (LR_RING - 1)];
-        const LrRec r1 = ring[(p0 + t + H) & (LR_RING - 1)];
-        const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
-        const double2 v1 = *(const double2*)(Vs + r1.off + 2 * kk);
-        a0 = fma(r0.w, v0.x, a0);
-        a1 = fma(r0.w, v0.y, a1);
-        b0 = fma(r1.w, v1.x, b0);
-        b1 = fma(r1.w, v1.y, b1);
-      }
-      if (t < deg) {
-        const LrRec r0 = ring[(p0 + t) & (LR_RING - 1)];
-        const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
-        a0 = fma(r0.w, v0.x, a0);
-        a1 = fma(r0.w, v0.y, a1);
-      }
-    };
-    // the row's new value from its partial sums: group sums, norm, scale
-    auto finish = [&](int i, double g0, double g1, double& f) {
-#pragma unroll
-      for (int o = LPV; o < 32; o <<= 1) {
-        g0 += __shfl_xor_sync(FULL, g0, o);
-        g1 += __shfl_xor_sync(FULL, g1, o);
-      }
-      double ss = g0 * g0 + g1 * g1;
-#pragma unroll
-      for (int o = LPV / 2; o > 0; o >>= 1) ss += __shfl_xor_sync(FULL, ss, o);
-      if (ss > 0.0) {
-        const double sc = sb[i] * lr_rsqrt(ss);
-        if (h == 0) {
-          if (act0) Vs[i * RL + 2 * kk] = g0 * sc;
-          if (act1) Vs[i * RL + 2 * kk + 1] = g1 * sc;
-        }
-        f += sc * ss;
-      }
-    };
     double fold = 0.0;
     int s = 0;
     while (s < max_sweeps) {
-      double f = 0.0;
-      for (int i = 0; i < n;) {
-        const int deg = rp[i + 1] - rp[i];
-        const int deg2 = (i + 1 < n) ? rp[i + 2] - rp[i + 1] : 0;
-        if (i + 1 < n && !adjn[i] && deg > 0 && deg2 > 0 && deg + deg2 <= LR_RING - 32) {
-          // rows i and i + 1 are not neighbours, so the update of i + 1 does
-          // not read row i: both update at once, with the results of the
-          // updates one after the other
-          lr_wait(issued - 1 - ((pos + deg + deg2 - 1) >> 5));
+      double fl = 0.0;  // this lane's share of sum_i sqrt(b_i) |g_i|
+      for (int g = 0; g < ng; ++g) {
+        const int k0 = gs[g], k1 = gs[g + 1];
+        const int tot = pp[k1] - pp[k0];
+        const bool inring = tot <= LR_RING - 32;
+        if (inring && tot > 0) {
+          lr_wait(issued - 1 - ((pos + tot - 1) >> 5));  // the chunk of the group's last record
           __syncwarp();
-          double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0, c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
-          acc_ring(pos, deg, a0, a1, b0, b1);
-          acc_ring(pos + deg, deg2, c0, c1, d0, d1);
-          double g0 = act0 ? a0 + b0 : 0.0, g1 = act1 ? a1 + b1 : 0.0;
-          double e0 = act0 ? c0 + d0 : 0.0, e1 = act1 ? c1 + d1 : 0.0;
-#pragma unroll
-          for (int o = LPV; o < 32; o <<= 1) {
-            g0 += __shfl_xor_sync(FULL, g0, o);
-            g1 += __shfl_xor_sync(FULL, g1, o);
-            e0 += __shfl_xor_sync(FULL, e0, o);
-            e1 += __shfl_xor_sync(FULL, e1, o);
-          }
-          double ss = g0 * g0 + g1 * g1, tt = e0 * e0 + e1 * e1;
-#pragma unroll
-          for (int o = LPV / 2; o > 0; o >>= 1) {
-            ss += __shfl_xor_sync(FULL, ss, o);
-            tt += __shfl_xor_sync(FULL, tt, o);
-          }
-          const double rs = lr_rsqrt(ss > 0.0 ? ss : 1.0), rt = lr_rsqrt(tt > 0.0 ? tt : 1.0);
-          const double sc = sb[i] * rs, sd = sb[i + 1] * rt;
-          if (h == 0) {
-            if (ss > 0.0 && act0) Vs[i * RL + 2 * kk] = g0 * sc;
-            if (ss > 0.0 && act1) Vs[i * RL + 2 * kk + 1] = g1 * sc;
-            if (tt > 0.0 && act0) Vs[(i + 1) * RL + 2 * kk] = e0 * sd;
-            if (tt > 0.0 && act1) Vs[(i + 1) * RL + 2 * kk + 1] = e1 * sd;
-          }
-          if (ss > 0.0) f += sc * ss;
-          if (tt > 0.0) f += sd * tt;
-          pos += deg + deg2;
-          i += 2;
-        } else {
-          double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-          if (deg > 0 && deg <= LR_RING - 32) {
-            lr_wait(issued - 1 - ((pos + deg - 1) >> 5));  // the chunk of the row's last record
-            __syncwarp();
-            acc_ring(pos, deg, a0, a1, b0, b1);
-          } else if (deg > 0) {
-            const LrRec* rr = crec + rp[i];
-            for (int t = h; t < deg; t += H) {
+        }
+        const int k = k0 + h;
+        const bool mine = k < k1;
+        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+        int row = 0;
+        if (mine) {
+          row = perm[k];
+          const int d = pp[k + 1] - pp[k];
+          if (inring) {
+            const int rb = pos + pp[k] - pp[k0];
+            int t = 0;
+            for (; t + 1 < d; t += 2) {
+              const LrRec r0 = ring[(rb + t) & (LR_RING - 1)];
+              const LrRec r1 = ring[(rb + t + 1) & (LR_RING - 1)];
+              const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
+              const double2 v1 = *(const double2*)(Vs + r1.off + 2 * kk);
+              a0 = fma(r0.w, v0.x, a0);
+              a1 = fma(r0.w, v0.y, a1);
+              b0 = fma(r1.w, v1.x, b0);
+              b1 = fma(r1.w, v1.y, b1);
+            }
+            if (t < d) {
+              const LrRec r0 = ring[(rb + t) & (LR_RING - 1)];
+              const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
+              a0 = fma(r0.w, v0.x, a0);
+              a1 = fma(r0.w, v0.y, a1);
+            }
+          } else {
+            const LrRec* rr = recB + pp[k];
+            for (int t = 0; t < d; ++t) {
               const LrRec r0 = rr[t];
               const double2 v0 = *(const double2*)(Vs + r0.off + 2 * kk);
               a0 = fma(r0.w, v0.x, a0);
               a1 = fma(r0.w, v0.y, a1);
             }
           }
-          finish(i, act0 ? a0 + b0 : 0.0, act1 ? a1 + b1 : 0.0, f);
-          pos += deg;
-          i += 1;
         }
-        __syncwarp();  // the rows' ring records are read, their V rows written
+        const double g0 = (mine && act0) ? a0 + b0 : 0.0, g1 = (mine && act1) ? a1 + b1 : 0.0;
+        double ss = g0 * g0 + g1 * g1;
+#pragma unroll
+        for (int o = LPV / 2; o > 0; o >>= 1) ss += __shfl_xor_sync(FULL, ss, o);
+        if (mine && ss > 0.0) {
+          const double sc = sb[row] * lr_rsqrt(ss);
+          if (act0) Vs[row * RL + 2 * kk] = g0 * sc;
+          if (act1) Vs[row * RL + 2 * kk + 1] = g1 * sc;
+          if (kk == 0) fl += sc * ss;
+        }
+        pos += tot;
+        __syncwarp();  // the group's ring records are read, its V rows written
         while (issued < (pos >> 5) + LR_SLOTS) issue();
       }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) fl += __shfl_xor_sync(FULL, fl, o);
       ++s;
-      if (s > 1 && fabs(f - fold) <= tol * fabs(f)) break;
-      fold = f;
+      if (s > 1 && fabs(fl - fold) <= tol * fabs(fl)) break;
+      fold = fl;
     }
     lr_wait(0);
     __syncwarp();
@@ -449,7 +482,7 @@ extern "C" int sdpab_lowrank_factor(const sdpab_batch* prob, long long num_entri
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return set_error(SDPAB_ENODEV, "lowrank_factor: no CUDA device");
   LrScratch& S = g_lr[(dev >= 0 && dev < LR_MAX_DEVICES) ? dev : 0];
-  const long long need = std::max<long long>(2 * num_entries, 32);
+  const long long need = std::max<long long>(4 * num_entries, 32);  // records by row, then by position
   if (S.cap < need) {
     S.release();
     if (cudaMalloc((void**)&S.rec, need * sizeof(LrRec)) != cudaSuccess ||

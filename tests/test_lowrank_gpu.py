@@ -1,8 +1,8 @@
 """The low-rank factor start (sdpab_lowrank_factor + SDPAB_INIT_FACTOR).
 
 * The mixing-method kernel against a numpy restatement of the same
-  iteration (same seeded start, rows in order): Y = V V^T agrees after a
-  fixed number of sweeps.
+  iteration (same seeded start, rows in the kernel's colour order): Y = V V^T
+  agrees after a fixed number of sweeps.
 * The benchmark's headline set (first 512 instances of the 4096-instance
   MaxCut batch) solved from the factor start against the reference SDPA's
   own results (tests/golden/headline.*): every instance pdOPT with both
@@ -50,6 +50,19 @@ def _f0(it, n):
     return F0
 
 
+def _update_order(A):
+    """The kernel's row order: greedy colours in row order (the smallest
+    colour below 64 no earlier neighbour has, else a class of its own after
+    all others), rows by colour, in row order within a colour."""
+    n = A.shape[0]
+    col = np.full(n, -1)
+    for i in range(n):
+        used = {int(col[j]) for j in np.nonzero(A[i])[0] if 0 <= col[j] < 64}
+        free = [c for c in range(64) if c not in used]
+        col[i] = free[0] if free else 64 + i
+    return sorted(range(n), key=lambda i: (min(col[i], 64), i))
+
+
 def _mixing(F0, rq, R, seed, q, sweeps):
     n = F0.shape[0]
     V = np.zeros((n, R))
@@ -57,8 +70,9 @@ def _mixing(F0, rq, R, seed, q, sweeps):
         V[i, :rq] = [_uniform(seed, q, i, k) for k in range(rq)]
         V[i] /= np.linalg.norm(V[i])
     A = F0 - np.diag(np.diag(F0))
+    order = _update_order(A)
     for _ in range(sweeps):
-        for i in range(n):
+        for i in order:
             g = A[i] @ V
             nr = np.linalg.norm(g)
             if nr > 0:
