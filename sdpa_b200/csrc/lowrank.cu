@@ -366,6 +366,7 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
           if (inring) {
             const int rb = pos + pp[k] - pp[k0];
             int t = 0;
+#pragma unroll 2
             for (; t + 1 < d; t += 2) {
               const LrRec r0 = ring[(rb + t) & (LR_RING - 1)];
               const LrRec r1 = ring[(rb + t + 1) & (LR_RING - 1)];
