@@ -140,6 +140,20 @@ SDPAB_API int sdpab_sdpa_tc_timeouts(sdpab_sdpa* h, int* out);
 SDPAB_API int sdpab_sdpa_solve(sdpab_sdpa* h);
 /* scalar getters (sdpa_call.cpp:719-847) */
 SDPAB_API int sdpab_sdpa_info(sdpab_sdpa* h, sdpab_sdpa_info_t* out);
+/* The constraint order of the host-driven solver's Schur factorisation (no
+ * counterpart in the reference, which leaves the order to MUMPS when it
+ * takes its sparse path, Chordal::ordering_bMat, sdpa_chordal.cpp:365-524).
+ * Problems of two or more SDP blocks and at least 512 constraints are put in
+ * a minimum-degree order of the constraint groups (constraints sharing an
+ * SDP block or an LP coordinate) when that leaves fewer 128 x 128 tile pairs
+ * in the symbolic factorisation than the caller's order; results always
+ * come back in the caller's order (SDPAB_ORDER=natural in the environment
+ * keeps the caller's order).  Host only, no device work: order[position] =
+ * constraint (0-based), pairs[0] / pairs[1] = the symbolic tile pairs in the
+ * caller's / the returned order.  Entries as for sdpab_sdpa_input_problem. */
+SDPAB_API int sdpab_constraint_order(int m, int nblock, const int* block_struct, long long nnz, const int* k,
+                                     const int* l, const int* i, const int* j, int* order, long long* pairs);
+
 /* Device seconds per solver phase (the reference's ComputeTime categories,
  * sdpa_parts.h:48-86): out8 = rMat+gVec, bMat, Cholesky, solves, dX/dZ,
  * step length, update (inverses), residuals. */

@@ -108,6 +108,8 @@ SIGNATURES = [
     ("sdpab_sdpa_info", c_int, [c_void_p, POINTER(SdpaInfo)]),
     ("sdpab_sdpa_phase_times", c_int, [c_void_p, c_void_p]),
     ("sdpab_sdpa_schur_pattern", c_int, [c_void_p, POINTER(c_int), c_void_p]),
+    ("sdpab_constraint_order", c_int, [c_int, c_int, c_void_p, c_longlong, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p]),
     ("sdpab_sdpa_get_xvec", c_int, [c_void_p, c_void_p]),
     ("sdpab_sdpa_get_block", c_int, [c_void_p, c_int, c_int, c_void_p]),
     ("sdpab_sdpa_block_size", c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),

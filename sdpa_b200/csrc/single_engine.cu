@@ -12,7 +12,10 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
+#include <map>
 #include <numeric>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -1482,7 +1485,208 @@ int Solver::formula_count(int f) const
   return c;
 }
 
+// ------------------------------------------------------------ constraint order
+// Groups of constraints (0-based) whose Schur entries couple: those with an
+// entry in the same SDP block, or at the same LP coordinate (the aggregate
+// sparsity pattern of B, Chordal's analysis, sdpa_chordal.cpp:365-524).
+static std::vector<std::vector<int>> constraint_groups(const ProblemData& p)
+{
+  const int nb = (int)p.blockStruct.size();
+  std::map<std::pair<int, int>, int> id;  // (block, LP coordinate or -1) -> group
+  std::vector<std::vector<int>> g;
+  for (const Entry& e : p.entries) {
+    if (e.k < 1 || e.k > p.m || e.l < 1 || e.l > nb) continue;
+    const int bs = p.blockStruct[e.l - 1];
+    const std::pair<int, int> key(e.l, (bs > 1) ? -1 : std::min(e.i, e.j));
+    auto it = id.find(key);
+    int gi;
+    if (it == id.end()) {
+      gi = (int)g.size();
+      id.emplace(key, gi);
+      g.emplace_back();
+    } else {
+      gi = it->second;
+    }
+    g[gi].push_back(e.k - 1);
+  }
+  for (auto& v : g) {
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+  }
+  return g;
+}
+
+// Trailing tile pairs of the symbolic 128 x 128 tile Cholesky of B with the
+// constraints at positions pos[k] (the count the factorisation would visit).
+static long long symbolic_tile_pairs(const std::vector<std::vector<int>>& groups, const std::vector<int>& pos, int m)
+{
+  const int nt = (m + NBG - 1) / NBG;
+  std::vector<std::vector<char>> P(nt, std::vector<char>(nt, 0));
+  std::vector<int> t;
+  for (const auto& grp : groups) {
+    t.clear();
+    for (int k : grp) t.push_back(pos[k] / NBG);
+    std::sort(t.begin(), t.end());
+    t.erase(std::unique(t.begin(), t.end()), t.end());
+    for (size_t a = 0; a < t.size(); ++a)
+      for (size_t b = 0; b <= a; ++b) P[t[a]][t[b]] = 1;
+  }
+  long long pairs = 0;
+  std::vector<int> R;
+  for (int k = 0; k < nt; ++k) {
+    R.clear();
+    for (int i = k + 1; i < nt; ++i)
+      if (P[i][k]) R.push_back(i);
+    for (size_t a = 0; a < R.size(); ++a)
+      for (size_t b = 0; b <= a; ++b) {
+        P[R[a]][R[b]] = 1;
+        if (R[b] >= k + 2) ++pairs;
+      }
+  }
+  return pairs;
+}
+
+// Minimum-degree elimination order of the constraints on the group
+// (clique) structure, by element absorption: eliminating a constraint merges
+// the groups that hold it into one new group of their other members; a
+// constraint's degree is taken as the sum of (size - 1) over its live
+// groups, an upper bound of its true degree (as in approximate minimum
+// degree orderings).  Ties go to the lower index, so the order is
+// deterministic.  Returns position -> constraint.
+static std::vector<int> min_degree_order(const std::vector<std::vector<int>>& groups, int m)
+{
+  std::vector<std::vector<int>> E = groups;
+  std::vector<char> alive(E.size(), 1);
+  std::vector<std::vector<int>> of(m);
+  for (int e = 0; e < (int)E.size(); ++e)
+    for (int k : E[e]) of[k].push_back(e);
+  auto degree = [&](int k) {
+    long long d = 0;
+    for (int e : of[k])
+      if (alive[e]) d += (long long)E[e].size() - 1;
+    return d;
+  };
+  using Item = std::pair<long long, int>;
+  std::priority_queue<Item, std::vector<Item>, std::greater<Item>> pq;
+  std::vector<long long> deg(m);
+  for (int k = 0; k < m; ++k) {
+    deg[k] = degree(k);
+    pq.push({deg[k], k});
+  }
+  std::vector<char> done(m, 0);
+  std::vector<int> stamp(m, -1), order;
+  order.reserve(m);
+  while (!pq.empty()) {
+    const Item it = pq.top();
+    pq.pop();
+    const int v = it.second;
+    if (done[v] || it.first != deg[v]) continue;  // stale entry
+    done[v] = 1;
+    order.push_back(v);
+    std::vector<int> U;
+    for (int e : of[v]) {
+      if (!alive[e]) continue;
+      for (int u : E[e])
+        if (!done[u] && stamp[u] != v) {
+          stamp[u] = v;
+          U.push_back(u);
+        }
+      alive[e] = 0;
+      std::vector<int>().swap(E[e]);
+    }
+    if (U.empty()) continue;
+    std::sort(U.begin(), U.end());
+    const int ne = (int)E.size();
+    E.push_back(U);
+    alive.push_back(1);
+    for (int u : U) {
+      auto& L = of[u];
+      L.erase(std::remove_if(L.begin(), L.end(), [&](int e) { return !alive[e]; }), L.end());
+      L.push_back(ne);
+      deg[u] = degree(u);
+      pq.push({deg[u], u});
+    }
+  }
+  return order;
+}
+
+// The constraints by the number of groups they touch, then by their first
+// group, then by index: constraints local to one block come first, grouped
+// by block, the coupling ones last (the arrowhead order, which keeps the
+// couplings out of the diagonal tiles).
+static std::vector<int> group_count_order(const std::vector<std::vector<int>>& groups, int m)
+{
+  std::vector<int> cnt(m, 0), first(m, 1 << 30);
+  for (int g = 0; g < (int)groups.size(); ++g)
+    for (int k : groups[g]) {
+      ++cnt[k];
+      first[k] = std::min(first[k], g);
+    }
+  std::vector<int> o(m);
+  std::iota(o.begin(), o.end(), 0);
+  std::stable_sort(o.begin(), o.end(), [&](int a, int b) {
+    if (cnt[a] != cnt[b]) return cnt[a] < cnt[b];
+    return first[a] < first[b];
+  });
+  return o;
+}
+
+// The order with the fewest symbolic tile pairs among the caller's, the
+// minimum-degree and the group-count orders (the caller's on ties).
+static std::vector<int> best_constraint_order(const std::vector<std::vector<int>>& groups, int m,
+                                              long long* pairs_natural, long long* pairs_best)
+{
+  std::vector<int> ident(m), pos(m);
+  std::iota(ident.begin(), ident.end(), 0);
+  const long long nat = symbolic_tile_pairs(groups, ident, m);
+  std::vector<int> best = ident;
+  long long bp = nat;
+  for (int cand = 0; cand < 2; ++cand) {
+    std::vector<int> o = cand == 0 ? min_degree_order(groups, m) : group_count_order(groups, m);
+    if ((int)o.size() != m) continue;
+    for (int q = 0; q < m; ++q) pos[o[q]] = q;
+    const long long pr = symbolic_tile_pairs(groups, pos, m);
+    if (pr < bp) {
+      bp = pr;
+      best = o;
+    }
+  }
+  if (pairs_natural) *pairs_natural = nat;
+  if (pairs_best) *pairs_best = bp;
+  return best;
+}
+
 int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
+{
+  perm_.clear();
+  const char* env = getenv("SDPAB_ORDER");
+  const bool natural = env && std::string(env) == "natural";
+  int nsdp = 0;
+  for (int b : p.blockStruct) nsdp += (b > 1) ? 1 : 0;
+  // a fill-reducing order pays only where the Schur pattern can be sparse:
+  // several SDP blocks and at least four 128-constraint tiles
+  if (!natural && nsdp >= 2 && p.m >= 4 * NBG && p.m <= 65536) {
+    const std::vector<std::vector<int>> groups = constraint_groups(p);
+    long long nat = 0, best = 0;
+    std::vector<int> order = best_constraint_order(groups, p.m, &nat, &best);
+    {
+      std::vector<int> pos(p.m);
+      for (int i = 0; i < p.m; ++i) pos[order[i]] = i;
+      if (best < nat) {
+        ProblemData q = p;
+        for (Entry& e : q.entries)
+          if (e.k >= 1 && e.k <= p.m) e.k = pos[e.k - 1] + 1;
+        for (int i = 0; i < p.m; ++i) q.c[i] = p.c[order[i]];
+        const int rc = setup_ordered(q, prm, kappa);
+        if (rc == SDPAB_OK) perm_ = order;
+        return rc;
+      }
+    }
+  }
+  return setup_ordered(p, prm, kappa);
+}
+
+int Solver::setup_ordered(const ProblemData& p, const Params& prm, double kappa)
 {
   release();
   int dev = 0;
@@ -1917,6 +2121,29 @@ int Solver::setup(const ProblemData& p, const Params& prm, double kappa)
 
 int Solver::solve(const InitPoint* init, const Params* prm)
 {
+  // in a fill-reducing constraint order: the initial x in that order, the
+  // result x back in the caller's
+  if (!perm_.empty()) {
+    InitPoint ip;
+    const InitPoint* ini = init;
+    if (init) {
+      ip = *init;
+      ip.xvec.assign(perm_.size(), 0.0);
+      for (size_t i = 0; i < perm_.size(); ++i)
+        if (perm_[i] < (int)init->xvec.size()) ip.xvec[i] = init->xvec[perm_[i]];
+      ini = &ip;
+    }
+    const std::vector<int> order = perm_;
+    perm_.clear();
+    const int rc = solve(ini, prm);
+    perm_ = order;
+    if (xvec_.size() == order.size()) {
+      std::vector<double> x(order.size());
+      for (size_t i = 0; i < order.size(); ++i) x[order[i]] = xvec_[i];
+      xvec_.swap(x);
+    }
+    return rc;
+  }
   if (d_ && prm) d_->prm = *prm;
   if (!d_) return set_error(SDPAB_ESTATE, "solve before initializeSolve");
   DevState& S = *d_;
@@ -2501,3 +2728,32 @@ int Solver::solve(const InitPoint* init, const Params* prm)
 }
 
 }  // namespace sdpab
+
+// The constraint order Solver::setup would use (host only, no device work):
+// order[position] = constraint (0-based), or the identity when the natural
+// order is kept; pairs[0] / pairs[1] = the symbolic tile pairs of the Schur
+// factorisation in the natural / the returned order.  Entries as for
+// sdpab_sdpa_input_problem (1-based k, l, i, j; k = 0 is F0).
+extern "C" SDPAB_API int sdpab_constraint_order(int m, int nblock, const int* block_struct, long long nnz,
+                                                const int* k, const int* l, const int* i, const int* j,
+                                                int* order, long long* pairs)
+{
+  if (m < 1 || nblock < 1 || nnz < 0 || !block_struct || !order || !pairs || (nnz > 0 && (!k || !l || !i || !j)))
+    return sdpab::set_error(SDPAB_EINVAL, "constraint_order: invalid arguments");
+  sdpab::ProblemData p;
+  p.m = m;
+  p.blockStruct.assign(block_struct, block_struct + nblock);
+  p.c.assign(m, 0.0);
+  for (long long t = 0; t < nnz; ++t) p.entries.push_back({k[t], l[t], i[t], j[t], 1.0});
+  const auto groups = sdpab::constraint_groups(p);
+  std::vector<int> ident(m);
+  for (int q = 0; q < m; ++q) ident[q] = q;
+  pairs[0] = sdpab::symbolic_tile_pairs(groups, ident, m);
+  int nsdp = 0;
+  for (int b : p.blockStruct) nsdp += (b > 1) ? 1 : 0;
+  std::vector<int> ord = ident;
+  pairs[1] = pairs[0];
+  if (nsdp >= 2 && m >= 4 * sdpab::NBG && m <= 65536) ord = sdpab::best_constraint_order(groups, m, nullptr, &pairs[1]);
+  std::copy(ord.begin(), ord.end(), order);
+  return SDPAB_OK;
+}

@@ -68,8 +68,14 @@ class Solver {
 
   // SDPA::initializeSolve (sdpa_solve.cpp:10-43): block layout, constraint
   // index, formula choice (computeFormula_SDP), device upload.  Returns an
-  // SDPAB_* status.
+  // SDPAB_* status.  For problems of several SDP blocks the constraints are
+  // first put in a fill-reducing order for the Schur factorisation (the
+  // reference leaves that to MUMPS's own ordering); the results are given
+  // back in the caller's order.
   int setup(const ProblemData& p, const Params& prm, double kappa);
+  // The constraint order of the last setup: internal position -> caller's
+  // constraint (0-based); empty when it is the caller's own order.
+  const std::vector<int>& constraint_order() const { return perm_; }
   // SDPA::solve (sdpa_solve.cpp:59-233); init may be NULL.  `prm` are the
   // parameters in force at the call (the reference reads its Parameter
   // object at solve time, so changes after initializeSolve apply); NULL
@@ -105,6 +111,8 @@ class Solver {
   long long tc_wait_ = -1;
   SolveStats stats_;
   std::vector<double> xvec_;
+  std::vector<int> perm_;  // internal constraint position -> caller's constraint
+  int setup_ordered(const ProblemData& p, const Params& prm, double kappa);
   std::vector<std::vector<double>> Xres_, Yres_;
 };
 

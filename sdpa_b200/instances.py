@@ -229,16 +229,20 @@ def random_block_sdp(m: int, blocks: list, density: float = 0.1, lp_per_constrai
 
 
 def block_arrow_sdp(nblk: int = 24, n: int = 8, m_per: int = 24, n_couple: int = 8, density: float = 0.3,
-                    seed: int = 1) -> Instance:
+                    seed: int = 1, shuffled: bool = False) -> Instance:
     """Many SDP blocks with a sparse Schur complement: m_per constraints touch
     only block b (b = 0 .. nblk-1, in order), then n_couple constraints touch
     two random blocks each, so the Schur matrix is block-diagonal with a
     dense border (an arrowhead).  Built like `random_block_sdp` (strictly
-    feasible from X = Y = I), no LP block."""
+    feasible from X = Y = I), no LP block.  shuffled: the constraints in a
+    seeded random order instead (the same problem up to the numbering, whose
+    Schur pattern in file order has no structure)."""
     rng = np.random.default_rng(seed)
     touch = [[b] for b in range(nblk) for _ in range(m_per)]
     for _ in range(n_couple):
         touch.append([int(x) for x in rng.choice(nblk, size=2, replace=False)])
+    if shuffled:
+        touch = [touch[t] for t in np.random.default_rng(seed + 1000).permutation(len(touch))]
     return random_block_sdp(len(touch), [n] * nblk, density, lp_per_constraint=0, seed=seed + 7, touch=touch,
                             name=f"block arrow sdp {nblk}x{n} m={len(touch)} seed {seed}")
 

@@ -114,3 +114,50 @@ def test_block_arrow_family_and_its_fixture():
     assert all(len(blk_of[k]) == 2 for k in range(24 * 24 + 1, it.m + 1))
     meta = json.load(open(os.path.join(GOLDEN, "arrow.json")))["arrow"]
     assert meta["phase"] == "pdOPT" and "restatement" in meta["source"]
+
+
+def _constraint_order(inst):
+    import ctypes
+    from sdpa_b200 import _native as N
+    m = inst.m
+    bs = np.asarray(inst.blocks, np.int32)
+    k, l, i, j = [np.ascontiguousarray(a, np.int32) for a in (inst.k, inst.l, inst.i, inst.j)]
+    out = np.zeros(m, np.int32)
+    pairs = np.zeros(2, np.int64)
+    rc = N.lib().sdpab_constraint_order(m, len(bs), bs.ctypes.data, len(k), k.ctypes.data, l.ctypes.data,
+                                        i.ctypes.data, j.ctypes.data, out.ctypes.data, pairs.ctypes.data)
+    assert rc == 0
+    return out, pairs
+
+
+def test_constraint_order_restores_the_arrowhead():
+    """The host solver's constraint order for the Schur factorisation (host
+    code, no device): a block-arrow problem whose constraints come in a
+    shuffled order has a dense symbolic tile pattern in that order; the
+    chosen order (the fewest tile pairs among minimum degree, the
+    group-count order and the caller's) is a permutation that brings back
+    the arrowhead: constraints local to one block contiguous, the coupling
+    ones last, and as few tile pairs as the problem in its generated order.
+    A single-block problem keeps the caller's order."""
+    from sdpa_b200 import instances
+    grouped = instances.block_arrow_sdp(nblk=200, m_per=40, n_couple=64)
+    shuffled = instances.block_arrow_sdp(nblk=200, m_per=40, n_couple=64, shuffled=True)
+    o_g, p_g = _constraint_order(grouped)
+    o_s, p_s = _constraint_order(shuffled)
+    assert sorted(o_s.tolist()) == list(range(shuffled.m))
+    assert p_s[0] > 10 * p_s[1], p_s
+    assert p_s[1] <= p_g[1] and p_g[1] <= p_g[0]
+    # which block each constraint touches (the coupling ones: two)
+    blocks_of = [set() for _ in range(shuffled.m)]
+    for kk, ll in zip(shuffled.k, shuffled.l):
+        if kk > 0:
+            blocks_of[kk - 1].add(int(ll))
+    seq = [blocks_of[c] for c in o_s]
+    n_local = sum(1 for b in seq if len(b) == 1)
+    assert all(len(b) == 1 for b in seq[:n_local]) and all(len(b) == 2 for b in seq[n_local:])
+    firsts = [min(b) for b in seq[:n_local]]
+    changes = sum(1 for a, b in zip(firsts, firsts[1:]) if a != b)
+    assert changes == 199  # each block's constraints contiguous
+    lt = instances.lovasz_theta(n=60, p=0.5, seed=1)
+    o_lt, p_lt = _constraint_order(lt)
+    assert np.array_equal(o_lt, np.arange(lt.m)) and p_lt[0] == p_lt[1]

@@ -251,3 +251,34 @@ def test_sparse_schur_on_a_block_arrow_problem(monkeypatch):
     assert not sparse2 and phase2 == "pdOPT" and iters2 == iters
     assert rel(pobj2, pobj) < 1e-9 and rel(dobj2, dobj) < 1e-9
     assert np.max(np.abs(x2 - x)) < 1e-7
+
+
+def test_constraint_order_on_a_shuffled_block_arrow(monkeypatch):
+    """A block-arrow problem with its constraints in a shuffled order: in
+    file order its symbolic Schur pattern is dense; the solver reorders the
+    constraints (minimum degree / arrowhead), takes the tile-sparse
+    factorisation, and returns x in the caller's order.  The result equals
+    the solve in the caller's order with the dense factorisation
+    (SDPAB_ORDER=natural, SDPAB_SCHUR=dense) to rounding."""
+    from sdpa_b200 import instances
+    from sdpa_b200.sdpa import SDPA
+    inst = instances.block_arrow_sdp(shuffled=True)
+    res = {}
+    for mode in ("ordered", "natural"):
+        if mode == "natural":
+            monkeypatch.setenv("SDPAB_ORDER", "natural")
+            monkeypatch.setenv("SDPAB_SCHUR", "dense")
+        else:
+            monkeypatch.delenv("SDPAB_ORDER", raising=False)
+            monkeypatch.delenv("SDPAB_SCHUR", raising=False)
+        s = SDPA()
+        s.inputProblem(inst)
+        s.solve()
+        res[mode] = (s.getPhaseString(), s.getIteration(), s.getPrimalObj(), s.getDualObj(),
+                     s.getResultXVec().copy(), s.schurPattern())
+    ph, it, po, do, x, (sparse, pairs, dense_pairs) = res["ordered"]
+    ph2, it2, po2, do2, x2, (sparse2, _, _) = res["natural"]
+    assert ph == ph2 == "pdOPT" and sparse and not sparse2 and pairs < 0.6 * dense_pairs
+    assert abs(it - it2) <= 1
+    assert rel(po, po2) < 1e-8 and rel(do, do2) < 1e-8
+    assert np.max(np.abs(x - x2)) < 1e-6
