@@ -16,16 +16,19 @@
 // Layout and schedule.  One warp (one block of 32 threads) per instance,
 // instances taken largest first from a work queue.  The warp keeps V in
 // shared memory (n rows of RL = 16 or 32 doubles) and F0's off-diagonal
-// entries in a global scratch laid out by rows (both triangles), as 16-byte
-// records (offset of the neighbour's V row, weight) built per instance from
-// the packed entries in a deterministic order.  The rows' neighbour lists,
-// sweep after sweep, form one periodic stream that the warp copies
-// (cp.async, 32 records at a time) into a ring in shared memory ahead of
-// the row being updated.  The lanes form H groups; each lane holds two
-// components of the row vector, each group takes every H-th neighbour, and
-// the groups' partial sums and the norm are combined by shuffles.  Rows run
-// in order (each update sees the rows updated before it), so an instance is
-// a chain of n row updates per sweep; instances run concurrently.
+// entries in a global scratch laid out as 16-byte records (offset of the
+// neighbour's V row, weight), built per instance from the packed entries in
+// a deterministic order.  The rows are greedily coloured (no two neighbours
+// share a colour) and updated colour by colour, in groups of up to H rows of
+// one colour at once: such rows do not read one another, so a group's
+// updates give exactly what updating its rows one after the other gives.
+// The groups' records, sweep after sweep, form one periodic stream that the
+// warp copies (cp.async, 32 records at a time) into a ring in shared memory
+// ahead of the group being updated.  Each group of RL / 2 lanes updates one
+// row, two components per lane: its neighbours one after another in two
+// FMA chains, then the norm by shuffles within the group and a reciprocal
+// square root.  An instance is a chain of about n / H group updates per
+// sweep; instances run concurrently.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
