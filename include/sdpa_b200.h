@@ -436,6 +436,8 @@ SDPAB_API int sdpab_batch_solve_noalloc(const sdpab_batch* prob, const sdpab_bat
  *   this form (its V is not written);
  *   order: DEVICE, [count] instance indices in the order warps take them
  *   (largest first balances the launch), or NULL for 0..count-1.
+ * Calls on different streams may run concurrently on disjoint instances
+ * (each call has its own work-queue counter; the row scratch is per entry).
  * One warp per instance, taken from a work queue; F0's off-diagonal entries are laid out by rows in a
  * library-owned scratch (2 * num_entries entries, kept between calls, freed
  * by sdpab_release_workspace).  SDPAB_ESIZE when one instance's factor does

@@ -258,20 +258,32 @@ class DeviceBatch:
         self._init_t = [conv(flag, np.int32), conv(xvec, np.float64), conv(X, np.float64), conv(Y, np.float64)]
         self.init = N.BatchInit(*[None if x is None else x.data_ptr() for x in self._init_t], margin)
 
+    def subset(self, order_tensor) -> "N.Batch":
+        """The batch struct restricted to the instances listed (device int32
+        tensor, in the order the solver takes them); pass it with that
+        tensor as `order` to solve only those."""
+        b = N.Batch.from_buffer_copy(self._bt)
+        b.count = int(order_tensor.numel())
+        return b
+
     def solve(self, params=None, precision=N.PREC_FP64, stream=None, ctas_per_sm=0, staging=0, block_threads=0,
-              mixed_products=0, mixed_switch_gap=0.0, refine_tol=0.0, factor_smem=0):
+              mixed_products=0, mixed_switch_gap=0.0, refine_tol=0.0, factor_smem=0, order=None):
         """block_threads / ctas_per_sm / staging: launch shape (0 = defaults;
         see sdpa_b200.autotune); mixed_products / mixed_switch_gap: options of
-        the mixed mode (sdpab_batch_config)."""
+        the mixed mode (sdpab_batch_config); order: a device int32 tensor of
+        instance indices to solve only those, in that order (default: all,
+        largest first)."""
         import torch
         prm = _params(params)
         cfg = _config(precision, ctas_per_sm, mixed_switch_gap, staging, mixed_products, block_threads, refine_tol,
                       factor_smem)
         s = stream if stream is not None else torch.cuda.current_stream()
-        N.check(N.lib().sdpab_batch_solve(ctypes.byref(self._bt),
+        bt = self._bt if order is None else self.subset(order)
+        od = self.order if order is None else order
+        N.check(N.lib().sdpab_batch_solve(ctypes.byref(bt),
                                           ctypes.byref(self.init) if self.init is not None else None,
                                           ctypes.byref(prm), ctypes.byref(cfg), ctypes.byref(self._br),
-                                          self.order.data_ptr(), s.cuda_stream), "sdpab_batch_solve")
+                                          od.data_ptr(), s.cuda_stream), "sdpab_batch_solve")
 
     def result(self) -> BatchResult:
         sc = self.sc.cpu().numpy()

@@ -430,10 +430,15 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
 
 // Row-layout records of F0's entries and the work-queue counter, per
 // device, kept between calls.
+// Each call takes the next of LR_QUEUES work-queue counters, so calls that
+// run concurrently on different streams (on disjoint instances) do not share
+// one.
+constexpr int LR_QUEUES = 1024;
 struct LrScratch {
   LrRec* rec = nullptr;
   int* queue = nullptr;
   long long cap = 0;
+  unsigned calls = 0;
   void release()
   {
     if (rec) cudaFree(rec);
@@ -490,13 +495,14 @@ extern "C" int sdpab_lowrank_factor(const sdpab_batch* prob, long long num_entri
   if (S.cap < need) {
     S.release();
     if (cudaMalloc((void**)&S.rec, need * sizeof(LrRec)) != cudaSuccess ||
-        cudaMalloc((void**)&S.queue, 256) != cudaSuccess) {
+        cudaMalloc((void**)&S.queue, LR_QUEUES * sizeof(int)) != cudaSuccess) {
       S.release();
       return set_error(SDPAB_ECUDA, "lowrank_factor: scratch allocation failed");
     }
     S.cap = need;
   }
-  cudaError_t e = cudaMemsetAsync(S.queue, 0, sizeof(int), (cudaStream_t)stream);
+  int* queue = S.queue + (S.calls++ % LR_QUEUES);
+  cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_error(e, "lowrank_factor: clearing the queue");
   auto kern = (RL == 16) ? k_mixing<16> : k_mixing<32>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -508,7 +514,7 @@ extern "C" int sdpab_lowrank_factor(const sdpab_batch* prob, long long num_entri
   if (bps < 1) return set_error(SDPAB_ESIZE, "lowrank_factor: the block does not fit on an SM");
   const int grid = (int)std::min<long long>(prob->count, (long long)sms * bps);
   kern<<<grid, 32, smem, (cudaStream_t)stream>>>(*prob, R, max_sweeps, tol, seed, num_entries, S.rec, V, sweeps,
-                                                 order, S.queue);
+                                                 order, queue);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "lowrank_factor: launch");
   return SDPAB_OK;

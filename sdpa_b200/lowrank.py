@@ -55,15 +55,21 @@ class FactorPipeline:
         db.init = N.BatchInit(self.flag.data_ptr(), None, None, None, 0.0, self.V.data_ptr(), self.rank,
                               float(init_mu))
 
-    def factor(self, stream=None):
+    def factor(self, stream=None, order=None):
+        """The factor of every instance (or of those in `order`)."""
         import torch
         s = stream if stream is not None else torch.cuda.current_stream()
-        N.check(N.lib().sdpab_lowrank_factor(ctypes.byref(self.db._bt), self.num_entries, self.rank,
+        od = self.order if order is None else order
+        bt = self.db._bt if order is None else self.db.subset(order)
+        N.check(N.lib().sdpab_lowrank_factor(ctypes.byref(bt), self.num_entries, self.rank,
                                              self.max_sweeps, self.tol, self.seed, self.V.data_ptr(),
-                                             self.sweeps.data_ptr(), self.order.data_ptr(), s.cuda_stream),
+                                             self.sweeps.data_ptr(), od.data_ptr(), s.cuda_stream),
                 "sdpab_lowrank_factor")
 
     def run(self, precision=N.PREC_FP64, stream=None, **shape):
-        """shape: launch shape and mixed-mode options of DeviceBatch.solve."""
+        """shape: launch shape and mixed-mode options of DeviceBatch.solve.
+        (Factoring the longest instances on a side stream while the rest
+        are solved was measured slower: those instances then finish the
+        solve alone.)"""
         self.factor(stream)
         self.db.solve(precision=precision, stream=stream, **shape)
