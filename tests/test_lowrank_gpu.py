@@ -165,3 +165,33 @@ def test_factor_start_other_forms_and_host_entry():
     hres = batch.solve_host(P, init=(flag, None, None, None, 0.0, fp.V.cpu().numpy(), fp.rank))
     assert np.array_equal(hres.iterations, res.iterations)
     assert np.array_equal(hres.primal_obj, res.primal_obj) and np.array_equal(hres.xvec, res.xvec)
+
+
+def test_subsets_solve_like_the_whole_batch():
+    """The factor and the solve of a batch in two instance subsets, on two
+    streams for the factor (each call has its own work-queue counter), give
+    bitwise the results of one call over the whole batch: every instance is
+    computed on its own."""
+    import torch
+    from sdpa_b200 import batch, instances, lowrank
+    P = batch.pack([instances.batch_maxcut(s, 20, 120) for s in range(64)])
+    dbw = batch.DeviceBatch(P)
+    fw = lowrank.FactorPipeline(dbw)
+    fw.run()
+    dbs = batch.DeviceBatch(P)
+    fs = lowrank.FactorPipeline(dbs)
+    o = fs.order.cpu().numpy()
+    a = torch.from_numpy(np.ascontiguousarray(o[::2])).cuda()
+    b = torch.from_numpy(np.ascontiguousarray(o[1::2])).cuda()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    fs.factor(side, a)
+    fs.factor(None, b)
+    torch.cuda.current_stream().wait_stream(side)
+    dbs.solve(order=b)
+    dbs.solve(order=a)
+    torch.cuda.synchronize()
+    assert torch.equal(fw.V, fs.V) and torch.equal(fw.sweeps, fs.sweeps)
+    rw, rs = dbw.result(), dbs.result()
+    assert np.array_equal(rw.iterations, rs.iterations) and np.array_equal(rw.primal_obj, rs.primal_obj)
+    assert np.array_equal(rw.xvec, rs.xvec)
