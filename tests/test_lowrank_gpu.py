@@ -164,14 +164,15 @@ def test_factor_start_other_forms_and_host_entry():
     flag = np.full(P.count, lowrank.INIT_FACTOR, np.int32)
     hres = batch.solve_host(P, init=(flag, None, None, None, 0.0, fp.V.cpu().numpy(), fp.rank))
     assert np.array_equal(hres.iterations, res.iterations)
-    assert np.array_equal(hres.primal_obj, res.primal_obj) and np.array_equal(hres.xvec, res.xvec)
+    assert np.max(np.abs(hres.primal_obj - res.primal_obj) / np.maximum(1.0, np.abs(res.primal_obj))) < 1e-12
+    assert np.max(np.abs(hres.xvec - res.xvec)) < 1e-9
 
 
 def test_subsets_solve_like_the_whole_batch():
     """The factor and the solve of a batch in two instance subsets, on two
     streams for the factor (each call has its own work-queue counter), give
-    bitwise the results of one call over the whole batch: every instance is
-    computed on its own."""
+    the results of one call over the whole batch: the factors bitwise, the
+    solves to rounding (every instance is computed on its own)."""
     import torch
     from sdpa_b200 import batch, instances, lowrank
     P = batch.pack([instances.batch_maxcut(s, 20, 120) for s in range(64)])
@@ -192,6 +193,9 @@ def test_subsets_solve_like_the_whole_batch():
     dbs.solve(order=a)
     torch.cuda.synchronize()
     assert torch.equal(fw.V, fs.V) and torch.equal(fw.sweeps, fs.sweeps)
+    # the solver's shared-memory accumulations may add in another order from
+    # one launch to the next: the same iterations, values to rounding
     rw, rs = dbw.result(), dbs.result()
-    assert np.array_equal(rw.iterations, rs.iterations) and np.array_equal(rw.primal_obj, rs.primal_obj)
-    assert np.array_equal(rw.xvec, rs.xvec)
+    assert np.array_equal(rw.iterations, rs.iterations)
+    assert np.max(np.abs(rw.primal_obj - rs.primal_obj) / np.maximum(1.0, np.abs(rw.primal_obj))) < 1e-12
+    assert np.max(np.abs(rw.xvec - rs.xvec)) < 1e-9
