@@ -312,7 +312,7 @@ typedef struct sdpab_batch_init {
                                   V + vec_off[q] * rank (may be NULL otherwise) */
   int rank;                    /* columns of V */
   double init_mu;              /* SDPAB_INIT_FACTOR: the smallest start mu relative to
-                                  mean |F0_ii| (0 = 3e-5) */
+                                  mean |F0_ii| (0 = 3e-6) */
 } sdpab_batch_init;
 
 typedef struct sdpab_batch_result {

@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
         zv = cta::block_sum<BT>(zv, RD);
         vv = cta::block_sum<BT>(vv, RD);
         const double rho = (vv > 0.0) ? sqrt(zv / vv) / cs : 0.0;
-        const double mu_s = fmax((a.init.init_mu > 0.0) ? a.init.init_mu : 3.0e-5, 3.0 * rho) * cs;
+        const double mu_s = fmax((a.init.init_mu > 0.0) ? a.init.init_mu : 3.0e-6, 3.0 * rho) * cs;
         const double tau = 0.3 * sqrt(mu_s * cs);
         // (Y + tau I)^-1 = (I - V M^-1 V^T) / tau, M = tau I + V^T V (R x R):
         // M = L L^T in W1, Li = L^-1 in LXi, U = V Li^T (n x R) in dX,

@@ -5,7 +5,7 @@ dual problem max <F0, Y> s.t. Y_ii = b_i, Y >= 0 is solved approximately in
 the factored form Y = V V^T by the mixing method (sdpab_lowrank_factor, one
 warp per instance), and the interior-point method starts near its central
 path from V (the SDPAB_INIT_FACTOR start of sdpab_batch_solve): the start is
-within about 3e-5 (relative) of optimal and centred, so the solve to a
+within about 3e-6 to 1e-4 (relative, by the factor's accuracy) of optimal and centred, so the solve to a
 relative gap of 1e-7 takes about three iterations instead of about
 fourteen from lambda* I.  The interior-point method still runs to its own
 tolerance; the factor only moves its starting point.  Nothing of this is in
@@ -23,9 +23,9 @@ import numpy as np
 from . import _native as N
 
 INIT_FACTOR = 3
-DEFAULT_SWEEPS = 150
+DEFAULT_SWEEPS = 220
 DEFAULT_TOL = 1e-10
-DEFAULT_MU = 3e-5
+DEFAULT_MU = 3e-6
 
 
 class FactorPipeline:
