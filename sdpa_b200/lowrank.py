@@ -4,10 +4,10 @@ For instances whose constraints are X_ii = b_i (one SDP block, m = n), the
 dual problem max <F0, Y> s.t. Y_ii = b_i, Y >= 0 is solved approximately in
 the factored form Y = V V^T by the mixing method (sdpab_lowrank_factor, one
 warp per instance), and the interior-point method starts near its central
-path from V (the SDPAB_INIT_FACTOR start of sdpab_batch_solve): the start is
-within about 3e-6 to 1e-4 (relative, by the factor's accuracy) of optimal and centred, so the solve to a
-relative gap of 1e-7 takes about three iterations instead of about
-fourteen from lambda* I.  The interior-point method still runs to its own
+path from V (the SDPAB_INIT_FACTOR start of sdpab_batch_solve): the start
+is centred and within 3e-6 to about 1e-4 (relative, set by the factor's
+accuracy) of optimal, so the solve to a relative gap of 1e-7 takes about
+three iterations instead of about fourteen from lambda* I.  The interior-point method still runs to its own
 tolerance; the factor only moves its starting point.  Nothing of this is in
 the reference, which starts from lambda* I or from a given point.
 
