@@ -7,9 +7,10 @@ warp per instance), and the interior-point method starts near its central
 path from V (the SDPAB_INIT_FACTOR start of sdpab_batch_solve): the start
 is centred and within 3e-6 to about 1e-4 (relative, set by the factor's
 accuracy) of optimal, so the solve to a relative gap of 1e-7 takes about
-three iterations instead of about fourteen from lambda* I.  The interior-point method still runs to its own
-tolerance; the factor only moves its starting point.  Nothing of this is in
-the reference, which starts from lambda* I or from a given point.
+three iterations instead of about fourteen from lambda* I.  The
+interior-point method still runs to its own tolerance; the factor only moves
+its starting point.  Nothing of this is in the reference, which starts from
+lambda* I or from a given point.
 
 `FactorPipeline` issues the factor and the solve on one stream, so the pair
 can be captured in one CUDA graph.

@@ -10,9 +10,10 @@
   from its epsilonStar = 1e-11 solution than the reference's own x (the
   bar of oracle.ref_runner.x_within_reference_accuracy) for all but 2 %;
   the median and 99th percentile of the distance to that solution no larger
-  than the reference's, the largest within 1.5 times the reference's; at most 1 % of the instances solved again from the standard
-  start (status 2); and the iterations cut to at most 4 on average (the
-  reference takes about 14).
+  than the reference's, the largest within 1.5 times the reference's; at
+  most 1 % of the instances solved again from the standard start (status
+  2); and the iterations cut to at most 4 on average (the reference takes
+  about 14).
 * Instances not of the form X_ii = b_i are reported (-1 sweeps) and solved
   from the standard start, and the host-pointer entry point takes the same
   start.
