@@ -57,10 +57,10 @@ def peaks():
 
 
 # DRAM bytes (read + write) of the headline solver launch (factor start,
-# mixed precision, 4096 instances), from one ncu capture of that launch
-# (profiles/batch_ipm_headline_maxcut4096.md): 15.75 GB read + 18.74 GB
-# written.  Other batch sizes are scaled by instances.
-TRAFFIC_BYTES_HEADLINE = 34.49e9
+# mixed precision, 4096 instances, 3.18 iterations), from one ncu capture of
+# that launch (profiles/batch_ipm_headline_maxcut4096.md): 14.28 GB read +
+# 17.00 GB written.  Other batch sizes are scaled by instances.
+TRAFFIC_BYTES_HEADLINE = 31.28e9
 TRAFFIC_COUNT = 4096
 TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4096-instance headline solver launch "
                 "(factor start, mixed), profiles/batch_ipm_headline_maxcut4096.md")
