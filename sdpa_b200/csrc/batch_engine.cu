@@ -643,9 +643,7 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
       bad = __syncthreads_or(bad);
       if (!bad) {
         const double* Vq = a.init.V + a.p.vec_off[inst] * R;
-        // X = Y = V V^T (V row-major n x R = column-major R x n, ld R)
-        cta::gemm_rect<BT, double, double>(n, n, R, true, Vq, R, false, Vq, R, X, n, 1.0, 0.0, gsm);
-        // C = -F0, its scale s and mu, tau
+        // C = -F0 and its scale s
         for (int t = tid; t < nn_i; t += BT) Z[t] = 0.0;
         __syncthreads();
         sp_axpy_block<BT>(er, ec, ev, mp[0], mp[1], -1.0, Z, n);
@@ -654,31 +652,35 @@ __global__ void __launch_bounds__(BT, 512 / BT) batch_ipm_fp64(BatchArgs a)
         for (int t = tid; t < n; t += BT) cs += fabs(Z[t + (size_t)n * t]);
         cs = cta::block_sum<BT>(cs, RD) / n;
         if (!(cs > 0.0)) cs = 1.0;
-        // (F0 Y)_ii = -sum_j C_ij Y_ij, one warp per row; y_k = -x_{row(k)}
-        {
-          const int lane = tid & 31, wid = tid >> 5;
-          for (int i = wid; i < n; i += BT / 32) {
-            double acc = 0.0;
-            for (int j = lane; j < n; j += 32) acc += Z[j + (size_t)n * i] * X[j + (size_t)n * i];
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) W2[i] = -acc;
-          }
-          __syncthreads();
-          for (int k = tid; k < m; k += BT) {
-            const int r = er[mp[k + 1]];
-            vy[k] = -W2[r] / bv[k];
-          }
-          __syncthreads();
+        // C V (n x R, in dX; V row-major n x R = column-major R x n, ld R):
+        // (F0 Y)_ii = -<v_i, (C V)_i> with Y = V V^T, so x_i = (F0 Y)_ii / b_i
+        // per row (in W1) and y_k = -x_{row(k)}
+        cta::gemm_rect<BT, double, double>(n, R, n, false, Z, n, true, Vq, R, dX, n, 1.0, 0.0, gsm);
+        for (int i = tid; i < n; i += BT) {
+          double acc = 0.0;
+          for (int k = 0; k < R; ++k) acc += Vq[(size_t)i * R + k] * dX[i + (size_t)n * k];
+          W2[i] = -acc;
         }
+        __syncthreads();
+        for (int k = tid; k < m; k += BT) {
+          const int r = er[mp[k + 1]];
+          const double xr = W2[r] / bv[k];
+          vy[k] = -xr;
+          W1[r] = xr;
+        }
+        __syncthreads();
         sp_axpy_constraints<BT>(er, ec, ev, mp, m, vy, -1.0, Z, n);  // Z = C - sum y_k A_k
         __syncthreads();
         // the factor's stationarity residual rho = |Z V| / (|V| s) (0 at the
-        // optimum) sets mu: a start closer than the factor's own error stalls
-        cta::gemm_rect<BT, double, double>(n, R, n, false, Z, n, true, Vq, R, dX, n, 1.0, 0.0, gsm);
+        // optimum; Z V = C V + diag(x) V) sets mu: a start closer than the
+        // factor's own error stalls
         double zv = 0.0, vv = 0.0;
         for (int t = tid; t < n * R; t += BT) {
-          zv += dX[t] * dX[t];
-          vv += Vq[t] * Vq[t];
+          const int i = t % n, k = t / n;
+          const double v = Vq[(size_t)i * R + k];
+          const double r = dX[t] + W1[i] * v;
+          zv += r * r;
+          vv += v * v;
         }
         zv = cta::block_sum<BT>(zv, RD);
         vv = cta::block_sum<BT>(vv, RD);
