@@ -428,7 +428,10 @@ SDPAB_API int sdpab_batch_solve_noalloc(const sdpab_batch* prob, const sdpab_bat
  * rows in order, from a seeded pseudo-random V.  Instance q uses
  * r_q = min(rank, ceil(sqrt(2 n_q)) + 1) columns (its other columns are
  * written as 0) and stops when a sweep changes sum_i <v_i, g_i> by at most
- * tol relative, or after max_sweeps sweeps.
+ * tol relative, or after max_sweeps sweeps, or, when sweep_work > 0, after
+ * sweep_work / (n + L) sweeps (L: the instance's off-diagonal entries of F0,
+ * counted in both triangles), which bounds the longest instances' share of
+ * the launch.
  *   prob: DEVICE batch; num_entries: length of its row / col / val arrays;
  *   rank: columns of V, 1..32 (0 = ceil(sqrt(2 nmax)) + 1, at most 32);
  *   V: DEVICE, [nvec * rank] doubles (instance q at V + vec_off[q] * rank);
@@ -443,8 +446,8 @@ SDPAB_API int sdpab_batch_solve_noalloc(const sdpab_batch* prob, const sdpab_bat
  * by sdpab_release_workspace).  SDPAB_ESIZE when one instance's factor does
  * not fit in shared memory (nmax * rank above about 24,000). */
 SDPAB_API int sdpab_lowrank_factor(const sdpab_batch* prob, long long num_entries, int rank, int max_sweeps,
-                                   double tol, unsigned long long seed, double* V, int* sweeps,
-                                   const int* order, void* stream);
+                                   double tol, long long sweep_work, unsigned long long seed, double* V,
+                                   int* sweeps, const int* order, void* stream);
 /* The rank sdpab_lowrank_factor uses for rank = 0. */
 SDPAB_API int sdpab_lowrank_default_rank(int nmax);
 

@@ -79,8 +79,8 @@ SIGNATURES = [
     ("sdpab_batch_solve_noalloc", c_int, [POINTER(Batch), POINTER(BatchInit), POINTER(Params),
                                           POINTER(BatchResult), c_void_p, c_void_p]),
     ("sdpab_workspace_bytes", c_longlong, []),
-    ("sdpab_lowrank_factor", c_int, [POINTER(Batch), c_longlong, c_int, c_int, c_double, ctypes.c_ulonglong,
-                                     c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sdpab_lowrank_factor", c_int, [POINTER(Batch), c_longlong, c_int, c_int, c_double, c_longlong,
+                                     ctypes.c_ulonglong, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sdpab_lowrank_default_rank", c_int, [c_int]),
     ("sdpab_mpnn_num_params", c_longlong, []),
     ("sdpab_mpnn_act_floats", c_longlong, [c_int]),

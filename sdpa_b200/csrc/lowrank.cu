@@ -123,7 +123,8 @@ __host__ __device__ inline int lr_rank_for(int n, int R)
 
 template <int RL>
 __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_sweeps, double tol,
-                                               unsigned long long seed, long long num_entries, LrRec* csr,
+                                               long long sweep_work, unsigned long long seed,
+                                               long long num_entries, LrRec* csr,
                                                double* V, int* sweeps, const int* order, int* queue)
 {
   extern __shared__ __align__(16) unsigned char lr_smem[];
@@ -349,7 +350,10 @@ __global__ void __launch_bounds__(32) k_mixing(sdpab_batch p, int R, int max_swe
     }
     double fold = 0.0;
     int s = 0;
-    while (s < max_sweeps) {
+    // at most max_sweeps sweeps, and at most sweep_work / (n + L) when set
+    int cap = max_sweeps;
+    if (sweep_work > 0) cap = (int)min((long long)cap, max(1LL, sweep_work / ((long long)n + L)));
+    while (s < cap) {
       double fl = 0.0;  // this lane's share of sum_i sqrt(b_i) |g_i|
       for (int g = 0; g < ng; ++g) {
         const int k0 = gs[g], k1 = gs[g + 1];
@@ -476,11 +480,11 @@ extern "C" int sdpab_lowrank_default_rank(int nmax)
 }
 
 extern "C" int sdpab_lowrank_factor(const sdpab_batch* prob, long long num_entries, int rank, int max_sweeps,
-                                    double tol, unsigned long long seed, double* V, int* sweeps, const int* order,
-                                    void* stream)
+                                    double tol, long long sweep_work, unsigned long long seed, double* V,
+                                    int* sweeps, const int* order, void* stream)
 {
   if (!prob || !V || !sweeps || prob->count < 0 || num_entries < 0 || rank < 0 || rank > LR_MAX_RANK ||
-      max_sweeps < 0 || !(tol >= 0.0))
+      max_sweeps < 0 || !(tol >= 0.0) || sweep_work < 0)
     return set_error(SDPAB_EINVAL, "lowrank_factor: invalid arguments");
   if (prob->count == 0) return SDPAB_OK;
   if (prob->nmax < 1) return set_error(SDPAB_EINVAL, "lowrank_factor: nmax must be positive");
@@ -513,8 +517,8 @@ extern "C" int sdpab_lowrank_factor(const sdpab_batch* prob, long long num_entri
   if (e != cudaSuccess) return cuda_error(e, "lowrank_factor: occupancy");
   if (bps < 1) return set_error(SDPAB_ESIZE, "lowrank_factor: the block does not fit on an SM");
   const int grid = (int)std::min<long long>(prob->count, (long long)sms * bps);
-  kern<<<grid, 32, smem, (cudaStream_t)stream>>>(*prob, R, max_sweeps, tol, seed, num_entries, S.rec, V, sweeps,
-                                                 order, queue);
+  kern<<<grid, 32, smem, (cudaStream_t)stream>>>(*prob, R, max_sweeps, tol, sweep_work, seed, num_entries, S.rec, V,
+                                                 sweeps, order, queue);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "lowrank_factor: launch");
   return SDPAB_OK;

@@ -35,7 +35,11 @@ class FactorPipeline:
     sweeps -1 and take the standard start (status 1)."""
 
     def __init__(self, db, rank: int = 0, max_sweeps: int = DEFAULT_SWEEPS, tol: float = DEFAULT_TOL,
-                 init_mu: float = DEFAULT_MU, seed: int = 1):
+                 init_mu: float = DEFAULT_MU, seed: int = 1, work_quantile: float = 0.0):
+        """work_quantile q in (0, 1]: the instances with more work per sweep
+        (rows plus neighbour records) than the q-quantile of the batch get
+        proportionally fewer sweeps, so that none takes longer than
+        max_sweeps sweeps of that quantile (0: no such cap)."""
         import torch
         self.db = db
         P = db.P
@@ -53,6 +57,10 @@ class FactorPipeline:
         cost = P.n.astype(np.int64) + 2 * f0.astype(np.int64)
         order = np.argsort(-cost, kind="stable").astype(np.int32)
         self.order = torch.from_numpy(order).to(dev)
+        # the kernel's n + L: rows plus off-diagonal records (both triangles)
+        work = 2 * f0.astype(np.int64) - P.n.astype(np.int64)
+        self.sweep_work = (int(self.max_sweeps * np.quantile(work, work_quantile))
+                           if 0.0 < work_quantile <= 1.0 and P.count > 0 else 0)
         db.init = N.BatchInit(self.flag.data_ptr(), None, None, None, 0.0, self.V.data_ptr(), self.rank,
                               float(init_mu))
 
@@ -63,7 +71,8 @@ class FactorPipeline:
         od = self.order if order is None else order
         bt = self.db._bt if order is None else self.db.subset(order)
         N.check(N.lib().sdpab_lowrank_factor(ctypes.byref(bt), self.num_entries, self.rank,
-                                             self.max_sweeps, self.tol, self.seed, self.V.data_ptr(),
+                                             self.max_sweeps, self.tol, self.sweep_work, self.seed,
+                                             self.V.data_ptr(),
                                              self.sweeps.data_ptr(), od.data_ptr(), s.cuda_stream),
                 "sdpab_lowrank_factor")
 
